@@ -1,0 +1,235 @@
+// C ABI of the evoc kNN-graph engine: argument checks, reference defaults,
+// device buffers, and dispatch to the kernels of each form.
+//
+// The host logic restates knn_graph_impl (src/knn.rs:377-454): the error
+// order (k == 0 before n == 0), the k clamp max(1, min(k, n-1)), f32
+// renormalisation (prepare_float), then the search and the per-dtype distance
+// transform (fused into the kernels' epilogues).
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "../../include/evoc_gpu.h"
+#include "common.cuh"
+#include "kernels.h"
+
+namespace {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  cudaError_t ensure(size_t want) {
+    if (want <= bytes) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    size_t grow = want + want / 8;
+    cudaError_t e = cudaMalloc(&p, grow);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return e;
+    }
+    bytes = grow;
+    return cudaSuccess;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+}  // namespace
+
+struct evoc_gpu_ctx {
+  int device = 0;
+  int sms = 148;
+  cudaStream_t stream = nullptr;
+  std::mutex mu;
+  std::string err;
+  DevBuf x, scratch, norms, flag, out_idx, out_raw, out_dist;
+};
+
+namespace {
+
+int fail(evoc_gpu_ctx* ctx, int code, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+  return code;
+}
+
+int cuda_fail(evoc_gpu_ctx* ctx, cudaError_t e, const char* where) {
+  std::string m = std::string(where) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+  return fail(ctx, e == cudaErrorMemoryAllocation ? EVOC_ERR_OOM : EVOC_ERR_CUDA, m);
+}
+
+#define EVOC_TRY(expr, where)                    \
+  do {                                           \
+    cudaError_t _e = (expr);                     \
+    if (_e != cudaSuccess) return cuda_fail(ctx, _e, where); \
+  } while (0)
+
+inline int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
+
+int resolve_form(int32_t dtype, int32_t form) {
+  if (form == EVOC_FORM_AUTO) return dtype == EVOC_DTYPE_F32 ? EVOC_FORM_BF16_RERANK : EVOC_FORM_EXACT_INT;
+  return form;
+}
+
+// Copies the caller's rows into a zero-padded device matrix of `ld` elements per row.
+int stage_rows(evoc_gpu_ctx* ctx, const void* data, int64_t n, int64_t row_bytes, int64_t ld_bytes, bool on_device) {
+  EVOC_TRY(ctx->x.ensure(size_t(n * ld_bytes)), "alloc rows");
+  if (ld_bytes != row_bytes) EVOC_TRY(cudaMemsetAsync(ctx->x.p, 0, size_t(n * ld_bytes), ctx->stream), "memset rows");
+  EVOC_TRY(cudaMemcpy2DAsync(ctx->x.p, size_t(ld_bytes), data, size_t(row_bytes), size_t(row_bytes), size_t(n),
+                             on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream),
+           "upload rows");
+  return EVOC_OK;
+}
+
+int knn_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtype, const void* data, int64_t n,
+             int64_t dim, int32_t k, const int64_t* rng_state, int32_t* out_idx, float* out_dist, float* out_raw,
+             int32_t* out_k) {
+  if (!ctx) return EVOC_ERR_ARG;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  ctx->err.clear();
+  evoc_gpu_opts opts;
+  evoc_gpu_default_opts(&opts);
+  if (opts_in) {
+    if (opts_in->struct_size != sizeof(evoc_gpu_opts)) return fail(ctx, EVOC_ERR_ARG, "opts.struct_size mismatch");
+    opts = *opts_in;
+  }
+  (void)rng_state;
+  if (k <= 0) return fail(ctx, EVOC_ERR_K, "n_neighbors must be positive");
+  if (n <= 0) return fail(ctx, EVOC_ERR_EMPTY, "empty embedding matrix");
+  if (!data || !out_idx) return fail(ctx, EVOC_ERR_ARG, "null data or out_idx");
+  if (dim <= 0) return fail(ctx, EVOC_ERR_ARG, "dim must be positive");
+  if (dtype < EVOC_DTYPE_F32 || dtype > EVOC_DTYPE_U8) return fail(ctx, EVOC_ERR_ARG, "unknown dtype");
+  if (n >= (int64_t(1) << 31) - 1) return fail(ctx, EVOC_ERR_ARG, "n exceeds int32 index range");
+  int64_t kk = k < n - 1 ? k : n - 1;
+  if (kk < 1) kk = 1;
+  const int keff = int(kk);
+  if (out_k) *out_k = keff;
+  const int form = resolve_form(dtype, opts.form);
+  const bool on_dev = opts.buffers_on_device != 0;
+  EVOC_TRY(cudaSetDevice(ctx->device), "cudaSetDevice");
+
+  // Output staging.
+  int32_t* d_idx = out_idx;
+  float* d_dist = out_dist;
+  float* d_raw = out_raw;
+  const size_t out_elems = size_t(n) * size_t(keff);
+  if (!on_dev) {
+    EVOC_TRY(ctx->out_idx.ensure(out_elems * 4), "alloc out_idx");
+    EVOC_TRY(ctx->out_dist.ensure(out_elems * 4), "alloc out_dist");
+    d_idx = ctx->out_idx.as<int32_t>();
+    d_dist = out_dist ? ctx->out_dist.as<float>() : nullptr;
+    if (out_raw) {
+      EVOC_TRY(ctx->out_raw.ensure(out_elems * 4), "alloc out_raw");
+      d_raw = ctx->out_raw.as<float>();
+    }
+  }
+
+  if (dtype == EVOC_DTYPE_F32) {
+    if (form != EVOC_FORM_FP32)
+      return fail(ctx, EVOC_ERR_UNSUPPORTED, "form not built for f32 in this library");
+    const int ld = int(round_up(dim, 16));
+    int rc = stage_rows(ctx, data, n, dim * 4, int64_t(ld) * 4, on_dev);
+    if (rc) return rc;
+    EVOC_TRY(ctx->norms.ensure(size_t(n) * 4), "alloc norms");
+    EVOC_TRY(ctx->flag.ensure(64), "alloc flag");
+    EVOC_TRY(evoc::launch_prepare_float(ctx->x.as<float>(), n, ld, int(dim), ctx->norms.as<float>(),
+                                        ctx->flag.as<int>(), ctx->sms, ctx->stream),
+             "prepare_float");
+    const int cap = evoc::topk_capacity(keff);
+    const int64_t qblocks = (n + 127) / 128;
+    const int grid = int(qblocks < int64_t(ctx->sms) * 2 ? qblocks : int64_t(ctx->sms) * 2);
+    EVOC_TRY(ctx->scratch.ensure(size_t(grid) * 128 * size_t(cap) * 8), "alloc scratch");
+    EVOC_TRY(evoc::launch_knn_f32_simt(ctx->x.as<float>(), n, ld, keff, cap, ctx->scratch.as<uint64_t>(), grid, d_idx,
+                                       d_raw, d_dist, 0, n, ctx->stream),
+             "knn_f32_simt");
+  } else {
+    return fail(ctx, EVOC_ERR_UNSUPPORTED, "dtype form not built in this library");
+  }
+
+  if (!on_dev) {
+    EVOC_TRY(cudaMemcpyAsync(out_idx, d_idx, out_elems * 4, cudaMemcpyDeviceToHost, ctx->stream), "download idx");
+    if (out_dist)
+      EVOC_TRY(cudaMemcpyAsync(out_dist, d_dist, out_elems * 4, cudaMemcpyDeviceToHost, ctx->stream),
+               "download dist");
+    if (out_raw)
+      EVOC_TRY(cudaMemcpyAsync(out_raw, d_raw, out_elems * 4, cudaMemcpyDeviceToHost, ctx->stream), "download raw");
+  }
+  EVOC_TRY(cudaStreamSynchronize(ctx->stream), "knn_graph");
+  return EVOC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int evoc_gpu_version(void) { return 100; }
+
+void evoc_gpu_default_opts(evoc_gpu_opts* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->struct_size = sizeof(evoc_gpu_opts);
+  o->form = EVOC_FORM_AUTO;
+  o->oversample = 2;
+  o->buffers_on_device = 0;
+  o->deterministic = 0;
+  o->n_iters = 0;
+  o->max_candidates = 0;
+  o->delta = 0.001f;
+  o->delta_improv = 0.001f;
+}
+
+int evoc_gpu_ctx_create(int device, evoc_gpu_ctx** out) {
+  if (!out) return EVOC_ERR_ARG;
+  *out = nullptr;
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) return EVOC_ERR_CUDA;
+  if (device < 0 || device >= count) return EVOC_ERR_ARG;
+  e = cudaSetDevice(device);
+  if (e != cudaSuccess) return EVOC_ERR_CUDA;
+  evoc_gpu_ctx* ctx = new evoc_gpu_ctx();
+  ctx->device = device;
+  cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device);
+  e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete ctx;
+    return EVOC_ERR_CUDA;
+  }
+  *out = ctx;
+  return EVOC_OK;
+}
+
+void evoc_gpu_ctx_destroy(evoc_gpu_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  DevBuf* bufs[] = {&ctx->x, &ctx->scratch, &ctx->norms, &ctx->flag, &ctx->out_idx, &ctx->out_raw, &ctx->out_dist};
+  for (DevBuf* b : bufs) b->release();
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+const char* evoc_gpu_last_error(const evoc_gpu_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int evoc_gpu_knn_graph(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts, int32_t dtype, const void* data, int64_t n,
+                       int64_t dim, int32_t k, const int64_t* rng_state, int32_t* out_idx, float* out_dist,
+                       int32_t* out_k) {
+  return knn_impl(ctx, opts, dtype, data, n, dim, k, rng_state, out_idx, out_dist, nullptr, out_k);
+}
+
+int evoc_gpu_knn_graph_raw(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts, int32_t dtype, const void* data,
+                           int64_t n, int64_t dim, int32_t k, const int64_t* rng_state, int32_t* out_idx,
+                           float* out_dist, float* out_raw, int32_t* out_k) {
+  return knn_impl(ctx, opts, dtype, data, n, dim, k, rng_state, out_idx, out_dist, out_raw, out_k);
+}
+
+}  // extern "C"

@@ -1,0 +1,74 @@
+// Input preparation on the device.
+//
+// prepare_float (src/knn.rs:78-113): if any row's L2 norm differs from 1 by
+// more than 1e-5, every row is divided by its norm (a zero norm divides by 1).
+// The norm is the serial f32 sum of squares followed by sqrt, exactly as the
+// reference rounds it: each product and each partial sum is rounded on its
+// own (no FMA contraction), sqrt and division are IEEE.  One thread owns one
+// row; rows are staged through shared memory in 32-column slabs so the
+// global reads stay coalesced.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace evoc {
+
+namespace {
+constexpr int kRows = 128;
+constexpr int kSlab = 32;
+}
+
+__global__ void __launch_bounds__(kRows)
+row_norms_kernel(const float* __restrict__ X, int64_t n, int ld, int d, float* __restrict__ norms,
+                 int* __restrict__ not_unit) {
+  __shared__ float slab[kRows][kSlab + 1];
+  const int64_t r0 = int64_t(blockIdx.x) * kRows;
+  const int tid = threadIdx.x;
+  float acc = 0.0f;
+  for (int c0 = 0; c0 < d; c0 += kSlab) {
+    // cooperative coalesced load: 128 rows x 32 columns
+    for (int e = tid; e < kRows * kSlab; e += kRows) {
+      const int r = e / kSlab, c = e % kSlab;
+      const int64_t g = r0 + r;
+      slab[r][c] = (g < n && c0 + c < d) ? X[g * ld + c0 + c] : 0.0f;
+    }
+    __syncthreads();
+    const int lim = min(kSlab, d - c0);
+    for (int c = 0; c < lim; c++) {
+      const float v = slab[tid][c];
+      acc = __fadd_rn(acc, __fmul_rn(v, v));
+    }
+    __syncthreads();
+  }
+  const int64_t row = r0 + tid;
+  if (row < n) {
+    const float nrm = __fsqrt_rn(acc);
+    norms[row] = nrm;
+    if (fabsf(__fsub_rn(nrm, 1.0f)) > 1e-5f) atomicOr(not_unit, 1);
+  }
+}
+
+__global__ void normalize_rows_kernel(float* __restrict__ X, int64_t n, int ld, int d,
+                                      const float* __restrict__ norms, const int* __restrict__ not_unit) {
+  if (*not_unit == 0) return;
+  const int64_t total = n * int64_t(d);
+  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t r = e / d, c = e % d;
+    float nrm = norms[r];
+    if (nrm == 0.0f) nrm = 1.0f;
+    X[r * ld + c] = __fdiv_rn(X[r * ld + c], nrm);
+  }
+}
+
+cudaError_t launch_prepare_float(float* X, int64_t n, int ld, int d, float* norms, int* not_unit, int sms,
+                                 cudaStream_t stream) {
+  cudaError_t e = cudaMemsetAsync(not_unit, 0, sizeof(int), stream);
+  if (e != cudaSuccess) return e;
+  const int64_t blocks = (n + kRows - 1) / kRows;
+  row_norms_kernel<<<unsigned(blocks), kRows, 0, stream>>>(X, n, ld, d, norms, not_unit);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  normalize_rows_kernel<<<sms * 8, 256, 0, stream>>>(X, n, ld, d, norms, not_unit);
+  return cudaGetLastError();
+}
+
+}  // namespace evoc

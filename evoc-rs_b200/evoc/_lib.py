@@ -1,0 +1,142 @@
+"""Loader for libevoc_gpu.so (the C ABI declared in include/evoc_gpu.h).
+
+There is no CPU fallback: if the library is missing or no CUDA device is
+present, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import threading
+
+PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_ROOT, "libevoc_gpu.so")
+HEADER_PATH = os.path.join(os.path.dirname(PKG_ROOT), "include", "evoc_gpu.h")
+
+EVOC_OK = 0
+EVOC_ERR_EMPTY = 1
+EVOC_ERR_K = 2
+EVOC_ERR_ARG = 3
+EVOC_ERR_OOM = 4
+EVOC_ERR_TIMEOUT = 5
+EVOC_ERR_CUDA = 6
+EVOC_ERR_UNSUPPORTED = 7
+EVOC_ERR_CANCELLED = 8
+EVOC_ERR_PENDING = 9
+
+DTYPE_F32, DTYPE_I8, DTYPE_U8 = 0, 1, 2
+FORM_AUTO, FORM_FP32, FORM_BF16_RERANK, FORM_EXACT_INT, FORM_NNDESCENT = 0, 1, 2, 3, 4
+FORM_NAMES = {"auto": FORM_AUTO, "fp32": FORM_FP32, "bf16_rerank": FORM_BF16_RERANK,
+              "exact_int": FORM_EXACT_INT, "nndescent": FORM_NNDESCENT}
+
+
+class Opts(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_uint32),
+        ("form", C.c_int32),
+        ("oversample", C.c_int32),
+        ("buffers_on_device", C.c_int32),
+        ("deterministic", C.c_int32),
+        ("n_iters", C.c_int32),
+        ("max_candidates", C.c_int32),
+        ("delta", C.c_float),
+        ("delta_improv", C.c_float),
+        ("reserved", C.c_int32 * 8),
+    ]
+
+
+_lib = None
+_lock = threading.Lock()
+
+
+def build() -> None:
+    """Compile libevoc_gpu.so in-tree for sm_100a (nvcc cross-compiles without a GPU)."""
+    subprocess.check_call(["make", "-s", "-C", PKG_ROOT, "-j8"])
+
+
+def lib():
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(f"libevoc_gpu.so not built at {LIB_PATH}; run build()")
+            L = C.CDLL(LIB_PATH)
+            P = C.c_void_p
+            i32, i64 = C.c_int32, C.c_int64
+            L.evoc_gpu_version.restype = C.c_int
+            L.evoc_gpu_default_opts.argtypes = [C.POINTER(Opts)]
+            L.evoc_gpu_ctx_create.argtypes = [C.c_int, C.POINTER(P)]
+            L.evoc_gpu_ctx_destroy.argtypes = [P]
+            L.evoc_gpu_last_error.argtypes = [P]
+            L.evoc_gpu_last_error.restype = C.c_char_p
+            L.evoc_gpu_knn_graph.argtypes = [P, C.POINTER(Opts), i32, P, i64, i64, i32, P, P, P, C.POINTER(i32)]
+            L.evoc_gpu_knn_graph_raw.argtypes = [P, C.POINTER(Opts), i32, P, i64, i64, i32, P, P, P, P,
+                                                 C.POINTER(i32)]
+            _bind_optional(L)
+            _lib = L
+    return _lib
+
+
+def _bind_optional(L) -> None:
+    """Signatures of entry points added by later parts of the library."""
+    P = C.c_void_p
+    i32, i64 = C.c_int32, C.c_int64
+    if hasattr(L, "evoc_gpu_fuzzy_graph"):
+        L.evoc_gpu_fuzzy_graph.argtypes = [P, P, P, i64, i32, C.c_float, i32, i32, P, P, P, P, P, i64,
+                                           C.POINTER(i64)]
+    if hasattr(L, "evoc_gpu_smooth_knn_dist"):
+        L.evoc_gpu_smooth_knn_dist.argtypes = [P, P, i64, i32, C.c_float, i32, P, P]
+
+
+def header_symbols() -> list[str]:
+    """Function names declared in include/evoc_gpu.h."""
+    import re
+
+    src = open(HEADER_PATH).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(evoc_gpu_[a-z0-9_]+)\s*\(", src)))
+
+
+def default_opts() -> Opts:
+    o = Opts()
+    lib().evoc_gpu_default_opts(C.byref(o))
+    return o
+
+
+class Context:
+    """One evoc_gpu_ctx (a CUDA stream plus scratch on one device)."""
+
+    def __init__(self, device: int = 0):
+        self.h = C.c_void_p()
+        rc = lib().evoc_gpu_ctx_create(device, C.byref(self.h))
+        if rc != EVOC_OK:
+            raise RuntimeError(f"evoc_gpu_ctx_create(device={device}) failed with status {rc}")
+        self.device = device
+
+    def last_error(self) -> str:
+        return lib().evoc_gpu_last_error(self.h).decode()
+
+    def close(self) -> None:
+        if self.h:
+            lib().evoc_gpu_ctx_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_contexts: dict[int, Context] = {}
+
+
+def context(device: int = 0) -> Context:
+    with _lock:
+        ctx = _contexts.get(device)
+    if ctx is None:
+        ctx = Context(device)
+        with _lock:
+            _contexts[device] = ctx
+    return ctx

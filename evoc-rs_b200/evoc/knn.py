@@ -1,0 +1,225 @@
+"""kNN graph construction on the GPU: the host-side mirror of evoc-rs src/knn.rs.
+
+Names, argument meaning and error behaviour follow the reference:
+  EmbeddingData      src/knn.rs:16-30
+  KnnError           src/knn.rs:32-41
+  KnnGraphOptions    src/knn.rs:44-76
+  knn_graph          src/knn.rs:345-359   (-> evoc_gpu_knn_graph)
+  knn_graph_ref      src/knn.rs:365-375
+The search itself runs in libevoc_gpu.so; this module only marshals arrays
+and keeps the reference's RNG draw contract: knn_graph advances the caller's
+NumPy RandomState by randint3_for_tau() (3 draws, src/numpy_rng.rs:204-212)
+and, unless the integer brute-force branch applies, by the 3*n_trees forest
+draws of make_forest (src/knn.rs:124-129), so code that consumes the RNG
+afterwards sees the same state as with the CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+
+INT32_MIN = -(2**31) + 1  # i32::MIN + 1, src/knn.rs:11
+INT32_MAX = 2**31 - 2     # i32::MAX - 1, src/knn.rs:12
+
+
+class KnnError(Exception):
+    """Mirror of KnnError (src/knn.rs:32-41)."""
+
+
+class EmptyData(KnnError):
+    def __init__(self):
+        super().__init__("empty embedding matrix")
+
+
+class InvalidNeighbors(KnnError):
+    def __init__(self):
+        super().__init__("n_neighbors must be positive")
+
+
+class BackendError(KnnError):
+    """A failure inside the GPU backend (CUDA error, out of memory, unsupported form)."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"evoc_gpu status {status}: {message}")
+        self.status = status
+
+
+class EmbeddingData:
+    """Tagged embedding matrix (src/knn.rs:16-20): Float32, Int8 or UInt8 (alias Binary)."""
+
+    __slots__ = ("kind", "array")
+
+    def __init__(self, kind: str, array: np.ndarray):
+        want = {"Float32": np.float32, "Int8": np.int8, "UInt8": np.uint8}[kind]
+        array = np.asarray(array)
+        if array.ndim != 2:
+            raise ValueError("embedding must be a 2-D array")
+        if array.dtype != want:
+            raise TypeError(f"{kind} expects dtype {np.dtype(want)}, got {array.dtype}")
+        self.kind = kind
+        self.array = array
+
+    @classmethod
+    def Float32(cls, a):
+        return cls("Float32", a)
+
+    @classmethod
+    def Int8(cls, a):
+        return cls("Int8", a)
+
+    @classmethod
+    def UInt8(cls, a):
+        return cls("UInt8", a)
+
+    Binary = UInt8
+
+    @classmethod
+    def wrap(cls, a) -> "EmbeddingData":
+        if isinstance(a, EmbeddingData):
+            return a
+        a = np.asarray(a)
+        kind = {np.dtype(np.float32): "Float32", np.dtype(np.int8): "Int8", np.dtype(np.uint8): "UInt8"}.get(a.dtype)
+        if kind is None:
+            raise TypeError(f"unsupported embedding dtype {a.dtype}")
+        return cls(kind, a)
+
+    def nrows(self) -> int:
+        return int(self.array.shape[0])
+
+    @property
+    def dtype_code(self) -> int:
+        return {"Float32": _lib.DTYPE_F32, "Int8": _lib.DTYPE_I8, "UInt8": _lib.DTYPE_U8}[self.kind]
+
+
+@dataclass
+class KnnGraphOptions:
+    """KnnGraphOptions (src/knn.rs:44-76) plus the GPU form selection."""
+
+    n_neighbors: int = 30
+    n_trees: Optional[int] = None
+    leaf_size: Optional[int] = None
+    max_candidates: Optional[int] = None
+    max_rptree_depth: int = 200
+    n_iters: Optional[int] = None
+    delta: float = 0.001
+    delta_improv: float = 0.001
+    use_sorted_updates: bool = True
+    brute_force_max_n: int = 0
+    deterministic: bool = False
+    # GPU-only fields
+    form: str = "auto"          # auto | fp32 | bf16_rerank | exact_int | nndescent
+    oversample: int = 2         # bf16_rerank: candidates per row = oversample * k
+    device: int = 0
+
+
+def _n_trees(options: KnnGraphOptions) -> int:
+    if options.n_trees is not None:
+        return options.n_trees
+    threads = 1 if options.deterministic else (os.cpu_count() or 1)
+    return max(4, min(8, threads))
+
+
+def _to_opts(options: KnnGraphOptions, on_device: bool = False) -> _lib.Opts:
+    o = _lib.default_opts()
+    o.form = _lib.FORM_NAMES[options.form]
+    o.oversample = int(options.oversample)
+    o.buffers_on_device = 1 if on_device else 0
+    o.deterministic = 1 if options.deterministic else 0
+    o.n_iters = int(options.n_iters or 0)
+    o.max_candidates = int(options.max_candidates or 0)
+    o.delta = float(options.delta)
+    o.delta_improv = float(options.delta_improv)
+    return o
+
+
+def _advance_rng(rng, data: EmbeddingData, options: KnnGraphOptions) -> np.ndarray:
+    """The reference's draws: randint3_for_tau, then make_forest's 3*n_trees."""
+    tau = np.array([rng.randint(INT32_MIN, INT32_MAX) for _ in range(3)], dtype=np.int64)
+    n = data.nrows()
+    brute = n <= options.brute_force_max_n and data.kind != "Float32"
+    if not brute:
+        for _ in range(3 * _n_trees(options)):
+            rng.randint(INT32_MIN, INT32_MAX)
+    return tau
+
+
+def _raise_for(status: int, ctx: _lib.Context) -> None:
+    if status == _lib.EVOC_OK:
+        return
+    if status == _lib.EVOC_ERR_EMPTY:
+        raise EmptyData()
+    if status == _lib.EVOC_ERR_K:
+        raise InvalidNeighbors()
+    raise BackendError(status, ctx.last_error())
+
+
+def knn_graph(data, options: KnnGraphOptions, rng=None, *, return_raw: bool = False):
+    """Build the kNN graph on the GPU.  Returns (indices int32 (n,k), distances f32 (n,k))."""
+    data = EmbeddingData.wrap(data)
+    if options.n_neighbors <= 0:
+        raise InvalidNeighbors()
+    if data.nrows() == 0:
+        raise EmptyData()
+    tau = _advance_rng(rng, data, options) if rng is not None else np.zeros(3, np.int64)
+    arr = np.ascontiguousarray(data.array)
+    n, dim = arr.shape
+    k = max(1, min(options.n_neighbors, n - 1))
+    ctx = _lib.context(options.device)
+    o = _to_opts(options)
+    ind = np.empty((n, k), np.int32)
+    dst = np.empty((n, k), np.float32)
+    raw = np.empty((n, k), np.float32) if return_raw else None
+    kout = C.c_int32(0)
+    P = C.c_void_p
+    if return_raw:
+        st = _lib.lib().evoc_gpu_knn_graph_raw(ctx.h, C.byref(o), data.dtype_code, arr.ctypes.data_as(P), n, dim,
+                                              int(options.n_neighbors), tau.ctypes.data_as(P),
+                                              ind.ctypes.data_as(P), dst.ctypes.data_as(P), raw.ctypes.data_as(P),
+                                              C.byref(kout))
+    else:
+        st = _lib.lib().evoc_gpu_knn_graph(ctx.h, C.byref(o), data.dtype_code, arr.ctypes.data_as(P), n, dim,
+                                          int(options.n_neighbors), tau.ctypes.data_as(P), ind.ctypes.data_as(P),
+                                          dst.ctypes.data_as(P), C.byref(kout))
+    _raise_for(st, ctx)
+    assert kout.value == k
+    return (ind, dst, raw) if return_raw else (ind, dst)
+
+
+def knn_graph_ref(data, options: KnnGraphOptions, rng=None):
+    """Same as knn_graph; the GPU path never takes ownership of the caller's array."""
+    return knn_graph(data, options, rng)
+
+
+def knn_graph_device(ptr: int, dtype_code: int, n: int, dim: int, k: int, out_idx_ptr: int, out_dist_ptr: int,
+                     options: Optional[KnnGraphOptions] = None, tau: Optional[np.ndarray] = None,
+                     out_raw_ptr: int = 0) -> int:
+    """Device-pointer entry: all buffers live on the context's GPU (e.g. torch tensors)."""
+    options = options or KnnGraphOptions(n_neighbors=k)
+    ctx = _lib.context(options.device)
+    o = _to_opts(options, on_device=True)
+    tau = np.zeros(3, np.int64) if tau is None else np.ascontiguousarray(tau, np.int64)
+    kout = C.c_int32(0)
+    P = C.c_void_p
+    st = _lib.lib().evoc_gpu_knn_graph_raw(ctx.h, C.byref(o), dtype_code, P(ptr), n, dim, k, tau.ctypes.data_as(P),
+                                          P(out_idx_ptr), P(out_dist_ptr) if out_dist_ptr else None,
+                                          P(out_raw_ptr) if out_raw_ptr else None, C.byref(kout))
+    _raise_for(st, ctx)
+    return kout.value
+
+
+def transform_distances_float(distances: np.ndarray) -> np.ndarray:
+    """transform_distances_float (src/knn.rs:156-171), host-side helper."""
+    d = np.asarray(distances, np.float32)
+    out = np.zeros_like(d)
+    neg = d < 0
+    sim = (-d[neg]).astype(np.float64)
+    with np.errstate(divide="ignore"):
+        v = np.where(sim >= 1.0, 0.0, np.maximum(-np.log2(sim), 0.0))
+    out[neg] = v.astype(np.float32)
+    return out

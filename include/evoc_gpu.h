@@ -1,0 +1,117 @@
+/*
+ * evoc_gpu.h -- C ABI of the B200 kNN-graph engine for evoc.
+ *
+ * Plain pointers and sizes only.  Every entry point returns an evoc_status;
+ * evoc_gpu_last_error() gives the message of the last failure on a context.
+ * Entry points are synchronous: they return after the results are written.
+ * A context owns one CUDA stream and its scratch memory; calls on one context
+ * are serialised by the context, calls on different contexts may overlap.
+ *
+ * Each declaration cites the evoc-rs interface it replaces (paths relative to
+ * the evoc-rs source tree).
+ */
+#ifndef EVOC_GPU_H
+#define EVOC_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  1 and 2 are KnnError::{EmptyData, InvalidNeighbors}
+ * (src/knn.rs:32-41); the rest are conditions the CPU path never meets. */
+typedef enum {
+  EVOC_OK = 0,
+  EVOC_ERR_EMPTY = 1,       /* n == 0                                   */
+  EVOC_ERR_K = 2,           /* k == 0                                   */
+  EVOC_ERR_ARG = 3,         /* null pointer, bad dtype/dim, bad option  */
+  EVOC_ERR_OOM = 4,         /* device allocation or admission budget    */
+  EVOC_ERR_TIMEOUT = 5,     /* a bounded wait ran out                   */
+  EVOC_ERR_CUDA = 6,        /* CUDA runtime error                       */
+  EVOC_ERR_UNSUPPORTED = 7, /* form not available for this dtype/shape  */
+  EVOC_ERR_CANCELLED = 8,   /* serving: job was cancelled               */
+  EVOC_ERR_PENDING = 9      /* serving: job has not finished            */
+} evoc_status;
+
+/* EmbeddingData variants (src/knn.rs:16-20).  BINARY is the name README and
+ * the north star use for the UInt8 (packed bits, Jaccard) variant. */
+typedef enum {
+  EVOC_DTYPE_F32 = 0,
+  EVOC_DTYPE_I8 = 1,
+  EVOC_DTYPE_U8 = 2,
+  EVOC_DTYPE_BINARY = 2
+} evoc_dtype;
+
+/* How the neighbours are found. */
+typedef enum {
+  EVOC_FORM_AUTO = 0,        /* f32 -> BF16_RERANK; i8/u8 -> EXACT_INT            */
+  EVOC_FORM_FP32 = 1,        /* f32 exact search, FP32 SIMT dot products          */
+  EVOC_FORM_BF16_RERANK = 2, /* f32: tcgen05 BF16 scan keeps oversample*k         */
+                             /* candidates per row, reranked in FP32 (FP64 at the */
+                             /* k-th boundary)                                    */
+  EVOC_FORM_EXACT_INT = 3,   /* i8: tcgen05 int8 dots; u8: popcount Jaccard       */
+  EVOC_FORM_NNDESCENT = 4    /* GPU NN-descent (approximate, all dtypes)          */
+} evoc_form;
+
+/* Options.  evoc_gpu_default_opts() fills the defaults; fields that mirror
+ * KnnGraphOptions (src/knn.rs:44-76) keep its meaning. */
+typedef struct {
+  uint32_t struct_size;      /* sizeof(evoc_gpu_opts)                          */
+  int32_t form;              /* evoc_form                                      */
+  int32_t oversample;        /* BF16 form: candidates per row = oversample*k;  */
+                             /* <= 0 -> 2                                      */
+  int32_t buffers_on_device; /* 1: data and outputs are device pointers on the */
+                             /* context's device; 0: host pointers             */
+  int32_t deterministic;     /* KnnGraphOptions.deterministic                  */
+  int32_t n_iters;           /* NN-descent; <= 0 -> max(5, round(log2 n))      */
+  int32_t max_candidates;    /* NN-descent; <= 0 -> min(60, floor(1.5 k))      */
+  float delta;               /* NN-descent; KnnGraphOptions.delta (0.001)      */
+  float delta_improv;        /* NN-descent; KnnGraphOptions.delta_improv       */
+  int32_t reserved[8];
+} evoc_gpu_opts;
+
+typedef struct evoc_gpu_ctx evoc_gpu_ctx;
+
+/* ABI version: major*10000 + minor*100 + patch. */
+int evoc_gpu_version(void);
+
+void evoc_gpu_default_opts(evoc_gpu_opts* opts);
+
+/* Context on one CUDA device (one stream + scratch).  No counterpart in
+ * evoc-rs, whose backends are stateless trait objects
+ * (src/rlx_backend/mod.rs:204-216); the Rust shim keeps one per backend. */
+int evoc_gpu_ctx_create(int device, evoc_gpu_ctx** out);
+void evoc_gpu_ctx_destroy(evoc_gpu_ctx* ctx);
+const char* evoc_gpu_last_error(const evoc_gpu_ctx* ctx);
+
+/*
+ * kNN graph.  Replaces knn_graph / knn_graph_impl (src/knn.rs:345-454) behind
+ * RlxBackend::knn_graph (src/rlx_backend/mod.rs:135-144).
+ *   data       n x dim row-major: f32, i8, or u8 (dim = bytes per row)
+ *   k          n_neighbors; clamped to max(1, min(k, n-1)) as the reference does
+ *   rng_state  tau seed from NumpyRandomState::randint3_for_tau
+ *              (src/numpy_rng.rs:204-212); read by the NN-descent form only,
+ *              may be NULL otherwise
+ *   out_idx    n x k_eff int32, row-major, each row sorted ascending
+ *   out_dist   n x k_eff f32 transformed distances (src/knn.rs:156-187)
+ *   out_k      receives k_eff (may be NULL)
+ * f32 rows are renormalised first when any row's norm is off by > 1e-5
+ * (prepare_float, src/knn.rs:95-113).
+ */
+int evoc_gpu_knn_graph(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts, int32_t dtype, const void* data, int64_t n,
+                       int64_t dim, int32_t k, const int64_t* rng_state, int32_t* out_idx, float* out_dist,
+                       int32_t* out_k);
+
+/* As evoc_gpu_knn_graph, and also writes the raw pre-transform
+ * dissimilarities the reference's heaps hold (src/knn.rs:456-520 checks
+ * them) into out_raw (n x k_eff, may be NULL). */
+int evoc_gpu_knn_graph_raw(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts, int32_t dtype, const void* data,
+                           int64_t n, int64_t dim, int32_t k, const int64_t* rng_state, int32_t* out_idx,
+                           float* out_dist, float* out_raw, int32_t* out_k);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EVOC_GPU_H */

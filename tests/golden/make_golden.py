@@ -1,0 +1,59 @@
+"""Build tests/golden/*.npz from the evoc-rs golden fixtures.
+
+Run once in a container where the reference tree is mounted:
+
+    python tests/golden/make_golden.py [/path/to/evoc-rs]
+
+The reference's fixtures (tests/fixtures/{small_200,medium_800,large_2000}) were
+produced by upstream Python EVoC (scripts/generate_parity_fixtures.py:18-25,
+156-160 in evoc-rs) and are the golden vectors its own parity suites use:
+  tests/parity.rs:34-68,134-260     kNN indices/distances (assert_knn_parity rules)
+  tests/graph_parity.rs:28-90       sigma/rho and the fuzzy-union graph
+  tests/parity_intermediates.rs:655-687  NumPy RNG state after knn_graph
+The arrays are copied unchanged into one compressed .npz per fixture so the
+tests can run where the reference tree is absent.
+"""
+import json
+import os
+import sys
+
+import numpy as np
+
+REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+
+def main():
+    root = os.path.join(REF, "tests", "fixtures")
+    summary = json.load(open(os.path.join(root, "summary.json")))
+    for name in ("small_200", "medium_800", "large_2000"):
+        d = os.path.join(root, name)
+        inter = os.path.join(d, "intermediates")
+        arrs = {
+            "data": np.load(os.path.join(d, "data.npy")),
+            "nn_inds": np.load(os.path.join(d, "nn_inds.npy")),
+            "nn_dists": np.load(os.path.join(d, "nn_dists.npy")),
+            "rng_after_knn_key": np.load(os.path.join(inter, "rng_after_knn_key.npy")),
+            "seed": np.array(summary[name]["seed"], np.int64),
+        }
+        meta = np.load(os.path.join(inter, "rng_after_knn_meta.npz"))
+        arrs["rng_after_knn_pos"] = meta["pos"]
+        for g in ("graph_coo", "graph_csr"):
+            p = os.path.join(inter, g + ".npz")
+            if os.path.exists(p):
+                z = np.load(p)
+                for key in z.files:
+                    arrs[f"{g}_{key}"] = z[key]
+        for f in ("sigmas_py", "rhos_py", "sigmas", "rhos"):
+            p = os.path.join(inter, f + ".npy")
+            if os.path.exists(p):
+                arrs[f] = np.load(p)
+        p = os.path.join(d, "leaf_array.npy")
+        if os.path.exists(p):
+            arrs["leaf_array"] = np.load(p)
+        np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **arrs)
+        print(name, {k: v.shape for k, v in arrs.items()})
+
+
+if __name__ == "__main__":
+    main()
