@@ -43,6 +43,10 @@ __device__ __forceinline__ float raw_jaccard(uint32_t inter, uint32_t uni) {
   return uni > 0 ? -__fdiv_rn(__uint2float_rn(inter), __uint2float_rn(uni)) : 0.0f;
 }
 
+// Ordering keys fold -0.0 onto +0.0.  An int8 dissimilarity of zero is
+// -(0 as f32) = -0.0 in the reference, so the writer restores that sign.
+__device__ __forceinline__ float int8_raw_from_key(float r) { return r == 0.0f ? -0.0f : r; }
+
 // Distance transforms, src/knn.rs:156-187 (f64 log2 for f32/u8, f32 division for i8).
 __device__ __forceinline__ float transform_raw(int dtype, float d) {
   if (dtype == 0) {

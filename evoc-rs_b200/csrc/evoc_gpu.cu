@@ -53,6 +53,8 @@ struct evoc_gpu_ctx {
   std::mutex mu;
   std::string err;
   DevBuf x, scratch, norms, flag, out_idx, out_raw, out_dist;
+  DevBuf xb, cand, cand_raw, labels, order, hist, cursor, pivots, scratch2;
+  uint64_t timeout_ns = 4000000000ull;  // longest a pipeline wait inside a kernel may take
 };
 
 namespace {
@@ -81,12 +83,108 @@ int resolve_form(int32_t dtype, int32_t form) {
 }
 
 // Copies the caller's rows into a zero-padded device matrix of `ld` elements per row.
+// Rows past n (up to padded_rows(n)) are zero.
 int stage_rows(evoc_gpu_ctx* ctx, const void* data, int64_t n, int64_t row_bytes, int64_t ld_bytes, bool on_device) {
-  EVOC_TRY(ctx->x.ensure(size_t(n * ld_bytes)), "alloc rows");
-  if (ld_bytes != row_bytes) EVOC_TRY(cudaMemsetAsync(ctx->x.p, 0, size_t(n * ld_bytes), ctx->stream), "memset rows");
+  const int64_t rows = evoc::padded_rows(n);
+  EVOC_TRY(ctx->x.ensure(size_t(rows * ld_bytes)), "alloc rows");
+  if (ld_bytes != row_bytes)
+    EVOC_TRY(cudaMemsetAsync(ctx->x.p, 0, size_t(rows * ld_bytes), ctx->stream), "memset rows");
+  else if (rows > n)
+    EVOC_TRY(cudaMemsetAsync(ctx->x.as<uint8_t>() + n * ld_bytes, 0, size_t((rows - n) * ld_bytes), ctx->stream),
+             "memset pad rows");
   EVOC_TRY(cudaMemcpy2DAsync(ctx->x.p, size_t(ld_bytes), data, size_t(row_bytes), size_t(row_bytes), size_t(n),
                              on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream),
            "upload rows");
+  return EVOC_OK;
+}
+
+
+int run_fp32(evoc_gpu_ctx* ctx, int64_t n, int ld, int d, int keff, int32_t* d_idx, float* d_raw, float* d_dist) {
+  const int cap = evoc::topk_capacity(keff);
+  const int64_t qblocks = (n + 127) / 128;
+  const int grid = int(qblocks < int64_t(ctx->sms) * 2 ? qblocks : int64_t(ctx->sms) * 2);
+  EVOC_TRY(ctx->scratch.ensure(size_t(grid) * 128 * size_t(cap) * 8), "alloc scratch");
+  EVOC_TRY(evoc::launch_knn_f32_simt(ctx->x.as<float>(), n, ld, keff, cap, ctx->scratch.as<uint64_t>(), grid, d_idx,
+                                     d_raw, d_dist, 0, n, ctx->stream),
+           "knn_f32_simt");
+  (void)d;
+  return EVOC_OK;
+}
+
+// Grid of the persistent tensor-core scan over n_q query rows.
+int scan_grid(const evoc_gpu_ctx* ctx, int64_t n_q) {
+  const int64_t qblocks = (n_q + 127) / 128;
+  return int(qblocks < ctx->sms ? qblocks : ctx->sms);
+}
+
+// Query rows grouped by nearest pivot so that concurrently reranked rows share
+// candidates in L2.  Leaves ctx->order holding a permutation of 0..n-1.
+int locality_order(evoc_gpu_ctx* ctx, const void* rows, int64_t n, int64_t row_bytes, bool int8, int* status) {
+  int64_t n_piv = n / 256;
+  if (n_piv > 4096) n_piv = 4096;
+  if (n_piv < 2) n_piv = 2;
+  const int64_t piv_rows = evoc::padded_rows(n_piv);
+  EVOC_TRY(ctx->pivots.ensure(size_t(piv_rows * row_bytes)), "alloc pivots");
+  EVOC_TRY(cudaMemsetAsync(ctx->pivots.p, 0, size_t(piv_rows * row_bytes), ctx->stream), "clear pivots");
+  EVOC_TRY(evoc::launch_gather_pivots(rows, row_bytes, n, n_piv, ctx->pivots.p, ctx->sms, ctx->stream),
+           "gather pivots");
+  const int cap = evoc::topk_capacity(1);
+  const int grid = scan_grid(ctx, n);
+  EVOC_TRY(ctx->scratch2.ensure(size_t(grid) * 128 * size_t(cap) * 8), "alloc scratch2");
+  EVOC_TRY(ctx->labels.ensure(size_t(n) * 4), "alloc labels");
+  EVOC_TRY(evoc::launch_tc_scan(int8, rows, evoc::padded_rows(n), n, ctx->pivots.p, piv_rows, n_piv, row_bytes, 1, cap, ctx->scratch2.as<uint64_t>(),
+                                grid, 0, 0, 0, ctx->labels.as<int32_t>(), nullptr, nullptr, status, ctx->timeout_ns,
+                                ctx->stream),
+           "pivot scan");
+  EVOC_TRY(ctx->order.ensure(size_t(n) * 4), "alloc order");
+  EVOC_TRY(ctx->hist.ensure(size_t(n_piv) * 4), "alloc hist");
+  EVOC_TRY(ctx->cursor.ensure(size_t(n_piv) * 4), "alloc cursor");
+  EVOC_TRY(evoc::launch_order_by_label(ctx->labels.as<int32_t>(), n, int(n_piv), ctx->hist.as<int32_t>(),
+                                       ctx->cursor.as<int32_t>(), ctx->order.as<int32_t>(), ctx->sms, ctx->stream),
+           "order by pivot");
+  return EVOC_OK;
+}
+
+int run_bf16_rerank(evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, int64_t n, int ld, int d, int keff,
+                    int32_t* d_idx, float* d_raw, float* d_dist, int* status) {
+  const int over = opts.oversample > 0 ? opts.oversample : 2;
+  int64_t C = int64_t(over) * keff;
+  if (C > n) C = n;
+  if (C < keff) C = keff;
+  if (C > 256) return fail(ctx, EVOC_ERR_UNSUPPORTED, "oversample * k must be <= 256");
+  const int64_t ldb = round_up(d, 64);
+  const int64_t rows = evoc::padded_rows(n);
+  EVOC_TRY(ctx->xb.ensure(size_t(rows * ldb * 2)), "alloc bf16 rows");
+  EVOC_TRY(evoc::launch_to_bf16(ctx->x.as<float>(), rows, ld, d, ctx->xb.p, int(ldb), ctx->sms, ctx->stream), "to bf16");
+  const int cap = evoc::topk_capacity(int(C));
+  const int grid = scan_grid(ctx, n);
+  EVOC_TRY(ctx->scratch.ensure(size_t(grid) * 128 * size_t(cap) * 8), "alloc scratch");
+  EVOC_TRY(ctx->cand.ensure(size_t(n * C) * 4), "alloc candidates");
+  EVOC_TRY(evoc::launch_tc_scan(false, ctx->xb.p, rows, n, ctx->xb.p, rows, n, ldb * 2, int(C), cap, ctx->scratch.as<uint64_t>(),
+                                grid, 1, 0, 0, ctx->cand.as<int32_t>(), nullptr, nullptr, status, ctx->timeout_ns,
+                                ctx->stream),
+           "bf16 scan");
+  const int32_t* order = nullptr;
+  if (n >= 65536) {
+    int rc = locality_order(ctx, ctx->xb.p, n, ldb * 2, false, status);
+    if (rc) return rc;
+    order = ctx->order.as<int32_t>();
+  }
+  EVOC_TRY(evoc::launch_rerank_f32(ctx->x.as<float>(), ld, d, n, ctx->cand.as<int32_t>(), int(C), keff, order, d_idx,
+                                   d_raw, d_dist, ctx->sms, ctx->stream),
+           "rerank");
+  return EVOC_OK;
+}
+
+int run_int8(evoc_gpu_ctx* ctx, int64_t n, int64_t ldb, int keff, int32_t* d_idx, float* d_raw, float* d_dist,
+             int* status) {
+  const int cap = evoc::topk_capacity(keff);
+  const int grid = scan_grid(ctx, n);
+  EVOC_TRY(ctx->scratch.ensure(size_t(grid) * 128 * size_t(cap) * 8), "alloc scratch");
+  const int64_t rows = evoc::padded_rows(n);
+  EVOC_TRY(evoc::launch_tc_scan(true, ctx->x.p, rows, n, ctx->x.p, rows, n, ldb, keff, cap, ctx->scratch.as<uint64_t>(), grid, 1,
+                                1, EVOC_DTYPE_I8, d_idx, d_raw, d_dist, status, ctx->timeout_ns, ctx->stream),
+           "int8 scan");
   return EVOC_OK;
 }
 
@@ -133,27 +231,37 @@ int knn_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtype, con
     }
   }
 
+  EVOC_TRY(ctx->flag.ensure(64), "alloc flag");
+  int* d_flags = ctx->flag.as<int>();  // [0] prepare_float, [1] scan status
+  EVOC_TRY(cudaMemsetAsync(d_flags, 0, 64, ctx->stream), "clear flags");
+  int rc = EVOC_OK;
   if (dtype == EVOC_DTYPE_F32) {
-    if (form != EVOC_FORM_FP32)
+    if (form != EVOC_FORM_FP32 && form != EVOC_FORM_BF16_RERANK)
       return fail(ctx, EVOC_ERR_UNSUPPORTED, "form not built for f32 in this library");
     const int ld = int(round_up(dim, 16));
-    int rc = stage_rows(ctx, data, n, dim * 4, int64_t(ld) * 4, on_dev);
+    rc = stage_rows(ctx, data, n, dim * 4, int64_t(ld) * 4, on_dev);
     if (rc) return rc;
     EVOC_TRY(ctx->norms.ensure(size_t(n) * 4), "alloc norms");
-    EVOC_TRY(ctx->flag.ensure(64), "alloc flag");
-    EVOC_TRY(evoc::launch_prepare_float(ctx->x.as<float>(), n, ld, int(dim), ctx->norms.as<float>(),
-                                        ctx->flag.as<int>(), ctx->sms, ctx->stream),
+    EVOC_TRY(evoc::launch_prepare_float(ctx->x.as<float>(), n, ld, int(dim), ctx->norms.as<float>(), d_flags,
+                                        ctx->sms, ctx->stream),
              "prepare_float");
-    const int cap = evoc::topk_capacity(keff);
-    const int64_t qblocks = (n + 127) / 128;
-    const int grid = int(qblocks < int64_t(ctx->sms) * 2 ? qblocks : int64_t(ctx->sms) * 2);
-    EVOC_TRY(ctx->scratch.ensure(size_t(grid) * 128 * size_t(cap) * 8), "alloc scratch");
-    EVOC_TRY(evoc::launch_knn_f32_simt(ctx->x.as<float>(), n, ld, keff, cap, ctx->scratch.as<uint64_t>(), grid, d_idx,
-                                       d_raw, d_dist, 0, n, ctx->stream),
-             "knn_f32_simt");
+    if (form == EVOC_FORM_FP32) rc = run_fp32(ctx, n, ld, int(dim), keff, d_idx, d_raw, d_dist);
+    else rc = run_bf16_rerank(ctx, opts, n, ld, int(dim), keff, d_idx, d_raw, d_dist, d_flags + 1);
+  } else if (dtype == EVOC_DTYPE_I8) {
+    if (form != EVOC_FORM_EXACT_INT) return fail(ctx, EVOC_ERR_UNSUPPORTED, "form not built for i8 in this library");
+    const int64_t ldb = round_up(dim, 128);
+    rc = stage_rows(ctx, data, n, dim, ldb, on_dev);
+    if (rc) return rc;
+    rc = run_int8(ctx, n, ldb, keff, d_idx, d_raw, d_dist, d_flags + 1);
   } else {
     return fail(ctx, EVOC_ERR_UNSUPPORTED, "dtype form not built in this library");
   }
+  if (rc) return rc;
+  int flags[2] = {0, 0};
+  EVOC_TRY(cudaMemcpyAsync(flags, d_flags, sizeof(flags), cudaMemcpyDeviceToHost, ctx->stream), "read status");
+  EVOC_TRY(cudaStreamSynchronize(ctx->stream), "knn_graph");
+  if (flags[1] != 0)
+    return fail(ctx, EVOC_ERR_TIMEOUT, "a kernel pipeline wait timed out (stage " + std::to_string(flags[1]) + ")");
 
   if (!on_dev) {
     EVOC_TRY(cudaMemcpyAsync(out_idx, d_idx, out_elems * 4, cudaMemcpyDeviceToHost, ctx->stream), "download idx");
@@ -163,7 +271,7 @@ int knn_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtype, con
     if (out_raw)
       EVOC_TRY(cudaMemcpyAsync(out_raw, d_raw, out_elems * 4, cudaMemcpyDeviceToHost, ctx->stream), "download raw");
   }
-  EVOC_TRY(cudaStreamSynchronize(ctx->stream), "knn_graph");
+  EVOC_TRY(cudaStreamSynchronize(ctx->stream), "knn_graph outputs");
   return EVOC_OK;
 }
 
@@ -212,7 +320,9 @@ void evoc_gpu_ctx_destroy(evoc_gpu_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-  DevBuf* bufs[] = {&ctx->x, &ctx->scratch, &ctx->norms, &ctx->flag, &ctx->out_idx, &ctx->out_raw, &ctx->out_dist};
+  DevBuf* bufs[] = {&ctx->x,      &ctx->scratch, &ctx->norms,  &ctx->flag,   &ctx->out_idx, &ctx->out_raw,
+                    &ctx->out_dist, &ctx->xb,    &ctx->cand,   &ctx->cand_raw, &ctx->labels, &ctx->order,
+                    &ctx->hist,   &ctx->cursor,  &ctx->pivots, &ctx->scratch2};
   for (DevBuf* b : bufs) b->release();
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;

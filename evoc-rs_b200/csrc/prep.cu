@@ -7,6 +7,8 @@
 // own (no FMA contraction), sqrt and division are IEEE.  One thread owns one
 // row; rows are staged through shared memory in 32-column slabs so the
 // global reads stay coalesced.
+#include <cuda_bf16.h>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -68,6 +70,26 @@ cudaError_t launch_prepare_float(float* X, int64_t n, int ld, int d, float* norm
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   normalize_rows_kernel<<<sms * 8, 256, 0, stream>>>(X, n, ld, d, norms, not_unit);
+  return cudaGetLastError();
+}
+
+}  // namespace evoc
+
+namespace evoc {
+
+// f32 rows (ld floats) -> bf16 rows (ldb elements, zero padded), round to nearest even.
+__global__ void to_bf16_kernel(const float* __restrict__ X, int64_t n, int ld, int d, __nv_bfloat16* __restrict__ Y,
+                               int ldb) {
+  const int64_t total = n * int64_t(ldb);
+  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t r = e / ldb;
+    const int c = int(e % ldb);
+    Y[e] = __float2bfloat16_rn(c < d ? X[r * ld + c] : 0.0f);
+  }
+}
+
+cudaError_t launch_to_bf16(const float* X, int64_t n, int ld, int d, void* Y, int ldb, int sms, cudaStream_t stream) {
+  to_bf16_kernel<<<sms * 8, 256, 0, stream>>>(X, n, ld, d, static_cast<__nv_bfloat16*>(Y), ldb);
   return cudaGetLastError();
 }
 

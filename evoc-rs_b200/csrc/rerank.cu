@@ -1,0 +1,243 @@
+// Second stage of the BF16 form: FP32 rerank of the oversampled candidates.
+//
+// The BF16 tensor-core scan (tc_scan.cu) keeps C = oversample*k candidates
+// per row.  Here each warp takes one query row, recomputes the C dot products
+// in FP32 from the original (renormalised) f32 rows, ranks them by the
+// reference's dissimilarity (src/fast_cosine.rs:33-45; self = -1.0) with ties
+// by index, and only for candidates whose FP32 value lies within 1e-6 of the
+// k-th value recomputes the dot product in FP64 to settle the order at the
+// boundary.  Output is the final sorted row with transformed distances
+// (src/knn.rs:156-171).
+//
+// The candidate rows are gathered from HBM, so the order in which query rows
+// are reranked decides how often those rows are found in L2.  Rows are
+// processed grouped by their nearest pivot (a deterministic sample of the
+// data found with the same tensor-core scan), so the warps in flight at any
+// moment work on nearby points whose candidates overlap.
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace evoc {
+
+namespace {
+constexpr int RW = 8;          // warps per block
+constexpr int MAXC = 256;      // candidates per row handled in shared memory
+constexpr int GROUP = 4;       // candidates per pass over the query row
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ void warp_bitonic(uint64_t* keys, int P, int lane) {
+  for (int size = 2; size <= P; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = lane; i < (P >> 1); i += 32) {
+        const int lo = 2 * stride * (i / stride) + (i % stride);
+        const int hi = lo + stride;
+        const bool up = (lo & size) == 0;
+        const uint64_t a = keys[lo], b = keys[hi];
+        if ((a > b) == up) {
+          keys[lo] = b;
+          keys[hi] = a;
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+__device__ __forceinline__ float key_raw(uint64_t key) { return from_orderable(uint32_t(key >> 32)); }
+}  // namespace
+
+__global__ void __launch_bounds__(RW * 32)
+rerank_f32_kernel(const float* __restrict__ X, int ld, int d, int64_t n, const int32_t* __restrict__ cand, int C,
+                  int k, const int32_t* __restrict__ order, int32_t* __restrict__ out_idx, float* __restrict__ out_raw,
+                  float* __restrict__ out_dist) {
+  __shared__ uint64_t keys[RW][MAXC];
+  __shared__ double d64[RW][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint64_t* kw = keys[warp];
+  int P = 1;
+  while (P < C) P <<= 1;
+  for (int64_t w = int64_t(blockIdx.x) * RW + warp; w < n; w += int64_t(gridDim.x) * RW) {
+    const int64_t q = order ? order[w] : w;
+    const float* xq = X + q * ld;
+    const int32_t* cq = cand + q * C;
+    for (int j0 = 0; j0 < C; j0 += GROUP) {
+      int32_t id[GROUP];
+      float acc[GROUP];
+#pragma unroll
+      for (int u = 0; u < GROUP; u++) {
+        id[u] = (j0 + u < C) ? cq[j0 + u] : -1;
+        acc[u] = 0.0f;
+      }
+      for (int t = lane; t < d; t += 32) {
+        const float xv = xq[t];
+#pragma unroll
+        for (int u = 0; u < GROUP; u++)
+          if (id[u] >= 0) acc[u] = fmaf(xv, X[int64_t(id[u]) * ld + t], acc[u]);
+      }
+#pragma unroll
+      for (int u = 0; u < GROUP; u++) {
+        const float dot = warp_sum(acc[u]);
+        if (lane == u && j0 + u < C) {
+          uint64_t key = kKeyInf;
+          if (id[u] >= 0) key = make_key(id[u] == q ? -1.0f : raw_cosine(dot), id[u]);
+          kw[j0 + u] = key;
+        }
+      }
+    }
+    for (int j = C + lane; j < P; j += 32) kw[j] = kKeyInf;
+    __syncwarp();
+    warp_bitonic(kw, P, lane);
+
+    // FP64 only where FP32 cannot separate candidates at the k-th boundary.
+    const int kk = k < C ? k : C;
+    if (kk < C && kw[kk - 1] != kKeyInf && kw[kk] != kKeyInf) {
+      const float rk = key_raw(kw[kk - 1]);
+      int lo = kk - 1, hi = kk;
+      while (lo > 0 && kw[lo - 1] != kKeyInf && key_raw(kw[lo - 1]) >= rk - 1e-6f) lo--;
+      while (hi < C && kw[hi] != kKeyInf && key_raw(kw[hi]) <= rk + 1e-6f) hi++;
+      const int g = hi - lo;
+      if (g > 1 && g <= 32) {
+        for (int j = 0; j < g; j++) {
+          const int32_t c = key_index(kw[lo + j]);
+          double acc = 0.0;
+          for (int t = lane; t < d; t += 32) acc = fma(double(xq[t]), double(X[int64_t(c) * ld + t]), acc);
+          acc = warp_sum_d(acc);
+          // FP64 dissimilarity under the reference's rule: self -1, -dot, or the
+          // MIN_POSITIVE sentinel for dots <= 0 (a true tie, broken by index).
+          if (lane == 0) d64[warp][j] = (c == q) ? -1.0 : (acc > 0.0 ? -acc : double(kMinPositive));
+        }
+        __syncwarp();
+        if (lane == 0) {
+          // insertion sort of the boundary group by (FP64 dissimilarity, index)
+          for (int i = 1; i < g; i++) {
+            const double dv = d64[warp][i];
+            const uint64_t kv = kw[lo + i];
+            int j = i - 1;
+            while (j >= 0 && (d64[warp][j] > dv || (d64[warp][j] == dv && key_index(kw[lo + j]) > key_index(kv)))) {
+              d64[warp][j + 1] = d64[warp][j];
+              kw[lo + j + 1] = kw[lo + j];
+              j--;
+            }
+            d64[warp][j + 1] = dv;
+            kw[lo + j + 1] = kv;
+          }
+        }
+        __syncwarp();
+      }
+    }
+    // Write the row (lane j writes entries j, j+32, ...).
+    for (int j = lane; j < k; j += 32) {
+      const uint64_t key = j < C ? kw[j] : kKeyInf;
+      const bool ok = key != kKeyInf;
+      const float raw = ok ? key_raw(key) : kHeapInf;
+      out_idx[q * k + j] = ok ? key_index(key) : -1;
+      if (out_raw) out_raw[q * k + j] = raw;
+      if (out_dist) out_dist[q * k + j] = transform_raw(0, raw);
+    }
+    __syncwarp();
+  }
+}
+
+cudaError_t launch_rerank_f32(const float* X, int ld, int d, int64_t n, const int32_t* cand, int C, int k,
+                              const int32_t* order, int32_t* out_idx, float* out_raw, float* out_dist, int sms,
+                              cudaStream_t stream) {
+  if (C > MAXC || C < 1) return cudaErrorInvalidValue;
+  int64_t blocks = (n + RW - 1) / RW;
+  if (blocks > int64_t(sms) * 16) blocks = int64_t(sms) * 16;
+  rerank_f32_kernel<<<unsigned(blocks), RW * 32, 0, stream>>>(X, ld, d, n, cand, C, k, order, out_idx, out_raw,
+                                                               out_dist);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Locality order: pivot rows, nearest-pivot labels, counting sort.
+// ---------------------------------------------------------------------------
+__global__ void gather_rows_kernel(const uint8_t* __restrict__ src, int64_t row_bytes, int64_t n, int64_t n_piv,
+                                   uint8_t* __restrict__ dst) {
+  // pivot p is row floor(p * n / n_piv)
+  const int64_t total = n_piv * row_bytes;
+  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t p = e / row_bytes, b = e % row_bytes;
+    const int64_t r = p * n / n_piv;
+    dst[e] = src[r * row_bytes + b];
+  }
+}
+
+__global__ void label_hist_kernel(const int32_t* __restrict__ label, int64_t n, int nb, int32_t* __restrict__ hist) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    int b = label[i];
+    b = (b < 0 || b >= nb) ? 0 : b;
+    atomicAdd(&hist[b], 1);
+  }
+}
+
+// Single block: exclusive prefix sum of hist[0..nb) into cursor.
+__global__ void exclusive_scan_kernel(const int32_t* __restrict__ hist, int nb, int32_t* __restrict__ cursor) {
+  __shared__ int32_t part[1024];
+  const int t = threadIdx.x;
+  const int per = (nb + blockDim.x - 1) / blockDim.x;
+  int32_t s = 0;
+  for (int i = 0; i < per; i++) {
+    const int b = t * per + i;
+    if (b < nb) s += hist[b];
+  }
+  part[t] = s;
+  __syncthreads();
+  for (int off = 1; off < blockDim.x; off <<= 1) {
+    const int32_t v = t >= off ? part[t - off] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  int32_t run = part[t] - s;
+  for (int i = 0; i < per; i++) {
+    const int b = t * per + i;
+    if (b < nb) {
+      cursor[b] = run;
+      run += hist[b];
+    }
+  }
+}
+
+__global__ void label_scatter_kernel(const int32_t* __restrict__ label, int64_t n, int nb, int32_t* __restrict__ cursor,
+                                     int32_t* __restrict__ order) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    int b = label[i];
+    b = (b < 0 || b >= nb) ? 0 : b;
+    const int32_t pos = atomicAdd(&cursor[b], 1);
+    order[pos] = int32_t(i);
+  }
+}
+
+cudaError_t launch_gather_pivots(const void* src, int64_t row_bytes, int64_t n, int64_t n_piv, void* dst, int sms,
+                                 cudaStream_t stream) {
+  gather_rows_kernel<<<sms * 4, 256, 0, stream>>>(static_cast<const uint8_t*>(src), row_bytes, n, n_piv,
+                                                  static_cast<uint8_t*>(dst));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_order_by_label(const int32_t* label, int64_t n, int nb, int32_t* hist, int32_t* cursor,
+                                  int32_t* order, int sms, cudaStream_t stream) {
+  if (nb > 1024 * 64) return cudaErrorInvalidValue;
+  cudaError_t e = cudaMemsetAsync(hist, 0, size_t(nb) * sizeof(int32_t), stream);
+  if (e != cudaSuccess) return e;
+  label_hist_kernel<<<sms * 4, 256, 0, stream>>>(label, n, nb, hist);
+  exclusive_scan_kernel<<<1, 1024, 0, stream>>>(hist, nb, cursor);
+  label_scatter_kernel<<<sms * 4, 256, 0, stream>>>(label, n, nb, cursor, order);
+  return cudaGetLastError();
+}
+
+}  // namespace evoc

@@ -1,0 +1,342 @@
+// Tensor-core exact scan with the top-k selection fused into the epilogue.
+//
+// One persistent CTA per SM walks 128-row query blocks; for each it streams
+// every 256-row key tile through a 4-stage shared-memory pipeline and
+// multiplies on the 5th-generation tensor cores (tcgen05.mma, M=128, N=256,
+// BF16 -> F32 or S8 -> S32), accumulating in TMEM.  Two accumulators let the
+// epilogue read tile t while the MMAs of tile t+1 run.  Nothing of the n x n
+// score matrix is written to HBM: each epilogue thread owns one query row,
+// reads its 256 scores straight from TMEM and offers the few that beat its
+// row threshold to a thread-private candidate buffer (common.cuh).
+//
+// Warp roles (192 threads):
+//   warp 0      TMA producer (one elected lane, no multicast)
+//   warp 1      TMEM allocator + MMA issuer (one elected lane)
+//   warps 2..5  epilogue; warp w reads TMEM lanes 32*(w%4) .. +31
+//
+// Replaces the distance evaluations of the reference's NN-descent local join
+// (src/nndescent/float.rs:552-660 with fast_cosine, src/fast_cosine.rs:33-45;
+// src/nndescent/int8.rs:15-21 for the int8 dissimilarity).
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include "common.cuh"
+#include "kernels.h"
+#include "sm100.cuh"
+
+namespace evoc {
+
+namespace {
+constexpr int BM = 128;              // query rows per block (TMEM lanes)
+constexpr int BN = 256;              // key rows per tile (accumulator columns)
+constexpr int KCB = 128;             // bytes of K per pipeline stage (one 128B swizzle span)
+constexpr int STAGES = 4;
+constexpr int A_BYTES = BM * KCB;    // 16 KB
+constexpr int B_BYTES = BN * KCB;    // 32 KB
+constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+constexpr int TMEM_COLS = 2 * BN;    // two f32/s32 accumulators
+constexpr int NTHREADS = 192;
+constexpr size_t SMEM_BYTES = size_t(STAGES) * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+}  // namespace
+
+struct ScanParams {
+  int64_t n_q, n_k;
+  int n_kchunks;     // 128-byte K chunks per row
+  int keep;          // entries kept per query row
+  int cap;           // candidate buffer capacity per row
+  uint64_t* scratch; // gridDim.x * BM * cap keys
+  int self_mode;     // 1: query row i is key row i (offer self with raw -1.0, skip it in the scan)
+  int final_mode;    // 1: write sorted idx/raw/transformed dist; 0: write candidates (idx, raw)
+  int dtype;         // distance transform for final_mode
+  int32_t* out_idx;
+  float* out_raw;
+  float* out_dist;
+  int* status;       // 0 ok; set non-zero by the first role that gives up
+  uint64_t timeout_ns;
+};
+
+namespace {
+
+__device__ __forceinline__ void set_status(int* status, int code) { atomicCAS(status, 0, code); }
+
+// Offer path, out of line: it runs for a small fraction of the scores.
+__device__ __noinline__ float offer_slow(RowTopK* top, float raw, int32_t idx, bool int_scores) {
+  top->offer(raw, idx);
+  const float t = top->thr_raw;
+  if (int_scores) return -t;  // score >= -thr_raw can still enter
+  return t < 0.0f ? -t : __int_as_float(0xff800000);
+}
+
+}  // namespace
+
+template <bool kInt8>
+__global__ void __launch_bounds__(NTHREADS, 1)
+tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const ScanParams p) {
+  using namespace sm100;
+  extern __shared__ uint8_t smem_dyn[];
+  const uint32_t pad = (1024u - (smem_addr(smem_dyn) & 1023u)) & 1023u;
+  uint8_t* smem = smem_dyn + pad;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
+  uint64_t* full = bars;
+  uint64_t* empty = bars + STAGES;
+  uint64_t* tfull = bars + 2 * STAGES;
+  uint64_t* tempty = bars + 2 * STAGES + 2;
+  uint64_t* mma_done = bars + 2 * STAGES + 4;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 5);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int a = 0; a < 2; a++) {
+      mbar_init(&tfull[a], 1);
+      mbar_init(&tempty[a], 4 * 32);
+    }
+    mbar_init(mma_done, 1);
+    fence_barrier_init();
+  }
+  if (warp == 0 && lane == 0) {
+    prefetch_tmap(&tmA);
+    prefetch_tmap(&tmB);
+  }
+  if (warp == 1) {
+    tmem_alloc(tmem_slot, TMEM_COLS);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  const int64_t n_qblocks = (p.n_q + BM - 1) / BM;
+  const int64_t n_ktiles = (p.n_k + BN - 1) / BN;
+  const volatile int* abort = p.status;
+  constexpr int KC_ELEMS = kInt8 ? KCB : KCB / 2;
+  constexpr uint32_t IDESC = kInt8 ? idesc_s8_s32(BM, BN) : idesc_bf16_f32(BM, BN);
+
+  if (warp == 0) {
+    // ------------------------------------------------------------ producer
+    if (lane == 0) {
+      uint32_t it = 0;
+      bool ok = true;
+      for (int64_t qb = blockIdx.x; ok && qb < n_qblocks; qb += gridDim.x) {
+        for (int64_t kt = 0; ok && kt < n_ktiles; kt++) {
+          for (int kc = 0; kc < p.n_kchunks; kc++) {
+            const uint32_t s = it % STAGES, ph = (it / STAGES) & 1u;
+            if (!mbar_wait(&empty[s], ph ^ 1u, abort, p.timeout_ns)) {
+              set_status(p.status, 1);
+              ok = false;
+              break;
+            }
+            uint8_t* a_dst = smem + s * STAGE_BYTES;
+            mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
+            tma_load_2d(a_dst, &tmA, &full[s], kc * KC_ELEMS, int32_t(qb * BM));
+            tma_load_2d(a_dst + A_BYTES, &tmB, &full[s], kc * KC_ELEMS, int32_t(kt * BN));
+            it++;
+          }
+        }
+      }
+      // Let the last loads land before the CTA can exit.
+      for (uint32_t j = (it > STAGES ? it - STAGES : 0); j < it; j++)
+        mbar_wait(&full[j % STAGES], (j / STAGES) & 1u, nullptr, p.timeout_ns);
+    }
+  } else if (warp == 1) {
+    // ----------------------------------------------------------- MMA issuer
+    if (lane == 0) {
+      uint32_t it = 0, tile = 0;
+      bool ok = true;
+      for (int64_t qb = blockIdx.x; ok && qb < n_qblocks; qb += gridDim.x) {
+        for (int64_t kt = 0; ok && kt < n_ktiles; kt++, tile++) {
+          const uint32_t a = tile & 1u, tph = (tile >> 1) & 1u;
+          if (!mbar_wait(&tempty[a], tph ^ 1u, abort, p.timeout_ns)) {
+            set_status(p.status, 2);
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t d_tmem = tmem_base + a * BN;
+          for (int kc = 0; kc < p.n_kchunks; kc++) {
+            const uint32_t s = it % STAGES, ph = (it / STAGES) & 1u;
+            if (!mbar_wait(&full[s], ph, abort, p.timeout_ns)) {
+              set_status(p.status, 2);
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t a_addr = smem_addr(smem + s * STAGE_BYTES);
+            const uint64_t adesc = sw128_kmajor_desc(a_addr);
+            const uint64_t bdesc = sw128_kmajor_desc(a_addr + A_BYTES);
+#pragma unroll
+            for (int j = 0; j < KCB / 32; j++) {  // 32 bytes of K per instruction
+              const uint32_t acc = (kc > 0 || j > 0) ? 1u : 0u;
+              if (kInt8) mma_i8(d_tmem, adesc + 2 * j, bdesc + 2 * j, IDESC, acc);
+              else mma_f16(d_tmem, adesc + 2 * j, bdesc + 2 * j, IDESC, acc);
+            }
+            mma_commit(&empty[s]);  // stage is free once these MMAs have read it
+            it++;
+          }
+          if (!ok) break;
+          mma_commit(&tfull[a]);  // accumulator ready for the epilogue
+        }
+      }
+      mma_commit(mma_done);
+      mbar_wait(mma_done, 0, nullptr, p.timeout_ns);
+    }
+  } else {
+    // -------------------------------------------------------------- epilogue
+    const int quad = warp & 3;
+    const int row_local = quad * 32 + lane;
+    uint64_t* buf = p.scratch + (int64_t(blockIdx.x) * BM + row_local) * p.cap;
+    const float NEG_INF = __int_as_float(0xff800000);
+    uint32_t tile = 0;
+    bool ok = true;
+    RowTopK top;
+    for (int64_t qb = blockIdx.x; ok && qb < n_qblocks; qb += gridDim.x) {
+      const int64_t q = qb * BM + row_local;
+      const bool valid = q < p.n_q;
+      top.init(buf, p.keep, p.cap);
+      float thr_s = NEG_INF;
+      if (valid && p.self_mode) thr_s = offer_slow(&top, -1.0f, int32_t(q), kInt8);
+      for (int64_t kt = 0; kt < n_ktiles; kt++, tile++) {
+        const uint32_t a = tile & 1u, tph = (tile >> 1) & 1u;
+        int got = 1;
+        if (lane == 0) got = mbar_wait(&tfull[a], tph, abort, p.timeout_ns) ? 1 : 0;
+        got = __shfl_sync(0xffffffffu, got, 0);
+        if (!got) {
+          set_status(p.status, 3);
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t tbase = tmem_base + (uint32_t(quad * 32) << 16) + a * BN;
+        const int64_t k0 = kt * BN;
+#pragma unroll 1
+        for (int c = 0; c < BN / 32; c++) {
+          uint32_t v[32];
+          tmem_ld_32x32b_x32(tbase + c * 32, v);
+          tmem_ld_wait();
+          if (valid) {
+#pragma unroll
+            for (int j = 0; j < 32; j++) {
+              const float s = kInt8 ? __int2float_rn(int32_t(v[j])) : __uint_as_float(v[j]);
+              if (s >= thr_s) {
+                const int64_t key = k0 + c * 32 + j;
+                if (key < p.n_k && !(p.self_mode && key == q)) {
+                  const float raw = kInt8 ? -s : raw_cosine(s);
+                  thr_s = offer_slow(&top, raw, int32_t(key), kInt8);
+                }
+              }
+            }
+          }
+        }
+        tc_fence_before();
+        mbar_arrive(&tempty[a]);
+      }
+      if (!ok) break;
+      if (valid) {
+        const int got = top.finish();
+        const int64_t orow = q * p.keep;
+        for (int j = 0; j < p.keep; j++) {
+          float raw = kHeapInf;
+          int32_t idx = -1;
+          if (j < got) {
+            raw = from_orderable(uint32_t(top.buf[j] >> 32));
+            if (kInt8) raw = int8_raw_from_key(raw);
+            idx = key_index(top.buf[j]);
+          }
+          p.out_idx[orow + j] = idx;
+          if (p.out_raw) p.out_raw[orow + j] = raw;
+          if (p.final_mode && p.out_dist) p.out_dist[orow + j] = transform_raw(p.dtype, raw);
+        }
+      }
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem_base, TMEM_COLS);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// 2-D map over `rows` rows of `row_bytes` (a multiple of 128); box = 128 bytes x box_rows.
+bool make_map(CUtensorMap* m, const void* base, int64_t rows, int64_t row_bytes, int elem_bytes, int box_rows) {
+  auto enc = get_encode();
+  if (!enc) return false;
+  const cuuint64_t dims[2] = {cuuint64_t(row_bytes / elem_bytes), cuuint64_t(rows)};
+  const cuuint64_t strides[1] = {cuuint64_t(row_bytes)};
+  const cuuint32_t box[2] = {cuuint32_t(KCB / elem_bytes), cuuint32_t(box_rows)};
+  const cuuint32_t estr[2] = {1, 1};
+  CUresult r = enc(m, elem_bytes == 2 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_UINT8, 2,
+                   const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+}  // namespace
+
+size_t tc_scan_smem_bytes() { return SMEM_BYTES; }
+
+cudaError_t launch_tc_scan(bool int8, const void* Q, int64_t q_rows, int64_t n_q, const void* K, int64_t k_rows,
+                           int64_t n_k, int64_t row_bytes, int keep, int cap, uint64_t* scratch, int grid, int self_mode, int final_mode, int dtype,
+                           int32_t* out_idx, float* out_raw, float* out_dist, int* status, uint64_t timeout_ns,
+                           cudaStream_t stream) {
+  // q_rows / k_rows: rows present in memory (multiples of the box heights);
+  // n_q / n_k: rows that take part.  Rows past n are zero and never offered.
+  if (row_bytes % KCB != 0 || n_q <= 0 || n_k <= 0) return cudaErrorInvalidValue;
+  if (q_rows < n_q || k_rows < n_k || q_rows % BM != 0 || k_rows % BN != 0) return cudaErrorInvalidValue;
+  if ((reinterpret_cast<uintptr_t>(Q) & 15) || (reinterpret_cast<uintptr_t>(K) & 15)) return cudaErrorInvalidValue;
+  const int eb = int8 ? 1 : 2;
+  alignas(64) CUtensorMap ma, mb;
+  if (!make_map(&ma, Q, q_rows, row_bytes, eb, BM) || !make_map(&mb, K, k_rows, row_bytes, eb, BN))
+    return cudaErrorInvalidValue;
+  ScanParams p;
+  p.n_q = n_q;
+  p.n_k = n_k;
+  p.n_kchunks = int(row_bytes / KCB);
+  p.keep = keep;
+  p.cap = cap;
+  p.scratch = scratch;
+  p.self_mode = self_mode;
+  p.final_mode = final_mode;
+  p.dtype = dtype;
+  p.out_idx = out_idx;
+  p.out_raw = out_raw;
+  p.out_dist = out_dist;
+  p.status = status;
+  p.timeout_ns = timeout_ns;
+  cudaError_t e;
+  if (int8) {
+    e = cudaFuncSetAttribute(tc_scan_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_BYTES));
+    if (e != cudaSuccess) return e;
+    tc_scan_kernel<true><<<grid, NTHREADS, SMEM_BYTES, stream>>>(ma, mb, p);
+  } else {
+    e = cudaFuncSetAttribute(tc_scan_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_BYTES));
+    if (e != cudaSuccess) return e;
+    tc_scan_kernel<false><<<grid, NTHREADS, SMEM_BYTES, stream>>>(ma, mb, p);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace evoc

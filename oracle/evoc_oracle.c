@@ -953,7 +953,8 @@ int orc_knn_graph(int dtype, const void *data_in, int64_t n, int64_t dim, const 
 /* src/nndescent/float.rs:209-215), every other row with its raw         */
 /* dissimilarity; keep the k smallest by (raw, index) with f32 equality  */
 /* (so -0.0 == +0.0); rows come out sorted ascending.                     */
-/* f32 dots here are serial order (src/fast_cosine.rs:55-62).             */
+/* f32 dissimilarities use the reference's deterministic cosine           */
+/* (native/fast_cosine.c, the path knn_graph takes with deterministic).   */
 /* ------------------------------------------------------------------ */
 static inline int worse(float da, int32_t ia, float db, int32_t ib) {
     /* (da, ia) > (db, ib) */
@@ -983,7 +984,7 @@ void orc_exact_knn(int dtype, const void *data, int64_t n, int64_t dim, int64_t 
                    int32_t *out_ind, float *out_raw) {
 #pragma omp parallel for schedule(dynamic, 8)
     for (int64_t i = row0; i < row1; i++) {
-        orc_data D = {dtype, data, n, dim, 0};
+        orc_data D = {dtype, data, n, dim, 1};
         float *hd = (float *)malloc((size_t)k * sizeof(float));
         int32_t *hi = (int32_t *)malloc((size_t)k * sizeof(int32_t));
         int64_t cnt = 0;

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import evoc
-from conftest import FIXTURES, assert_knn_parity, knn_parity_counts
+from conftest import FIXTURES, assert_knn_parity
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -35,20 +35,34 @@ def test_fp32_matches_golden(golden, name):
 
 
 def _check_against_oracle(x, k, max_tie_frac=0.01):
+    """Neighbour sets equal to the oracle's except for ties within 1e-6 cosine,
+    and every reported raw dissimilarity within 1e-6 of the FP64 value for
+    that pair.  (Two FP32 summation orders differ by a few 1e-7 in the dot,
+    which the -log2 transform can stretch past 1e-6, so distances are held to
+    FP64 truth rather than to another FP32 ordering.)"""
     ind, dst, raw = evoc.knn_graph(x, opts(k), None, return_raw=True)
     xn = O.prepare_float(x)
     kk = max(1, min(k, len(x) - 1))
     ei, er = O.exact_knn(xn, kk)
-    ed = O.transform(O.DT_F32, er)
     assert ind.shape == ei.shape
-    dm, bad, tie = knn_parity_counts(ind, dst, ei, ed)
-    assert dm == 0 and bad == 0, (dm, bad)
-    assert tie <= max(8, max_tie_frac * ind.size), tie
-    assert np.all(np.abs(raw - er) <= 1e-6)
+    x64 = xn.astype(np.float64)
+    dots = np.einsum("rkd,rd->rk", x64[ind], x64)
+    want = np.where(dots > 0, -dots, 1.17549435e-38)
+    want[ind == np.arange(len(x))[:, None]] = -1.0
+    assert np.abs(raw - want).max() <= 1e-6
+    # index disagreements only where the oracle's raw values tie within 1e-6
+    diff = ind != ei
+    assert np.all(np.abs(raw[diff] - er[diff]) <= 1e-6)
+    assert diff.sum() <= max(8, max_tie_frac * ind.size), diff.sum()
+    assert np.array_equal(dst, transform_f32(raw))
     # raw is -dot, or f32::MIN_POSITIVE when the dot is <= 0 (src/fast_cosine.rs:40-44)
     assert raw.max() <= np.float32(1.17549435e-38)
     assert np.all(np.diff(raw, axis=1) >= -1e-6)
     return ind, dst
+
+
+def transform_f32(raw):
+    return O.transform(O.DT_F32, raw)
 
 
 @pytest.mark.parametrize("n,d,k", [(2, 3, 1), (3, 5, 10), (17, 16, 4), (129, 33, 15), (300, 128, 30),
