@@ -155,3 +155,67 @@ struct RowTopK {
 };
 
 }  // namespace evoc
+
+namespace evoc {
+
+// ---------------------------------------------------------------------------
+// Thread-private bounded max-heap of ordering keys (one owner thread per query
+// row).  Holds the `cap` smallest keys offered so far; its root is the exact
+// cap-th best, so it is also the admission threshold.  The storage may be
+// shared memory (row stride chosen odd in 8-byte words, so the 32 owners of a
+// warp touching the same slot hit distinct banks) or global memory.
+// ---------------------------------------------------------------------------
+struct KeyHeap {
+  uint64_t* h;
+  int size;
+  int cap;
+
+  __device__ __forceinline__ void init(uint64_t* storage, int capacity) {
+    h = storage;
+    size = 0;
+    cap = capacity;
+  }
+
+  __device__ __forceinline__ uint64_t threshold() const { return size < cap ? kKeyInf : h[0]; }
+
+  __device__ inline void sift_down(int e) {
+    const uint64_t v = h[e];
+    for (;;) {
+      int c = 2 * e + 1;
+      if (c >= cap) break;
+      uint64_t cv = h[c];
+      if (c + 1 < cap) {
+        const uint64_t r = h[c + 1];
+        if (r > cv) {
+          cv = r;
+          c++;
+        }
+      }
+      if (cv <= v) break;
+      h[e] = cv;
+      e = c;
+    }
+    h[e] = v;
+  }
+
+  // Keys are unique (they embed the row index), so a strict compare suffices.
+  __device__ inline void offer(uint64_t key) {
+    if (size < cap) {
+      h[size++] = key;
+      if (size == cap)
+        for (int e = cap / 2 - 1; e >= 0; e--) sift_down(e);
+      return;
+    }
+    if (key >= h[0]) return;
+    h[0] = key;
+    sift_down(0);
+  }
+
+  // Sorts ascending in place (insertion sort; cap is small) and returns the count.
+  __device__ inline int finish() {
+    sort_keys(h, size);
+    return size;
+  }
+};
+
+}  // namespace evoc

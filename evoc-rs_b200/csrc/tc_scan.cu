@@ -30,21 +30,26 @@ namespace {
 constexpr int BM = 128;              // query rows per block (TMEM lanes)
 constexpr int BN = 256;              // key rows per tile (accumulator columns)
 constexpr int KCB = 128;             // bytes of K per pipeline stage (one 128B swizzle span)
-constexpr int STAGES = 4;
 constexpr int A_BYTES = BM * KCB;    // 16 KB
 constexpr int B_BYTES = BN * KCB;    // 32 KB
 constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
 constexpr int TMEM_COLS = 2 * BN;    // two f32/s32 accumulators
-constexpr int NTHREADS = 192;
-constexpr size_t SMEM_BYTES = size_t(STAGES) * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+constexpr size_t SMEM_LIMIT = 232448;      // 227 KB opt-in maximum per block
+constexpr size_t SMEM_FIXED = 1024 /*align*/ + 256 /*barriers*/;
+
+// Shared memory for a pipeline depth, a number of epilogue warp groups (each
+// with one heap per row) and a heap stride (0: heaps in global memory).
+constexpr size_t smem_bytes(int stages, int groups, int heap_stride) {
+  return size_t(stages) * STAGE_BYTES + size_t(groups) * BM * size_t(heap_stride) * 8 + SMEM_FIXED;
+}
 }  // namespace
 
 struct ScanParams {
   int64_t n_q, n_k;
   int n_kchunks;     // 128-byte K chunks per row
-  int keep;          // entries kept per query row
-  int cap;           // candidate buffer capacity per row
-  uint64_t* scratch; // gridDim.x * BM * cap keys
+  int keep;          // entries kept per query row (the heap size)
+  int heap_stride;   // 8-byte words between rows' heaps (odd when heaps are in shared memory)
+  uint64_t* scratch; // gridDim.x * BM * keep keys, used when heaps are in global memory
   int self_mode;     // 1: query row i is key row i (offer self with raw -1.0, skip it in the scan)
   int final_mode;    // 1: write sorted idx/raw/transformed dist; 0: write candidates (idx, raw)
   int dtype;         // distance transform for final_mode
@@ -59,24 +64,74 @@ namespace {
 
 __device__ __forceinline__ void set_status(int* status, int code) { atomicCAS(status, 0, code); }
 
-// Offer path, out of line: it runs for a small fraction of the scores.
-__device__ __noinline__ float offer_slow(RowTopK* top, float raw, int32_t idx, bool int_scores) {
-  top->offer(raw, idx);
-  const float t = top->thr_raw;
-  if (int_scores) return -t;  // score >= -thr_raw can still enter
-  return t < 0.0f ? -t : __int_as_float(0xff800000);
+// Quick-reject threshold as the raw 32-bit score pattern the accumulator holds:
+// a score below it cannot enter the heap.  For int8 it is an s32 lower bound
+// (exact while |dot| < 2^24, loosened by 256 beyond, where f32 rounds); for
+// BF16 it is an f32.  Passing scores are re-checked exactly by the key compare.
+__device__ __forceinline__ uint32_t pass_threshold(const KeyHeap& heap, bool int_scores) {
+  const uint64_t t = heap.threshold();
+  if (int_scores) {
+    if (t == kKeyInf) return uint32_t(INT32_MIN);
+    const float ts = -from_orderable(uint32_t(t >> 32));  // raw = -score
+    int32_t ti = int32_t(ts);
+    if (!(fabsf(ts) < 16777216.0f)) ti -= 256;
+    return uint32_t(ti);
+  }
+  const uint32_t NEG_INF = 0xff800000u;
+  if (t == kKeyInf) return NEG_INF;
+  const float raw = from_orderable(uint32_t(t >> 32));
+  return raw < 0.0f ? __float_as_uint(-raw) : NEG_INF;  // raw = -score, or MIN_POSITIVE for scores <= 0
+}
+
+template <bool kInt8>
+__device__ __forceinline__ bool passes(uint32_t v, uint32_t thr) {
+  return kInt8 ? (int32_t(v) >= int32_t(thr)) : (__uint_as_float(v) >= __uint_as_float(thr));
+}
+
+// Offers the scores of one 32-column chunk that beat the threshold.  The
+// chunk's values stay in registers; a survivor's value is picked by an
+// unrolled select (survivors are rare once the heap is full).
+template <bool kInt8>
+__device__ __forceinline__ void offer_chunk(const uint32_t (&v)[32], uint32_t mask, int64_t col0, int64_t n_k,
+                                            bool self_mode, int64_t q, KeyHeap& heap, uint32_t& thr) {
+  while (mask) {
+    const int j = __ffs(mask) - 1;
+    mask &= mask - 1;
+    uint32_t bits = 0;
+#pragma unroll
+    for (int jj = 0; jj < 32; jj++) bits = (jj == j) ? v[jj] : bits;
+    if (!passes<kInt8>(bits, thr)) continue;  // threshold may have moved
+    const int64_t key = col0 + j;
+    if (key >= n_k || (self_mode && key == q)) continue;
+    const float raw = kInt8 ? -__int2float_rn(int32_t(bits)) : raw_cosine(__uint_as_float(bits));
+    heap.offer(make_key(raw, int32_t(key)));
+    thr = pass_threshold(heap, kInt8);
+  }
+}
+
+template <bool kInt8>
+__device__ __forceinline__ uint32_t chunk_mask(const uint32_t (&v)[32], uint32_t thr) {
+  uint32_t m = 0;
+#pragma unroll
+  for (int j = 0; j < 32; j++) m |= (passes<kInt8>(v[j], thr) ? 1u : 0u) << j;
+  return m;
+}
+
+__device__ __forceinline__ void epilogue_sync(int nthreads) {
+  asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
 }
 
 }  // namespace
 
-template <bool kInt8>
-__global__ void __launch_bounds__(NTHREADS, 1)
+template <bool kInt8, int STAGES, int GROUPS, bool kSmemHeap>
+__global__ void __launch_bounds__(64 + GROUPS * 128, 1)
 tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const ScanParams p) {
   using namespace sm100;
   extern __shared__ uint8_t smem_dyn[];
   const uint32_t pad = (1024u - (smem_addr(smem_dyn) & 1023u)) & 1023u;
   uint8_t* smem = smem_dyn + pad;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
+  uint64_t* heaps = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
+  uint64_t* bars = kSmemHeap ? heaps + BM * p.heap_stride : heaps;
   uint64_t* full = bars;
   uint64_t* empty = bars + STAGES;
   uint64_t* tfull = bars + 2 * STAGES;
@@ -92,7 +147,7 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     }
     for (int a = 0; a < 2; a++) {
       mbar_init(&tfull[a], 1);
-      mbar_init(&tempty[a], 4 * 32);
+      mbar_init(&tempty[a], GROUPS * 128);
     }
     mbar_init(mma_done, 1);
     fence_barrier_init();
@@ -186,19 +241,25 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     }
   } else {
     // -------------------------------------------------------------- epilogue
+    // Epilogue warp e = warp - 2 reads TMEM lanes 32*(warp%4).. (its row
+    // quadrant) and columns [group*BN/GROUPS, (group+1)*BN/GROUPS) of every tile.
     const int quad = warp & 3;
+    const int group = (warp - 2) / 4;
     const int row_local = quad * 32 + lane;
-    uint64_t* buf = p.scratch + (int64_t(blockIdx.x) * BM + row_local) * p.cap;
-    const float NEG_INF = __int_as_float(0xff800000);
+    constexpr int NCH = BN / GROUPS / 32;  // 32-column chunks per tile per group
+    const int col_base = group * (BN / GROUPS);
+    const int heap_slot = group * BM + row_local;
+    uint64_t* hstore = kSmemHeap ? heaps + int64_t(heap_slot) * p.heap_stride
+                                 : p.scratch + (int64_t(blockIdx.x) * GROUPS * BM + heap_slot) * p.heap_stride;
     uint32_t tile = 0;
     bool ok = true;
-    RowTopK top;
     for (int64_t qb = blockIdx.x; ok && qb < n_qblocks; qb += gridDim.x) {
       const int64_t q = qb * BM + row_local;
       const bool valid = q < p.n_q;
-      top.init(buf, p.keep, p.cap);
-      float thr_s = NEG_INF;
-      if (valid && p.self_mode) thr_s = offer_slow(&top, -1.0f, int32_t(q), kInt8);
+      KeyHeap heap;
+      heap.init(hstore, p.keep);
+      if (valid && p.self_mode && group == 0) heap.offer(make_key(-1.0f, int32_t(q)));
+      uint32_t thr = pass_threshold(heap, kInt8);
       for (int64_t kt = 0; kt < n_ktiles; kt++, tile++) {
         const uint32_t a = tile & 1u, tph = (tile >> 1) & 1u;
         int got = 1;
@@ -210,47 +271,60 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
           break;
         }
         tc_fence_after();
-        const uint32_t tbase = tmem_base + (uint32_t(quad * 32) << 16) + a * BN;
-        const int64_t k0 = kt * BN;
+        const uint32_t tbase = tmem_base + (uint32_t(quad * 32) << 16) + a * BN + col_base;
+        const int64_t k0 = kt * BN + col_base;
+        uint32_t va[32], vb[32];
+        tmem_ld_32x32b_x32(tbase, va);
 #pragma unroll 1
-        for (int c = 0; c < BN / 32; c++) {
-          uint32_t v[32];
-          tmem_ld_32x32b_x32(tbase + c * 32, v);
+        for (int c = 0; c < NCH; c += 2) {
           tmem_ld_wait();
-          if (valid) {
-#pragma unroll
-            for (int j = 0; j < 32; j++) {
-              const float s = kInt8 ? __int2float_rn(int32_t(v[j])) : __uint_as_float(v[j]);
-              if (s >= thr_s) {
-                const int64_t key = k0 + c * 32 + j;
-                if (key < p.n_k && !(p.self_mode && key == q)) {
-                  const float raw = kInt8 ? -s : raw_cosine(s);
-                  thr_s = offer_slow(&top, raw, int32_t(key), kInt8);
-                }
-              }
-            }
-          }
+          tmem_ld_32x32b_x32(tbase + (c + 1) * 32, vb);
+          uint32_t m = chunk_mask<kInt8>(va, thr);
+          if (valid && m) offer_chunk<kInt8>(va, m, k0 + c * 32, p.n_k, p.self_mode, q, heap, thr);
+          tmem_ld_wait();
+          if (c + 2 < NCH) tmem_ld_32x32b_x32(tbase + (c + 2) * 32, va);
+          m = chunk_mask<kInt8>(vb, thr);
+          if (valid && m) offer_chunk<kInt8>(vb, m, k0 + (c + 1) * 32, p.n_k, p.self_mode, q, heap, thr);
         }
         tc_fence_before();
         mbar_arrive(&tempty[a]);
       }
       if (!ok) break;
-      if (valid) {
-        const int got = top.finish();
+      if (GROUPS > 1) {
+        // Fold the other groups' heaps for this row into group 0's.  Unused
+        // slots of a heap that never filled are marked empty first.
+        if (group > 0)
+          for (int j = heap.size; j < p.keep; j++) heap.h[j] = kKeyInf;
+        epilogue_sync(GROUPS * 128);
+        if (group == 0 && valid) {
+          for (int g = 1; g < GROUPS; g++) {
+            const uint64_t* other = kSmemHeap ? heaps + int64_t(g * BM + row_local) * p.heap_stride
+                                              : p.scratch + (int64_t(blockIdx.x) * GROUPS * BM + g * BM + row_local) *
+                                                                p.heap_stride;
+            for (int j = 0; j < p.keep; j++) {
+              const uint64_t kv = other[j];
+              if (kv != kKeyInf) heap.offer(kv);
+            }
+          }
+        }
+      }
+      if (group == 0 && valid) {
+        const int got = heap.finish();
         const int64_t orow = q * p.keep;
         for (int j = 0; j < p.keep; j++) {
           float raw = kHeapInf;
           int32_t idx = -1;
           if (j < got) {
-            raw = from_orderable(uint32_t(top.buf[j] >> 32));
+            raw = from_orderable(uint32_t(heap.h[j] >> 32));
             if (kInt8) raw = int8_raw_from_key(raw);
-            idx = key_index(top.buf[j]);
+            idx = key_index(heap.h[j]);
           }
           p.out_idx[orow + j] = idx;
           if (p.out_raw) p.out_raw[orow + j] = raw;
           if (p.final_mode && p.out_dist) p.out_dist[orow + j] = transform_raw(p.dtype, raw);
         }
       }
+      if (GROUPS > 1) epilogue_sync(GROUPS * 128);  // heaps are reused by the next block
     }
   }
 
@@ -296,15 +370,46 @@ bool make_map(CUtensorMap* m, const void* base, int64_t rows, int64_t row_bytes,
 
 }  // namespace
 
-size_t tc_scan_smem_bytes() { return SMEM_BYTES; }
+size_t tc_scan_smem_bytes() { return smem_bytes(4, 1, 0); }
+
+namespace {
+template <bool kInt8, int STAGES, int GROUPS, bool kSmemHeap>
+cudaError_t launch_variant(const CUtensorMap& ma, const CUtensorMap& mb, const ScanParams& p, int grid, size_t smem,
+                           cudaStream_t stream) {
+  auto kern = tc_scan_kernel<kInt8, STAGES, GROUPS, kSmemHeap>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  kern<<<grid, 64 + GROUPS * 128, smem, stream>>>(ma, mb, p);
+  return cudaGetLastError();
+}
+
+template <bool kInt8>
+cudaError_t launch_dtype(const CUtensorMap& ma, const CUtensorMap& mb, ScanParams p, int grid, cudaStream_t stream) {
+  const int odd = p.keep | 1;
+  p.heap_stride = odd;
+  // Prefer two epilogue groups (more warps to hide TMEM/issue latency), then
+  // the deeper pipeline; heaps fall back to global memory for very large keep.
+  if (smem_bytes(4, 2, odd) <= SMEM_LIMIT)
+    return launch_variant<kInt8, 4, 2, true>(ma, mb, p, grid, smem_bytes(4, 2, odd), stream);
+  if (smem_bytes(3, 2, odd) <= SMEM_LIMIT)
+    return launch_variant<kInt8, 3, 2, true>(ma, mb, p, grid, smem_bytes(3, 2, odd), stream);
+  if (smem_bytes(4, 1, odd) <= SMEM_LIMIT)
+    return launch_variant<kInt8, 4, 1, true>(ma, mb, p, grid, smem_bytes(4, 1, odd), stream);
+  if (smem_bytes(3, 1, odd) <= SMEM_LIMIT)
+    return launch_variant<kInt8, 3, 1, true>(ma, mb, p, grid, smem_bytes(3, 1, odd), stream);
+  if (!p.scratch) return cudaErrorInvalidValue;
+  p.heap_stride = p.keep;
+  return launch_variant<kInt8, 4, 1, false>(ma, mb, p, grid, smem_bytes(4, 1, 0), stream);
+}
+}  // namespace
 
 cudaError_t launch_tc_scan(bool int8, const void* Q, int64_t q_rows, int64_t n_q, const void* K, int64_t k_rows,
-                           int64_t n_k, int64_t row_bytes, int keep, int cap, uint64_t* scratch, int grid, int self_mode, int final_mode, int dtype,
-                           int32_t* out_idx, float* out_raw, float* out_dist, int* status, uint64_t timeout_ns,
-                           cudaStream_t stream) {
+                           int64_t n_k, int64_t row_bytes, int keep, int /*cap*/, uint64_t* scratch, int grid,
+                           int self_mode, int final_mode, int dtype, int32_t* out_idx, float* out_raw, float* out_dist,
+                           int* status, uint64_t timeout_ns, cudaStream_t stream) {
   // q_rows / k_rows: rows present in memory (multiples of the box heights);
   // n_q / n_k: rows that take part.  Rows past n are zero and never offered.
-  if (row_bytes % KCB != 0 || n_q <= 0 || n_k <= 0) return cudaErrorInvalidValue;
+  if (row_bytes % KCB != 0 || n_q <= 0 || n_k <= 0 || keep < 1) return cudaErrorInvalidValue;
   if (q_rows < n_q || k_rows < n_k || q_rows % BM != 0 || k_rows % BN != 0) return cudaErrorInvalidValue;
   if ((reinterpret_cast<uintptr_t>(Q) & 15) || (reinterpret_cast<uintptr_t>(K) & 15)) return cudaErrorInvalidValue;
   const int eb = int8 ? 1 : 2;
@@ -316,7 +421,6 @@ cudaError_t launch_tc_scan(bool int8, const void* Q, int64_t q_rows, int64_t n_q
   p.n_k = n_k;
   p.n_kchunks = int(row_bytes / KCB);
   p.keep = keep;
-  p.cap = cap;
   p.scratch = scratch;
   p.self_mode = self_mode;
   p.final_mode = final_mode;
@@ -326,17 +430,7 @@ cudaError_t launch_tc_scan(bool int8, const void* Q, int64_t q_rows, int64_t n_q
   p.out_dist = out_dist;
   p.status = status;
   p.timeout_ns = timeout_ns;
-  cudaError_t e;
-  if (int8) {
-    e = cudaFuncSetAttribute(tc_scan_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_BYTES));
-    if (e != cudaSuccess) return e;
-    tc_scan_kernel<true><<<grid, NTHREADS, SMEM_BYTES, stream>>>(ma, mb, p);
-  } else {
-    e = cudaFuncSetAttribute(tc_scan_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_BYTES));
-    if (e != cudaSuccess) return e;
-    tc_scan_kernel<false><<<grid, NTHREADS, SMEM_BYTES, stream>>>(ma, mb, p);
-  }
-  return cudaGetLastError();
+  return int8 ? launch_dtype<true>(ma, mb, p, grid, stream) : launch_dtype<false>(ma, mb, p, grid, stream);
 }
 
 }  // namespace evoc
