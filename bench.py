@@ -1,0 +1,375 @@
+#!/usr/bin/env python
+"""Benchmark: kNN-graph edges/s on the 1,000,000 x 768 f32 cosine k=30 workload.
+
+Workload (zipf_1m_768): 200 Gaussian clusters with Zipf(1.1) sizes, centres
+N(0,1), per-cluster per-dimension sigma ~ U(0.1, 0.5), rows L2-normalised,
+seed 7 (+ rank), k = 30; generated on the device (synthetic stand-in for the
+reference's own make_blobs workloads; no dataset is downloaded).
+
+One step = one kNN-graph build of the whole workload (every row's 30
+neighbours) in the headline form: tcgen05 BF16 exact scan keeping 2k
+candidates per row, FP32 rerank (FP64 at the k-th boundary).
+
+  value    edges/s (rows x k / step time) with the rows already in HBM,
+           step timed with CUDA events on the library's own stream, max over
+           ranks; each rank builds its own independent graph (weak scaling).
+  e2e      the same through the public API with pinned HOST buffers: the
+           host->device copy of the rows and the device->host copy of the
+           indices and distances are inside every timed step.
+  roofline the dominant kernel (the BF16 scan): 2 n^2 d algorithmic FLOPs per
+           launch over its CUDA-event duration, against the measured BF16 peak.
+  fp32_form the plain FP32 SIMT form on a slice of query rows against all rows.
+  cpu_baseline  the reference's NN-descent (restated in oracle/, all host
+           threads) on a bounded prefix of the same workload.
+
+--impl reference runs only that CPU path, on the same metric and workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "evoc-rs_b200"))
+sys.path.insert(0, ROOT)
+
+METRIC = "kNN edges/s at recall@k>=0.99 vs FP64 (BF16+FP32-rerank form)"
+UNIT = "edges/s"
+WORKLOAD = "zipf_1m_768: 1,000,000 x 768 f32, 200 Zipf(1.1) clusters, cosine k=30, seed 7"
+
+# DRAM bytes (read + write) of one launch of the BF16 scan, from
+#   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum --clock-control none -k regex:tc_scan
+# on the full workload (see profiles/tc_scan_bf16_zipf_1m_768.md); None until captured.
+SCAN_TRAFFIC_BYTES = None
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampled every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str, path: str):
+        self.path = path
+        self.proc = None
+        try:
+            self.f = open(path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", gpu_id], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        loaded = [s for s, p in zip(sm, power) if p > 0.5 * max(power)] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm), "power_w_max": max(power)}
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_nndescent_sample(x_host, k, rows, threads, deterministic=False):
+    """The reference's knn_graph NN-descent (restated in oracle/) on a prefix."""
+    from oracle import oracle as O
+
+    O.build()
+    O.set_num_threads(threads)
+    sub = x_host[:rows].copy()
+    t0 = time.perf_counter()
+    ind, dst = O.knn_graph(sub, k, O.RandomState(7), deterministic=deterministic, n_threads=threads)
+    return time.perf_counter() - t0, ind
+
+
+def run_reference(args, world, rank):
+    import numpy as np
+
+    from evoc import synthetic
+
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    rows = args.cpu_rows
+    x = synthetic.zipf_f32(n=rows, dim=args.dim, seed=7)
+    for _ in range(args.warmup):
+        cpu_nndescent_sample(x, args.k, rows, threads)
+    times = []
+    for _ in range(args.steps):
+        t, _ = cpu_nndescent_sample(x, args.k, rows, threads)
+        times.append(t)
+    ms = 1000.0 * sum(times) / len(times)
+    value = rows * args.k / (ms / 1000.0)
+    sample = (f"NN-descent (RP forest + sorted local join, src/knn.rs / src/nndescent/float.rs restated in "
+              f"oracle/evoc_oracle.c) on a {rows}-row prefix-sized draw of the same distribution, {threads} threads")
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": WORKLOAD, "n": args.n, "d": args.dim, "k": args.k, "sample_rows": rows},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def recall_vs_fp64(x, ind, rows, k):
+    """recall@k and max |distance - FP64 distance| of the reported pairs, on query rows [0, rows)."""
+    import torch
+
+    hits = 0
+    max_err = 0.0
+    X64 = x.double()
+    for r0 in range(0, rows, 256):
+        r1 = min(rows, r0 + 256)
+        q = X64[r0:r1]
+        s = q @ X64.T
+        s[torch.arange(r1 - r0), torch.arange(r0, r1)] = 2.0  # self first
+        top = s.topk(k, dim=1).indices
+        got = ind[r0:r1].long()
+        hits += (top.unsqueeze(2) == got.unsqueeze(1)).any(dim=2).sum().item()
+    return hits / (rows * k), max_err
+
+
+def transform_f64(dots, self_mask):
+    import torch
+
+    d = torch.where(dots > 0, -torch.log2(dots.clamp(min=1e-300)), torch.zeros_like(dots))
+    d = torch.clamp(d, min=0.0)
+    d[self_mask] = 0.0
+    return d
+
+
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+
+    import evoc
+    from evoc import _lib, synthetic
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+        pg = dist
+    n, d, k = args.n, args.dim, args.k
+    x = synthetic.zipf_f32(n=n, dim=d, seed=7 + rank, device=dev)
+    oi = torch.empty((n, k), dtype=torch.int32, device=dev)
+    od = torch.empty((n, k), dtype=torch.float32, device=dev)
+    torch.cuda.synchronize()
+    ctx = _lib.context(local)
+    ctx.profile(True)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=dev)
+    opts = evoc.KnnGraphOptions(n_neighbors=k, form="bf16_rerank", oversample=2, device=local)
+
+    def step():
+        evoc.knn_graph_device(x.data_ptr(), 0, n, d, k, oi.data_ptr(), od.data_ptr(), opts)
+
+    for _ in range(args.warmup):
+        step()
+    gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
+    clocks = ClockSampler(gpu_id, os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv"))
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    stage_ms = {}
+    launches = 0
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+        for name, ms in ctx.stages():
+            stage_ms.setdefault(name, []).append(ms)
+        launches += ctx.launches()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    clk = clocks.stop()
+    total_ms = ev0.elapsed_time(ev1)
+    ms_step = total_ms / args.steps
+    if pg:
+        t = torch.tensor([ms_step], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms_step = float(t.item())
+    value = world * n * k / (ms_step / 1000.0)
+
+    # Recall / error vs FP64 on a 10,000-row query sample (untimed).
+    sample = min(args.recall_rows, n)
+    rec, _ = recall_vs_fp64(x, oi, sample, k)
+    X64 = x.double()
+    got = oi[:sample].long()
+    dots = (X64[:sample].unsqueeze(1) * X64[got]).sum(-1)
+    selfm = got == torch.arange(sample, device=dev).unsqueeze(1)
+    want = transform_f64(dots, selfm)
+    max_err = float((od[:sample].double() - want).abs().max().item())
+
+    # End to end through the public API with pinned host buffers.
+    xh = torch.empty((n, d), dtype=torch.float32, pin_memory=True)
+    xh.copy_(x)
+    ih = torch.empty((n, k), dtype=torch.int32, pin_memory=True)
+    dh = torch.empty((n, k), dtype=torch.float32, pin_memory=True)
+    xh_np, ih_np, dh_np = xh.numpy(), ih.numpy(), dh.numpy()
+    evoc.knn_graph(xh_np, opts, None, out=(ih_np, dh_np))  # warm the host path
+    if pg:
+        pg.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        evoc.knn_graph(xh_np, opts, None, out=(ih_np, dh_np))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.e2e_steps
+    if pg:
+        t = torch.tensor([e2e_ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * n * k / (e2e_ms / 1000.0)
+    e2e_consistent = bool(np.array_equal(ih_np[:1000], oi[:1000].cpu().numpy()))
+
+    # Plain FP32 SIMT form on a slice of query rows against all n rows.
+    fp32 = None
+    if args.fp32_rows > 0:
+        rows = min(args.fp32_rows, n)
+        fo = evoc.KnnGraphOptions(n_neighbors=k, form="fp32", device=local, row_begin=0, row_end=rows)
+        fi = torch.empty((rows, k), dtype=torch.int32, device=dev)
+        fd = torch.empty((rows, k), dtype=torch.float32, device=dev)
+        warm = evoc.KnnGraphOptions(n_neighbors=k, form="fp32", device=local, row_begin=0, row_end=128)
+        evoc.knn_graph_device(x.data_ptr(), 0, n, d, k, fi.data_ptr(), fd.data_ptr(), warm)
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        evoc.knn_graph_device(x.data_ptr(), 0, n, d, k, fi.data_ptr(), fd.data_ptr(), fo)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        fms = f0.elapsed_time(f1)
+        frec, _ = recall_vs_fp64(x, fi, min(sample, rows), k)
+        same = (fi[:sample] == oi[:sample]).float().mean().item()
+        fp32 = {"value": rows * k / (fms / 1000.0), "unit": UNIT, "query_rows": rows, "key_rows": n,
+                "ms": fms, "recall_at_k_vs_fp64": frec, "index_agreement_with_bf16_form": same,
+                "tflops_fp32": 2.0 * rows * n * d / (fms / 1000.0) / 1e12}
+
+    peaks, peak_kind = measured_peaks()
+    scan_ms = statistics.mean(stage_ms.get("bf16_scan", [float("nan")]))
+    flops = 2.0 * n * n * d
+    achieved = flops / (scan_ms / 1000.0) / 1e12
+    peak = float(peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops")))
+    roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": SCAN_TRAFFIC_BYTES, "kernel": "tc_scan_kernel (BF16, fused top-2k)",
+                "peak_kind": f"{peak_kind} bf16 sustained (burst {peaks.get('bf16_tflops')})",
+                "launch_ms": scan_ms}
+
+    cpu = None
+    if rank == 0 and world == 1 and args.cpu_rows > 0:
+        xs = x[: args.cpu_rows].cpu().numpy()
+        threads = os.cpu_count() or 1
+        t, cind = cpu_nndescent_sample(xs, k, args.cpu_rows, threads)
+        xs64 = torch.from_numpy(xs).double().to(dev)
+        s = xs64 @ xs64.T
+        s.fill_diagonal_(2.0)
+        top = s.topk(k, dim=1).indices
+        cg = torch.from_numpy(cind).long().to(dev)
+        crec = (top.unsqueeze(2) == cg.unsqueeze(1)).any(dim=2).float().mean().item()
+        cpu = {"value": args.cpu_rows * k / t, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": (f"reference NN-descent restated in oracle/ (rlx-cpu path: serial-order f32 dot, "
+                          f"{threads} threads) on the first {args.cpu_rows} rows of the workload; "
+                          f"{t:.1f} s; its recall@{k} vs FP64 on that sample {crec:.4f}")}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16 tensor-core scan + f32 rerank", "data": "synthetic (generated on device, seeded)",
+        "config": {"workload": WORKLOAD, "n": n, "d": d, "k": k, "form": "bf16_rerank", "oversample": 2,
+                   "l2": "inputs larger than L2 (3.1 GB f32 + 1.5 GB bf16 vs 126 MB)",
+                   "per_rank": "independent graph per rank"},
+        "recall_at_k_vs_fp64": rec, "max_abs_dist_err_vs_fp64": max_err, "recall_sample_rows": sample,
+        "stages_ms": {kname: statistics.mean(v) for kname, v in stage_ms.items()},
+        "roofline": roofline,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n * d * 4, "d2h_bytes_per_step": n * k * 8,
+                "ms_per_step": e2e_ms, "matches_device_path": e2e_consistent},
+        "fp32_form": fp32,
+        "cpu_baseline": cpu,
+        "clocks": clk,
+        "gpu_launches": launches,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=1_000_000)
+    ap.add_argument("--dim", type=int, default=768)
+    ap.add_argument("--k", type=int, default=30)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--fp32-rows", type=int, default=75_776)  # 2 full waves of 296 CTAs x 128 rows
+    ap.add_argument("--recall-rows", type=int, default=10_000)
+    ap.add_argument("--cpu-rows", type=int, default=6_000)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    world, rank, local = dist_env()
+    if args.impl == "reference":
+        return run_reference(args, world, rank)
+    return run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

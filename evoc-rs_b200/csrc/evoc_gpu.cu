@@ -9,6 +9,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "../../include/evoc_gpu.h"
 #include "common.cuh"
@@ -44,6 +45,11 @@ struct DevBuf {
   }
 };
 
+struct StageRec {
+  std::string name;
+  cudaEvent_t a = nullptr, b = nullptr;
+};
+
 }  // namespace
 
 struct evoc_gpu_ctx {
@@ -53,8 +59,12 @@ struct evoc_gpu_ctx {
   std::mutex mu;
   std::string err;
   DevBuf x, scratch, norms, flag, out_idx, out_raw, out_dist;
-  DevBuf xb, cand, cand_raw, labels, order, hist, cursor, pivots, scratch2;
+  DevBuf xb, cand, labels, order, hist, cursor, pivots;
   uint64_t timeout_ns = 4000000000ull;  // longest a pipeline wait inside a kernel may take
+  bool profiling = false;
+  std::vector<StageRec> stages;  // event pool; the first n_stages belong to the last call
+  int n_stages = 0;
+  int launches = 0;
 };
 
 namespace {
@@ -69,11 +79,33 @@ int cuda_fail(evoc_gpu_ctx* ctx, cudaError_t e, const char* where) {
   return fail(ctx, e == cudaErrorMemoryAllocation ? EVOC_ERR_OOM : EVOC_ERR_CUDA, m);
 }
 
-#define EVOC_TRY(expr, where)                    \
-  do {                                           \
-    cudaError_t _e = (expr);                     \
+#define EVOC_TRY(expr, where)                                \
+  do {                                                       \
+    cudaError_t _e = (expr);                                 \
     if (_e != cudaSuccess) return cuda_fail(ctx, _e, where); \
   } while (0)
+
+// Records CUDA events around one stage on the context's stream when profiling.
+struct Stage {
+  evoc_gpu_ctx* ctx;
+  int idx = -1;
+  Stage(evoc_gpu_ctx* c, const char* name) : ctx(c) {
+    if (!ctx->profiling) return;
+    if (ctx->n_stages == int(ctx->stages.size())) {
+      StageRec r;
+      if (cudaEventCreate(&r.a) != cudaSuccess || cudaEventCreate(&r.b) != cudaSuccess) return;
+      ctx->stages.push_back(r);
+    }
+    idx = ctx->n_stages++;
+    ctx->stages[size_t(idx)].name = name;
+    cudaEventRecord(ctx->stages[size_t(idx)].a, ctx->stream);
+  }
+  void end() {
+    if (idx >= 0) cudaEventRecord(ctx->stages[size_t(idx)].b, ctx->stream);
+    idx = -1;
+  }
+  ~Stage() { end(); }
+};
 
 inline int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 
@@ -82,9 +114,10 @@ int resolve_form(int32_t dtype, int32_t form) {
   return form;
 }
 
-// Copies the caller's rows into a zero-padded device matrix of `ld` elements per row.
-// Rows past n (up to padded_rows(n)) are zero.
+// Copies the caller's rows into a zero-padded device matrix of `ld_bytes` per
+// row.  Rows past n (up to padded_rows(n)) are zero.
 int stage_rows(evoc_gpu_ctx* ctx, const void* data, int64_t n, int64_t row_bytes, int64_t ld_bytes, bool on_device) {
+  Stage st(ctx, on_device ? "copy_rows" : "h2d_rows");
   const int64_t rows = evoc::padded_rows(n);
   EVOC_TRY(ctx->x.ensure(size_t(rows * ld_bytes)), "alloc rows");
   if (ld_bytes != row_bytes)
@@ -98,93 +131,112 @@ int stage_rows(evoc_gpu_ctx* ctx, const void* data, int64_t n, int64_t row_bytes
   return EVOC_OK;
 }
 
-
-int run_fp32(evoc_gpu_ctx* ctx, int64_t n, int ld, int d, int keff, int32_t* d_idx, float* d_raw, float* d_dist) {
-  const int cap = evoc::topk_capacity(keff);
-  const int64_t qblocks = (n + 127) / 128;
-  const int grid = int(qblocks < int64_t(ctx->sms) * 2 ? qblocks : int64_t(ctx->sms) * 2);
-  EVOC_TRY(ctx->scratch.ensure(size_t(grid) * 128 * size_t(cap) * 8), "alloc scratch");
-  EVOC_TRY(evoc::launch_knn_f32_simt(ctx->x.as<float>(), n, ld, keff, cap, ctx->scratch.as<uint64_t>(), grid, d_idx,
-                                     d_raw, d_dist, 0, n, ctx->stream),
-           "knn_f32_simt");
-  (void)d;
-  return EVOC_OK;
-}
-
-// Grid of the persistent tensor-core scan over n_q query rows.
 int scan_grid(const evoc_gpu_ctx* ctx, int64_t n_q) {
   const int64_t qblocks = (n_q + 127) / 128;
   return int(qblocks < ctx->sms ? qblocks : ctx->sms);
 }
 
+// One kNN request: all n rows are keys; query rows r0 .. r0+nq-1 are output rows 0 .. nq-1.
+struct Job {
+  int64_t n, r0, nq;
+  int keff;
+  int32_t* idx;
+  float* raw;
+  float* dist;
+  int* status;
+};
+
+int run_fp32(evoc_gpu_ctx* ctx, const Job& j, int ld) {
+  Stage st(ctx, "fp32_scan");
+  const int cap = evoc::topk_capacity(j.keff);
+  const int64_t qblocks = (j.nq + 127) / 128;
+  const int grid = int(qblocks < int64_t(ctx->sms) * 2 ? qblocks : int64_t(ctx->sms) * 2);
+  EVOC_TRY(ctx->scratch.ensure(size_t(grid) * 128 * size_t(cap) * 8), "alloc scratch");
+  EVOC_TRY(evoc::launch_knn_f32_simt(ctx->x.as<float>(), j.n, ld, j.keff, cap, ctx->scratch.as<uint64_t>(), grid,
+                                     j.idx, j.raw, j.dist, j.r0, j.r0 + j.nq, ctx->stream),
+           "knn_f32_simt");
+  ctx->launches += 1;
+  return EVOC_OK;
+}
+
 // Query rows grouped by nearest pivot so that concurrently reranked rows share
-// candidates in L2.  Leaves ctx->order holding a permutation of 0..n-1.
-int locality_order(evoc_gpu_ctx* ctx, const void* rows, int64_t n, int64_t row_bytes, bool int8, int* status) {
-  int64_t n_piv = n / 256;
+// candidates in L2.  Leaves ctx->order holding a permutation of 0..nq-1.
+int locality_order(evoc_gpu_ctx* ctx, const Job& j, const void* rows, int64_t row_bytes, bool int8) {
+  Stage st(ctx, "pivot_order");
+  int64_t n_piv = j.n / 256;
   if (n_piv > 4096) n_piv = 4096;
   if (n_piv < 2) n_piv = 2;
   const int64_t piv_rows = evoc::padded_rows(n_piv);
   EVOC_TRY(ctx->pivots.ensure(size_t(piv_rows * row_bytes)), "alloc pivots");
   EVOC_TRY(cudaMemsetAsync(ctx->pivots.p, 0, size_t(piv_rows * row_bytes), ctx->stream), "clear pivots");
-  EVOC_TRY(evoc::launch_gather_pivots(rows, row_bytes, n, n_piv, ctx->pivots.p, ctx->sms, ctx->stream),
+  EVOC_TRY(evoc::launch_gather_pivots(rows, row_bytes, j.n, n_piv, ctx->pivots.p, ctx->sms, ctx->stream),
            "gather pivots");
-  const int cap = evoc::topk_capacity(1);
-  const int grid = scan_grid(ctx, n);
-  EVOC_TRY(ctx->scratch2.ensure(size_t(grid) * 128 * size_t(cap) * 8), "alloc scratch2");
-  EVOC_TRY(ctx->labels.ensure(size_t(n) * 4), "alloc labels");
-  EVOC_TRY(evoc::launch_tc_scan(int8, rows, evoc::padded_rows(n), n, ctx->pivots.p, piv_rows, n_piv, row_bytes, 1, cap, ctx->scratch2.as<uint64_t>(),
-                                grid, 0, 0, 0, ctx->labels.as<int32_t>(), nullptr, nullptr, status, ctx->timeout_ns,
-                                ctx->stream),
+  const int grid = scan_grid(ctx, j.nq);
+  EVOC_TRY(ctx->labels.ensure(size_t(j.nq) * 4), "alloc labels");
+  EVOC_TRY(evoc::launch_tc_scan(int8, rows, evoc::padded_rows(j.n), j.r0, j.nq, ctx->pivots.p, piv_rows, n_piv,
+                                row_bytes, 1, nullptr, grid, 0, 0, 0, ctx->labels.as<int32_t>(), nullptr, nullptr,
+                                j.status, ctx->timeout_ns, ctx->stream),
            "pivot scan");
-  EVOC_TRY(ctx->order.ensure(size_t(n) * 4), "alloc order");
+  EVOC_TRY(ctx->order.ensure(size_t(j.nq) * 4), "alloc order");
   EVOC_TRY(ctx->hist.ensure(size_t(n_piv) * 4), "alloc hist");
   EVOC_TRY(ctx->cursor.ensure(size_t(n_piv) * 4), "alloc cursor");
-  EVOC_TRY(evoc::launch_order_by_label(ctx->labels.as<int32_t>(), n, int(n_piv), ctx->hist.as<int32_t>(),
+  EVOC_TRY(evoc::launch_order_by_label(ctx->labels.as<int32_t>(), j.nq, int(n_piv), ctx->hist.as<int32_t>(),
                                        ctx->cursor.as<int32_t>(), ctx->order.as<int32_t>(), ctx->sms, ctx->stream),
            "order by pivot");
+  ctx->launches += 5;
   return EVOC_OK;
 }
 
-int run_bf16_rerank(evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, int64_t n, int ld, int d, int keff,
-                    int32_t* d_idx, float* d_raw, float* d_dist, int* status) {
+int run_bf16_rerank(evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, const Job& j, int ld, int d) {
   const int over = opts.oversample > 0 ? opts.oversample : 2;
-  int64_t C = int64_t(over) * keff;
-  if (C > n) C = n;
-  if (C < keff) C = keff;
+  int64_t C = int64_t(over) * j.keff;
+  if (C > j.n) C = j.n;
+  if (C < j.keff) C = j.keff;
   if (C > 256) return fail(ctx, EVOC_ERR_UNSUPPORTED, "oversample * k must be <= 256");
   const int64_t ldb = round_up(d, 64);
-  const int64_t rows = evoc::padded_rows(n);
-  EVOC_TRY(ctx->xb.ensure(size_t(rows * ldb * 2)), "alloc bf16 rows");
-  EVOC_TRY(evoc::launch_to_bf16(ctx->x.as<float>(), rows, ld, d, ctx->xb.p, int(ldb), ctx->sms, ctx->stream), "to bf16");
-  const int cap = evoc::topk_capacity(int(C));
-  const int grid = scan_grid(ctx, n);
-  EVOC_TRY(ctx->scratch.ensure(size_t(grid) * 128 * size_t(cap) * 8), "alloc scratch");
-  EVOC_TRY(ctx->cand.ensure(size_t(n * C) * 4), "alloc candidates");
-  EVOC_TRY(evoc::launch_tc_scan(false, ctx->xb.p, rows, n, ctx->xb.p, rows, n, ldb * 2, int(C), cap, ctx->scratch.as<uint64_t>(),
-                                grid, 1, 0, 0, ctx->cand.as<int32_t>(), nullptr, nullptr, status, ctx->timeout_ns,
-                                ctx->stream),
-           "bf16 scan");
+  const int64_t rows = evoc::padded_rows(j.n);
+  {
+    Stage st(ctx, "to_bf16");
+    EVOC_TRY(ctx->xb.ensure(size_t(rows * ldb * 2)), "alloc bf16 rows");
+    EVOC_TRY(evoc::launch_to_bf16(ctx->x.as<float>(), rows, ld, d, ctx->xb.p, int(ldb), ctx->sms, ctx->stream),
+             "to bf16");
+    ctx->launches += 1;
+  }
+  const int grid = scan_grid(ctx, j.nq);
+  EVOC_TRY(ctx->cand.ensure(size_t(j.nq * C) * 4), "alloc candidates");
+  {
+    Stage st(ctx, "bf16_scan");
+    EVOC_TRY(ctx->scratch.ensure(size_t(grid) * 256 * size_t(C) * 8), "alloc scratch");
+    EVOC_TRY(evoc::launch_tc_scan(false, ctx->xb.p, rows, j.r0, j.nq, ctx->xb.p, rows, j.n, ldb * 2, int(C),
+                                  ctx->scratch.as<uint64_t>(), grid, 1, 0, 0, ctx->cand.as<int32_t>(), nullptr,
+                                  nullptr, j.status, ctx->timeout_ns, ctx->stream),
+             "bf16 scan");
+    ctx->launches += 1;
+  }
   const int32_t* order = nullptr;
-  if (n >= 65536) {
-    int rc = locality_order(ctx, ctx->xb.p, n, ldb * 2, false, status);
+  if (j.nq >= 65536) {
+    int rc = locality_order(ctx, j, ctx->xb.p, ldb * 2, false);
     if (rc) return rc;
     order = ctx->order.as<int32_t>();
   }
-  EVOC_TRY(evoc::launch_rerank_f32(ctx->x.as<float>(), ld, d, n, ctx->cand.as<int32_t>(), int(C), keff, order, d_idx,
-                                   d_raw, d_dist, ctx->sms, ctx->stream),
+  Stage st(ctx, "rerank");
+  EVOC_TRY(evoc::launch_rerank_f32(ctx->x.as<float>(), ld, d, j.nq, j.r0, ctx->cand.as<int32_t>(), int(C), j.keff,
+                                   order, j.idx, j.raw, j.dist, ctx->sms, ctx->stream),
            "rerank");
+  ctx->launches += 1;
   return EVOC_OK;
 }
 
-int run_int8(evoc_gpu_ctx* ctx, int64_t n, int64_t ldb, int keff, int32_t* d_idx, float* d_raw, float* d_dist,
-             int* status) {
-  const int cap = evoc::topk_capacity(keff);
-  const int grid = scan_grid(ctx, n);
-  EVOC_TRY(ctx->scratch.ensure(size_t(grid) * 128 * size_t(cap) * 8), "alloc scratch");
-  const int64_t rows = evoc::padded_rows(n);
-  EVOC_TRY(evoc::launch_tc_scan(true, ctx->x.p, rows, n, ctx->x.p, rows, n, ldb, keff, cap, ctx->scratch.as<uint64_t>(), grid, 1,
-                                1, EVOC_DTYPE_I8, d_idx, d_raw, d_dist, status, ctx->timeout_ns, ctx->stream),
+int run_int8(evoc_gpu_ctx* ctx, const Job& j, int64_t ldb) {
+  Stage st(ctx, "int8_scan");
+  const int grid = scan_grid(ctx, j.nq);
+  const int64_t rows = evoc::padded_rows(j.n);
+  EVOC_TRY(ctx->scratch.ensure(size_t(grid) * 256 * size_t(j.keff) * 8), "alloc scratch");
+  EVOC_TRY(evoc::launch_tc_scan(true, ctx->x.p, rows, j.r0, j.nq, ctx->x.p, rows, j.n, ldb, j.keff,
+                                ctx->scratch.as<uint64_t>(), grid, 1, 1, EVOC_DTYPE_I8, j.idx, j.raw, j.dist, j.status,
+                                ctx->timeout_ns, ctx->stream),
            "int8 scan");
+  ctx->launches += 1;
   return EVOC_OK;
 }
 
@@ -194,6 +246,8 @@ int knn_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtype, con
   if (!ctx) return EVOC_ERR_ARG;
   std::lock_guard<std::mutex> lock(ctx->mu);
   ctx->err.clear();
+  ctx->n_stages = 0;
+  ctx->launches = 0;
   evoc_gpu_opts opts;
   evoc_gpu_default_opts(&opts);
   if (opts_in) {
@@ -207,6 +261,12 @@ int knn_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtype, con
   if (dim <= 0) return fail(ctx, EVOC_ERR_ARG, "dim must be positive");
   if (dtype < EVOC_DTYPE_F32 || dtype > EVOC_DTYPE_U8) return fail(ctx, EVOC_ERR_ARG, "unknown dtype");
   if (n >= (int64_t(1) << 31) - 1) return fail(ctx, EVOC_ERR_ARG, "n exceeds int32 index range");
+  int64_t r0 = 0, r1 = n;
+  if (opts.row_begin != 0 || opts.row_end != 0) {
+    r0 = opts.row_begin;
+    r1 = opts.row_end;
+    if (r0 < 0 || r1 > n || r0 >= r1) return fail(ctx, EVOC_ERR_ARG, "row_begin/row_end out of range");
+  }
   int64_t kk = k < n - 1 ? k : n - 1;
   if (kk < 1) kk = 1;
   const int keff = int(kk);
@@ -214,26 +274,28 @@ int knn_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtype, con
   const int form = resolve_form(dtype, opts.form);
   const bool on_dev = opts.buffers_on_device != 0;
   EVOC_TRY(cudaSetDevice(ctx->device), "cudaSetDevice");
+  Stage total(ctx, "total");
 
   // Output staging.
-  int32_t* d_idx = out_idx;
-  float* d_dist = out_dist;
-  float* d_raw = out_raw;
-  const size_t out_elems = size_t(n) * size_t(keff);
+  const int64_t nq = r1 - r0;
+  const size_t out_elems = size_t(nq) * size_t(keff);
+  Job job{n, r0, nq, keff, out_idx, out_raw, out_dist, nullptr};
   if (!on_dev) {
     EVOC_TRY(ctx->out_idx.ensure(out_elems * 4), "alloc out_idx");
-    EVOC_TRY(ctx->out_dist.ensure(out_elems * 4), "alloc out_dist");
-    d_idx = ctx->out_idx.as<int32_t>();
-    d_dist = out_dist ? ctx->out_dist.as<float>() : nullptr;
+    job.idx = ctx->out_idx.as<int32_t>();
+    if (out_dist) {
+      EVOC_TRY(ctx->out_dist.ensure(out_elems * 4), "alloc out_dist");
+      job.dist = ctx->out_dist.as<float>();
+    }
     if (out_raw) {
       EVOC_TRY(ctx->out_raw.ensure(out_elems * 4), "alloc out_raw");
-      d_raw = ctx->out_raw.as<float>();
+      job.raw = ctx->out_raw.as<float>();
     }
   }
-
   EVOC_TRY(ctx->flag.ensure(64), "alloc flag");
   int* d_flags = ctx->flag.as<int>();  // [0] prepare_float, [1] scan status
   EVOC_TRY(cudaMemsetAsync(d_flags, 0, 64, ctx->stream), "clear flags");
+  job.status = d_flags + 1;
   int rc = EVOC_OK;
   if (dtype == EVOC_DTYPE_F32) {
     if (form != EVOC_FORM_FP32 && form != EVOC_FORM_BF16_RERANK)
@@ -241,37 +303,41 @@ int knn_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtype, con
     const int ld = int(round_up(dim, 16));
     rc = stage_rows(ctx, data, n, dim * 4, int64_t(ld) * 4, on_dev);
     if (rc) return rc;
-    EVOC_TRY(ctx->norms.ensure(size_t(n) * 4), "alloc norms");
-    EVOC_TRY(evoc::launch_prepare_float(ctx->x.as<float>(), n, ld, int(dim), ctx->norms.as<float>(), d_flags,
-                                        ctx->sms, ctx->stream),
-             "prepare_float");
-    if (form == EVOC_FORM_FP32) rc = run_fp32(ctx, n, ld, int(dim), keff, d_idx, d_raw, d_dist);
-    else rc = run_bf16_rerank(ctx, opts, n, ld, int(dim), keff, d_idx, d_raw, d_dist, d_flags + 1);
+    {
+      Stage st(ctx, "prepare_float");
+      EVOC_TRY(ctx->norms.ensure(size_t(n) * 4), "alloc norms");
+      EVOC_TRY(evoc::launch_prepare_float(ctx->x.as<float>(), n, ld, int(dim), ctx->norms.as<float>(), d_flags,
+                                          ctx->sms, ctx->stream),
+               "prepare_float");
+      ctx->launches += 2;
+    }
+    if (form == EVOC_FORM_FP32) rc = run_fp32(ctx, job, ld);
+    else rc = run_bf16_rerank(ctx, opts, job, ld, int(dim));
   } else if (dtype == EVOC_DTYPE_I8) {
     if (form != EVOC_FORM_EXACT_INT) return fail(ctx, EVOC_ERR_UNSUPPORTED, "form not built for i8 in this library");
     const int64_t ldb = round_up(dim, 128);
     rc = stage_rows(ctx, data, n, dim, ldb, on_dev);
     if (rc) return rc;
-    rc = run_int8(ctx, n, ldb, keff, d_idx, d_raw, d_dist, d_flags + 1);
+    rc = run_int8(ctx, job, ldb);
   } else {
     return fail(ctx, EVOC_ERR_UNSUPPORTED, "dtype form not built in this library");
   }
   if (rc) return rc;
   int flags[2] = {0, 0};
+  if (!on_dev) {
+    Stage st(ctx, "d2h_out");
+    EVOC_TRY(cudaMemcpyAsync(out_idx, job.idx, out_elems * 4, cudaMemcpyDeviceToHost, ctx->stream), "download idx");
+    if (out_dist)
+      EVOC_TRY(cudaMemcpyAsync(out_dist, job.dist, out_elems * 4, cudaMemcpyDeviceToHost, ctx->stream),
+               "download dist");
+    if (out_raw)
+      EVOC_TRY(cudaMemcpyAsync(out_raw, job.raw, out_elems * 4, cudaMemcpyDeviceToHost, ctx->stream), "download raw");
+  }
   EVOC_TRY(cudaMemcpyAsync(flags, d_flags, sizeof(flags), cudaMemcpyDeviceToHost, ctx->stream), "read status");
+  total.end();
   EVOC_TRY(cudaStreamSynchronize(ctx->stream), "knn_graph");
   if (flags[1] != 0)
     return fail(ctx, EVOC_ERR_TIMEOUT, "a kernel pipeline wait timed out (stage " + std::to_string(flags[1]) + ")");
-
-  if (!on_dev) {
-    EVOC_TRY(cudaMemcpyAsync(out_idx, d_idx, out_elems * 4, cudaMemcpyDeviceToHost, ctx->stream), "download idx");
-    if (out_dist)
-      EVOC_TRY(cudaMemcpyAsync(out_dist, d_dist, out_elems * 4, cudaMemcpyDeviceToHost, ctx->stream),
-               "download dist");
-    if (out_raw)
-      EVOC_TRY(cudaMemcpyAsync(out_raw, d_raw, out_elems * 4, cudaMemcpyDeviceToHost, ctx->stream), "download raw");
-  }
-  EVOC_TRY(cudaStreamSynchronize(ctx->stream), "knn_graph outputs");
   return EVOC_OK;
 }
 
@@ -287,10 +353,6 @@ void evoc_gpu_default_opts(evoc_gpu_opts* o) {
   o->struct_size = sizeof(evoc_gpu_opts);
   o->form = EVOC_FORM_AUTO;
   o->oversample = 2;
-  o->buffers_on_device = 0;
-  o->deterministic = 0;
-  o->n_iters = 0;
-  o->max_candidates = 0;
   o->delta = 0.001f;
   o->delta_improv = 0.001f;
 }
@@ -320,15 +382,46 @@ void evoc_gpu_ctx_destroy(evoc_gpu_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-  DevBuf* bufs[] = {&ctx->x,      &ctx->scratch, &ctx->norms,  &ctx->flag,   &ctx->out_idx, &ctx->out_raw,
-                    &ctx->out_dist, &ctx->xb,    &ctx->cand,   &ctx->cand_raw, &ctx->labels, &ctx->order,
-                    &ctx->hist,   &ctx->cursor,  &ctx->pivots, &ctx->scratch2};
+  DevBuf* bufs[] = {&ctx->x,        &ctx->scratch, &ctx->norms, &ctx->flag,   &ctx->out_idx,
+                    &ctx->out_raw,  &ctx->out_dist, &ctx->xb,   &ctx->cand,   &ctx->labels,
+                    &ctx->order,    &ctx->hist,    &ctx->cursor, &ctx->pivots};
   for (DevBuf* b : bufs) b->release();
+  for (auto& r : ctx->stages) {
+    if (r.a) cudaEventDestroy(r.a);
+    if (r.b) cudaEventDestroy(r.b);
+  }
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
 
 const char* evoc_gpu_last_error(const evoc_gpu_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+void* evoc_gpu_ctx_stream(const evoc_gpu_ctx* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
+
+int evoc_gpu_profile_enable(evoc_gpu_ctx* ctx, int enable) {
+  if (!ctx) return EVOC_ERR_ARG;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  ctx->profiling = enable != 0;
+  return EVOC_OK;
+}
+
+int evoc_gpu_profile_count(const evoc_gpu_ctx* ctx) { return ctx ? ctx->n_stages : 0; }
+
+int evoc_gpu_profile_stage(const evoc_gpu_ctx* ctx, int i, char* name, int name_len, float* ms) {
+  if (!ctx || i < 0 || i >= ctx->n_stages) return EVOC_ERR_ARG;
+  const StageRec& r = ctx->stages[size_t(i)];
+  if (name && name_len > 0) {
+    std::strncpy(name, r.name.c_str(), size_t(name_len) - 1);
+    name[name_len - 1] = '\0';
+  }
+  if (ms) {
+    cudaSetDevice(ctx->device);
+    if (cudaEventElapsedTime(ms, r.a, r.b) != cudaSuccess) return EVOC_ERR_CUDA;
+  }
+  return EVOC_OK;
+}
+
+int evoc_gpu_last_launch_count(const evoc_gpu_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
 int evoc_gpu_knn_graph(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts, int32_t dtype, const void* data, int64_t n,
                        int64_t dim, int32_t k, const int64_t* rng_state, int32_t* out_idx, float* out_dist,

@@ -35,18 +35,19 @@ namespace evoc {
 cudaError_t launch_to_bf16(const float* X, int64_t n, int ld, int d, void* Y, int ldb, int sms, cudaStream_t stream);
 
 // tc_scan.cu: tcgen05 exact scan (BF16 -> F32, or S8 -> S32) with fused top-k.
-//   Q: n_q of q_rows rows, K: n_k of k_rows rows, `row_bytes` per row (multiple of 128, 16-byte aligned
-//   bases); q_rows is a multiple of 128 and k_rows of 256, rows past n are zero.
+//   Q: query rows q_row0 .. q_row0+n_q-1 of a q_rows-row matrix; K: the first n_k of k_rows rows;
+//   `row_bytes` per row (multiple of 128, 16-byte aligned bases); q_rows and k_rows are multiples
+//   of 256 and rows past the data are zero.  Query i is written to output row i.
 //   final_mode 1: out rows of `keep` sorted (idx, raw, transformed dist); 0: candidates (idx, raw).
 size_t tc_scan_smem_bytes();
-cudaError_t launch_tc_scan(bool int8, const void* Q, int64_t q_rows, int64_t n_q, const void* K, int64_t k_rows,
-                           int64_t n_k, int64_t row_bytes, int keep, int cap, uint64_t* scratch, int grid, int self_mode, int final_mode, int dtype,
-                           int32_t* out_idx, float* out_raw, float* out_dist, int* status, uint64_t timeout_ns,
-                           cudaStream_t stream);
+cudaError_t launch_tc_scan(bool int8, const void* Q, int64_t q_rows, int64_t q_row0, int64_t n_q, const void* K,
+                           int64_t k_rows, int64_t n_k, int64_t row_bytes, int keep, uint64_t* scratch, int grid,
+                           int self_mode, int final_mode, int dtype, int32_t* out_idx, float* out_raw, float* out_dist,
+                           int* status, uint64_t timeout_ns, cudaStream_t stream);
 
 // rerank.cu
-cudaError_t launch_rerank_f32(const float* X, int ld, int d, int64_t n, const int32_t* cand, int C, int k,
-                              const int32_t* order, int32_t* out_idx, float* out_raw, float* out_dist, int sms,
+cudaError_t launch_rerank_f32(const float* X, int ld, int d, int64_t n_q, int64_t q_row0, const int32_t* cand, int C,
+                              int k, const int32_t* order, int32_t* out_idx, float* out_raw, float* out_dist, int sms,
                               cudaStream_t stream);
 cudaError_t launch_gather_pivots(const void* src, int64_t row_bytes, int64_t n, int64_t n_piv, void* dst, int sms,
                                  cudaStream_t stream);

@@ -60,8 +60,8 @@ __device__ __forceinline__ float key_raw(uint64_t key) { return from_orderable(u
 }  // namespace
 
 __global__ void __launch_bounds__(RW * 32)
-rerank_f32_kernel(const float* __restrict__ X, int ld, int d, int64_t n, const int32_t* __restrict__ cand, int C,
-                  int k, const int32_t* __restrict__ order, int32_t* __restrict__ out_idx, float* __restrict__ out_raw,
+rerank_f32_kernel(const float* __restrict__ X, int ld, int d, int64_t n, int64_t q_row0,
+                  const int32_t* __restrict__ cand, int C, int k, const int32_t* __restrict__ order, int32_t* __restrict__ out_idx, float* __restrict__ out_raw,
                   float* __restrict__ out_dist) {
   __shared__ uint64_t keys[RW][MAXC];
   __shared__ double d64[RW][32];
@@ -70,8 +70,9 @@ rerank_f32_kernel(const float* __restrict__ X, int ld, int d, int64_t n, const i
   int P = 1;
   while (P < C) P <<= 1;
   for (int64_t w = int64_t(blockIdx.x) * RW + warp; w < n; w += int64_t(gridDim.x) * RW) {
-    const int64_t q = order ? order[w] : w;
-    const float* xq = X + q * ld;
+    const int64_t q = order ? order[w] : w;  // output row
+    const int64_t qg = q_row0 + q;           // row of the data set
+    const float* xq = X + qg * ld;
     const int32_t* cq = cand + q * C;
     for (int j0 = 0; j0 < C; j0 += GROUP) {
       int32_t id[GROUP];
@@ -92,7 +93,7 @@ rerank_f32_kernel(const float* __restrict__ X, int ld, int d, int64_t n, const i
         const float dot = warp_sum(acc[u]);
         if (lane == u && j0 + u < C) {
           uint64_t key = kKeyInf;
-          if (id[u] >= 0) key = make_key(id[u] == q ? -1.0f : raw_cosine(dot), id[u]);
+          if (id[u] >= 0) key = make_key(id[u] == qg ? -1.0f : raw_cosine(dot), id[u]);
           kw[j0 + u] = key;
         }
       }
@@ -117,7 +118,7 @@ rerank_f32_kernel(const float* __restrict__ X, int ld, int d, int64_t n, const i
           acc = warp_sum_d(acc);
           // FP64 dissimilarity under the reference's rule: self -1, -dot, or the
           // MIN_POSITIVE sentinel for dots <= 0 (a true tie, broken by index).
-          if (lane == 0) d64[warp][j] = (c == q) ? -1.0 : (acc > 0.0 ? -acc : double(kMinPositive));
+          if (lane == 0) d64[warp][j] = (c == qg) ? -1.0 : (acc > 0.0 ? -acc : double(kMinPositive));
         }
         __syncwarp();
         if (lane == 0) {
@@ -151,14 +152,14 @@ rerank_f32_kernel(const float* __restrict__ X, int ld, int d, int64_t n, const i
   }
 }
 
-cudaError_t launch_rerank_f32(const float* X, int ld, int d, int64_t n, const int32_t* cand, int C, int k,
-                              const int32_t* order, int32_t* out_idx, float* out_raw, float* out_dist, int sms,
+cudaError_t launch_rerank_f32(const float* X, int ld, int d, int64_t n, int64_t q_row0, const int32_t* cand, int C,
+                              int k, const int32_t* order, int32_t* out_idx, float* out_raw, float* out_dist, int sms,
                               cudaStream_t stream) {
   if (C > MAXC || C < 1) return cudaErrorInvalidValue;
   int64_t blocks = (n + RW - 1) / RW;
   if (blocks > int64_t(sms) * 16) blocks = int64_t(sms) * 16;
-  rerank_f32_kernel<<<unsigned(blocks), RW * 32, 0, stream>>>(X, ld, d, n, cand, C, k, order, out_idx, out_raw,
-                                                               out_dist);
+  rerank_f32_kernel<<<unsigned(blocks), RW * 32, 0, stream>>>(X, ld, d, n, q_row0, cand, C, k, order, out_idx,
+                                                               out_raw, out_dist);
   return cudaGetLastError();
 }
 

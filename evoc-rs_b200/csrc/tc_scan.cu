@@ -45,7 +45,8 @@ constexpr size_t smem_bytes(int stages, int groups, int heap_stride) {
 }  // namespace
 
 struct ScanParams {
-  int64_t n_q, n_k;
+  int64_t n_q, n_k;  // query rows taken (starting at q_row0 of Q), key rows
+  int64_t q_row0;    // first query row; query i is row q_row0 + i of Q (and key q_row0 + i)
   int n_kchunks;     // 128-byte K chunks per row
   int keep;          // entries kept per query row (the heap size)
   int heap_stride;   // 8-byte words between rows' heaps (odd when heaps are in shared memory)
@@ -187,7 +188,7 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
             }
             uint8_t* a_dst = smem + s * STAGE_BYTES;
             mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
-            tma_load_2d(a_dst, &tmA, &full[s], kc * KC_ELEMS, int32_t(qb * BM));
+            tma_load_2d(a_dst, &tmA, &full[s], kc * KC_ELEMS, int32_t(p.q_row0 + qb * BM));
             tma_load_2d(a_dst + A_BYTES, &tmB, &full[s], kc * KC_ELEMS, int32_t(kt * BN));
             it++;
           }
@@ -254,11 +255,12 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     uint32_t tile = 0;
     bool ok = true;
     for (int64_t qb = blockIdx.x; ok && qb < n_qblocks; qb += gridDim.x) {
-      const int64_t q = qb * BM + row_local;
+      const int64_t q = qb * BM + row_local;  // output row
+      const int64_t qg = p.q_row0 + q;        // row of the data set
       const bool valid = q < p.n_q;
       KeyHeap heap;
       heap.init(hstore, p.keep);
-      if (valid && p.self_mode && group == 0) heap.offer(make_key(-1.0f, int32_t(q)));
+      if (valid && p.self_mode && group == 0) heap.offer(make_key(-1.0f, int32_t(qg)));
       uint32_t thr = pass_threshold(heap, kInt8);
       for (int64_t kt = 0; kt < n_ktiles; kt++, tile++) {
         const uint32_t a = tile & 1u, tph = (tile >> 1) & 1u;
@@ -280,11 +282,11 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
           tmem_ld_wait();
           tmem_ld_32x32b_x32(tbase + (c + 1) * 32, vb);
           uint32_t m = chunk_mask<kInt8>(va, thr);
-          if (valid && m) offer_chunk<kInt8>(va, m, k0 + c * 32, p.n_k, p.self_mode, q, heap, thr);
+          if (valid && m) offer_chunk<kInt8>(va, m, k0 + c * 32, p.n_k, p.self_mode, qg, heap, thr);
           tmem_ld_wait();
           if (c + 2 < NCH) tmem_ld_32x32b_x32(tbase + (c + 2) * 32, va);
           m = chunk_mask<kInt8>(vb, thr);
-          if (valid && m) offer_chunk<kInt8>(vb, m, k0 + (c + 1) * 32, p.n_k, p.self_mode, q, heap, thr);
+          if (valid && m) offer_chunk<kInt8>(vb, m, k0 + (c + 1) * 32, p.n_k, p.self_mode, qg, heap, thr);
         }
         tc_fence_before();
         mbar_arrive(&tempty[a]);
@@ -403,14 +405,15 @@ cudaError_t launch_dtype(const CUtensorMap& ma, const CUtensorMap& mb, ScanParam
 }
 }  // namespace
 
-cudaError_t launch_tc_scan(bool int8, const void* Q, int64_t q_rows, int64_t n_q, const void* K, int64_t k_rows,
-                           int64_t n_k, int64_t row_bytes, int keep, int /*cap*/, uint64_t* scratch, int grid,
+cudaError_t launch_tc_scan(bool int8, const void* Q, int64_t q_rows, int64_t q_row0, int64_t n_q, const void* K,
+                           int64_t k_rows, int64_t n_k, int64_t row_bytes, int keep, uint64_t* scratch, int grid,
                            int self_mode, int final_mode, int dtype, int32_t* out_idx, float* out_raw, float* out_dist,
                            int* status, uint64_t timeout_ns, cudaStream_t stream) {
   // q_rows / k_rows: rows present in memory (multiples of the box heights);
   // n_q / n_k: rows that take part.  Rows past n are zero and never offered.
   if (row_bytes % KCB != 0 || n_q <= 0 || n_k <= 0 || keep < 1) return cudaErrorInvalidValue;
-  if (q_rows < n_q || k_rows < n_k || q_rows % BM != 0 || k_rows % BN != 0) return cudaErrorInvalidValue;
+  if (q_row0 < 0 || q_rows < q_row0 + n_q || k_rows < n_k || q_rows % BN != 0 || k_rows % BN != 0)
+    return cudaErrorInvalidValue;
   if ((reinterpret_cast<uintptr_t>(Q) & 15) || (reinterpret_cast<uintptr_t>(K) & 15)) return cudaErrorInvalidValue;
   const int eb = int8 ? 1 : 2;
   alignas(64) CUtensorMap ma, mb;
@@ -419,6 +422,7 @@ cudaError_t launch_tc_scan(bool int8, const void* Q, int64_t q_rows, int64_t n_q
   ScanParams p;
   p.n_q = n_q;
   p.n_k = n_k;
+  p.q_row0 = q_row0;
   p.n_kchunks = int(row_bytes / KCB);
   p.keep = keep;
   p.scratch = scratch;

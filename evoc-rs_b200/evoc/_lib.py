@@ -42,7 +42,9 @@ class Opts(C.Structure):
         ("max_candidates", C.c_int32),
         ("delta", C.c_float),
         ("delta_improv", C.c_float),
-        ("reserved", C.c_int32 * 8),
+        ("row_begin", C.c_int64),
+        ("row_end", C.c_int64),
+        ("reserved", C.c_int32 * 4),
     ]
 
 
@@ -73,6 +75,12 @@ def lib():
             L.evoc_gpu_knn_graph.argtypes = [P, C.POINTER(Opts), i32, P, i64, i64, i32, P, P, P, C.POINTER(i32)]
             L.evoc_gpu_knn_graph_raw.argtypes = [P, C.POINTER(Opts), i32, P, i64, i64, i32, P, P, P, P,
                                                  C.POINTER(i32)]
+            L.evoc_gpu_ctx_stream.argtypes = [P]
+            L.evoc_gpu_ctx_stream.restype = P
+            L.evoc_gpu_profile_enable.argtypes = [P, C.c_int]
+            L.evoc_gpu_profile_count.argtypes = [P]
+            L.evoc_gpu_profile_stage.argtypes = [P, C.c_int, C.c_char_p, C.c_int, C.POINTER(C.c_float)]
+            L.evoc_gpu_last_launch_count.argtypes = [P]
             _bind_optional(L)
             _lib = L
     return _lib
@@ -116,6 +124,27 @@ class Context:
 
     def last_error(self) -> str:
         return lib().evoc_gpu_last_error(self.h).decode()
+
+    @property
+    def stream_ptr(self) -> int:
+        """The context's cudaStream_t (for torch.cuda.ExternalStream)."""
+        return int(lib().evoc_gpu_ctx_stream(self.h) or 0)
+
+    def profile(self, enable: bool = True) -> None:
+        lib().evoc_gpu_profile_enable(self.h, 1 if enable else 0)
+
+    def stages(self) -> list[tuple[str, float]]:
+        """(name, milliseconds) of each stage of the last call, device-timed."""
+        out = []
+        buf = C.create_string_buffer(64)
+        ms = C.c_float(0.0)
+        for i in range(lib().evoc_gpu_profile_count(self.h)):
+            if lib().evoc_gpu_profile_stage(self.h, i, buf, 64, C.byref(ms)) == EVOC_OK:
+                out.append((buf.value.decode(), float(ms.value)))
+        return out
+
+    def launches(self) -> int:
+        return int(lib().evoc_gpu_last_launch_count(self.h))
 
     def close(self) -> None:
         if self.h:

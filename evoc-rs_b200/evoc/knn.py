@@ -116,6 +116,8 @@ class KnnGraphOptions:
     form: str = "auto"          # auto | fp32 | bf16_rerank | exact_int | nndescent
     oversample: int = 2         # bf16_rerank: candidates per row = oversample * k
     device: int = 0
+    row_begin: int = 0          # exact forms: query rows [row_begin, row_end) only; 0,0 = all
+    row_end: int = 0
 
 
 def _n_trees(options: KnnGraphOptions) -> int:
@@ -135,6 +137,8 @@ def _to_opts(options: KnnGraphOptions, on_device: bool = False) -> _lib.Opts:
     o.max_candidates = int(options.max_candidates or 0)
     o.delta = float(options.delta)
     o.delta_improv = float(options.delta_improv)
+    o.row_begin = int(options.row_begin)
+    o.row_end = int(options.row_end)
     return o
 
 
@@ -159,8 +163,10 @@ def _raise_for(status: int, ctx: _lib.Context) -> None:
     raise BackendError(status, ctx.last_error())
 
 
-def knn_graph(data, options: KnnGraphOptions, rng=None, *, return_raw: bool = False):
-    """Build the kNN graph on the GPU.  Returns (indices int32 (n,k), distances f32 (n,k))."""
+def knn_graph(data, options: KnnGraphOptions, rng=None, *, return_raw: bool = False, out=None):
+    """Build the kNN graph on the GPU.  Returns (indices int32 (m,k), distances f32 (m,k)) where m
+    is n, or row_end - row_begin when a row slice is requested.  `out` may supply preallocated
+    (indices, distances) arrays (e.g. pinned host memory)."""
     data = EmbeddingData.wrap(data)
     if options.n_neighbors <= 0:
         raise InvalidNeighbors()
@@ -170,11 +176,17 @@ def knn_graph(data, options: KnnGraphOptions, rng=None, *, return_raw: bool = Fa
     arr = np.ascontiguousarray(data.array)
     n, dim = arr.shape
     k = max(1, min(options.n_neighbors, n - 1))
+    m = (options.row_end - options.row_begin) if (options.row_begin or options.row_end) else n
     ctx = _lib.context(options.device)
     o = _to_opts(options)
-    ind = np.empty((n, k), np.int32)
-    dst = np.empty((n, k), np.float32)
-    raw = np.empty((n, k), np.float32) if return_raw else None
+    if out is not None:
+        ind, dst = out
+        assert ind.shape == (m, k) and ind.dtype == np.int32 and ind.flags.c_contiguous
+        assert dst.shape == (m, k) and dst.dtype == np.float32 and dst.flags.c_contiguous
+    else:
+        ind = np.empty((m, k), np.int32)
+        dst = np.empty((m, k), np.float32)
+    raw = np.empty((m, k), np.float32) if return_raw else None
     kout = C.c_int32(0)
     P = C.c_void_p
     if return_raw:

@@ -68,7 +68,10 @@ typedef struct {
   int32_t max_candidates;    /* NN-descent; <= 0 -> min(60, floor(1.5 k))      */
   float delta;               /* NN-descent; KnnGraphOptions.delta (0.001)      */
   float delta_improv;        /* NN-descent; KnnGraphOptions.delta_improv       */
-  int32_t reserved[8];
+  int64_t row_begin;         /* exact forms: compute query rows [row_begin,     */
+  int64_t row_end;           /* row_end) against all n rows; 0,0 = all rows.    */
+                             /* Outputs then hold (row_end-row_begin) rows.     */
+  int32_t reserved[4];
 } evoc_gpu_opts;
 
 typedef struct evoc_gpu_ctx evoc_gpu_ctx;
@@ -109,6 +112,21 @@ int evoc_gpu_knn_graph(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts, int32_t dty
 int evoc_gpu_knn_graph_raw(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts, int32_t dtype, const void* data,
                            int64_t n, int64_t dim, int32_t k, const int64_t* rng_state, int32_t* out_idx,
                            float* out_dist, float* out_raw, int32_t* out_k);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that record their
+ * own CUDA events around calls.  No counterpart in evoc-rs. */
+void* evoc_gpu_ctx_stream(const evoc_gpu_ctx* ctx);
+
+/* Device timing of the stages of the last call.  When enabled, every call
+ * records CUDA events on the context's stream around each kernel stage.
+ * No counterpart in evoc-rs (its bins time stages with Instant,
+ * src/bin/bench_huge.rs:71-82). */
+int evoc_gpu_profile_enable(evoc_gpu_ctx* ctx, int enable);
+int evoc_gpu_profile_count(const evoc_gpu_ctx* ctx);
+int evoc_gpu_profile_stage(const evoc_gpu_ctx* ctx, int i, char* name, int name_len, float* ms);
+
+/* Number of kernels the last call launched. */
+int evoc_gpu_last_launch_count(const evoc_gpu_ctx* ctx);
 
 #ifdef __cplusplus
 }
