@@ -362,7 +362,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--fp32-rows", type=int, default=75_776)  # 2 full waves of 296 CTAs x 128 rows
     ap.add_argument("--recall-rows", type=int, default=10_000)
-    ap.add_argument("--cpu-rows", type=int, default=6_000)
+    ap.add_argument("--cpu-rows", type=int, default=150_000)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world, rank, local = dist_env()
