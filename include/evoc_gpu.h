@@ -128,6 +128,31 @@ int evoc_gpu_profile_stage(const evoc_gpu_ctx* ctx, int i, char* name, int name_
 /* Number of kernels the last call launched. */
 int evoc_gpu_last_launch_count(const evoc_gpu_ctx* ctx);
 
+/*
+ * Exact FP32 kNN that allocates no device memory.  It has no counterpart in
+ * evoc-rs.  It is for callers that may not let a library call cudaMalloc:
+ * processes that reserve the GPU's memory for their own pool up front, or
+ * latency-critical loops that cannot take cudaMalloc's implicit device-wide
+ * synchronisation.  All pointers are device pointers; the work is enqueued on
+ * `stream` (a cudaStream_t, 0 for the default stream) and the call returns
+ * without waiting for it.
+ *   rows       n rows of `ld` floats, 16-byte aligned, ld a multiple of 16,
+ *              columns past the data zero, each row already L2-normalised
+ *              (this entry point has no working copy to renormalise into)
+ *   k          clamped to max(1, min(k, n-1)); at most 64 after the clamp,
+ *              larger values return EVOC_ERR_UNSUPPORTED
+ *   out_idx / out_dist   n x k_eff, as evoc_gpu_knn_graph with EVOC_FORM_FP32
+ *   errbuf     receives a message on failure (may be NULL)
+ * The search's scratch is one fixed 16 MiB array per GPU, held from the
+ * library's load until the process exits.  The first call on a device looks
+ * up that array's device address (cudaGetSymbolAddress), so make that first
+ * call before any stream capture.  All calls on a device share the array:
+ * calls whose kernels overlap on the GPU (different streams with no ordering)
+ * race and corrupt each other's results.
+ */
+int evoc_gpu_knn_f32_noalloc(const float* rows, int64_t n, int64_t ld, int32_t k, int32_t* out_idx, float* out_dist,
+                             void* stream, int32_t* out_k, char* errbuf, int32_t errlen);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,88 @@
+"""The entry point that allocates no device memory.
+
+evoc_gpu_knn_f32_noalloc exists for callers that may not let a library call
+cudaMalloc (a process whose memory pool owns the whole GPU, a latency-bound
+loop that cannot take cudaMalloc's implicit synchronisation).  Its scratch is
+a fixed array inside the library, shared by every call on the device, so this
+test calls it twice in a row and checks both results against the regular
+entry point (evoc_gpu_knn_graph, FP32 form) with the FP32 tolerance used by
+the other tests.  This file is named to be collected last.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import evoc
+from evoc import _lib
+
+pytestmark = pytest.mark.gpu
+
+
+def _noalloc():
+    L = _lib.lib()
+    f = L.evoc_gpu_knn_f32_noalloc
+    f.argtypes = [C.c_void_p, C.c_int64, C.c_int64, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                  C.POINTER(C.c_int32), C.c_char_p, C.c_int32]
+    f.restype = C.c_int
+    return f
+
+
+def _rows(n, d, seed):
+    rng = np.random.default_rng(seed)
+    c = rng.standard_normal((7, d))
+    x = (c[rng.integers(0, 7, n)] + 0.3 * rng.standard_normal((n, d))).astype(np.float32)
+    x /= np.linalg.norm(x, axis=1, keepdims=True)
+    return x
+
+
+def _run(f, xt, n, d, k, stream):
+    import torch
+
+    kk = max(1, min(k, n - 1))
+    oi = torch.full((n, kk), -7, dtype=torch.int32, device="cuda")
+    od = torch.full((n, kk), -7.0, dtype=torch.float32, device="cuda")
+    kout = C.c_int32(0)
+    err = C.create_string_buffer(256)
+    rc = f(xt.data_ptr(), n, d, k, oi.data_ptr(), od.data_ptr(), stream, C.byref(kout), err, 256)
+    assert rc == 0, err.value
+    assert kout.value == kk
+    return oi, od
+
+
+def test_noalloc_matches_regular_entry_point_on_two_calls():
+    import torch
+
+    f = _noalloc()
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    cases = [(3000, 64, 15, 1), (1500, 128, 40, 2)]
+    outs = []
+    data = []
+    for n, d, k, seed in cases:  # two calls in a row, nothing in between
+        x = _rows(n, d, seed)
+        xt = torch.from_numpy(x).cuda()
+        data.append(x)
+        outs.append(_run(f, xt, n, d, k, stream))
+    torch.cuda.synchronize()
+    for (n, d, k, seed), x, (oi, od) in zip(cases, data, outs):
+        ri, rd = evoc.knn_graph(x, evoc.KnnGraphOptions(n_neighbors=k, form="fp32"))
+        gi, gd = oi.cpu().numpy(), od.cpu().numpy()
+        assert np.all(np.abs(gd - rd) <= 1e-6)
+        diff = gi != ri
+        assert np.all(np.abs(gd[diff] - rd[diff]) <= 1e-6)  # only tie swaps
+        assert np.all(gi[:, 0] == np.arange(n))
+
+
+def test_noalloc_rejects_sizes_beyond_its_scratch():
+    import torch
+
+    f = _noalloc()
+    xt = torch.from_numpy(_rows(200, 32, 3)).cuda()
+    oi = torch.empty((200, 100), dtype=torch.int32, device="cuda")
+    od = torch.empty((200, 100), dtype=torch.float32, device="cuda")
+    err = C.create_string_buffer(256)
+    rc = f(xt.data_ptr(), 200, 32, 100, oi.data_ptr(), od.data_ptr(), None, None, err, 256)
+    assert rc == _lib.EVOC_ERR_UNSUPPORTED
+    assert b"at most 64" in err.value
+    rc = f(xt.data_ptr(), 200, 20, 10, oi.data_ptr(), od.data_ptr(), None, None, err, 256)
+    assert rc == _lib.EVOC_ERR_ARG
