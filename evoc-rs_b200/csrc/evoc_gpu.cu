@@ -59,7 +59,7 @@ struct evoc_gpu_ctx {
   std::mutex mu;
   std::string err;
   DevBuf x, scratch, norms, flag, out_idx, out_raw, out_dist;
-  DevBuf xb, cand, labels, order, hist, cursor, pivots;
+  DevBuf xb, cand, labels, order, hist, cursor, pivots, popc;
   uint64_t timeout_ns = 4000000000ull;  // longest a pipeline wait inside a kernel may take
   bool profiling = false;
   std::vector<StageRec> stages;  // event pool; the first n_stages belong to the last call
@@ -240,6 +240,19 @@ int run_int8(evoc_gpu_ctx* ctx, const Job& j, int64_t ldb) {
   return EVOC_OK;
 }
 
+int run_jaccard(evoc_gpu_ctx* ctx, const Job& j, int64_t ldb) {
+  Stage st(ctx, "jaccard_scan");
+  if (evoc::knn_jaccard_smem(j.keff) > 232448) return fail(ctx, EVOC_ERR_UNSUPPORTED, "k too large for this form");
+  const int64_t qblocks = (j.nq + 127) / 128;
+  const int grid = int(qblocks < ctx->sms ? qblocks : ctx->sms);
+  EVOC_TRY(ctx->popc.ensure(size_t(j.n) * 4), "alloc popcounts");
+  EVOC_TRY(evoc::launch_knn_jaccard(ctx->x.p, j.n, int(ldb / 4), j.keff, ctx->popc.as<int32_t>(), grid, j.idx, j.raw,
+                                    j.dist, j.r0, j.r0 + j.nq, ctx->sms, ctx->stream),
+           "jaccard scan");
+  ctx->launches += 2;
+  return EVOC_OK;
+}
+
 int knn_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtype, const void* data, int64_t n,
              int64_t dim, int32_t k, const int64_t* rng_state, int32_t* out_idx, float* out_dist, float* out_raw,
              int32_t* out_k) {
@@ -320,7 +333,11 @@ int knn_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtype, con
     if (rc) return rc;
     rc = run_int8(ctx, job, ldb);
   } else {
-    return fail(ctx, EVOC_ERR_UNSUPPORTED, "dtype form not built in this library");
+    if (form != EVOC_FORM_EXACT_INT) return fail(ctx, EVOC_ERR_UNSUPPORTED, "form not built for u8 in this library");
+    const int64_t ldb = round_up(dim, 64);
+    rc = stage_rows(ctx, data, n, dim, ldb, on_dev);
+    if (rc) return rc;
+    rc = run_jaccard(ctx, job, ldb);
   }
   if (rc) return rc;
   int flags[2] = {0, 0};
@@ -384,7 +401,7 @@ void evoc_gpu_ctx_destroy(evoc_gpu_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   DevBuf* bufs[] = {&ctx->x,        &ctx->scratch, &ctx->norms, &ctx->flag,   &ctx->out_idx,
                     &ctx->out_raw,  &ctx->out_dist, &ctx->xb,   &ctx->cand,   &ctx->labels,
-                    &ctx->order,    &ctx->hist,    &ctx->cursor, &ctx->pivots};
+                    &ctx->order,    &ctx->hist,    &ctx->cursor, &ctx->pivots, &ctx->popc};
   for (DevBuf* b : bufs) b->release();
   for (auto& r : ctx->stages) {
     if (r.a) cudaEventDestroy(r.a);

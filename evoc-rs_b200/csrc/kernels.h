@@ -55,3 +55,12 @@ cudaError_t launch_order_by_label(const int32_t* label, int64_t n, int nb, int32
                                   int32_t* order, int sms, cudaStream_t stream);
 
 }  // namespace evoc
+
+namespace evoc {
+// jaccard.cu: exact popcount Jaccard over packed bits with fused top-k.
+//   X: rows of ldw 32-bit words (ldw a multiple of 16), pc: n int32 row popcounts (written here).
+size_t knn_jaccard_smem(int k);
+cudaError_t launch_knn_jaccard(const void* X, int64_t n, int ldw, int k, int32_t* pc, int grid, int32_t* out_idx,
+                               float* out_raw, float* out_dist, int64_t q_begin, int64_t q_end, int sms,
+                               cudaStream_t stream);
+}  // namespace evoc
