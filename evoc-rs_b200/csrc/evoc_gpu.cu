@@ -60,6 +60,7 @@ struct evoc_gpu_ctx {
   std::string err;
   DevBuf x, scratch, norms, flag, out_idx, out_raw, out_dist;
   DevBuf xb, cand, labels, order, hist, cursor, pivots, popc;
+  DevBuf g_idx, g_dist, g_sigma, g_rho, g_indptr, g_indices, g_data, g_work;
   uint64_t timeout_ns = 4000000000ull;  // longest a pipeline wait inside a kernel may take
   bool profiling = false;
   std::vector<StageRec> stages;  // event pool; the first n_stages belong to the last call
@@ -253,6 +254,137 @@ int run_jaccard(evoc_gpu_ctx* ctx, const Job& j, int64_t ldb) {
   return EVOC_OK;
 }
 
+// Carves the fuzzy-graph work buffers out of one allocation.
+int fuzzy_work(evoc_gpu_ctx* ctx, int64_t n, int k, evoc::FuzzyWork* w) {
+  const size_t nk = size_t(n) * size_t(k);
+  const size_t sizes[] = {64, 64, nk * 4, nk * 4, size_t(n) * 4, size_t(n) * 4, size_t(n + 1) * 8, size_t(n) * 4,
+                          nk * 4, nk * 4, size_t(n) * 4};
+  size_t total = 0;
+  for (size_t s : sizes) total += (s + 255) / 256 * 256;
+  EVOC_TRY(ctx->g_work.ensure(total), "alloc graph work");
+  uint8_t* p = ctx->g_work.as<uint8_t>();
+  void* ptrs[11];
+  for (int i = 0; i < 11; i++) {
+    ptrs[i] = p;
+    p += (sizes[i] + 255) / 256 * 256;
+  }
+  w->flags = static_cast<int*>(ptrs[0]);
+  w->mean = static_cast<float*>(ptrs[1]);
+  w->a_cols = static_cast<int32_t*>(ptrs[2]);
+  w->a_vals = static_cast<float*>(ptrs[3]);
+  w->a_cnt = static_cast<int32_t*>(ptrs[4]);
+  w->indeg = static_cast<int32_t*>(ptrs[5]);
+  w->colptr = static_cast<int64_t*>(ptrs[6]);
+  w->fill = static_cast<int32_t*>(ptrs[7]);
+  w->at_rows = static_cast<int32_t*>(ptrs[8]);
+  w->at_vals = static_cast<float*>(ptrs[9]);
+  w->row_cnt = static_cast<int32_t*>(ptrs[10]);
+  return EVOC_OK;
+}
+
+int fuzzy_impl(evoc_gpu_ctx* ctx, const int32_t* idx, const float* dist, int64_t n, int32_t k, float n_neighbors,
+               int32_t symmetrize, int32_t on_dev, float* sigma, float* rho, bool graph, int64_t* indptr,
+               int32_t* indices, float* data, int64_t cap, int64_t* nnz) {
+  if (!ctx) return EVOC_ERR_ARG;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  ctx->err.clear();
+  ctx->n_stages = 0;
+  ctx->launches = 0;
+  if (n <= 0) return fail(ctx, EVOC_ERR_EMPTY, "empty kNN graph");
+  if (k <= 0 || k > 64) return fail(ctx, EVOC_ERR_ARG, "k must be in 1..64");
+  if (!dist || (graph && (!idx || !indptr))) return fail(ctx, EVOC_ERR_ARG, "null input or output");
+  EVOC_TRY(cudaSetDevice(ctx->device), "cudaSetDevice");
+  Stage total(ctx, "total");
+  const size_t nk = size_t(n) * size_t(k);
+  const int32_t* d_idx = idx;
+  const float* d_dist = dist;
+  if (!on_dev) {
+    Stage st(ctx, "h2d_knn");
+    EVOC_TRY(ctx->g_dist.ensure(nk * 4), "alloc dist");
+    EVOC_TRY(cudaMemcpyAsync(ctx->g_dist.p, dist, nk * 4, cudaMemcpyHostToDevice, ctx->stream), "upload dist");
+    d_dist = ctx->g_dist.as<float>();
+    if (idx) {
+      EVOC_TRY(ctx->g_idx.ensure(nk * 4), "alloc idx");
+      EVOC_TRY(cudaMemcpyAsync(ctx->g_idx.p, idx, nk * 4, cudaMemcpyHostToDevice, ctx->stream), "upload idx");
+      d_idx = ctx->g_idx.as<int32_t>();
+    }
+  }
+  evoc::FuzzyWork w;
+  int rc = fuzzy_work(ctx, n, k, &w);
+  if (rc) return rc;
+  float* d_sigma = (on_dev && sigma) ? sigma : nullptr;
+  float* d_rho = (on_dev && rho) ? rho : nullptr;
+  if (!d_sigma) {
+    EVOC_TRY(ctx->g_sigma.ensure(size_t(n) * 4), "alloc sigma");
+    d_sigma = ctx->g_sigma.as<float>();
+  }
+  if (!d_rho) {
+    EVOC_TRY(ctx->g_rho.ensure(size_t(n) * 4), "alloc rho");
+    d_rho = ctx->g_rho.as<float>();
+  }
+  // Without indices there is no graph: membership rows are still built from a
+  // dummy index array so sigma/rho come from the same kernel.
+  if (!d_idx) {
+    EVOC_TRY(ctx->g_idx.ensure(nk * 4), "alloc idx");
+    EVOC_TRY(cudaMemsetAsync(ctx->g_idx.p, 0xff, nk * 4, ctx->stream), "fill idx");
+    d_idx = ctx->g_idx.as<int32_t>();
+  }
+  {
+    Stage st(ctx, "smooth_knn_dist");
+    EVOC_TRY(evoc::launch_smooth_and_membership(d_idx, d_dist, n, k, n_neighbors, w, d_sigma, d_rho, ctx->sms,
+                                                ctx->stream),
+             "smooth_knn_dist");
+    ctx->launches += 3;
+  }
+  int64_t total_nnz = 0;
+  if (graph) {
+    int64_t* d_indptr = on_dev ? indptr : nullptr;
+    if (!d_indptr) {
+      EVOC_TRY(ctx->g_indptr.ensure(size_t(n + 1) * 8), "alloc indptr");
+      d_indptr = ctx->g_indptr.as<int64_t>();
+    }
+    {
+      Stage st(ctx, "union_count");
+      EVOC_TRY(evoc::launch_fuzzy_union_count(n, k, symmetrize, w, d_indptr, ctx->sms, ctx->stream), "union count");
+      ctx->launches += symmetrize ? 5 : 2;
+    }
+    EVOC_TRY(cudaMemcpyAsync(&total_nnz, d_indptr + n, 8, cudaMemcpyDeviceToHost, ctx->stream), "read nnz");
+    EVOC_TRY(cudaStreamSynchronize(ctx->stream), "union count");
+    if (nnz) *nnz = total_nnz;
+    if (total_nnz > cap) return fail(ctx, EVOC_ERR_ARG, "cap too small for the graph; *nnz holds the size needed");
+    int32_t* d_indices = on_dev ? indices : nullptr;
+    float* d_data = on_dev ? data : nullptr;
+    if (!on_dev) {
+      EVOC_TRY(ctx->g_indices.ensure(size_t(total_nnz > 0 ? total_nnz : 1) * 4), "alloc indices");
+      EVOC_TRY(ctx->g_data.ensure(size_t(total_nnz > 0 ? total_nnz : 1) * 4), "alloc data");
+      d_indices = ctx->g_indices.as<int32_t>();
+      d_data = ctx->g_data.as<float>();
+    }
+    {
+      Stage st(ctx, "union_write");
+      EVOC_TRY(evoc::launch_fuzzy_union_write(n, k, symmetrize, w, d_indptr, d_indices, d_data, ctx->sms,
+                                              ctx->stream),
+               "union write");
+      ctx->launches += 1;
+    }
+    if (!on_dev) {
+      EVOC_TRY(cudaMemcpyAsync(indptr, d_indptr, size_t(n + 1) * 8, cudaMemcpyDeviceToHost, ctx->stream), "indptr");
+      if (total_nnz > 0) {
+        EVOC_TRY(cudaMemcpyAsync(indices, d_indices, size_t(total_nnz) * 4, cudaMemcpyDeviceToHost, ctx->stream),
+                 "indices");
+        EVOC_TRY(cudaMemcpyAsync(data, d_data, size_t(total_nnz) * 4, cudaMemcpyDeviceToHost, ctx->stream), "data");
+      }
+    }
+  }
+  if (!on_dev) {
+    if (sigma) EVOC_TRY(cudaMemcpyAsync(sigma, d_sigma, size_t(n) * 4, cudaMemcpyDeviceToHost, ctx->stream), "sigma");
+    if (rho) EVOC_TRY(cudaMemcpyAsync(rho, d_rho, size_t(n) * 4, cudaMemcpyDeviceToHost, ctx->stream), "rho");
+  }
+  total.end();
+  EVOC_TRY(cudaStreamSynchronize(ctx->stream), "fuzzy graph");
+  return EVOC_OK;
+}
+
 int knn_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtype, const void* data, int64_t n,
              int64_t dim, int32_t k, const int64_t* rng_state, int32_t* out_idx, float* out_dist, float* out_raw,
              int32_t* out_k) {
@@ -401,7 +533,9 @@ void evoc_gpu_ctx_destroy(evoc_gpu_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   DevBuf* bufs[] = {&ctx->x,        &ctx->scratch, &ctx->norms, &ctx->flag,   &ctx->out_idx,
                     &ctx->out_raw,  &ctx->out_dist, &ctx->xb,   &ctx->cand,   &ctx->labels,
-                    &ctx->order,    &ctx->hist,    &ctx->cursor, &ctx->pivots, &ctx->popc};
+                    &ctx->order,    &ctx->hist,    &ctx->cursor, &ctx->pivots, &ctx->popc,
+                    &ctx->g_idx,    &ctx->g_dist,  &ctx->g_sigma, &ctx->g_rho, &ctx->g_indptr,
+                    &ctx->g_indices, &ctx->g_data, &ctx->g_work};
   for (DevBuf* b : bufs) b->release();
   for (auto& r : ctx->stages) {
     if (r.a) cudaEventDestroy(r.a);
@@ -439,6 +573,19 @@ int evoc_gpu_profile_stage(const evoc_gpu_ctx* ctx, int i, char* name, int name_
 }
 
 int evoc_gpu_last_launch_count(const evoc_gpu_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int evoc_gpu_smooth_knn_dist(evoc_gpu_ctx* ctx, const float* dist, int64_t n, int32_t k, float n_neighbors,
+                             int32_t buffers_on_device, float* sigma, float* rho) {
+  return fuzzy_impl(ctx, nullptr, dist, n, k, n_neighbors, 0, buffers_on_device, sigma, rho, false, nullptr, nullptr,
+                    nullptr, 0, nullptr);
+}
+
+int evoc_gpu_fuzzy_graph(evoc_gpu_ctx* ctx, const int32_t* idx, const float* dist, int64_t n, int32_t k,
+                         float n_neighbors, int32_t symmetrize, int32_t buffers_on_device, float* sigma, float* rho,
+                         int64_t* indptr, int32_t* indices, float* data, int64_t cap, int64_t* nnz) {
+  return fuzzy_impl(ctx, idx, dist, n, k, n_neighbors, symmetrize, buffers_on_device, sigma, rho, true, indptr,
+                    indices, data, cap, nnz);
+}
 
 int evoc_gpu_knn_graph(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts, int32_t dtype, const void* data, int64_t n,
                        int64_t dim, int32_t k, const int64_t* rng_state, int32_t* out_idx, float* out_dist,

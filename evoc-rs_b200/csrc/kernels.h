@@ -64,3 +64,26 @@ cudaError_t launch_knn_jaccard(const void* X, int64_t n, int ldw, int k, int32_t
                                float* out_raw, float* out_dist, int64_t q_begin, int64_t q_end, int sms,
                                cudaStream_t stream);
 }  // namespace evoc
+
+namespace evoc {
+// graph.cu: smooth_knn_dist, membership strengths and the fuzzy union on the device.
+struct FuzzyWork {
+  int* flags;         // [0]: some row has rho == 0 (its sigma floor needs the global mean)
+  float* mean;        // mean of all distances, in ndarray's f32 order (only when flags[0])
+  int32_t* a_cols;    // n x k: row i's nonzero memberships, sorted by column
+  float* a_vals;
+  int32_t* a_cnt;     // n
+  int32_t* indeg;     // n: entries per column of A
+  int64_t* colptr;    // n + 1: CSR pointer of A^T
+  int32_t* fill;      // n
+  int32_t* at_rows;   // n x k capacity: A^T row indices per column bucket
+  float* at_vals;
+  int32_t* row_cnt;   // n: entries per row of the result
+};
+cudaError_t launch_smooth_and_membership(const int32_t* idx, const float* dist, int64_t n, int k, float n_neighbors,
+                                         const FuzzyWork& w, float* sigma, float* rho, int sms, cudaStream_t stream);
+cudaError_t launch_fuzzy_union_count(int64_t n, int k, int symmetrize, const FuzzyWork& w, int64_t* indptr, int sms,
+                                     cudaStream_t stream);
+cudaError_t launch_fuzzy_union_write(int64_t n, int k, int symmetrize, const FuzzyWork& w, const int64_t* indptr,
+                                     int32_t* indices, float* data, int sms, cudaStream_t stream);
+}  // namespace evoc

@@ -113,6 +113,31 @@ int evoc_gpu_knn_graph_raw(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts, int32_t
                            int64_t n, int64_t dim, int32_t k, const int64_t* rng_state, int32_t* out_idx,
                            float* out_dist, float* out_raw, int32_t* out_k);
 
+/*
+ * sigma and rho of every row.  Replaces smooth_knn_dist
+ * (src/graph_construction.rs:16-80): rho = first positive distance; sigma by
+ * f64 bisection (64 steps, tolerance 1e-5) on log2(n_neighbors), floored at
+ * 1e-3 x the row mean (rho > 0) or 1e-3 x the mean of all distances.
+ *   dist   n x k transformed distances, rows sorted ascending (k <= 64)
+ */
+int evoc_gpu_smooth_knn_dist(evoc_gpu_ctx* ctx, const float* dist, int64_t n, int32_t k, float n_neighbors,
+                             int32_t buffers_on_device, float* sigma, float* rho);
+
+/*
+ * Fuzzy simplicial set as canonical CSR.  Replaces neighbor_graph_matrix /
+ * neighbor_graph_matrix_with_coo (src/graph_construction.rs:176-235) with
+ * compute_membership_strengths (82-115) and the SciPy-order union
+ * A + A^T - A o A^T (src/csr_matmul.rs:62-150); symmetrize = 0 gives A.
+ *   idx, dist   n x k output of evoc_gpu_knn_graph (-1 entries skipped)
+ *   sigma, rho  n each (may be NULL)
+ *   indptr      n + 1 int64; indices int32 / data f32 with room for `cap`
+ *               entries (at most 2 n k).  When cap is too small the call
+ *               returns EVOC_ERR_ARG and *nnz holds the size needed.
+ */
+int evoc_gpu_fuzzy_graph(evoc_gpu_ctx* ctx, const int32_t* idx, const float* dist, int64_t n, int32_t k,
+                         float n_neighbors, int32_t symmetrize, int32_t buffers_on_device, float* sigma, float* rho,
+                         int64_t* indptr, int32_t* indices, float* data, int64_t cap, int64_t* nnz);
+
 /* The context's CUDA stream (a cudaStream_t), for callers that record their
  * own CUDA events around calls.  No counterpart in evoc-rs. */
 void* evoc_gpu_ctx_stream(const evoc_gpu_ctx* ctx);
