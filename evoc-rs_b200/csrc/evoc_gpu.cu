@@ -5,6 +5,8 @@
 // order (k == 0 before n == 0), the k clamp max(1, min(k, n-1)), f32
 // renormalisation (prepare_float), then the search and the per-dtype distance
 // transform (fused into the kernels' epilogues).
+#include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -61,11 +63,13 @@ struct evoc_gpu_ctx {
   DevBuf x, scratch, norms, flag, out_idx, out_raw, out_dist;
   DevBuf xb, cand, labels, order, hist, cursor, pivots, popc;
   DevBuf g_idx, g_dist, g_sigma, g_rho, g_indptr, g_indices, g_data, g_work;
+  DevBuf nnd_work;
   uint64_t timeout_ns = 4000000000ull;  // longest a pipeline wait inside a kernel may take
   bool profiling = false;
   std::vector<StageRec> stages;  // event pool; the first n_stages belong to the last call
   int n_stages = 0;
   int launches = 0;
+  int nnd_iterations = 0;
 };
 
 namespace {
@@ -184,7 +188,7 @@ int locality_order(evoc_gpu_ctx* ctx, const Job& j, const void* rows, int64_t ro
   EVOC_TRY(evoc::launch_order_by_label(ctx->labels.as<int32_t>(), j.nq, int(n_piv), ctx->hist.as<int32_t>(),
                                        ctx->cursor.as<int32_t>(), ctx->order.as<int32_t>(), ctx->sms, ctx->stream),
            "order by pivot");
-  ctx->launches += 5;
+  ctx->launches += 6;
   return EVOC_OK;
 }
 
@@ -385,6 +389,104 @@ int fuzzy_impl(evoc_gpu_ctx* ctx, const int32_t* idx, const float* dist, int64_t
   return EVOC_OK;
 }
 
+// GPU NN-descent over the staged rows (see nndescent.cu).  Row slices are not
+// supported: the graph is built for every row.
+// `piv_rows` / `piv_row_bytes`: the rows the pivot scan runs on (BF16 for f32
+// data, the int8 rows themselves for i8); unused for binary rows.
+int run_nndescent(evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, const Job& j, int32_t dtype, int64_t row_bytes,
+                  const void* rows, int ld_f32, int d, const int64_t* rng_state, const void* piv_rows,
+                  int64_t piv_row_bytes) {
+  if (j.r0 != 0 || j.nq != j.n) return fail(ctx, EVOC_ERR_UNSUPPORTED, "the NN-descent form builds whole graphs only");
+  if (j.keff > 32) return fail(ctx, EVOC_ERR_UNSUPPORTED, "the NN-descent form supports k <= 32");
+  const int64_t n = j.n;
+  const int k = j.keff;
+  const int rcap = k;
+  evoc::NndArgs a{};
+  a.X = static_cast<const uint8_t*>(rows);
+  a.row_bytes = row_bytes;
+  a.n = n;
+  a.k = k;
+  a.dtype = dtype;
+  a.sms = ctx->sms;
+  a.rcap = rcap;
+  uint64_t seed = 0x5eed5eedull;
+  if (rng_state)
+    seed = (uint64_t(rng_state[0]) * 0x9e3779b97f4a7c15ull) ^ (uint64_t(rng_state[1]) << 21) ^ uint64_t(rng_state[2]);
+  a.seed = seed;
+  if (dtype == EVOC_DTYPE_U8) {
+    EVOC_TRY(ctx->popc.ensure(size_t(n) * 4), "alloc popcounts");
+    EVOC_TRY(evoc::launch_popcount_rows(rows, n, int(row_bytes / 4), ctx->popc.as<int32_t>(), ctx->sms, ctx->stream),
+             "popcounts");
+    a.pc = ctx->popc.as<int32_t>();
+    ctx->launches += 1;
+  } else {
+    // Pivot cells seed the graph and fix the visiting order.
+    int rc = locality_order(ctx, j, piv_rows, piv_row_bytes, dtype == EVOC_DTYPE_I8);
+    if (rc) return rc;
+    a.order = ctx->order.as<int32_t>();
+    a.label = ctx->labels.as<int32_t>();
+    a.cell_end = ctx->cursor.as<int32_t>();
+    a.cell_cnt = ctx->hist.as<int32_t>();
+  }
+  const size_t nk = size_t(n) * size_t(k);
+  const size_t sizes[] = {nk * 8, nk * 8, nk, nk, size_t(n) * 4, size_t(n + 1) * 8, size_t(n) * 4, nk * 4,
+                          size_t(n) * size_t(rcap) * 4, size_t(n) * 4, 64};
+  size_t total = 0;
+  for (size_t s : sizes) total += (s + 255) / 256 * 256;
+  EVOC_TRY(ctx->nnd_work.ensure(total), "alloc NN-descent work");
+  uint8_t* p = ctx->nnd_work.as<uint8_t>();
+  void* ptrs[11];
+  for (int i = 0; i < 11; i++) {
+    ptrs[i] = p;
+    p += (sizes[i] + 255) / 256 * 256;
+  }
+  a.keys[0] = static_cast<uint64_t*>(ptrs[0]);
+  a.keys[1] = static_cast<uint64_t*>(ptrs[1]);
+  a.isnew[0] = static_cast<uint8_t*>(ptrs[2]);
+  a.isnew[1] = static_cast<uint8_t*>(ptrs[3]);
+  a.rcnt = static_cast<int32_t*>(ptrs[4]);
+  a.rptr = static_cast<int64_t*>(ptrs[5]);
+  a.rfill = static_cast<int32_t*>(ptrs[6]);
+  a.rrows = static_cast<int32_t*>(ptrs[7]);
+  a.rsel = static_cast<int32_t*>(ptrs[8]);
+  a.rn = static_cast<int32_t*>(ptrs[9]);
+  a.changes = static_cast<unsigned long long*>(ptrs[10]);
+  {
+    Stage st(ctx, "nnd_init");
+    EVOC_TRY(evoc::launch_nnd_init(a, ctx->stream), "NN-descent init");
+    ctx->launches += 1;
+  }
+  int n_iters = opts.n_iters > 0 ? opts.n_iters : int(std::max(5.0, std::round(std::log2(double(n)))));
+  const float delta = opts.delta;
+  const double limit = double(float(delta * float(k)) * float(n));
+  int cur = 0;
+  for (int it = 0; it < n_iters; it++) {
+    Stage st(ctx, "nnd_iteration");
+    EVOC_TRY(cudaMemsetAsync(a.changes, 0, 8, ctx->stream), "clear changes");
+    EVOC_TRY(evoc::launch_nnd_iteration(a, cur, it, ctx->stream), "NN-descent iteration");
+    ctx->launches += 5;
+    cur ^= 1;
+    unsigned long long ch = 0;
+    EVOC_TRY(cudaMemcpyAsync(&ch, a.changes, 8, cudaMemcpyDeviceToHost, ctx->stream), "read changes");
+    EVOC_TRY(cudaStreamSynchronize(ctx->stream), "NN-descent iteration");
+    ctx->nnd_iterations = it + 1;
+    if (double(ch) <= limit) break;
+  }
+  Stage st(ctx, "nnd_finish");
+  if (dtype == EVOC_DTYPE_F32) {
+    EVOC_TRY(ctx->cand.ensure(nk * 4), "alloc candidates");
+    EVOC_TRY(evoc::launch_nnd_emit(a, cur, ctx->cand.as<int32_t>(), nullptr, nullptr, ctx->stream), "emit");
+    EVOC_TRY(evoc::launch_rerank_f32(ctx->x.as<float>(), ld_f32, d, n, 0, ctx->cand.as<int32_t>(), k, k, a.order,
+                                     j.idx, j.raw, j.dist, ctx->sms, ctx->stream),
+             "rerank");
+    ctx->launches += 2;
+  } else {
+    EVOC_TRY(evoc::launch_nnd_emit(a, cur, j.idx, j.raw, j.dist, ctx->stream), "emit");
+    ctx->launches += 1;
+  }
+  return EVOC_OK;
+}
+
 int knn_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtype, const void* data, int64_t n,
              int64_t dim, int32_t k, const int64_t* rng_state, int32_t* out_idx, float* out_dist, float* out_raw,
              int32_t* out_k) {
@@ -399,7 +501,6 @@ int knn_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtype, con
     if (opts_in->struct_size != sizeof(evoc_gpu_opts)) return fail(ctx, EVOC_ERR_ARG, "opts.struct_size mismatch");
     opts = *opts_in;
   }
-  (void)rng_state;
   if (k <= 0) return fail(ctx, EVOC_ERR_K, "n_neighbors must be positive");
   if (n <= 0) return fail(ctx, EVOC_ERR_EMPTY, "empty embedding matrix");
   if (!data || !out_idx) return fail(ctx, EVOC_ERR_ARG, "null data or out_idx");
@@ -443,7 +544,7 @@ int knn_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtype, con
   job.status = d_flags + 1;
   int rc = EVOC_OK;
   if (dtype == EVOC_DTYPE_F32) {
-    if (form != EVOC_FORM_FP32 && form != EVOC_FORM_BF16_RERANK)
+    if (form != EVOC_FORM_FP32 && form != EVOC_FORM_BF16_RERANK && form != EVOC_FORM_NNDESCENT)
       return fail(ctx, EVOC_ERR_UNSUPPORTED, "form not built for f32 in this library");
     const int ld = int(round_up(dim, 16));
     rc = stage_rows(ctx, data, n, dim * 4, int64_t(ld) * 4, on_dev);
@@ -457,19 +558,38 @@ int knn_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtype, con
       ctx->launches += 2;
     }
     if (form == EVOC_FORM_FP32) rc = run_fp32(ctx, job, ld);
-    else rc = run_bf16_rerank(ctx, opts, job, ld, int(dim));
+    else if (form == EVOC_FORM_BF16_RERANK) rc = run_bf16_rerank(ctx, opts, job, ld, int(dim));
+    else {
+      // The pivot cells come from the BF16 tensor-core scan; the join reads the f32 rows.
+      const int64_t ldb = round_up(dim, 64);
+      const int64_t rows = evoc::padded_rows(n);
+      {
+        Stage st(ctx, "to_bf16");
+        EVOC_TRY(ctx->xb.ensure(size_t(rows * ldb * 2)), "alloc bf16 rows");
+        EVOC_TRY(evoc::launch_to_bf16(ctx->x.as<float>(), rows, ld, int(dim), ctx->xb.p, int(ldb), ctx->sms,
+                                      ctx->stream),
+                 "to bf16");
+        ctx->launches += 1;
+      }
+      rc = run_nndescent(ctx, opts, job, EVOC_DTYPE_F32, int64_t(ld) * 4, ctx->x.p, ld, int(dim), rng_state,
+                         ctx->xb.p, ldb * 2);
+    }
   } else if (dtype == EVOC_DTYPE_I8) {
-    if (form != EVOC_FORM_EXACT_INT) return fail(ctx, EVOC_ERR_UNSUPPORTED, "form not built for i8 in this library");
+    if (form != EVOC_FORM_EXACT_INT && form != EVOC_FORM_NNDESCENT)
+      return fail(ctx, EVOC_ERR_UNSUPPORTED, "form not built for i8 in this library");
     const int64_t ldb = round_up(dim, 128);
     rc = stage_rows(ctx, data, n, dim, ldb, on_dev);
     if (rc) return rc;
-    rc = run_int8(ctx, job, ldb);
+    if (form == EVOC_FORM_EXACT_INT) rc = run_int8(ctx, job, ldb);
+    else rc = run_nndescent(ctx, opts, job, EVOC_DTYPE_I8, ldb, ctx->x.p, 0, int(dim), rng_state, ctx->x.p, ldb);
   } else {
-    if (form != EVOC_FORM_EXACT_INT) return fail(ctx, EVOC_ERR_UNSUPPORTED, "form not built for u8 in this library");
+    if (form != EVOC_FORM_EXACT_INT && form != EVOC_FORM_NNDESCENT)
+      return fail(ctx, EVOC_ERR_UNSUPPORTED, "form not built for u8 in this library");
     const int64_t ldb = round_up(dim, 64);
     rc = stage_rows(ctx, data, n, dim, ldb, on_dev);
     if (rc) return rc;
-    rc = run_jaccard(ctx, job, ldb);
+    if (form == EVOC_FORM_EXACT_INT) rc = run_jaccard(ctx, job, ldb);
+    else rc = run_nndescent(ctx, opts, job, EVOC_DTYPE_U8, ldb, ctx->x.p, 0, int(dim), rng_state, nullptr, 0);
   }
   if (rc) return rc;
   int flags[2] = {0, 0};
@@ -535,7 +655,7 @@ void evoc_gpu_ctx_destroy(evoc_gpu_ctx* ctx) {
                     &ctx->out_raw,  &ctx->out_dist, &ctx->xb,   &ctx->cand,   &ctx->labels,
                     &ctx->order,    &ctx->hist,    &ctx->cursor, &ctx->pivots, &ctx->popc,
                     &ctx->g_idx,    &ctx->g_dist,  &ctx->g_sigma, &ctx->g_rho, &ctx->g_indptr,
-                    &ctx->g_indices, &ctx->g_data, &ctx->g_work};
+                    &ctx->g_indices, &ctx->g_data, &ctx->g_work, &ctx->nnd_work};
   for (DevBuf* b : bufs) b->release();
   for (auto& r : ctx->stages) {
     if (r.a) cudaEventDestroy(r.a);

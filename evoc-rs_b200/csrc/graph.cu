@@ -267,6 +267,11 @@ __global__ void union_write_kernel(int64_t n, int k, const int32_t* __restrict__
               data + indptr[i], true);
 }
 
+cudaError_t launch_scan_counts(const int32_t* cnt, int64_t n, int64_t* out, cudaStream_t stream) {
+  scan_counts_kernel<<<1, 1024, 0, stream>>>(cnt, n, out);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_smooth_and_membership(const int32_t* idx, const float* dist, int64_t n, int k, float n_neighbors,
                                          const FuzzyWork& w, float* sigma, float* rho, int sms, cudaStream_t stream) {
   if (k < 1 || k > kMaxK) return cudaErrorInvalidValue;

@@ -178,6 +178,11 @@ knn_jaccard_kernel(const uint32_t* __restrict__ X, const int32_t* __restrict__ p
   }
 }
 
+cudaError_t launch_popcount_rows(const void* X, int64_t n, int ldw, int32_t* pc, int sms, cudaStream_t stream) {
+  popcount_rows_kernel<<<sms * 4, 256, 0, stream>>>(static_cast<const uint32_t*>(X), n, ldw, pc);
+  return cudaGetLastError();
+}
+
 size_t knn_jaccard_smem(int k) { return sizeof(JacSmem) + size_t(BM) * size_t(k | 1) * 8; }
 
 cudaError_t launch_knn_jaccard(const void* X, int64_t n, int ldw, int k, int32_t* pc, int grid, int32_t* out_idx,

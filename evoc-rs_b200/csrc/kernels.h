@@ -87,3 +87,40 @@ cudaError_t launch_fuzzy_union_count(int64_t n, int k, int symmetrize, const Fuz
 cudaError_t launch_fuzzy_union_write(int64_t n, int k, int symmetrize, const FuzzyWork& w, const int64_t* indptr,
                                      int32_t* indices, float* data, int sms, cudaStream_t stream);
 }  // namespace evoc
+
+namespace evoc {
+// graph.cu: out[0] = 0, out[i+1] = cnt[0] + ... + cnt[i].
+cudaError_t launch_scan_counts(const int32_t* cnt, int64_t n, int64_t* out, cudaStream_t stream);
+// jaccard.cu: per-row popcounts of rows of ldw 32-bit words.
+cudaError_t launch_popcount_rows(const void* X, int64_t n, int ldw, int32_t* pc, int sms, cudaStream_t stream);
+
+// nndescent.cu: GPU NN-descent.
+struct NndArgs {
+  const uint8_t* X;       // rows of row_bytes (f32, int8, or packed bits)
+  int64_t row_bytes;      // multiple of 16
+  const int32_t* pc;      // row popcounts (binary rows), else null
+  int64_t n;
+  int k;                  // <= 32
+  int dtype;              // 0 f32, 1 i8, 2 u8
+  int sms;
+  const int32_t* order;   // visit order (rows grouped by pivot cell) or null
+  const int32_t* label;   // pivot cell of each row or null
+  const int32_t* cell_end;
+  const int32_t* cell_cnt;
+  uint64_t seed;
+  uint64_t* keys[2];      // n x k sorted (raw, index) keys, double buffered
+  uint8_t* isnew[2];      // n x k flags
+  int32_t* rcnt;          // n
+  int64_t* rptr;          // n + 1
+  int32_t* rfill;         // n
+  int32_t* rrows;         // n x k
+  int32_t* rsel;          // n x rcap
+  int32_t* rn;            // n
+  int rcap;
+  unsigned long long* changes;
+};
+cudaError_t launch_nnd_init(const NndArgs& a, cudaStream_t stream);
+cudaError_t launch_nnd_iteration(const NndArgs& a, int cur, int iter, cudaStream_t stream);
+cudaError_t launch_nnd_emit(const NndArgs& a, int cur, int32_t* out_idx, float* out_raw, float* out_dist,
+                            cudaStream_t stream);
+}  // namespace evoc

@@ -223,6 +223,30 @@ __global__ void label_scatter_kernel(const int32_t* __restrict__ label, int64_t 
   }
 }
 
+// Rows inside each cell sorted by index, so the order does not depend on the
+// order the scatter's atomics ran in (Shell sort, one thread per cell).
+__global__ void sort_cells_kernel(const int32_t* __restrict__ cell_end, const int32_t* __restrict__ cell_cnt, int nb,
+                                  int32_t* __restrict__ order) {
+  const int gaps[] = {701, 301, 132, 57, 23, 10, 4, 1};
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+    const int64_t m = cell_cnt[b];
+    int32_t* r = order + (cell_end[b] - m);
+    for (int gi = 0; gi < 8; gi++) {
+      const int64_t g = gaps[gi];
+      if (g >= m) continue;
+      for (int64_t a = g; a < m; a++) {
+        const int32_t v = r[a];
+        int64_t j = a;
+        while (j >= g && r[j - g] > v) {
+          r[j] = r[j - g];
+          j -= g;
+        }
+        r[j] = v;
+      }
+    }
+  }
+}
+
 cudaError_t launch_gather_pivots(const void* src, int64_t row_bytes, int64_t n, int64_t n_piv, void* dst, int sms,
                                  cudaStream_t stream) {
   gather_rows_kernel<<<sms * 4, 256, 0, stream>>>(static_cast<const uint8_t*>(src), row_bytes, n, n_piv,
@@ -238,6 +262,7 @@ cudaError_t launch_order_by_label(const int32_t* label, int64_t n, int nb, int32
   label_hist_kernel<<<sms * 4, 256, 0, stream>>>(label, n, nb, hist);
   exclusive_scan_kernel<<<1, 1024, 0, stream>>>(hist, nb, cursor);
   label_scatter_kernel<<<sms * 4, 256, 0, stream>>>(label, n, nb, cursor, order);
+  sort_cells_kernel<<<(nb + 127) / 128, 128, 0, stream>>>(cursor, hist, nb, order);
   return cudaGetLastError();
 }
 

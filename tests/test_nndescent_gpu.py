@@ -1,0 +1,100 @@
+"""GPU NN-descent form (EVOC_FORM_NNDESCENT), judged by recall.
+
+The reference's kNN is NN-descent (src/nndescent/*.rs); the GPU form is an
+NN-descent too, so it is held to recall@k against exact neighbours (FP64 for
+f32, the oracle's exact integer selection for i8 / binary), reported next to
+the reference NN-descent's own recall (the oracle's restatement) on the same
+data.  Distances it reports must be the true dissimilarities of the pairs
+(f32: within 1e-6 of FP64 after the FP32 rerank; integer forms: bit-exact).
+"""
+import numpy as np
+import pytest
+
+import evoc
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def nnd(k, **kw):
+    return evoc.KnnGraphOptions(n_neighbors=k, form="nndescent", **kw)
+
+
+def _recall(ind, truth):
+    return np.mean([len(set(ind[r]) & set(truth[r])) / truth.shape[1] for r in range(len(ind))])
+
+
+def test_nndescent_f32_recall_and_exact_distances():
+    from evoc import synthetic
+
+    x = synthetic.blobs(n_per=600, centres=10, dim=64, noise=0.3, seed=9)
+    k = 15
+    ind, dst, raw = evoc.knn_graph(x, nnd(k), np.random.RandomState(3), return_raw=True)
+    ei, er = O.exact_knn(x, k)
+    rec = _recall(ind, ei)
+    ref_ind, _ = O.knn_graph(x, k, O.RandomState(3), deterministic=False, n_threads=4)
+    ref_rec = _recall(ref_ind, ei)
+    print(f"GPU NN-descent recall {rec:.4f}, reference NN-descent recall {ref_rec:.4f}")
+    assert rec >= 0.95 and rec >= ref_rec - 0.02
+    x64 = x.astype(np.float64)
+    dots = np.einsum("rkd,rd->rk", x64[ind], x64)
+    want = np.where(dots > 0, -dots, 1.17549435e-38)
+    want[ind == np.arange(len(x))[:, None]] = -1.0
+    assert np.abs(raw - want).max() <= 1e-6
+    assert np.all(ind[:, 0] == np.arange(len(x)))
+
+
+def test_nndescent_deterministic():
+    from evoc import synthetic
+
+    x = synthetic.blobs(n_per=300, centres=8, dim=48, seed=2)
+    a = evoc.knn_graph(x, nnd(10), np.random.RandomState(5))
+    b = evoc.knn_graph(x, nnd(10), np.random.RandomState(5))
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+def _int8(n, d, seed):
+    rng = np.random.default_rng(seed)
+    c = rng.standard_normal((12, d))
+    v = c[rng.integers(0, 12, n)] + 0.3 * rng.standard_normal((n, d))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    return np.clip(np.round(127 * v), -127, 127).astype(np.int8)
+
+
+def test_nndescent_int8_recall_exact_values():
+    x = _int8(4000, 96, 1)
+    k = 12
+    ind, dst, raw = evoc.knn_graph(x, nnd(k), np.random.RandomState(1), return_raw=True)
+    ei, er = O.exact_knn(x, k)
+    hits = np.mean([np.sum(raw[r] <= er[r][-1]) / k for r in range(len(x))])
+    assert hits >= 0.95
+    for r in range(0, len(x), 97):
+        for j in range(k):
+            c = ind[r, j]
+            want = -1.0 if c == r else O.distance(x, r, c)
+            assert raw[r, j] == np.float32(want)
+
+
+def test_nndescent_binary_recall_exact_values():
+    rng = np.random.default_rng(4)
+    P = rng.random((20, 512)) < 0.1
+    rows = P[rng.integers(0, 20, 3000)] ^ (rng.random((3000, 512)) < 0.05)
+    x = np.packbits(rows, axis=1)
+    k = 10
+    ind, dst, raw = evoc.knn_graph(x, nnd(k), np.random.RandomState(2), return_raw=True)
+    ei, er = O.exact_knn(x, k)
+    hits = np.mean([np.sum(raw[r] <= er[r][-1]) / k for r in range(len(x))])
+    assert hits >= 0.9
+    for r in range(0, len(x), 89):
+        for j in range(k):
+            c = ind[r, j]
+            want = -1.0 if c == r else O.distance(x, r, c)
+            assert raw[r, j] == np.float32(want)
+
+
+def test_nndescent_rejects_unsupported():
+    x = np.random.default_rng(0).standard_normal((100, 16)).astype(np.float32)
+    with pytest.raises(evoc.BackendError):
+        evoc.knn_graph(x, nnd(40))
+    with pytest.raises(evoc.BackendError):
+        evoc.knn_graph(x, nnd(5, row_begin=0, row_end=50))
