@@ -188,6 +188,134 @@ def transform_f64(dots, self_mask):
     return d
 
 
+SERVING_WORKLOAD = ("serving_10k: Poisson arrivals at 200 req/s; n log-uniform [500, 200000], d from "
+                    "{128, 384, 768}, 80% f32 / 20% i8, 5-50-cluster GMM sigma 0.3, k=15, HBM budget 150 GB")
+
+
+def _pct(v, q):
+    import numpy as np
+
+    return float(np.percentile(np.asarray(v, dtype=np.float64), q)) if len(v) else None
+
+
+def serve_stream(srv, pools, sched, ids, k, paced, forms=("bf16_rerank", "exact_int"), stall_s=300.0):
+    """Open-loop client: submits request i at its scheduled arrival (or all at
+    once), fetches each finished graph to host memory, and returns per-request
+    (arrival, admit, done-with-result-on-host) times in ns plus edges."""
+    import threading
+
+    import evoc
+    from evoc.serving import Server
+
+    opts = {False: evoc.KnnGraphOptions(n_neighbors=k, form=forms[0]),
+            True: evoc.KnnGraphOptions(n_neighbors=k, form=forms[1])}
+    lock = threading.Lock()
+    jid_to_i, arrival_ns = {}, {}
+    failures = []
+    t0 = Server.now_ns() + 20_000_000
+
+    def submitter():
+        try:
+            for i in ids:
+                at = t0 + (int(sched["arrival"][i] * 1e9) if paced else 0)
+                while True:
+                    now = Server.now_ns()
+                    if now >= at:
+                        break
+                    time.sleep(min(0.002, (at - now) / 1e9))
+                n, d, q = int(sched["n"][i]), int(sched["dim"][i]), bool(sched["i8"][i])
+                jid = srv.submit(pools.rows_for(int(i), n, d, q), opts[q], borrow=True)
+                with lock:
+                    jid_to_i[jid] = int(i)
+                    arrival_ns[int(i)] = at
+        except Exception as e:  # surfaced by the collector
+            failures.append(repr(e))
+
+    th = threading.Thread(target=submitter, daemon=True)
+    th.start()
+    rec = {}
+    while len(rec) < len(ids):
+        got = srv.wait_any(timeout=stall_s)
+        if got is None or failures:
+            raise RuntimeError(f"serving stalled or failed: {failures}")
+        jid, rc = got
+        info = srv.info(jid)
+        ind, _ = srv.result(jid)
+        t_done = Server.now_ns()
+        while True:
+            with lock:
+                i = jid_to_i.get(jid)
+            if i is not None:
+                break
+            time.sleep(0.0005)
+        rec[i] = (arrival_ns[i], info["admit_ns"], t_done, int(ind.shape[0]) * int(ind.shape[1]))
+    th.join()
+    return t0, rec
+
+
+def serving_summary(t0, rec):
+    arr = [rec[i][0] for i in rec]
+    lat = [(rec[i][2] - rec[i][0]) / 1e6 for i in rec]
+    queue = [(rec[i][1] - rec[i][0]) / 1e6 for i in rec]
+    end = max(rec[i][2] for i in rec)
+    edges = sum(rec[i][3] for i in rec)
+    span = (end - t0) / 1e9
+    return {"requests": len(rec), "edges": edges, "makespan_s": span, "edges_per_s": edges / span,
+            "arrival_window_s": (max(arr) - t0) / 1e9,
+            "latency_ms": {"p50": _pct(lat, 50), "p95": _pct(lat, 95), "p99": _pct(lat, 99), "max": max(lat)},
+            "queue_ms": {"p50": _pct(queue, 50), "p99": _pct(queue, 99)}}
+
+
+def run_serving(args, dev):
+    """The continuous-batching server on the serving workload, next to the
+    plain FP32 form run one request at a time on the same arrivals."""
+    import numpy as np
+
+    from evoc import synthetic
+    from evoc.serving import Server
+
+    k = 15
+    sched = synthetic.serving_schedule(count=args.serve_requests, rate=args.serve_rate)
+    pools = synthetic.ServingPools(dev)
+    offered = float((sched["n"] * k).sum() / max(sched["arrival"][-1], 1e-9))
+    # Warm-up requests: the largest shape of each (d, dtype) once per lane, then small ones.
+    warm = [(200_000, d, q) for d in (128, 384, 768) for q in (False, True) for _ in range(args.serve_lanes)]
+    small = [(500 + 97 * t, (128, 384, 768)[t % 3], t % 5 == 0) for t in range(16)]
+    warm += small
+    warm_sched = {"arrival": np.zeros(len(warm)), "n": np.array([w[0] for w in warm], np.int64),
+                  "dim": np.array([w[1] for w in warm], np.int64), "i8": np.array([w[2] for w in warm], bool)}
+    out = {"workload": SERVING_WORKLOAD, "lanes": args.serve_lanes, "budget_bytes": 150 * 10**9,
+           "offered_edges_per_s": offered,
+           "data": "rows cut from 4 pinned-host mixtures per (d, dtype), window chosen by request id",
+           "timing": "host monotonic clock: scheduled arrival -> graph copied back to host memory"}
+    with Server(budget_bytes=150 * 10**9, max_inflight=args.serve_lanes) as srv:
+        serve_stream(srv, pools, warm_sched, list(range(len(warm_sched["n"]))), k, paced=False)
+        t0, rec = serve_stream(srv, pools, sched, list(range(len(sched["n"]))), k, paced=True)
+        out.update(serving_summary(t0, rec))
+        st = srv.stats()
+        out["peak_bytes"] = st["peak_bytes"]
+        out["failed"] = st["failed"]
+        out["workspace_misses"] = st["workspace_misses"]
+        if args.serve_capacity > 0:
+            ids = list(range(min(args.serve_capacity, len(sched["n"]))))
+            t0c, recc = serve_stream(srv, pools, sched, ids, k, paced=False)
+            c = serving_summary(t0c, recc)
+            out["capacity"] = {"requests": c["requests"], "edges_per_s": c["edges_per_s"], "makespan_s": c["makespan_s"],
+                               "note": "the first requests of the stream submitted at once (closed queue)"}
+    if args.serve_baseline > 0:
+        ids = list(range(min(args.serve_baseline, len(sched["n"]))))
+        with Server(budget_bytes=150 * 10**9, max_inflight=1) as base:
+            serve_stream(base, pools, warm_sched, list(range(len(warm) - len(small), len(warm))), k, paced=False,
+                         forms=("fp32", "exact_int"))
+            t0b, recb = serve_stream(base, pools, sched, ids, k, paced=True, forms=("fp32", "exact_int"))
+        b = serving_summary(t0b, recb)
+        b["note"] = ("plain FP32 SIMT form (i8 requests: exact int8 form), one request at a time, on the first "
+                     f"{len(ids)} arrivals of the same stream; the queue grows without bound at this rate")
+        out["fp32_one_at_a_time"] = b
+        out["edges_per_s_vs_fp32_one_at_a_time"] = out["edges_per_s"] / b["edges_per_s"]
+    return out
+
+
 def run_ours(args, world, rank, local):
     import numpy as np
     import torch
@@ -353,6 +481,10 @@ def run_ours(args, world, rank, local):
         "clocks": clk,
         "gpu_launches": launches,
     }
+    if world == 1 and args.serve_requests > 0:
+        del xh, ih, dh, xh_np, ih_np, dh_np, x, oi, od
+        torch.cuda.empty_cache()
+        line["serving"] = run_serving(args, dev)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if pg:
@@ -374,6 +506,11 @@ def main():
     ap.add_argument("--fp32-rows", type=int, default=75_776)  # 2 full waves of 296 CTAs x 128 rows
     ap.add_argument("--recall-rows", type=int, default=10_000)
     ap.add_argument("--cpu-rows", type=int, default=150_000)
+    ap.add_argument("--serve-requests", type=int, default=10_000)
+    ap.add_argument("--serve-rate", type=float, default=200.0)
+    ap.add_argument("--serve-lanes", type=int, default=8)
+    ap.add_argument("--serve-capacity", type=int, default=2000)
+    ap.add_argument("--serve-baseline", type=int, default=250)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world, rank, local = dist_env()

@@ -17,6 +17,13 @@ constexpr float kMinPositive = 1.17549435e-38f;  // f32::MIN_POSITIVE
 constexpr float kHeapInf = 3.40282347e+38f;      // f32::MAX, heap.rs:8
 constexpr uint64_t kKeyInf = ~0ull;
 
+// Codes of a request's device status word (0 = ok).  1..3: a pipeline wait of
+// the tensor-core scan ran out (producer, MMA issuer, epilogue); 16, 17: a
+// self-check found a malformed row order or a candidate index out of range
+// and skipped it.
+constexpr int kStatusBadOrder = 16;
+constexpr int kStatusBadCandidate = 17;
+
 // Order-preserving map f32 -> u32 (after folding -0.0 onto +0.0).
 __device__ __forceinline__ uint32_t orderable(float f) {
   f = f + 0.0f;  // -0.0 + 0.0 == +0.0 under round-to-nearest

@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -15,6 +16,7 @@
 
 #include "../../include/evoc_gpu.h"
 #include "common.cuh"
+#include "ctx_plan.h"
 #include "kernels.h"
 
 namespace {
@@ -65,6 +67,7 @@ struct evoc_gpu_ctx {
   DevBuf g_idx, g_dist, g_sigma, g_rho, g_indptr, g_indices, g_data, g_work;
   DevBuf nnd_work;
   uint64_t timeout_ns = 4000000000ull;  // longest a pipeline wait inside a kernel may take
+  bool sync_check = false;  // EVOC_SYNC_CHECK=1: wait for and check every kernel stage (fault diagnosis)
   bool profiling = false;
   std::vector<StageRec> stages;  // event pool; the first n_stages belong to the last call
   int n_stages = 0;
@@ -88,6 +91,10 @@ int cuda_fail(evoc_gpu_ctx* ctx, cudaError_t e, const char* where) {
   do {                                                       \
     cudaError_t _e = (expr);                                 \
     if (_e != cudaSuccess) return cuda_fail(ctx, _e, where); \
+    if (ctx->sync_check) {                                   \
+      _e = cudaStreamSynchronize(ctx->stream);               \
+      if (_e != cudaSuccess) return cuda_fail(ctx, _e, where); \
+    }                                                        \
   } while (0)
 
 // Records CUDA events around one stage on the context's stream when profiling.
@@ -166,11 +173,16 @@ int run_fp32(evoc_gpu_ctx* ctx, const Job& j, int ld) {
 
 // Query rows grouped by nearest pivot so that concurrently reranked rows share
 // candidates in L2.  Leaves ctx->order holding a permutation of 0..nq-1.
-int locality_order(evoc_gpu_ctx* ctx, const Job& j, const void* rows, int64_t row_bytes, bool int8) {
-  Stage st(ctx, "pivot_order");
-  int64_t n_piv = j.n / 256;
+int64_t pivot_count(int64_t n) {
+  int64_t n_piv = n / 256;
   if (n_piv > 4096) n_piv = 4096;
   if (n_piv < 2) n_piv = 2;
+  return n_piv;
+}
+
+int locality_order(evoc_gpu_ctx* ctx, const Job& j, const void* rows, int64_t row_bytes, bool int8) {
+  Stage st(ctx, "pivot_order");
+  const int64_t n_piv = pivot_count(j.n);
   const int64_t piv_rows = evoc::padded_rows(n_piv);
   EVOC_TRY(ctx->pivots.ensure(size_t(piv_rows * row_bytes)), "alloc pivots");
   EVOC_TRY(cudaMemsetAsync(ctx->pivots.p, 0, size_t(piv_rows * row_bytes), ctx->stream), "clear pivots");
@@ -192,11 +204,17 @@ int locality_order(evoc_gpu_ctx* ctx, const Job& j, const void* rows, int64_t ro
   return EVOC_OK;
 }
 
-int run_bf16_rerank(evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, const Job& j, int ld, int d) {
+// Candidates kept per row by the BF16 scan: oversample * k, within [k, n].
+int64_t bf16_candidates(const evoc_gpu_opts& opts, int64_t n, int keff) {
   const int over = opts.oversample > 0 ? opts.oversample : 2;
-  int64_t C = int64_t(over) * j.keff;
-  if (C > j.n) C = j.n;
-  if (C < j.keff) C = j.keff;
+  int64_t C = int64_t(over) * keff;
+  if (C > n) C = n;
+  if (C < keff) C = keff;
+  return C;
+}
+
+int run_bf16_rerank(evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, const Job& j, int ld, int d) {
+  const int64_t C = bf16_candidates(opts, j.n, j.keff);
   if (C > 256) return fail(ctx, EVOC_ERR_UNSUPPORTED, "oversample * k must be <= 256");
   const int64_t ldb = round_up(d, 64);
   const int64_t rows = evoc::padded_rows(j.n);
@@ -225,8 +243,8 @@ int run_bf16_rerank(evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, const Job& j, 
     order = ctx->order.as<int32_t>();
   }
   Stage st(ctx, "rerank");
-  EVOC_TRY(evoc::launch_rerank_f32(ctx->x.as<float>(), ld, d, j.nq, j.r0, ctx->cand.as<int32_t>(), int(C), j.keff,
-                                   order, j.idx, j.raw, j.dist, ctx->sms, ctx->stream),
+  EVOC_TRY(evoc::launch_rerank_f32(ctx->x.as<float>(), ld, d, j.nq, j.n, j.r0, ctx->cand.as<int32_t>(), int(C),
+                                   j.keff, order, j.idx, j.raw, j.dist, j.status, ctx->sms, ctx->stream),
            "rerank");
   ctx->launches += 1;
   return EVOC_OK;
@@ -393,6 +411,25 @@ int fuzzy_impl(evoc_gpu_ctx* ctx, const int32_t* idx, const float* dist, int64_t
 // supported: the graph is built for every row.
 // `piv_rows` / `piv_row_bytes`: the rows the pivot scan runs on (BF16 for f32
 // data, the int8 rows themselves for i8); unused for binary rows.
+constexpr int kNndParts = 11;
+
+// Parts of the NN-descent work buffer (graph keys and newness flags, double
+// buffered; reverse-edge counts, offsets, fill cursors, rows; the sampled
+// reverse lists and their lengths; the change counter), each 256-byte aligned.
+// Returns the total.
+size_t nnd_work_sizes(int64_t n, int k, size_t* sizes) {
+  const size_t nk = size_t(n) * size_t(k);
+  const size_t rcap = size_t(k);
+  const size_t v[kNndParts] = {nk * 8, nk * 8, nk, nk, size_t(n) * 4, size_t(n + 1) * 8, size_t(n) * 4, nk * 4,
+                               size_t(n) * rcap * 4, size_t(n) * 4, 64};
+  size_t total = 0;
+  for (int i = 0; i < kNndParts; i++) {
+    sizes[i] = v[i];
+    total += (v[i] + 255) / 256 * 256;
+  }
+  return total;
+}
+
 int run_nndescent(evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, const Job& j, int32_t dtype, int64_t row_bytes,
                   const void* rows, int ld_f32, int d, const int64_t* rng_state, const void* piv_rows,
                   int64_t piv_row_bytes) {
@@ -429,14 +466,12 @@ int run_nndescent(evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, const Job& j, in
     a.cell_cnt = ctx->hist.as<int32_t>();
   }
   const size_t nk = size_t(n) * size_t(k);
-  const size_t sizes[] = {nk * 8, nk * 8, nk, nk, size_t(n) * 4, size_t(n + 1) * 8, size_t(n) * 4, nk * 4,
-                          size_t(n) * size_t(rcap) * 4, size_t(n) * 4, 64};
-  size_t total = 0;
-  for (size_t s : sizes) total += (s + 255) / 256 * 256;
+  size_t sizes[kNndParts];
+  const size_t total = nnd_work_sizes(n, k, sizes);
   EVOC_TRY(ctx->nnd_work.ensure(total), "alloc NN-descent work");
   uint8_t* p = ctx->nnd_work.as<uint8_t>();
-  void* ptrs[11];
-  for (int i = 0; i < 11; i++) {
+  void* ptrs[kNndParts];
+  for (int i = 0; i < kNndParts; i++) {
     ptrs[i] = p;
     p += (sizes[i] + 255) / 256 * 256;
   }
@@ -476,8 +511,8 @@ int run_nndescent(evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, const Job& j, in
   if (dtype == EVOC_DTYPE_F32) {
     EVOC_TRY(ctx->cand.ensure(nk * 4), "alloc candidates");
     EVOC_TRY(evoc::launch_nnd_emit(a, cur, ctx->cand.as<int32_t>(), nullptr, nullptr, ctx->stream), "emit");
-    EVOC_TRY(evoc::launch_rerank_f32(ctx->x.as<float>(), ld_f32, d, n, 0, ctx->cand.as<int32_t>(), k, k, a.order,
-                                     j.idx, j.raw, j.dist, ctx->sms, ctx->stream),
+    EVOC_TRY(evoc::launch_rerank_f32(ctx->x.as<float>(), ld_f32, d, n, n, 0, ctx->cand.as<int32_t>(), k, k, a.order,
+                                     j.idx, j.raw, j.dist, j.status, ctx->sms, ctx->stream),
              "rerank");
     ctx->launches += 2;
   } else {
@@ -605,6 +640,8 @@ int knn_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtype, con
   EVOC_TRY(cudaMemcpyAsync(flags, d_flags, sizeof(flags), cudaMemcpyDeviceToHost, ctx->stream), "read status");
   total.end();
   EVOC_TRY(cudaStreamSynchronize(ctx->stream), "knn_graph");
+  if (flags[1] == evoc::kStatusBadOrder || flags[1] == evoc::kStatusBadCandidate)
+    return fail(ctx, EVOC_ERR_CUDA, "device self-check failed (code " + std::to_string(flags[1]) + ")");
   if (flags[1] != 0)
     return fail(ctx, EVOC_ERR_TIMEOUT, "a kernel pipeline wait timed out (stage " + std::to_string(flags[1]) + ")");
   return EVOC_OK;
@@ -638,6 +675,7 @@ int evoc_gpu_ctx_create(int device, evoc_gpu_ctx** out) {
   evoc_gpu_ctx* ctx = new evoc_gpu_ctx();
   ctx->device = device;
   cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device);
+  if (const char* v = std::getenv("EVOC_SYNC_CHECK")) ctx->sync_check = v[0] == '1';
   e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     delete ctx;
@@ -720,3 +758,95 @@ int evoc_gpu_knn_graph_raw(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts, int32_t
 }
 
 }  // extern "C"
+
+namespace evoc {
+
+// Mirrors the ensure() calls of knn_impl and the run_* functions above for a
+// whole-graph request with device-resident outputs.  A form that fails its
+// own checks (k or candidate limits) allocates no more than listed here.
+void knn_buffer_needs(const evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, int32_t dtype, int64_t n, int64_t dim,
+                      int32_t k, CtxSizes* need) {
+  *need = CtxSizes{};
+  size_t* b = need->b;
+  const int64_t keff = std::max<int64_t>(1, std::min<int64_t>(k, n - 1));
+  const int form = resolve_form(dtype, opts.form);
+  const int64_t rows = padded_rows(n);
+  const int64_t qblocks = (n + 127) / 128;
+  const int64_t grid = std::min<int64_t>(qblocks, ctx->sms);
+  auto locality = [&](int64_t row_bytes) {
+    const int64_t n_piv = pivot_count(n);
+    b[kBufPivots] = size_t(padded_rows(n_piv) * row_bytes);
+    b[kBufLabels] = size_t(n) * 4;
+    b[kBufOrder] = size_t(n) * 4;
+    b[kBufHist] = size_t(n_piv) * 4;
+    b[kBufCursor] = size_t(n_piv) * 4;
+  };
+  auto nnd = [&]() {
+    size_t sizes[kNndParts];
+    b[kBufNnd] = nnd_work_sizes(n, int(keff), sizes);
+  };
+  b[kBufFlag] = 64;
+  if (dtype == EVOC_DTYPE_F32) {
+    b[kBufX] = size_t(rows * round_up(dim, 16) * 4);
+    b[kBufNorms] = size_t(n) * 4;
+    const int64_t ldb = round_up(dim, 64);
+    if (form == EVOC_FORM_FP32) {
+      const int64_t g = std::min<int64_t>(qblocks, int64_t(ctx->sms) * 2);
+      b[kBufScratch] = size_t(g) * 128 * size_t(topk_capacity(int(keff))) * 8;
+    } else if (form == EVOC_FORM_BF16_RERANK) {
+      const int64_t C = bf16_candidates(opts, n, int(keff));
+      b[kBufXb] = size_t(rows * ldb * 2);
+      b[kBufCand] = size_t(n * C) * 4;
+      b[kBufScratch] = size_t(grid) * 256 * size_t(C) * 8;
+      if (n >= 65536) locality(ldb * 2);
+    } else if (form == EVOC_FORM_NNDESCENT) {
+      b[kBufXb] = size_t(rows * ldb * 2);
+      locality(ldb * 2);
+      nnd();
+      b[kBufCand] = size_t(n) * size_t(keff) * 4;
+    }
+  } else if (dtype == EVOC_DTYPE_I8) {
+    const int64_t ldb = round_up(dim, 128);
+    b[kBufX] = size_t(rows * ldb);
+    if (form == EVOC_FORM_EXACT_INT) {
+      b[kBufScratch] = size_t(grid) * 256 * size_t(keff) * 8;
+    } else if (form == EVOC_FORM_NNDESCENT) {
+      locality(ldb);
+      nnd();
+    }
+  } else {
+    b[kBufX] = size_t(rows * round_up(dim, 64));
+    if (form == EVOC_FORM_EXACT_INT) {
+      b[kBufPopc] = size_t(n) * 4;
+    } else if (form == EVOC_FORM_NNDESCENT) {
+      b[kBufPopc] = size_t(n) * 4;
+      nnd();
+    }
+  }
+}
+
+void ctx_buffer_sizes(const evoc_gpu_ctx* ctx, CtxSizes* cur) {
+  const DevBuf* bufs[kBufCount] = {&ctx->x,      &ctx->scratch, &ctx->norms, &ctx->flag,   &ctx->xb,
+                                   &ctx->cand,   &ctx->labels,  &ctx->order, &ctx->hist,   &ctx->cursor,
+                                   &ctx->pivots, &ctx->popc,    &ctx->nnd_work};
+  for (int i = 0; i < kBufCount; i++) cur->b[i] = bufs[i]->bytes;
+}
+
+CtxSizes grown_sizes(const CtxSizes& cur, const CtxSizes& need) {
+  CtxSizes out = cur;
+  for (int i = 0; i < kBufCount; i++)
+    if (need.b[i] > cur.b[i]) out.b[i] = need.b[i] + need.b[i] / 8;
+  return out;
+}
+
+void ctx_release_buffers(evoc_gpu_ctx* ctx) {
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  DevBuf* bufs[kBufCount] = {&ctx->x,      &ctx->scratch, &ctx->norms, &ctx->flag,   &ctx->xb,
+                             &ctx->cand,   &ctx->labels,  &ctx->order, &ctx->hist,   &ctx->cursor,
+                             &ctx->pivots, &ctx->popc,    &ctx->nnd_work};
+  for (DevBuf* b : bufs) b->release();
+}
+
+}  // namespace evoc

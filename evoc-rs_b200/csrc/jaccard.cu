@@ -193,7 +193,9 @@ cudaError_t launch_knn_jaccard(const void* X, int64_t n, int ldw, int k, int32_t
   popcount_rows_kernel<<<sms * 4, 256, 0, stream>>>(static_cast<const uint32_t*>(X), n, ldw, pc);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(knn_jaccard_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  // The opt-in limit rather than `smem` (which varies with k), so concurrent
+  // callers never lower each other's limit before their launch.
+  e = cudaFuncSetAttribute(knn_jaccard_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 232448);
   if (e != cudaSuccess) return e;
   knn_jaccard_kernel<<<grid, NT, smem, stream>>>(static_cast<const uint32_t*>(X), pc, n, ldw, k, k | 1, out_idx,
                                                  out_raw, out_dist, q_begin, q_end);

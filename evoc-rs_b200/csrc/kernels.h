@@ -46,9 +46,9 @@ cudaError_t launch_tc_scan(bool int8, const void* Q, int64_t q_rows, int64_t q_r
                            int* status, uint64_t timeout_ns, cudaStream_t stream);
 
 // rerank.cu
-cudaError_t launch_rerank_f32(const float* X, int ld, int d, int64_t n_q, int64_t q_row0, const int32_t* cand, int C,
-                              int k, const int32_t* order, int32_t* out_idx, float* out_raw, float* out_dist, int sms,
-                              cudaStream_t stream);
+cudaError_t launch_rerank_f32(const float* X, int ld, int d, int64_t n_q, int64_t n_keys, int64_t q_row0,
+                              const int32_t* cand, int C, int k, const int32_t* order, int32_t* out_idx, float* out_raw,
+                              float* out_dist, int* status, int sms, cudaStream_t stream);
 cudaError_t launch_gather_pivots(const void* src, int64_t row_bytes, int64_t n, int64_t n_piv, void* dst, int sms,
                                  cudaStream_t stream);
 cudaError_t launch_order_by_label(const int32_t* label, int64_t n, int nb, int32_t* hist, int32_t* cursor,

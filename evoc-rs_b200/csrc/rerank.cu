@@ -60,17 +60,24 @@ __device__ __forceinline__ float key_raw(uint64_t key) { return from_orderable(u
 }  // namespace
 
 __global__ void __launch_bounds__(RW * 32)
-rerank_f32_kernel(const float* __restrict__ X, int ld, int d, int64_t n, int64_t q_row0,
-                  const int32_t* __restrict__ cand, int C, int k, const int32_t* __restrict__ order, int32_t* __restrict__ out_idx, float* __restrict__ out_raw,
-                  float* __restrict__ out_dist) {
+rerank_f32_kernel(const float* __restrict__ X, int ld, int d, int64_t n, int64_t n_keys, int64_t q_row0,
+                  const int32_t* __restrict__ cand, int C, int k, const int32_t* __restrict__ order,
+                  int32_t* __restrict__ out_idx, float* __restrict__ out_raw, float* __restrict__ out_dist,
+                  int* status) {
   __shared__ uint64_t keys[RW][MAXC];
   __shared__ double d64[RW][32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // The candidates are only complete when the scan that wrote them finished.
+  if (status && *reinterpret_cast<volatile int*>(status) != 0) return;
   uint64_t* kw = keys[warp];
   int P = 1;
   while (P < C) P <<= 1;
   for (int64_t w = int64_t(blockIdx.x) * RW + warp; w < n; w += int64_t(gridDim.x) * RW) {
-    const int64_t q = order ? order[w] : w;  // output row
+    int64_t q = order ? order[w] : w;  // output row
+    if (q < 0 || q >= n) {               // a malformed order: record it, skip the row
+      if (lane == 0 && status) atomicCAS(status, 0, kStatusBadOrder);
+      continue;
+    }
     const int64_t qg = q_row0 + q;           // row of the data set
     const float* xq = X + qg * ld;
     const int32_t* cq = cand + q * C;
@@ -80,6 +87,10 @@ rerank_f32_kernel(const float* __restrict__ X, int ld, int d, int64_t n, int64_t
 #pragma unroll
       for (int u = 0; u < GROUP; u++) {
         id[u] = (j0 + u < C) ? cq[j0 + u] : -1;
+        if (id[u] >= n_keys) {  // never written by a finished scan: record it, skip the candidate
+          if (status) atomicCAS(status, 0, kStatusBadCandidate);
+          id[u] = -1;
+        }
         acc[u] = 0.0f;
       }
       for (int t = lane; t < d; t += 32) {
@@ -152,14 +163,14 @@ rerank_f32_kernel(const float* __restrict__ X, int ld, int d, int64_t n, int64_t
   }
 }
 
-cudaError_t launch_rerank_f32(const float* X, int ld, int d, int64_t n, int64_t q_row0, const int32_t* cand, int C,
-                              int k, const int32_t* order, int32_t* out_idx, float* out_raw, float* out_dist, int sms,
-                              cudaStream_t stream) {
+cudaError_t launch_rerank_f32(const float* X, int ld, int d, int64_t n, int64_t n_keys, int64_t q_row0,
+                              const int32_t* cand, int C, int k, const int32_t* order, int32_t* out_idx, float* out_raw,
+                              float* out_dist, int* status, int sms, cudaStream_t stream) {
   if (C > MAXC || C < 1) return cudaErrorInvalidValue;
   int64_t blocks = (n + RW - 1) / RW;
   if (blocks > int64_t(sms) * 16) blocks = int64_t(sms) * 16;
-  rerank_f32_kernel<<<unsigned(blocks), RW * 32, 0, stream>>>(X, ld, d, n, q_row0, cand, C, k, order, out_idx,
-                                                               out_raw, out_dist);
+  rerank_f32_kernel<<<unsigned(blocks), RW * 32, 0, stream>>>(X, ld, d, n, n_keys, q_row0, cand, C, k, order,
+                                                               out_idx, out_raw, out_dist, status);
   return cudaGetLastError();
 }
 
@@ -219,7 +230,7 @@ __global__ void label_scatter_kernel(const int32_t* __restrict__ label, int64_t 
     int b = label[i];
     b = (b < 0 || b >= nb) ? 0 : b;
     const int32_t pos = atomicAdd(&cursor[b], 1);
-    order[pos] = int32_t(i);
+    if (pos >= 0 && pos < n) order[pos] = int32_t(i);
   }
 }
 

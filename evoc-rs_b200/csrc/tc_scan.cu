@@ -132,7 +132,8 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
   const uint32_t pad = (1024u - (smem_addr(smem_dyn) & 1023u)) & 1023u;
   uint8_t* smem = smem_dyn + pad;
   uint64_t* heaps = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
-  uint64_t* bars = kSmemHeap ? heaps + BM * p.heap_stride : heaps;
+  // Barriers follow every group's heaps (GROUPS x BM rows of heap_stride words).
+  uint64_t* bars = kSmemHeap ? heaps + GROUPS * BM * p.heap_stride : heaps;
   uint64_t* full = bars;
   uint64_t* empty = bars + STAGES;
   uint64_t* tfull = bars + 2 * STAGES;
@@ -343,16 +344,18 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
 // ---------------------------------------------------------------------------
 namespace {
 
+// Looked up once per process; the initialisation of a local static is
+// thread-safe, so serving lanes may make their first scans concurrently.
 PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  if (!fn) {
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = []() -> PFN_cuTensorMapEncodeTiled_v12000 {
     void* p = nullptr;
     cudaDriverEntryPointQueryResult q;
     if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
             cudaSuccess &&
         q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-  }
+      return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    return nullptr;
+  }();
   return fn;
 }
 
@@ -379,7 +382,10 @@ template <bool kInt8, int STAGES, int GROUPS, bool kSmemHeap>
 cudaError_t launch_variant(const CUtensorMap& ma, const CUtensorMap& mb, const ScanParams& p, int grid, size_t smem,
                            cudaStream_t stream) {
   auto kern = tc_scan_kernel<kInt8, STAGES, GROUPS, kSmemHeap>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  // The opt-in limit, not `smem`: the launch's shared memory varies with keep,
+  // and concurrent callers (serving lanes) must not lower each other's limit
+  // between this call and their launch.
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_LIMIT));
   if (e != cudaSuccess) return e;
   kern<<<grid, 64 + GROUPS * 128, smem, stream>>>(ma, mb, p);
   return cudaGetLastError();

@@ -95,6 +95,57 @@ def _bind_optional(L) -> None:
                                            C.POINTER(i64)]
     if hasattr(L, "evoc_gpu_smooth_knn_dist"):
         L.evoc_gpu_smooth_knn_dist.argtypes = [P, P, i64, i32, C.c_float, i32, P, P]
+    if hasattr(L, "evoc_gpu_server_create"):
+        L.evoc_gpu_server_default_opts.argtypes = [C.POINTER(ServerOpts)]
+        L.evoc_gpu_server_create.argtypes = [C.POINTER(ServerOpts), C.POINTER(P)]
+        L.evoc_gpu_server_destroy.argtypes = [P]
+        L.evoc_gpu_server_now_ns.restype = i64
+        L.evoc_gpu_server_submit.argtypes = [P, C.POINTER(Opts), i32, P, i64, i64, i32, P, i32, C.POINTER(i64)]
+        L.evoc_gpu_server_request_bytes.argtypes = [P, C.POINTER(Opts), i32, i64, i64, i32, C.POINTER(i64),
+                                                    C.POINTER(i64)]
+        L.evoc_gpu_server_poll.argtypes = [P, i64]
+        L.evoc_gpu_server_wait.argtypes = [P, i64, i64]
+        L.evoc_gpu_server_wait_any.argtypes = [P, i64, C.POINTER(i64)]
+        L.evoc_gpu_server_result.argtypes = [P, i64, P, P, C.POINTER(i32), i32]
+        L.evoc_gpu_server_result_device.argtypes = [P, i64, C.POINTER(P), C.POINTER(P), C.POINTER(i32)]
+        L.evoc_gpu_server_release.argtypes = [P, i64]
+        L.evoc_gpu_server_cancel.argtypes = [P, i64]
+        L.evoc_gpu_server_job_info.argtypes = [P, i64, C.POINTER(JobInfo)]
+        L.evoc_gpu_server_stats.argtypes = [P, C.POINTER(ServerCounters)]
+
+
+class ServerOpts(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_uint32),
+        ("device", C.c_int32),
+        ("budget_bytes", C.c_int64),
+        ("max_inflight", C.c_int32),
+        ("reserved", C.c_int32 * 5),
+    ]
+
+
+class ServerCounters(C.Structure):
+    _fields_ = [(name, C.c_int64) for name in (
+        "submitted", "completed", "failed", "cancelled", "rejected", "pending", "running", "bytes_in_use",
+        "peak_bytes", "budget_bytes", "workspace_bytes", "workspace_misses", "lanes")]
+
+
+class JobInfo(C.Structure):
+    _fields_ = [
+        ("submit_ns", C.c_int64),
+        ("admit_ns", C.c_int64),
+        ("done_ns", C.c_int64),
+        ("n", C.c_int64),
+        ("dim", C.c_int64),
+        ("dtype", C.c_int32),
+        ("k_eff", C.c_int32),
+        ("lane", C.c_int32),
+        ("status", C.c_int32),
+        ("error", C.c_char * 160),
+    ]
+
+
+SUBMIT_BORROW = 1
 
 
 def header_symbols() -> list[str]:

@@ -13,6 +13,12 @@ documents the distribution it draws.
   bits_4m_1024     4,000,000 x 128 u8 (1,024 bits): 500 Bernoulli(0.1)
                    prototypes, each row copies a uniform prototype and flips
                    each bit with p = 0.05, packed big-endian, seed 13
+  serving_10k      10,000 requests, Poisson arrivals at 200 req/s; per
+                   request n log-uniform in [500, 200,000], d uniform from
+                   {128, 384, 768}, f32 (80%) or i8 (20%, round(127 x));
+                   each request's rows are a window of one of a few
+                   5-50-cluster Gaussian mixtures (sigma 0.3, L2-normalised),
+                   chosen and placed by the request id (seed 17)
 Rows are emitted in a seeded random order (not grouped by cluster).
 Large sets are generated on a CUDA device with torch when one is given.
 """
@@ -140,3 +146,51 @@ def bits_u8(n: int = 4_000_000, nbits: int = 1024, protos: int = 500, p_on: floa
         packed = (rows.view(len(l), nbytes, 8).to(torch.int32) * weights).sum(-1)
         out[s0:s0 + step] = packed.to(torch.uint8)
     return out
+
+
+def serving_schedule(count: int = 10_000, rate: float = 200.0, n_lo: int = 500, n_hi: int = 200_000,
+                     dims=(128, 384, 768), p_i8: float = 0.2, seed: int = 17) -> dict:
+    """Arrival times (s, first at 0), n, d and dtype of each request of the serving workload."""
+    rng = np.random.RandomState(seed)
+    gaps = rng.exponential(1.0 / rate, count)
+    arrival = np.cumsum(gaps) - gaps[0]
+    n = np.exp(rng.uniform(np.log(n_lo), np.log(n_hi), count)).astype(np.int64)
+    dim = np.asarray(dims, np.int64)[rng.randint(0, len(dims), count)]
+    i8 = rng.random_sample(count) < p_i8
+    return {"arrival": arrival, "n": n, "dim": dim, "i8": i8}
+
+
+class ServingPools:
+    """Row pools the serving requests are cut from: for each d, `mixtures`
+    Gaussian mixtures of 5..50 equal-weight clusters (centres N(0,1), sigma
+    0.3, rows L2-normalised) of `rows` rows, as f32 and as i8 (round(127 x),
+    clipped), in pinned host memory.  Request i reads mixture i % mixtures at a
+    seeded offset, so requests differ in data as well as in shape."""
+
+    def __init__(self, device, rows: int = 200_000, dims=(128, 384, 768), mixtures: int = 4, seed: int = 17):
+        import torch
+
+        self.rows, self.mixtures = rows, mixtures
+        self.pool = {}
+        g = torch.Generator(device=device)
+        g.manual_seed(seed)
+        clusters = np.linspace(5, 50, mixtures).round().astype(int)
+        for d in dims:
+            for m in range(mixtures):
+                c = int(clusters[m])
+                centres = torch.randn(c, d, generator=g, device=device)
+                lab = torch.randint(0, c, (rows,), generator=g, device=device)
+                v = centres[lab] + 0.3 * torch.randn(rows, d, generator=g, device=device)
+                v = v / v.norm(dim=1, keepdim=True)
+                f = torch.empty((rows, d), dtype=torch.float32, pin_memory=True)
+                f.copy_(v)
+                q = torch.empty((rows, d), dtype=torch.int8, pin_memory=True)
+                q.copy_(torch.clamp(torch.round(127.0 * v), -127, 127).to(torch.int8))
+                self.pool[(int(d), m, False)] = f.numpy()
+                self.pool[(int(d), m, True)] = q.numpy()
+                del v, centres, lab
+
+    def rows_for(self, request_id: int, n: int, dim: int, i8: bool) -> np.ndarray:
+        m = request_id % self.mixtures
+        off = np.random.RandomState(request_id).randint(0, self.rows - n + 1)
+        return self.pool[(int(dim), m, bool(i8))][off:off + n]

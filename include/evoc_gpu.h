@@ -178,6 +178,102 @@ int evoc_gpu_last_launch_count(const evoc_gpu_ctx* ctx);
 int evoc_gpu_knn_f32_noalloc(const float* rows, int64_t n, int64_t ld, int32_t k, int32_t* out_idx, float* out_dist,
                              void* stream, int32_t* out_k, char* errbuf, int32_t errlen);
 
+/*
+ * Serving: a kNN-graph server with continuous batching.  No counterpart in
+ * evoc-rs, whose Evoc::fit_predict builds one data set's graph at a time
+ * (src/clustering.rs:650-716); the Rust request loop calls these.
+ *
+ * Requests of any n, dim and dtype are queued by evoc_gpu_server_submit and
+ * run by `max_inflight` lanes, each with its own context (stream and
+ * scratch), so several requests are on the device at once.  A lane admits the
+ * oldest pending request that fits the budget: n*dim*size(dtype) for the rows
+ * + n*k_eff*8 for the graph + what the lane's buffers must grow by for that
+ * shape (lane buffers are kept between requests and counted once; an idle lane
+ * frees them when they alone keep the oldest request out).  A request passed
+ * over 16 times by later ones is admitted next.  The rows go back to the
+ * budget once the graph is built; the graph stays resident in HBM until it is
+ * fetched without keep_resident or released.  Every job id must end in
+ * evoc_gpu_server_result (without keep_resident) or evoc_gpu_server_release.
+ */
+typedef struct evoc_gpu_server evoc_gpu_server;
+
+typedef struct {
+  uint32_t struct_size;  /* sizeof(evoc_gpu_server_opts)                    */
+  int32_t device;        /* CUDA device                                     */
+  int64_t budget_bytes;  /* HBM admission budget; default 150e9             */
+  int32_t max_inflight;  /* lanes (requests on the device at once), 1..64;  */
+                         /* default 4                                       */
+  int32_t reserved[5];
+} evoc_gpu_server_opts;
+
+typedef struct {
+  int64_t submitted, completed, failed, cancelled, rejected;
+  int64_t pending, running;
+  int64_t bytes_in_use;    /* counted against the budget now               */
+  int64_t peak_bytes;      /* high-water mark of bytes_in_use              */
+  int64_t budget_bytes;
+  int64_t workspace_bytes; /* lane contexts' buffers, counted in bytes_in_use */
+  int64_t workspace_misses;/* requests whose buffers outgrew the plan       */
+  int64_t lanes;
+} evoc_gpu_server_counters;
+
+typedef struct {
+  int64_t submit_ns, admit_ns, done_ns; /* evoc_gpu_server_now_ns clock; 0 = not yet */
+  int64_t n, dim;
+  int32_t dtype, k_eff, lane, status;   /* status as evoc_gpu_server_poll returns */
+  char error[160];
+} evoc_gpu_job_info;
+
+/* submit flag: the server reads the caller's host rows in place instead of
+ * copying them at submit; the buffer must stay valid and unchanged until the
+ * job has finished. */
+#define EVOC_SUBMIT_BORROW 1
+
+void evoc_gpu_server_default_opts(evoc_gpu_server_opts* opts);
+int evoc_gpu_server_create(const evoc_gpu_server_opts* opts, evoc_gpu_server** out);
+/* Cancels pending jobs, waits for running ones and frees everything. */
+void evoc_gpu_server_destroy(evoc_gpu_server* server);
+/* Monotonic clock of the job times (CLOCK_MONOTONIC on Linux), in ns. */
+int64_t evoc_gpu_server_now_ns(void);
+
+/* Queues one request; arguments as evoc_gpu_knn_graph.  opts may be NULL
+ * (defaults); opts->buffers_on_device = 1 means `data` is a device pointer
+ * that stays valid until the job has finished (outputs always stay on the
+ * device until fetched); row_begin/row_end must be 0.  EVOC_ERR_OOM when the
+ * request cannot fit the budget even alone.  *job_id > 0 on success. */
+int evoc_gpu_server_submit(evoc_gpu_server* server, const evoc_gpu_opts* opts, int32_t dtype, const void* data,
+                           int64_t n, int64_t dim, int32_t k, const int64_t* rng_state, int32_t flags,
+                           int64_t* job_id);
+/* Bytes a request is admitted against: *resident = rows (unless on the
+ * device) + graph; *workspace = lane buffers it needs on a lane that holds
+ * none.  A request fits an otherwise empty server when their sum is at most
+ * the budget. */
+int evoc_gpu_server_request_bytes(evoc_gpu_server* server, const evoc_gpu_opts* opts, int32_t dtype, int64_t n,
+                                  int64_t dim, int32_t k, int64_t* resident, int64_t* workspace);
+/* EVOC_ERR_PENDING while queued or running, else the job's final status. */
+int evoc_gpu_server_poll(evoc_gpu_server* server, int64_t job_id);
+/* Waits until the job has finished (timeout_ms < 0: no limit); returns its
+ * status or EVOC_ERR_TIMEOUT. */
+int evoc_gpu_server_wait(evoc_gpu_server* server, int64_t job_id, int64_t timeout_ms);
+/* Waits for the next job to finish that no wait_any or result call has
+ * reported yet, in completion order; returns its status, *job_id its id. */
+int evoc_gpu_server_wait_any(evoc_gpu_server* server, int64_t timeout_ms, int64_t* job_id);
+/* Waits for the job and copies its graph (n x k_eff, as evoc_gpu_knn_graph)
+ * into host buffers (either may be NULL).  Unless keep_resident, the job is
+ * then released (also when it failed or was cancelled). */
+int evoc_gpu_server_result(evoc_gpu_server* server, int64_t job_id, int32_t* out_idx, float* out_dist,
+                           int32_t* out_k, int32_t keep_resident);
+/* Device pointers of a finished job's graph, valid until it is released. */
+int evoc_gpu_server_result_device(evoc_gpu_server* server, int64_t job_id, const int32_t** d_idx,
+                                  const float** d_dist, int32_t* out_k);
+/* Frees the job (cancelling it first if it has not finished). */
+int evoc_gpu_server_release(evoc_gpu_server* server, int64_t job_id);
+/* A pending job is dropped; a running job's graph is discarded when its lane
+ * finishes.  Its status becomes EVOC_ERR_CANCELLED. */
+int evoc_gpu_server_cancel(evoc_gpu_server* server, int64_t job_id);
+int evoc_gpu_server_job_info(evoc_gpu_server* server, int64_t job_id, evoc_gpu_job_info* info);
+int evoc_gpu_server_stats(evoc_gpu_server* server, evoc_gpu_server_counters* stats);
+
 #ifdef __cplusplus
 }
 #endif
