@@ -190,9 +190,10 @@ int locality_order(evoc_gpu_ctx* ctx, const Job& j, const void* rows, int64_t ro
            "gather pivots");
   const int grid = scan_grid(ctx, j.nq);
   EVOC_TRY(ctx->labels.ensure(size_t(j.nq) * 4), "alloc labels");
-  EVOC_TRY(evoc::launch_tc_scan(int8, rows, evoc::padded_rows(j.n), j.r0, j.nq, ctx->pivots.p, piv_rows, n_piv,
+  EVOC_TRY(evoc::launch_tc_scan(int8 ? evoc::kScanInt8 : evoc::kScanBf16, rows, evoc::padded_rows(j.n), j.r0, j.nq,
+                                ctx->pivots.p, piv_rows, n_piv,
                                 row_bytes, 1, nullptr, grid, 0, 0, 0, ctx->labels.as<int32_t>(), nullptr, nullptr,
-                                j.status, ctx->timeout_ns, ctx->stream),
+                                j.status, ctx->timeout_ns, nullptr, ctx->stream),
            "pivot scan");
   EVOC_TRY(ctx->order.ensure(size_t(j.nq) * 4), "alloc order");
   EVOC_TRY(ctx->hist.ensure(size_t(n_piv) * 4), "alloc hist");
@@ -230,9 +231,9 @@ int run_bf16_rerank(evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, const Job& j, 
   {
     Stage st(ctx, "bf16_scan");
     EVOC_TRY(ctx->scratch.ensure(size_t(grid) * 256 * size_t(C) * 8), "alloc scratch");
-    EVOC_TRY(evoc::launch_tc_scan(false, ctx->xb.p, rows, j.r0, j.nq, ctx->xb.p, rows, j.n, ldb * 2, int(C),
+    EVOC_TRY(evoc::launch_tc_scan(evoc::kScanBf16, ctx->xb.p, rows, j.r0, j.nq, ctx->xb.p, rows, j.n, ldb * 2, int(C),
                                   ctx->scratch.as<uint64_t>(), grid, 1, 0, 0, ctx->cand.as<int32_t>(), nullptr,
-                                  nullptr, j.status, ctx->timeout_ns, ctx->stream),
+                                  nullptr, j.status, ctx->timeout_ns, nullptr, ctx->stream),
              "bf16 scan");
     ctx->launches += 1;
   }
@@ -255,10 +256,39 @@ int run_int8(evoc_gpu_ctx* ctx, const Job& j, int64_t ldb) {
   const int grid = scan_grid(ctx, j.nq);
   const int64_t rows = evoc::padded_rows(j.n);
   EVOC_TRY(ctx->scratch.ensure(size_t(grid) * 256 * size_t(j.keff) * 8), "alloc scratch");
-  EVOC_TRY(evoc::launch_tc_scan(true, ctx->x.p, rows, j.r0, j.nq, ctx->x.p, rows, j.n, ldb, j.keff,
+  EVOC_TRY(evoc::launch_tc_scan(evoc::kScanInt8, ctx->x.p, rows, j.r0, j.nq, ctx->x.p, rows, j.n, ldb, j.keff,
                                 ctx->scratch.as<uint64_t>(), grid, 1, 1, EVOC_DTYPE_I8, j.idx, j.raw, j.dist, j.status,
-                                ctx->timeout_ns, ctx->stream),
+                                ctx->timeout_ns, nullptr, ctx->stream),
            "int8 scan");
+  ctx->launches += 1;
+  return EVOC_OK;
+}
+
+// Bytes per row of the 0/1 int8 expansion of `nbytes` packed bytes.
+int64_t expanded_row_bytes(int64_t nbytes) { return round_up(nbytes * 8, 128); }
+
+// Binary rows on the tensor cores: popcounts and the 0/1 expansion, then the
+// int8 scan in Jaccard mode.  ldb: bytes between staged packed rows.
+int run_jaccard_tc(evoc_gpu_ctx* ctx, const Job& j, int64_t ldb, int64_t nbytes) {
+  const int64_t rows = evoc::padded_rows(j.n);
+  const int64_t lde = expanded_row_bytes(nbytes);
+  {
+    Stage st(ctx, "expand_bits");
+    EVOC_TRY(ctx->popc.ensure(size_t(j.n) * 4), "alloc popcounts");
+    EVOC_TRY(evoc::launch_popcount_rows(ctx->x.p, j.n, int(ldb / 4), ctx->popc.as<int32_t>(), ctx->sms, ctx->stream),
+             "popcounts");
+    EVOC_TRY(ctx->xb.ensure(size_t(rows * lde)), "alloc expanded rows");
+    EVOC_TRY(evoc::launch_expand_bits(ctx->x.p, j.n, ldb, nbytes, ctx->xb.p, rows, lde, ctx->sms, ctx->stream),
+             "expand bits");
+    ctx->launches += 2;
+  }
+  Stage st(ctx, "jaccard_scan");
+  const int grid = scan_grid(ctx, j.nq);
+  EVOC_TRY(ctx->scratch.ensure(size_t(grid) * 256 * size_t(j.keff) * 8), "alloc scratch");
+  EVOC_TRY(evoc::launch_tc_scan(evoc::kScanJaccard, ctx->xb.p, rows, j.r0, j.nq, ctx->xb.p, rows, j.n, lde, j.keff,
+                                ctx->scratch.as<uint64_t>(), grid, 1, 1, EVOC_DTYPE_U8, j.idx, j.raw, j.dist, j.status,
+                                ctx->timeout_ns, ctx->popc.as<int32_t>(), ctx->stream),
+           "jaccard scan");
   ctx->launches += 1;
   return EVOC_OK;
 }
@@ -618,12 +648,13 @@ int knn_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtype, con
     if (form == EVOC_FORM_EXACT_INT) rc = run_int8(ctx, job, ldb);
     else rc = run_nndescent(ctx, opts, job, EVOC_DTYPE_I8, ldb, ctx->x.p, 0, int(dim), rng_state, ctx->x.p, ldb);
   } else {
-    if (form != EVOC_FORM_EXACT_INT && form != EVOC_FORM_NNDESCENT)
+    if (form != EVOC_FORM_EXACT_INT && form != EVOC_FORM_POPCOUNT && form != EVOC_FORM_NNDESCENT)
       return fail(ctx, EVOC_ERR_UNSUPPORTED, "form not built for u8 in this library");
     const int64_t ldb = round_up(dim, 64);
     rc = stage_rows(ctx, data, n, dim, ldb, on_dev);
     if (rc) return rc;
-    if (form == EVOC_FORM_EXACT_INT) rc = run_jaccard(ctx, job, ldb);
+    if (form == EVOC_FORM_EXACT_INT) rc = run_jaccard_tc(ctx, job, ldb, dim);
+    else if (form == EVOC_FORM_POPCOUNT) rc = run_jaccard(ctx, job, ldb);
     else rc = run_nndescent(ctx, opts, job, EVOC_DTYPE_U8, ldb, ctx->x.p, 0, int(dim), rng_state, nullptr, 0);
   }
   if (rc) return rc;
@@ -817,6 +848,10 @@ void knn_buffer_needs(const evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, int32_
   } else {
     b[kBufX] = size_t(rows * round_up(dim, 64));
     if (form == EVOC_FORM_EXACT_INT) {
+      b[kBufPopc] = size_t(n) * 4;
+      b[kBufXb] = size_t(rows * expanded_row_bytes(dim));
+      b[kBufScratch] = size_t(grid) * 256 * size_t(keff) * 8;
+    } else if (form == EVOC_FORM_POPCOUNT) {
       b[kBufPopc] = size_t(n) * 4;
     } else if (form == EVOC_FORM_NNDESCENT) {
       b[kBufPopc] = size_t(n) * 4;

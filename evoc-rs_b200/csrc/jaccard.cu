@@ -178,6 +178,39 @@ knn_jaccard_kernel(const uint32_t* __restrict__ X, const int32_t* __restrict__ p
   }
 }
 
+// One thread per 16 output bytes (two input bytes): each input bit becomes a
+// 0/1 byte, most significant bit first (the order np.packbits uses; any fixed
+// order gives the same intersection counts).
+__global__ void expand_bits_kernel(const uint8_t* __restrict__ X, int64_t n, int64_t ld_in, int64_t nbytes,
+                                   uint8_t* __restrict__ Y, int64_t rows, int64_t ld_out) {
+  const int64_t per_row = ld_out / 16;
+  const int64_t total = rows * per_row;
+  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t r = e / per_row, c = e % per_row;  // c-th 16-byte group = input bytes 2c, 2c+1
+    uint32_t w[4] = {0u, 0u, 0u, 0u};
+    if (r < n) {
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int64_t b = 2 * c + h;
+        const uint32_t v = b < nbytes ? X[r * ld_in + b] : 0u;
+        // bits 7..4 -> bytes 0..3 of word 2h, bits 3..0 -> bytes 0..3 of word 2h+1
+        w[2 * h] = ((v >> 7) & 1u) | (((v >> 6) & 1u) << 8) | (((v >> 5) & 1u) << 16) | (((v >> 4) & 1u) << 24);
+        w[2 * h + 1] = ((v >> 3) & 1u) | (((v >> 2) & 1u) << 8) | (((v >> 1) & 1u) << 16) | ((v & 1u) << 24);
+      }
+    }
+    *reinterpret_cast<uint4*>(Y + r * ld_out + c * 16) = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+}
+
+cudaError_t launch_expand_bits(const void* X, int64_t n, int64_t ld_in, int64_t nbytes, void* Y, int64_t rows,
+                               int64_t ld_out, int sms, cudaStream_t stream) {
+  if (ld_out % 16 != 0 || ld_out < 8 * nbytes || rows < n || (reinterpret_cast<uintptr_t>(Y) & 15))
+    return cudaErrorInvalidValue;
+  expand_bits_kernel<<<sms * 8, 256, 0, stream>>>(static_cast<const uint8_t*>(X), n, ld_in, nbytes,
+                                                   static_cast<uint8_t*>(Y), rows, ld_out);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_popcount_rows(const void* X, int64_t n, int ldw, int32_t* pc, int sms, cudaStream_t stream) {
   popcount_rows_kernel<<<sms * 4, 256, 0, stream>>>(static_cast<const uint32_t*>(X), n, ldw, pc);
   return cudaGetLastError();

@@ -39,11 +39,14 @@ cudaError_t launch_to_bf16(const float* X, int64_t n, int ld, int d, void* Y, in
 //   `row_bytes` per row (multiple of 128, 16-byte aligned bases); q_rows and k_rows are multiples
 //   of 256 and rows past the data are zero.  Query i is written to output row i.
 //   final_mode 1: out rows of `keep` sorted (idx, raw, transformed dist); 0: candidates (idx, raw).
+//   mode 0: BF16 rows, cosine; 1: int8 rows, -(dot); 2: 0/1 int8 rows (expanded bits), Jaccard from
+//   the intersection counts and the row popcounts `pc` (self_mode, Q == K).
 size_t tc_scan_smem_bytes();
-cudaError_t launch_tc_scan(bool int8, const void* Q, int64_t q_rows, int64_t q_row0, int64_t n_q, const void* K,
+enum ScanMode { kScanBf16 = 0, kScanInt8 = 1, kScanJaccard = 2 };
+cudaError_t launch_tc_scan(int mode, const void* Q, int64_t q_rows, int64_t q_row0, int64_t n_q, const void* K,
                            int64_t k_rows, int64_t n_k, int64_t row_bytes, int keep, uint64_t* scratch, int grid,
                            int self_mode, int final_mode, int dtype, int32_t* out_idx, float* out_raw, float* out_dist,
-                           int* status, uint64_t timeout_ns, cudaStream_t stream);
+                           int* status, uint64_t timeout_ns, const int32_t* pc, cudaStream_t stream);
 
 // rerank.cu
 cudaError_t launch_rerank_f32(const float* X, int ld, int d, int64_t n_q, int64_t n_keys, int64_t q_row0,
@@ -93,6 +96,10 @@ namespace evoc {
 cudaError_t launch_scan_counts(const int32_t* cnt, int64_t n, int64_t* out, cudaStream_t stream);
 // jaccard.cu: per-row popcounts of rows of ldw 32-bit words.
 cudaError_t launch_popcount_rows(const void* X, int64_t n, int ldw, int32_t* pc, int sms, cudaStream_t stream);
+// jaccard.cu: packed bit rows (ld_in bytes apart, nbytes used) -> 0/1 int8 rows of ld_out bytes
+// (ld_out >= 8 * nbytes, multiple of 16) for `rows` rows; rows past n and columns past 8*nbytes are 0.
+cudaError_t launch_expand_bits(const void* X, int64_t n, int64_t ld_in, int64_t nbytes, void* Y, int64_t rows,
+                               int64_t ld_out, int sms, cudaStream_t stream);
 
 // nndescent.cu: GPU NN-descent.
 struct NndArgs {

@@ -14,6 +14,13 @@
 //   warp 1      TMEM allocator + MMA issuer (one elected lane)
 //   warps 2..5  epilogue; warp w reads TMEM lanes 32*(w%4) .. +31
 //
+// Three score modes share the kernel: BF16 dot products (cosine), int8 dot
+// products, and binary Jaccard, where the packed bits are expanded to 0/1
+// int8 rows so that the intersection popcount is an exact s8 x s8 -> s32
+// contraction; the epilogue then forms -(inter / union) with union =
+// |a| + |b| - inter from per-row popcounts, as the reference does
+// (src/nndescent/uint8.rs:21-35).
+//
 // Replaces the distance evaluations of the reference's NN-descent local join
 // (src/nndescent/float.rs:552-660 with fast_cosine, src/fast_cosine.rs:33-45;
 // src/nndescent/int8.rs:15-21 for the int8 dissimilarity).
@@ -59,24 +66,40 @@ struct ScanParams {
   float* out_dist;
   int* status;       // 0 ok; set non-zero by the first role that gives up
   uint64_t timeout_ns;
+  const int32_t* pc; // Jaccard mode: popcount of every row (queries and keys)
 };
 
 namespace {
 
 __device__ __forceinline__ void set_status(int* status, int code) { atomicCAS(status, 0, code); }
 
+constexpr int kModeBf16 = 0;     // BF16 dot products, cosine dissimilarity
+constexpr int kModeInt8 = 1;     // int8 dot products, -(dot as f32)
+constexpr int kModeJaccard = 2;  // 0/1 int8 rows: intersection counts, -(inter / union)
+
 // Quick-reject threshold as the raw 32-bit score pattern the accumulator holds:
 // a score below it cannot enter the heap.  For int8 it is an s32 lower bound
 // (exact while |dot| < 2^24, loosened by 256 beyond, where f32 rounds); for
-// BF16 it is an f32.  Passing scores are re-checked exactly by the key compare.
-__device__ __forceinline__ uint32_t pass_threshold(const KeyHeap& heap, bool int_scores) {
+// BF16 it is an f32.  For Jaccard it is a lower bound on the intersection:
+// J = inter / (pa + pb - inter) <= inter / pa, so a key reaching the heap's
+// similarity t needs inter >= t * pa (taken 1e-6 looser so f32 rounding of J
+// never rejects a key the exact compare would admit).  Passing scores are
+// re-checked exactly by the key compare.
+template <int MODE>
+__device__ __forceinline__ uint32_t pass_threshold(const KeyHeap& heap, int32_t pa) {
   const uint64_t t = heap.threshold();
-  if (int_scores) {
+  if (MODE == kModeInt8) {
     if (t == kKeyInf) return uint32_t(INT32_MIN);
     const float ts = -from_orderable(uint32_t(t >> 32));  // raw = -score
     int32_t ti = int32_t(ts);
     if (!(fabsf(ts) < 16777216.0f)) ti -= 256;
     return uint32_t(ti);
+  }
+  if (MODE == kModeJaccard) {
+    if (t == kKeyInf) return uint32_t(INT32_MIN);
+    const float sim = -from_orderable(uint32_t(t >> 32));  // raw = -J (or +0.0 for J = 0)
+    if (!(sim > 0.0f)) return uint32_t(INT32_MIN);
+    return uint32_t(int32_t(floorf(sim * float(pa) * (1.0f - 1e-6f))));
   }
   const uint32_t NEG_INF = 0xff800000u;
   if (t == kKeyInf) return NEG_INF;
@@ -84,37 +107,49 @@ __device__ __forceinline__ uint32_t pass_threshold(const KeyHeap& heap, bool int
   return raw < 0.0f ? __float_as_uint(-raw) : NEG_INF;  // raw = -score, or MIN_POSITIVE for scores <= 0
 }
 
-template <bool kInt8>
+template <int MODE>
 __device__ __forceinline__ bool passes(uint32_t v, uint32_t thr) {
-  return kInt8 ? (int32_t(v) >= int32_t(thr)) : (__uint_as_float(v) >= __uint_as_float(thr));
+  return MODE != kModeBf16 ? (int32_t(v) >= int32_t(thr)) : (__uint_as_float(v) >= __uint_as_float(thr));
+}
+
+// Jaccard dissimilarity from exact counts, as the reference computes it.
+__device__ __forceinline__ float jaccard_raw_counts(int32_t inter, int32_t uni) {
+  return uni > 0 ? -__fdiv_rn(__int2float_rn(inter), __int2float_rn(uni)) : 0.0f;
 }
 
 // Offers the scores of one 32-column chunk that beat the threshold.  The
 // chunk's values stay in registers; a survivor's value is picked by an
 // unrolled select (survivors are rare once the heap is full).
-template <bool kInt8>
+template <int MODE>
 __device__ __forceinline__ void offer_chunk(const uint32_t (&v)[32], uint32_t mask, int64_t col0, int64_t n_k,
-                                            bool self_mode, int64_t q, KeyHeap& heap, uint32_t& thr) {
+                                            bool self_mode, int64_t q, KeyHeap& heap, uint32_t& thr, int32_t pa,
+                                            const int32_t* __restrict__ pc) {
   while (mask) {
     const int j = __ffs(mask) - 1;
     mask &= mask - 1;
     uint32_t bits = 0;
 #pragma unroll
     for (int jj = 0; jj < 32; jj++) bits = (jj == j) ? v[jj] : bits;
-    if (!passes<kInt8>(bits, thr)) continue;  // threshold may have moved
+    if (!passes<MODE>(bits, thr)) continue;  // threshold may have moved
     const int64_t key = col0 + j;
     if (key >= n_k || (self_mode && key == q)) continue;
-    const float raw = kInt8 ? -__int2float_rn(int32_t(bits)) : raw_cosine(__uint_as_float(bits));
+    float raw;
+    if (MODE == kModeJaccard) {
+      const int32_t inter = int32_t(bits);
+      raw = jaccard_raw_counts(inter, pa + pc[key] - inter);
+    } else {
+      raw = MODE == kModeInt8 ? -__int2float_rn(int32_t(bits)) : raw_cosine(__uint_as_float(bits));
+    }
     heap.offer(make_key(raw, int32_t(key)));
-    thr = pass_threshold(heap, kInt8);
+    thr = pass_threshold<MODE>(heap, pa);
   }
 }
 
-template <bool kInt8>
+template <int MODE>
 __device__ __forceinline__ uint32_t chunk_mask(const uint32_t (&v)[32], uint32_t thr) {
   uint32_t m = 0;
 #pragma unroll
-  for (int j = 0; j < 32; j++) m |= (passes<kInt8>(v[j], thr) ? 1u : 0u) << j;
+  for (int j = 0; j < 32; j++) m |= (passes<MODE>(v[j], thr) ? 1u : 0u) << j;
   return m;
 }
 
@@ -124,7 +159,7 @@ __device__ __forceinline__ void epilogue_sync(int nthreads) {
 
 }  // namespace
 
-template <bool kInt8, int STAGES, int GROUPS, bool kSmemHeap>
+template <int MODE, int STAGES, int GROUPS, bool kSmemHeap>
 __global__ void __launch_bounds__(64 + GROUPS * 128, 1)
 tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const ScanParams p) {
   using namespace sm100;
@@ -167,6 +202,7 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
 
+  constexpr bool kInt8 = MODE != kModeBf16;
   const int64_t n_qblocks = (p.n_q + BM - 1) / BM;
   const int64_t n_ktiles = (p.n_k + BN - 1) / BN;
   const volatile int* abort = p.status;
@@ -262,7 +298,8 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
       KeyHeap heap;
       heap.init(hstore, p.keep);
       if (valid && p.self_mode && group == 0) heap.offer(make_key(-1.0f, int32_t(qg)));
-      uint32_t thr = pass_threshold(heap, kInt8);
+      const int32_t pa = (MODE == kModeJaccard && valid) ? p.pc[qg] : 0;
+      uint32_t thr = pass_threshold<MODE>(heap, pa);
       for (int64_t kt = 0; kt < n_ktiles; kt++, tile++) {
         const uint32_t a = tile & 1u, tph = (tile >> 1) & 1u;
         int got = 1;
@@ -282,12 +319,12 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         for (int c = 0; c < NCH; c += 2) {
           tmem_ld_wait();
           tmem_ld_32x32b_x32(tbase + (c + 1) * 32, vb);
-          uint32_t m = chunk_mask<kInt8>(va, thr);
-          if (valid && m) offer_chunk<kInt8>(va, m, k0 + c * 32, p.n_k, p.self_mode, qg, heap, thr);
+          uint32_t m = chunk_mask<MODE>(va, thr);
+          if (valid && m) offer_chunk<MODE>(va, m, k0 + c * 32, p.n_k, p.self_mode, qg, heap, thr, pa, p.pc);
           tmem_ld_wait();
           if (c + 2 < NCH) tmem_ld_32x32b_x32(tbase + (c + 2) * 32, va);
-          m = chunk_mask<kInt8>(vb, thr);
-          if (valid && m) offer_chunk<kInt8>(vb, m, k0 + (c + 1) * 32, p.n_k, p.self_mode, qg, heap, thr);
+          m = chunk_mask<MODE>(vb, thr);
+          if (valid && m) offer_chunk<MODE>(vb, m, k0 + (c + 1) * 32, p.n_k, p.self_mode, qg, heap, thr, pa, p.pc);
         }
         tc_fence_before();
         mbar_arrive(&tempty[a]);
@@ -319,8 +356,11 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
           int32_t idx = -1;
           if (j < got) {
             raw = from_orderable(uint32_t(heap.h[j] >> 32));
-            if (kInt8) raw = int8_raw_from_key(raw);
             idx = key_index(heap.h[j]);
+            // Keys fold -0.0 onto +0.0; restore the reference's sign: an int8
+            // zero dot is -0.0; a Jaccard zero is +0.0 only for two empty rows.
+            if (MODE == kModeInt8) raw = int8_raw_from_key(raw);
+            if (MODE == kModeJaccard && raw == 0.0f) raw = (pa + p.pc[idx] == 0) ? 0.0f : -0.0f;
           }
           p.out_idx[orow + j] = idx;
           if (p.out_raw) p.out_raw[orow + j] = raw;
@@ -378,10 +418,10 @@ bool make_map(CUtensorMap* m, const void* base, int64_t rows, int64_t row_bytes,
 size_t tc_scan_smem_bytes() { return smem_bytes(4, 1, 0); }
 
 namespace {
-template <bool kInt8, int STAGES, int GROUPS, bool kSmemHeap>
+template <int MODE, int STAGES, int GROUPS, bool kSmemHeap>
 cudaError_t launch_variant(const CUtensorMap& ma, const CUtensorMap& mb, const ScanParams& p, int grid, size_t smem,
                            cudaStream_t stream) {
-  auto kern = tc_scan_kernel<kInt8, STAGES, GROUPS, kSmemHeap>;
+  auto kern = tc_scan_kernel<MODE, STAGES, GROUPS, kSmemHeap>;
   // The opt-in limit, not `smem`: the launch's shared memory varies with keep,
   // and concurrent callers (serving lanes) must not lower each other's limit
   // between this call and their launch.
@@ -391,37 +431,40 @@ cudaError_t launch_variant(const CUtensorMap& ma, const CUtensorMap& mb, const S
   return cudaGetLastError();
 }
 
-template <bool kInt8>
-cudaError_t launch_dtype(const CUtensorMap& ma, const CUtensorMap& mb, ScanParams p, int grid, cudaStream_t stream) {
+template <int MODE>
+cudaError_t launch_mode(const CUtensorMap& ma, const CUtensorMap& mb, ScanParams p, int grid, cudaStream_t stream) {
   const int odd = p.keep | 1;
   p.heap_stride = odd;
   // Prefer two epilogue groups (more warps to hide TMEM/issue latency), then
   // the deeper pipeline; heaps fall back to global memory for very large keep.
   if (smem_bytes(4, 2, odd) <= SMEM_LIMIT)
-    return launch_variant<kInt8, 4, 2, true>(ma, mb, p, grid, smem_bytes(4, 2, odd), stream);
+    return launch_variant<MODE, 4, 2, true>(ma, mb, p, grid, smem_bytes(4, 2, odd), stream);
   if (smem_bytes(3, 2, odd) <= SMEM_LIMIT)
-    return launch_variant<kInt8, 3, 2, true>(ma, mb, p, grid, smem_bytes(3, 2, odd), stream);
+    return launch_variant<MODE, 3, 2, true>(ma, mb, p, grid, smem_bytes(3, 2, odd), stream);
   if (smem_bytes(4, 1, odd) <= SMEM_LIMIT)
-    return launch_variant<kInt8, 4, 1, true>(ma, mb, p, grid, smem_bytes(4, 1, odd), stream);
+    return launch_variant<MODE, 4, 1, true>(ma, mb, p, grid, smem_bytes(4, 1, odd), stream);
   if (smem_bytes(3, 1, odd) <= SMEM_LIMIT)
-    return launch_variant<kInt8, 3, 1, true>(ma, mb, p, grid, smem_bytes(3, 1, odd), stream);
+    return launch_variant<MODE, 3, 1, true>(ma, mb, p, grid, smem_bytes(3, 1, odd), stream);
   if (!p.scratch) return cudaErrorInvalidValue;
   p.heap_stride = p.keep;
-  return launch_variant<kInt8, 4, 1, false>(ma, mb, p, grid, smem_bytes(4, 1, 0), stream);
+  return launch_variant<MODE, 4, 1, false>(ma, mb, p, grid, smem_bytes(4, 1, 0), stream);
 }
 }  // namespace
 
-cudaError_t launch_tc_scan(bool int8, const void* Q, int64_t q_rows, int64_t q_row0, int64_t n_q, const void* K,
+cudaError_t launch_tc_scan(int mode, const void* Q, int64_t q_rows, int64_t q_row0, int64_t n_q, const void* K,
                            int64_t k_rows, int64_t n_k, int64_t row_bytes, int keep, uint64_t* scratch, int grid,
                            int self_mode, int final_mode, int dtype, int32_t* out_idx, float* out_raw, float* out_dist,
-                           int* status, uint64_t timeout_ns, cudaStream_t stream) {
+                           int* status, uint64_t timeout_ns, const int32_t* pc, cudaStream_t stream) {
   // q_rows / k_rows: rows present in memory (multiples of the box heights);
   // n_q / n_k: rows that take part.  Rows past n are zero and never offered.
   if (row_bytes % KCB != 0 || n_q <= 0 || n_k <= 0 || keep < 1) return cudaErrorInvalidValue;
   if (q_row0 < 0 || q_rows < q_row0 + n_q || k_rows < n_k || q_rows % BN != 0 || k_rows % BN != 0)
     return cudaErrorInvalidValue;
   if ((reinterpret_cast<uintptr_t>(Q) & 15) || (reinterpret_cast<uintptr_t>(K) & 15)) return cudaErrorInvalidValue;
-  const int eb = int8 ? 1 : 2;
+  if (mode < kModeBf16 || mode > kModeJaccard) return cudaErrorInvalidValue;
+  // Jaccard reads one popcount per query row and key row: queries are keys.
+  if (mode == kModeJaccard && (!pc || !self_mode || Q != K)) return cudaErrorInvalidValue;
+  const int eb = mode == kModeBf16 ? 2 : 1;
   alignas(64) CUtensorMap ma, mb;
   if (!make_map(&ma, Q, q_rows, row_bytes, eb, BM) || !make_map(&mb, K, k_rows, row_bytes, eb, BN))
     return cudaErrorInvalidValue;
@@ -440,7 +483,10 @@ cudaError_t launch_tc_scan(bool int8, const void* Q, int64_t q_rows, int64_t q_r
   p.out_dist = out_dist;
   p.status = status;
   p.timeout_ns = timeout_ns;
-  return int8 ? launch_dtype<true>(ma, mb, p, grid, stream) : launch_dtype<false>(ma, mb, p, grid, stream);
+  p.pc = pc;
+  if (mode == kModeInt8) return launch_mode<kModeInt8>(ma, mb, p, grid, stream);
+  if (mode == kModeJaccard) return launch_mode<kModeJaccard>(ma, mb, p, grid, stream);
+  return launch_mode<kModeBf16>(ma, mb, p, grid, stream);
 }
 
 }  // namespace evoc

@@ -26,9 +26,9 @@ EVOC_ERR_CANCELLED = 8
 EVOC_ERR_PENDING = 9
 
 DTYPE_F32, DTYPE_I8, DTYPE_U8 = 0, 1, 2
-FORM_AUTO, FORM_FP32, FORM_BF16_RERANK, FORM_EXACT_INT, FORM_NNDESCENT = 0, 1, 2, 3, 4
+FORM_AUTO, FORM_FP32, FORM_BF16_RERANK, FORM_EXACT_INT, FORM_NNDESCENT, FORM_POPCOUNT = 0, 1, 2, 3, 4, 5
 FORM_NAMES = {"auto": FORM_AUTO, "fp32": FORM_FP32, "bf16_rerank": FORM_BF16_RERANK,
-              "exact_int": FORM_EXACT_INT, "nndescent": FORM_NNDESCENT}
+              "exact_int": FORM_EXACT_INT, "nndescent": FORM_NNDESCENT, "popcount": FORM_POPCOUNT}
 
 
 class Opts(C.Structure):

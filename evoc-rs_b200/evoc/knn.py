@@ -113,7 +113,7 @@ class KnnGraphOptions:
     brute_force_max_n: int = 0
     deterministic: bool = False
     # GPU-only fields
-    form: str = "auto"          # auto | fp32 | bf16_rerank | exact_int | nndescent
+    form: str = "auto"          # auto | fp32 | bf16_rerank | exact_int | nndescent | popcount
     oversample: int = 2         # bf16_rerank: candidates per row = oversample * k
     device: int = 0
     row_begin: int = 0          # exact forms: query rows [row_begin, row_end) only; 0,0 = all

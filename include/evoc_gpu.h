@@ -50,8 +50,10 @@ typedef enum {
   EVOC_FORM_BF16_RERANK = 2, /* f32: tcgen05 BF16 scan keeps oversample*k         */
                              /* candidates per row, reranked in FP32 (FP64 at the */
                              /* k-th boundary)                                    */
-  EVOC_FORM_EXACT_INT = 3,   /* i8: tcgen05 int8 dots; u8: popcount Jaccard       */
-  EVOC_FORM_NNDESCENT = 4    /* GPU NN-descent (approximate, all dtypes)          */
+  EVOC_FORM_EXACT_INT = 3,   /* i8: tcgen05 int8 dots; u8: tcgen05 int8 on bits  */
+                             /* expanded to 0/1 bytes (exact intersection counts) */
+  EVOC_FORM_NNDESCENT = 4,   /* GPU NN-descent (approximate, all dtypes)          */
+  EVOC_FORM_POPCOUNT = 5     /* u8: SIMT AND + popcount over the packed words     */
 } evoc_form;
 
 /* Options.  evoc_gpu_default_opts() fills the defaults; fields that mirror
