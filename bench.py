@@ -22,7 +22,14 @@ candidates per row, FP32 rerank (FP64 at the k-th boundary).
   cpu_baseline  the reference's NN-descent (restated in oracle/, all host
            threads) on a bounded prefix of the same workload.
 
---impl reference runs only that CPU path, on the same metric and workload.
+  serving  (default run) the continuous-batching server on 10,000 Poisson
+           requests at 200 req/s: edges/s and p50/p95/p99 latency, next to
+           the plain FP32 form run one request at a time.
+
+--workload gmm_i8 (2,000,000 x 384 i8, k=15) and --workload bits
+(4,000,000 x 1,024 bits, k=15) measure the exact integer forms instead, with
+a sampled exactness check and the int8 roofline.
+--impl reference runs only the CPU path, on the same metric and workload.
 """
 from __future__ import annotations
 
@@ -39,8 +46,17 @@ sys.path.insert(0, os.path.join(ROOT, "evoc-rs_b200"))
 sys.path.insert(0, ROOT)
 
 METRIC = "kNN edges/s at recall@k>=0.99 vs FP64 (BF16+FP32-rerank form)"
+METRIC_INT = "kNN edges/s, exact integer arithmetic (bit-exact to the reference's {kind} path)"
 UNIT = "edges/s"
 WORKLOAD = "zipf_1m_768: 1,000,000 x 768 f32, 200 Zipf(1.1) clusters, cosine k=30, seed 7"
+# Workload name -> (rows, dim or bytes per row, k) and its description.
+WORKLOADS = {
+    "zipf_f32": (1_000_000, 768, 30, WORKLOAD),
+    "gmm_i8": (2_000_000, 384, 15, "gmm_i8_2m_384: round(127 x) of L2-normalised 100-cluster GMM (sigma 0.25), "
+                                   "i8, k=15, seed 11"),
+    "bits": (4_000_000, 128, 15, "bits_4m_1024: 500 Bernoulli(0.1) prototypes over 1,024 bits, 5% flips, packed "
+                                 "128 B/row, Jaccard k=15, seed 13"),
+}
 
 # DRAM bytes (read + write) of one launch of the BF16 scan: 5.826e9 B captured
 # with ncu (dram__bytes_read.sum + dram__bytes_write.sum) at n = 262,144, scaled
@@ -129,16 +145,25 @@ def cpu_nndescent_sample(x_host, k, rows, threads, deterministic=False):
     return time.perf_counter() - t0, ind
 
 
+def host_workload(name, rows, dim, seed_offset=0):
+    """A bounded draw of the workload on the host (the CPU arms' sample)."""
+    from evoc import synthetic
+
+    if name == "gmm_i8":
+        return synthetic.gmm_i8(n=rows, dim=dim, seed=11 + seed_offset)
+    if name == "bits":
+        return synthetic.bits_u8(n=rows, nbits=dim * 8, seed=13 + seed_offset)
+    return synthetic.zipf_f32(n=rows, dim=dim, seed=7 + seed_offset)
+
+
 def run_reference(args, world, rank):
     import numpy as np
-
-    from evoc import synthetic
 
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
     rows = args.cpu_rows
-    x = synthetic.zipf_f32(n=rows, dim=args.dim, seed=7)
+    x = host_workload(args.workload, rows, args.dim)
     for _ in range(args.warmup):
         cpu_nndescent_sample(x, args.k, rows, threads)
     times = []
@@ -147,13 +172,19 @@ def run_reference(args, world, rank):
         times.append(t)
     ms = 1000.0 * sum(times) / len(times)
     value = rows * args.k / (ms / 1000.0)
-    sample = (f"NN-descent (RP forest + sorted local join, src/knn.rs / src/nndescent/float.rs restated in "
-              f"oracle/evoc_oracle.c) on a {rows}-row prefix-sized draw of the same distribution, {threads} threads")
+    sample = (f"NN-descent (RP forest + sorted local join, src/knn.rs / src/nndescent/*.rs restated in "
+              f"oracle/evoc_oracle.c) on a {rows}-row draw of the same distribution, {threads} threads")
+    metric, dtype = METRIC, "f32"
+    if args.workload == "gmm_i8":
+        metric, dtype = METRIC_INT.format(kind="Int8"), "int8"
+    elif args.workload == "bits":
+        metric, dtype = METRIC_INT.format(kind="Binary (UInt8)"), "u8"
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
         "data": "synthetic", "impl": "reference",
-        "config": {"workload": WORKLOAD, "n": args.n, "d": args.dim, "k": args.k, "sample_rows": rows},
+        "config": {"workload": WORKLOADS[args.workload][3], "n": args.n, "d": args.dim, "k": args.k,
+                   "sample_rows": rows},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -314,6 +345,208 @@ def run_serving(args, dev):
         out["fp32_one_at_a_time"] = b
         out["edges_per_s_vs_fp32_one_at_a_time"] = out["edges_per_s"] / b["edges_per_s"]
     return out
+
+
+def int8_peak_tops(dev):
+    """int8 GEMM throughput of the library path torch uses (cuBLASLt via torch._int_mm), 8192^3, best of
+    10 with CUDA events: the measured denominator for the int8 roofline (no int8 figure is recorded in
+    MEASURED_PEAKS.json)."""
+    import torch
+
+    try:
+        m = 8192
+        a = torch.randint(-127, 128, (m, m), dtype=torch.int8, device=dev)
+        b = torch.randint(-127, 128, (m, m), dtype=torch.int8, device=dev).t()
+        for _ in range(3):
+            torch._int_mm(a, b)
+        best = float("inf")
+        for _ in range(10):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch._int_mm(a, b)
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        return 2.0 * m ** 3 / (best / 1e3) / 1e12, "measured in this run: torch._int_mm 8192^3 int8, best of 10"
+    except Exception as e:  # noqa: BLE001
+        return 4500.0, f"nominal dense int8 (torch._int_mm unavailable: {type(e).__name__})"
+
+
+def sampled_exact_check(x, oi, oraw, k, kind, rows=128):
+    """Sampled query rows against a brute force on the GPU: FP64 dots for i8 (exact integers), f32 0/1
+    matmul for binary (exact counts, IEEE division for the Jaccard value).  Indices and raw values must
+    match exactly (the k smallest by (raw, index), self raw -1)."""
+    import numpy as np
+    import torch
+
+    n = x.shape[0]
+    q = torch.arange(0, n, max(1, n // rows), device=x.device)[:rows]
+    if kind == "i8":
+        X = x.double()
+        raw = -(X[q] @ X.T)
+        del X
+    else:
+        nb = x.shape[1]
+        bits = torch.stack([(x >> (7 - b)) & 1 for b in range(8)], dim=2).reshape(n, nb * 8).float()
+        inter = bits[q] @ bits.T
+        pc = bits.sum(1)
+        del bits
+        uni = pc[q][:, None] + pc[None, :] - inter
+        raw = torch.where(uni > 0, -(inter / uni), torch.zeros_like(inter)).double()
+    raw[torch.arange(len(q), device=x.device), q] = -1.0
+    vals, idx = torch.topk(raw, k + 64, dim=1, largest=False)
+    vals, idx = vals.cpu().numpy(), idx.cpu().numpy()
+    gi, gr = oi[q].cpu().numpy(), oraw[q].cpu().numpy().astype(np.float64)
+    ok_i = ok_r = True
+    for r in range(len(q)):
+        o = np.lexsort((idx[r], vals[r]))[:k]
+        ok_i &= bool(np.array_equal(gi[r], idx[r][o]))
+        ok_r &= bool(np.array_equal(np.abs(gr[r]), np.abs(vals[r][o])))
+    return {"rows": int(len(q)), "indices_exact": ok_i, "raw_exact": ok_r}
+
+
+def run_exact_int(args, world, rank, local):
+    """C3 / C4: the exact integer forms (int8 dots; binary Jaccard on 0/1-expanded int8 rows)."""
+    import numpy as np
+    import torch
+
+    import evoc
+    from evoc import _lib, synthetic
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+        pg = dist
+    n, d, k = args.n, args.dim, args.k
+    i8 = args.workload == "gmm_i8"
+    if i8:
+        x = synthetic.gmm_i8(n=n, dim=d, seed=11 + rank, device=dev)
+        code, stage, kind = _lib.DTYPE_I8, "int8_scan", "i8"
+        ops_per_pair = 2.0 * d
+    else:
+        x = synthetic.bits_u8(n=n, nbits=d * 8, seed=13 + rank, device=dev)
+        code, stage, kind = _lib.DTYPE_U8, "jaccard_scan", "u8"
+        ops_per_pair = 2.0 * d * 8
+    oi = torch.empty((n, k), dtype=torch.int32, device=dev)
+    od = torch.empty((n, k), dtype=torch.float32, device=dev)
+    oraw = torch.empty((n, k), dtype=torch.float32, device=dev)
+    torch.cuda.synchronize()
+    ctx = _lib.context(local)
+    ctx.profile(True)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=dev)
+    opts = evoc.KnnGraphOptions(n_neighbors=k, form="exact_int", device=local)
+
+    def step():
+        evoc.knn_graph_device(x.data_ptr(), code, n, d, k, oi.data_ptr(), od.data_ptr(), opts,
+                              out_raw_ptr=oraw.data_ptr())
+
+    for _ in range(args.warmup):
+        step()
+    gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
+    clocks = ClockSampler(gpu_id, os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv"))
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stage_ms, launches = {}, 0
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+        for name, ms in ctx.stages():
+            stage_ms.setdefault(name, []).append(ms)
+        launches += ctx.launches()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    clk = clocks.stop()
+    ms_step = ev0.elapsed_time(ev1) / args.steps
+    if pg:
+        t = torch.tensor([ms_step], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms_step = float(t.item())
+    value = world * n * k / (ms_step / 1000.0)
+    check = sampled_exact_check(x, oi, oraw, k, kind, rows=args.check_rows)
+
+    # End to end through the public API with pinned host buffers.
+    xh = torch.empty(x.shape, dtype=x.dtype, pin_memory=True)
+    xh.copy_(x)
+    ih = torch.empty((n, k), dtype=torch.int32, pin_memory=True)
+    dh = torch.empty((n, k), dtype=torch.float32, pin_memory=True)
+    xh_np, ih_np, dh_np = xh.numpy(), ih.numpy(), dh.numpy()
+    if pg:
+        pg.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        evoc.knn_graph(xh_np, opts, None, out=(ih_np, dh_np))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.e2e_steps
+    if pg:
+        t = torch.tensor([e2e_ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_consistent = bool(np.array_equal(ih_np[:1000], oi[:1000].cpu().numpy()))
+
+    peak, peak_kind = int8_peak_tops(dev)
+    scan_ms = statistics.mean(stage_ms[stage])
+    achieved = ops_per_pair * n * n / (scan_ms / 1000.0) / 1e12
+    roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TOPS (int8)", "frac": achieved / peak,
+                "traffic": None, "kernel": f"tc_scan_kernel ({'int8' if i8 else 'Jaccard on 0/1 int8'}, fused top-k)",
+                "peak_kind": peak_kind, "launch_ms": scan_ms,
+                "ops_per_launch": ops_per_pair * n * n}
+
+    cpu = None
+    if rank == 0 and world == 1 and args.cpu_rows > 0:
+        from oracle import oracle as O
+
+        threads = os.cpu_count() or 1
+        rows = min(args.cpu_rows, n)
+        xs = x[:rows].cpu().numpy()
+        O.build()
+        O.set_num_threads(threads)
+        t0 = time.perf_counter()
+        cind, _ = O.knn_graph(xs, k, O.RandomState(7), deterministic=False, n_threads=threads)
+        t = time.perf_counter() - t0
+        qn = min(2000, rows)
+        ei, _ = O.exact_knn(xs, k, 0, qn)
+        crec = float(np.mean([len(set(cind[r]) & set(ei[r])) / k for r in range(qn)]))
+        cpu = {"value": rows * k / t, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": (f"reference NN-descent for {'Int8' if i8 else 'UInt8 (Jaccard)'} restated in oracle/ on the "
+                          f"first {rows} rows, {threads} threads, {t:.1f} s; its recall@{k} vs exact on {qn} of "
+                          f"those rows {crec:.4f} (this form is exact)")}
+
+    metric = METRIC_INT.format(kind="Int8" if i8 else "Binary (UInt8)")
+    line = {
+        "metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int8" if i8 else "u8 (expanded to 0/1 int8)", "data": "synthetic (generated on device, seeded)",
+        "config": {"workload": WORKLOADS[args.workload][3], "n": n, "d": d, "k": k, "form": "exact_int",
+                   "l2": f"inputs larger than L2 ({x.numel() / 1e9:.2f} GB vs 126 MB)",
+                   "per_rank": "independent graph per rank"},
+        "sampled_exact_check": check,
+        "stages_ms": {kname: statistics.mean(v) for kname, v in stage_ms.items()},
+        "roofline": roofline,
+        "e2e": {"value": world * n * k / (e2e_ms / 1000.0), "unit": UNIT, "h2d_bytes_per_step": int(x.numel()),
+                "d2h_bytes_per_step": n * k * 8, "ms_per_step": e2e_ms, "matches_device_path": e2e_consistent},
+        "cpu_baseline": cpu,
+        "clocks": clk,
+        "gpu_launches": launches,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
 
 
 def run_ours(args, world, rank, local):
@@ -499,23 +732,33 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=1_000_000)
-    ap.add_argument("--dim", type=int, default=768)
-    ap.add_argument("--k", type=int, default=30)
+    ap.add_argument("--workload", default="zipf_f32", choices=sorted(WORKLOADS))
+    ap.add_argument("--n", type=int, default=None)
+    ap.add_argument("--dim", type=int, default=None, help="features (f32, i8) or bytes per row (bits)")
+    ap.add_argument("--k", type=int, default=None)
+    ap.add_argument("--check-rows", type=int, default=128)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--fp32-rows", type=int, default=75_776)  # 2 full waves of 296 CTAs x 128 rows
     ap.add_argument("--recall-rows", type=int, default=10_000)
-    ap.add_argument("--cpu-rows", type=int, default=150_000)
+    ap.add_argument("--cpu-rows", type=int, default=None, help="CPU baseline sample rows (default per workload)")
     ap.add_argument("--serve-requests", type=int, default=10_000)
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-lanes", type=int, default=8)
     ap.add_argument("--serve-capacity", type=int, default=2000)
     ap.add_argument("--serve-baseline", type=int, default=250)
     args = ap.parse_args()
+    wn, wd, wk, _ = WORKLOADS[args.workload]
+    args.n = wn if args.n is None else args.n
+    args.dim = wd if args.dim is None else args.dim
+    args.k = wk if args.k is None else args.k
+    if args.cpu_rows is None:
+        args.cpu_rows = {"zipf_f32": 150_000, "gmm_i8": 150_000, "bits": 50_000}[args.workload]
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world, rank, local = dist_env()
     if args.impl == "reference":
         return run_reference(args, world, rank)
+    if args.workload != "zipf_f32":
+        return run_exact_int(args, world, rank, local)
     return run_ours(args, world, rank, local)
 
 
