@@ -85,20 +85,25 @@ constexpr int kModeJaccard = 2;  // 0/1 int8 rows: intersection counts, -(inter 
 // similarity t needs inter >= t * pa (taken 1e-6 looser so f32 rounding of J
 // never rejects a key the exact compare would admit).  Passing scores are
 // re-checked exactly by the key compare.
+// Integer scores are below 2^29 in magnitude (int8 dots for rows of fewer than
+// 33,000 bytes, intersection counts), so the "admit everything" threshold
+// -2^30 keeps score - threshold free of overflow.
+constexpr int32_t kIntOpen = -(1 << 30);
+
 template <int MODE>
 __device__ __forceinline__ uint32_t pass_threshold(const KeyHeap& heap, int32_t pa) {
   const uint64_t t = heap.threshold();
   if (MODE == kModeInt8) {
-    if (t == kKeyInf) return uint32_t(INT32_MIN);
+    if (t == kKeyInf) return uint32_t(kIntOpen);
     const float ts = -from_orderable(uint32_t(t >> 32));  // raw = -score
     int32_t ti = int32_t(ts);
     if (!(fabsf(ts) < 16777216.0f)) ti -= 256;
     return uint32_t(ti);
   }
   if (MODE == kModeJaccard) {
-    if (t == kKeyInf) return uint32_t(INT32_MIN);
+    if (t == kKeyInf) return uint32_t(kIntOpen);
     const float sim = -from_orderable(uint32_t(t >> 32));  // raw = -J (or +0.0 for J = 0)
-    if (!(sim > 0.0f)) return uint32_t(INT32_MIN);
+    if (!(sim > 0.0f)) return uint32_t(kIntOpen);
     return uint32_t(int32_t(floorf(sim * float(pa) * (1.0f - 1e-6f))));
   }
   const uint32_t NEG_INF = 0xff800000u;
@@ -119,14 +124,15 @@ __device__ __forceinline__ float jaccard_raw_counts(int32_t inter, int32_t uni) 
 
 // Offers the scores of one 32-column chunk that beat the threshold.  The
 // chunk's values stay in registers; a survivor's value is picked by an
-// unrolled select (survivors are rare once the heap is full).
+// unrolled select (survivors are rare once the heap is full).  Bit 31 - j of
+// `mask` stands for column j (the order chunk_mask builds).
 template <int MODE>
 __device__ __forceinline__ void offer_chunk(const uint32_t (&v)[32], uint32_t mask, int64_t col0, int64_t n_k,
                                             bool self_mode, int64_t q, KeyHeap& heap, uint32_t& thr, int32_t pa,
                                             const int32_t* __restrict__ pc) {
   while (mask) {
-    const int j = __ffs(mask) - 1;
-    mask &= mask - 1;
+    const int j = __clz(mask);
+    mask &= ~(0x80000000u >> j);
     uint32_t bits = 0;
 #pragma unroll
     for (int jj = 0; jj < 32; jj++) bits = (jj == j) ? v[jj] : bits;
@@ -145,12 +151,21 @@ __device__ __forceinline__ void offer_chunk(const uint32_t (&v)[32], uint32_t ma
   }
 }
 
+// Pass mask of a 32-column chunk, bit 31 - j for column j.  Two instructions
+// per score: the sign of (score - threshold) -- an integer subtraction, or an
+// f32 subtraction on the FMA pipe for BF16 -- is funnel-shifted into one of
+// four independent accumulators (short dependency chains), then inverted.
+// Equal scores pass (their difference is +0), as `passes` admits them.
 template <int MODE>
 __device__ __forceinline__ uint32_t chunk_mask(const uint32_t (&v)[32], uint32_t thr) {
-  uint32_t m = 0;
+  uint32_t f[4] = {0u, 0u, 0u, 0u};  // fail bits
 #pragma unroll
-  for (int j = 0; j < 32; j++) m |= (passes<MODE>(v[j], thr) ? 1u : 0u) << j;
-  return m;
+  for (int j = 0; j < 32; j++) {
+    const uint32_t d = MODE != kModeBf16 ? uint32_t(int32_t(v[j]) - int32_t(thr))
+                                         : __float_as_uint(__uint_as_float(v[j]) - __uint_as_float(thr));
+    f[j >> 3] = __funnelshift_l(d, f[j >> 3], 1);  // (f << 1) | sign(d)
+  }
+  return ~((f[0] << 24) | (f[1] << 16) | (f[2] << 8) | f[3]);
 }
 
 __device__ __forceinline__ void epilogue_sync(int nthreads) {
