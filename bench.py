@@ -319,7 +319,7 @@ def run_serving(args, dev):
            "offered_edges_per_s": offered,
            "data": "rows cut from 4 pinned-host mixtures per (d, dtype), window chosen by request id",
            "timing": "host monotonic clock: scheduled arrival -> graph copied back to host memory"}
-    with Server(budget_bytes=150 * 10**9, max_inflight=args.serve_lanes) as srv:
+    with Server(budget_bytes=150 * 10**9, max_inflight=args.serve_lanes, profile=True) as srv:
         serve_stream(srv, pools, warm_sched, list(range(len(warm_sched["n"]))), k, paced=False)
         t0, rec = serve_stream(srv, pools, sched, list(range(len(sched["n"]))), k, paced=True)
         out.update(serving_summary(t0, rec))
@@ -329,10 +329,22 @@ def run_serving(args, dev):
         out["workspace_misses"] = st["workspace_misses"]
         if args.serve_capacity > 0:
             ids = list(range(min(args.serve_capacity, len(sched["n"]))))
+            st0, busy0 = srv.stage_totals(), srv.lane_busy_ms()
             t0c, recc = serve_stream(srv, pools, sched, ids, k, paced=False)
             c = serving_summary(t0c, recc)
+            st1, busy1 = srv.stage_totals(), srv.lane_busy_ms()
+            stages = {nm: round(v[0] - st0.get(nm, (0.0, 0))[0], 1) for nm, v in st1.items()}
+            scan_ops = 0.0
+            for i in ids:
+                nn, dd, q = float(sched["n"][i]), float(sched["dim"][i]), bool(sched["i8"][i])
+                scan_ops += 2.0 * nn * nn * dd
             out["capacity"] = {"requests": c["requests"], "edges_per_s": c["edges_per_s"], "makespan_s": c["makespan_s"],
-                               "note": "the first requests of the stream submitted at once (closed queue)"}
+                               "scan_ops_per_s": scan_ops / c["makespan_s"],
+                               "stage_device_ms_sum": stages,
+                               "lane_busy_frac": (busy1 - busy0) / (args.serve_lanes * c["makespan_s"] * 1e3),
+                               "note": ("the first requests of the stream submitted at once (closed queue); "
+                                        "stage_device_ms_sum adds each request's stage times (CUDA events on its "
+                                        "lane's stream), so stages of concurrent requests overlap")}
     if args.serve_baseline > 0:
         ids = list(range(min(args.serve_baseline, len(sched["n"]))))
         with Server(budget_bytes=150 * 10**9, max_inflight=1) as base:

@@ -132,13 +132,21 @@ int stage_rows(evoc_gpu_ctx* ctx, const void* data, int64_t n, int64_t row_bytes
   Stage st(ctx, on_device ? "copy_rows" : "h2d_rows");
   const int64_t rows = evoc::padded_rows(n);
   EVOC_TRY(ctx->x.ensure(size_t(rows * ld_bytes)), "alloc rows");
+  if (on_device) {
+    // One SM pass copies, pads and zero-fills (the copy engines may be busy
+    // with other streams' host transfers).
+    EVOC_TRY(evoc::launch_copy_rows(data, n, row_bytes, ctx->x.p, rows, ld_bytes, ctx->sms, ctx->stream),
+             "copy rows");
+    ctx->launches += 1;
+    return EVOC_OK;
+  }
   if (ld_bytes != row_bytes)
     EVOC_TRY(cudaMemsetAsync(ctx->x.p, 0, size_t(rows * ld_bytes), ctx->stream), "memset rows");
   else if (rows > n)
     EVOC_TRY(cudaMemsetAsync(ctx->x.as<uint8_t>() + n * ld_bytes, 0, size_t((rows - n) * ld_bytes), ctx->stream),
              "memset pad rows");
   EVOC_TRY(cudaMemcpy2DAsync(ctx->x.p, size_t(ld_bytes), data, size_t(row_bytes), size_t(row_bytes), size_t(n),
-                             on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream),
+                             cudaMemcpyHostToDevice, ctx->stream),
            "upload rows");
   return EVOC_OK;
 }
@@ -180,7 +188,8 @@ int64_t pivot_count(int64_t n) {
   return n_piv;
 }
 
-int locality_order(evoc_gpu_ctx* ctx, const Job& j, const void* rows, int64_t row_bytes, bool int8) {
+int locality_order(evoc_gpu_ctx* ctx, const Job& j, const void* rows, int64_t row_bytes, bool int8,
+                   bool sorted_cells) {
   Stage st(ctx, "pivot_order");
   const int64_t n_piv = pivot_count(j.n);
   const int64_t piv_rows = evoc::padded_rows(n_piv);
@@ -199,9 +208,10 @@ int locality_order(evoc_gpu_ctx* ctx, const Job& j, const void* rows, int64_t ro
   EVOC_TRY(ctx->hist.ensure(size_t(n_piv) * 4), "alloc hist");
   EVOC_TRY(ctx->cursor.ensure(size_t(n_piv) * 4), "alloc cursor");
   EVOC_TRY(evoc::launch_order_by_label(ctx->labels.as<int32_t>(), j.nq, int(n_piv), ctx->hist.as<int32_t>(),
-                                       ctx->cursor.as<int32_t>(), ctx->order.as<int32_t>(), ctx->sms, ctx->stream),
+                                       ctx->cursor.as<int32_t>(), ctx->order.as<int32_t>(), sorted_cells, ctx->sms,
+                                       ctx->stream),
            "order by pivot");
-  ctx->launches += 6;
+  ctx->launches += sorted_cells ? 6 : 5;
   return EVOC_OK;
 }
 
@@ -239,7 +249,7 @@ int run_bf16_rerank(evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, const Job& j, 
   }
   const int32_t* order = nullptr;
   if (j.nq >= 65536) {
-    int rc = locality_order(ctx, j, ctx->xb.p, ldb * 2, false);
+    int rc = locality_order(ctx, j, ctx->xb.p, ldb * 2, false, false);  // the order only schedules the rerank
     if (rc) return rc;
     order = ctx->order.as<int32_t>();
   }
@@ -488,7 +498,7 @@ int run_nndescent(evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, const Job& j, in
     ctx->launches += 1;
   } else {
     // Pivot cells seed the graph and fix the visiting order.
-    int rc = locality_order(ctx, j, piv_rows, piv_row_bytes, dtype == EVOC_DTYPE_I8);
+    int rc = locality_order(ctx, j, piv_rows, piv_row_bytes, dtype == EVOC_DTYPE_I8, true);
     if (rc) return rc;
     a.order = ctx->order.as<int32_t>();
     a.label = ctx->labels.as<int32_t>();

@@ -54,8 +54,18 @@ cudaError_t launch_rerank_f32(const float* X, int ld, int d, int64_t n_q, int64_
                               float* out_dist, int* status, int sms, cudaStream_t stream);
 cudaError_t launch_gather_pivots(const void* src, int64_t row_bytes, int64_t n, int64_t n_piv, void* dst, int sms,
                                  cudaStream_t stream);
+// Counting sort of rows by label.  sorted_cells: rows inside each cell ordered
+// by index (deterministic; the NN-descent initialisation reads cells by
+// position); otherwise rows inside a cell keep the scatter's order, which is
+// enough where the order only schedules work (the rerank).
 cudaError_t launch_order_by_label(const int32_t* label, int64_t n, int nb, int32_t* hist, int32_t* cursor,
-                                  int32_t* order, int sms, cudaStream_t stream);
+                                  int32_t* order, bool sorted_cells, int sms, cudaStream_t stream);
+
+// prep.cu: rows of `row_bytes` (packed) -> rows of `ld_bytes` (>= row_bytes),
+// columns past row_bytes and rows n..rows-1 zero-filled; SM copy, so it does
+// not queue behind host<->device traffic on the copy engines.
+cudaError_t launch_copy_rows(const void* src, int64_t n, int64_t row_bytes, void* dst, int64_t rows, int64_t ld_bytes,
+                             int sms, cudaStream_t stream);
 
 }  // namespace evoc
 

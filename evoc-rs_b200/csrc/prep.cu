@@ -94,3 +94,39 @@ cudaError_t launch_to_bf16(const float* X, int64_t n, int ld, int d, void* Y, in
 }
 
 }  // namespace evoc
+
+namespace evoc {
+
+// Row copy with padding.  Wide path: 16-byte words when both strides and
+// both base addresses allow it; otherwise 4-byte words; otherwise bytes.
+template <typename W>
+__global__ void copy_rows_kernel(const uint8_t* __restrict__ src, int64_t n, int64_t row_bytes,
+                                 uint8_t* __restrict__ dst, int64_t rows, int64_t ld_bytes) {
+  const int64_t wpr = ld_bytes / int64_t(sizeof(W));      // words per destination row
+  const int64_t src_w = row_bytes / int64_t(sizeof(W));   // words of data per row
+  const int64_t total = rows * wpr;
+  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t r = e / wpr, c = e % wpr;
+    W v{};
+    if (r < n && c < src_w) v = reinterpret_cast<const W*>(src + r * row_bytes)[c];
+    reinterpret_cast<W*>(dst + r * ld_bytes)[c] = v;
+  }
+}
+
+cudaError_t launch_copy_rows(const void* src, int64_t n, int64_t row_bytes, void* dst, int64_t rows, int64_t ld_bytes,
+                             int sms, cudaStream_t stream) {
+  if (ld_bytes < row_bytes || rows < n) return cudaErrorInvalidValue;
+  const uintptr_t a = reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst);
+  const auto* s8 = static_cast<const uint8_t*>(src);
+  auto* d8 = static_cast<uint8_t*>(dst);
+  const int grid = sms * 8;
+  if (row_bytes % 16 == 0 && ld_bytes % 16 == 0 && (a & 15) == 0)
+    copy_rows_kernel<uint4><<<grid, 256, 0, stream>>>(s8, n, row_bytes, d8, rows, ld_bytes);
+  else if (row_bytes % 4 == 0 && ld_bytes % 4 == 0 && (a & 3) == 0)
+    copy_rows_kernel<uint32_t><<<grid, 256, 0, stream>>>(s8, n, row_bytes, d8, rows, ld_bytes);
+  else
+    copy_rows_kernel<uint8_t><<<grid, 256, 0, stream>>>(s8, n, row_bytes, d8, rows, ld_bytes);
+  return cudaGetLastError();
+}
+
+}  // namespace evoc

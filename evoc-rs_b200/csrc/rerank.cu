@@ -266,14 +266,14 @@ cudaError_t launch_gather_pivots(const void* src, int64_t row_bytes, int64_t n, 
 }
 
 cudaError_t launch_order_by_label(const int32_t* label, int64_t n, int nb, int32_t* hist, int32_t* cursor,
-                                  int32_t* order, int sms, cudaStream_t stream) {
+                                  int32_t* order, bool sorted_cells, int sms, cudaStream_t stream) {
   if (nb > 1024 * 64) return cudaErrorInvalidValue;
   cudaError_t e = cudaMemsetAsync(hist, 0, size_t(nb) * sizeof(int32_t), stream);
   if (e != cudaSuccess) return e;
   label_hist_kernel<<<sms * 4, 256, 0, stream>>>(label, n, nb, hist);
   exclusive_scan_kernel<<<1, 1024, 0, stream>>>(hist, nb, cursor);
   label_scatter_kernel<<<sms * 4, 256, 0, stream>>>(label, n, nb, cursor, order);
-  sort_cells_kernel<<<(nb + 127) / 128, 128, 0, stream>>>(cursor, hist, nb, order);
+  if (sorted_cells) sort_cells_kernel<<<(nb + 127) / 128, 128, 0, stream>>>(cursor, hist, nb, order);
   return cudaGetLastError();
 }
 

@@ -107,6 +107,10 @@ struct evoc_gpu_server {
   cudaMemPool_t pool = nullptr;
   std::vector<std::thread> workers;
   bool stopping = false;
+  bool profile = false;
+  std::vector<std::string> stage_names;            // first-seen order
+  std::unordered_map<std::string, std::pair<double, int64_t>> stage_totals;
+  double lane_busy_ms = 0.0;
 };
 
 namespace {
@@ -176,8 +180,26 @@ void run_job(evoc_gpu_server* s, int lane, Job* j) {
   nvtxRangePop();
   evoc::CtxSizes actual;
   evoc::ctx_buffer_sizes(ctx, &actual);
+  std::vector<std::pair<std::string, float>> stages;
+  if (s->profile && rc == EVOC_OK) {
+    char name[64];
+    float ms = 0.0f;
+    for (int i = 0, n = evoc_gpu_profile_count(ctx); i < n; i++)
+      if (evoc_gpu_profile_stage(ctx, i, name, sizeof(name), &ms) == EVOC_OK) stages.emplace_back(name, ms);
+  }
+  const int64_t t_end = now_ns();
   std::lock_guard<std::mutex> lock(s->mu);
   s->running--;
+  s->lane_busy_ms += double(t_end - j->t_admit) * 1e-6;
+  for (const auto& st_ms : stages) {
+    auto it = s->stage_totals.find(st_ms.first);
+    if (it == s->stage_totals.end()) {
+      s->stage_names.push_back(st_ms.first);
+      it = s->stage_totals.emplace(st_ms.first, std::make_pair(0.0, int64_t(0))).first;
+    }
+    it->second.first += st_ms.second;
+    it->second.second += 1;
+  }
   // The plan should match the context exactly; if it ever falls short, count
   // the real size from now on.
   const int64_t planned = int64_t(s->lane_sizes[size_t(lane)].total());
@@ -334,10 +356,12 @@ int evoc_gpu_server_create(const evoc_gpu_server_opts* opts, evoc_gpu_server** o
     delete s;
     return rc;
   };
+  s->profile = o.profile != 0;
   for (int i = 0; i < s->lanes; i++) {
     evoc_gpu_ctx* c = nullptr;
     const int rc = evoc_gpu_ctx_create(o.device, &c);
     if (rc != EVOC_OK) return bail(rc);
+    if (s->profile) evoc_gpu_profile_enable(c, 1);
     s->ctxs.push_back(c);
     s->streams.push_back(static_cast<cudaStream_t>(evoc_gpu_ctx_stream(c)));
   }
@@ -624,6 +648,34 @@ int evoc_gpu_server_stats(evoc_gpu_server* s, evoc_gpu_server_counters* out) {
   out->workspace_misses = s->ws_misses;
   out->lanes = s->lanes;
   return EVOC_OK;
+}
+
+int evoc_gpu_server_stage_count(evoc_gpu_server* s) {
+  if (!s) return 0;
+  std::lock_guard<std::mutex> lock(s->mu);
+  return int(s->stage_names.size());
+}
+
+int evoc_gpu_server_stage(evoc_gpu_server* s, int i, char* name, int32_t name_len, double* total_ms,
+                          int64_t* count) {
+  if (!s) return EVOC_ERR_ARG;
+  std::lock_guard<std::mutex> lock(s->mu);
+  if (i < 0 || i >= int(s->stage_names.size())) return EVOC_ERR_ARG;
+  const std::string& nm = s->stage_names[size_t(i)];
+  const auto& v = s->stage_totals[nm];
+  if (name && name_len > 0) {
+    std::strncpy(name, nm.c_str(), size_t(name_len) - 1);
+    name[name_len - 1] = '\0';
+  }
+  if (total_ms) *total_ms = v.first;
+  if (count) *count = v.second;
+  return EVOC_OK;
+}
+
+double evoc_gpu_server_lane_busy_ms(evoc_gpu_server* s) {
+  if (!s) return 0.0;
+  std::lock_guard<std::mutex> lock(s->mu);
+  return s->lane_busy_ms;
 }
 
 }  // extern "C"

@@ -112,6 +112,10 @@ def _bind_optional(L) -> None:
         L.evoc_gpu_server_cancel.argtypes = [P, i64]
         L.evoc_gpu_server_job_info.argtypes = [P, i64, C.POINTER(JobInfo)]
         L.evoc_gpu_server_stats.argtypes = [P, C.POINTER(ServerCounters)]
+        L.evoc_gpu_server_stage_count.argtypes = [P]
+        L.evoc_gpu_server_stage.argtypes = [P, C.c_int, C.c_char_p, i32, C.POINTER(C.c_double), C.POINTER(i64)]
+        L.evoc_gpu_server_lane_busy_ms.argtypes = [P]
+        L.evoc_gpu_server_lane_busy_ms.restype = C.c_double
 
 
 class ServerOpts(C.Structure):
@@ -120,7 +124,8 @@ class ServerOpts(C.Structure):
         ("device", C.c_int32),
         ("budget_bytes", C.c_int64),
         ("max_inflight", C.c_int32),
-        ("reserved", C.c_int32 * 5),
+        ("profile", C.c_int32),
+        ("reserved", C.c_int32 * 4),
     ]
 
 

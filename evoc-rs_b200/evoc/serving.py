@@ -32,13 +32,15 @@ class JobCancelled(BackendError):
 class Server:
     """One evoc_gpu_server on one device."""
 
-    def __init__(self, budget_bytes: int = 150 * 10**9, max_inflight: int = 4, device: int = 0):
+    def __init__(self, budget_bytes: int = 150 * 10**9, max_inflight: int = 4, device: int = 0,
+                 profile: bool = False):
         L = _lib.lib()
         o = _lib.ServerOpts()
         L.evoc_gpu_server_default_opts(C.byref(o))
         o.device = int(device)
         o.budget_bytes = int(budget_bytes)
         o.max_inflight = int(max_inflight)
+        o.profile = 1 if profile else 0
         self.h = C.c_void_p()
         rc = L.evoc_gpu_server_create(C.byref(o), C.byref(self.h))
         if rc != _lib.EVOC_OK:
@@ -170,6 +172,21 @@ class Server:
         c = _lib.ServerCounters()
         self._raise(_lib.lib().evoc_gpu_server_stats(self.h, C.byref(c)), "stats")
         return {name: int(getattr(c, name)) for name, _ in _lib.ServerCounters._fields_}
+
+    def stage_totals(self) -> dict:
+        """{stage: (summed device ms, requests)} over all finished requests (profile=True)."""
+        L = _lib.lib()
+        out = {}
+        buf = C.create_string_buffer(64)
+        ms, cnt = C.c_double(0.0), C.c_int64(0)
+        for i in range(L.evoc_gpu_server_stage_count(self.h)):
+            if L.evoc_gpu_server_stage(self.h, i, buf, 64, C.byref(ms), C.byref(cnt)) == _lib.EVOC_OK:
+                out[buf.value.decode()] = (float(ms.value), int(cnt.value))
+        return out
+
+    def lane_busy_ms(self) -> float:
+        """Host time the lanes spent on requests, summed over lanes."""
+        return float(_lib.lib().evoc_gpu_server_lane_busy_ms(self.h))
 
     @staticmethod
     def now_ns() -> int:

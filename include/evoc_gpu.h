@@ -205,7 +205,9 @@ typedef struct {
   int64_t budget_bytes;  /* HBM admission budget; default 150e9             */
   int32_t max_inflight;  /* lanes (requests on the device at once), 1..64;  */
                          /* default 4                                       */
-  int32_t reserved[5];
+  int32_t profile;       /* 1: time every request's stages with CUDA events */
+                         /* and keep per-stage totals (server_stage)        */
+  int32_t reserved[4];
 } evoc_gpu_server_opts;
 
 typedef struct {
@@ -275,6 +277,13 @@ int evoc_gpu_server_release(evoc_gpu_server* server, int64_t job_id);
 int evoc_gpu_server_cancel(evoc_gpu_server* server, int64_t job_id);
 int evoc_gpu_server_job_info(evoc_gpu_server* server, int64_t job_id, evoc_gpu_job_info* info);
 int evoc_gpu_server_stats(evoc_gpu_server* server, evoc_gpu_server_counters* stats);
+/* With opts.profile: the number of distinct stages seen, and stage i's name,
+ * summed device time (CUDA events on the lanes' streams) and request count.
+ * lane_busy_ms sums, over lanes, the host time a lane spent on requests. */
+int evoc_gpu_server_stage_count(evoc_gpu_server* server);
+int evoc_gpu_server_stage(evoc_gpu_server* server, int i, char* name, int32_t name_len, double* total_ms,
+                          int64_t* count);
+double evoc_gpu_server_lane_busy_ms(evoc_gpu_server* server);
 
 #ifdef __cplusplus
 }
