@@ -1,0 +1,77 @@
+// Batches of small requests in one pass (internal; not part of the C ABI).
+//
+// A batch lives in device tables: a header with the counts and one status
+// word, one BatchRowJob per request for the row kernels (copy and pad,
+// prepare_float, BF16 conversion, FP32 rerank), one ScanJob per request for
+// the tensor-core scan (its two tensor maps and scan parameters) and a
+// work-list of (request, 128-row query block) items.  Every kernel reads its
+// counts and pointers from these tables, so its launch parameters do not
+// depend on the batch and the whole sequence can be captured once in a CUDA
+// graph and replayed for every batch.
+#pragma once
+#include <cstdint>
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+namespace evoc {
+
+struct BatchHeader {
+  int32_t n_jobs;        // requests in the batch
+  int32_t n_items;       // scan work items
+  int32_t status;        // 0 ok; the scan / rerank status codes of any request
+  int32_t pad_;
+  int64_t total_rows;    // sum of n over the requests (rerank rows)
+  int64_t total_blocks;  // sum of ceil(n / 128) (row-norm blocks)
+};
+
+struct BatchRowJob {
+  int64_t n, dim;          // rows, features (f32) or bytes (i8)
+  int64_t rows;            // padded rows (multiple of 256)
+  int64_t row_bytes;       // packed input bytes per row
+  int64_t ld;              // f32 stride in floats (f32 requests)
+  int64_t ldb;             // BF16 / int8 stride in bytes
+  int64_t row_base;        // first global row of this request (prefix of n)
+  int64_t blk_base;        // first global 128-row block (prefix of ceil(n/128))
+  const uint8_t* src;      // packed input rows on the device
+  float* x;                // f32 padded rows (f32 requests)
+  uint8_t* xb;             // BF16 or int8 padded rows
+  float* norms;            // f32 row norms (f32 requests)
+  int32_t* flag;           // prepare_float: some row's norm is off by > 1e-5
+  int32_t* cand;           // n x C scan candidates (f32 requests)
+  int32_t C, keff;         // candidates kept per row, neighbours returned
+  int32_t* out_idx;
+  float* out_dist;
+  float* out_raw;          // may be null
+};
+
+struct alignas(64) ScanJob {
+  CUtensorMap ma, mb;      // query rows (box 128) and key rows (box 256)
+  int64_t n_q, n_k, q_row0;
+  int32_t n_kchunks, keep, self_mode, final_mode, dtype, pad_;
+  int32_t* out_idx;
+  float* out_raw;
+  float* out_dist;
+  const int32_t* pc;
+};
+
+struct ScanItem {
+  int32_t job, qb;
+};
+
+// tc_scan.cu.  Encodes a request's tensor maps and parameters (self mode:
+// every row is a query and a key).  mode 0: BF16 rows; 1: int8 rows.
+bool encode_scan_job(ScanJob* sj, int mode, const void* rows, int64_t rows_mem, int64_t n, int64_t row_bytes,
+                     int keep, int final_mode, int dtype, int32_t* out_idx, float* out_raw, float* out_dist);
+// Sets the kernels' shared-memory limit (call before a stream capture).
+cudaError_t prepare_tc_scan_batch(int mode, int max_keep);
+cudaError_t launch_tc_scan_batch(int mode, BatchHeader* hdr, const ScanJob* jobs, const ScanItem* items,
+                                 int max_keep, int grid, uint64_t timeout_ns, cudaStream_t stream);
+
+// batch.cu.  f32 requests: copy + pad into x, prepare_float, BF16 rows into
+// xb.  i8 requests: copy + pad into xb.
+cudaError_t launch_batch_rows(bool f32, const BatchHeader* hdr, const BatchRowJob* jobs, int sms,
+                              cudaStream_t stream);
+// f32 requests: FP32 rerank of the scan candidates into the outputs.
+cudaError_t launch_batch_rerank(BatchHeader* hdr, const BatchRowJob* jobs, int sms, cudaStream_t stream);
+
+}  // namespace evoc

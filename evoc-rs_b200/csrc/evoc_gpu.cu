@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "../../include/evoc_gpu.h"
+#include "batch.h"
 #include "common.cuh"
 #include "ctx_plan.h"
 #include "kernels.h"
@@ -66,6 +67,17 @@ struct evoc_gpu_ctx {
   DevBuf xb, cand, labels, order, hist, cursor, pivots, popc;
   DevBuf g_idx, g_dist, g_sigma, g_rho, g_indptr, g_indices, g_data, g_work;
   DevBuf nnd_work;
+  DevBuf batch_ws, batch_tab;  // batches: per-request work arena, device tables
+  void* batch_host = nullptr;  // pinned staging of the tables
+  size_t batch_host_bytes = 0;
+  struct BatchGraph {
+    bool f32;
+    int keep_odd;
+    void* tab;
+    cudaGraphExec_t exec;
+  };
+  std::vector<BatchGraph> batch_graphs;  // captured batch pipelines, replayed per batch
+  bool use_graphs = true;                // EVOC_NO_GRAPHS=1 launches the kernels directly
   uint64_t timeout_ns = 4000000000ull;  // longest a pipeline wait inside a kernel may take
   bool sync_check = false;  // EVOC_SYNC_CHECK=1: wait for and check every kernel stage (fault diagnosis)
   bool profiling = false;
@@ -688,6 +700,254 @@ int knn_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtype, con
   return EVOC_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Batches of small requests (evoc_gpu_knn_graph_batch)
+// ---------------------------------------------------------------------------
+inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+struct BatchJobPlan {
+  int64_t n, dim, rows, ld, ldb;
+  int keff, C, keep;
+  size_t off_x, off_xb, off_norms, off_cand, off_flag;
+};
+
+struct BatchLayout {
+  std::vector<BatchJobPlan> jobs;
+  size_t ws_bytes = 0;
+  size_t off_sj = 0, off_rj = 0, off_it = 0, tab_bytes = 0;
+  int max_keep = 1;
+  int64_t n_items = 0, total_rows = 0, total_blocks = 0;
+};
+
+// Largest keep the batch scan supports (its heaps must fit in shared memory).
+constexpr int kBatchMaxKeep = 80;
+constexpr int32_t kBatchMaxJobs = 4096;
+
+// Sizes and offsets of a batch's arena and tables; the serving planner uses
+// the same function, so admission counts exactly what the batch allocates.
+int batch_layout(bool f32, const evoc_gpu_opts& opts, int32_t n_jobs, const int64_t* n, const int64_t* dim,
+                 int32_t k, BatchLayout* L) {
+  L->jobs.resize(size_t(n_jobs));
+  size_t ws = 0;
+  for (int i = 0; i < n_jobs; i++) {
+    BatchJobPlan& J = L->jobs[size_t(i)];
+    if (n[i] <= 0) return EVOC_ERR_EMPTY;
+    if (dim[i] <= 0) return EVOC_ERR_ARG;
+    J.n = n[i];
+    J.dim = dim[i];
+    J.rows = evoc::padded_rows(J.n);
+    J.keff = int(std::max<int64_t>(1, std::min<int64_t>(k, J.n - 1)));
+    if (f32) {
+      J.ld = round_up(J.dim, 16);
+      J.ldb = round_up(J.dim, 64) * 2;
+      J.C = int(bf16_candidates(opts, J.n, J.keff));
+      J.keep = J.C;
+      J.off_x = ws;
+      ws += align_up(size_t(J.rows * J.ld * 4), 256);
+      J.off_xb = ws;
+      ws += align_up(size_t(J.rows * J.ldb), 256);
+      J.off_norms = ws;
+      ws += align_up(size_t(J.n) * 4, 256);
+      J.off_cand = ws;
+      ws += align_up(size_t(J.n) * size_t(J.C) * 4, 256);
+      J.off_flag = ws;
+      ws += 256;
+    } else {
+      J.ld = 0;
+      J.ldb = round_up(J.dim, 128);
+      J.C = J.keff;
+      J.keep = J.keff;
+      J.off_xb = ws;
+      ws += align_up(size_t(J.rows * J.ldb), 256);
+      J.off_x = J.off_norms = J.off_cand = J.off_flag = 0;
+    }
+    L->max_keep = std::max(L->max_keep, J.keep);
+    L->n_items += (J.n + 127) / 128;
+    L->total_rows += J.n;
+    L->total_blocks += (J.n + 127) / 128;
+  }
+  L->ws_bytes = std::max<size_t>(ws, 256);
+  // Fixed offsets (room for the largest batch), so the tables' addresses --
+  // which the kernels take as launch parameters -- do not depend on the batch
+  // and one captured graph serves every batch on this buffer.
+  L->off_sj = 64;
+  L->off_rj = align_up(L->off_sj + sizeof(evoc::ScanJob) * size_t(kBatchMaxJobs), 64);
+  L->off_it = align_up(L->off_rj + sizeof(evoc::BatchRowJob) * size_t(kBatchMaxJobs), 64);
+  L->tab_bytes = align_up(L->off_it + sizeof(evoc::ScanItem) * size_t(L->n_items), 256);
+  return EVOC_OK;
+}
+
+int knn_batch_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtype, int32_t n_jobs,
+                   const void* const* data, const int64_t* n, const int64_t* dim, int32_t k, int32_t* const* out_idx,
+                   float* const* out_dist, float* const* out_raw, int32_t* out_k) {
+  if (!ctx) return EVOC_ERR_ARG;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  ctx->err.clear();
+  ctx->n_stages = 0;
+  ctx->launches = 0;
+  evoc_gpu_opts opts;
+  evoc_gpu_default_opts(&opts);
+  if (opts_in) {
+    if (opts_in->struct_size != sizeof(evoc_gpu_opts)) return fail(ctx, EVOC_ERR_ARG, "opts.struct_size mismatch");
+    opts = *opts_in;
+  }
+  if (k <= 0) return fail(ctx, EVOC_ERR_K, "n_neighbors must be positive");
+  if (n_jobs <= 0 || n_jobs > kBatchMaxJobs || !data || !n || !dim || !out_idx)
+    return fail(ctx, EVOC_ERR_ARG, "bad batch arguments (1 <= n_jobs <= 4096, non-null arrays)");
+  if (!opts.buffers_on_device) return fail(ctx, EVOC_ERR_ARG, "batches take device buffers (buffers_on_device = 1)");
+  if (opts.row_begin != 0 || opts.row_end != 0) return fail(ctx, EVOC_ERR_ARG, "batches build whole graphs");
+  const bool f32 = dtype == EVOC_DTYPE_F32;
+  const int form = resolve_form(dtype, opts.form);
+  if (!((f32 && form == EVOC_FORM_BF16_RERANK) || (dtype == EVOC_DTYPE_I8 && form == EVOC_FORM_EXACT_INT)))
+    return fail(ctx, EVOC_ERR_UNSUPPORTED, "batches run the BF16+rerank form (f32) or the exact int8 form (i8)");
+  for (int i = 0; i < n_jobs; i++) {
+    if (n[i] <= 0) return fail(ctx, EVOC_ERR_EMPTY, "empty embedding matrix in the batch");
+    if (n[i] >= (int64_t(1) << 31) - 1) return fail(ctx, EVOC_ERR_ARG, "n exceeds int32 index range");
+    if (!data[i] || !out_idx[i]) return fail(ctx, EVOC_ERR_ARG, "null data or out_idx in the batch");
+  }
+  BatchLayout L;
+  int rc = batch_layout(f32, opts, n_jobs, n, dim, k, &L);
+  if (rc) return fail(ctx, rc, "bad request in the batch");
+  if (L.max_keep > kBatchMaxKeep) return fail(ctx, EVOC_ERR_UNSUPPORTED, "k too large for a batch");
+  EVOC_TRY(cudaSetDevice(ctx->device), "cudaSetDevice");
+  Stage total(ctx, "batch");
+  EVOC_TRY(ctx->batch_ws.ensure(L.ws_bytes), "alloc batch arena");
+  EVOC_TRY(ctx->batch_tab.ensure(L.tab_bytes), "alloc batch tables");
+  if (ctx->batch_host_bytes < L.tab_bytes) {
+    if (ctx->batch_host) cudaFreeHost(ctx->batch_host);
+    ctx->batch_host = nullptr;
+    ctx->batch_host_bytes = 0;
+    const size_t want = L.tab_bytes + L.tab_bytes / 4;
+    EVOC_TRY(cudaHostAlloc(&ctx->batch_host, want, cudaHostAllocDefault), "alloc pinned batch tables");
+    ctx->batch_host_bytes = want;
+  }
+  // Host tables.
+  uint8_t* H = static_cast<uint8_t*>(ctx->batch_host);
+  uint8_t* W = ctx->batch_ws.as<uint8_t>();
+  uint8_t* T = ctx->batch_tab.as<uint8_t>();
+  std::memset(H, 0, L.off_sj);
+  auto* hdr = reinterpret_cast<evoc::BatchHeader*>(H);
+  hdr->n_jobs = n_jobs;
+  hdr->n_items = int32_t(L.n_items);
+  hdr->status = 0;
+  hdr->total_rows = L.total_rows;
+  hdr->total_blocks = L.total_blocks;
+  auto* sj = reinterpret_cast<evoc::ScanJob*>(H + L.off_sj);
+  auto* rj = reinterpret_cast<evoc::BatchRowJob*>(H + L.off_rj);
+  auto* it = reinterpret_cast<evoc::ScanItem*>(H + L.off_it);
+  int64_t row_base = 0, blk_base = 0;
+  for (int i = 0; i < n_jobs; i++) {
+    const BatchJobPlan& J = L.jobs[size_t(i)];
+    evoc::BatchRowJob& R = rj[i];
+    R.n = J.n;
+    R.dim = J.dim;
+    R.rows = J.rows;
+    R.row_bytes = f32 ? J.dim * 4 : J.dim;
+    R.ld = J.ld;
+    R.ldb = J.ldb;
+    R.row_base = row_base;
+    R.blk_base = blk_base;
+    row_base += J.n;
+    blk_base += (J.n + 127) / 128;
+    R.src = static_cast<const uint8_t*>(data[i]);
+    R.x = f32 ? reinterpret_cast<float*>(W + J.off_x) : nullptr;
+    R.xb = W + J.off_xb;
+    R.norms = f32 ? reinterpret_cast<float*>(W + J.off_norms) : nullptr;
+    R.flag = f32 ? reinterpret_cast<int32_t*>(W + J.off_flag) : nullptr;
+    R.cand = f32 ? reinterpret_cast<int32_t*>(W + J.off_cand) : nullptr;
+    R.C = J.C;
+    R.keff = J.keff;
+    R.out_idx = out_idx[i];
+    R.out_dist = out_dist ? out_dist[i] : nullptr;
+    R.out_raw = out_raw ? out_raw[i] : nullptr;
+    const bool ok =
+        f32 ? evoc::encode_scan_job(&sj[i], evoc::kScanBf16, R.xb, J.rows, J.n, J.ldb, J.C, 0, 0, R.cand, nullptr,
+                                    nullptr)
+            : evoc::encode_scan_job(&sj[i], evoc::kScanInt8, R.xb, J.rows, J.n, J.ldb, J.keff, 1, EVOC_DTYPE_I8,
+                                    R.out_idx, R.out_raw, R.out_dist);
+    if (!ok) return fail(ctx, EVOC_ERR_CUDA, "tensor map encoding failed for a batch request");
+    if (out_k) out_k[i] = J.keff;
+  }
+  // Work-list: the query blocks of the largest requests first, so the
+  // persistent CTAs' round-robin share of the items is balanced.
+  std::vector<int32_t> by_size(static_cast<size_t>(n_jobs));
+  for (int i = 0; i < n_jobs; i++) by_size[size_t(i)] = i;
+  std::stable_sort(by_size.begin(), by_size.end(),
+                   [&](int32_t a, int32_t b) { return L.jobs[size_t(a)].n > L.jobs[size_t(b)].n; });
+  int64_t w = 0;
+  for (int32_t i : by_size)
+    for (int64_t qb = 0; qb < (L.jobs[size_t(i)].n + 127) / 128; qb++) it[w++] = evoc::ScanItem{i, int32_t(qb)};
+  EVOC_TRY(cudaMemcpyAsync(T, H, L.off_sj + sizeof(evoc::ScanJob) * size_t(n_jobs), cudaMemcpyHostToDevice,
+                           ctx->stream),
+           "upload batch tables");
+  EVOC_TRY(cudaMemcpyAsync(T + L.off_rj, H + L.off_rj, sizeof(evoc::BatchRowJob) * size_t(n_jobs),
+                           cudaMemcpyHostToDevice, ctx->stream),
+           "upload batch tables");
+  EVOC_TRY(cudaMemcpyAsync(T + L.off_it, H + L.off_it, sizeof(evoc::ScanItem) * size_t(L.n_items),
+                           cudaMemcpyHostToDevice, ctx->stream),
+           "upload batch tables");
+  auto* d_hdr = reinterpret_cast<evoc::BatchHeader*>(T);
+  auto* d_sj = reinterpret_cast<const evoc::ScanJob*>(T + L.off_sj);
+  auto* d_rj = reinterpret_cast<const evoc::BatchRowJob*>(T + L.off_rj);
+  auto* d_it = reinterpret_cast<const evoc::ScanItem*>(T + L.off_it);
+  const int mode = f32 ? evoc::kScanBf16 : evoc::kScanInt8;
+  EVOC_TRY(evoc::prepare_tc_scan_batch(mode, L.max_keep), "batch scan attributes");
+  // The table offsets depend on n_jobs; the graph is keyed on everything its
+  // launch parameters hold.
+  const int keep_odd = L.max_keep | 1;
+  auto launch_all = [&](cudaStream_t st) -> cudaError_t {
+    cudaError_t e = evoc::launch_batch_rows(f32, d_hdr, d_rj, ctx->sms, st);
+    if (e == cudaSuccess)
+      e = evoc::launch_tc_scan_batch(mode, d_hdr, d_sj, d_it, L.max_keep, ctx->sms, ctx->timeout_ns, st);
+    if (e == cudaSuccess && f32) e = evoc::launch_batch_rerank(d_hdr, d_rj, ctx->sms, st);
+    return e;
+  };
+  ctx->launches += f32 ? 6 : 2;
+  if (ctx->use_graphs && !ctx->sync_check) {
+    // Drop graphs captured over an older table buffer.
+    for (size_t g = 0; g < ctx->batch_graphs.size();) {
+      if (ctx->batch_graphs[g].tab != ctx->batch_tab.p) {
+        cudaGraphExecDestroy(ctx->batch_graphs[g].exec);
+        ctx->batch_graphs.erase(ctx->batch_graphs.begin() + long(g));
+      } else {
+        g++;
+      }
+    }
+    cudaGraphExec_t exec = nullptr;
+    for (const auto& g : ctx->batch_graphs)
+      if (g.f32 == f32 && g.keep_odd == keep_odd && g.tab == ctx->batch_tab.p) exec = g.exec;
+    if (!exec) {
+      cudaGraph_t graph = nullptr;
+      EVOC_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal), "begin batch capture");
+      const cudaError_t le = launch_all(ctx->stream);
+      const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
+      if (le != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return cuda_fail(ctx, le, "batch launches");
+      }
+      EVOC_TRY(ce, "end batch capture");
+      const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+      cudaGraphDestroy(graph);
+      EVOC_TRY(ie, "instantiate batch graph");
+      ctx->batch_graphs.push_back({f32, keep_odd, ctx->batch_tab.p, exec});
+    }
+    EVOC_TRY(cudaGraphLaunch(exec, ctx->stream), "launch batch graph");
+  } else {
+    EVOC_TRY(launch_all(ctx->stream), "batch launches");
+  }
+  int status = 0;
+  EVOC_TRY(cudaMemcpyAsync(&status, &d_hdr->status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream),
+           "read batch status");
+  total.end();
+  EVOC_TRY(cudaStreamSynchronize(ctx->stream), "batch");
+  if (status == evoc::kStatusBadOrder || status == evoc::kStatusBadCandidate)
+    return fail(ctx, EVOC_ERR_CUDA, "device self-check failed in a batch (code " + std::to_string(status) + ")");
+  if (status != 0)
+    return fail(ctx, EVOC_ERR_TIMEOUT, "a kernel pipeline wait timed out in a batch (stage " +
+                                           std::to_string(status) + ")");
+  return EVOC_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -717,6 +977,7 @@ int evoc_gpu_ctx_create(int device, evoc_gpu_ctx** out) {
   ctx->device = device;
   cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device);
   if (const char* v = std::getenv("EVOC_SYNC_CHECK")) ctx->sync_check = v[0] == '1';
+  if (const char* v = std::getenv("EVOC_NO_GRAPHS")) ctx->use_graphs = v[0] != '1';
   e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     delete ctx;
@@ -736,6 +997,10 @@ void evoc_gpu_ctx_destroy(evoc_gpu_ctx* ctx) {
                     &ctx->g_idx,    &ctx->g_dist,  &ctx->g_sigma, &ctx->g_rho, &ctx->g_indptr,
                     &ctx->g_indices, &ctx->g_data, &ctx->g_work, &ctx->nnd_work};
   for (DevBuf* b : bufs) b->release();
+  for (auto& g : ctx->batch_graphs) cudaGraphExecDestroy(g.exec);
+  ctx->batch_ws.release();
+  ctx->batch_tab.release();
+  if (ctx->batch_host) cudaFreeHost(ctx->batch_host);
   for (auto& r : ctx->stages) {
     if (r.a) cudaEventDestroy(r.a);
     if (r.b) cudaEventDestroy(r.b);
@@ -790,6 +1055,12 @@ int evoc_gpu_knn_graph(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts, int32_t dty
                        int64_t dim, int32_t k, const int64_t* rng_state, int32_t* out_idx, float* out_dist,
                        int32_t* out_k) {
   return knn_impl(ctx, opts, dtype, data, n, dim, k, rng_state, out_idx, out_dist, nullptr, out_k);
+}
+
+int evoc_gpu_knn_graph_batch(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts, int32_t dtype, int32_t n_jobs,
+                             const void* const* data, const int64_t* n, const int64_t* dim, int32_t k,
+                             int32_t* const* out_idx, float* const* out_dist, float* const* out_raw, int32_t* out_k) {
+  return knn_batch_impl(ctx, opts, dtype, n_jobs, data, n, dim, k, out_idx, out_dist, out_raw, out_k);
 }
 
 int evoc_gpu_knn_graph_raw(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts, int32_t dtype, const void* data,

@@ -9,6 +9,7 @@
 // global reads stay coalesced.
 #include <cuda_bf16.h>
 
+#include "batch.h"
 #include "common.cuh"
 #include "kernels.h"
 
@@ -19,11 +20,10 @@ constexpr int kRows = 128;
 constexpr int kSlab = 32;
 }
 
-__global__ void __launch_bounds__(kRows)
-row_norms_kernel(const float* __restrict__ X, int64_t n, int ld, int d, float* __restrict__ norms,
-                 int* __restrict__ not_unit) {
-  __shared__ float slab[kRows][kSlab + 1];
-  const int64_t r0 = int64_t(blockIdx.x) * kRows;
+// Norms of rows r0 .. r0+127 (one thread per row, serial f32 sum of squares).
+__device__ __forceinline__ void row_norms_block(const float* __restrict__ X, int64_t n, int ld, int d,
+                                                float* __restrict__ norms, int* __restrict__ not_unit, int64_t r0,
+                                                float (*slab)[kSlab + 1]) {
   const int tid = threadIdx.x;
   float acc = 0.0f;
   for (int c0 = 0; c0 < d; c0 += kSlab) {
@@ -47,6 +47,13 @@ row_norms_kernel(const float* __restrict__ X, int64_t n, int ld, int d, float* _
     norms[row] = nrm;
     if (fabsf(__fsub_rn(nrm, 1.0f)) > 1e-5f) atomicOr(not_unit, 1);
   }
+}
+
+__global__ void __launch_bounds__(kRows)
+row_norms_kernel(const float* __restrict__ X, int64_t n, int ld, int d, float* __restrict__ norms,
+                 int* __restrict__ not_unit) {
+  __shared__ float slab[kRows][kSlab + 1];
+  row_norms_block(X, n, ld, d, norms, not_unit, int64_t(blockIdx.x) * kRows, slab);
 }
 
 __global__ void normalize_rows_kernel(float* __restrict__ X, int64_t n, int ld, int d,
@@ -126,6 +133,104 @@ cudaError_t launch_copy_rows(const void* src, int64_t n, int64_t row_bytes, void
     copy_rows_kernel<uint32_t><<<grid, 256, 0, stream>>>(s8, n, row_bytes, d8, rows, ld_bytes);
   else
     copy_rows_kernel<uint8_t><<<grid, 256, 0, stream>>>(s8, n, row_bytes, d8, rows, ld_bytes);
+  return cudaGetLastError();
+}
+
+}  // namespace evoc
+
+// ---------------------------------------------------------------------------
+// Batches: the same per-request steps over the request table of a batch.
+// ---------------------------------------------------------------------------
+namespace evoc {
+
+namespace {
+__device__ __forceinline__ int find_block_job(const BatchRowJob* __restrict__ jobs, int nj, int64_t g) {
+  int lo = 0, hi = nj - 1;
+  while (lo < hi) {  // last request with blk_base <= g
+    const int mid = (lo + hi + 1) >> 1;
+    if (jobs[mid].blk_base <= g) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+}  // namespace
+
+// Packed input rows -> padded rows (f32: x, ld floats; i8: xb, ldb bytes),
+// zero-filled past the data; also clears each request's prepare_float flag.
+__global__ void batch_copy_kernel(const BatchHeader* __restrict__ hdr, const BatchRowJob* __restrict__ jobs,
+                                  bool f32) {
+  const int nj = hdr->n_jobs;
+  for (int j = 0; j < nj; j++) {
+    const BatchRowJob& J = jobs[j];
+    if (blockIdx.x == 0 && threadIdx.x == 0 && J.flag) *J.flag = 0;
+    uint8_t* dst = f32 ? reinterpret_cast<uint8_t*>(J.x) : J.xb;
+    const int64_t ld_bytes = f32 ? J.ld * 4 : J.ldb;
+    if (J.row_bytes % 4 == 0) {
+      const int64_t wpr = ld_bytes / 4, src_w = J.row_bytes / 4, total = J.rows * wpr;
+      for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+           e += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t r = e / wpr, c = e % wpr;
+        uint32_t v = 0u;
+        if (r < J.n && c < src_w) v = reinterpret_cast<const uint32_t*>(J.src + r * J.row_bytes)[c];
+        reinterpret_cast<uint32_t*>(dst + r * ld_bytes)[c] = v;
+      }
+    } else {
+      const int64_t total = J.rows * ld_bytes;
+      for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+           e += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t r = e / ld_bytes, c = e % ld_bytes;
+        dst[e] = (r < J.n && c < J.row_bytes) ? J.src[r * J.row_bytes + c] : uint8_t(0);
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kRows)
+batch_row_norms_kernel(const BatchHeader* __restrict__ hdr, const BatchRowJob* __restrict__ jobs) {
+  __shared__ float slab[kRows][kSlab + 1];
+  const int nj = hdr->n_jobs;
+  const int64_t total = hdr->total_blocks;
+  for (int64_t g = blockIdx.x; g < total; g += gridDim.x) {
+    const BatchRowJob& J = jobs[find_block_job(jobs, nj, g)];
+    row_norms_block(J.x, J.n, int(J.ld), int(J.dim), J.norms, J.flag, (g - J.blk_base) * kRows, slab);
+  }
+}
+
+__global__ void batch_normalize_kernel(const BatchHeader* __restrict__ hdr, const BatchRowJob* __restrict__ jobs) {
+  const int nj = hdr->n_jobs;
+  for (int j = 0; j < nj; j++) {
+    const BatchRowJob& J = jobs[j];
+    if (*J.flag == 0) continue;
+    const int64_t d = J.dim, total = J.n * d;
+    for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x) {
+      const int64_t r = e / d, c = e % d;
+      float nrm = J.norms[r];
+      if (nrm == 0.0f) nrm = 1.0f;
+      J.x[r * J.ld + c] = __fdiv_rn(J.x[r * J.ld + c], nrm);
+    }
+  }
+}
+
+__global__ void batch_to_bf16_kernel(const BatchHeader* __restrict__ hdr, const BatchRowJob* __restrict__ jobs) {
+  const int nj = hdr->n_jobs;
+  for (int j = 0; j < nj; j++) {
+    const BatchRowJob& J = jobs[j];
+    const int64_t lde = J.ldb / 2, total = J.rows * lde;
+    __nv_bfloat16* Y = reinterpret_cast<__nv_bfloat16*>(J.xb);
+    for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x) {
+      const int64_t r = e / lde, c = e % lde;
+      Y[e] = __float2bfloat16_rn(c < J.dim ? J.x[r * J.ld + c] : 0.0f);
+    }
+  }
+}
+
+cudaError_t launch_batch_rows(bool f32, const BatchHeader* hdr, const BatchRowJob* jobs, int sms,
+                              cudaStream_t stream) {
+  batch_copy_kernel<<<sms * 8, 256, 0, stream>>>(hdr, jobs, f32);
+  if (!f32) return cudaGetLastError();
+  batch_row_norms_kernel<<<sms * 8, kRows, 0, stream>>>(hdr, jobs);
+  batch_normalize_kernel<<<sms * 8, 256, 0, stream>>>(hdr, jobs);
+  batch_to_bf16_kernel<<<sms * 8, 256, 0, stream>>>(hdr, jobs);
   return cudaGetLastError();
 }
 

@@ -16,6 +16,7 @@
 // moment work on nearby points whose candidates overlap.
 #include <cuda_bf16.h>
 
+#include "batch.h"
 #include "common.cuh"
 #include "kernels.h"
 
@@ -59,6 +60,96 @@ __device__ __forceinline__ void warp_bitonic(uint64_t* keys, int P, int lane) {
 __device__ __forceinline__ float key_raw(uint64_t key) { return from_orderable(uint32_t(key >> 32)); }
 }  // namespace
 
+// One query row: FP32 dot products with its C candidates, a warp bitonic
+// sort of (raw, index) keys, FP64 at the k-th boundary, the sorted row
+// written to output row q.  kw: this warp's P key slots; dw: its 32 doubles.
+__device__ __forceinline__ void rerank_row(const float* __restrict__ X, int ld, int d, int64_t n_keys, int64_t q,
+                                           int64_t qg, const int32_t* __restrict__ cq, int C, int P, int k,
+                                           int32_t* __restrict__ out_idx, float* __restrict__ out_raw,
+                                           float* __restrict__ out_dist, int* status, uint64_t* kw, double* dw,
+                                           int lane) {
+  const float* xq = X + qg * ld;
+  for (int j0 = 0; j0 < C; j0 += GROUP) {
+    int32_t id[GROUP];
+    float acc[GROUP];
+#pragma unroll
+    for (int u = 0; u < GROUP; u++) {
+      id[u] = (j0 + u < C) ? cq[j0 + u] : -1;
+      if (id[u] >= n_keys) {  // never written by a finished scan: record it, skip the candidate
+        if (status) atomicCAS(status, 0, kStatusBadCandidate);
+        id[u] = -1;
+      }
+      acc[u] = 0.0f;
+    }
+    for (int t = lane; t < d; t += 32) {
+      const float xv = xq[t];
+#pragma unroll
+      for (int u = 0; u < GROUP; u++)
+        if (id[u] >= 0) acc[u] = fmaf(xv, X[int64_t(id[u]) * ld + t], acc[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < GROUP; u++) {
+      const float dot = warp_sum(acc[u]);
+      if (lane == u && j0 + u < C) {
+        uint64_t key = kKeyInf;
+        if (id[u] >= 0) key = make_key(id[u] == qg ? -1.0f : raw_cosine(dot), id[u]);
+        kw[j0 + u] = key;
+      }
+    }
+  }
+  for (int j = C + lane; j < P; j += 32) kw[j] = kKeyInf;
+  __syncwarp();
+  warp_bitonic(kw, P, lane);
+
+  // FP64 only where FP32 cannot separate candidates at the k-th boundary.
+  const int kk = k < C ? k : C;
+  if (kk < C && kw[kk - 1] != kKeyInf && kw[kk] != kKeyInf) {
+    const float rk = key_raw(kw[kk - 1]);
+    int lo = kk - 1, hi = kk;
+    while (lo > 0 && kw[lo - 1] != kKeyInf && key_raw(kw[lo - 1]) >= rk - 1e-6f) lo--;
+    while (hi < C && kw[hi] != kKeyInf && key_raw(kw[hi]) <= rk + 1e-6f) hi++;
+    const int g = hi - lo;
+    if (g > 1 && g <= 32) {
+      for (int j = 0; j < g; j++) {
+        const int32_t c = key_index(kw[lo + j]);
+        double acc = 0.0;
+        for (int t = lane; t < d; t += 32) acc = fma(double(xq[t]), double(X[int64_t(c) * ld + t]), acc);
+        acc = warp_sum_d(acc);
+        // FP64 dissimilarity under the reference's rule: self -1, -dot, or the
+        // MIN_POSITIVE sentinel for dots <= 0 (a true tie, broken by index).
+        if (lane == 0) dw[j] = (c == qg) ? -1.0 : (acc > 0.0 ? -acc : double(kMinPositive));
+      }
+      __syncwarp();
+      if (lane == 0) {
+        // insertion sort of the boundary group by (FP64 dissimilarity, index)
+        for (int i = 1; i < g; i++) {
+          const double dv = dw[i];
+          const uint64_t kv = kw[lo + i];
+          int j = i - 1;
+          while (j >= 0 && (dw[j] > dv || (dw[j] == dv && key_index(kw[lo + j]) > key_index(kv)))) {
+            dw[j + 1] = dw[j];
+            kw[lo + j + 1] = kw[lo + j];
+            j--;
+          }
+          dw[j + 1] = dv;
+          kw[lo + j + 1] = kv;
+        }
+      }
+      __syncwarp();
+    }
+  }
+  // Write the row (lane j writes entries j, j+32, ...).
+  for (int j = lane; j < k; j += 32) {
+    const uint64_t key = j < C ? kw[j] : kKeyInf;
+    const bool ok = key != kKeyInf;
+    const float raw = ok ? key_raw(key) : kHeapInf;
+    out_idx[q * k + j] = ok ? key_index(key) : -1;
+    if (out_raw) out_raw[q * k + j] = raw;
+    if (out_dist) out_dist[q * k + j] = transform_raw(0, raw);
+  }
+  __syncwarp();
+}
+
 __global__ void __launch_bounds__(RW * 32)
 rerank_f32_kernel(const float* __restrict__ X, int ld, int d, int64_t n, int64_t n_keys, int64_t q_row0,
                   const int32_t* __restrict__ cand, int C, int k, const int32_t* __restrict__ order,
@@ -69,7 +160,6 @@ rerank_f32_kernel(const float* __restrict__ X, int ld, int d, int64_t n, int64_t
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // The candidates are only complete when the scan that wrote them finished.
   if (status && *reinterpret_cast<volatile int*>(status) != 0) return;
-  uint64_t* kw = keys[warp];
   int P = 1;
   while (P < C) P <<= 1;
   for (int64_t w = int64_t(blockIdx.x) * RW + warp; w < n; w += int64_t(gridDim.x) * RW) {
@@ -78,88 +168,39 @@ rerank_f32_kernel(const float* __restrict__ X, int ld, int d, int64_t n, int64_t
       if (lane == 0 && status) atomicCAS(status, 0, kStatusBadOrder);
       continue;
     }
-    const int64_t qg = q_row0 + q;           // row of the data set
-    const float* xq = X + qg * ld;
-    const int32_t* cq = cand + q * C;
-    for (int j0 = 0; j0 < C; j0 += GROUP) {
-      int32_t id[GROUP];
-      float acc[GROUP];
-#pragma unroll
-      for (int u = 0; u < GROUP; u++) {
-        id[u] = (j0 + u < C) ? cq[j0 + u] : -1;
-        if (id[u] >= n_keys) {  // never written by a finished scan: record it, skip the candidate
-          if (status) atomicCAS(status, 0, kStatusBadCandidate);
-          id[u] = -1;
-        }
-        acc[u] = 0.0f;
-      }
-      for (int t = lane; t < d; t += 32) {
-        const float xv = xq[t];
-#pragma unroll
-        for (int u = 0; u < GROUP; u++)
-          if (id[u] >= 0) acc[u] = fmaf(xv, X[int64_t(id[u]) * ld + t], acc[u]);
-      }
-#pragma unroll
-      for (int u = 0; u < GROUP; u++) {
-        const float dot = warp_sum(acc[u]);
-        if (lane == u && j0 + u < C) {
-          uint64_t key = kKeyInf;
-          if (id[u] >= 0) key = make_key(id[u] == qg ? -1.0f : raw_cosine(dot), id[u]);
-          kw[j0 + u] = key;
-        }
-      }
-    }
-    for (int j = C + lane; j < P; j += 32) kw[j] = kKeyInf;
-    __syncwarp();
-    warp_bitonic(kw, P, lane);
+    rerank_row(X, ld, d, n_keys, q, q_row0 + q, cand + q * C, C, P, k, out_idx, out_raw, out_dist, status, keys[warp],
+               d64[warp], lane);
+  }
+}
 
-    // FP64 only where FP32 cannot separate candidates at the k-th boundary.
-    const int kk = k < C ? k : C;
-    if (kk < C && kw[kk - 1] != kKeyInf && kw[kk] != kKeyInf) {
-      const float rk = key_raw(kw[kk - 1]);
-      int lo = kk - 1, hi = kk;
-      while (lo > 0 && kw[lo - 1] != kKeyInf && key_raw(kw[lo - 1]) >= rk - 1e-6f) lo--;
-      while (hi < C && kw[hi] != kKeyInf && key_raw(kw[hi]) <= rk + 1e-6f) hi++;
-      const int g = hi - lo;
-      if (g > 1 && g <= 32) {
-        for (int j = 0; j < g; j++) {
-          const int32_t c = key_index(kw[lo + j]);
-          double acc = 0.0;
-          for (int t = lane; t < d; t += 32) acc = fma(double(xq[t]), double(X[int64_t(c) * ld + t]), acc);
-          acc = warp_sum_d(acc);
-          // FP64 dissimilarity under the reference's rule: self -1, -dot, or the
-          // MIN_POSITIVE sentinel for dots <= 0 (a true tie, broken by index).
-          if (lane == 0) d64[warp][j] = (c == qg) ? -1.0 : (acc > 0.0 ? -acc : double(kMinPositive));
-        }
-        __syncwarp();
-        if (lane == 0) {
-          // insertion sort of the boundary group by (FP64 dissimilarity, index)
-          for (int i = 1; i < g; i++) {
-            const double dv = d64[warp][i];
-            const uint64_t kv = kw[lo + i];
-            int j = i - 1;
-            while (j >= 0 && (d64[warp][j] > dv || (d64[warp][j] == dv && key_index(kw[lo + j]) > key_index(kv)))) {
-              d64[warp][j + 1] = d64[warp][j];
-              kw[lo + j + 1] = kw[lo + j];
-              j--;
-            }
-            d64[warp][j + 1] = dv;
-            kw[lo + j + 1] = kv;
-          }
-        }
-        __syncwarp();
-      }
+// The same per row over the requests of a batch: warp per global row, the
+// request found by binary search over the rows' prefix offsets.
+__global__ void __launch_bounds__(RW * 32)
+batch_rerank_kernel(BatchHeader* hdr, const BatchRowJob* __restrict__ jobs) {
+  __shared__ uint64_t keys[RW][MAXC];
+  __shared__ double d64[RW][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int* status = &hdr->status;
+  if (*reinterpret_cast<volatile int*>(status) != 0) return;
+  const int nj = hdr->n_jobs;
+  const int64_t total = hdr->total_rows;
+  for (int64_t w = int64_t(blockIdx.x) * RW + warp; w < total; w += int64_t(gridDim.x) * RW) {
+    int lo = 0, hi = nj - 1;
+    while (lo < hi) {  // last job with row_base <= w
+      const int mid = (lo + hi + 1) >> 1;
+      if (jobs[mid].row_base <= w) lo = mid;
+      else hi = mid - 1;
     }
-    // Write the row (lane j writes entries j, j+32, ...).
-    for (int j = lane; j < k; j += 32) {
-      const uint64_t key = j < C ? kw[j] : kKeyInf;
-      const bool ok = key != kKeyInf;
-      const float raw = ok ? key_raw(key) : kHeapInf;
-      out_idx[q * k + j] = ok ? key_index(key) : -1;
-      if (out_raw) out_raw[q * k + j] = raw;
-      if (out_dist) out_dist[q * k + j] = transform_raw(0, raw);
+    const BatchRowJob& J = jobs[lo];
+    const int64_t q = w - J.row_base;
+    if (q < 0 || q >= J.n) {
+      if (lane == 0) atomicCAS(status, 0, kStatusBadOrder);
+      continue;
     }
-    __syncwarp();
+    int P = 1;
+    while (P < J.C) P <<= 1;
+    rerank_row(J.x, int(J.ld), int(J.dim), J.n, q, q, J.cand + q * J.C, J.C, P, J.keff, J.out_idx, J.out_raw,
+               J.out_dist, status, keys[warp], d64[warp], lane);
   }
 }
 
@@ -171,6 +212,11 @@ cudaError_t launch_rerank_f32(const float* X, int ld, int d, int64_t n, int64_t 
   if (blocks > int64_t(sms) * 16) blocks = int64_t(sms) * 16;
   rerank_f32_kernel<<<unsigned(blocks), RW * 32, 0, stream>>>(X, ld, d, n, n_keys, q_row0, cand, C, k, order,
                                                                out_idx, out_raw, out_dist, status);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_rerank(BatchHeader* hdr, const BatchRowJob* jobs, int sms, cudaStream_t stream) {
+  batch_rerank_kernel<<<unsigned(sms * 16), RW * 32, 0, stream>>>(hdr, jobs);
   return cudaGetLastError();
 }
 

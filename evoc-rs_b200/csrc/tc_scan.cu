@@ -24,9 +24,11 @@
 // Replaces the distance evaluations of the reference's NN-descent local join
 // (src/nndescent/float.rs:552-660 with fast_cosine, src/fast_cosine.rs:33-45;
 // src/nndescent/int8.rs:15-21 for the int8 dissimilarity).
+#include <cstring>
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include "batch.h"
 #include "common.cuh"
 #include "kernels.h"
 #include "sm100.cuh"
@@ -67,6 +69,11 @@ struct ScanParams {
   int* status;       // 0 ok; set non-zero by the first role that gives up
   uint64_t timeout_ns;
   const int32_t* pc; // Jaccard mode: popcount of every row (queries and keys)
+  // Batch mode: the work-list of (request, query block) items and the
+  // requests' tensor maps and parameters, all in device memory.
+  const ScanJob* jobs;
+  const ScanItem* items;
+  const int32_t* n_items;
 };
 
 namespace {
@@ -168,13 +175,75 @@ __device__ __forceinline__ uint32_t chunk_mask(const uint32_t (&v)[32], uint32_t
   return ~((f[0] << 24) | (f[1] << 16) | (f[2] << 8) | f[3]);
 }
 
+// One work item as every role sees it: a 128-row query block of one request.
+struct ItemView {
+  const CUtensorMap* ma;
+  const CUtensorMap* mb;
+  int64_t qb, n_q, n_k, q_row0, n_ktiles;
+  int n_kchunks, keep, self_mode, final_mode, dtype;
+  int32_t* out_idx;
+  float* out_raw;
+  float* out_dist;
+  const int32_t* pc;
+};
+
+template <bool kBatch>
+__device__ __forceinline__ ItemView item_view(const ScanParams& p, const CUtensorMap* tmA, const CUtensorMap* tmB,
+                                              int64_t it) {
+  ItemView v;
+  if (kBatch) {
+    const ScanItem si = p.items[it];
+    const ScanJob* J = p.jobs + si.job;
+    v.ma = &J->ma;
+    v.mb = &J->mb;
+    v.qb = si.qb;
+    v.n_q = J->n_q;
+    v.n_k = J->n_k;
+    v.q_row0 = J->q_row0;
+    v.n_kchunks = J->n_kchunks;
+    v.keep = J->keep;
+    v.self_mode = J->self_mode;
+    v.final_mode = J->final_mode;
+    v.dtype = J->dtype;
+    v.out_idx = J->out_idx;
+    v.out_raw = J->out_raw;
+    v.out_dist = J->out_dist;
+    v.pc = J->pc;
+  } else {
+    v.ma = tmA;
+    v.mb = tmB;
+    v.qb = it;
+    v.n_q = p.n_q;
+    v.n_k = p.n_k;
+    v.q_row0 = p.q_row0;
+    v.n_kchunks = p.n_kchunks;
+    v.keep = p.keep;
+    v.self_mode = p.self_mode;
+    v.final_mode = p.final_mode;
+    v.dtype = p.dtype;
+    v.out_idx = p.out_idx;
+    v.out_raw = p.out_raw;
+    v.out_dist = p.out_dist;
+    v.pc = p.pc;
+  }
+  v.n_ktiles = (v.n_k + BN - 1) / BN;
+  return v;
+}
+
+// A tensor map in global memory written before the launch: order the
+// tensor-map proxy's reads after it.
+__device__ __forceinline__ void tensormap_acquire(const CUtensorMap* map) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(reinterpret_cast<uint64_t>(map))
+               : "memory");
+}
+
 __device__ __forceinline__ void epilogue_sync(int nthreads) {
   asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
 }
 
 }  // namespace
 
-template <int MODE, int STAGES, int GROUPS, bool kSmemHeap>
+template <int MODE, int STAGES, int GROUPS, bool kSmemHeap, bool kBatch>
 __global__ void __launch_bounds__(64 + GROUPS * 128, 1)
 tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const ScanParams p) {
   using namespace sm100;
@@ -204,7 +273,7 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     mbar_init(mma_done, 1);
     fence_barrier_init();
   }
-  if (warp == 0 && lane == 0) {
+  if (!kBatch && warp == 0 && lane == 0) {
     prefetch_tmap(&tmA);
     prefetch_tmap(&tmB);
   }
@@ -218,8 +287,7 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
   const uint32_t tmem_base = *tmem_slot;
 
   constexpr bool kInt8 = MODE != kModeBf16;
-  const int64_t n_qblocks = (p.n_q + BM - 1) / BM;
-  const int64_t n_ktiles = (p.n_k + BN - 1) / BN;
+  const int64_t n_items = kBatch ? int64_t(*p.n_items) : (p.n_q + BM - 1) / BM;
   const volatile int* abort = p.status;
   constexpr int KC_ELEMS = kInt8 ? KCB : KCB / 2;
   constexpr uint32_t IDESC = kInt8 ? idesc_s8_s32(BM, BN) : idesc_bf16_f32(BM, BN);
@@ -229,9 +297,14 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     if (lane == 0) {
       uint32_t it = 0;
       bool ok = true;
-      for (int64_t qb = blockIdx.x; ok && qb < n_qblocks; qb += gridDim.x) {
-        for (int64_t kt = 0; ok && kt < n_ktiles; kt++) {
-          for (int kc = 0; kc < p.n_kchunks; kc++) {
+      for (int64_t itm = blockIdx.x; ok && itm < n_items; itm += gridDim.x) {
+        const ItemView v = item_view<kBatch>(p, &tmA, &tmB, itm);
+        if (kBatch) {
+          tensormap_acquire(v.ma);
+          tensormap_acquire(v.mb);
+        }
+        for (int64_t kt = 0; ok && kt < v.n_ktiles; kt++) {
+          for (int kc = 0; kc < v.n_kchunks; kc++) {
             const uint32_t s = it % STAGES, ph = (it / STAGES) & 1u;
             if (!mbar_wait(&empty[s], ph ^ 1u, abort, p.timeout_ns)) {
               set_status(p.status, 1);
@@ -240,8 +313,8 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
             }
             uint8_t* a_dst = smem + s * STAGE_BYTES;
             mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
-            tma_load_2d(a_dst, &tmA, &full[s], kc * KC_ELEMS, int32_t(p.q_row0 + qb * BM));
-            tma_load_2d(a_dst + A_BYTES, &tmB, &full[s], kc * KC_ELEMS, int32_t(kt * BN));
+            tma_load_2d(a_dst, v.ma, &full[s], kc * KC_ELEMS, int32_t(v.q_row0 + v.qb * BM));
+            tma_load_2d(a_dst + A_BYTES, v.mb, &full[s], kc * KC_ELEMS, int32_t(kt * BN));
             it++;
           }
         }
@@ -255,8 +328,9 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     if (lane == 0) {
       uint32_t it = 0, tile = 0;
       bool ok = true;
-      for (int64_t qb = blockIdx.x; ok && qb < n_qblocks; qb += gridDim.x) {
-        for (int64_t kt = 0; ok && kt < n_ktiles; kt++, tile++) {
+      for (int64_t itm = blockIdx.x; ok && itm < n_items; itm += gridDim.x) {
+        const ItemView v = item_view<kBatch>(p, &tmA, &tmB, itm);
+        for (int64_t kt = 0; ok && kt < v.n_ktiles; kt++, tile++) {
           const uint32_t a = tile & 1u, tph = (tile >> 1) & 1u;
           if (!mbar_wait(&tempty[a], tph ^ 1u, abort, p.timeout_ns)) {
             set_status(p.status, 2);
@@ -265,7 +339,7 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
           }
           tc_fence_after();
           const uint32_t d_tmem = tmem_base + a * BN;
-          for (int kc = 0; kc < p.n_kchunks; kc++) {
+          for (int kc = 0; kc < v.n_kchunks; kc++) {
             const uint32_t s = it % STAGES, ph = (it / STAGES) & 1u;
             if (!mbar_wait(&full[s], ph, abort, p.timeout_ns)) {
               set_status(p.status, 2);
@@ -306,16 +380,17 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
                                  : p.scratch + (int64_t(blockIdx.x) * GROUPS * BM + heap_slot) * p.heap_stride;
     uint32_t tile = 0;
     bool ok = true;
-    for (int64_t qb = blockIdx.x; ok && qb < n_qblocks; qb += gridDim.x) {
-      const int64_t q = qb * BM + row_local;  // output row
-      const int64_t qg = p.q_row0 + q;        // row of the data set
-      const bool valid = q < p.n_q;
+    for (int64_t itm = blockIdx.x; ok && itm < n_items; itm += gridDim.x) {
+      const ItemView v = item_view<kBatch>(p, &tmA, &tmB, itm);
+      const int64_t q = v.qb * BM + row_local;  // output row
+      const int64_t qg = v.q_row0 + q;          // row of the data set
+      const bool valid = q < v.n_q;
       KeyHeap heap;
-      heap.init(hstore, p.keep);
-      if (valid && p.self_mode && group == 0) heap.offer(make_key(-1.0f, int32_t(qg)));
-      const int32_t pa = (MODE == kModeJaccard && valid) ? p.pc[qg] : 0;
+      heap.init(hstore, v.keep);
+      if (valid && v.self_mode && group == 0) heap.offer(make_key(-1.0f, int32_t(qg)));
+      const int32_t pa = (MODE == kModeJaccard && valid) ? v.pc[qg] : 0;
       uint32_t thr = pass_threshold<MODE>(heap, pa);
-      for (int64_t kt = 0; kt < n_ktiles; kt++, tile++) {
+      for (int64_t kt = 0; kt < v.n_ktiles; kt++, tile++) {
         const uint32_t a = tile & 1u, tph = (tile >> 1) & 1u;
         int got = 1;
         if (lane == 0) got = mbar_wait(&tfull[a], tph, abort, p.timeout_ns) ? 1 : 0;
@@ -335,11 +410,11 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
           tmem_ld_wait();
           tmem_ld_32x32b_x32(tbase + (c + 1) * 32, vb);
           uint32_t m = chunk_mask<MODE>(va, thr);
-          if (valid && m) offer_chunk<MODE>(va, m, k0 + c * 32, p.n_k, p.self_mode, qg, heap, thr, pa, p.pc);
+          if (valid && m) offer_chunk<MODE>(va, m, k0 + c * 32, v.n_k, v.self_mode, qg, heap, thr, pa, v.pc);
           tmem_ld_wait();
           if (c + 2 < NCH) tmem_ld_32x32b_x32(tbase + (c + 2) * 32, va);
           m = chunk_mask<MODE>(vb, thr);
-          if (valid && m) offer_chunk<MODE>(vb, m, k0 + (c + 1) * 32, p.n_k, p.self_mode, qg, heap, thr, pa, p.pc);
+          if (valid && m) offer_chunk<MODE>(vb, m, k0 + (c + 1) * 32, v.n_k, v.self_mode, qg, heap, thr, pa, v.pc);
         }
         tc_fence_before();
         mbar_arrive(&tempty[a]);
@@ -349,14 +424,14 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         // Fold the other groups' heaps for this row into group 0's.  Unused
         // slots of a heap that never filled are marked empty first.
         if (group > 0)
-          for (int j = heap.size; j < p.keep; j++) heap.h[j] = kKeyInf;
+          for (int j = heap.size; j < v.keep; j++) heap.h[j] = kKeyInf;
         epilogue_sync(GROUPS * 128);
         if (group == 0 && valid) {
           for (int g = 1; g < GROUPS; g++) {
             const uint64_t* other = kSmemHeap ? heaps + int64_t(g * BM + row_local) * p.heap_stride
                                               : p.scratch + (int64_t(blockIdx.x) * GROUPS * BM + g * BM + row_local) *
                                                                 p.heap_stride;
-            for (int j = 0; j < p.keep; j++) {
+            for (int j = 0; j < v.keep; j++) {
               const uint64_t kv = other[j];
               if (kv != kKeyInf) heap.offer(kv);
             }
@@ -365,8 +440,8 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
       }
       if (group == 0 && valid) {
         const int got = heap.finish();
-        const int64_t orow = q * p.keep;
-        for (int j = 0; j < p.keep; j++) {
+        const int64_t orow = q * v.keep;
+        for (int j = 0; j < v.keep; j++) {
           float raw = kHeapInf;
           int32_t idx = -1;
           if (j < got) {
@@ -375,11 +450,11 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
             // Keys fold -0.0 onto +0.0; restore the reference's sign: an int8
             // zero dot is -0.0; a Jaccard zero is +0.0 only for two empty rows.
             if (MODE == kModeInt8) raw = int8_raw_from_key(raw);
-            if (MODE == kModeJaccard && raw == 0.0f) raw = (pa + p.pc[idx] == 0) ? 0.0f : -0.0f;
+            if (MODE == kModeJaccard && raw == 0.0f) raw = (pa + v.pc[idx] == 0) ? 0.0f : -0.0f;
           }
-          p.out_idx[orow + j] = idx;
-          if (p.out_raw) p.out_raw[orow + j] = raw;
-          if (p.final_mode && p.out_dist) p.out_dist[orow + j] = transform_raw(p.dtype, raw);
+          v.out_idx[orow + j] = idx;
+          if (v.out_raw) v.out_raw[orow + j] = raw;
+          if (v.final_mode && v.out_dist) v.out_dist[orow + j] = transform_raw(v.dtype, raw);
         }
       }
       if (GROUPS > 1) epilogue_sync(GROUPS * 128);  // heaps are reused by the next block
@@ -433,10 +508,10 @@ bool make_map(CUtensorMap* m, const void* base, int64_t rows, int64_t row_bytes,
 size_t tc_scan_smem_bytes() { return smem_bytes(4, 1, 0); }
 
 namespace {
-template <int MODE, int STAGES, int GROUPS, bool kSmemHeap>
+template <int MODE, int STAGES, int GROUPS, bool kSmemHeap, bool kBatch = false>
 cudaError_t launch_variant(const CUtensorMap& ma, const CUtensorMap& mb, const ScanParams& p, int grid, size_t smem,
                            cudaStream_t stream) {
-  auto kern = tc_scan_kernel<MODE, STAGES, GROUPS, kSmemHeap>;
+  auto kern = tc_scan_kernel<MODE, STAGES, GROUPS, kSmemHeap, kBatch>;
   // The opt-in limit, not `smem`: the launch's shared memory varies with keep,
   // and concurrent callers (serving lanes) must not lower each other's limit
   // between this call and their launch.
@@ -483,7 +558,7 @@ cudaError_t launch_tc_scan(int mode, const void* Q, int64_t q_rows, int64_t q_ro
   alignas(64) CUtensorMap ma, mb;
   if (!make_map(&ma, Q, q_rows, row_bytes, eb, BM) || !make_map(&mb, K, k_rows, row_bytes, eb, BN))
     return cudaErrorInvalidValue;
-  ScanParams p;
+  ScanParams p{};
   p.n_q = n_q;
   p.n_k = n_k;
   p.q_row0 = q_row0;
@@ -502,6 +577,108 @@ cudaError_t launch_tc_scan(int mode, const void* Q, int64_t q_rows, int64_t q_ro
   if (mode == kModeInt8) return launch_mode<kModeInt8>(ma, mb, p, grid, stream);
   if (mode == kModeJaccard) return launch_mode<kModeJaccard>(ma, mb, p, grid, stream);
   return launch_mode<kModeBf16>(ma, mb, p, grid, stream);
+}
+
+// ---------------------------------------------------------------------------
+// Batches: one persistent launch over the work-list of many requests.
+// ---------------------------------------------------------------------------
+bool encode_scan_job(ScanJob* sj, int mode, const void* rows, int64_t rows_mem, int64_t n, int64_t row_bytes,
+                     int keep, int final_mode, int dtype, int32_t* out_idx, float* out_raw, float* out_dist) {
+  if (mode != kModeBf16 && mode != kModeInt8) return false;
+  if (row_bytes % KCB != 0 || n <= 0 || keep < 1 || rows_mem < n || rows_mem % BN != 0) return false;
+  if (reinterpret_cast<uintptr_t>(rows) & 15) return false;
+  const int eb = mode == kModeBf16 ? 2 : 1;
+  if (!make_map(&sj->ma, rows, rows_mem, row_bytes, eb, BM) || !make_map(&sj->mb, rows, rows_mem, row_bytes, eb, BN))
+    return false;
+  sj->n_q = n;
+  sj->n_k = n;
+  sj->q_row0 = 0;
+  sj->n_kchunks = int(row_bytes / KCB);
+  sj->keep = keep;
+  sj->self_mode = 1;
+  sj->final_mode = final_mode;
+  sj->dtype = dtype;
+  sj->pad_ = 0;
+  sj->out_idx = out_idx;
+  sj->out_raw = out_raw;
+  sj->out_dist = out_dist;
+  sj->pc = nullptr;
+  return true;
+}
+
+namespace {
+// The batch variants: shared-memory heaps only (keep stays small for batched
+// requests), chosen by the largest keep in the batch as launch_mode chooses.
+template <int MODE>
+int batch_variant(int max_keep, size_t* smem) {
+  const int odd = max_keep | 1;
+  const int cfg[4][2] = {{4, 2}, {3, 2}, {4, 1}, {3, 1}};
+  for (int i = 0; i < 4; i++)
+    if (smem_bytes(cfg[i][0], cfg[i][1], odd) <= SMEM_LIMIT) {
+      *smem = smem_bytes(cfg[i][0], cfg[i][1], odd);
+      return i;
+    }
+  return -1;
+}
+
+template <int MODE>
+cudaError_t set_batch_attr(int v) {
+  const void* kerns[4] = {reinterpret_cast<const void*>(tc_scan_kernel<MODE, 4, 2, true, true>),
+                          reinterpret_cast<const void*>(tc_scan_kernel<MODE, 3, 2, true, true>),
+                          reinterpret_cast<const void*>(tc_scan_kernel<MODE, 4, 1, true, true>),
+                          reinterpret_cast<const void*>(tc_scan_kernel<MODE, 3, 1, true, true>)};
+  return cudaFuncSetAttribute(kerns[v], cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_LIMIT));
+}
+
+template <int MODE>
+cudaError_t launch_batch_mode(const ScanParams& p, int max_keep, int grid, cudaStream_t stream) {
+  size_t smem = 0;
+  const int v = batch_variant<MODE>(max_keep, &smem);
+  if (v < 0) return cudaErrorInvalidValue;
+  CUtensorMap none;
+  std::memset(&none, 0, sizeof(none));  // unused in batch mode: every item names its request's maps
+  switch (v) {
+    case 0:
+      tc_scan_kernel<MODE, 4, 2, true, true><<<grid, 64 + 2 * 128, smem, stream>>>(none, none, p);
+      break;
+    case 1:
+      tc_scan_kernel<MODE, 3, 2, true, true><<<grid, 64 + 2 * 128, smem, stream>>>(none, none, p);
+      break;
+    case 2:
+      tc_scan_kernel<MODE, 4, 1, true, true><<<grid, 64 + 1 * 128, smem, stream>>>(none, none, p);
+      break;
+    default:
+      tc_scan_kernel<MODE, 3, 1, true, true><<<grid, 64 + 1 * 128, smem, stream>>>(none, none, p);
+  }
+  return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t prepare_tc_scan_batch(int mode, int max_keep) {
+  size_t smem = 0;
+  if (mode == kModeBf16) {
+    const int v = batch_variant<kModeBf16>(max_keep, &smem);
+    return v < 0 ? cudaErrorInvalidValue : set_batch_attr<kModeBf16>(v);
+  }
+  if (mode == kModeInt8) {
+    const int v = batch_variant<kModeInt8>(max_keep, &smem);
+    return v < 0 ? cudaErrorInvalidValue : set_batch_attr<kModeInt8>(v);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_tc_scan_batch(int mode, BatchHeader* hdr, const ScanJob* jobs, const ScanItem* items,
+                                 int max_keep, int grid, uint64_t timeout_ns, cudaStream_t stream) {
+  ScanParams p{};
+  p.heap_stride = max_keep | 1;
+  p.status = &hdr->status;
+  p.timeout_ns = timeout_ns;
+  p.jobs = jobs;
+  p.items = items;
+  p.n_items = &hdr->n_items;
+  if (mode == kModeBf16) return launch_batch_mode<kModeBf16>(p, max_keep, grid, stream);
+  if (mode == kModeInt8) return launch_batch_mode<kModeInt8>(p, max_keep, grid, stream);
+  return cudaErrorInvalidValue;
 }
 
 }  // namespace evoc

@@ -14,6 +14,8 @@ from .knn import (  # noqa: F401
     KnnError,
     KnnGraphOptions,
     knn_graph,
+    knn_graph_batch,
+    knn_graph_batch_device,
     knn_graph_device,
     knn_graph_ref,
     transform_distances_float,

@@ -225,6 +225,55 @@ def knn_graph_device(ptr: int, dtype_code: int, n: int, dim: int, k: int, out_id
     return kout.value
 
 
+def knn_graph_batch_device(ptrs, dtype_code: int, ns, dims, k: int, out_idx_ptrs, out_dist_ptrs,
+                           options: Optional[KnnGraphOptions] = None, out_raw_ptrs=None) -> list[int]:
+    """Many graphs in one pass (evoc_gpu_knn_graph_batch); every pointer is a device pointer.
+    Returns k_eff of each request."""
+    options = options or KnnGraphOptions(n_neighbors=k)
+    ctx = _lib.context(options.device)
+    o = _to_opts(options, on_device=True)
+    m = len(ptrs)
+    P = C.c_void_p
+    arr = lambda xs: (P * m)(*[P(int(x)) if x else None for x in xs])  # noqa: E731
+    n = (C.c_int64 * m)(*[int(v) for v in ns])
+    d = (C.c_int64 * m)(*[int(v) for v in dims])
+    kout = (C.c_int32 * m)()
+    raw = arr(out_raw_ptrs) if out_raw_ptrs is not None else None
+    st = _lib.lib().evoc_gpu_knn_graph_batch(ctx.h, C.byref(o), dtype_code, m, arr(ptrs), n, d, int(k),
+                                            arr(out_idx_ptrs), arr(out_dist_ptrs), raw, kout)
+    _raise_for(st, ctx)
+    return list(kout)
+
+
+def knn_graph_batch(datas, options: KnnGraphOptions, rngs=None):
+    """Build the graphs of many embedding sets of one dtype in one pass.  Returns a list of
+    (indices, distances) as knn_graph returns them; each result equals knn_graph on that set.
+    With `rngs`, each RandomState is advanced by knn_graph's draws."""
+    import torch
+
+    datas = [EmbeddingData.wrap(x) for x in datas]
+    if options.n_neighbors <= 0:
+        raise InvalidNeighbors()
+    if not datas:
+        return []
+    if any(x.nrows() == 0 for x in datas):
+        raise EmptyData()
+    if rngs is not None:
+        for x, r in zip(datas, rngs):
+            _advance_rng(r, x, options)
+    code = datas[0].dtype_code
+    dev = torch.device("cuda", options.device)
+    xs = [torch.from_numpy(np.ascontiguousarray(x.array)).to(dev) for x in datas]
+    ks = [max(1, min(options.n_neighbors, x.nrows() - 1)) for x in datas]
+    oi = [torch.empty((x.nrows(), kk), dtype=torch.int32, device=dev) for x, kk in zip(datas, ks)]
+    od = [torch.empty((x.nrows(), kk), dtype=torch.float32, device=dev) for x, kk in zip(datas, ks)]
+    torch.cuda.current_stream(dev).synchronize()  # the library runs on its own stream
+    knn_graph_batch_device([t.data_ptr() for t in xs], code, [x.nrows() for x in datas],
+                           [x.array.shape[1] for x in datas], options.n_neighbors, [t.data_ptr() for t in oi],
+                           [t.data_ptr() for t in od], options)
+    return [(a.cpu().numpy(), b.cpu().numpy()) for a, b in zip(oi, od)]
+
+
 def transform_distances_float(distances: np.ndarray) -> np.ndarray:
     """transform_distances_float (src/knn.rs:156-171), host-side helper."""
     d = np.asarray(distances, np.float32)

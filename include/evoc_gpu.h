@@ -108,6 +108,32 @@ int evoc_gpu_knn_graph(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts, int32_t dty
                        int64_t dim, int32_t k, const int64_t* rng_state, int32_t* out_idx, float* out_dist,
                        int32_t* out_k);
 
+/*
+ * Many independent kNN graphs in one pass: the BF16+rerank form for f32
+ * requests, the exact int8 form for i8.  No counterpart in evoc-rs (each
+ * fit_predict builds one graph, src/clustering.rs:650-716); it is the serving
+ * loop's path for small requests and open to any caller with many small sets.
+ * One persistent tensor-core launch takes the query blocks of every request
+ * from a device work-list, so requests too small to fill the GPU share it;
+ * the kernels read all per-request data from device tables, and the sequence
+ * is captured once per context in a CUDA graph and replayed (EVOC_NO_GRAPHS=1
+ * launches it directly).  Results are identical to evoc_gpu_knn_graph's on
+ * each request.
+ *   opts       buffers_on_device must be 1 (all pointers are device pointers);
+ *              form AUTO, BF16_RERANK (f32) or EXACT_INT (i8)
+ *   dtype      EVOC_DTYPE_F32 or EVOC_DTYPE_I8, the same for every request
+ *   n_jobs     1..4096 requests; request i has n[i] rows of dim[i] at data[i]
+ *   k          n_neighbors for every request (k_eff_i = max(1, min(k, n_i - 1)));
+ *              the kept candidates (2k for f32, k for i8) must be <= 80
+ *   out_idx[i], out_dist[i], out_raw[i]   n_i x k_eff_i each (out_dist and
+ *              out_raw arrays, or their entries, may be NULL)
+ *   out_k      n_jobs entries receiving k_eff_i (may be NULL)
+ * The call returns after every graph is written; one failure fails the batch.
+ */
+int evoc_gpu_knn_graph_batch(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts, int32_t dtype, int32_t n_jobs,
+                             const void* const* data, const int64_t* n, const int64_t* dim, int32_t k,
+                             int32_t* const* out_idx, float* const* out_dist, float* const* out_raw, int32_t* out_k);
+
 /* As evoc_gpu_knn_graph, and also writes the raw pre-transform
  * dissimilarities the reference's heaps hold (src/knn.rs:456-520 checks
  * them) into out_raw (n x k_eff, may be NULL). */

@@ -183,6 +183,7 @@ def test_device_rows_and_resident_result():
     x = _f32(2048, 128, 70)
     ind0, dst0 = evoc.knn_graph(x, _opts("bf16_rerank", 15))
     t = torch.from_numpy(x).cuda()
+    torch.cuda.synchronize()  # the upload runs on torch's stream; the lanes read on their own
     with Server(max_inflight=2) as srv:
         j = srv.submit_device(t.data_ptr(), _lib.DTYPE_F32, 2048, 128, _opts("bf16_rerank", 15), keep_alive=t)
         assert srv.wait(j, timeout=60) == _lib.EVOC_OK
