@@ -297,6 +297,51 @@ def serving_summary(t0, rec):
             "queue_ms": {"p50": _pct(queue, 50), "p99": _pct(queue, 99)}}
 
 
+def small_graph_batch(dev, m=256, n=2000, d=384, k=15, reps=3):
+    """Many small graphs: one evoc_gpu_knn_graph_batch call against one evoc_gpu_knn_graph call per
+    graph (device-resident f32 rows, BF16+rerank form), wall time of whole passes."""
+    import torch
+
+    import evoc
+    from evoc import _lib
+
+    g = torch.Generator(device=dev)
+    g.manual_seed(5)
+    xs = []
+    for _ in range(m):
+        x = torch.randn(n, d, generator=g, device=dev)
+        xs.append(x / x.norm(dim=1, keepdim=True))
+    opts = evoc.KnnGraphOptions(n_neighbors=k, form="bf16_rerank")
+    oi = [torch.empty((n, k), dtype=torch.int32, device=dev) for _ in range(m)]
+    od = [torch.empty((n, k), dtype=torch.float32, device=dev) for _ in range(m)]
+    torch.cuda.synchronize()
+
+    def singles():
+        for x, a, b in zip(xs, oi, od):
+            evoc.knn_graph_device(x.data_ptr(), _lib.DTYPE_F32, n, d, k, a.data_ptr(), b.data_ptr(), opts)
+
+    def batch():
+        evoc.knn_graph_batch_device([x.data_ptr() for x in xs], _lib.DTYPE_F32, [n] * m, [d] * m, k,
+                                    [a.data_ptr() for a in oi], [b.data_ptr() for b in od], opts)
+
+    out = {"graphs": m, "n": n, "d": d, "k": k}
+    for name, fn in (("one_call_per_graph_ms", singles), ("batch_ms", batch)):
+        fn()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        torch.cuda.synchronize()
+        out[name] = (time.perf_counter() - t) / reps * 1e3
+    batch()
+    first = [a.clone() for a in oi]
+    singles()
+    out["identical"] = all(torch.equal(a, b) for a, b in zip(first, oi))
+    out["speedup"] = out["one_call_per_graph_ms"] / out["batch_ms"]
+    out["batch_edges_per_s"] = m * n * k / (out["batch_ms"] / 1e3)
+    return out
+
+
 def run_serving(args, dev):
     """The continuous-batching server on the serving workload, next to the
     plain FP32 form run one request at a time on the same arrivals."""
@@ -319,7 +364,8 @@ def run_serving(args, dev):
            "offered_edges_per_s": offered,
            "data": "rows cut from 4 pinned-host mixtures per (d, dtype), window chosen by request id",
            "timing": "host monotonic clock: scheduled arrival -> graph copied back to host memory"}
-    with Server(budget_bytes=150 * 10**9, max_inflight=args.serve_lanes, profile=True) as srv:
+    with Server(budget_bytes=150 * 10**9, max_inflight=args.serve_lanes, profile=True,
+                batch_max=args.serve_batch) as srv:
         serve_stream(srv, pools, warm_sched, list(range(len(warm_sched["n"]))), k, paced=False)
         t0, rec = serve_stream(srv, pools, sched, list(range(len(sched["n"]))), k, paced=True)
         out.update(serving_summary(t0, rec))
@@ -327,6 +373,7 @@ def run_serving(args, dev):
         out["peak_bytes"] = st["peak_bytes"]
         out["failed"] = st["failed"]
         out["workspace_misses"] = st["workspace_misses"]
+        out["batches"], out["batched_requests"] = st["batches"], st["batched"]
         if args.serve_capacity > 0:
             ids = list(range(min(args.serve_capacity, len(sched["n"]))))
             st0, busy0 = srv.stage_totals(), srv.lane_busy_ms()
@@ -345,6 +392,7 @@ def run_serving(args, dev):
                                "note": ("the first requests of the stream submitted at once (closed queue); "
                                         "stage_device_ms_sum adds each request's stage times (CUDA events on its "
                                         "lane's stream), so stages of concurrent requests overlap")}
+    out["small_graph_batch"] = small_graph_batch(dev)
     if args.serve_baseline > 0:
         ids = list(range(min(args.serve_baseline, len(sched["n"]))))
         with Server(budget_bytes=150 * 10**9, max_inflight=1) as base:
@@ -770,6 +818,7 @@ def main():
     ap.add_argument("--serve-lanes", type=int, default=8)
     ap.add_argument("--serve-capacity", type=int, default=2000)
     ap.add_argument("--serve-baseline", type=int, default=250)
+    ap.add_argument("--serve-batch", type=int, default=64, help="most small requests per batch (0: none)")
     args = ap.parse_args()
     wn, wd, wk, _ = WORKLOADS[args.workload]
     args.n = wn if args.n is None else args.n

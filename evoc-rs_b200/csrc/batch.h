@@ -67,11 +67,13 @@ cudaError_t prepare_tc_scan_batch(int mode, int max_keep);
 cudaError_t launch_tc_scan_batch(int mode, BatchHeader* hdr, const ScanJob* jobs, const ScanItem* items,
                                  int max_keep, int grid, uint64_t timeout_ns, cudaStream_t stream);
 
-// batch.cu.  f32 requests: copy + pad into x, prepare_float, BF16 rows into
+// prep.cu.  f32 requests: copy + pad into x, prepare_float, BF16 rows into
 // xb.  i8 requests: copy + pad into xb.
-cudaError_t launch_batch_rows(bool f32, const BatchHeader* hdr, const BatchRowJob* jobs, int sms,
-                              cudaStream_t stream);
-// f32 requests: FP32 rerank of the scan candidates into the outputs.
-cudaError_t launch_batch_rerank(BatchHeader* hdr, const BatchRowJob* jobs, int sms, cudaStream_t stream);
+// Grids are sized by the caller for the batch (grid-stride loops cover any
+// count), so a small batch occupies a few SMs and runs beside other work.
+cudaError_t launch_batch_rows(bool f32, const BatchHeader* hdr, const BatchRowJob* jobs, int grid_rows,
+                              int grid_norms, cudaStream_t stream);
+// rerank.cu.  f32 requests: FP32 rerank of the scan candidates into the outputs.
+cudaError_t launch_batch_rerank(BatchHeader* hdr, const BatchRowJob* jobs, int grid, cudaStream_t stream);
 
 }  // namespace evoc

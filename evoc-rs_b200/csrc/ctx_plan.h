@@ -23,6 +23,8 @@ enum CtxBuf {
   kBufPivots,
   kBufPopc,
   kBufNnd,
+  kBufBatchWs,   // batches: per-request work arena
+  kBufBatchTab,  // batches: device tables
   kBufCount
 };
 
@@ -40,6 +42,12 @@ struct CtxSizes {
 // the form runners pass to DevBuf::ensure.
 void knn_buffer_needs(const evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, int32_t dtype, int64_t n, int64_t dim,
                       int32_t k, CtxSizes* need);
+
+// The buffers evoc_gpu_knn_graph_batch needs for these requests (all other
+// entries zero).  Returns false when the batch path does not take them
+// (dtype/form, k too large).
+bool batch_buffer_needs(const evoc_gpu_opts& opts, int32_t dtype, int32_t n_jobs, const int64_t* n,
+                        const int64_t* dim, int32_t k, CtxSizes* need);
 
 // Allocated size of each of the context's buffers.  Call only from the thread
 // that makes the context's calls.

@@ -74,6 +74,7 @@ struct evoc_gpu_ctx {
     bool f32;
     int keep_odd;
     void* tab;
+    int grids[4];  // rows, norms, scan, rerank
     cudaGraphExec_t exec;
   };
   std::vector<BatchGraph> batch_graphs;  // captured batch pipelines, replayed per batch
@@ -892,14 +893,27 @@ int knn_batch_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtyp
   auto* d_it = reinterpret_cast<const evoc::ScanItem*>(T + L.off_it);
   const int mode = f32 ? evoc::kScanBf16 : evoc::kScanInt8;
   EVOC_TRY(evoc::prepare_tc_scan_batch(mode, L.max_keep), "batch scan attributes");
-  // The table offsets depend on n_jobs; the graph is keyed on everything its
+  // Grids sized for this batch (rounded up to a power of two, so few distinct
+  // launch configurations occur): a small batch takes a few SMs and runs
+  // beside the other lanes' work instead of waiting for every SM.
+  auto bucket = [](int64_t v, int64_t cap) {
+    int64_t b = 1;
+    while (b < v && b < cap) b <<= 1;
+    return int(b < cap ? b : cap);
+  };
+  int64_t words = 0;
+  for (const BatchJobPlan& J : L.jobs) words += f32 ? J.rows * J.ld : J.rows * J.ldb / 4;
+  const int grids[4] = {bucket((words + 255) / 256, int64_t(ctx->sms) * 8),
+                        bucket(L.total_blocks, int64_t(ctx->sms) * 8), bucket(L.n_items, ctx->sms),
+                        bucket((L.total_rows + 7) / 8, int64_t(ctx->sms) * 16)};
+  // The table offsets are fixed; the graph is keyed on everything else its
   // launch parameters hold.
   const int keep_odd = L.max_keep | 1;
   auto launch_all = [&](cudaStream_t st) -> cudaError_t {
-    cudaError_t e = evoc::launch_batch_rows(f32, d_hdr, d_rj, ctx->sms, st);
+    cudaError_t e = evoc::launch_batch_rows(f32, d_hdr, d_rj, grids[0], grids[1], st);
     if (e == cudaSuccess)
-      e = evoc::launch_tc_scan_batch(mode, d_hdr, d_sj, d_it, L.max_keep, ctx->sms, ctx->timeout_ns, st);
-    if (e == cudaSuccess && f32) e = evoc::launch_batch_rerank(d_hdr, d_rj, ctx->sms, st);
+      e = evoc::launch_tc_scan_batch(mode, d_hdr, d_sj, d_it, L.max_keep, grids[2], ctx->timeout_ns, st);
+    if (e == cudaSuccess && f32) e = evoc::launch_batch_rerank(d_hdr, d_rj, grids[3], st);
     return e;
   };
   ctx->launches += f32 ? 6 : 2;
@@ -915,7 +929,9 @@ int knn_batch_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtyp
     }
     cudaGraphExec_t exec = nullptr;
     for (const auto& g : ctx->batch_graphs)
-      if (g.f32 == f32 && g.keep_odd == keep_odd && g.tab == ctx->batch_tab.p) exec = g.exec;
+      if (g.f32 == f32 && g.keep_odd == keep_odd && g.tab == ctx->batch_tab.p &&
+          std::equal(grids, grids + 4, g.grids))
+        exec = g.exec;
     if (!exec) {
       cudaGraph_t graph = nullptr;
       EVOC_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal), "begin batch capture");
@@ -929,7 +945,7 @@ int knn_batch_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtyp
       const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
       cudaGraphDestroy(graph);
       EVOC_TRY(ie, "instantiate batch graph");
-      ctx->batch_graphs.push_back({f32, keep_odd, ctx->batch_tab.p, exec});
+      ctx->batch_graphs.push_back({f32, keep_odd, ctx->batch_tab.p, {grids[0], grids[1], grids[2], grids[3]}, exec});
     }
     EVOC_TRY(cudaGraphLaunch(exec, ctx->stream), "launch batch graph");
   } else {
@@ -1141,10 +1157,25 @@ void knn_buffer_needs(const evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, int32_
   }
 }
 
+bool batch_buffer_needs(const evoc_gpu_opts& opts, int32_t dtype, int32_t n_jobs, const int64_t* n,
+                        const int64_t* dim, int32_t k, CtxSizes* need) {
+  *need = CtxSizes{};
+  const int form = resolve_form(dtype, opts.form);
+  const bool f32 = dtype == EVOC_DTYPE_F32;
+  if (!((f32 && form == EVOC_FORM_BF16_RERANK) || (dtype == EVOC_DTYPE_I8 && form == EVOC_FORM_EXACT_INT)))
+    return false;
+  if (n_jobs <= 0 || n_jobs > kBatchMaxJobs || k <= 0) return false;
+  BatchLayout L;
+  if (batch_layout(f32, opts, n_jobs, n, dim, k, &L) != EVOC_OK || L.max_keep > kBatchMaxKeep) return false;
+  need->b[kBufBatchWs] = L.ws_bytes;
+  need->b[kBufBatchTab] = L.tab_bytes;
+  return true;
+}
+
 void ctx_buffer_sizes(const evoc_gpu_ctx* ctx, CtxSizes* cur) {
-  const DevBuf* bufs[kBufCount] = {&ctx->x,      &ctx->scratch, &ctx->norms, &ctx->flag,   &ctx->xb,
-                                   &ctx->cand,   &ctx->labels,  &ctx->order, &ctx->hist,   &ctx->cursor,
-                                   &ctx->pivots, &ctx->popc,    &ctx->nnd_work};
+  const DevBuf* bufs[kBufCount] = {&ctx->x,      &ctx->scratch, &ctx->norms,    &ctx->flag,     &ctx->xb,
+                                   &ctx->cand,   &ctx->labels,  &ctx->order,    &ctx->hist,     &ctx->cursor,
+                                   &ctx->pivots, &ctx->popc,    &ctx->nnd_work, &ctx->batch_ws, &ctx->batch_tab};
   for (int i = 0; i < kBufCount; i++) cur->b[i] = bufs[i]->bytes;
 }
 
@@ -1159,10 +1190,12 @@ void ctx_release_buffers(evoc_gpu_ctx* ctx) {
   std::lock_guard<std::mutex> lock(ctx->mu);
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
-  DevBuf* bufs[kBufCount] = {&ctx->x,      &ctx->scratch, &ctx->norms, &ctx->flag,   &ctx->xb,
-                             &ctx->cand,   &ctx->labels,  &ctx->order, &ctx->hist,   &ctx->cursor,
-                             &ctx->pivots, &ctx->popc,    &ctx->nnd_work};
+  DevBuf* bufs[kBufCount] = {&ctx->x,      &ctx->scratch, &ctx->norms,    &ctx->flag,     &ctx->xb,
+                             &ctx->cand,   &ctx->labels,  &ctx->order,    &ctx->hist,     &ctx->cursor,
+                             &ctx->pivots, &ctx->popc,    &ctx->nnd_work, &ctx->batch_ws, &ctx->batch_tab};
   for (DevBuf* b : bufs) b->release();
+  for (auto& g : ctx->batch_graphs) cudaGraphExecDestroy(g.exec);  // they name the freed tables
+  ctx->batch_graphs.clear();
 }
 
 }  // namespace evoc

@@ -224,13 +224,13 @@ __global__ void batch_to_bf16_kernel(const BatchHeader* __restrict__ hdr, const 
   }
 }
 
-cudaError_t launch_batch_rows(bool f32, const BatchHeader* hdr, const BatchRowJob* jobs, int sms,
-                              cudaStream_t stream) {
-  batch_copy_kernel<<<sms * 8, 256, 0, stream>>>(hdr, jobs, f32);
+cudaError_t launch_batch_rows(bool f32, const BatchHeader* hdr, const BatchRowJob* jobs, int grid_rows,
+                              int grid_norms, cudaStream_t stream) {
+  batch_copy_kernel<<<grid_rows, 256, 0, stream>>>(hdr, jobs, f32);
   if (!f32) return cudaGetLastError();
-  batch_row_norms_kernel<<<sms * 8, kRows, 0, stream>>>(hdr, jobs);
-  batch_normalize_kernel<<<sms * 8, 256, 0, stream>>>(hdr, jobs);
-  batch_to_bf16_kernel<<<sms * 8, 256, 0, stream>>>(hdr, jobs);
+  batch_row_norms_kernel<<<grid_norms, kRows, 0, stream>>>(hdr, jobs);
+  batch_normalize_kernel<<<grid_rows, 256, 0, stream>>>(hdr, jobs);
+  batch_to_bf16_kernel<<<grid_rows, 256, 0, stream>>>(hdr, jobs);
   return cudaGetLastError();
 }
 

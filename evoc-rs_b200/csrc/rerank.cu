@@ -215,8 +215,8 @@ cudaError_t launch_rerank_f32(const float* X, int ld, int d, int64_t n, int64_t 
   return cudaGetLastError();
 }
 
-cudaError_t launch_batch_rerank(BatchHeader* hdr, const BatchRowJob* jobs, int sms, cudaStream_t stream) {
-  batch_rerank_kernel<<<unsigned(sms * 16), RW * 32, 0, stream>>>(hdr, jobs);
+cudaError_t launch_batch_rerank(BatchHeader* hdr, const BatchRowJob* jobs, int grid, cudaStream_t stream) {
+  batch_rerank_kernel<<<unsigned(grid), RW * 32, 0, stream>>>(hdr, jobs);
   return cudaGetLastError();
 }
 

@@ -65,7 +65,10 @@ struct Job {
   float* d_dist = nullptr;
   int64_t row_bytes_total = 0;  // n*dim*size(dtype) when the server copies the rows in
   int64_t out_bytes = 0;        // n*k_eff*8
-  evoc::CtxSizes need;          // context buffers the request needs
+  evoc::CtxSizes need;          // context buffers the request needs alone
+  bool batch_ok = false;        // small enough for a multi-request batch
+  int32_t form = 0;             // resolved form
+  double work = 0.0;            // 2 n^2 dim: the scan's operations
   int64_t held = 0;             // bytes counted against the budget right now
   int skipped = 0;              // times a later request was admitted first
   int state = kPending;
@@ -82,6 +85,17 @@ int64_t elem_size(int32_t dtype) { return dtype == EVOC_DTYPE_F32 ? 4 : 1; }
 // A request passed over this many times by later, smaller ones reserves the
 // next admission: first fit without starvation.
 constexpr int kMaxSkips = 16;
+
+// Small requests (f32 BF16+rerank, i8 exact) are admitted together and built
+// by one evoc_gpu_knn_graph_batch call: up to kBatchJobs requests of at most
+// kBatchRows rows each, and at most kBatchWork scan operations in all, so a
+// batch stays a few milliseconds long.
+constexpr int64_t kBatchRows = 16384;
+constexpr int kBatchJobs = 64;
+constexpr double kBatchWork = 4e12;
+// A batch forms only under backlog: at least this many compatible small
+// requests pending.  With fewer, each runs alone at its lowest latency.
+constexpr int kBatchMin = 4;
 
 }  // namespace
 
@@ -111,6 +125,8 @@ struct evoc_gpu_server {
   std::vector<std::string> stage_names;            // first-seen order
   std::unordered_map<std::string, std::pair<double, int64_t>> stage_totals;
   double lane_busy_ms = 0.0;
+  int64_t batches = 0, batched = 0;  // multi-request calls and the requests they carried
+  int batch_max = kBatchJobs;
 };
 
 namespace {
@@ -141,42 +157,74 @@ void finish_locked(evoc_gpu_server* s, Job* j, int state, int status, const std:
   s->cv_done.notify_all();
 }
 
-void run_job(evoc_gpu_server* s, int lane, Job* j) {
-  evoc_gpu_ctx* ctx = s->ctxs[size_t(lane)];
-  cudaStream_t st = s->streams[size_t(lane)];
-  nvtxRangePushA("evoc_job");
-  int rc = EVOC_OK;
-  std::string err;
+// Allocates a request's device buffers on the lane's stream and queues the
+// copy of its rows; *rows receives the device rows.
+cudaError_t stage_job(evoc_gpu_server* s, cudaStream_t st, Job* j, const void** rows) {
   const size_t out_elems = size_t(j->n) * size_t(j->keff);
   cudaError_t e = cudaSuccess;
-  const void* rows = j->src;
+  *rows = j->src;
   if (!j->src_on_device) {
     e = cudaMallocFromPoolAsync(&j->d_rows, size_t(j->row_bytes_total), s->pool, st);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(j->d_rows, j->src, size_t(j->row_bytes_total), cudaMemcpyHostToDevice, st);
-    rows = j->d_rows;
+    *rows = j->d_rows;
   }
   if (e == cudaSuccess) e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&j->d_idx), out_elems * 4, s->pool, st);
   if (e == cudaSuccess) e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&j->d_dist), out_elems * 4, s->pool, st);
-  if (e != cudaSuccess) {
-    rc = e == cudaErrorMemoryAllocation ? EVOC_ERR_OOM : EVOC_ERR_CUDA;
-    err = std::string("serving: ") + cudaGetErrorString(e);
-    cudaGetLastError();
-  } else {
-    evoc_gpu_opts o = j->opts;
-    o.buffers_on_device = 1;
-    int32_t kout = 0;
-    rc = evoc_gpu_knn_graph(ctx, &o, j->dtype, rows, j->n, j->dim, j->k, j->has_tau ? j->tau : nullptr, j->d_idx,
-                            j->d_dist, &kout);
-    if (rc != EVOC_OK)
-      err = std::string(evoc_gpu_last_error(ctx)) + " [request n=" + std::to_string(j->n) +
-            " dim=" + std::to_string(j->dim) + " dtype=" + std::to_string(j->dtype) +
-            " form=" + std::to_string(j->opts.form) + " lane=" + std::to_string(lane) + "]";
+  return e;
+}
+
+std::string tag(const Job* j, int lane, size_t batch) {
+  return " [request n=" + std::to_string(j->n) + " dim=" + std::to_string(j->dim) +
+         " dtype=" + std::to_string(j->dtype) + " form=" + std::to_string(j->opts.form) +
+         " lane=" + std::to_string(lane) + (batch > 1 ? " batch of " + std::to_string(batch) : "") + "]";
+}
+
+// Builds the graphs of `group` on the lane: one request through
+// evoc_gpu_knn_graph, or a batch of small ones through evoc_gpu_knn_graph_batch.
+void run_work(evoc_gpu_server* s, int lane, const std::vector<Job*>& group, bool batch) {
+  evoc_gpu_ctx* ctx = s->ctxs[size_t(lane)];
+  cudaStream_t st = s->streams[size_t(lane)];
+  nvtxRangePushA(batch ? "evoc_batch" : "evoc_job");
+  const size_t m = group.size();
+  int rc = EVOC_OK;
+  std::string err;
+  std::vector<const void*> rows(m, nullptr);
+  for (size_t i = 0; i < m && rc == EVOC_OK; i++) {
+    const cudaError_t e = stage_job(s, st, group[i], &rows[i]);
+    if (e != cudaSuccess) {
+      rc = e == cudaErrorMemoryAllocation ? EVOC_ERR_OOM : EVOC_ERR_CUDA;
+      err = std::string("serving: ") + cudaGetErrorString(e);
+      cudaGetLastError();
+    }
   }
-  // evoc_gpu_knn_graph returns after its stream is idle, so the rows are no
+  if (rc == EVOC_OK) {
+    const Job* j0 = group.front();
+    evoc_gpu_opts o = j0->opts;
+    o.buffers_on_device = 1;
+    if (batch) {
+      std::vector<int64_t> n(m), dim(m);
+      std::vector<int32_t*> idx(m);
+      std::vector<float*> dist(m);
+      for (size_t i = 0; i < m; i++) {
+        n[i] = group[i]->n;
+        dim[i] = group[i]->dim;
+        idx[i] = group[i]->d_idx;
+        dist[i] = group[i]->d_dist;
+      }
+      rc = evoc_gpu_knn_graph_batch(ctx, &o, j0->dtype, int32_t(m), rows.data(), n.data(), dim.data(), j0->k,
+                                    idx.data(), dist.data(), nullptr, nullptr);
+    } else {
+      int32_t kout = 0;
+      rc = evoc_gpu_knn_graph(ctx, &o, j0->dtype, rows[0], j0->n, j0->dim, j0->k, j0->has_tau ? j0->tau : nullptr,
+                              j0->d_idx, j0->d_dist, &kout);
+    }
+    if (rc != EVOC_OK) err = std::string(evoc_gpu_last_error(ctx)) + tag(j0, lane, m);
+  }
+  // The graph calls return after their stream is idle, so the rows are no
   // longer read; on an error path wait for the copies before freeing.
   if (rc != EVOC_OK) cudaStreamSynchronize(st);
-  std::vector<uint8_t>().swap(j->host_copy);
+  for (Job* j : group) std::vector<uint8_t>().swap(j->host_copy);
   nvtxRangePop();
   evoc::CtxSizes actual;
   evoc::ctx_buffer_sizes(ctx, &actual);
@@ -189,8 +237,12 @@ void run_job(evoc_gpu_server* s, int lane, Job* j) {
   }
   const int64_t t_end = now_ns();
   std::lock_guard<std::mutex> lock(s->mu);
-  s->running--;
-  s->lane_busy_ms += double(t_end - j->t_admit) * 1e-6;
+  s->running -= int64_t(m);
+  s->lane_busy_ms += double(t_end - group.front()->t_admit) * 1e-6;
+  if (batch) {
+    s->batches++;
+    s->batched += int64_t(m);
+  }
   for (const auto& st_ms : stages) {
     auto it = s->stage_totals.find(st_ms.first);
     if (it == s->stage_totals.end()) {
@@ -207,22 +259,85 @@ void run_job(evoc_gpu_server* s, int lane, Job* j) {
   s->in_use += int64_t(actual.total()) - planned;
   s->lane_sizes[size_t(lane)] = actual;
   s->peak = std::max(s->peak, s->in_use);
-  if (j->d_rows) {
-    cudaFreeAsync(j->d_rows, s->free_stream);
-    j->d_rows = nullptr;
+  for (Job* j : group) {
+    if (j->d_rows) {
+      cudaFreeAsync(j->d_rows, s->free_stream);
+      j->d_rows = nullptr;
+    }
+    s->in_use -= j->row_bytes_total;
+    j->held -= j->row_bytes_total;
+    if (j->cancel) {
+      free_job_memory_locked(s, j);
+      finish_locked(s, j, kCancelled, EVOC_ERR_CANCELLED, "cancelled");
+    } else if (rc != EVOC_OK) {
+      free_job_memory_locked(s, j);
+      finish_locked(s, j, kFailed, rc, err);
+    } else {
+      finish_locked(s, j, kDone, EVOC_OK, "");
+    }
   }
-  s->in_use -= j->row_bytes_total;
-  j->held -= j->row_bytes_total;
   s->cv_work.notify_all();
-  if (j->cancel) {
-    free_job_memory_locked(s, j);
-    finish_locked(s, j, kCancelled, EVOC_ERR_CANCELLED, "cancelled");
-  } else if (rc != EVOC_OK) {
-    free_job_memory_locked(s, j);
-    finish_locked(s, j, kFailed, rc, err);
-  } else {
-    finish_locked(s, j, kDone, EVOC_OK, "");
+}
+
+bool batch_compatible(const Job* a, const Job* b) {
+  return b->batch_ok && a->dtype == b->dtype && a->k == b->k && a->form == b->form &&
+         a->opts.oversample == b->opts.oversample;
+}
+
+// Buffers a batch of `group` needs on a lane (plan of evoc_gpu_knn_graph_batch).
+evoc::CtxSizes batch_need(evoc_gpu_server* s, const std::vector<Job*>& group) {
+  std::vector<int64_t> n, dim;
+  for (const Job* j : group) {
+    n.push_back(j->n);
+    dim.push_back(j->dim);
   }
+  evoc::CtxSizes need;
+  evoc::batch_buffer_needs(group.front()->opts, group.front()->dtype, int32_t(group.size()), n.data(), dim.data(),
+                           group.front()->k, &need);
+  (void)s;
+  return need;
+}
+
+// Under backlog, admits the small request at `it` with compatible pending
+// ones after it as one batch (first fit for each addition).  Returns false,
+// admitting nothing, when fewer than kBatchMin would go together.
+bool try_admit_batch(evoc_gpu_server* s, std::deque<std::shared_ptr<Job>>::iterator it, evoc::CtxSizes& mine,
+                     std::vector<std::shared_ptr<Job>>* group) {
+  Job* j = it->get();
+  std::vector<Job*> cand{j};
+  evoc::CtxSizes grown = evoc::grown_sizes(mine, batch_need(s, cand));
+  int64_t held = j->row_bytes_total + j->out_bytes;
+  if (s->in_use + held + int64_t(grown.total()) - int64_t(mine.total()) > s->budget) return false;
+  double work = j->work;
+  for (auto jt = std::next(it); jt != s->pending.end() && int(cand.size()) < s->batch_max; ++jt) {
+    Job* o = jt->get();
+    if (!batch_compatible(j, o) || work + o->work > kBatchWork) continue;
+    cand.push_back(o);
+    const evoc::CtxSizes g2 = evoc::grown_sizes(mine, batch_need(s, cand));
+    const int64_t h2 = held + o->row_bytes_total + o->out_bytes;
+    if (s->in_use + h2 + int64_t(g2.total()) - int64_t(mine.total()) > s->budget) {
+      cand.pop_back();
+      continue;
+    }
+    grown = g2;
+    held = h2;
+    work += o->work;
+  }
+  if (int(cand.size()) < kBatchMin) return false;
+  if (it != s->pending.begin()) s->pending.front()->skipped++;
+  s->in_use += held + int64_t(grown.total()) - int64_t(mine.total());
+  for (Job* c : cand) {
+    for (auto kt = s->pending.begin(); kt != s->pending.end(); ++kt)
+      if (kt->get() == c) {
+        group->push_back(*kt);
+        s->pending.erase(kt);
+        break;
+      }
+    c->held = c->row_bytes_total + c->out_bytes;
+  }
+  mine = grown;
+  s->peak = std::max(s->peak, s->in_use);
+  return true;
 }
 
 void worker(evoc_gpu_server* s, int lane) {
@@ -230,19 +345,25 @@ void worker(evoc_gpu_server* s, int lane) {
   evoc::CtxSizes& mine = s->lane_sizes[size_t(lane)];
   std::unique_lock<std::mutex> lock(s->mu);
   for (;;) {
-    std::shared_ptr<Job> pick;
+    std::vector<std::shared_ptr<Job>> group;
+    bool batch = false;
     bool trim = false;
     while (!s->stopping) {
       // First fit over the pending requests, oldest first; a request skipped
-      // kMaxSkips times holds the next admission for itself.
+      // kMaxSkips times holds the next admission for itself.  A small request
+      // takes compatible small ones after it into the same batch.
       for (auto it = s->pending.begin(); it != s->pending.end(); ++it) {
         Job* j = it->get();
+        if (j->batch_ok && s->batch_max > 1 && try_admit_batch(s, it, mine, &group)) {
+          batch = true;
+          break;
+        }
         const evoc::CtxSizes grown = evoc::grown_sizes(mine, j->need);
         const int64_t grow = int64_t(grown.total()) - int64_t(mine.total());
         const int64_t need = j->row_bytes_total + j->out_bytes + grow;
         if (s->in_use + need <= s->budget) {
           if (it != s->pending.begin()) s->pending.front()->skipped++;
-          pick = *it;
+          group.push_back(*it);
           s->pending.erase(it);
           s->in_use += need;
           j->held = j->row_bytes_total + j->out_bytes;
@@ -252,7 +373,7 @@ void worker(evoc_gpu_server* s, int lane) {
         }
         if (it == s->pending.begin() && j->skipped >= kMaxSkips) break;
       }
-      if (pick) break;
+      if (!group.empty()) break;
       // Nothing fits.  An idle lane whose own buffers keep the oldest request
       // out gives them back.
       if (!s->pending.empty() && mine.total() > 0) {
@@ -275,13 +396,19 @@ void worker(evoc_gpu_server* s, int lane) {
       s->cv_work.notify_all();
       continue;
     }
-    if (!pick) return;
-    pick->state = kRunning;
-    pick->lane = lane;
-    pick->t_admit = now_ns();
-    s->running++;
+    if (group.empty()) return;
+    const int64_t t_admit = now_ns();
+    std::vector<Job*> jobs;
+    for (auto& g : group) {
+      g->state = kRunning;
+      g->lane = lane;
+      g->t_admit = t_admit;
+      jobs.push_back(g.get());
+    }
+    s->running += int64_t(jobs.size());
     lock.unlock();
-    run_job(s, lane, pick.get());
+    run_work(s, lane, jobs, batch);
+    group.clear();
     lock.lock();
   }
 }
@@ -327,6 +454,7 @@ void evoc_gpu_server_default_opts(evoc_gpu_server_opts* o) {
   o->device = 0;
   o->budget_bytes = int64_t(150) * 1000 * 1000 * 1000;
   o->max_inflight = 4;
+  o->batch_max = kBatchJobs;
 }
 
 int evoc_gpu_server_create(const evoc_gpu_server_opts* opts, evoc_gpu_server** out) {
@@ -357,6 +485,7 @@ int evoc_gpu_server_create(const evoc_gpu_server_opts* opts, evoc_gpu_server** o
     return rc;
   };
   s->profile = o.profile != 0;
+  s->batch_max = std::min(std::max(o.batch_max, 0), kBatchJobs);
   for (int i = 0; i < s->lanes; i++) {
     evoc_gpu_ctx* c = nullptr;
     const int rc = evoc_gpu_ctx_create(o.device, &c);
@@ -440,6 +569,16 @@ int evoc_gpu_server_submit(evoc_gpu_server* s, const evoc_gpu_opts* opts, int32_
   j->row_bytes_total = j->src_on_device ? 0 : in_bytes;
   j->out_bytes = n * int64_t(j->keff) * 8;
   evoc::knn_buffer_needs(s->ctxs[0], j->opts, dtype, n, dim, k, &j->need);
+  j->form = j->opts.form == EVOC_FORM_AUTO
+                ? (dtype == EVOC_DTYPE_F32 ? EVOC_FORM_BF16_RERANK : EVOC_FORM_EXACT_INT)
+                : j->opts.form;
+  j->work = 2.0 * double(n) * double(n) * double(dim);
+  {
+    evoc::CtxSizes bneed;
+    const int64_t n1 = n, d1 = dim;
+    // (the batched forms do not read the tau seed)
+    j->batch_ok = n <= kBatchRows && evoc::batch_buffer_needs(j->opts, dtype, 1, &n1, &d1, k, &bneed);
+  }
   const int64_t alone = int64_t(evoc::grown_sizes(evoc::CtxSizes{}, j->need).total());
   if (j->row_bytes_total + j->out_bytes + alone > s->budget) {
     std::lock_guard<std::mutex> lock(s->mu);
@@ -647,6 +786,8 @@ int evoc_gpu_server_stats(evoc_gpu_server* s, evoc_gpu_server_counters* out) {
   out->workspace_bytes = ws;
   out->workspace_misses = s->ws_misses;
   out->lanes = s->lanes;
+  out->batches = s->batches;
+  out->batched = s->batched;
   return EVOC_OK;
 }
 

@@ -127,14 +127,15 @@ class ServerOpts(C.Structure):
         ("budget_bytes", C.c_int64),
         ("max_inflight", C.c_int32),
         ("profile", C.c_int32),
-        ("reserved", C.c_int32 * 4),
+        ("batch_max", C.c_int32),
+        ("reserved", C.c_int32 * 3),
     ]
 
 
 class ServerCounters(C.Structure):
     _fields_ = [(name, C.c_int64) for name in (
         "submitted", "completed", "failed", "cancelled", "rejected", "pending", "running", "bytes_in_use",
-        "peak_bytes", "budget_bytes", "workspace_bytes", "workspace_misses", "lanes")]
+        "peak_bytes", "budget_bytes", "workspace_bytes", "workspace_misses", "lanes", "batches", "batched")]
 
 
 class JobInfo(C.Structure):

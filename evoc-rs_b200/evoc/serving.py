@@ -33,7 +33,7 @@ class Server:
     """One evoc_gpu_server on one device."""
 
     def __init__(self, budget_bytes: int = 150 * 10**9, max_inflight: int = 4, device: int = 0,
-                 profile: bool = False):
+                 profile: bool = False, batch_max: int = 64):
         L = _lib.lib()
         o = _lib.ServerOpts()
         L.evoc_gpu_server_default_opts(C.byref(o))
@@ -41,6 +41,7 @@ class Server:
         o.budget_bytes = int(budget_bytes)
         o.max_inflight = int(max_inflight)
         o.profile = 1 if profile else 0
+        o.batch_max = int(batch_max)
         self.h = C.c_void_p()
         rc = L.evoc_gpu_server_create(C.byref(o), C.byref(self.h))
         if rc != _lib.EVOC_OK:

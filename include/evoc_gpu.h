@@ -218,7 +218,11 @@ int evoc_gpu_knn_f32_noalloc(const float* rows, int64_t n, int64_t ld, int32_t k
  * + n*k_eff*8 for the graph + what the lane's buffers must grow by for that
  * shape (lane buffers are kept between requests and counted once; an idle lane
  * frees them when they alone keep the oldest request out).  A request passed
- * over 16 times by later ones is admitted next.  The rows go back to the
+ * over 16 times by later ones is admitted next.  Under backlog -- at least 4
+ * compatible small requests pending (f32 with the BF16+rerank form or i8 with
+ * the exact form, at most 16,384 rows; same dtype, k and form) -- they are
+ * admitted together (up to batch_max requests and 4e12 scan operations) and
+ * built by one evoc_gpu_knn_graph_batch call; otherwise each runs alone.  The rows go back to the
  * budget once the graph is built; the graph stays resident in HBM until it is
  * fetched without keep_resident or released.  Every job id must end in
  * evoc_gpu_server_result (without keep_resident) or evoc_gpu_server_release.
@@ -233,7 +237,9 @@ typedef struct {
                          /* default 4                                       */
   int32_t profile;       /* 1: time every request's stages with CUDA events */
                          /* and keep per-stage totals (server_stage)        */
-  int32_t reserved[4];
+  int32_t batch_max;     /* most small requests in one batch; 0 or 1: no    */
+                         /* batching; default 64                            */
+  int32_t reserved[3];
 } evoc_gpu_server_opts;
 
 typedef struct {
@@ -245,6 +251,8 @@ typedef struct {
   int64_t workspace_bytes; /* lane contexts' buffers, counted in bytes_in_use */
   int64_t workspace_misses;/* requests whose buffers outgrew the plan       */
   int64_t lanes;
+  int64_t batches;         /* multi-request calls (small requests together)  */
+  int64_t batched;         /* requests those calls carried                   */
 } evoc_gpu_server_counters;
 
 typedef struct {

@@ -84,6 +84,23 @@ def test_same_result_alone_and_in_the_mix(alone, lanes):
         assert st["bytes_in_use"] == st["workspace_bytes"] and st["peak_bytes"] <= st["budget_bytes"]
 
 
+def test_small_requests_are_batched_with_identical_results():
+    """Many small requests submitted together are built in multi-request
+    batches; each graph equals the one built alone."""
+    xs = [(_f32(300 + 53 * i, 32 + 16 * (i % 4), 90 + i) if i % 3 else _i8(400 + 31 * i, 128, 90 + i))
+          for i in range(40)]
+    forms = ["exact_int" if x.dtype == np.int8 else "bf16_rerank" for x in xs]
+    want = [evoc.knn_graph(x, _opts(f, 15)) for x, f in zip(xs, forms)]
+    with Server(max_inflight=2) as srv:
+        jobs = [srv.submit(x, _opts(f, 15)) for x, f in zip(xs, forms)]
+        got = [srv.result(j) for j in jobs]
+        st = srv.stats()
+    assert st["batches"] >= 1 and st["batched"] > st["batches"], st
+    assert st["workspace_misses"] == 0
+    for (gi, gd), (wi, wd) in zip(got, want):
+        assert np.array_equal(gi, wi) and np.array_equal(gd.view(np.uint32), wd.view(np.uint32))
+
+
 def test_requests_overlap_on_the_device():
     """With four lanes, requests submitted together run at the same time."""
     xs = [_f32(20000, 256, 20 + i) for i in range(8)]
