@@ -513,6 +513,7 @@ def run_exact_int(args, world, rank, local):
     ctx.profile(True)
     stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=dev)
     opts = evoc.KnnGraphOptions(n_neighbors=k, form="exact_int", device=local)
+    tuned = evoc.autotune("Int8" if i8 else "UInt8", n, d, k, "exact_int", device=local) if args.autotune else None
 
     def step():
         evoc.knn_graph_device(x.data_ptr(), code, n, d, k, oi.data_ptr(), od.data_ptr(), opts,
@@ -605,6 +606,7 @@ def run_exact_int(args, world, rank, local):
                    "l2": f"inputs larger than L2 ({x.numel() / 1e9:.2f} GB vs 126 MB)",
                    "per_rank": "independent graph per rank"},
         "sampled_exact_check": check,
+        "autotune": tuned and {"variants_ms_65536_rows": tuned["variants_ms"], "chosen": tuned["chosen"]},
         "stages_ms": {kname: statistics.mean(v) for kname, v in stage_ms.items()},
         "roofline": roofline,
         "e2e": {"value": world * n * k / (e2e_ms / 1000.0), "unit": UNIT, "h2d_bytes_per_step": int(x.numel()),
@@ -647,6 +649,7 @@ def run_ours(args, world, rank, local):
     ctx.profile(True)
     stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=dev)
     opts = evoc.KnnGraphOptions(n_neighbors=k, form="bf16_rerank", oversample=2, device=local)
+    tuned = evoc.autotune("Float32", n, d, k, "bf16_rerank", device=local) if args.autotune else None
 
     def step():
         evoc.knn_graph_device(x.data_ptr(), 0, n, d, k, oi.data_ptr(), od.data_ptr(), opts)
@@ -782,6 +785,7 @@ def run_ours(args, world, rank, local):
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n * d * 4, "d2h_bytes_per_step": n * k * 8,
                 "ms_per_step": e2e_ms, "matches_device_path": e2e_consistent},
         "fp32_form": fp32,
+        "autotune": tuned and {"variants_ms_65536_rows": tuned["variants_ms"], "chosen": tuned["chosen"]},
         "cpu_baseline": cpu,
         "clocks": clk,
         "gpu_launches": launches,
@@ -809,6 +813,7 @@ def main():
     ap.add_argument("--dim", type=int, default=None, help="features (f32, i8) or bytes per row (bits)")
     ap.add_argument("--k", type=int, default=None)
     ap.add_argument("--check-rows", type=int, default=128)
+    ap.add_argument("--autotune", type=int, default=1, help="tune the scan's kernel variant before timing")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--fp32-rows", type=int, default=75_776)  # 2 full waves of 296 CTAs x 128 rows
     ap.add_argument("--recall-rows", type=int, default=10_000)

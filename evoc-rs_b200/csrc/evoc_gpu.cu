@@ -10,7 +10,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <fstream>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -79,6 +82,8 @@ struct evoc_gpu_ctx {
   };
   std::vector<BatchGraph> batch_graphs;  // captured batch pipelines, replayed per batch
   bool use_graphs = true;                // EVOC_NO_GRAPHS=1 launches the kernels directly
+  // Autotuned scan variants: (scan mode, keep, row bytes, floor(log2 n)) -> variant.
+  std::map<std::tuple<int, int, int64_t, int>, int> tune;
   uint64_t timeout_ns = 4000000000ull;  // longest a pipeline wait inside a kernel may take
   bool sync_check = false;  // EVOC_SYNC_CHECK=1: wait for and check every kernel stage (fault diagnosis)
   bool profiling = false;
@@ -162,6 +167,21 @@ int stage_rows(evoc_gpu_ctx* ctx, const void* data, int64_t n, int64_t row_bytes
                              cudaMemcpyHostToDevice, ctx->stream),
            "upload rows");
   return EVOC_OK;
+}
+
+int ilog2(int64_t v) {
+  int l = 0;
+  while (v > 1) {
+    v >>= 1;
+    l++;
+  }
+  return l;
+}
+
+// The autotuned scan variant for this shape, or -1 (automatic).
+int tuned_variant(const evoc_gpu_ctx* ctx, int mode, int keep, int64_t row_bytes, int64_t n) {
+  auto it = ctx->tune.find(std::make_tuple(mode, keep, row_bytes, ilog2(n)));
+  return it == ctx->tune.end() ? -1 : it->second;
 }
 
 int scan_grid(const evoc_gpu_ctx* ctx, int64_t n_q) {
@@ -256,7 +276,8 @@ int run_bf16_rerank(evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, const Job& j, 
     EVOC_TRY(ctx->scratch.ensure(size_t(grid) * 256 * size_t(C) * 8), "alloc scratch");
     EVOC_TRY(evoc::launch_tc_scan(evoc::kScanBf16, ctx->xb.p, rows, j.r0, j.nq, ctx->xb.p, rows, j.n, ldb * 2, int(C),
                                   ctx->scratch.as<uint64_t>(), grid, 1, 0, 0, ctx->cand.as<int32_t>(), nullptr,
-                                  nullptr, j.status, ctx->timeout_ns, nullptr, ctx->stream),
+                                  nullptr, j.status, ctx->timeout_ns, nullptr, ctx->stream,
+                                  tuned_variant(ctx, evoc::kScanBf16, int(C), ldb * 2, j.n)),
              "bf16 scan");
     ctx->launches += 1;
   }
@@ -281,7 +302,8 @@ int run_int8(evoc_gpu_ctx* ctx, const Job& j, int64_t ldb) {
   EVOC_TRY(ctx->scratch.ensure(size_t(grid) * 256 * size_t(j.keff) * 8), "alloc scratch");
   EVOC_TRY(evoc::launch_tc_scan(evoc::kScanInt8, ctx->x.p, rows, j.r0, j.nq, ctx->x.p, rows, j.n, ldb, j.keff,
                                 ctx->scratch.as<uint64_t>(), grid, 1, 1, EVOC_DTYPE_I8, j.idx, j.raw, j.dist, j.status,
-                                ctx->timeout_ns, nullptr, ctx->stream),
+                                ctx->timeout_ns, nullptr, ctx->stream,
+                                tuned_variant(ctx, evoc::kScanInt8, j.keff, ldb, j.n)),
            "int8 scan");
   ctx->launches += 1;
   return EVOC_OK;
@@ -310,7 +332,8 @@ int run_jaccard_tc(evoc_gpu_ctx* ctx, const Job& j, int64_t ldb, int64_t nbytes)
   EVOC_TRY(ctx->scratch.ensure(size_t(grid) * 256 * size_t(j.keff) * 8), "alloc scratch");
   EVOC_TRY(evoc::launch_tc_scan(evoc::kScanJaccard, ctx->xb.p, rows, j.r0, j.nq, ctx->xb.p, rows, j.n, lde, j.keff,
                                 ctx->scratch.as<uint64_t>(), grid, 1, 1, EVOC_DTYPE_U8, j.idx, j.raw, j.dist, j.status,
-                                ctx->timeout_ns, ctx->popc.as<int32_t>(), ctx->stream),
+                                ctx->timeout_ns, ctx->popc.as<int32_t>(), ctx->stream,
+                                tuned_variant(ctx, evoc::kScanJaccard, j.keff, lde, j.n)),
            "jaccard scan");
   ctx->launches += 1;
   return EVOC_OK;
@@ -964,6 +987,153 @@ int knn_batch_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtyp
   return EVOC_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Autotuner of the scan's kernel variants
+// ---------------------------------------------------------------------------
+std::mutex g_tune_file_mu;  // appends to a cache file from several contexts
+
+int tune_load_impl(evoc_gpu_ctx* ctx, const char* path) {
+  std::ifstream f(path);
+  if (!f) return -1;
+  std::string line;
+  int loaded = 0;
+  while (std::getline(f, line)) {
+    int ver = 0, mode = 0, keep = 0, l2 = 0, v = 0;
+    long long rb = 0;
+    double ms = 0.0;
+    if (std::sscanf(line.c_str(), "evoc-tune %d mode=%d keep=%d row_bytes=%lld log2n=%d variant=%d ms=%lf", &ver,
+                    &mode, &keep, &rb, &l2, &v, &ms) == 7 &&
+        ver == 1 && v >= 0 && v < evoc::kScanVariants) {
+      ctx->tune[std::make_tuple(mode, keep, int64_t(rb), l2)] = v;
+      loaded++;
+    }
+  }
+  return loaded;
+}
+
+int autotune_impl(evoc_gpu_ctx* ctx, int32_t dtype, int32_t form_in, int64_t n, int64_t dim, int32_t k,
+                  const char* cache_path, char* report, int32_t report_len) {
+  if (!ctx) return EVOC_ERR_ARG;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  ctx->err.clear();
+  if (k <= 0) return fail(ctx, EVOC_ERR_K, "n_neighbors must be positive");
+  if (n <= 1 || dim <= 0) return fail(ctx, EVOC_ERR_ARG, "n > 1 and dim > 0 required");
+  evoc_gpu_opts opts;
+  evoc_gpu_default_opts(&opts);
+  const int form = resolve_form(dtype, form_in);
+  const int keff = int(std::max<int64_t>(1, std::min<int64_t>(k, n - 1)));
+  int mode, keep, final_mode, out_dtype;
+  int64_t row_bytes;
+  if (dtype == EVOC_DTYPE_F32 && form == EVOC_FORM_BF16_RERANK) {
+    mode = evoc::kScanBf16;
+    keep = int(bf16_candidates(opts, n, keff));
+    row_bytes = round_up(dim, 64) * 2;
+    final_mode = 0;
+    out_dtype = 0;
+  } else if (dtype == EVOC_DTYPE_I8 && form == EVOC_FORM_EXACT_INT) {
+    mode = evoc::kScanInt8;
+    keep = keff;
+    row_bytes = round_up(dim, 128);
+    final_mode = 1;
+    out_dtype = EVOC_DTYPE_I8;
+  } else if (dtype == EVOC_DTYPE_U8 && form == EVOC_FORM_EXACT_INT) {
+    mode = evoc::kScanJaccard;
+    keep = keff;
+    row_bytes = expanded_row_bytes(dim);
+    final_mode = 1;
+    out_dtype = EVOC_DTYPE_U8;
+  } else {
+    return fail(ctx, EVOC_ERR_UNSUPPORTED, "only the tensor-core forms (BF16+rerank, exact int8 / binary) are tuned");
+  }
+  EVOC_TRY(cudaSetDevice(ctx->device), "cudaSetDevice");
+  // Synthetic rows of the request's shape; a sample of up to 65,536 rows is
+  // enough to rank the variants (their cost per (query, key) pair).
+  const int64_t nt = std::min<int64_t>(n, 65536);
+  const int64_t rows = evoc::padded_rows(nt);
+  EVOC_TRY(ctx->xb.ensure(size_t(rows * row_bytes)), "alloc tuning rows");
+  const int32_t* pc = nullptr;
+  if (mode == evoc::kScanJaccard) {
+    const int64_t ldp = round_up(dim, 64);
+    EVOC_TRY(ctx->x.ensure(size_t(rows * ldp)), "alloc tuning bits");
+    EVOC_TRY(evoc::launch_fill_random(2, ctx->x.p, rows, ldp, nt, dim, 0x7157u, ctx->sms, ctx->stream), "fill");
+    EVOC_TRY(ctx->popc.ensure(size_t(nt) * 4), "alloc popcounts");
+    EVOC_TRY(evoc::launch_popcount_rows(ctx->x.p, nt, int(ldp / 4), ctx->popc.as<int32_t>(), ctx->sms, ctx->stream),
+             "popcounts");
+    EVOC_TRY(evoc::launch_expand_bits(ctx->x.p, nt, ldp, dim, ctx->xb.p, rows, row_bytes, ctx->sms, ctx->stream),
+             "expand bits");
+    pc = ctx->popc.as<int32_t>();
+  } else {
+    const int64_t bytes = mode == evoc::kScanBf16 ? dim * 2 : dim;
+    EVOC_TRY(evoc::launch_fill_random(mode == evoc::kScanBf16 ? 0 : 1, ctx->xb.p, rows, row_bytes, nt, bytes, 0x7157u,
+                                      ctx->sms, ctx->stream),
+             "fill");
+  }
+  const int grid = scan_grid(ctx, nt);
+  EVOC_TRY(ctx->cand.ensure(size_t(nt) * size_t(keep) * 4), "alloc tuning outputs");
+  EVOC_TRY(ctx->out_dist.ensure(size_t(nt) * size_t(keep) * 4), "alloc tuning outputs");
+  EVOC_TRY(ctx->scratch.ensure(size_t(grid) * 256 * size_t(keep) * 8), "alloc scratch");
+  EVOC_TRY(ctx->flag.ensure(64), "alloc flag");
+  int* status = ctx->flag.as<int>() + 1;
+  cudaEvent_t e0, e1;
+  EVOC_TRY(cudaEventCreate(&e0), "event");
+  EVOC_TRY(cudaEventCreate(&e1), "event");
+  std::string rep;
+  int best = -1;
+  float best_ms = 0.0f;
+  for (int v = 0; v < evoc::kScanVariants; v++) {
+    if (!evoc::tc_scan_variant_feasible(v, keep, true)) continue;
+    auto run = [&]() {
+      return evoc::launch_tc_scan(mode, ctx->xb.p, rows, 0, nt, ctx->xb.p, rows, nt, row_bytes, keep,
+                                  ctx->scratch.as<uint64_t>(), grid, 1, final_mode, out_dtype, ctx->cand.as<int32_t>(),
+                                  nullptr, final_mode ? ctx->out_dist.as<float>() : nullptr, status, ctx->timeout_ns,
+                                  pc, ctx->stream, v);
+    };
+    cudaError_t e = cudaMemsetAsync(status, 0, sizeof(int), ctx->stream);
+    if (e == cudaSuccess) e = run();  // warm-up
+    if (e == cudaSuccess) e = cudaEventRecord(e0, ctx->stream);
+    for (int r = 0; r < 2 && e == cudaSuccess; r++) e = run();
+    if (e == cudaSuccess) e = cudaEventRecord(e1, ctx->stream);
+    int st = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&st, status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      return cuda_fail(ctx, e, "tuning run");
+    }
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    ms /= 2.0f;
+    char buf[160];
+    std::snprintf(buf, sizeof(buf), "%d %.3f ms %s%s\n", v, double(ms), evoc::tc_scan_variant_name(v),
+                  st ? " (timed out)" : "");
+    rep += buf;
+    if (st == 0 && (best < 0 || ms < best_ms)) {
+      best = v;
+      best_ms = ms;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (best < 0) return fail(ctx, EVOC_ERR_TIMEOUT, "no variant completed");
+  ctx->tune[std::make_tuple(mode, keep, row_bytes, ilog2(n))] = best;
+  char line[200];
+  std::snprintf(line, sizeof(line), "evoc-tune 1 mode=%d keep=%d row_bytes=%lld log2n=%d variant=%d ms=%.3f\n", mode,
+                keep, static_cast<long long>(row_bytes), ilog2(n), best, double(best_ms));
+  rep += std::string("chosen: ") + line;
+  if (cache_path && cache_path[0]) {
+    std::lock_guard<std::mutex> flock(g_tune_file_mu);
+    std::ofstream f(cache_path, std::ios::app);
+    if (!f) return fail(ctx, EVOC_ERR_ARG, std::string("cannot append to ") + cache_path);
+    f << line;
+  }
+  if (report && report_len > 0) {
+    std::strncpy(report, rep.c_str(), size_t(report_len) - 1);
+    report[report_len - 1] = '\0';
+  }
+  return EVOC_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -994,6 +1164,8 @@ int evoc_gpu_ctx_create(int device, evoc_gpu_ctx** out) {
   cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device);
   if (const char* v = std::getenv("EVOC_SYNC_CHECK")) ctx->sync_check = v[0] == '1';
   if (const char* v = std::getenv("EVOC_NO_GRAPHS")) ctx->use_graphs = v[0] != '1';
+  if (const char* v = std::getenv("EVOC_TUNE_CACHE"))
+    if (v[0]) tune_load_impl(ctx, v);
   e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     delete ctx;
@@ -1071,6 +1243,17 @@ int evoc_gpu_knn_graph(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts, int32_t dty
                        int64_t dim, int32_t k, const int64_t* rng_state, int32_t* out_idx, float* out_dist,
                        int32_t* out_k) {
   return knn_impl(ctx, opts, dtype, data, n, dim, k, rng_state, out_idx, out_dist, nullptr, out_k);
+}
+
+int evoc_gpu_autotune(evoc_gpu_ctx* ctx, int32_t dtype, int32_t form, int64_t n, int64_t dim, int32_t k,
+                      const char* cache_path, char* report, int32_t report_len) {
+  return autotune_impl(ctx, dtype, form, n, dim, k, cache_path, report, report_len);
+}
+
+int evoc_gpu_tune_load(evoc_gpu_ctx* ctx, const char* cache_path) {
+  if (!ctx || !cache_path) return -1;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  return tune_load_impl(ctx, cache_path);
 }
 
 int evoc_gpu_knn_graph_batch(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts, int32_t dtype, int32_t n_jobs,

@@ -46,7 +46,17 @@ enum ScanMode { kScanBf16 = 0, kScanInt8 = 1, kScanJaccard = 2 };
 cudaError_t launch_tc_scan(int mode, const void* Q, int64_t q_rows, int64_t q_row0, int64_t n_q, const void* K,
                            int64_t k_rows, int64_t n_k, int64_t row_bytes, int keep, uint64_t* scratch, int grid,
                            int self_mode, int final_mode, int dtype, int32_t* out_idx, float* out_raw, float* out_dist,
-                           int* status, uint64_t timeout_ns, const int32_t* pc, cudaStream_t stream);
+                           int* status, uint64_t timeout_ns, const int32_t* pc, cudaStream_t stream,
+                           int variant = -1);
+// Kernel variants of the scan (0..4; -1 = automatic: the first that fits
+// shared memory in the order 0..3, else 4 with global heaps).
+constexpr int kScanVariants = 5;
+bool tc_scan_variant_feasible(int variant, int keep, bool has_scratch);
+const char* tc_scan_variant_name(int variant);
+// prep.cu: synthetic rows for the autotuner (mode 0: BF16 values in [-1, 1];
+// 1: int8; 2: packed bits, about 1 in 8 set), zero past n rows / `bytes` bytes.
+cudaError_t launch_fill_random(int mode, void* rows, int64_t n_rows_mem, int64_t row_bytes, int64_t n,
+                               int64_t bytes, uint64_t seed, int sms, cudaStream_t stream);
 
 // rerank.cu
 cudaError_t launch_rerank_f32(const float* X, int ld, int d, int64_t n_q, int64_t n_keys, int64_t q_row0,

@@ -235,3 +235,45 @@ cudaError_t launch_batch_rows(bool f32, const BatchHeader* hdr, const BatchRowJo
 }
 
 }  // namespace evoc
+
+namespace evoc {
+
+namespace {
+__device__ __forceinline__ uint64_t fill_hash(uint64_t z) {  // splitmix64 finaliser
+  z += 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+}  // namespace
+
+__global__ void fill_random_kernel(int mode, uint8_t* __restrict__ rows, int64_t n_rows_mem, int64_t row_bytes,
+                                   int64_t n, int64_t bytes, uint64_t seed) {
+  const int64_t total = n_rows_mem * row_bytes;
+  const int64_t eb = mode == 0 ? 2 : 1;
+  for (int64_t e = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) * eb; e < total;
+       e += int64_t(gridDim.x) * blockDim.x * eb) {
+    const int64_t r = e / row_bytes, c = e % row_bytes;
+    const bool live = r < n && c < bytes;
+    const uint64_t h = fill_hash(seed ^ uint64_t(e));
+    if (mode == 0) {
+      const float v = live ? float(int32_t(h & 0xffff) - 32768) / 32768.0f : 0.0f;
+      *reinterpret_cast<__nv_bfloat16*>(rows + e) = __float2bfloat16_rn(v);
+    } else if (mode == 1) {
+      rows[e] = live ? uint8_t(int8_t(int32_t(h % 255) - 127)) : uint8_t(0);
+    } else {
+      const uint64_t b = h & (h >> 8) & (h >> 16);  // each bit set with probability 1/8
+      rows[e] = live ? uint8_t(b) : uint8_t(0);
+    }
+  }
+}
+
+cudaError_t launch_fill_random(int mode, void* rows, int64_t n_rows_mem, int64_t row_bytes, int64_t n,
+                               int64_t bytes, uint64_t seed, int sms, cudaStream_t stream) {
+  if (mode < 0 || mode > 2 || (mode == 0 && (row_bytes % 2 || bytes % 2))) return cudaErrorInvalidValue;
+  fill_random_kernel<<<sms * 8, 256, 0, stream>>>(mode, static_cast<uint8_t*>(rows), n_rows_mem, row_bytes, n, bytes,
+                                                  seed);
+  return cudaGetLastError();
+}
+
+}  // namespace evoc

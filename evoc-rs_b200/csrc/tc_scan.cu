@@ -521,8 +521,37 @@ cudaError_t launch_variant(const CUtensorMap& ma, const CUtensorMap& mb, const S
   return cudaGetLastError();
 }
 
+// The kernel variants an autotuner may choose between: pipeline stages,
+// epilogue warp groups, heaps in shared (s) or global (g) memory.
+constexpr int kVariantCfg[5][3] = {{4, 2, 1}, {3, 2, 1}, {4, 1, 1}, {3, 1, 1}, {4, 1, 0}};
+
+bool variant_feasible(int v, int keep, bool has_scratch) {
+  if (v < 0 || v > 4) return false;
+  if (kVariantCfg[v][2] == 0) return has_scratch;
+  return smem_bytes(kVariantCfg[v][0], kVariantCfg[v][1], keep | 1) <= SMEM_LIMIT;
+}
+
 template <int MODE>
-cudaError_t launch_mode(const CUtensorMap& ma, const CUtensorMap& mb, ScanParams p, int grid, cudaStream_t stream) {
+cudaError_t launch_forced(const CUtensorMap& ma, const CUtensorMap& mb, ScanParams p, int grid, int v,
+                          cudaStream_t stream) {
+  const int odd = p.keep | 1;
+  p.heap_stride = odd;
+  switch (v) {
+    case 0: return launch_variant<MODE, 4, 2, true>(ma, mb, p, grid, smem_bytes(4, 2, odd), stream);
+    case 1: return launch_variant<MODE, 3, 2, true>(ma, mb, p, grid, smem_bytes(3, 2, odd), stream);
+    case 2: return launch_variant<MODE, 4, 1, true>(ma, mb, p, grid, smem_bytes(4, 1, odd), stream);
+    case 3: return launch_variant<MODE, 3, 1, true>(ma, mb, p, grid, smem_bytes(3, 1, odd), stream);
+    default:
+      p.heap_stride = p.keep;
+      return launch_variant<MODE, 4, 1, false>(ma, mb, p, grid, smem_bytes(4, 1, 0), stream);
+  }
+}
+
+template <int MODE>
+cudaError_t launch_mode(const CUtensorMap& ma, const CUtensorMap& mb, ScanParams p, int grid, int variant,
+                        cudaStream_t stream) {
+  if (variant >= 0 && variant_feasible(variant, p.keep, p.scratch != nullptr))
+    return launch_forced<MODE>(ma, mb, p, grid, variant, stream);
   const int odd = p.keep | 1;
   p.heap_stride = odd;
   // Prefer two epilogue groups (more warps to hide TMEM/issue latency), then
@@ -544,7 +573,8 @@ cudaError_t launch_mode(const CUtensorMap& ma, const CUtensorMap& mb, ScanParams
 cudaError_t launch_tc_scan(int mode, const void* Q, int64_t q_rows, int64_t q_row0, int64_t n_q, const void* K,
                            int64_t k_rows, int64_t n_k, int64_t row_bytes, int keep, uint64_t* scratch, int grid,
                            int self_mode, int final_mode, int dtype, int32_t* out_idx, float* out_raw, float* out_dist,
-                           int* status, uint64_t timeout_ns, const int32_t* pc, cudaStream_t stream) {
+                           int* status, uint64_t timeout_ns, const int32_t* pc, cudaStream_t stream,
+                           int variant) {
   // q_rows / k_rows: rows present in memory (multiples of the box heights);
   // n_q / n_k: rows that take part.  Rows past n are zero and never offered.
   if (row_bytes % KCB != 0 || n_q <= 0 || n_k <= 0 || keep < 1) return cudaErrorInvalidValue;
@@ -574,9 +604,22 @@ cudaError_t launch_tc_scan(int mode, const void* Q, int64_t q_rows, int64_t q_ro
   p.status = status;
   p.timeout_ns = timeout_ns;
   p.pc = pc;
-  if (mode == kModeInt8) return launch_mode<kModeInt8>(ma, mb, p, grid, stream);
-  if (mode == kModeJaccard) return launch_mode<kModeJaccard>(ma, mb, p, grid, stream);
-  return launch_mode<kModeBf16>(ma, mb, p, grid, stream);
+  if (mode == kModeInt8) return launch_mode<kModeInt8>(ma, mb, p, grid, variant, stream);
+  if (mode == kModeJaccard) return launch_mode<kModeJaccard>(ma, mb, p, grid, variant, stream);
+  return launch_mode<kModeBf16>(ma, mb, p, grid, variant, stream);
+}
+
+bool tc_scan_variant_feasible(int variant, int keep, bool has_scratch) {
+  return variant_feasible(variant, keep, has_scratch);
+}
+
+const char* tc_scan_variant_name(int variant) {
+  static const char* names[5] = {"4 stages, 2 epilogue groups, shared-memory heaps",
+                                 "3 stages, 2 epilogue groups, shared-memory heaps",
+                                 "4 stages, 1 epilogue group, shared-memory heaps",
+                                 "3 stages, 1 epilogue group, shared-memory heaps",
+                                 "4 stages, 1 epilogue group, global-memory heaps"};
+  return variant >= 0 && variant < 5 ? names[variant] : "automatic";
 }
 
 // ---------------------------------------------------------------------------

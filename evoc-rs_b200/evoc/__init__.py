@@ -13,6 +13,7 @@ from .knn import (  # noqa: F401
     InvalidNeighbors,
     KnnError,
     KnnGraphOptions,
+    autotune,
     knn_graph,
     knn_graph_batch,
     knn_graph_batch_device,

@@ -95,6 +95,9 @@ def _bind_optional(L) -> None:
                                            C.POINTER(i64)]
     if hasattr(L, "evoc_gpu_smooth_knn_dist"):
         L.evoc_gpu_smooth_knn_dist.argtypes = [P, P, i64, i32, C.c_float, i32, P, P]
+    if hasattr(L, "evoc_gpu_autotune"):
+        L.evoc_gpu_autotune.argtypes = [P, i32, i32, i64, i64, i32, C.c_char_p, C.c_char_p, i32]
+        L.evoc_gpu_tune_load.argtypes = [P, C.c_char_p]
     if hasattr(L, "evoc_gpu_knn_graph_batch"):
         L.evoc_gpu_knn_graph_batch.argtypes = [P, C.POINTER(Opts), i32, i32, P, P, P, i32, P, P, P, P]
     if hasattr(L, "evoc_gpu_server_create"):

@@ -274,6 +274,29 @@ def knn_graph_batch(datas, options: KnnGraphOptions, rngs=None):
     return [(a.cpu().numpy(), b.cpu().numpy()) for a, b in zip(oi, od)]
 
 
+def autotune(kind: str, n: int, dim: int, k: int, form: str = "auto", cache_path: Optional[str] = None,
+             device: int = 0) -> dict:
+    """Time the scan's kernel variants for requests of this shape (evoc_gpu_autotune) and keep the
+    fastest for this device's context; with cache_path, append it to that tuning cache file.
+    kind: "Float32", "Int8" or "UInt8"."""
+    code = {"Float32": _lib.DTYPE_F32, "Int8": _lib.DTYPE_I8, "UInt8": _lib.DTYPE_U8}[kind]
+    ctx = _lib.context(device)
+    buf = C.create_string_buffer(2048)
+    st = _lib.lib().evoc_gpu_autotune(ctx.h, code, _lib.FORM_NAMES[form], int(n), int(dim), int(k),
+                                     cache_path.encode() if cache_path else None, buf, 2048)
+    _raise_for(st, ctx)
+    lines = buf.value.decode().strip().splitlines()
+    variants = {}
+    chosen = None
+    for ln in lines:
+        if ln.startswith("chosen: "):
+            chosen = int(ln.split("variant=")[1].split()[0])
+        else:
+            v, ms = ln.split()[:2]
+            variants[int(v)] = float(ms)
+    return {"variants_ms": variants, "chosen": chosen, "report": lines}
+
+
 def transform_distances_float(distances: np.ndarray) -> np.ndarray:
     """transform_distances_float (src/knn.rs:156-171), host-side helper."""
     d = np.asarray(distances, np.float32)

@@ -134,6 +134,24 @@ int evoc_gpu_knn_graph_batch(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts, int32
                              const void* const* data, const int64_t* n, const int64_t* dim, int32_t k,
                              int32_t* const* out_idx, float* const* out_dist, float* const* out_raw, int32_t* out_k);
 
+/*
+ * Autotuner.  Times the tensor-core scan's kernel variants (pipeline depth,
+ * epilogue warp groups, heaps in shared or global memory) for requests of
+ * this shape on synthetic rows (a sample of up to 65,536 rows), keeps the
+ * fastest for this context -- later calls with the same dtype, form, k, dim
+ * and floor(log2 n) use it -- and, when cache_path is not NULL, appends it to
+ * that file.  A context created while EVOC_TUNE_CACHE names such a file loads
+ * it.  Only the tensor-core forms are tuned (f32 BF16_RERANK, i8 and u8
+ * EXACT_INT); every variant gives the same results.  report (may be NULL)
+ * receives one line per variant and the chosen entry.  No counterpart in
+ * evoc-rs (its CPU kernels have no tile parameters).
+ */
+int evoc_gpu_autotune(evoc_gpu_ctx* ctx, int32_t dtype, int32_t form, int64_t n, int64_t dim, int32_t k,
+                      const char* cache_path, char* report, int32_t report_len);
+/* Loads a tuning cache file into the context; returns the entries loaded,
+ * or -1 when the file cannot be read. */
+int evoc_gpu_tune_load(evoc_gpu_ctx* ctx, const char* cache_path);
+
 /* As evoc_gpu_knn_graph, and also writes the raw pre-transform
  * dissimilarities the reference's heaps hold (src/knn.rs:456-520 checks
  * them) into out_raw (n x k_eff, may be NULL). */
