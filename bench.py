@@ -648,8 +648,10 @@ def run_ours(args, world, rank, local):
     ctx = _lib.context(local)
     ctx.profile(True)
     stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=dev)
-    opts = evoc.KnnGraphOptions(n_neighbors=k, form="bf16_rerank", oversample=2, device=local)
-    tuned = evoc.autotune("Float32", n, d, k, "bf16_rerank", device=local) if args.autotune else None
+    form = args.form
+    opts = evoc.KnnGraphOptions(n_neighbors=k, form=form, oversample=2, device=local)
+    tuned = (evoc.autotune("Float32", n, d, k, "bf16_rerank", device=local)
+             if args.autotune and form == "bf16_rerank" else None)
 
     def step():
         evoc.knn_graph_device(x.data_ptr(), 0, n, d, k, oi.data_ptr(), od.data_ptr(), opts)
@@ -695,6 +697,34 @@ def run_ours(args, world, rank, local):
     want = transform_f64(dots, selfm)
     max_err = float((od[:sample].double() - want).abs().max().item())
 
+    # The fuzzy simplicial set of the graph, on the device (σ/ρ, membership,
+    # symmetric union as canonical CSR), timed on the library's stream.
+    fuzzy = None
+    if args.fuzzy:
+        import ctypes as C
+
+        cap = 2 * n * k
+        f_indptr = torch.empty(n + 1, dtype=torch.int64, device=dev)
+        f_ind = torch.empty(cap, dtype=torch.int32, device=dev)
+        f_dat = torch.empty(cap, dtype=torch.float32, device=dev)
+        f_sig = torch.empty(n, dtype=torch.float32, device=dev)
+        f_rho = torch.empty(n, dtype=torch.float32, device=dev)
+        nnz = C.c_int64(0)
+        P = C.c_void_p
+        times = []
+        for rep in range(4):
+            st = _lib.lib().evoc_gpu_fuzzy_graph(ctx.h, P(oi.data_ptr()), P(od.data_ptr()), n, k, float(k), 1, 1,
+                                                 P(f_sig.data_ptr()), P(f_rho.data_ptr()), P(f_indptr.data_ptr()),
+                                                 P(f_ind.data_ptr()), P(f_dat.data_ptr()), cap, C.byref(nnz))
+            assert st == 0, ctx.last_error()
+            if rep:
+                times.append(dict(ctx.stages()))
+        fuzzy = {"ms": statistics.mean(t["total"] for t in times),
+                 "stages_ms": {nm: statistics.mean(t[nm] for t in times) for nm in times[0] if nm != "total"},
+                 "nnz": int(nnz.value), "rows": n, "k": k,
+                 "note": "sigma/rho bisection, membership strengths, A + A^T - A o A^T as canonical CSR"}
+        del f_indptr, f_ind, f_dat, f_sig, f_rho
+
     # End to end through the public API with pinned host buffers.
     xh = torch.empty((n, d), dtype=torch.float32, pin_memory=True)
     xh.copy_(x)
@@ -721,7 +751,7 @@ def run_ours(args, world, rank, local):
 
     # Plain FP32 SIMT form on a slice of query rows against all n rows.
     fp32 = None
-    if args.fp32_rows > 0:
+    if args.fp32_rows > 0 and form == "bf16_rerank":
         rows = min(args.fp32_rows, n)
         fo = evoc.KnnGraphOptions(n_neighbors=k, form="fp32", device=local, row_begin=0, row_end=rows)
         fi = torch.empty((rows, k), dtype=torch.int32, device=dev)
@@ -742,14 +772,22 @@ def run_ours(args, world, rank, local):
                 "tflops_fp32": 2.0 * rows * n * d / (fms / 1000.0) / 1e12}
 
     peaks, peak_kind = measured_peaks()
-    scan_ms = statistics.mean(stage_ms.get("bf16_scan", [float("nan")]))
-    flops = 2.0 * n * n * d
-    achieved = flops / (scan_ms / 1000.0) / 1e12
-    peak = float(peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops")))
-    roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "traffic": scan_traffic(n), "traffic_unit": "bytes per launch (ncu, scaled)", "kernel": "tc_scan_kernel (BF16, fused top-2k)",
-                "peak_kind": f"{peak_kind} bf16 sustained (burst {peaks.get('bf16_tflops')})",
-                "launch_ms": scan_ms}
+    if form == "bf16_rerank":
+        scan_ms = statistics.mean(stage_ms.get("bf16_scan", [float("nan")]))
+        flops = 2.0 * n * n * d
+        achieved = flops / (scan_ms / 1000.0) / 1e12
+        peak = float(peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops")))
+        roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                    "traffic": scan_traffic(n), "traffic_unit": "bytes per launch (ncu, scaled)",
+                    "kernel": "tc_scan_kernel (BF16, fused top-2k)",
+                    "peak_kind": f"{peak_kind} bf16 sustained (burst {peaks.get('bf16_tflops')})",
+                    "launch_ms": scan_ms}
+    else:
+        it_ms = stage_ms.get("nnd_iteration", [float("nan")])
+        roofline = {"bound": "hbm", "achieved": None, "peak": float(peaks.get("hbm_gbs")), "unit": "GB/s",
+                    "frac": None, "traffic": None, "kernel": "nnd_join_kernel (candidate row gathers)",
+                    "launch_ms": statistics.mean(it_ms),
+                    "note": "the join's gathered bytes depend on the candidate sets; DRAM counters in profiles/"}
 
     cpu = None
     if rank == 0 and world == 1 and args.cpu_rows > 0:
@@ -772,11 +810,13 @@ def run_ours(args, world, rank, local):
                           f"{threads} threads) on the first {args.cpu_rows} rows of the workload; "
                           f"{t:.1f} s; its recall@{k} vs FP64 on {qrows} of those rows {crec:.4f}")}
 
+    metric = METRIC if form == "bf16_rerank" else "kNN edges/s, GPU NN-descent form (recall vs FP64 reported)"
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "bf16 tensor-core scan + f32 rerank", "data": "synthetic (generated on device, seeded)",
-        "config": {"workload": WORKLOAD, "n": n, "d": d, "k": k, "form": "bf16_rerank", "oversample": 2,
+        "dtype": "bf16 tensor-core scan + f32 rerank" if form == "bf16_rerank" else "f32 (NN-descent joins, f32 rerank)",
+        "data": "synthetic (generated on device, seeded)",
+        "config": {"workload": WORKLOAD, "n": n, "d": d, "k": k, "form": form, "oversample": 2,
                    "l2": "inputs larger than L2 (3.1 GB f32 + 1.5 GB bf16 vs 126 MB)",
                    "per_rank": "independent graph per rank"},
         "recall_at_k_vs_fp64": rec, "max_abs_dist_err_vs_fp64": max_err, "recall_sample_rows": sample,
@@ -785,6 +825,7 @@ def run_ours(args, world, rank, local):
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n * d * 4, "d2h_bytes_per_step": n * k * 8,
                 "ms_per_step": e2e_ms, "matches_device_path": e2e_consistent},
         "fp32_form": fp32,
+        "fuzzy_graph": fuzzy,
         "autotune": tuned and {"variants_ms_65536_rows": tuned["variants_ms"], "chosen": tuned["chosen"]},
         "cpu_baseline": cpu,
         "clocks": clk,
@@ -814,6 +855,9 @@ def main():
     ap.add_argument("--k", type=int, default=None)
     ap.add_argument("--check-rows", type=int, default=128)
     ap.add_argument("--autotune", type=int, default=1, help="tune the scan's kernel variant before timing")
+    ap.add_argument("--form", default="bf16_rerank", choices=["bf16_rerank", "nndescent"],
+                    help="zipf_f32 workload: the exact BF16+rerank form (headline) or GPU NN-descent")
+    ap.add_argument("--fuzzy", type=int, default=1, help="time the fuzzy graph of the built graph")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--fp32-rows", type=int, default=75_776)  # 2 full waves of 296 CTAs x 128 rows
     ap.add_argument("--recall-rows", type=int, default=10_000)

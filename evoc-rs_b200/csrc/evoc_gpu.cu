@@ -356,13 +356,14 @@ int run_jaccard(evoc_gpu_ctx* ctx, const Job& j, int64_t ldb) {
 int fuzzy_work(evoc_gpu_ctx* ctx, int64_t n, int k, evoc::FuzzyWork* w) {
   const size_t nk = size_t(n) * size_t(k);
   const size_t sizes[] = {64, 64, nk * 4, nk * 4, size_t(n) * 4, size_t(n) * 4, size_t(n + 1) * 8, size_t(n) * 4,
-                          nk * 4, nk * 4, size_t(n) * 4};
+                          nk * 4, nk * 4, size_t(n) * 4, size_t(n) * 4, 64};
+  constexpr int kParts = int(sizeof(sizes) / sizeof(sizes[0]));
   size_t total = 0;
   for (size_t s : sizes) total += (s + 255) / 256 * 256;
   EVOC_TRY(ctx->g_work.ensure(total), "alloc graph work");
   uint8_t* p = ctx->g_work.as<uint8_t>();
-  void* ptrs[11];
-  for (int i = 0; i < 11; i++) {
+  void* ptrs[kParts];
+  for (int i = 0; i < kParts; i++) {
     ptrs[i] = p;
     p += (sizes[i] + 255) / 256 * 256;
   }
@@ -377,6 +378,8 @@ int fuzzy_work(evoc_gpu_ctx* ctx, int64_t n, int k, evoc::FuzzyWork* w) {
   w->at_rows = static_cast<int32_t*>(ptrs[8]);
   w->at_vals = static_cast<float*>(ptrs[9]);
   w->row_cnt = static_cast<int32_t*>(ptrs[10]);
+  w->big = static_cast<int32_t*>(ptrs[11]);
+  w->n_big = static_cast<int32_t*>(ptrs[12]);
   return EVOC_OK;
 }
 

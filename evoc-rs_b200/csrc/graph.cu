@@ -181,31 +181,114 @@ __global__ void scatter_transpose_kernel(const int32_t* __restrict__ a_cols, con
   }
 }
 
-// Each column bucket of A^T sorted by row (Shell sort; buckets are small on
-// average, hubs are bounded by n).
-__global__ void sort_buckets_kernel(const int64_t* __restrict__ colptr, int64_t n, int32_t* __restrict__ rows,
-                                    float* __restrict__ vals) {
+// Each column bucket of A^T sorted by row.  A row appears at most once in a
+// column, so sorting the packed (row << 32 | value bits) keys sorts by row.
+// Buckets hold k entries on average but hubs can hold thousands: a warp sorts
+// each bucket of up to kWarpSort entries (bitonic, in registers up to 32, in
+// the warp's shared-memory slice above); larger buckets are listed and sorted
+// by a whole block each (kBlockSort entries in shared memory), and any larger
+// still by one thread (Shell sort).
+constexpr int kWarpSort = 1024;
+constexpr int kBlockSort = 8192;
+constexpr int kSortWarps = 4;
+
+__device__ __forceinline__ uint64_t bucket_key(int32_t r, float v) {
+  return (uint64_t(uint32_t(r)) << 32) | __float_as_uint(v);
+}
+
+template <int P_MAX>
+__device__ __forceinline__ void bitonic_shared(uint64_t* keys, int P, int tid, int nthreads, bool block) {
+  for (int size = 2; size <= P; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = tid; i < (P >> 1); i += nthreads) {
+        const int lo = 2 * stride * (i / stride) + (i % stride);
+        const int hi = lo + stride;
+        const bool up = (lo & size) == 0;
+        const uint64_t a = keys[lo], b = keys[hi];
+        if ((a > b) == up) {
+          keys[lo] = b;
+          keys[hi] = a;
+        }
+      }
+      if (block) __syncthreads();
+      else __syncwarp();
+    }
+  }
+}
+
+__device__ void shell_sort_bucket(int32_t* r, float* v, int64_t m) {
   const int gaps[] = {701, 301, 132, 57, 23, 10, 4, 1};
-  for (int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; c < n; c += int64_t(gridDim.x) * blockDim.x) {
+  for (int gi = 0; gi < 8; gi++) {
+    const int64_t g = gaps[gi];
+    if (g >= m) continue;
+    for (int64_t a = g; a < m; a++) {
+      const int32_t kr = r[a];
+      const float kv = v[a];
+      int64_t b = a;
+      while (b >= g && r[b - g] > kr) {
+        r[b] = r[b - g];
+        v[b] = v[b - g];
+        b -= g;
+      }
+      r[b] = kr;
+      v[b] = kv;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kSortWarps * 32)
+sort_buckets_warp_kernel(const int64_t* __restrict__ colptr, int64_t n, int32_t* __restrict__ rows,
+                         float* __restrict__ vals, int32_t* __restrict__ big, int32_t* __restrict__ n_big) {
+  __shared__ uint64_t slice[kSortWarps][kWarpSort];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint64_t* keys = slice[warp];
+  const int64_t wstride = int64_t(gridDim.x) * kSortWarps;
+  for (int64_t c = int64_t(blockIdx.x) * kSortWarps + warp; c < n; c += wstride) {
+    const int64_t s = colptr[c], m = colptr[c + 1] - s;
+    if (m <= 1) continue;
+    if (m > kWarpSort) {
+      if (lane == 0) big[atomicAdd(n_big, 1)] = int32_t(c);
+      continue;
+    }
+    int32_t* r = rows + s;
+    float* v = vals + s;
+    int P = 32;
+    while (P < m) P <<= 1;
+    for (int i = lane; i < P; i += 32) keys[i] = i < m ? bucket_key(r[i], v[i]) : ~0ull;
+    __syncwarp();
+    bitonic_shared<kWarpSort>(keys, P, lane, 32, false);
+    for (int i = lane; i < m; i += 32) {
+      r[i] = int32_t(keys[i] >> 32);
+      v[i] = __uint_as_float(uint32_t(keys[i]));
+    }
+    __syncwarp();
+  }
+}
+
+__global__ void sort_buckets_big_kernel(const int64_t* __restrict__ colptr, int32_t* __restrict__ rows,
+                                        float* __restrict__ vals, const int32_t* __restrict__ big,
+                                        const int32_t* __restrict__ n_big) {
+  extern __shared__ uint64_t keys[];
+  for (int b = blockIdx.x; b < *n_big; b += gridDim.x) {
+    const int64_t c = big[b];
     const int64_t s = colptr[c], m = colptr[c + 1] - s;
     int32_t* r = rows + s;
     float* v = vals + s;
-    for (int gi = 0; gi < 8; gi++) {
-      const int64_t g = gaps[gi];
-      if (g >= m) continue;
-      for (int64_t a = g; a < m; a++) {
-        const int32_t kr = r[a];
-        const float kv = v[a];
-        int64_t b = a;
-        while (b >= g && r[b - g] > kr) {
-          r[b] = r[b - g];
-          v[b] = v[b - g];
-          b -= g;
-        }
-        r[b] = kr;
-        v[b] = kv;
-      }
+    if (m > kBlockSort) {  // beyond a block's shared memory: one thread
+      if (threadIdx.x == 0) shell_sort_bucket(r, v, m);
+      __syncthreads();
+      continue;
     }
+    int P = 1;
+    while (P < m) P <<= 1;
+    for (int i = threadIdx.x; i < P; i += blockDim.x) keys[i] = i < m ? bucket_key(r[i], v[i]) : ~0ull;
+    __syncthreads();
+    bitonic_shared<kBlockSort>(keys, P, threadIdx.x, blockDim.x, true);
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+      r[i] = int32_t(keys[i] >> 32);
+      v[i] = __uint_as_float(uint32_t(keys[i]));
+    }
+    __syncthreads();
   }
 }
 
@@ -295,7 +378,15 @@ cudaError_t launch_fuzzy_union_count(int64_t n, int k, int symmetrize, const Fuz
     if (e != cudaSuccess) return e;
     scatter_transpose_kernel<<<sms * 8, 128, 0, stream>>>(w.a_cols, w.a_vals, w.a_cnt, n, k, w.colptr, w.fill,
                                                           w.at_rows, w.at_vals);
-    sort_buckets_kernel<<<sms * 8, 128, 0, stream>>>(w.colptr, n, w.at_rows, w.at_vals);
+    cudaError_t e = cudaMemsetAsync(w.n_big, 0, sizeof(int32_t), stream);
+    if (e != cudaSuccess) return e;
+    sort_buckets_warp_kernel<<<sms * 16, kSortWarps * 32, 0, stream>>>(w.colptr, n, w.at_rows, w.at_vals, w.big,
+                                                                       w.n_big);
+    e = cudaFuncSetAttribute(sort_buckets_big_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(kBlockSort * sizeof(uint64_t)));
+    if (e != cudaSuccess) return e;
+    sort_buckets_big_kernel<<<sms, 1024, kBlockSort * sizeof(uint64_t), stream>>>(w.colptr, w.at_rows, w.at_vals,
+                                                                                  w.big, w.n_big);
   }
   union_count_kernel<<<sms * 8, 128, 0, stream>>>(n, k, w.a_cols, w.a_vals, w.a_cnt, w.colptr, w.at_rows, w.at_vals,
                                                   symmetrize, w.row_cnt);

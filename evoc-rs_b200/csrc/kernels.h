@@ -102,6 +102,8 @@ struct FuzzyWork {
   int32_t* at_rows;   // n x k capacity: A^T row indices per column bucket
   float* at_vals;
   int32_t* row_cnt;   // n: entries per row of the result
+  int32_t* big;       // n: column buckets too large for a warp's sort
+  int32_t* n_big;     // 1: their count
 };
 cudaError_t launch_smooth_and_membership(const int32_t* idx, const float* dist, int64_t n, int k, float n_neighbors,
                                          const FuzzyWork& w, float* sigma, float* rho, int sms, cudaStream_t stream);

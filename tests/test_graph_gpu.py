@@ -68,3 +68,25 @@ def test_fuzzy_graph_int8_and_binary_knn():
     xb = np.packbits(rng.random((500, 256)) < 0.2, axis=1)
     ind, dst = evoc.knn_graph(xb, evoc.KnnGraphOptions(n_neighbors=12, form="exact_int"))
     _compare_with_oracle(ind, dst, 12.0)
+
+
+def test_fuzzy_graph_hub_columns():
+    # Hub rows that are neighbours of thousands of rows: the transpose's column
+    # buckets take the warp sort (small), the block sort (3,000 entries) and
+    # the single-thread fallback (> 8,192 entries).
+    n, k = 12000, 10
+    rng = np.random.default_rng(12)
+    ind = np.empty((n, k), np.int32)
+    for i in range(n):
+        row = [i, 0]
+        if i < 3000:
+            row.append(1)
+        while len(row) < k:
+            c = int(rng.integers(2, n))
+            if c != i and c not in row:
+                row.append(c)
+        ind[i] = row[:k]
+    ind[0, 1] = 5  # row 0 cannot list itself twice
+    dst = np.sort(rng.random((n, k)).astype(np.float32) * 2.0, axis=1)
+    dst[:, 0] = 0.0
+    _compare_with_oracle(ind, dst, 10.0)
