@@ -1081,8 +1081,12 @@ int autotune_impl(evoc_gpu_ctx* ctx, int32_t dtype, int32_t form_in, int64_t n, 
   EVOC_TRY(cudaEventCreate(&e0), "event");
   EVOC_TRY(cudaEventCreate(&e1), "event");
   std::string rep;
-  int best = -1;
-  float best_ms = 0.0f;
+  // The automatic choice (first that fits) stays unless another variant is
+  // clearly faster: timings within a few percent are noise at this sample size.
+  int automatic = -1;
+  for (int v = 0; v < evoc::kScanVariants && automatic < 0; v++)
+    if (evoc::tc_scan_variant_feasible(v, keep, v == evoc::kScanVariants - 1)) automatic = v;
+  std::vector<float> times(evoc::kScanVariants, -1.0f);
   for (int v = 0; v < evoc::kScanVariants; v++) {
     if (!evoc::tc_scan_variant_feasible(v, keep, true)) continue;
     auto run = [&]() {
@@ -1111,14 +1115,17 @@ int autotune_impl(evoc_gpu_ctx* ctx, int32_t dtype, int32_t form_in, int64_t n, 
     std::snprintf(buf, sizeof(buf), "%d %.3f ms %s%s\n", v, double(ms), evoc::tc_scan_variant_name(v),
                   st ? " (timed out)" : "");
     rep += buf;
-    if (st == 0 && (best < 0 || ms < best_ms)) {
-      best = v;
-      best_ms = ms;
-    }
+    if (st == 0) times[size_t(v)] = ms;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  int best = (automatic >= 0 && times[size_t(automatic)] >= 0.0f) ? automatic : -1;
+  for (int v = 0; v < evoc::kScanVariants; v++) {
+    if (times[size_t(v)] < 0.0f) continue;
+    if (best < 0 || times[size_t(v)] < 0.97f * times[size_t(best)]) best = v;
+  }
   if (best < 0) return fail(ctx, EVOC_ERR_TIMEOUT, "no variant completed");
+  const float best_ms = times[size_t(best)];
   ctx->tune[std::make_tuple(mode, keep, row_bytes, ilog2(n))] = best;
   char line[200];
   std::snprintf(line, sizeof(line), "evoc-tune 1 mode=%d keep=%d row_bytes=%lld log2n=%d variant=%d ms=%.3f\n", mode,

@@ -163,6 +163,34 @@ __device__ __forceinline__ void offer_chunk(const uint32_t (&v)[32], uint32_t ma
 // f32 subtraction on the FMA pipe for BF16 -- is funnel-shifted into one of
 // four independent accumulators (short dependency chains), then inverted.
 // Equal scores pass (their difference is +0), as `passes` admits them.
+// Whether any score of the chunk passes: a max tree (one min/max instruction
+// per score, independent at each level) and one compare.  Once a row's heap
+// is full most chunks fail here and skip the per-column mask.  Not for
+// Jaccard: its intersection bound is loose enough that the pre-check passes
+// too often to pay for itself.
+template <int MODE>
+__device__ __forceinline__ bool chunk_any(const uint32_t (&v)[32], uint32_t thr) {
+  if (MODE == kModeJaccard) return true;
+  if (MODE != kModeBf16) {
+    int32_t m[16];
+#pragma unroll
+    for (int j = 0; j < 16; j++) m[j] = max(int32_t(v[j]), int32_t(v[j + 16]));
+#pragma unroll
+    for (int w = 8; w > 0; w >>= 1)
+#pragma unroll
+      for (int j = 0; j < w; j++) m[j] = max(m[j], m[j + w]);
+    return m[0] >= int32_t(thr);
+  }
+  float m[16];
+#pragma unroll
+  for (int j = 0; j < 16; j++) m[j] = fmaxf(__uint_as_float(v[j]), __uint_as_float(v[j + 16]));
+#pragma unroll
+  for (int w = 8; w > 0; w >>= 1)
+#pragma unroll
+    for (int j = 0; j < w; j++) m[j] = fmaxf(m[j], m[j + w]);
+  return m[0] >= __uint_as_float(thr);
+}
+
 template <int MODE>
 __device__ __forceinline__ uint32_t chunk_mask(const uint32_t (&v)[32], uint32_t thr) {
   uint32_t f[4] = {0u, 0u, 0u, 0u};  // fail bits
@@ -409,12 +437,16 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         for (int c = 0; c < NCH; c += 2) {
           tmem_ld_wait();
           tmem_ld_32x32b_x32(tbase + (c + 1) * 32, vb);
-          uint32_t m = chunk_mask<MODE>(va, thr);
-          if (valid && m) offer_chunk<MODE>(va, m, k0 + c * 32, v.n_k, v.self_mode, qg, heap, thr, pa, v.pc);
+          if (valid && chunk_any<MODE>(va, thr)) {
+            const uint32_t m = chunk_mask<MODE>(va, thr);
+            offer_chunk<MODE>(va, m, k0 + c * 32, v.n_k, v.self_mode, qg, heap, thr, pa, v.pc);
+          }
           tmem_ld_wait();
           if (c + 2 < NCH) tmem_ld_32x32b_x32(tbase + (c + 2) * 32, va);
-          m = chunk_mask<MODE>(vb, thr);
-          if (valid && m) offer_chunk<MODE>(vb, m, k0 + (c + 1) * 32, v.n_k, v.self_mode, qg, heap, thr, pa, v.pc);
+          if (valid && chunk_any<MODE>(vb, thr)) {
+            const uint32_t m = chunk_mask<MODE>(vb, thr);
+            offer_chunk<MODE>(vb, m, k0 + (c + 1) * 32, v.n_k, v.self_mode, qg, heap, thr, pa, v.pc);
+          }
         }
         tc_fence_before();
         mbar_arrive(&tempty[a]);
