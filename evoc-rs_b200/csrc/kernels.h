@@ -48,9 +48,10 @@ cudaError_t launch_tc_scan(int mode, const void* Q, int64_t q_rows, int64_t q_ro
                            int self_mode, int final_mode, int dtype, int32_t* out_idx, float* out_raw, float* out_dist,
                            int* status, uint64_t timeout_ns, const int32_t* pc, cudaStream_t stream,
                            int variant = -1);
-// Kernel variants of the scan (0..4; -1 = automatic: the first that fits
-// shared memory in the order 0..3, else 4 with global heaps).
-constexpr int kScanVariants = 5;
+// Kernel variants of the scan (0..5; -1 = automatic: the first that fits
+// shared memory in the order 0..3, else 4 with global heaps; 5 -- 2 stages,
+// 2 groups -- is chosen only by the autotuner).
+constexpr int kScanVariants = 6;
 bool tc_scan_variant_feasible(int variant, int keep, bool has_scratch);
 const char* tc_scan_variant_name(int variant);
 // prep.cu: synthetic rows for the autotuner (mode 0: BF16 values in [-1, 1];

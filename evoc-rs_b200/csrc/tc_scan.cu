@@ -555,10 +555,10 @@ cudaError_t launch_variant(const CUtensorMap& ma, const CUtensorMap& mb, const S
 
 // The kernel variants an autotuner may choose between: pipeline stages,
 // epilogue warp groups, heaps in shared (s) or global (g) memory.
-constexpr int kVariantCfg[5][3] = {{4, 2, 1}, {3, 2, 1}, {4, 1, 1}, {3, 1, 1}, {4, 1, 0}};
+constexpr int kVariantCfg[6][3] = {{4, 2, 1}, {3, 2, 1}, {4, 1, 1}, {3, 1, 1}, {4, 1, 0}, {2, 2, 1}};
 
 bool variant_feasible(int v, int keep, bool has_scratch) {
-  if (v < 0 || v > 4) return false;
+  if (v < 0 || v > 5) return false;
   if (kVariantCfg[v][2] == 0) return has_scratch;
   return smem_bytes(kVariantCfg[v][0], kVariantCfg[v][1], keep | 1) <= SMEM_LIMIT;
 }
@@ -573,6 +573,7 @@ cudaError_t launch_forced(const CUtensorMap& ma, const CUtensorMap& mb, ScanPara
     case 1: return launch_variant<MODE, 3, 2, true>(ma, mb, p, grid, smem_bytes(3, 2, odd), stream);
     case 2: return launch_variant<MODE, 4, 1, true>(ma, mb, p, grid, smem_bytes(4, 1, odd), stream);
     case 3: return launch_variant<MODE, 3, 1, true>(ma, mb, p, grid, smem_bytes(3, 1, odd), stream);
+    case 5: return launch_variant<MODE, 2, 2, true>(ma, mb, p, grid, smem_bytes(2, 2, odd), stream);
     default:
       p.heap_stride = p.keep;
       return launch_variant<MODE, 4, 1, false>(ma, mb, p, grid, smem_bytes(4, 1, 0), stream);
@@ -646,12 +647,13 @@ bool tc_scan_variant_feasible(int variant, int keep, bool has_scratch) {
 }
 
 const char* tc_scan_variant_name(int variant) {
-  static const char* names[5] = {"4 stages, 2 epilogue groups, shared-memory heaps",
+  static const char* names[6] = {"4 stages, 2 epilogue groups, shared-memory heaps",
                                  "3 stages, 2 epilogue groups, shared-memory heaps",
                                  "4 stages, 1 epilogue group, shared-memory heaps",
                                  "3 stages, 1 epilogue group, shared-memory heaps",
-                                 "4 stages, 1 epilogue group, global-memory heaps"};
-  return variant >= 0 && variant < 5 ? names[variant] : "automatic";
+                                 "4 stages, 1 epilogue group, global-memory heaps",
+                                 "2 stages, 2 epilogue groups, shared-memory heaps"};
+  return variant >= 0 && variant < 6 ? names[variant] : "automatic";
 }
 
 // ---------------------------------------------------------------------------
