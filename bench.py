@@ -284,9 +284,16 @@ def serve_stream(srv, pools, sched, ids, k, paced, forms=("bf16_rerank", "exact_
     return t0, rec
 
 
-def serving_summary(t0, rec):
+def serving_summary(t0, rec, sched=None):
     arr = [rec[i][0] for i in rec]
     lat = [(rec[i][2] - rec[i][0]) / 1e6 for i in rec]
+    by_size = None
+    if sched is not None:
+        by_size = {}
+        for name, lo, hi in (("n<16384", 0, 16384), ("16384<=n<65536", 16384, 65536), ("n>=65536", 65536, 1 << 40)):
+            sel = [(rec[i][2] - rec[i][0]) / 1e6 for i in rec if lo <= sched["n"][i] < hi]
+            if sel:
+                by_size[name] = {"requests": len(sel), "p50": _pct(sel, 50), "p99": _pct(sel, 99)}
     queue = [(rec[i][1] - rec[i][0]) / 1e6 for i in rec]
     end = max(rec[i][2] for i in rec)
     edges = sum(rec[i][3] for i in rec)
@@ -294,6 +301,7 @@ def serving_summary(t0, rec):
     return {"requests": len(rec), "edges": edges, "makespan_s": span, "edges_per_s": edges / span,
             "arrival_window_s": (max(arr) - t0) / 1e9,
             "latency_ms": {"p50": _pct(lat, 50), "p95": _pct(lat, 95), "p99": _pct(lat, 99), "max": max(lat)},
+            "latency_ms_by_size": by_size,
             "queue_ms": {"p50": _pct(queue, 50), "p99": _pct(queue, 99)}}
 
 
@@ -368,7 +376,7 @@ def run_serving(args, dev):
                 batch_max=args.serve_batch) as srv:
         serve_stream(srv, pools, warm_sched, list(range(len(warm_sched["n"]))), k, paced=False)
         t0, rec = serve_stream(srv, pools, sched, list(range(len(sched["n"]))), k, paced=True)
-        out.update(serving_summary(t0, rec))
+        out.update(serving_summary(t0, rec, sched))
         st = srv.stats()
         out["peak_bytes"] = st["peak_bytes"]
         out["failed"] = st["failed"]
