@@ -12,6 +12,13 @@ produced by upstream Python EVoC (scripts/generate_parity_fixtures.py:18-25,
   tests/parity_intermediates.rs:655-687  NumPy RNG state after knn_graph
 The arrays are copied unchanged into one compressed .npz per fixture so the
 tests can run where the reference tree is absent.
+
+lp_<fixture>.npz carries the label-propagation and node-embedding goldens
+(tests/parity_intermediates.rs:46-135,327-375,405-457,593-653 read the same
+intermediates): per-iteration labels, the partition, the reduced data/graph,
+init and layout, the final init_embedding and embedding, NumPy RNG states
+between the stages, and (large_2000) the reference's own Rust node orders and
+embedding state after 20 reproducible epochs (rust_*_after19.npy).
 """
 import json
 import os
@@ -53,6 +60,41 @@ def main():
             arrs["leaf_array"] = np.load(p)
         np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **arrs)
         print(name, {k: v.shape for k, v in arrs.items()})
+        lp = label_prop_arrays(inter)
+        np.savez_compressed(os.path.join(OUT, f"lp_{name}.npz"), **lp)
+        print("lp_" + name, sorted(lp))
+
+
+LP_ARRAYS = ["labels_seeded", "labels_iter0", "labels_iter1", "labels_iter2", "labels_iter5", "labels_iter10",
+             "labels_iter19", "labels_after_outliers", "partition", "reduced_data", "reduced_init", "reduced_layout",
+             "pre_scale_result", "init_embedding", "embedding", "rust_emb_after19", "rust_updates_after19",
+             "rust_eon_after19", "rust_eos_after19", "rust_node_order_000", "rust_node_order_012",
+             "rust_node_order_024"]
+LP_CSR = ["graph_csr", "reduced_graph_csr", "temp_norm_t_graph"]
+LP_RNG = ["after_knn", "after_partition", "after_reduced_init", "after_init", "after_emb"]
+
+
+def label_prop_arrays(inter):
+    out = {}
+    for f in LP_ARRAYS:
+        p = os.path.join(inter, f + ".npy")
+        if os.path.exists(p):
+            out[f] = np.load(p)
+    for f in LP_CSR:
+        p = os.path.join(inter, f + ".npz")
+        if os.path.exists(p):
+            z = np.load(p)
+            for key in ("indptr", "indices", "data", "shape"):
+                out[f"{f}_{key}"] = z[key]
+    for tag in LP_RNG:
+        p = os.path.join(inter, f"rng_{tag}_key.npy")
+        if os.path.exists(p):
+            meta = np.load(os.path.join(inter, f"rng_{tag}_meta.npz"))
+            out[f"rng_{tag}_key"] = np.load(p)
+            out[f"rng_{tag}_pos"] = meta["pos"]
+            out[f"rng_{tag}_has_gauss"] = meta["has_gauss"]
+            out[f"rng_{tag}_gauss"] = meta["gauss"]
+    return out
 
 
 if __name__ == "__main__":
