@@ -20,122 +20,17 @@
 #include "../../include/evoc_gpu.h"
 #include "batch.h"
 #include "common.cuh"
+#include "ctx.h"
 #include "ctx_plan.h"
 #include "kernels.h"
 
-namespace {
-
-struct DevBuf {
-  void* p = nullptr;
-  size_t bytes = 0;
-  cudaError_t ensure(size_t want) {
-    if (want <= bytes) return cudaSuccess;
-    if (p) cudaFree(p);
-    p = nullptr;
-    bytes = 0;
-    size_t grow = want + want / 8;
-    cudaError_t e = cudaMalloc(&p, grow);
-    if (e != cudaSuccess) {
-      p = nullptr;
-      return e;
-    }
-    bytes = grow;
-    return cudaSuccess;
-  }
-  void release() {
-    if (p) cudaFree(p);
-    p = nullptr;
-    bytes = 0;
-  }
-  template <class T>
-  T* as() const {
-    return static_cast<T*>(p);
-  }
-};
-
-struct StageRec {
-  std::string name;
-  cudaEvent_t a = nullptr, b = nullptr;
-};
-
-}  // namespace
-
-struct evoc_gpu_ctx {
-  int device = 0;
-  int sms = 148;
-  cudaStream_t stream = nullptr;
-  std::mutex mu;
-  std::string err;
-  DevBuf x, scratch, norms, flag, out_idx, out_raw, out_dist;
-  DevBuf xb, cand, labels, order, hist, cursor, pivots, popc;
-  DevBuf g_idx, g_dist, g_sigma, g_rho, g_indptr, g_indices, g_data, g_work;
-  DevBuf nnd_work;
-  DevBuf batch_ws, batch_tab;  // batches: per-request work arena, device tables
-  void* batch_host = nullptr;  // pinned staging of the tables
-  size_t batch_host_bytes = 0;
-  struct BatchGraph {
-    bool f32;
-    int keep_odd;
-    void* tab;
-    int grids[4];  // rows, norms, scan, rerank
-    cudaGraphExec_t exec;
-  };
-  std::vector<BatchGraph> batch_graphs;  // captured batch pipelines, replayed per batch
-  bool use_graphs = true;                // EVOC_NO_GRAPHS=1 launches the kernels directly
-  // Autotuned scan variants: (scan mode, keep, row bytes, floor(log2 n)) -> variant.
-  std::map<std::tuple<int, int, int64_t, int>, int> tune;
-  uint64_t timeout_ns = 4000000000ull;  // longest a pipeline wait inside a kernel may take
-  bool sync_check = false;  // EVOC_SYNC_CHECK=1: wait for and check every kernel stage (fault diagnosis)
-  bool profiling = false;
-  std::vector<StageRec> stages;  // event pool; the first n_stages belong to the last call
-  int n_stages = 0;
-  int launches = 0;
-  int nnd_iterations = 0;
-};
+using evoc::cuda_fail;
+using evoc::DevBuf;
+using evoc::fail;
+using evoc::Stage;
+using evoc::StageRec;
 
 namespace {
-
-int fail(evoc_gpu_ctx* ctx, int code, const std::string& msg) {
-  if (ctx) ctx->err = msg;
-  return code;
-}
-
-int cuda_fail(evoc_gpu_ctx* ctx, cudaError_t e, const char* where) {
-  std::string m = std::string(where) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
-  return fail(ctx, e == cudaErrorMemoryAllocation ? EVOC_ERR_OOM : EVOC_ERR_CUDA, m);
-}
-
-#define EVOC_TRY(expr, where)                                \
-  do {                                                       \
-    cudaError_t _e = (expr);                                 \
-    if (_e != cudaSuccess) return cuda_fail(ctx, _e, where); \
-    if (ctx->sync_check) {                                   \
-      _e = cudaStreamSynchronize(ctx->stream);               \
-      if (_e != cudaSuccess) return cuda_fail(ctx, _e, where); \
-    }                                                        \
-  } while (0)
-
-// Records CUDA events around one stage on the context's stream when profiling.
-struct Stage {
-  evoc_gpu_ctx* ctx;
-  int idx = -1;
-  Stage(evoc_gpu_ctx* c, const char* name) : ctx(c) {
-    if (!ctx->profiling) return;
-    if (ctx->n_stages == int(ctx->stages.size())) {
-      StageRec r;
-      if (cudaEventCreate(&r.a) != cudaSuccess || cudaEventCreate(&r.b) != cudaSuccess) return;
-      ctx->stages.push_back(r);
-    }
-    idx = ctx->n_stages++;
-    ctx->stages[size_t(idx)].name = name;
-    cudaEventRecord(ctx->stages[size_t(idx)].a, ctx->stream);
-  }
-  void end() {
-    if (idx >= 0) cudaEventRecord(ctx->stages[size_t(idx)].b, ctx->stream);
-    idx = -1;
-  }
-  ~Stage() { end(); }
-};
 
 inline int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 

@@ -1,0 +1,1131 @@
+// Label-propagation initialisation and reproducible node-embedding kernels.
+//
+//   label_prop_iteration ........ src/label_prop.rs:39-91     lp_iteration_kernel
+//   label_outliers .............. src/label_prop.rs:94-132    lp_outliers_kernel
+//   remap_labels ................ src/label_prop.rs:135-157   remap_* kernels
+//   partition reduction maps .... src/label_prop.rs:188-230   part_* kernels
+//   csr_matmul_dense ............ src/label_prop.rs:233-250   reduce_data_kernel, expand_kernel
+//   scipy_csr_matmul (SMMP) ..... src/csr_matmul.rs:6-59      launch_reduce_graph, expand_kernel
+//   hadamard_symmetric .......... src/label_prop.rs:450-461   launch_hadamard_sym
+//   pca_init + small-graph norm . src/label_prop.rs:251-309   pca_kernel
+//   final centring / scaling .... src/label_prop.rs:660-672   center_* kernels
+//   make_epochs_per_sample ...... src/embed.rs:10-23          ne_schedule_kernel
+//   node_embedding_epoch_repr ... src/embed.rs:138-248        ne_block_kernel, ne_apply_kernel
+//
+// Every result matches the reference's rounding: f32 expressions are written
+// with __fmul_rn / __fadd_rn / __fsub_rn / __fdiv_rn / __fsqrt_rn so nvcc
+// cannot contract them into FMAs, and every order-dependent sum runs in the
+// reference's order.  Where the reference is serial (the outlier walk, the
+// per-part and per-row sums) the GPU runs independent rows / parts / columns
+// in parallel and each of them serially.
+//
+// The SciPy SMMP products keep SciPy's output order (each row's columns in
+// reverse order of first appearance), which the recursion's vote order and
+// the embedding's edge order depend on.  Instead of a per-row linked list the
+// product is formed by stable radix sorts:
+//   temp = N^T G:  edge e of row i (part p = part[i]) contributes x_p * g_e to
+//     (p, j); sorting the edges by (p, j), stable in e, lists each group's
+//     contributions in the reference's accumulation order (members ascending,
+//     then row order), and the group's first e is its first appearance.
+//   reduced = temp R:  temp entries sorted by (p, q = part[j], descending first
+//     e) list each (p, q) group in temp's row order; a group's head (largest
+//     first e) is where q first appears, so the row's output order is the
+//     heads' first e ascending.
+#include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
+
+#include "lp.h"
+
+namespace evoc {
+namespace lp {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int32_t kNoKey = INT32_MIN;
+
+// tau RNG step, src/rng.rs:5-35 (int64 state words, 32-bit result).
+__device__ int32_t tau_rand_int(int64_t st[3]) {
+  auto shl = [](int64_t v, int sh) { return (int64_t)((uint64_t)v << sh); };
+  st[0] = (shl(st[0] & 4294967294LL, 12) & 0xFFFFFFFFLL) ^ (((shl(st[0], 13) & 0xFFFFFFFFLL) ^ st[0]) >> 19);
+  st[1] = (shl(st[1] & 4294967288LL, 4) & 0xFFFFFFFFLL) ^ (((shl(st[1], 2) & 0xFFFFFFFFLL) ^ st[1]) >> 25);
+  st[2] = (shl(st[2] & 4294967280LL, 17) & 0xFFFFFFFFLL) ^ (((shl(st[2], 3) & 0xFFFFFFFFLL) ^ st[2]) >> 11);
+  return (int32_t)(uint32_t)(uint64_t)(st[0] ^ st[1] ^ st[2]);
+}
+
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+
+// Adds one chunk of up to 32 consecutive entries (lane order = entry order)
+// to an ordered table: keys in order of first appearance, each key's sum
+// built by adding its values in entry order, the first value stored as is.
+// Returns false, with the table as before the chunk, when the chunk's new
+// keys do not fit in `cap` slots.
+template <class Acc>
+__device__ bool table_chunk(int32_t key, Acc val, bool valid, int32_t* tkey, Acc* tsum, int cap, int& cnt) {
+  const int lane = threadIdx.x & 31;
+  const int32_t k = valid ? key : kNoKey;
+  const unsigned peers = __match_any_sync(kFull, k);
+  const bool leader = valid && (__ffs(peers) - 1 == lane);
+  int slot = -1;
+  if (leader)
+    for (int t = 0; t < cnt; t++)
+      if (tkey[t] == k) {
+        slot = t;
+        break;
+      }
+  const unsigned newm = __ballot_sync(kFull, leader && slot < 0);
+  if (cnt + __popc(newm) > cap) return false;
+  const bool fresh = leader && slot < 0;
+  if (fresh) slot = cnt + __popc(newm & ((1u << lane) - 1u));
+  const int gmax = __reduce_max_sync(kFull, leader ? __popc(peers) : 0);
+  Acc acc = (leader && !fresh) ? tsum[slot] : Acc(0);
+  unsigned rem = leader ? peers : 0u;
+  for (int it = 0; it < gmax; it++) {
+    const int src = rem ? __ffs(rem) - 1 : lane;
+    const Acc v = __shfl_sync(kFull, val, src);
+    if (rem) {
+      acc = (fresh && it == 0) ? v : add_rn(acc, v);
+      rem &= rem - 1u;
+    }
+  }
+  if (leader) {
+    if (fresh) tkey[slot] = k;
+    tsum[slot] = acc;
+  }
+  cnt += __popc(newm);
+  __syncwarp();
+  return true;
+}
+
+// ------------------------------------------------------------------ label propagation
+
+// Votes of row r in first-appearance order; *res = the label of the last vote
+// equal to max(1.0, largest vote), skipping label -1; cur when there is none
+// (the reference's loop, src/label_prop.rs:71-88, with cur == -1 for every
+// row that reaches it).
+__device__ bool vote_row(const Csr& g, int64_t r, const int32_t* lab, int32_t* tkey, double* tsum, int cap,
+                         int32_t cur, int32_t* res) {
+  const int lane = threadIdx.x & 31;
+  const int64_t s = g.indptr[r], e = g.indptr[r + 1];
+  int cnt = 0;
+  for (int64_t b = s; b < e; b += 32) {
+    const int64_t k = b + lane;
+    const bool valid = k < e;
+    int32_t l = 0;
+    double w = 0.0;
+    if (valid) {
+      l = lab[g.indices[k]];
+      w = (double)g.data[k];
+    }
+    if (!table_chunk<double>(l, w, valid, tkey, tsum, cap, cnt)) return false;
+  }
+  double m = 1.0;
+  for (int t = lane; t < cnt; t += 32)
+    if (tkey[t] != -1) m = fmax(m, tsum[t]);
+  for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(kFull, m, o));
+  int last = -1;
+  for (int t = lane; t < cnt; t += 32)
+    if (tkey[t] != -1 && tsum[t] == m) last = t;
+  last = __reduce_max_sync(kFull, last);
+  *res = last >= 0 ? tkey[last] : cur;
+  return true;
+}
+
+__global__ void __launch_bounds__(kRowWarps * 32)
+    lp_iteration_kernel(Csr g, const int32_t* lab_in, int32_t* lab_out, int32_t* overflow, int32_t* n_overflow) {
+  __shared__ int32_t skey[kRowWarps][kVoteSlots];
+  __shared__ double ssum[kRowWarps][kVoteSlots];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t)gridDim.x * kRowWarps;
+  for (int64_t r = (int64_t)blockIdx.x * kRowWarps + warp; r < g.n; r += nw) {
+    const int32_t cur = lab_in[r];
+    int32_t res = cur;
+    if (cur < 0 && !vote_row(g, r, lab_in, skey[warp], ssum[warp], kVoteSlots, cur, &res)) {
+      if (lane == 0) overflow[atomicAdd(n_overflow, 1)] = (int32_t)r;
+      continue;
+    }
+    if (lane == 0) lab_out[r] = res;
+  }
+}
+
+__global__ void __launch_bounds__(kRowWarps * 32)
+    lp_overflow_kernel(Csr g, const int32_t* lab_in, int32_t* lab_out, const int32_t* overflow,
+                       const int32_t* n_overflow, int32_t* skey, double* ssum, int64_t cap) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t gw = (int64_t)blockIdx.x * kRowWarps + warp, nw = (int64_t)gridDim.x * kRowWarps;
+  const int32_t cnt = *n_overflow;
+  for (int64_t i = gw; i < cnt; i += nw) {
+    const int64_t r = overflow[i];
+    int32_t res = lab_in[r];
+    vote_row(g, r, lab_in, skey + gw * cap, ssum + gw * cap, (int)cap, res, &res);
+    if (lane == 0) lab_out[r] = res;
+  }
+}
+
+__global__ void max_degree_kernel(const int64_t* indptr, int64_t n, int64_t* out) {
+  int64_t m = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    m = max(m, indptr[i + 1] - indptr[i]);
+  for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(kFull, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax((unsigned long long*)out, (unsigned long long)m);
+}
+
+// Caller graphs: indptr[0] == 0, non-decreasing, indptr[n] == nnz, columns in [0, n).
+__global__ void validate_csr_kernel(Csr g, int32_t* bad) {
+  const int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, step = (int64_t)gridDim.x * blockDim.x;
+  if (i0 == 0 && (g.indptr[0] != 0 || g.indptr[g.n] != g.nnz)) atomicExch(bad, 1);
+  for (int64_t i = i0; i < g.n; i += step)
+    if (g.indptr[i + 1] < g.indptr[i]) atomicExch(bad, 1);
+  for (int64_t e = i0; e < g.nnz; e += step)
+    if (g.indices[e] < 0 || g.indices[e] >= g.n) atomicExch(bad, 1);
+}
+
+__global__ void seed_labels_kernel(int32_t* labels, const int64_t* idx, int64_t count) {
+  for (int64_t i = 0; i < count; i++) labels[idx[i]] = (int32_t)i;
+}
+
+// label_outliers: one warp walks the unlabelled rows in row order.  The
+// stack holds at most 1 + 64 * max_deg entries (64 pops, each pushing at most
+// one row's columns); a walk that would pass `cap` sets status and stops.
+__global__ void lp_outliers_kernel(Csr g, int32_t* labels, const int64_t* rs_p, int32_t* stack, int64_t cap,
+                                   int32_t* status) {
+  const int lane = threadIdx.x & 31;
+  int32_t ml = 0;
+  for (int64_t i = lane; i < g.n; i += 32) ml = max(ml, labels[i]);
+  ml = __reduce_max_sync(kFull, ml);
+  const int64_t rs0 = rs_p[0], rs1 = rs_p[1], rs2 = rs_p[2];
+  for (int64_t base = 0; base < g.n; base += 32) {
+    const int64_t i = base + lane;
+    unsigned m = __ballot_sync(kFull, i < g.n && labels[i] < 0);
+    while (m) {
+      const int64_t row = base + __ffs(m) - 1;
+      m &= m - 1u;
+      if (lane == 0) stack[0] = (int32_t)row;
+      __syncwarp();
+      int64_t top = 1;
+      bool unl = true;
+      int it = 0;
+      while (unl && it < 64 && top > 0) {
+        it++;
+        top--;
+        const int64_t node = stack[top];
+        const int64_t s = g.indptr[node], e = g.indptr[node + 1];
+        for (int64_t b = s; b < e; b += 32) {
+          const int64_t k = b + lane;
+          const bool valid = k < e;
+          const int32_t j = valid ? g.indices[k] : 0;
+          const int32_t lj = valid ? labels[j] : -1;
+          const unsigned hit = __ballot_sync(kFull, valid && lj >= 0);
+          const int npush = hit ? __ffs(hit) - 1 : __popc(__ballot_sync(kFull, valid));
+          if (top + npush > cap) {
+            if (lane == 0) atomicExch(status, 1);
+            return;
+          }
+          if (lane < npush) stack[top + lane] = j;
+          top += npush;
+          if (hit) {
+            const int32_t lab = __shfl_sync(kFull, lj, __ffs(hit) - 1);
+            if (lane == 0) labels[row] = lab;
+            unl = false;
+            break;
+          }
+        }
+        __syncwarp();
+      }
+      if (lane == 0 && (it >= 64 || unl)) {
+        int64_t st[3] = {(int64_t)((uint64_t)rs0 + (uint64_t)row), (int64_t)((uint64_t)rs1 + (uint64_t)row),
+                         (int64_t)((uint64_t)rs2 + (uint64_t)row)};
+        const int64_t draw = tau_rand_int(st);
+        const int64_t mod = (int64_t)ml + 1;
+        const int64_t v = draw % mod;
+        labels[row] = (int32_t)(v < 0 ? v + mod : v);
+      }
+      __syncwarp();
+    }
+  }
+}
+
+__global__ void remap_flags_kernel(const int32_t* labels, int64_t n, int32_t bound, int32_t* flags,
+                                   int32_t* status) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t l = labels[i];
+    if (l < 0 || l >= bound) atomicExch(status, 2);
+    else flags[l] = 1;
+  }
+}
+
+__global__ void remap_apply_kernel(int32_t* labels, int64_t n, int32_t bound, const int32_t* flags,
+                                   const int32_t* map, int32_t* n_parts) {
+  const int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i0 == 0) *n_parts = map[bound - 1] + flags[bound - 1];
+  for (int64_t i = i0; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t l = labels[i];
+    if (l >= 0 && l < bound) labels[i] = map[l];
+  }
+}
+
+// ------------------------------------------------------------------ partition maps
+
+__global__ void part_count_kernel(const int32_t* part, int64_t n, int32_t* count, int32_t* iota) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    atomicAdd(&count[part[i]], 1);
+    iota[i] = (int32_t)i;
+  }
+}
+
+__global__ void part_start_kernel(const int32_t* sorted_part, int64_t n, int64_t* start) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    if (i == 0 || sorted_part[i] != sorted_part[i - 1]) start[sorted_part[i]] = i;
+}
+
+// normalize_cols_l2 of the 0/1 reduction map (column sums of 1.0*1.0 = the
+// part size) and normalize_rows_l1 of its transpose (|x_p| added c_p times).
+__global__ void part_norm_kernel(const int32_t* count, int32_t n_parts, float* xnorm, float* wred) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n_parts; p += gridDim.x * blockDim.x) {
+    const int32_t c = count[p];
+    float sq = 0.0f;
+    for (int32_t t = 0; t < c; t++) sq = __fadd_rn(sq, 1.0f);
+    const float norm = fmaxf(__fsqrt_rn(sq), 1e-12f);
+    const float x = __fdiv_rn(1.0f, norm);
+    float s = 0.0f;
+    for (int32_t t = 0; t < c; t++) s = __fadd_rn(s, fabsf(x));
+    s = fmaxf(s, 1e-12f);
+    xnorm[p] = x;
+    wred[p] = __fdiv_rn(x, s);
+  }
+}
+
+constexpr int kRedCols = 8;  // columns per lane per pass
+
+__global__ void __launch_bounds__(256)
+    reduce_data_kernel(const float* x, int64_t d, const int32_t* members, const int64_t* start, const int32_t* count,
+                       const float* wred, int32_t n_parts, float* out) {
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t p = gw; p < n_parts; p += nw) {
+    const double w = (double)wred[p];
+    const int64_t s0 = start[p];
+    const int32_t c = count[p];
+    for (int64_t col0 = 0; col0 < d; col0 += 32 * kRedCols) {
+      float acc[kRedCols];
+#pragma unroll
+      for (int q = 0; q < kRedCols; q++) acc[q] = 0.0f;
+      for (int32_t t = 0; t < c; t++) {
+        const float* row = x + (int64_t)members[s0 + t] * d;
+#pragma unroll
+        for (int q = 0; q < kRedCols; q++) {
+          const int64_t col = col0 + q * 32 + lane;
+          if (col < d) acc[q] = __fadd_rn(acc[q], __double2float_rn(__dmul_rn(w, (double)row[col])));
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < kRedCols; q++) {
+        const int64_t col = col0 + q * 32 + lane;
+        if (col < d) out[p * d + col] = acc[q];
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------ SMMP reduction
+
+__device__ __forceinline__ int64_t row_of(const int64_t* indptr, int64_t n, int64_t e) {
+  int64_t lo = 0, hi = n;  // largest r with indptr[r] <= e
+  while (hi - lo > 1) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (indptr[mid] <= e) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Step 1: key (part of the edge's row, column), value = edge index.
+__global__ void edge_keys_kernel(Csr g, const int32_t* part, uint64_t* key, uint32_t* val) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < g.nnz; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = row_of(g.indptr, g.n, e);
+    key[e] = ((uint64_t)(uint32_t)part[r] << 32) | (uint32_t)g.indices[e];
+    val[e] = (uint32_t)e;
+  }
+}
+
+// Head flags of runs of equal (key >> shift).
+__global__ void head_flags_kernel(const uint64_t* key, int64_t m, int shift, int32_t* flag) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x)
+    flag[i] = (i == 0 || (key[i] >> shift) != (key[i - 1] >> shift)) ? 1 : 0;
+}
+
+// Step 2: temp entries.  One thread per (p, j) group: the f32 sum of x_p * g_e
+// in edge order; nonzero sums become (p, q = part[j], ~first e) keys whose
+// value is the sum's bits.
+__global__ void temp_groups_kernel(const uint64_t* key, const uint32_t* val, int64_t m, const int32_t* pos,
+                                   const int32_t* n_groups, const float* gdata, const float* xnorm,
+                                   const int32_t* part, int qshift, uint64_t* okey, uint32_t* oval,
+                                   int32_t* counter) {
+  const int32_t ng = *n_groups;
+  for (int64_t gi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; gi < ng; gi += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t st = pos[gi], en = gi + 1 < ng ? pos[gi + 1] : m;
+    const uint32_t p = (uint32_t)(key[st] >> 32);
+    const uint32_t j = (uint32_t)key[st];
+    const float x = xnorm[p];
+    float acc = 0.0f;
+    for (int64_t t = st; t < en; t++) acc = __fadd_rn(acc, __fmul_rn(x, gdata[val[t]]));
+    if (acc != 0.0f) {
+      const int32_t o = atomicAdd(counter, 1);
+      const uint32_t q = (uint32_t)part[j];
+      okey[o] = ((uint64_t)p << (32 + qshift)) | ((uint64_t)q << 32) | (uint64_t)(0xffffffffu - val[st]);
+      oval[o] = __float_as_uint(acc);
+    }
+  }
+}
+
+// Step 3: reduced entries.  One thread per (p, q) group of sorted temp
+// entries: the f32 sum of temp * 1.0 in temp's row order; nonzero sums become
+// (p, first e of the group's head) keys with (q, sum) kept aside by index.
+__global__ void reduced_groups_kernel(const uint64_t* key, const uint32_t* val, int64_t m, const int32_t* pos,
+                                      const int32_t* n_groups, int qshift, uint64_t* okey, uint32_t* oidx,
+                                      uint32_t* oq, uint32_t* osum, int32_t* counter) {
+  const int32_t ng = *n_groups;
+  const uint64_t qmask = (1ull << qshift) - 1ull;
+  for (int64_t gi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; gi < ng; gi += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t st = pos[gi], en = gi + 1 < ng ? pos[gi + 1] : m;
+    float acc = 0.0f;
+    for (int64_t t = st; t < en; t++) acc = __fadd_rn(acc, __fmul_rn(__uint_as_float(val[t]), 1.0f));
+    if (acc != 0.0f) {
+      const int32_t o = atomicAdd(counter, 1);
+      const uint64_t k = key[st];
+      const uint32_t p = (uint32_t)(k >> (32 + qshift));
+      const uint32_t q = (uint32_t)((k >> 32) & qmask);
+      const uint32_t head_e = 0xffffffffu - (uint32_t)k;
+      okey[o] = ((uint64_t)p << 32) | head_e;
+      oidx[o] = (uint32_t)o;
+      oq[o] = q;
+      osum[o] = __float_as_uint(acc);
+    }
+  }
+}
+
+__global__ void row_count_kernel(const uint64_t* key, int64_t m, int shift, int64_t* count) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x)
+    atomicAdd((unsigned long long*)&count[key[i] >> shift], 1ull);
+}
+
+// Step 4: the reduced CSR, clamped to [0, 1].
+__global__ void reduced_write_kernel(const uint32_t* idx, int64_t m, const uint32_t* oq, const uint32_t* osum,
+                                     int32_t* r_indices, float* r_data) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t i = idx[t];
+    r_indices[t] = (int32_t)oq[i];
+    r_data[t] = fminf(fmaxf(__uint_as_float(osum[i]), 0.0f), 1.0f);
+  }
+}
+
+// Exclusive scan of `count` (m entries) into indptr (m + 1), one block.
+__global__ void __launch_bounds__(1024) scan_i64_kernel(const int64_t* count, int64_t m, int64_t* indptr) {
+  __shared__ int64_t part[1024];
+  const int t = threadIdx.x;
+  const int64_t per = (m + 1023) / 1024;
+  const int64_t b = t * per, e = min(m, b + per);
+  int64_t s = 0;
+  for (int64_t i = b; i < e; i++) s += count[i];
+  part[t] = s;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    const int64_t v = t >= o ? part[t - o] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  int64_t run = part[t] - s;
+  for (int64_t i = b; i < e; i++) {
+    indptr[i] = run;
+    run += count[i];
+  }
+  if (t == 1023) indptr[m] = part[1023];
+}
+
+// ------------------------------------------------------------------ hadamard_symmetric
+
+__global__ void sorted_flag_kernel(Csr g, int32_t* unsorted) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < g.nnz; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = row_of(g.indptr, g.n, e);
+    if (e > g.indptr[r] && g.indices[e] <= g.indices[e - 1]) atomicExch(unsorted, 1);
+  }
+}
+
+__global__ void row_col_keys_kernel(Csr g, uint64_t* key, uint32_t* val) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < g.nnz; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = row_of(g.indptr, g.n, e);
+    key[e] = ((uint64_t)r << 32) | (uint32_t)g.indices[e];
+    val[e] = __float_as_uint(g.data[e]);
+  }
+}
+
+// Entry (r, c, v) of the row-sorted graph keeps v * G[c, r] when G[c, r] != 0.
+__global__ void sym_keep_kernel(const int64_t* indptr, int64_t n, int64_t nnz, const uint64_t* key,
+                                const uint32_t* val, int32_t* keep, uint32_t* prod, int64_t* rcount) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t r = (uint32_t)(key[e] >> 32), c = (uint32_t)key[e];
+    int64_t lo = indptr[c], hi = indptr[c + 1];
+    const uint64_t want = ((uint64_t)c << 32) | r;
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (key[mid] < want) lo = mid + 1;
+      else hi = mid;
+    }
+    const float other = (lo < indptr[c + 1] && key[lo] == want) ? __uint_as_float(val[lo]) : 0.0f;
+    const int k = other != 0.0f;
+    keep[e] = k;
+    prod[e] = __float_as_uint(__fmul_rn(__uint_as_float(val[e]), other));
+    if (k) atomicAdd((unsigned long long*)&rcount[r], 1ull);
+  }
+}
+
+__global__ void sym_write_kernel(const uint64_t* key, const uint32_t* prod, const int32_t* keep,
+                                 const int32_t* dst, int64_t nnz, int32_t* s_indices, float* s_data) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += (int64_t)gridDim.x * blockDim.x)
+    if (keep[e]) {
+      s_indices[dst[e]] = (int32_t)(uint32_t)key[e];
+      s_data[dst[e]] = __uint_as_float(prod[e]);
+    }
+}
+
+// ------------------------------------------------------------------ expander
+
+// Row r of data_expander = SMMP(sym, N): part sums in first-appearance order,
+// stored (and summed for the L1 norm, and multiplied into the layout) in
+// reverse order; then the average with the row's own part layout.
+__device__ bool expand_row(const Csr& sym, int64_t r, const int32_t* part, const float* xnorm, const float* layout,
+                           int ncomp, int32_t* tkey, float* tsum, int cap, float* result) {
+  const int lane = threadIdx.x & 31;
+  const int64_t s = sym.indptr[r], e = sym.indptr[r + 1];
+  int cnt = 0;
+  for (int64_t b = s; b < e; b += 32) {
+    const int64_t k = b + lane;
+    const bool valid = k < e;
+    int32_t q = 0;
+    float v = 0.0f;
+    if (valid) {
+      q = part[sym.indices[k]];
+      v = __fmul_rn(sym.data[k], xnorm[q]);
+    }
+    if (!table_chunk<float>(q, v, valid, tkey, tsum, cap, cnt)) return false;
+  }
+  float rs = 0.0f;
+  for (int t = cnt - 1; t >= 0; t--) {
+    const float v = tsum[t];
+    if (v != 0.0f) rs = __fadd_rn(rs, fabsf(v));
+  }
+  rs = fmaxf(rs, 1e-12f);
+  if (lane < ncomp) {
+    float a = 0.0f;
+    for (int t = cnt - 1; t >= 0; t--) {
+      const float v = tsum[t];
+      if (v == 0.0f) continue;
+      const double vn = (double)__fdiv_rn(v, rs);
+      a = __fadd_rn(a, __double2float_rn(__dmul_rn(vn, (double)layout[(int64_t)tkey[t] * ncomp + lane])));
+    }
+    const float bb = __fadd_rn(0.0f, layout[(int64_t)part[r] * ncomp + lane]);
+    result[r * ncomp + lane] = __double2float_rn(__dmul_rn(__dadd_rn((double)a, (double)bb), 0.5));
+  }
+  __syncwarp();
+  return true;
+}
+
+__global__ void __launch_bounds__(kRowWarps * 32)
+    expand_kernel(Csr sym, const int32_t* part, const float* xnorm, const float* layout, int ncomp, float* result,
+                  int32_t* overflow, int32_t* n_overflow) {
+  __shared__ int32_t skey[kRowWarps][kVoteSlots];
+  __shared__ float ssum[kRowWarps][kVoteSlots];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t)gridDim.x * kRowWarps;
+  for (int64_t r = (int64_t)blockIdx.x * kRowWarps + warp; r < sym.n; r += nw)
+    if (!expand_row(sym, r, part, xnorm, layout, ncomp, skey[warp], ssum[warp], kVoteSlots, result) && lane == 0)
+      overflow[atomicAdd(n_overflow, 1)] = (int32_t)r;
+}
+
+__global__ void __launch_bounds__(kRowWarps * 32)
+    expand_overflow_kernel(Csr sym, const int32_t* part, const float* xnorm, const float* layout, int ncomp,
+                           float* result, const int32_t* overflow, const int32_t* n_overflow, int32_t* skey,
+                           float* ssum, int64_t cap) {
+  const int warp = threadIdx.x >> 5;
+  const int64_t gw = (int64_t)blockIdx.x * kRowWarps + warp, nw = (int64_t)gridDim.x * kRowWarps;
+  const int32_t cnt = *n_overflow;
+  for (int64_t i = gw; i < cnt; i += nw)
+    expand_row(sym, overflow[i], part, xnorm, layout, ncomp, skey + gw * cap, ssum + gw * cap, (int)cap, result);
+}
+
+// Column means summed in row order (f64), one thread per column, rows staged
+// through shared memory.
+__global__ void __launch_bounds__(1024) center_mean_kernel(const float* result, int64_t n, int ncomp, double* mean) {
+  __shared__ float tile[8192];
+  const int rows_per = 8192 / ncomp;
+  double acc = 0.0;
+  for (int64_t r0 = 0; r0 < n; r0 += rows_per) {
+    const int64_t rows = min((int64_t)rows_per, n - r0);
+    __syncthreads();
+    for (int64_t i = threadIdx.x; i < rows * ncomp; i += blockDim.x) tile[i] = result[r0 * ncomp + i];
+    __syncthreads();
+    if (threadIdx.x < ncomp)
+      for (int64_t r = 0; r < rows; r++) acc = __dadd_rn(acc, (double)tile[r * ncomp + threadIdx.x]);
+  }
+  if (threadIdx.x < ncomp) mean[threadIdx.x] = __ddiv_rn(acc, (double)n);
+}
+
+__global__ void center_apply_kernel(const float* result, int64_t n, int ncomp, float scaling, const double* mean,
+                                    float* out) {
+  const int64_t total = n * ncomp;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = __double2float_rn(__dmul_rn((double)scaling, __dsub_rn((double)result[i], mean[i % ncomp])));
+}
+
+// ------------------------------------------------------------------ PCA base init
+
+constexpr int kPcaMax = 64;
+
+// One block.  Centred rows X (f64, f32 column means), Gram G = X X^T, cyclic
+// Jacobi (one warp) for G's eigenpairs; component j = sign_j * sqrt(l_j) *
+// u_j with the sign that makes the largest-|.| entry of X^T u_j (the last on
+// ties) non-negative; then the small-graph normalisation.
+__global__ void __launch_bounds__(256) pca_kernel(const float* x, int64_t n, int64_t d, int ncomp, float* out,
+                                                  float* mean_ws, double* vws, int32_t* status) {
+  extern __shared__ double sh[];
+  double* A = sh;                    // n x n
+  double* V = sh + kPcaMax * kPcaMax;  // n x n
+  __shared__ double s_eval[kPcaMax];
+  __shared__ int s_order[kPcaMax];
+  __shared__ double s_sign[kPcaMax];
+  const int t = threadIdx.x;
+  const int nn = (int)n;
+  for (int64_t c = t; c < d; c += blockDim.x) {
+    float m = 0.0f;
+    for (int i = 0; i < nn; i++) m = __fadd_rn(m, x[(int64_t)i * d + c]);
+    mean_ws[c] = __fdiv_rn(m, (float)nn);
+  }
+  __syncthreads();
+  for (int pq = t; pq < nn * nn; pq += blockDim.x) {
+    const int a = pq / nn, b = pq % nn;
+    if (b < a) continue;
+    double s = 0.0;
+    for (int64_t c = 0; c < d; c++) {
+      const double mc = (double)mean_ws[c];
+      s += ((double)x[(int64_t)a * d + c] - mc) * ((double)x[(int64_t)b * d + c] - mc);
+    }
+    A[a * kPcaMax + b] = s;
+    A[b * kPcaMax + a] = s;
+  }
+  for (int i = t; i < kPcaMax * kPcaMax; i += blockDim.x) V[i] = (i / kPcaMax == i % kPcaMax) ? 1.0 : 0.0;
+  __syncthreads();
+  if (t < 32) {
+    const int lane = t;
+    for (int sweep = 0; sweep < 60; sweep++) {
+      double off = 0.0, tot = 0.0;
+      for (int i = lane; i < nn * nn; i += 32) {
+        const int a = i / nn, b = i % nn;
+        const double v = A[a * kPcaMax + b] * A[a * kPcaMax + b];
+        tot += v;
+        if (a != b) off += v;
+      }
+      for (int o = 16; o; o >>= 1) {
+        off += __shfl_xor_sync(kFull, off, o);
+        tot += __shfl_xor_sync(kFull, tot, o);
+      }
+      if (off <= 1e-30 * tot || off == 0.0) break;
+      for (int p = 0; p < nn - 1; p++)
+        for (int q = p + 1; q < nn; q++) {
+          const double apq = A[p * kPcaMax + q];
+          if (apq == 0.0) continue;
+          const double tau = (A[q * kPcaMax + q] - A[p * kPcaMax + p]) / (2.0 * apq);
+          const double tt = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+          const double c = 1.0 / sqrt(1.0 + tt * tt), s = tt * c;
+          for (int k = lane; k < nn; k += 32) {
+            const double akp = A[k * kPcaMax + p], akq = A[k * kPcaMax + q];
+            A[k * kPcaMax + p] = c * akp - s * akq;
+            A[k * kPcaMax + q] = s * akp + c * akq;
+            const double vkp = V[k * kPcaMax + p], vkq = V[k * kPcaMax + q];
+            V[k * kPcaMax + p] = c * vkp - s * vkq;
+            V[k * kPcaMax + q] = s * vkp + c * vkq;
+          }
+          __syncwarp();
+          for (int k = lane; k < nn; k += 32) {
+            const double apk = A[p * kPcaMax + k], aqk = A[q * kPcaMax + k];
+            A[p * kPcaMax + k] = c * apk - s * aqk;
+            A[q * kPcaMax + k] = s * apk + c * aqk;
+          }
+          __syncwarp();
+        }
+    }
+    if (lane == 0) {
+      for (int i = 0; i < nn; i++) {
+        s_eval[i] = A[i * kPcaMax + i];
+        s_order[i] = i;
+      }
+      for (int i = 0; i < nn; i++)  // descending eigenvalues (stable selection)
+        for (int j = i + 1; j < nn; j++)
+          if (s_eval[s_order[j]] > s_eval[s_order[i]]) {
+            const int tmp = s_order[i];
+            s_order[i] = s_order[j];
+            s_order[j] = tmp;
+          }
+    }
+  }
+  __syncthreads();
+  const int kc = min(ncomp, min(nn, d < kPcaMax ? (int)d : kPcaMax));
+  // signs from X^T u_j: per component, the block finds the last largest |entry|
+  for (int j = 0; j < kc; j++) {
+    const int col = s_order[j];
+    for (int64_t c = t; c < d; c += blockDim.x) {
+      const double mc = (double)mean_ws[c];
+      double v = 0.0;
+      for (int i = 0; i < nn; i++) v += ((double)x[(int64_t)i * d + c] - mc) * V[i * kPcaMax + col];
+      vws[c] = v;
+    }
+    __syncthreads();
+    if (t == 0) {
+      double best = -1.0, bv = 0.0;
+      for (int64_t c = 0; c < d; c++)
+        if (fabs(vws[c]) >= best) {
+          best = fabs(vws[c]);
+          bv = vws[c];
+        }
+      s_sign[j] = bv >= 0.0 ? 1.0 : -1.0;
+    }
+    __syncthreads();
+  }
+  for (int i = t; i < nn * ncomp; i += blockDim.x) {
+    const int r = i / ncomp, j = i % ncomp;
+    float v = 0.0f;
+    if (j < kc) {
+      const int col = s_order[j];
+      const double sv = sqrt(fmax(s_eval[col], 0.0));
+      v = (float)(s_sign[j] * V[r * kPcaMax + col] * sv);
+    }
+    out[i] = v;
+  }
+  __syncthreads();
+  if (t == 0) {
+    double m = 0.0;
+    for (int i = 0; i < nn * ncomp; i++) m = __dadd_rn(m, (double)out[i]);
+    m = __ddiv_rn(m, (double)(nn * ncomp));
+    float lo = INFINITY, hi = -INFINITY;
+    for (int i = 0; i < nn * ncomp; i++) {
+      const float v = __double2float_rn(__dsub_rn((double)out[i], m));
+      out[i] = v;
+      lo = fminf(lo, v);
+      hi = fmaxf(hi, v);
+    }
+    const float scale = __fdiv_rn(__fsub_rn(hi, lo), 2.0f);
+    if (scale > 0.0f)
+      for (int i = 0; i < nn * ncomp; i++) out[i] = __fdiv_rn(out[i], scale);
+  }
+}
+
+// ------------------------------------------------------------------ node embedding
+
+__global__ void ne_maxw_kernel(const float* w, int64_t m, float* max_w) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x)
+    if (w[i] > 0.0f) atomicMax((int*)max_w, __float_as_int(w[i]));
+}
+
+__global__ void ne_schedule_kernel(const float* w, int64_t m, float nf, float nsr, const float* max_w, float* eps,
+                                   float* epns, float* eonn, float* eons) {
+  const float mx = *max_w;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
+    float e;
+    if (mx == 0.0f) {
+      e = nf;
+    } else {
+      float ns = __fmul_rn(nf, __fdiv_rn(w[i], mx));
+      if (!(ns >= 1.0f)) ns = 1.0f;
+      e = __fdiv_rn(nf, ns);
+    }
+    float en = __fdiv_rn(e, nsr);
+    en = __fmul_rn(en, 1.5f);
+    eps[i] = e;
+    eons[i] = e;
+    epns[i] = en;
+    eonn[i] = en;
+  }
+}
+
+__device__ __forceinline__ uint64_t neg_count(float nf, float eon, float rate) {
+  const float v = __fdiv_rn(__fsub_rn(nf, eon), rate);
+  if (v <= 0.0f) return 0;
+  if (v != v) return 0;
+  if (v >= 2147483648.0f) return 2147483647ull;
+  return (uint64_t)(int32_t)v;
+}
+
+__device__ __forceinline__ float clip4(float v) { return v > 4.0f ? 4.0f : (v < -4.0f ? -4.0f : v); }
+
+template <int MAXD>
+__global__ void __launch_bounds__(128)
+    ne_block_kernel(Csr g, float* emb, float* upd, const uint32_t* order, int64_t bs, int64_t be, const float* eps,
+                    const float* epns, float* eonn, float* eons, uint32_t rng_state, int ncomp, float alpha,
+                    uint32_t epoch, float noise, float gamma, float decay, int apply_decay) {
+  const int64_t ni = bs + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (ni >= be) return;
+  const uint64_t nv = (uint64_t)g.n;
+  const uint64_t from = order[ni];
+  if (from >= nv) return;
+  float cur[MAXD], u[MAXD];
+#pragma unroll
+  for (int d = 0; d < MAXD; d++) {
+    if (d < ncomp) {
+      cur[d] = emb[from * ncomp + d];
+      u[d] = apply_decay ? __fmul_rn(upd[from * ncomp + d], decay) : upd[from * ncomp + d];
+    }
+  }
+  const float nf = (float)epoch;
+  const uint64_t e0 = (uint64_t)g.indptr[from], e1 = (uint64_t)g.indptr[from + 1];
+  for (uint64_t raw = e0; raw < e1; raw++) {
+    if (eons[raw] > nf) continue;
+    const uint64_t to = (uint64_t)(uint32_t)g.indices[raw];
+    if (to >= nv) continue;
+    const float* yt = emb + to * ncomp;
+    float ds = 0.0f;
+#pragma unroll
+    for (int d = 0; d < MAXD; d++)
+      if (d < ncomp) {
+        const float df = __fsub_rn(cur[d], yt[d]);
+        ds = __fadd_rn(ds, __fmul_rn(df, df));
+      }
+    if (ds > 0.0f) {
+      const float dist = __fsqrt_rn(ds);
+      const float num = __fsub_rn(__fmul_rn(__fmul_rn(-2.0f, noise), dist), 2.0f);
+      const float den = __fadd_rn(__fsub_rn(__fmul_rn(2.0f, ds), __fmul_rn(0.5f, dist)), 1.0f);
+      const float gc = __fdiv_rn(num, den);
+#pragma unroll
+      for (int d = 0; d < MAXD; d++)
+        if (d < ncomp) u[d] = __fadd_rn(u[d], __fmul_rn(__fmul_rn(gc, __fsub_rn(cur[d], yt[d])), alpha));
+    }
+    eons[raw] = __fadd_rn(eons[raw], eps[raw]);
+    const float rate = epns[raw];
+    const uint64_t nneg = neg_count(nf, eonn[raw], rate);
+    for (uint64_t p = 0; p < nneg; p++) {
+      const uint64_t idx = (raw * ((uint64_t)epoch + p + 1ull) * (uint64_t)rng_state) % nv;
+      const uint64_t tn = order[idx];
+      if (tn >= nv) continue;
+      const float* yn = emb + tn * ncomp;
+      float dn = 0.0f;
+#pragma unroll
+      for (int d = 0; d < MAXD; d++)
+        if (d < ncomp) {
+          const float df = __fsub_rn(cur[d], yn[d]);
+          dn = __fadd_rn(dn, __fmul_rn(df, df));
+        }
+      if (dn > 1e-2f) {
+        const float gc = __fdiv_rn(__fmul_rn(gamma, 4.0f), __fmul_rn(__fadd_rn(1.0f, __fmul_rn(0.25f, dn)), dn));
+        if (gc > 0.0f) {
+#pragma unroll
+          for (int d = 0; d < MAXD; d++)
+            if (d < ncomp) u[d] = __fadd_rn(u[d], __fmul_rn(clip4(__fmul_rn(gc, __fsub_rn(cur[d], yn[d]))), alpha));
+        }
+      }
+    }
+    eonn[raw] = __fadd_rn(eonn[raw], __fmul_rn(__ull2float_rn(nneg), rate));
+  }
+#pragma unroll
+  for (int d = 0; d < MAXD; d++)
+    if (d < ncomp) upd[from * ncomp + d] = u[d];
+}
+
+__global__ void ne_apply_kernel(float* emb, const float* upd, const uint32_t* order, int64_t bs, int64_t be,
+                                uint64_t nv, int ncomp) {
+  const int64_t total = (be - bs) * ncomp;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t from = order[bs + i / ncomp];
+    if (from >= nv) continue;
+    const uint64_t o = from * ncomp + i % ncomp;
+    emb[o] = __fadd_rn(emb[o], upd[o]);
+  }
+}
+
+inline int grid_for(int64_t work, int threads, int cap) {
+  const int64_t b = (work + threads - 1) / threads;
+  return (int)(b < 1 ? 1 : (b > cap ? cap : b));
+}
+
+int bits_for(int64_t v) {  // bits to hold values 0..v-1
+  int b = 1;
+  while ((int64_t(1) << b) < v) b++;
+  return b;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ launchers
+
+cudaError_t launch_max_degree(const int64_t* indptr, int64_t n, int64_t* out, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(out, 0, 8, s);
+  if (e != cudaSuccess) return e;
+  max_degree_kernel<<<grid_for(n, 256, 1184), 256, 0, s>>>(indptr, n, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_validate_csr(const Csr& g, int32_t* bad, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(bad, 0, 4, s);
+  if (e != cudaSuccess) return e;
+  validate_csr_kernel<<<grid_for(std::max(g.n, g.nnz), 256, 4096), 256, 0, s>>>(g, bad);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_seed_labels(int32_t* labels, const int64_t* idx, int64_t count, cudaStream_t s) {
+  if (count <= 0) return cudaSuccess;
+  seed_labels_kernel<<<1, 1, 0, s>>>(labels, idx, count);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lp_iteration(const Csr& g, const int32_t* lab_in, int32_t* lab_out, int32_t* overflow,
+                                int32_t* n_overflow, int32_t* scratch_key, double* scratch_sum, int64_t max_deg,
+                                int sms, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(n_overflow, 0, 4, s);
+  if (e != cudaSuccess) return e;
+  const int grid = grid_for(g.n, kRowWarps, sms * 8);
+  lp_iteration_kernel<<<grid, kRowWarps * 32, 0, s>>>(g, lab_in, lab_out, overflow, n_overflow);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (max_deg > kVoteSlots) {
+    lp_overflow_kernel<<<sms, kRowWarps * 32, 0, s>>>(g, lab_in, lab_out, overflow, n_overflow, scratch_key,
+                                                      scratch_sum, max_deg);
+    e = cudaGetLastError();
+  }
+  return e;
+}
+
+cudaError_t launch_lp_outliers(const Csr& g, int32_t* labels, const int64_t* rs, int32_t* stack, int64_t stack_cap,
+                               int32_t* status, cudaStream_t s) {
+  lp_outliers_kernel<<<1, 32, 0, s>>>(g, labels, rs, stack, stack_cap, status);
+  return cudaGetLastError();
+}
+
+size_t lp_remap_tmp_bytes(int32_t bound) {
+  size_t b = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, b, (int32_t*)nullptr, (int32_t*)nullptr, bound);
+  return b;
+}
+
+cudaError_t launch_lp_remap(int32_t* labels, int64_t n, int32_t bound, int32_t* flags, int32_t* map,
+                            int32_t* n_parts, int32_t* status, void* tmp, size_t tmp_bytes, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(flags, 0, size_t(bound) * 4, s);
+  if (e != cudaSuccess) return e;
+  remap_flags_kernel<<<grid_for(n, 256, 1184), 256, 0, s>>>(labels, n, bound, flags, status);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  e = cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, flags, map, bound, s);
+  if (e != cudaSuccess) return e;
+  remap_apply_kernel<<<grid_for(n, 256, 1184), 256, 0, s>>>(labels, n, bound, flags, map, n_parts);
+  return cudaGetLastError();
+}
+
+size_t part_members_tmp_bytes(int64_t n, int32_t n_parts) {
+  size_t b = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, b, (const int32_t*)nullptr, (int32_t*)nullptr, (const int32_t*)nullptr,
+                                  (int32_t*)nullptr, (int)n, 0, bits_for(n_parts));
+  return b;
+}
+
+cudaError_t launch_part_members(const int32_t* part, int64_t n, int32_t n_parts, int32_t* count, int64_t* start,
+                                int32_t* members, float* xnorm, float* wred, void* tmp, size_t tmp_bytes,
+                                int32_t* keys_tmp, int32_t* vals_tmp, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(count, 0, size_t(n_parts) * 4, s);
+  if (e != cudaSuccess) return e;
+  part_count_kernel<<<grid_for(n, 256, 1184), 256, 0, s>>>(part, n, count, vals_tmp);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  e = cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, part, keys_tmp, vals_tmp, members, (int)n, 0,
+                                      bits_for(n_parts), s);
+  if (e != cudaSuccess) return e;
+  part_start_kernel<<<grid_for(n, 256, 1184), 256, 0, s>>>(keys_tmp, n, start);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  part_norm_kernel<<<grid_for(n_parts, 128, 1184), 128, 0, s>>>(count, n_parts, xnorm, wred);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_data(const float* x, int64_t d, const int32_t* members, const int64_t* start,
+                               const int32_t* count, const float* wred, int32_t n_parts, float* out, int sms,
+                               cudaStream_t s) {
+  reduce_data_kernel<<<grid_for(int64_t(n_parts) * 32, 256, sms * 16), 256, 0, s>>>(x, d, members, start, count,
+                                                                                       wred, n_parts, out);
+  return cudaGetLastError();
+}
+
+size_t reduce_sort_tmp_bytes(int64_t nnz) {
+  size_t a = 0, b = 0, c = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, a, (const uint64_t*)nullptr, (uint64_t*)nullptr, (const uint32_t*)nullptr,
+                                  (uint32_t*)nullptr, (int)nnz, 0, 64);
+  cub::DeviceSelect::Flagged(nullptr, b, thrust::counting_iterator<int32_t>(0), (const int32_t*)nullptr,
+                             (int32_t*)nullptr, (int32_t*)nullptr, (int)nnz);
+  cub::DeviceScan::ExclusiveSum(nullptr, c, (const int64_t*)nullptr, (int64_t*)nullptr, (int)nnz + 1);
+  return std::max(a, std::max(b, c));
+}
+
+namespace {
+
+// Start positions of runs of equal (key >> shift): pos[0..*count).
+cudaError_t group_starts(const uint64_t* key, int64_t m, int shift, const ReduceScratch& w, int32_t* pos,
+                         int32_t* count, cudaStream_t s) {
+  head_flags_kernel<<<grid_for(m, 256, 4096), 256, 0, s>>>(key, m, shift, w.head);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  size_t tb = w.tmp_bytes;
+  return cub::DeviceSelect::Flagged(w.tmp, tb, thrust::counting_iterator<int32_t>(0), w.head, pos, count, (int)m,
+                                    s);
+}
+
+}  // namespace
+
+cudaError_t launch_reduce_graph(const Csr& g, const int32_t* part, const float* xnorm, int32_t n_parts,
+                                const ReduceScratch& w, int64_t* r_indptr, int32_t* r_indices, float* r_data,
+                                int64_t* r_nnz, cudaStream_t s) {
+  const int pb = bits_for(n_parts);
+  cudaError_t e;
+  int32_t* ctr = w.counter;  // [0] temp groups, [1] temp entries, [2] reduced groups, [3] reduced entries
+  if ((e = cudaMemsetAsync(ctr, 0, 16, s)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(w.rcount, 0, size_t(n_parts + 1) * 8, s)) != cudaSuccess) return e;
+  int32_t n_temp = 0, n_red = 0;
+  if (g.nnz > 0) {
+    // (part of row, column) keys, stable in edge order
+    edge_keys_kernel<<<grid_for(g.nnz, 256, 8192), 256, 0, s>>>(g, part, w.k0, w.v0);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    size_t tb = w.tmp_bytes;
+    e = cub::DeviceRadixSort::SortPairs(w.tmp, tb, w.k0, w.k1, w.v0, w.v1, (int)g.nnz, 0, 32 + pb, s);
+    if (e != cudaSuccess) return e;
+    if ((e = group_starts(w.k1, g.nnz, 0, w, w.pos, ctr + 0, s)) != cudaSuccess) return e;
+    temp_groups_kernel<<<grid_for(g.nnz, 256, 8192), 256, 0, s>>>(w.k1, w.v1, g.nnz, w.pos, ctr + 0, g.data, xnorm,
+                                                                  part, pb, w.k0, w.v0, ctr + 1);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(&n_temp, ctr + 1, 4, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+  }
+  if (n_temp > 0) {
+    // (p, q, descending first e): each (p, q) group in temp's row order
+    size_t tb = w.tmp_bytes;
+    e = cub::DeviceRadixSort::SortPairs(w.tmp, tb, w.k0, w.k1, w.v0, w.v1, n_temp, 0, 32 + 2 * pb, s);
+    if (e != cudaSuccess) return e;
+    if ((e = group_starts(w.k1, n_temp, 32, w, w.pos, ctr + 2, s)) != cudaSuccess) return e;
+    reduced_groups_kernel<<<grid_for(n_temp, 256, 8192), 256, 0, s>>>(w.k1, w.v1, n_temp, w.pos, ctr + 2, pb, w.k0,
+                                                                      w.v0, w.v2, w.v3, ctr + 3);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(&n_red, ctr + 3, 4, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+  }
+  if (n_red > 0) {
+    // rows in order of p, each row's parts by the first e of their heads
+    size_t tb = w.tmp_bytes;
+    e = cub::DeviceRadixSort::SortPairs(w.tmp, tb, w.k0, w.k1, w.v0, w.v1, n_red, 0, 32 + pb, s);
+    if (e != cudaSuccess) return e;
+    row_count_kernel<<<grid_for(n_red, 256, 8192), 256, 0, s>>>(w.k1, n_red, 32, w.rcount);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    reduced_write_kernel<<<grid_for(n_red, 256, 8192), 256, 0, s>>>(w.v1, n_red, w.v2, w.v3, r_indices, r_data);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  scan_i64_kernel<<<1, 1024, 0, s>>>(w.rcount, n_parts, r_indptr);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  const int64_t nr = n_red;
+  return cudaMemcpyAsync(r_nnz, &nr, 8, cudaMemcpyHostToDevice, s);
+}
+
+cudaError_t launch_hadamard_sym(const Csr& g, const ReduceScratch& w, int64_t* s_indptr, int32_t* s_indices,
+                                float* s_data, int64_t* s_nnz, cudaStream_t s) {
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(w.rcount, 0, size_t(g.n + 1) * 8, s)) != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(w.counter, 0, 16, s)) != cudaSuccess) return e;
+  if (g.nnz > 0) {
+    sorted_flag_kernel<<<grid_for(g.nnz, 256, 8192), 256, 0, s>>>(g, w.counter);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    int32_t unsorted = 0;
+    if ((e = cudaMemcpyAsync(&unsorted, w.counter, 4, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+    // (row, column) keys; rows already in column order skip the sort
+    row_col_keys_kernel<<<grid_for(g.nnz, 256, 8192), 256, 0, s>>>(g, unsorted ? w.k0 : w.k1,
+                                                                   unsorted ? w.v0 : w.v1);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (unsorted) {
+      size_t tb = w.tmp_bytes;
+      e = cub::DeviceRadixSort::SortPairs(w.tmp, tb, w.k0, w.k1, w.v0, w.v1, (int)g.nnz, 0, 32 + bits_for(g.n), s);
+      if (e != cudaSuccess) return e;
+    }
+    sym_keep_kernel<<<grid_for(g.nnz, 256, 8192), 256, 0, s>>>(g.indptr, g.n, g.nnz, w.k1, w.v1, w.head, w.v2,
+                                                               w.rcount);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    size_t tb = w.tmp_bytes;
+    e = cub::DeviceScan::ExclusiveSum(w.tmp, tb, w.head, w.pos, (int)g.nnz, s);
+    if (e != cudaSuccess) return e;
+  }
+  scan_i64_kernel<<<1, 1024, 0, s>>>(w.rcount, g.n, s_indptr);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (g.nnz > 0) {
+    sym_write_kernel<<<grid_for(g.nnz, 256, 8192), 256, 0, s>>>(w.k1, w.v2, w.head, w.pos, g.nnz, s_indices, s_data);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  return cudaMemcpyAsync(s_nnz, s_indptr + g.n, 8, cudaMemcpyDeviceToDevice, s);
+}
+
+cudaError_t launch_expand(const Csr& sym, const int32_t* part, const float* xnorm, const float* layout, int ncomp,
+                          float* result, int32_t* overflow, int32_t* n_overflow, int32_t* scratch_key,
+                          float* scratch_sum, int64_t max_deg, int sms, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(n_overflow, 0, 4, s);
+  if (e != cudaSuccess) return e;
+  expand_kernel<<<grid_for(sym.n, kRowWarps, sms * 8), kRowWarps * 32, 0, s>>>(sym, part, xnorm, layout, ncomp,
+                                                                               result, overflow, n_overflow);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (max_deg > kVoteSlots) {
+    expand_overflow_kernel<<<sms, kRowWarps * 32, 0, s>>>(sym, part, xnorm, layout, ncomp, result, overflow,
+                                                          n_overflow, scratch_key, scratch_sum, max_deg);
+    e = cudaGetLastError();
+  }
+  return e;
+}
+
+cudaError_t launch_center_scale(const float* result, int64_t n, int ncomp, float scaling, float* out,
+                                double* mean, cudaStream_t s) {
+  center_mean_kernel<<<1, 1024, 0, s>>>(result, n, ncomp, mean);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  center_apply_kernel<<<grid_for(n * ncomp, 256, 4096), 256, 0, s>>>(result, n, ncomp, scaling, mean, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pca_init(const float* x, int64_t n, int64_t d, int ncomp, float* out, float* mean_ws,
+                            double* vws, int32_t* status, cudaStream_t s) {
+  if (n <= 0 || n > kPcaMax) return cudaErrorInvalidValue;
+  const size_t smem = size_t(2) * kPcaMax * kPcaMax * sizeof(double);
+  cudaError_t e = cudaFuncSetAttribute(pca_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  pca_kernel<<<1, 256, smem, s>>>(x, n, d, ncomp, out, mean_ws, vws, status);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ne_schedule(const float* w, int64_t m, int32_t n_epochs, float negative_sample_rate, float* eps,
+                               float* epns, float* eonn, float* eons, float* max_w, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(max_w, 0, 4, s);
+  if (e != cudaSuccess || m == 0) return e;
+  ne_maxw_kernel<<<grid_for(m, 256, 4096), 256, 0, s>>>(w, m, max_w);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  ne_schedule_kernel<<<grid_for(m, 256, 4096), 256, 0, s>>>(w, m, (float)n_epochs, negative_sample_rate, max_w, eps,
+                                                           epns, eonn, eons);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ne_block(const Csr& g, float* emb, float* upd, const uint32_t* order, int64_t bs, int64_t be,
+                            const float* eps, const float* epns, float* eonn, float* eons, uint32_t rng_state,
+                            int ncomp, float alpha, uint8_t epoch, float noise, float gamma, float decay,
+                            int apply_decay, cudaStream_t s) {
+  const int grid = (int)((be - bs + 127) / 128);
+  if (grid <= 0) return cudaSuccess;
+  if (ncomp <= 16)
+    ne_block_kernel<16><<<grid, 128, 0, s>>>(g, emb, upd, order, bs, be, eps, epns, eonn, eons, rng_state, ncomp,
+                                             alpha, epoch, noise, gamma, decay, apply_decay);
+  else
+    ne_block_kernel<32><<<grid, 128, 0, s>>>(g, emb, upd, order, bs, be, eps, epns, eonn, eons, rng_state, ncomp,
+                                             alpha, epoch, noise, gamma, decay, apply_decay);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ne_apply(float* emb, const float* upd, const uint32_t* order, int64_t bs, int64_t be, int64_t nv,
+                            int ncomp, cudaStream_t s) {
+  ne_apply_kernel<<<grid_for((be - bs) * ncomp, 256, 4096), 256, 0, s>>>(emb, upd, order, bs, be, (uint64_t)nv,
+                                                                         ncomp);
+  return cudaGetLastError();
+}
+
+}  // namespace lp
+}  // namespace evoc

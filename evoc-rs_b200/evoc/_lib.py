@@ -100,6 +100,14 @@ def _bind_optional(L) -> None:
         L.evoc_gpu_tune_load.argtypes = [P, C.c_char_p]
     if hasattr(L, "evoc_gpu_knn_graph_batch"):
         L.evoc_gpu_knn_graph_batch.argtypes = [P, C.POINTER(Opts), i32, i32, P, P, P, i32, P, P, P, P]
+    if hasattr(L, "evoc_gpu_label_propagation_init"):
+        f32 = C.c_float
+        L.evoc_gpu_label_prop_loop.argtypes = [P, P, P, P, i64, i32, i64, C.POINTER(NumpyRng), i32, P,
+                                               C.POINTER(i64)]
+        L.evoc_gpu_label_propagation_init.argtypes = [P, P, P, P, i64, i32, i32, i64, i32, f32, f32, f32,
+                                                      C.POINTER(NumpyRng), P, i64, i32, P]
+        L.evoc_gpu_node_embedding.argtypes = [P, P, P, P, i64, i32, i32, P, f32, f32, f32, C.POINTER(NumpyRng),
+                                              i32, i32, P]
     if hasattr(L, "evoc_gpu_server_create"):
         L.evoc_gpu_server_default_opts.argtypes = [C.POINTER(ServerOpts)]
         L.evoc_gpu_server_create.argtypes = [C.POINTER(ServerOpts), C.POINTER(P)]
@@ -121,6 +129,12 @@ def _bind_optional(L) -> None:
         L.evoc_gpu_server_stage.argtypes = [P, C.c_int, C.c_char_p, i32, C.POINTER(C.c_double), C.POINTER(i64)]
         L.evoc_gpu_server_lane_busy_ms.argtypes = [P]
         L.evoc_gpu_server_lane_busy_ms.restype = C.c_double
+
+
+class NumpyRng(C.Structure):
+    """evoc_numpy_rng: the fields of numpy.random.RandomState.get_state()."""
+
+    _fields_ = [("key", C.c_uint32 * 624), ("pos", C.c_int32), ("has_gauss", C.c_int32), ("gauss", C.c_double)]
 
 
 class ServerOpts(C.Structure):

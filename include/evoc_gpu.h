@@ -184,6 +184,66 @@ int evoc_gpu_fuzzy_graph(evoc_gpu_ctx* ctx, const int32_t* idx, const float* dis
                          float n_neighbors, int32_t symmetrize, int32_t buffers_on_device, float* sigma, float* rho,
                          int64_t* indptr, int32_t* indices, float* data, int64_t cap, int64_t* nnz);
 
+/*
+ * NumPy RandomState (MT19937) state, the fields of get_state() and of the
+ * reference's NumpyRandomState (src/numpy_rng.rs:11-17, from_numpy_state
+ * 154-168).  Calls that draw from the caller's RNG advance it in place with
+ * the reference's draws, in the reference's order.
+ */
+typedef struct {
+  uint32_t key[624];
+  int32_t pos;
+  int32_t has_gauss;
+  double gauss;
+} evoc_numpy_rng;
+
+/*
+ * Partition of a graph by label propagation.  Replaces label_prop_loop
+ * (src/label_prop.rs:160-185) called on all -1 labels: 3 tau-seed draws,
+ * approx_n_parts seeds labels[randint(0, n)] = i, n_iter sweeps of
+ * label_prop_iteration (39-91), label_outliers (94-132), remap_labels
+ * (135-157).  Bit-identical to the reference.
+ *   indptr (n + 1, int64), indices (int32), data (f32): CSR, any column order
+ *   labels   n int64 out: part of each row, 0 .. *n_parts - 1
+ */
+int evoc_gpu_label_prop_loop(evoc_gpu_ctx* ctx, const int64_t* indptr, const int32_t* indices, const float* data,
+                             int64_t n, int32_t n_iter, int64_t approx_n_parts, evoc_numpy_rng* rng,
+                             int32_t buffers_on_device, int64_t* labels, int64_t* n_parts);
+
+/*
+ * Initial node embedding by label propagation.  Replaces label_propagation_init
+ * (src/label_prop.rs:464-494) and RlxBackend::label_propagation_init
+ * (src/rlx_backend/mod.rs:146-159): recursive init on the reduced graph, PCA
+ * base init below 64 vertices, the partition expander.
+ *   x        n x dim f32, the caller's rows (reduced level by level; required
+ *            when the recursion reaches a graph of fewer than 64 vertices,
+ *            else EVOC_ERR_ARG as LabelPropError::PcaRequiresData)
+ *   out      n x n_components f32 (n_components 1..32)
+ *   random_scale  unused by the partition expander (kept for the signature)
+ * Partitions, reduced graphs, node orders and the embedding epochs match the
+ * reference bit for bit; the PCA base init is f64 eigen-decomposition (the
+ * reference uses an f64 thin SVD), equal within its rounding.
+ */
+int evoc_gpu_label_propagation_init(evoc_gpu_ctx* ctx, const int64_t* indptr, const int32_t* indices,
+                                    const float* data, int64_t n, int32_t n_label_prop_iter,
+                                    int32_t n_embedding_epochs, int64_t approx_n_parts, int32_t n_components,
+                                    float scaling, float random_scale, float noise_level, evoc_numpy_rng* rng,
+                                    const float* x, int64_t dim, int32_t buffers_on_device, float* out);
+
+/*
+ * UMAP-like node embedding.  Replaces node_embedding (src/embed.rs:251-369)
+ * and RlxBackend::node_embedding (src/rlx_backend/mod.rs:161-173) with
+ * reproducible_flag = true: block-synchronous epochs
+ * (node_embedding_epoch_repr, 138-248), bit-identical to the reference.
+ *   initial_embedding  n x n_components, or NULL for normal(0.25) draws
+ *   reproducible       must be 1 (the other epoch is serial in-place SGD);
+ *                      0 returns EVOC_ERR_UNSUPPORTED
+ */
+int evoc_gpu_node_embedding(evoc_gpu_ctx* ctx, const int64_t* indptr, const int32_t* indices, const float* data,
+                            int64_t n, int32_t n_components, int32_t n_epochs, const float* initial_embedding,
+                            float initial_alpha, float negative_sample_rate, float noise_level, evoc_numpy_rng* rng,
+                            int32_t reproducible, int32_t buffers_on_device, float* out);
+
 /* The context's CUDA stream (a cudaStream_t), for callers that record their
  * own CUDA events around calls.  No counterpart in evoc-rs. */
 void* evoc_gpu_ctx_stream(const evoc_gpu_ctx* ctx);

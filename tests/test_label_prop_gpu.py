@@ -1,0 +1,176 @@
+"""GPU label propagation / node embedding against the oracle (and the golden vectors).
+
+Partitions and node embeddings are compared bit for bit with the oracle on the
+same graph and the same NumPy RNG state, and the RNG must end in the same
+state.  The full label_propagation_init ends in a PCA of fewer than 64 rows
+(f64; the oracle uses NumPy's SVD, the GPU a Jacobi eigen-decomposition), so
+it is compared within the reference's own init tolerance, 1e-4
+(tests/parity_intermediates.rs:127), and against the golden init_embedding.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import evoc
+from oracle import label_prop as L
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _lp(name):
+    return np.load(os.path.join(GOLDEN, f"lp_{name}.npz"))
+
+
+def _main(name):
+    return np.load(os.path.join(GOLDEN, f"{name}.npz"))
+
+
+def _graph(name):
+    z = _lp(name)
+    if "graph_csr_indptr" in z.files:
+        return L.Csr.make(z["graph_csr_indptr"], z["graph_csr_indices"], z["graph_csr_data"], z["graph_csr_shape"])
+    m = _main(name)
+    r, c, d = m["graph_coo_rows"], m["graph_coo_cols"], m["graph_coo_data"]
+    n = int(m["graph_coo_shape"][0])
+    o = np.lexsort((c, r))
+    indptr = np.zeros(n + 1, np.int64)
+    np.cumsum(np.bincount(r, minlength=n), out=indptr[1:])
+    return L.Csr.make(indptr, c[o], d[o], (n, n))
+
+
+def _tuple(g):
+    return (g.indptr, g.indices, g.data, g.shape[0])
+
+
+def _np_state(z, tag):
+    rs = np.random.RandomState(0)
+    rs.set_state(("MT19937", z[f"rng_{tag}_key"].astype(np.uint32), int(z[f"rng_{tag}_pos"]),
+                  int(z[f"rng_{tag}_has_gauss"]), float(z[f"rng_{tag}_gauss"])))
+    return rs
+
+
+def _oracle_rng(rs):
+    _, key, pos, hg, g = rs.get_state()
+    return L.mt_from_state(key, pos, hg, g)
+
+
+def _same_state(rs, orng):
+    _, key, pos, _, _ = rs.get_state()
+    return np.array_equal(key, orng.key) and int(pos) == orng.pos
+
+
+def _approx(n):
+    return int(np.clip(8 * np.sqrt(n), 256, 16384))
+
+
+@pytest.fixture(scope="module")
+def blob_graph():
+    """A 12,000-vertex fuzzy graph (GPU kNN + fuzzy union) and its data, built once."""
+    rng = np.random.default_rng(21)
+    c = rng.normal(size=(40, 48))
+    x = (c[rng.integers(0, 40, 12000)] + 0.35 * rng.normal(size=(12000, 48))).astype(np.float32)
+    ind, dst = evoc.knn_graph(x, evoc.KnnGraphOptions(n_neighbors=15, form="fp32"))
+    indptr, indices, data, _, _ = evoc.neighbor_graph_csr(15.0, ind, dst)
+    return L.Csr.make(indptr, indices, data, (len(x), len(x))), x
+
+
+@pytest.mark.parametrize("name", ["medium_800", "large_2000"])
+def test_label_prop_loop_matches_oracle_and_golden(name):
+    z = _lp(name)
+    g = _graph(name)
+    rs = _np_state(z, "after_knn")
+    orng = _oracle_rng(rs)
+    part = evoc.label_prop_loop(_tuple(g), rs, 20, _approx(g.shape[0]))
+    want = L.label_prop_loop(g, orng, 20, _approx(g.shape[0]))
+    assert np.array_equal(part, want) and np.array_equal(part, z["partition"])
+    assert _same_state(rs, orng)
+
+
+def test_label_prop_loop_larger_graph(blob_graph):
+    g, _ = blob_graph
+    for seed, approx in ((3, 876), (4, 40), (5, 5000)):
+        rs = np.random.RandomState(seed)
+        orng = _oracle_rng(rs)
+        part = evoc.label_prop_loop(_tuple(g), rs, 20, approx)
+        want = L.label_prop_loop(g, orng, 20, approx)
+        assert np.array_equal(part, want), (seed, approx, int((part != want).sum()))
+        assert _same_state(rs, orng)
+
+
+def test_label_prop_loop_few_iterations_leaves_outliers(blob_graph):
+    """With one sweep most rows are still unlabelled: the outlier walk (64-pop limit, random
+    fallback label, labels set earlier in the pass visible) decides them."""
+    g, _ = blob_graph
+    rs = np.random.RandomState(9)
+    orng = _oracle_rng(rs)
+    part = evoc.label_prop_loop(_tuple(g), rs, 1, 64)
+    want = L.label_prop_loop(g, orng, 1, 64)
+    assert np.array_equal(part, want)
+
+
+@pytest.mark.parametrize("name", ["small_200", "medium_800", "large_2000"])
+def test_node_embedding_bit_exact(name):
+    z = _lp(name)
+    g = _graph(name)
+    rs = _np_state(z, "after_init")
+    orng = _oracle_rng(rs)
+    emb = evoc.node_embedding(_tuple(g), 4, 50, z["init_embedding"], 0.1, 1.0, 0.5, rs)
+    want = L.node_embedding(g, 4, 50, z["init_embedding"], 0.1, 1.0, 0.5, orng)
+    assert np.array_equal(emb.view(np.uint32), want.view(np.uint32))
+    assert _same_state(rs, orng)
+    assert np.abs(emb - z["embedding"]).max() <= (3.6e-4 if name == "medium_800" else 2e-3)
+
+
+def test_node_embedding_random_init_and_wide(blob_graph):
+    """Initial embedding drawn from the RNG (normal(0.25)), 15 components, more than 8 blocks per
+    epoch on a 12,000-vertex graph."""
+    g, _ = blob_graph
+    rs = np.random.RandomState(77)
+    orng = _oracle_rng(rs)
+    emb = evoc.node_embedding(_tuple(g), 15, 12, None, 0.1, 1.0, 0.5, rs)
+    want = L.node_embedding(g, 15, 12, None, 0.1, 1.0, 0.5, orng)
+    assert np.array_equal(emb.view(np.uint32), want.view(np.uint32))
+    assert _same_state(rs, orng)
+
+
+@pytest.mark.parametrize("name", ["small_200", "medium_800", "large_2000"])
+def test_label_propagation_init_matches_oracle_and_golden(name):
+    z = _lp(name)
+    g = _graph(name)
+    data = _main(name)["data"]
+    rs = _np_state(z, "after_knn")
+    orng = _oracle_rng(rs)
+    init = evoc.label_propagation_init(_tuple(g), 20, 50, _approx(g.shape[0]), 4, 0.5, 0.1, 0.5, rs, data)
+    want = L.label_propagation_init(g, 20, 50, _approx(g.shape[0]), 4, 0.5, 0.1, 0.5, orng, data)
+    assert np.abs(init - want).max() <= 1e-4
+    assert np.abs(init - z["init_embedding"]).max() <= 1e-4
+    assert _same_state(rs, orng)
+
+
+def test_label_propagation_init_larger_graph(blob_graph):
+    g, x = blob_graph
+    rs = np.random.RandomState(5)
+    orng = _oracle_rng(rs)
+    init = evoc.label_propagation_init(_tuple(g), 20, 30, _approx(g.shape[0]), 7, 0.5, 0.1, 0.5, rs, x)
+    want = L.label_propagation_init(g, 20, 30, _approx(g.shape[0]), 7, 0.5, 0.1, 0.5, orng, x)
+    assert init.shape == (len(x), 7)
+    assert np.abs(init - want).max() <= 1e-4
+    assert _same_state(rs, orng)
+
+
+def test_errors_are_reported_not_faulted(blob_graph):
+    g, _ = blob_graph
+    with pytest.raises(evoc.BackendError):  # PCA base init needs the data (LabelPropError::PcaRequiresData)
+        evoc.label_propagation_init(_tuple(g), 20, 5, 300, 4, 0.5, 0.1, 0.5, np.random.RandomState(1), None)
+    with pytest.raises(evoc.BackendError):  # only the reproducible epoch is offered
+        evoc.node_embedding(_tuple(g), 4, 5, None, 0.1, 1.0, 0.5, np.random.RandomState(1),
+                            reproducible_flag=False)
+    bad = g.indices.copy()
+    bad[7] = g.shape[0]  # a column outside the graph is caught before any kernel reads through it
+    with pytest.raises(evoc.BackendError):
+        evoc.label_prop_loop((g.indptr, bad, g.data, g.shape[0]), np.random.RandomState(1), 3, 100)
+    with pytest.raises(evoc.EmptyData):
+        evoc.node_embedding((np.zeros(1, np.int64), np.zeros(0, np.int32), np.zeros(0, np.float32), 0), 4, 5)
