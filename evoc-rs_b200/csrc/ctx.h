@@ -79,6 +79,9 @@ struct evoc_gpu_ctx {
   int n_stages = 0;
   int launches = 0;
   int nnd_iterations = 0;
+  // Stream-ordered pool of the label-propagation / embedding calls; it keeps
+  // freed blocks (release threshold = max) so repeated calls do not remap.
+  cudaMemPool_t lp_pool = nullptr;
 };
 
 namespace evoc {

@@ -1094,6 +1094,7 @@ void evoc_gpu_ctx_destroy(evoc_gpu_ctx* ctx) {
   ctx->batch_ws.release();
   ctx->batch_tab.release();
   if (ctx->batch_host) cudaFreeHost(ctx->batch_host);
+  if (ctx->lp_pool) cudaMemPoolDestroy(ctx->lp_pool);
   for (auto& r : ctx->stages) {
     if (r.a) cudaEventDestroy(r.a);
     if (r.b) cudaEventDestroy(r.b);

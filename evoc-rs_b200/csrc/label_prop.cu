@@ -184,64 +184,71 @@ __global__ void seed_labels_kernel(int32_t* labels, const int64_t* idx, int64_t 
   for (int64_t i = 0; i < count; i++) labels[idx[i]] = (int32_t)i;
 }
 
-// label_outliers: one warp walks the unlabelled rows in row order.  The
-// stack holds at most 1 + 64 * max_deg entries (64 pops, each pushing at most
-// one row's columns); a walk that would pass `cap` sets status and stops.
-__global__ void lp_outliers_kernel(Csr g, int32_t* labels, const int64_t* rs_p, int32_t* stack, int64_t cap,
+// Unlabelled-row flags and the largest label, before the outlier walk.
+__global__ void outlier_flags_kernel(const int32_t* labels, int64_t n, int32_t* flag, int32_t* max_label) {
+  int32_t m = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t l = labels[i];
+    flag[i] = l < 0;
+    m = max(m, l);
+  }
+  m = __reduce_max_sync(kFull, m);
+  if ((threadIdx.x & 31) == 0) atomicMax(max_label, m);
+}
+
+// label_outliers: one warp walks the unlabelled rows (rows[0 .. *count), in
+// row order).  The stack holds at most 1 + 64 * max_deg entries (64 pops,
+// each pushing at most one row's columns); a walk that would pass `cap` sets
+// status and stops.
+__global__ void lp_outliers_kernel(Csr g, int32_t* labels, const int64_t* rs_p, const int32_t* rows,
+                                   const int32_t* count, const int32_t* max_label, int32_t* stack, int64_t cap,
                                    int32_t* status) {
   const int lane = threadIdx.x & 31;
-  int32_t ml = 0;
-  for (int64_t i = lane; i < g.n; i += 32) ml = max(ml, labels[i]);
-  ml = __reduce_max_sync(kFull, ml);
+  const int32_t ml = *max_label, n_rows = *count;
   const int64_t rs0 = rs_p[0], rs1 = rs_p[1], rs2 = rs_p[2];
-  for (int64_t base = 0; base < g.n; base += 32) {
-    const int64_t i = base + lane;
-    unsigned m = __ballot_sync(kFull, i < g.n && labels[i] < 0);
-    while (m) {
-      const int64_t row = base + __ffs(m) - 1;
-      m &= m - 1u;
-      if (lane == 0) stack[0] = (int32_t)row;
-      __syncwarp();
-      int64_t top = 1;
-      bool unl = true;
-      int it = 0;
-      while (unl && it < 64 && top > 0) {
-        it++;
-        top--;
-        const int64_t node = stack[top];
-        const int64_t s = g.indptr[node], e = g.indptr[node + 1];
-        for (int64_t b = s; b < e; b += 32) {
-          const int64_t k = b + lane;
-          const bool valid = k < e;
-          const int32_t j = valid ? g.indices[k] : 0;
-          const int32_t lj = valid ? labels[j] : -1;
-          const unsigned hit = __ballot_sync(kFull, valid && lj >= 0);
-          const int npush = hit ? __ffs(hit) - 1 : __popc(__ballot_sync(kFull, valid));
-          if (top + npush > cap) {
-            if (lane == 0) atomicExch(status, 1);
-            return;
-          }
-          if (lane < npush) stack[top + lane] = j;
-          top += npush;
-          if (hit) {
-            const int32_t lab = __shfl_sync(kFull, lj, __ffs(hit) - 1);
-            if (lane == 0) labels[row] = lab;
-            unl = false;
-            break;
-          }
+  for (int32_t oi = 0; oi < n_rows; oi++) {
+    const int64_t row = rows[oi];
+    if (lane == 0) stack[0] = (int32_t)row;
+    __syncwarp();
+    int64_t top = 1;
+    bool unl = true;
+    int it = 0;
+    while (unl && it < 64 && top > 0) {
+      it++;
+      top--;
+      const int64_t node = stack[top];
+      const int64_t s = g.indptr[node], e = g.indptr[node + 1];
+      for (int64_t b = s; b < e; b += 32) {
+        const int64_t k = b + lane;
+        const bool valid = k < e;
+        const int32_t j = valid ? g.indices[k] : 0;
+        const int32_t lj = valid ? labels[j] : -1;
+        const unsigned hit = __ballot_sync(kFull, valid && lj >= 0);
+        const int npush = hit ? __ffs(hit) - 1 : __popc(__ballot_sync(kFull, valid));
+        if (top + npush > cap) {
+          if (lane == 0) atomicExch(status, 1);
+          return;
         }
-        __syncwarp();
-      }
-      if (lane == 0 && (it >= 64 || unl)) {
-        int64_t st[3] = {(int64_t)((uint64_t)rs0 + (uint64_t)row), (int64_t)((uint64_t)rs1 + (uint64_t)row),
-                         (int64_t)((uint64_t)rs2 + (uint64_t)row)};
-        const int64_t draw = tau_rand_int(st);
-        const int64_t mod = (int64_t)ml + 1;
-        const int64_t v = draw % mod;
-        labels[row] = (int32_t)(v < 0 ? v + mod : v);
+        if (lane < npush) stack[top + lane] = j;
+        top += npush;
+        if (hit) {
+          const int32_t lab = __shfl_sync(kFull, lj, __ffs(hit) - 1);
+          if (lane == 0) labels[row] = lab;
+          unl = false;
+          break;
+        }
       }
       __syncwarp();
     }
+    if (lane == 0 && (it >= 64 || unl)) {
+      int64_t st[3] = {(int64_t)((uint64_t)rs0 + (uint64_t)row), (int64_t)((uint64_t)rs1 + (uint64_t)row),
+                       (int64_t)((uint64_t)rs2 + (uint64_t)row)};
+      const int64_t draw = tau_rand_int(st);
+      const int64_t mod = (int64_t)ml + 1;
+      const int64_t v = draw % mod;
+      labels[row] = (int32_t)(v < 0 ? v + mod : v);
+    }
+    __syncwarp();
   }
 }
 
@@ -295,36 +302,33 @@ __global__ void part_norm_kernel(const int32_t* count, int32_t n_parts, float* x
   }
 }
 
-constexpr int kRedCols = 8;  // columns per lane per pass
-
+// One warp per (part, 32 columns): each lane sums its column over the part's
+// members in order; the member rows are loaded 8 ahead of the adds.
 __global__ void __launch_bounds__(256)
     reduce_data_kernel(const float* x, int64_t d, const int32_t* members, const int64_t* start, const int32_t* count,
                        const float* wred, int32_t n_parts, float* out) {
   const int lane = threadIdx.x & 31;
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t p = gw; p < n_parts; p += nw) {
+  const int64_t chunks = (d + 31) / 32;
+  const int64_t tasks = (int64_t)n_parts * chunks;
+  for (int64_t task = gw; task < tasks; task += nw) {
+    const int64_t p = task / chunks, col = (task % chunks) * 32 + lane;
+    if (col >= d) continue;
     const double w = (double)wred[p];
-    const int64_t s0 = start[p];
+    const int32_t* mem = members + start[p];
     const int32_t c = count[p];
-    for (int64_t col0 = 0; col0 < d; col0 += 32 * kRedCols) {
-      float acc[kRedCols];
+    float acc = 0.0f;
+    int32_t t = 0;
+    for (; t + 8 <= c; t += 8) {
+      float v[8];
 #pragma unroll
-      for (int q = 0; q < kRedCols; q++) acc[q] = 0.0f;
-      for (int32_t t = 0; t < c; t++) {
-        const float* row = x + (int64_t)members[s0 + t] * d;
+      for (int u = 0; u < 8; u++) v[u] = x[(int64_t)mem[t + u] * d + col];
 #pragma unroll
-        for (int q = 0; q < kRedCols; q++) {
-          const int64_t col = col0 + q * 32 + lane;
-          if (col < d) acc[q] = __fadd_rn(acc[q], __double2float_rn(__dmul_rn(w, (double)row[col])));
-        }
-      }
-#pragma unroll
-      for (int q = 0; q < kRedCols; q++) {
-        const int64_t col = col0 + q * 32 + lane;
-        if (col < d) out[p * d + col] = acc[q];
-      }
+      for (int u = 0; u < 8; u++) acc = __fadd_rn(acc, __double2float_rn(__dmul_rn(w, (double)v[u])));
     }
+    for (; t < c; t++) acc = __fadd_rn(acc, __double2float_rn(__dmul_rn(w, (double)x[(int64_t)mem[t] * d + col])));
+    out[p * d + col] = acc;
   }
 }
 
@@ -758,76 +762,159 @@ __device__ __forceinline__ uint64_t neg_count(float nf, float eon, float rate) {
 
 __device__ __forceinline__ float clip4(float v) { return v > 4.0f ? 4.0f : (v < -4.0f ? -4.0f : v); }
 
+constexpr int kNeWarps = 4;    // warps (nodes in flight) per CTA
+constexpr int kNegSlots = 3;   // negative samples per edge staged at once
+
+// Per-warp staging: [32 lanes][1 + kNegSlots][ncomp] contributions, then 32
+// applied-slot masks and 32 negative-sample counts.
+__host__ __device__ inline int ne_stage_floats(int ncomp) { return 32 * (1 + kNegSlots) * ncomp + 64; }
+
+// One warp per node of the block.  The lanes take 32 consecutive edges and
+// compute their contributions (positive move, then each negative sample)
+// from the embedding as it stood at the block's start; then every lane adds
+// them, in edge order and within an edge in sample order, to its own copy of
+// the node's update row -- the reference's serial order of f32 additions.
+// Edges wanting more than kNegSlots negative samples in a chunk are handed
+// through the staging one contribution at a time instead.
 template <int MAXD>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(kNeWarps * 32)
     ne_block_kernel(Csr g, float* emb, float* upd, const uint32_t* order, int64_t bs, int64_t be, const float* eps,
                     const float* epns, float* eonn, float* eons, uint32_t rng_state, int ncomp, float alpha,
                     uint32_t epoch, float noise, float gamma, float decay, int apply_decay) {
-  const int64_t ni = bs + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (ni >= be) return;
+  extern __shared__ float ne_sh[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int kSlots = 1 + kNegSlots;
+  float* vec = ne_sh + (size_t)warp * ne_stage_floats(ncomp);
+  uint32_t* fmask = reinterpret_cast<uint32_t*>(vec + 32 * kSlots * ncomp);
+  int32_t* ncount = reinterpret_cast<int32_t*>(fmask + 32);
   const uint64_t nv = (uint64_t)g.n;
-  const uint64_t from = order[ni];
-  if (from >= nv) return;
-  float cur[MAXD], u[MAXD];
-#pragma unroll
-  for (int d = 0; d < MAXD; d++) {
-    if (d < ncomp) {
-      cur[d] = emb[from * ncomp + d];
-      u[d] = apply_decay ? __fmul_rn(upd[from * ncomp + d], decay) : upd[from * ncomp + d];
-    }
-  }
   const float nf = (float)epoch;
-  const uint64_t e0 = (uint64_t)g.indptr[from], e1 = (uint64_t)g.indptr[from + 1];
-  for (uint64_t raw = e0; raw < e1; raw++) {
-    if (eons[raw] > nf) continue;
-    const uint64_t to = (uint64_t)(uint32_t)g.indices[raw];
-    if (to >= nv) continue;
-    const float* yt = emb + to * ncomp;
-    float ds = 0.0f;
+  for (int64_t ni = bs + (int64_t)blockIdx.x * kNeWarps + warp; ni < be; ni += (int64_t)gridDim.x * kNeWarps) {
+    const uint64_t from = order[ni];
+    if (from >= nv) continue;
+    float cur[MAXD], u[MAXD];
 #pragma unroll
     for (int d = 0; d < MAXD; d++)
       if (d < ncomp) {
-        const float df = __fsub_rn(cur[d], yt[d]);
-        ds = __fadd_rn(ds, __fmul_rn(df, df));
+        cur[d] = emb[from * ncomp + d];
+        u[d] = apply_decay ? __fmul_rn(upd[from * ncomp + d], decay) : upd[from * ncomp + d];
       }
-    if (ds > 0.0f) {
-      const float dist = __fsqrt_rn(ds);
-      const float num = __fsub_rn(__fmul_rn(__fmul_rn(-2.0f, noise), dist), 2.0f);
-      const float den = __fadd_rn(__fsub_rn(__fmul_rn(2.0f, ds), __fmul_rn(0.5f, dist)), 1.0f);
-      const float gc = __fdiv_rn(num, den);
+    const uint64_t e0 = (uint64_t)g.indptr[from], e1 = (uint64_t)g.indptr[from + 1];
+    for (uint64_t base = e0; base < e1; base += 32) {
+      const uint64_t raw = base + lane;
+      bool act = false;
+      uint64_t to = 0;
+      if (raw < e1 && !(eons[raw] > nf)) {
+        to = (uint64_t)(uint32_t)g.indices[raw];
+        act = to < nv;
+      }
+      uint32_t fl = 0;
+      uint64_t nneg = 0;
+      float rate = 0.0f;
+      float cp[MAXD];
+      if (act) {
+        const float* yt = emb + to * ncomp;
+        float ds = 0.0f;
 #pragma unroll
-      for (int d = 0; d < MAXD; d++)
-        if (d < ncomp) u[d] = __fadd_rn(u[d], __fmul_rn(__fmul_rn(gc, __fsub_rn(cur[d], yt[d])), alpha));
-    }
-    eons[raw] = __fadd_rn(eons[raw], eps[raw]);
-    const float rate = epns[raw];
-    const uint64_t nneg = neg_count(nf, eonn[raw], rate);
-    for (uint64_t p = 0; p < nneg; p++) {
-      const uint64_t idx = (raw * ((uint64_t)epoch + p + 1ull) * (uint64_t)rng_state) % nv;
-      const uint64_t tn = order[idx];
-      if (tn >= nv) continue;
-      const float* yn = emb + tn * ncomp;
-      float dn = 0.0f;
-#pragma unroll
-      for (int d = 0; d < MAXD; d++)
-        if (d < ncomp) {
-          const float df = __fsub_rn(cur[d], yn[d]);
-          dn = __fadd_rn(dn, __fmul_rn(df, df));
-        }
-      if (dn > 1e-2f) {
-        const float gc = __fdiv_rn(__fmul_rn(gamma, 4.0f), __fmul_rn(__fadd_rn(1.0f, __fmul_rn(0.25f, dn)), dn));
-        if (gc > 0.0f) {
+        for (int d = 0; d < MAXD; d++)
+          if (d < ncomp) {
+            const float df = __fsub_rn(cur[d], yt[d]);
+            ds = __fadd_rn(ds, __fmul_rn(df, df));
+          }
+        if (ds > 0.0f) {
+          const float dist = __fsqrt_rn(ds);
+          const float num = __fsub_rn(__fmul_rn(__fmul_rn(-2.0f, noise), dist), 2.0f);
+          const float den = __fadd_rn(__fsub_rn(__fmul_rn(2.0f, ds), __fmul_rn(0.5f, dist)), 1.0f);
+          const float gc = __fdiv_rn(num, den);
 #pragma unroll
           for (int d = 0; d < MAXD; d++)
-            if (d < ncomp) u[d] = __fadd_rn(u[d], __fmul_rn(clip4(__fmul_rn(gc, __fsub_rn(cur[d], yn[d]))), alpha));
+            if (d < ncomp) cp[d] = __fmul_rn(__fmul_rn(gc, __fsub_rn(cur[d], yt[d])), alpha);
+          fl = 1u;
+        }
+        eons[raw] = __fadd_rn(eons[raw], eps[raw]);
+        rate = epns[raw];
+        nneg = neg_count(nf, eonn[raw], rate);
+      }
+      // contribution s of this lane's edge into staging slot `slot`; returns whether it applies
+      auto neg_contrib = [&](uint64_t p, int slot) -> bool {
+        const uint64_t idx = (raw * ((uint64_t)epoch + p + 1ull) * (uint64_t)rng_state) % nv;
+        const uint64_t tn = order[idx];
+        if (tn >= nv) return false;
+        const float* yn = emb + tn * ncomp;
+        float dn = 0.0f;
+#pragma unroll
+        for (int d = 0; d < MAXD; d++)
+          if (d < ncomp) {
+            const float df = __fsub_rn(cur[d], yn[d]);
+            dn = __fadd_rn(dn, __fmul_rn(df, df));
+          }
+        if (!(dn > 1e-2f)) return false;
+        const float gc = __fdiv_rn(__fmul_rn(gamma, 4.0f), __fmul_rn(__fadd_rn(1.0f, __fmul_rn(0.25f, dn)), dn));
+        if (!(gc > 0.0f)) return false;
+        float* dst = vec + ((size_t)lane * kSlots + slot) * ncomp;
+#pragma unroll
+        for (int d = 0; d < MAXD; d++)
+          if (d < ncomp) dst[d] = __fmul_rn(clip4(__fmul_rn(gc, __fsub_rn(cur[d], yn[d]))), alpha);
+        return true;
+      };
+      auto add_slot = [&](int L, int slot) {
+        const float* src = vec + ((size_t)L * kSlots + slot) * ncomp;
+#pragma unroll
+        for (int d = 0; d < MAXD; d++)
+          if (d < ncomp) u[d] = __fadd_rn(u[d], src[d]);
+      };
+      const int maxneg = (int)__reduce_max_sync(kFull, (unsigned)(nneg < (1ull << 30) ? nneg : (1ull << 30)));
+      if (maxneg <= kNegSlots) {
+        if (fl) {
+          float* dst = vec + (size_t)lane * kSlots * ncomp;
+#pragma unroll
+          for (int d = 0; d < MAXD; d++)
+            if (d < ncomp) dst[d] = cp[d];
+        }
+        for (int p = 0; p < maxneg; p++)
+          if ((uint64_t)p < nneg && neg_contrib((uint64_t)p, 1 + p)) fl |= 2u << p;
+        fmask[lane] = fl;
+        ncount[lane] = (int32_t)nneg;
+        __syncwarp();
+        for (int L = 0; L < 32; L++) {
+          const uint32_t f = fmask[L];
+          if (!f) continue;
+          const int cnt = 1 + ncount[L];
+          for (int sl = 0; sl < cnt; sl++)
+            if ((f >> sl) & 1u) add_slot(L, sl);
+        }
+        __syncwarp();
+      } else {
+        for (int L = 0; L < 32; L++) {
+          const uint64_t nL = __shfl_sync(kFull, nneg, L);
+          const uint32_t fL = __shfl_sync(kFull, fl, L);
+          if (fL) {
+            if (lane == L) {
+              float* dst = vec + (size_t)lane * kSlots * ncomp;
+#pragma unroll
+              for (int d = 0; d < MAXD; d++)
+                if (d < ncomp) dst[d] = cp[d];
+            }
+            __syncwarp();
+            add_slot(L, 0);
+            __syncwarp();
+          }
+          for (uint64_t p = 0; p < nL; p++) {
+            if (lane == L) fmask[L] = neg_contrib(p, 1) ? 1u : 0u;
+            __syncwarp();
+            if (fmask[L]) add_slot(L, 1);
+            __syncwarp();
+          }
         }
       }
+      if (act) eonn[raw] = __fadd_rn(eonn[raw], __fmul_rn(__ull2float_rn(nneg), rate));
     }
-    eonn[raw] = __fadd_rn(eonn[raw], __fmul_rn(__ull2float_rn(nneg), rate));
-  }
+    if (lane == 0) {
 #pragma unroll
-  for (int d = 0; d < MAXD; d++)
-    if (d < ncomp) upd[from * ncomp + d] = u[d];
+      for (int d = 0; d < MAXD; d++)
+        if (d < ncomp) upd[from * ncomp + d] = u[d];
+    }
+  }
 }
 
 __global__ void ne_apply_kernel(float* emb, const float* upd, const uint32_t* order, int64_t bs, int64_t be,
@@ -892,9 +979,24 @@ cudaError_t launch_lp_iteration(const Csr& g, const int32_t* lab_in, int32_t* la
   return e;
 }
 
+size_t lp_outliers_tmp_bytes(int64_t n) {
+  size_t b = 0;
+  cub::DeviceSelect::Flagged(nullptr, b, thrust::counting_iterator<int32_t>(0), (const int32_t*)nullptr,
+                             (int32_t*)nullptr, (int32_t*)nullptr, (int)n);
+  return b;
+}
+
 cudaError_t launch_lp_outliers(const Csr& g, int32_t* labels, const int64_t* rs, int32_t* stack, int64_t stack_cap,
-                               int32_t* status, cudaStream_t s) {
-  lp_outliers_kernel<<<1, 32, 0, s>>>(g, labels, rs, stack, stack_cap, status);
+                               int32_t* flag, int32_t* rows, int32_t* count, int32_t* max_label, void* tmp,
+                               size_t tmp_bytes, int32_t* status, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(max_label, 0, 4, s);
+  if (e != cudaSuccess) return e;
+  outlier_flags_kernel<<<grid_for(g.n, 256, 2048), 256, 0, s>>>(labels, g.n, flag, max_label);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  e = cub::DeviceSelect::Flagged(tmp, tmp_bytes, thrust::counting_iterator<int32_t>(0), flag, rows, count, (int)g.n,
+                                 s);
+  if (e != cudaSuccess) return e;
+  lp_outliers_kernel<<<1, 32, 0, s>>>(g, labels, rs, rows, count, max_label, stack, stack_cap, status);
   return cudaGetLastError();
 }
 
@@ -942,8 +1044,9 @@ cudaError_t launch_part_members(const int32_t* part, int64_t n, int32_t n_parts,
 cudaError_t launch_reduce_data(const float* x, int64_t d, const int32_t* members, const int64_t* start,
                                const int32_t* count, const float* wred, int32_t n_parts, float* out, int sms,
                                cudaStream_t s) {
-  reduce_data_kernel<<<grid_for(int64_t(n_parts) * 32, 256, sms * 16), 256, 0, s>>>(x, d, members, start, count,
-                                                                                       wred, n_parts, out);
+  const int64_t tasks = int64_t(n_parts) * ((d + 31) / 32);
+  reduce_data_kernel<<<grid_for(tasks * 32, 256, sms * 64), 256, 0, s>>>(x, d, members, start, count, wred, n_parts,
+                                                                        out);
   return cudaGetLastError();
 }
 
@@ -1109,14 +1212,24 @@ cudaError_t launch_ne_block(const Csr& g, float* emb, float* upd, const uint32_t
                             const float* eps, const float* epns, float* eonn, float* eons, uint32_t rng_state,
                             int ncomp, float alpha, uint8_t epoch, float noise, float gamma, float decay,
                             int apply_decay, cudaStream_t s) {
-  const int grid = (int)((be - bs + 127) / 128);
-  if (grid <= 0) return cudaSuccess;
-  if (ncomp <= 16)
-    ne_block_kernel<16><<<grid, 128, 0, s>>>(g, emb, upd, order, bs, be, eps, epns, eonn, eons, rng_state, ncomp,
-                                             alpha, epoch, noise, gamma, decay, apply_decay);
-  else
-    ne_block_kernel<32><<<grid, 128, 0, s>>>(g, emb, upd, order, bs, be, eps, epns, eonn, eons, rng_state, ncomp,
-                                             alpha, epoch, noise, gamma, decay, apply_decay);
+  const int64_t warps = be - bs;
+  if (warps <= 0) return cudaSuccess;
+  const int grid = (int)std::min<int64_t>((warps + kNeWarps - 1) / kNeWarps, 1 << 20);
+  const size_t smem = size_t(kNeWarps) * ne_stage_floats(ncomp) * sizeof(float);
+  cudaError_t e;
+  if (ncomp <= 16) {
+    if ((e = cudaFuncSetAttribute(ne_block_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
+      return e;
+    ne_block_kernel<16><<<grid, kNeWarps * 32, smem, s>>>(g, emb, upd, order, bs, be, eps, epns, eonn, eons,
+                                                         rng_state, ncomp, alpha, epoch, noise, gamma, decay,
+                                                         apply_decay);
+  } else {
+    if ((e = cudaFuncSetAttribute(ne_block_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
+      return e;
+    ne_block_kernel<32><<<grid, kNeWarps * 32, smem, s>>>(g, emb, upd, order, bs, be, eps, epns, eonn, eons,
+                                                         rng_state, ncomp, alpha, epoch, noise, gamma, decay,
+                                                         apply_decay);
+  }
   return cudaGetLastError();
 }
 

@@ -37,9 +37,13 @@ cudaError_t launch_lp_iteration(const Csr& g, const int32_t* lab_in, int32_t* la
                                 int32_t* n_overflow, int32_t* scratch_key, double* scratch_sum, int64_t max_deg,
                                 int sms, cudaStream_t s);
 
-// label_outliers in row order (one warp); labels are int32; rs = tau seed (3 x int64).
+// label_outliers in row order (one warp over the compacted unlabelled rows);
+// labels are int32; rs = tau seed (3 x int64); flag/rows hold n ints, count
+// and max_label one each, tmp lp_outliers_tmp_bytes(n).
 cudaError_t launch_lp_outliers(const Csr& g, int32_t* labels, const int64_t* rs, int32_t* stack, int64_t stack_cap,
-                               int32_t* status, cudaStream_t s);
+                               int32_t* flag, int32_t* rows, int32_t* count, int32_t* max_label, void* tmp,
+                               size_t tmp_bytes, int32_t* status, cudaStream_t s);
+size_t lp_outliers_tmp_bytes(int64_t n);
 
 // remap_labels: dense ranks of the labels present (all labels are >= 0 here).
 // flags/map hold `bound` ints; *n_parts receives the number of labels.

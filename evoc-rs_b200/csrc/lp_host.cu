@@ -100,15 +100,16 @@ struct Mt {
 
 struct Arena {
   cudaStream_t s;
+  cudaMemPool_t pool;
   std::vector<void*> ptrs;
-  explicit Arena(cudaStream_t st) : s(st) {}
+  explicit Arena(evoc_gpu_ctx* ctx) : s(ctx->stream), pool(ctx->lp_pool) {}
   ~Arena() {
     for (void* p : ptrs) cudaFreeAsync(p, s);
   }
   template <class T>
   cudaError_t get(T** out, size_t count) {
     void* p = nullptr;
-    cudaError_t e = cudaMallocAsync(&p, std::max<size_t>(count, 1) * sizeof(T), s);
+    cudaError_t e = cudaMallocFromPoolAsync(&p, std::max<size_t>(count, 1) * sizeof(T), pool, s);
     if (e != cudaSuccess) return e;
     ptrs.push_back(p);
     *out = static_cast<T*>(p);
@@ -200,9 +201,18 @@ int lp_loop_dev(evoc_gpu_ctx* ctx, Arena& A, const lp::Csr& g, Mt& rng, int32_t 
   {
     Stage st(ctx, "label_outliers");
     const int64_t cap = 64 * max_deg + 1;
+    int32_t *oflag, *orows, *ocount, *omax;
     EVOC_TRY(A.get(&stack, size_t(cap)), "alloc outlier stack");
-    EVOC_TRY(lp::launch_lp_outliers(g, labels, d_rs, stack, cap, status, s), "label_outliers");
-    ctx->launches += 1;
+    EVOC_TRY(A.get(&oflag, size_t(g.n)), "alloc");
+    EVOC_TRY(A.get(&orows, size_t(g.n)), "alloc");
+    EVOC_TRY(A.get(&ocount, 1), "alloc");
+    EVOC_TRY(A.get(&omax, 1), "alloc");
+    const size_t otb = lp::lp_outliers_tmp_bytes(g.n);
+    uint8_t* otmp;
+    EVOC_TRY(A.get(&otmp, otb), "alloc");
+    EVOC_TRY(lp::launch_lp_outliers(g, labels, d_rs, stack, cap, oflag, orows, ocount, omax, otmp, otb, status, s),
+             "label_outliers");
+    ctx->launches += 3;
   }
   const int32_t bound = int32_t(std::max<int64_t>(approx, 1));
   EVOC_TRY(A.get(&flags, size_t(bound)), "alloc");
@@ -309,7 +319,7 @@ int node_embedding_dev(evoc_gpu_ctx* ctx, Arena& A, const lp::Csr& g, const floa
 int lp_init_level(evoc_gpu_ctx* ctx, const lp::ReduceScratch& W, const lp::Csr& g, const float* x, int64_t d,
                   const Level& L, Mt& rng, float* out) {
   cudaStream_t s = ctx->stream;
-  Arena A(s);
+  Arena A(ctx);
   if (g.n < kBaseInitThreshold) {
     if (!x) return fail(ctx, EVOC_ERR_ARG, "base_init 'pca' requires data");
     float* mean_ws;
@@ -464,6 +474,15 @@ int begin_call(evoc_gpu_ctx* ctx) {
   ctx->n_stages = 0;
   ctx->launches = 0;
   EVOC_TRY(cudaSetDevice(ctx->device), "cudaSetDevice");
+  if (!ctx->lp_pool) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = ctx->device;
+    EVOC_TRY(cudaMemPoolCreate(&ctx->lp_pool, &props), "memory pool");
+    uint64_t keep = UINT64_MAX;
+    EVOC_TRY(cudaMemPoolSetAttribute(ctx->lp_pool, cudaMemPoolAttrReleaseThreshold, &keep), "memory pool");
+  }
   return EVOC_OK;
 }
 
@@ -482,7 +501,7 @@ int label_propagation_init_impl(evoc_gpu_ctx* ctx, const int64_t* indptr, const 
   Stage total(ctx, "total");
   int rc;
   {
-    Arena A(s);
+    Arena A(ctx);
     lp::Csr g;
     if ((rc = stage_graph(ctx, A, indptr, indices, data, n, on_dev, &g))) return rc;
     if (g.nnz >= (int64_t(1) << 31) - 1) return fail(ctx, EVOC_ERR_UNSUPPORTED, "graphs of 2^31 or more entries");
@@ -535,7 +554,7 @@ int node_embedding_impl(evoc_gpu_ctx* ctx, const int64_t* indptr, const int32_t*
   Mt rng{rs};
   Stage total(ctx, "total");
   {
-    Arena A(s);
+    Arena A(ctx);
     lp::Csr g;
     if (int rc = stage_graph(ctx, A, indptr, indices, data, n, on_dev, &g)) return rc;
     if (g.nnz > (int64_t(1) << 32) - 1) return fail(ctx, EVOC_ERR_UNSUPPORTED, "2^32 or more edges");
@@ -567,7 +586,7 @@ int label_prop_loop_impl(evoc_gpu_ctx* ctx, const int64_t* indptr, const int32_t
   Mt rng{rs};
   Stage total(ctx, "total");
   {
-    Arena A(s);
+    Arena A(ctx);
     lp::Csr g;
     if (int rc = stage_graph(ctx, A, indptr, indices, data, n, on_dev, &g)) return rc;
     int32_t* part;

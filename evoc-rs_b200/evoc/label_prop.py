@@ -117,3 +117,35 @@ def node_embedding(graph, n_components: int, n_epochs: int, initial_embedding=No
     _check(st, ctx)
     _rng_out(rs, r)
     return out
+
+
+def label_propagation_init_device(indptr_ptr: int, indices_ptr: int, data_ptr: int, n: int, x_ptr: int, dim: int,
+                                  out_ptr: int, random_state, n_label_prop_iter: int = 20,
+                                  n_embedding_epochs: int = 50, approx_n_parts: int = 512, n_components: int = 4,
+                                  scaling: float = 0.5, random_scale: float = 0.1, noise_level: float = 0.5,
+                                  device: int = 0):
+    """label_propagation_init on device buffers (CSR int64/int32/f32, rows n x dim f32, out n x n_components)."""
+    rs = _state(random_state)
+    r = _rng_in(rs)
+    ctx = _lib.context(device)
+    st = _lib.lib().evoc_gpu_label_propagation_init(
+        ctx.h, P(indptr_ptr), P(indices_ptr), P(data_ptr), int(n), int(n_label_prop_iter), int(n_embedding_epochs),
+        int(approx_n_parts), int(n_components), float(scaling), float(random_scale), float(noise_level),
+        C.byref(r), P(x_ptr) if x_ptr else None, int(dim), 1, P(out_ptr))
+    _check(st, ctx)
+    _rng_out(rs, r)
+
+
+def node_embedding_device(indptr_ptr: int, indices_ptr: int, data_ptr: int, n: int, n_components: int,
+                          n_epochs: int, init_ptr: int, out_ptr: int, random_state, initial_alpha: float = 0.1,
+                          negative_sample_rate: float = 1.0, noise_level: float = 0.5, device: int = 0):
+    """node_embedding (reproducible) on device buffers; init_ptr 0 draws the initial embedding."""
+    rs = _state(random_state)
+    r = _rng_in(rs)
+    ctx = _lib.context(device)
+    st = _lib.lib().evoc_gpu_node_embedding(
+        ctx.h, P(indptr_ptr), P(indices_ptr), P(data_ptr), int(n), int(n_components), int(n_epochs),
+        P(init_ptr) if init_ptr else None, float(initial_alpha), float(negative_sample_rate), float(noise_level),
+        C.byref(r), 1, 1, P(out_ptr))
+    _check(st, ctx)
+    _rng_out(rs, r)

@@ -250,6 +250,12 @@ int64_t orc_smmp(int64_t n_row, int64_t n_col, const int64_t *ap, const int32_t 
     return nnz;
 }
 
+/* Per-segment f32 sums, each segment's values added one at a time in order. */
+void orc_seg_sum_f32(const float *v, const int64_t *seg, int64_t m, int64_t nseg, float *out) {
+    memset(out, 0, sizeof(float) * (size_t)nseg);
+    for (int64_t i = 0; i < m; i++) out[seg[i]] += v[i];
+}
+
 /* out[r, c] += (w as f64 * dense[col, c] as f64) as f32, entries in CSR order. */
 void orc_csr_dense(int64_t n_row, const int64_t *ap, const int32_t *ai, const float *ad, const float *dense,
                    int64_t k, float *out) {

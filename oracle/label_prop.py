@@ -34,6 +34,7 @@ def _lib():
         L.orc_smmp.restype = i64
         L.orc_csr_dense.argtypes = [i64, P, P, P, P, i64, P]
         L.orc_make_epochs_per_sample.argtypes = [P, i64, i32, P]
+        L.orc_seg_sum_f32.argtypes = [P, P, i64, i64, P]
         L.orc_node_embedding_repr.argtypes = [i64, P, P, P, i32, i32, P, i32, f32, f32, f32, C.POINTER(O.MT), i32, P,
                                               P, P]
         _ready = True
@@ -147,9 +148,10 @@ def transpose_sorted(a: Csr) -> Csr:
 
 def _seq_sum_f32(values: np.ndarray, seg: np.ndarray, nseg: int) -> np.ndarray:
     """Per-segment f32 sum, added one value at a time in storage order."""
-    out = np.zeros(nseg, np.float32)
-    for v, s in zip(values.astype(np.float32), seg):
-        out[s] = np.float32(out[s] + v)
+    v = np.ascontiguousarray(values, np.float32)
+    sg = np.ascontiguousarray(seg, np.int64)
+    out = np.empty(nseg, np.float32)
+    _lib().orc_seg_sum_f32(_p(v), _p(sg), len(v), nseg, _p(out))
     return out
 
 
