@@ -631,6 +631,97 @@ def run_exact_int(args, world, rank, local):
     return 0
 
 
+def run_label_prop(args, dev, ctx, stream, x, f_indptr, f_ind, f_dat, nnz, opts):
+    """label_propagation_init (src/label_prop.rs:464-494) on the workload's fuzzy graph, resident in
+    HBM, then the full-graph node embedding (src/embed.rs:251-369, reproducible) from it; the
+    oracle's restatement timed on the fuzzy graph of the first cpu_lp_rows rows beside the GPU
+    on the same graph."""
+    import numpy as np
+    import torch
+
+    import evoc
+    from evoc import label_prop as LP
+
+    n, d, k = args.n, args.dim, args.k
+    ncomp = min(max(k // 4, 4), 15)
+    approx = int(np.clip(8 * np.sqrt(n), 256, 16384))
+    out = torch.empty((n, ncomp), dtype=torch.float32, device=dev)
+    emb = torch.empty((n, ncomp), dtype=torch.float32, device=dev)
+
+    def lp_once():
+        LP.label_propagation_init_device(f_indptr.data_ptr(), f_ind.data_ptr(), f_dat.data_ptr(), n, x.data_ptr(), d,
+                                         out.data_ptr(), np.random.RandomState(42), 20, 50, approx, ncomp)
+        st = {}
+        for nm, ms in ctx.stages():
+            st[nm] = st.get(nm, 0.0) + ms
+        return st, ctx.launches()
+
+    lp_once()
+    runs = [lp_once() for _ in range(3)]
+    lp_ms = statistics.median(r[0]["total"] for r in runs)
+    stages = {nm: statistics.median(r[0][nm] for r in runs) for nm in runs[0][0] if nm != "total"}
+
+    def ne_once():
+        LP.node_embedding_device(f_indptr.data_ptr(), f_ind.data_ptr(), f_dat.data_ptr(), n, ncomp, 50,
+                                 out.data_ptr(), emb.data_ptr(), np.random.RandomState(43))
+        return dict(ctx.stages())
+
+    ne_once()
+    ne_ms = statistics.median(ne_once()["total"] for _ in range(2))
+    # effective bandwidth of the full-graph epochs: per edge the five f32 schedule words (three read,
+    # two written) and the column index, plus one embedding row gathered
+    ne_bytes = 50 * nnz * (6 * 4 + ncomp * 4)
+    peaks, peak_kind = measured_peaks()
+    res = {
+        "metric": "graph edges/s through label_propagation_init (partition, reductions, recursive init, "
+                  "reduced-graph embedding, expander)",
+        "value": nnz / (lp_ms / 1000.0), "unit": "edges/s", "ms": lp_ms, "graph_nnz": nnz, "rows": n,
+        "n_components": ncomp, "approx_n_parts": approx, "n_label_prop_iter": 20, "n_embedding_epochs": 50,
+        "stages_ms": stages, "gpu_launches": runs[-1][1],
+        "node_embedding_full_graph": {
+            "ms": ne_ms, "epochs": 50, "ms_per_epoch": ne_ms / 50, "edge_epochs_per_s": 50 * nnz / (ne_ms / 1000.0),
+            "roofline": {"bound": "hbm", "achieved": ne_bytes / (ne_ms / 1000.0) / 1e9,
+                         "peak": float(peaks.get("hbm_gbs")), "unit": "GB/s",
+                         "frac": ne_bytes / (ne_ms / 1000.0) / 1e9 / float(peaks.get("hbm_gbs")),
+                         "peak_kind": peak_kind, "traffic": None,
+                         "note": "latency-bound gathers; bytes = 6 schedule/index words + one embedding row "
+                                 "per edge per epoch"}},
+        "parity": "bit-identical to the oracle (tests/test_label_prop_gpu.py); oracle pinned to the "
+                  "reference's golden intermediates",
+    }
+    m = min(args.cpu_lp_rows, n)
+    if m > 0:
+        from oracle import label_prop as OL
+
+        xs = x[:m].contiguous()
+        si = torch.empty((m, k), dtype=torch.int32, device=dev)
+        sd = torch.empty((m, k), dtype=torch.float32, device=dev)
+        evoc.knn_graph_device(xs.data_ptr(), 0, m, d, k, si.data_ptr(), sd.data_ptr(), opts)
+        torch.cuda.synchronize()
+        indptr, indices, data, _, _ = evoc.neighbor_graph_csr(float(k), si.cpu().numpy(), sd.cpu().numpy())
+        g = OL.Csr.make(indptr, indices, data, (m, m))
+        xh = xs.cpu().numpy()
+        ap2 = int(np.clip(8 * np.sqrt(m), 256, 16384))
+        LP.label_propagation_init((indptr, indices, data, m), 20, 50, ap2, ncomp, 0.5, 0.1, 0.5,
+                                  np.random.RandomState(5), xh)
+        t0 = time.perf_counter()
+        gi = LP.label_propagation_init((indptr, indices, data, m), 20, 50, ap2, ncomp, 0.5, 0.1, 0.5,
+                                       np.random.RandomState(5), xh)
+        tg = time.perf_counter() - t0
+        rs = np.random.RandomState(5)
+        _, key, pos, hg, ga = rs.get_state()
+        t0 = time.perf_counter()
+        oi = OL.label_propagation_init(g, 20, 50, ap2, ncomp, 0.5, 0.1, 0.5, OL.mt_from_state(key, pos, hg, ga), xh)
+        to = time.perf_counter() - t0
+        res["cpu_baseline"] = {
+            "value": g.nnz / to, "unit": "edges/s", "cores": 1, "kind": "port",
+            "sample": (f"oracle restatement of label_propagation_init (C + NumPy, one thread; the reference's "
+                       f"label propagation and reproducible epochs are serial) on the fuzzy graph of the first "
+                       f"{m} rows ({g.nnz} entries): {to:.2f} s; the GPU with host buffers on the same graph "
+                       f"{tg * 1000:.1f} ms, max |GPU - oracle| = {float(np.abs(gi - oi).max()):.3g}")}
+    return res
+
+
 def run_ours(args, world, rank, local):
     import numpy as np
     import torch
@@ -731,6 +822,9 @@ def run_ours(args, world, rank, local):
                  "stages_ms": {nm: statistics.mean(t[nm] for t in times) for nm in times[0] if nm != "total"},
                  "nnz": int(nnz.value), "rows": n, "k": k,
                  "note": "sigma/rho bisection, membership strengths, A + A^T - A o A^T as canonical CSR"}
+        if args.label_prop and world == 1:
+            fuzzy["label_propagation_init"] = run_label_prop(args, dev, ctx, stream, x, f_indptr, f_ind, f_dat,
+                                                             int(nnz.value), opts)
         del f_indptr, f_ind, f_dat, f_sig, f_rho
 
     # End to end through the public API with pinned host buffers.
@@ -866,6 +960,10 @@ def main():
     ap.add_argument("--form", default="bf16_rerank", choices=["bf16_rerank", "nndescent"],
                     help="zipf_f32 workload: the exact BF16+rerank form (headline) or GPU NN-descent")
     ap.add_argument("--fuzzy", type=int, default=1, help="time the fuzzy graph of the built graph")
+    ap.add_argument("--label-prop", type=int, default=1,
+                    help="time label_propagation_init and the node embedding on the fuzzy graph")
+    ap.add_argument("--cpu-lp-rows", type=int, default=100000,
+                    help="rows of the graph the oracle's label_propagation_init is timed on")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--fp32-rows", type=int, default=75_776)  # 2 full waves of 296 CTAs x 128 rows
     ap.add_argument("--recall-rows", type=int, default=10_000)

@@ -726,9 +726,13 @@ __global__ void __launch_bounds__(256) pca_kernel(const float* x, int64_t n, int
 
 // ------------------------------------------------------------------ node embedding
 
+// Largest positive weight (as int bits: positive floats order like their bits).
 __global__ void ne_maxw_kernel(const float* w, int64_t m, float* max_w) {
+  int best = 0;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x)
-    if (w[i] > 0.0f) atomicMax((int*)max_w, __float_as_int(w[i]));
+    if (w[i] > 0.0f) best = max(best, __float_as_int(w[i]));
+  best = __reduce_max_sync(kFull, best);
+  if ((threadIdx.x & 31) == 0 && best > 0) atomicMax((int*)max_w, best);
 }
 
 __global__ void ne_schedule_kernel(const float* w, int64_t m, float nf, float nsr, const float* max_w, float* eps,
@@ -762,11 +766,205 @@ __device__ __forceinline__ uint64_t neg_count(float nf, float eon, float rate) {
 
 __device__ __forceinline__ float clip4(float v) { return v > 4.0f ? 4.0f : (v < -4.0f ? -4.0f : v); }
 
+// Rows of more than min_deg edges, deferred by ne_block_kernel to ne_heavy_kernel.
+struct HeavyRows {
+  int64_t min_deg;
+  uint32_t* rows;
+  int32_t* count;
+};
+
+// The positive move of one edge (scaled by alpha); false when the squared
+// distance is 0 (the reference adds nothing then).
+template <int MAXD>
+__device__ __forceinline__ bool ne_pos(const float* cur, const float* yt, int ncomp, float noise, float alpha,
+                                       float* out) {
+  float ds = 0.0f;
+#pragma unroll
+  for (int d = 0; d < MAXD; d++)
+    if (d < ncomp) {
+      const float df = __fsub_rn(cur[d], yt[d]);
+      ds = __fadd_rn(ds, __fmul_rn(df, df));
+    }
+  if (!(ds > 0.0f)) return false;
+  const float dist = __fsqrt_rn(ds);
+  const float num = __fsub_rn(__fmul_rn(__fmul_rn(-2.0f, noise), dist), 2.0f);
+  const float den = __fadd_rn(__fsub_rn(__fmul_rn(2.0f, ds), __fmul_rn(0.5f, dist)), 1.0f);
+  const float gc = __fdiv_rn(num, den);
+#pragma unroll
+  for (int d = 0; d < MAXD; d++)
+    if (d < ncomp) out[d] = __fmul_rn(__fmul_rn(gc, __fsub_rn(cur[d], yt[d])), alpha);
+  return true;
+}
+
+// Negative sample p of edge `raw` (scaled and clipped); false when it adds nothing.
+template <int MAXD>
+__device__ __forceinline__ bool ne_neg(const float* cur, const float* emb, const uint32_t* order, uint64_t nv,
+                                       uint64_t raw, uint64_t p, uint32_t epoch, uint32_t rng_state, int ncomp,
+                                       float gamma, float alpha, float* out) {
+  const uint64_t idx = (raw * ((uint64_t)epoch + p + 1ull) * (uint64_t)rng_state) % nv;
+  const uint64_t tn = order[idx];
+  if (tn >= nv) return false;
+  const float* yn = emb + tn * ncomp;
+  float dn = 0.0f;
+#pragma unroll
+  for (int d = 0; d < MAXD; d++)
+    if (d < ncomp) {
+      const float df = __fsub_rn(cur[d], yn[d]);
+      dn = __fadd_rn(dn, __fmul_rn(df, df));
+    }
+  if (!(dn > 1e-2f)) return false;
+  const float gc = __fdiv_rn(__fmul_rn(gamma, 4.0f), __fmul_rn(__fadd_rn(1.0f, __fmul_rn(0.25f, dn)), dn));
+  if (!(gc > 0.0f)) return false;
+#pragma unroll
+  for (int d = 0; d < MAXD; d++)
+    if (d < ncomp) out[d] = __fmul_rn(clip4(__fmul_rn(gc, __fsub_rn(cur[d], yn[d]))), alpha);
+  return true;
+}
+
+constexpr int kHeavyWarps = 16;
+constexpr int kHeavySlots = 4;  // positive move + 3 negative samples staged per edge
+constexpr uint32_t kHeavyOverflow = 0x80000000u;
+
+__host__ __device__ inline int heavy_tile_edges(int ncomp) { return ncomp <= 8 ? 512 : (ncomp <= 16 ? 256 : 128); }
+__host__ __device__ inline size_t heavy_smem_bytes(int ncomp) {
+  return size_t(2) * heavy_tile_edges(ncomp) * (size_t(kHeavySlots) * ncomp + 2) * sizeof(float) +
+         size_t(heavy_tile_edges(ncomp)) * kHeavySlots * sizeof(uint32_t);
+}
+
+// One CTA per deferred row.  Warps 1..15 compute the contributions of a tile
+// of the row's edges into shared memory while warp 0 adds the previous
+// tile's, in edge order, lane d keeping component d of the update row (the
+// reference's order of f32 additions for that component).  An edge wanting
+// more negative samples than the staging holds is flagged and its samples
+// are computed by warp 0 in order.
+template <int MAXD>
+__global__ void __launch_bounds__(kHeavyWarps * 32)
+    ne_heavy_kernel(Csr g, float* emb, float* upd, const uint32_t* order, const float* eps, const float* epns,
+                    float* eonn, float* eons, uint32_t rng_state, int ncomp, float alpha, uint32_t epoch,
+                    float noise, float gamma, float decay, int apply_decay, HeavyRows heavy) {
+  extern __shared__ float hv_sh[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int te = heavy_tile_edges(ncomp);
+  const int stride = kHeavySlots * ncomp + 2;  // floats per staged edge: slots, mask, count
+  const uint64_t nv = (uint64_t)g.n;
+  const float nf = (float)epoch;
+  const int32_t cnt = *heavy.count;
+  for (int32_t h = blockIdx.x; h < cnt; h += gridDim.x) {
+    const uint64_t from = heavy.rows[h];
+    float cur[MAXD];
+#pragma unroll
+    for (int d = 0; d < MAXD; d++)
+      if (d < ncomp) cur[d] = emb[from * ncomp + d];
+    const uint64_t e0 = (uint64_t)g.indptr[from], e1 = (uint64_t)g.indptr[from + 1];
+    const int64_t tiles = (int64_t)((e1 - e0 + te - 1) / te);
+    float ud = 0.0f;
+    if (warp == 0 && lane < ncomp)
+      ud = apply_decay ? __fmul_rn(upd[from * ncomp + lane], decay) : upd[from * ncomp + lane];
+    auto stage = [&](int64_t tile, int first_thread, int threads) {
+      float* buf = hv_sh + (size_t)(tile & 1) * te * stride;
+      for (int i = (int)threadIdx.x - first_thread; i < te; i += threads) {
+        const uint64_t raw = e0 + (uint64_t)tile * te + i;
+        float* ent = buf + (size_t)i * stride;
+        uint32_t m = 0, nn = 0;
+        if (raw < e1 && !(eons[raw] > nf)) {
+          const uint64_t to = (uint64_t)(uint32_t)g.indices[raw];
+          if (to < nv) {
+            if (ne_pos<MAXD>(cur, emb + to * ncomp, ncomp, noise, alpha, ent)) m |= 1u;
+            eons[raw] = __fadd_rn(eons[raw], eps[raw]);
+            const float rate = epns[raw];
+            const uint64_t nneg = neg_count(nf, eonn[raw], rate);
+            nn = (uint32_t)nneg;
+            if (nneg < (uint64_t)kHeavySlots) {
+              for (uint64_t p = 0; p < nneg; p++)
+                if (ne_neg<MAXD>(cur, emb, order, nv, raw, p, epoch, rng_state, ncomp, gamma, alpha,
+                                 ent + (1 + p) * ncomp))
+                  m |= 2u << p;
+            } else {
+              m |= kHeavyOverflow;
+            }
+            eonn[raw] = __fadd_rn(eonn[raw], __fmul_rn(__ull2float_rn(nneg), rate));
+          }
+        }
+        reinterpret_cast<uint32_t*>(ent)[kHeavySlots * ncomp] = m;
+        reinterpret_cast<uint32_t*>(ent)[kHeavySlots * ncomp + 1] = nn;
+      }
+    };
+    stage(0, 0, blockDim.x);
+    __syncthreads();
+    uint32_t* offs = reinterpret_cast<uint32_t*>(hv_sh + (size_t)2 * te * stride);  // te * kHeavySlots
+    for (int64_t t = 0; t < tiles; t++) {
+      if (warp == 0) {
+        const float* buf = hv_sh + (size_t)(t & 1) * te * stride;
+        const int64_t left = (int64_t)(e1 - e0) - t * te;
+        const int n_in = (int)(left < te ? left : te);
+        // offsets (in floats) of the applied contributions, in edge order and slot order; an edge
+        // whose negative samples were not staged is listed as 0x80000000 | edge
+        const int per = (n_in + 31) / 32;
+        const int i0 = lane * per, i1 = min(n_in, i0 + per);
+        int mine = 0;
+        for (int i = i0; i < i1; i++) {
+          const uint32_t m = reinterpret_cast<const uint32_t*>(buf + (size_t)i * stride)[kHeavySlots * ncomp];
+          mine += (m & kHeavyOverflow) ? (int)(m & 1u) + 1 : __popc(m);
+        }
+        int at = mine;
+        for (int o = 1; o < 32; o <<= 1) {
+          const int v = __shfl_up_sync(kFull, at, o);
+          if (lane >= o) at += v;
+        }
+        const int total = __shfl_sync(kFull, at, 31);
+        at -= mine;
+        for (int i = i0; i < i1; i++) {
+          const uint32_t m = reinterpret_cast<const uint32_t*>(buf + (size_t)i * stride)[kHeavySlots * ncomp];
+          for (uint32_t bits = m & ~kHeavyOverflow; bits; bits &= bits - 1u)
+            offs[at++] = (uint32_t)(i * stride + (__ffs(bits) - 1) * ncomp);
+          if (m & kHeavyOverflow) offs[at++] = kHeavyOverflow | (uint32_t)i;
+        }
+        __syncwarp();
+        int q = 0;
+        for (; q + 4 <= total; q += 4) {
+          uint32_t o4[4];
+          float v4[4];
+#pragma unroll
+          for (int j = 0; j < 4; j++) o4[j] = offs[q + j];
+          if ((o4[0] | o4[1] | o4[2] | o4[3]) & kHeavyOverflow) break;
+#pragma unroll
+          for (int j = 0; j < 4; j++) v4[j] = lane < ncomp ? buf[o4[j] + lane] : 0.0f;
+#pragma unroll
+          for (int j = 0; j < 4; j++)
+            if (lane < ncomp) ud = __fadd_rn(ud, v4[j]);
+        }
+        for (; q < total; q++) {
+          const uint32_t o = offs[q];
+          if (o & kHeavyOverflow) {
+            const int i = (int)(o & ~kHeavyOverflow);
+            const uint32_t nn = reinterpret_cast<const uint32_t*>(buf + (size_t)i * stride)[kHeavySlots * ncomp + 1];
+            const uint64_t raw = e0 + (uint64_t)t * te + i;
+            float c[MAXD];
+            for (uint64_t p = 0; p < nn; p++)
+              if (ne_neg<MAXD>(cur, emb, order, nv, raw, p, epoch, rng_state, ncomp, gamma, alpha, c)) {
+#pragma unroll
+                for (int d = 0; d < MAXD; d++)
+                  if (d == lane && d < ncomp) ud = __fadd_rn(ud, c[d]);
+              }
+          } else if (lane < ncomp) {
+            ud = __fadd_rn(ud, buf[o + lane]);
+          }
+        }
+      } else if (t + 1 < tiles) {
+        stage(t + 1, 32, blockDim.x - 32);
+      }
+      __syncthreads();
+    }
+    if (warp == 0 && lane < ncomp) upd[from * ncomp + lane] = ud;
+    __syncthreads();
+  }
+}
+
 constexpr int kNeWarps = 4;    // warps (nodes in flight) per CTA
 constexpr int kNegSlots = 3;   // negative samples per edge staged at once
 
 // Per-warp staging: [32 lanes][1 + kNegSlots][ncomp] contributions, then 32
-// applied-slot masks and 32 negative-sample counts.
+// flags (and 32 spare words).
 __host__ __device__ inline int ne_stage_floats(int ncomp) { return 32 * (1 + kNegSlots) * ncomp + 64; }
 
 // One warp per node of the block.  The lanes take 32 consecutive edges and
@@ -780,18 +978,35 @@ template <int MAXD>
 __global__ void __launch_bounds__(kNeWarps * 32)
     ne_block_kernel(Csr g, float* emb, float* upd, const uint32_t* order, int64_t bs, int64_t be, const float* eps,
                     const float* epns, float* eonn, float* eons, uint32_t rng_state, int ncomp, float alpha,
-                    uint32_t epoch, float noise, float gamma, float decay, int apply_decay) {
+                    uint32_t epoch, float noise, float gamma, float decay, int apply_decay, HeavyRows heavy) {
   extern __shared__ float ne_sh[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   constexpr int kSlots = 1 + kNegSlots;
   float* vec = ne_sh + (size_t)warp * ne_stage_floats(ncomp);
   uint32_t* fmask = reinterpret_cast<uint32_t*>(vec + 32 * kSlots * ncomp);
-  int32_t* ncount = reinterpret_cast<int32_t*>(fmask + 32);
   const uint64_t nv = (uint64_t)g.n;
   const float nf = (float)epoch;
-  for (int64_t ni = bs + (int64_t)blockIdx.x * kNeWarps + warp; ni < be; ni += (int64_t)gridDim.x * kNeWarps) {
-    const uint64_t from = order[ni];
+  const int64_t step = (int64_t)gridDim.x * kNeWarps;
+  int64_t ni = bs + (int64_t)blockIdx.x * kNeWarps + warp;
+  // the next node's id and row bounds are loaded while the current one runs
+  uint64_t nfrom = ni < be ? order[ni] : nv;
+  uint64_t ne0 = 0, ne1 = 0;
+  if (nfrom < nv) {
+    ne0 = (uint64_t)g.indptr[nfrom];
+    ne1 = (uint64_t)g.indptr[nfrom + 1];
+  }
+  for (; ni < be; ni += step) {
+    const uint64_t from = nfrom, e0 = ne0, e1 = ne1;
+    nfrom = ni + step < be ? order[ni + step] : nv;
+    if (nfrom < nv) {
+      ne0 = (uint64_t)g.indptr[nfrom];
+      ne1 = (uint64_t)g.indptr[nfrom + 1];
+    }
     if (from >= nv) continue;
+    if ((int64_t)(e1 - e0) > heavy.min_deg) {  // deferred to ne_heavy_kernel
+      if (lane == 0) heavy.rows[atomicAdd(heavy.count, 1)] = (uint32_t)from;
+      continue;
+    }
     float cur[MAXD], u[MAXD];
 #pragma unroll
     for (int d = 0; d < MAXD; d++)
@@ -799,7 +1014,6 @@ __global__ void __launch_bounds__(kNeWarps * 32)
         cur[d] = emb[from * ncomp + d];
         u[d] = apply_decay ? __fmul_rn(upd[from * ncomp + d], decay) : upd[from * ncomp + d];
       }
-    const uint64_t e0 = (uint64_t)g.indptr[from], e1 = (uint64_t)g.indptr[from + 1];
     for (uint64_t base = e0; base < e1; base += 32) {
       const uint64_t raw = base + lane;
       bool act = false;
@@ -808,55 +1022,17 @@ __global__ void __launch_bounds__(kNeWarps * 32)
         to = (uint64_t)(uint32_t)g.indices[raw];
         act = to < nv;
       }
+      if (!__any_sync(kFull, act)) continue;
       uint32_t fl = 0;
       uint64_t nneg = 0;
       float rate = 0.0f;
       float cp[MAXD];
       if (act) {
-        const float* yt = emb + to * ncomp;
-        float ds = 0.0f;
-#pragma unroll
-        for (int d = 0; d < MAXD; d++)
-          if (d < ncomp) {
-            const float df = __fsub_rn(cur[d], yt[d]);
-            ds = __fadd_rn(ds, __fmul_rn(df, df));
-          }
-        if (ds > 0.0f) {
-          const float dist = __fsqrt_rn(ds);
-          const float num = __fsub_rn(__fmul_rn(__fmul_rn(-2.0f, noise), dist), 2.0f);
-          const float den = __fadd_rn(__fsub_rn(__fmul_rn(2.0f, ds), __fmul_rn(0.5f, dist)), 1.0f);
-          const float gc = __fdiv_rn(num, den);
-#pragma unroll
-          for (int d = 0; d < MAXD; d++)
-            if (d < ncomp) cp[d] = __fmul_rn(__fmul_rn(gc, __fsub_rn(cur[d], yt[d])), alpha);
-          fl = 1u;
-        }
+        if (ne_pos<MAXD>(cur, emb + to * ncomp, ncomp, noise, alpha, cp)) fl = 1u;
         eons[raw] = __fadd_rn(eons[raw], eps[raw]);
         rate = epns[raw];
         nneg = neg_count(nf, eonn[raw], rate);
       }
-      // contribution s of this lane's edge into staging slot `slot`; returns whether it applies
-      auto neg_contrib = [&](uint64_t p, int slot) -> bool {
-        const uint64_t idx = (raw * ((uint64_t)epoch + p + 1ull) * (uint64_t)rng_state) % nv;
-        const uint64_t tn = order[idx];
-        if (tn >= nv) return false;
-        const float* yn = emb + tn * ncomp;
-        float dn = 0.0f;
-#pragma unroll
-        for (int d = 0; d < MAXD; d++)
-          if (d < ncomp) {
-            const float df = __fsub_rn(cur[d], yn[d]);
-            dn = __fadd_rn(dn, __fmul_rn(df, df));
-          }
-        if (!(dn > 1e-2f)) return false;
-        const float gc = __fdiv_rn(__fmul_rn(gamma, 4.0f), __fmul_rn(__fadd_rn(1.0f, __fmul_rn(0.25f, dn)), dn));
-        if (!(gc > 0.0f)) return false;
-        float* dst = vec + ((size_t)lane * kSlots + slot) * ncomp;
-#pragma unroll
-        for (int d = 0; d < MAXD; d++)
-          if (d < ncomp) dst[d] = __fmul_rn(clip4(__fmul_rn(gc, __fsub_rn(cur[d], yn[d]))), alpha);
-        return true;
-      };
       auto add_slot = [&](int L, int slot) {
         const float* src = vec + ((size_t)L * kSlots + slot) * ncomp;
 #pragma unroll
@@ -872,16 +1048,16 @@ __global__ void __launch_bounds__(kNeWarps * 32)
             if (d < ncomp) dst[d] = cp[d];
         }
         for (int p = 0; p < maxneg; p++)
-          if ((uint64_t)p < nneg && neg_contrib((uint64_t)p, 1 + p)) fl |= 2u << p;
-        fmask[lane] = fl;
-        ncount[lane] = (int32_t)nneg;
+          if ((uint64_t)p < nneg &&
+              ne_neg<MAXD>(cur, emb, order, nv, raw, (uint64_t)p, epoch, rng_state, ncomp, gamma, alpha,
+                           vec + ((size_t)lane * kSlots + 1 + p) * ncomp))
+            fl |= 2u << p;
         __syncwarp();
-        for (int L = 0; L < 32; L++) {
-          const uint32_t f = fmask[L];
-          if (!f) continue;
-          const int cnt = 1 + ncount[L];
-          for (int sl = 0; sl < cnt; sl++)
-            if ((f >> sl) & 1u) add_slot(L, sl);
+        // lanes with something to add, in lane (= edge) order; their slots in sample order
+        for (unsigned live = __ballot_sync(kFull, fl != 0); live; live &= live - 1u) {
+          const int L = __ffs(live) - 1;
+          const uint32_t f = __shfl_sync(kFull, fl, L);
+          for (uint32_t bits = f; bits; bits &= bits - 1u) add_slot(L, __ffs(bits) - 1);
         }
         __syncwarp();
       } else {
@@ -900,7 +1076,11 @@ __global__ void __launch_bounds__(kNeWarps * 32)
             __syncwarp();
           }
           for (uint64_t p = 0; p < nL; p++) {
-            if (lane == L) fmask[L] = neg_contrib(p, 1) ? 1u : 0u;
+            if (lane == L)
+              fmask[L] = ne_neg<MAXD>(cur, emb, order, nv, raw, p, epoch, rng_state, ncomp, gamma, alpha,
+                                      vec + (size_t)lane * kSlots * ncomp + ncomp)
+                             ? 1u
+                             : 0u;
             __syncwarp();
             if (fmask[L]) add_slot(L, 1);
             __syncwarp();
@@ -1211,24 +1391,40 @@ cudaError_t launch_ne_schedule(const float* w, int64_t m, int32_t n_epochs, floa
 cudaError_t launch_ne_block(const Csr& g, float* emb, float* upd, const uint32_t* order, int64_t bs, int64_t be,
                             const float* eps, const float* epns, float* eonn, float* eons, uint32_t rng_state,
                             int ncomp, float alpha, uint8_t epoch, float noise, float gamma, float decay,
-                            int apply_decay, cudaStream_t s) {
+                            int apply_decay, int64_t heavy_deg, uint32_t* heavy_rows, int32_t* heavy_count, int sms,
+                            cudaStream_t s) {
   const int64_t warps = be - bs;
   if (warps <= 0) return cudaSuccess;
+  cudaError_t e = cudaMemsetAsync(heavy_count, 0, 4, s);
+  if (e != cudaSuccess) return e;
+  const HeavyRows heavy{heavy_deg, heavy_rows, heavy_count};
   const int grid = (int)std::min<int64_t>((warps + kNeWarps - 1) / kNeWarps, 1 << 20);
   const size_t smem = size_t(kNeWarps) * ne_stage_floats(ncomp) * sizeof(float);
-  cudaError_t e;
+  const size_t hsmem = heavy_smem_bytes(ncomp);
   if (ncomp <= 16) {
     if ((e = cudaFuncSetAttribute(ne_block_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
       return e;
     ne_block_kernel<16><<<grid, kNeWarps * 32, smem, s>>>(g, emb, upd, order, bs, be, eps, epns, eonn, eons,
                                                          rng_state, ncomp, alpha, epoch, noise, gamma, decay,
-                                                         apply_decay);
+                                                         apply_decay, heavy);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(ne_heavy_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem)))
+      return e;
+    ne_heavy_kernel<16><<<sms * 2, kHeavyWarps * 32, hsmem, s>>>(g, emb, upd, order, eps, epns, eonn, eons,
+                                                                 rng_state, ncomp, alpha, epoch, noise, gamma,
+                                                                 decay, apply_decay, heavy);
   } else {
     if ((e = cudaFuncSetAttribute(ne_block_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
       return e;
     ne_block_kernel<32><<<grid, kNeWarps * 32, smem, s>>>(g, emb, upd, order, bs, be, eps, epns, eonn, eons,
                                                          rng_state, ncomp, alpha, epoch, noise, gamma, decay,
-                                                         apply_decay);
+                                                         apply_decay, heavy);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(ne_heavy_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem)))
+      return e;
+    ne_heavy_kernel<32><<<sms * 2, kHeavyWarps * 32, hsmem, s>>>(g, emb, upd, order, eps, epns, eonn, eons,
+                                                                 rng_state, ncomp, alpha, epoch, noise, gamma,
+                                                                 decay, apply_decay, heavy);
   }
   return cudaGetLastError();
 }

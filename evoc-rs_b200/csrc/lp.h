@@ -115,11 +115,13 @@ cudaError_t launch_pca_init(const float* x, int64_t n, int64_t d, int ncomp, flo
 // node_embedding (reproducible): per-edge schedules.
 cudaError_t launch_ne_schedule(const float* w, int64_t m, int32_t n_epochs, float negative_sample_rate, float* eps,
                                float* epns, float* eonn, float* eons, float* max_w, cudaStream_t s);
-// One block of one epoch: nodes order[bs, be); then the apply launch.
+// One block of one epoch: nodes order[bs, be), rows of more than heavy_deg
+// edges by one CTA each (heavy_rows holds be - bs ids); then the apply launch.
 cudaError_t launch_ne_block(const Csr& g, float* emb, float* upd, const uint32_t* order, int64_t bs, int64_t be,
                             const float* eps, const float* epns, float* eonn, float* eons, uint32_t rng_state,
                             int ncomp, float alpha, uint8_t epoch, float noise, float gamma, float decay,
-                            int apply_decay, cudaStream_t s);
+                            int apply_decay, int64_t heavy_deg, uint32_t* heavy_rows, int32_t* heavy_count, int sms,
+                            cudaStream_t s);
 cudaError_t launch_ne_apply(float* emb, const float* upd, const uint32_t* order, int64_t bs, int64_t be, int64_t nv,
                             int ncomp, cudaStream_t s);
 

@@ -119,6 +119,7 @@ struct Arena {
 
 constexpr int64_t kBaseInitThreshold = 64;  // src/label_prop.rs:507 default
 constexpr int32_t kMaxParts = 65536;        // parts fit the 16-bit fields of the sort keys
+constexpr int64_t kHeavyDegree = 512;       // embedding rows above this many edges get a CTA each
 
 struct Level {
   int32_t n_iter, n_epochs, ncomp;
@@ -244,7 +245,8 @@ int node_embedding_dev(evoc_gpu_ctx* ctx, Arena& A, const lp::Csr& g, const floa
     EVOC_TRY(cudaStreamSynchronize(s), "upload init");
   }
   float *eps, *epns, *eonn, *eons, *upd, *maxw;
-  uint32_t* d_order;
+  uint32_t *d_order, *heavy_rows;
+  int32_t* heavy_count;
   EVOC_TRY(A.get(&eps, size_t(m)), "alloc schedule");
   EVOC_TRY(A.get(&epns, size_t(m)), "alloc schedule");
   EVOC_TRY(A.get(&eonn, size_t(m)), "alloc schedule");
@@ -252,6 +254,8 @@ int node_embedding_dev(evoc_gpu_ctx* ctx, Arena& A, const lp::Csr& g, const floa
   EVOC_TRY(A.get(&maxw, 1), "alloc");
   EVOC_TRY(A.get(&upd, size_t(n * ncomp)), "alloc updates");
   EVOC_TRY(A.get(&d_order, size_t(2 * n)), "alloc node order");
+  EVOC_TRY(A.get(&heavy_rows, size_t(std::max<int64_t>(1024, n / 8))), "alloc heavy rows");
+  EVOC_TRY(A.get(&heavy_count, 1), "alloc");
   EVOC_TRY(cudaMemsetAsync(upd, 0, size_t(n * ncomp) * 4, s), "memset updates");
   {
     Stage st(ctx, "epochs_per_sample");
@@ -294,9 +298,10 @@ int node_embedding_dev(evoc_gpu_ctx* ctx, Arena& A, const lp::Csr& g, const floa
     for (int64_t bs = 0; bs < n && e == cudaSuccess; bs += block) {
       const int64_t be = std::min(n, bs + block);
       e = lp::launch_ne_block(g, emb, upd, d_order + size_t(slot) * n, bs, be, eps, epns, eonn, eons,
-                              seeds[size_t(ep)], ncomp, alpha, uint8_t(ep), noise, gamma, decay, ep > 0 ? 1 : 0, s);
+                              seeds[size_t(ep)], ncomp, alpha, uint8_t(ep), noise, gamma, decay, ep > 0 ? 1 : 0,
+                              kHeavyDegree, heavy_rows, heavy_count, ctx->sms, s);
       if (e == cudaSuccess) e = lp::launch_ne_apply(emb, upd, d_order + size_t(slot) * n, bs, be, n, ncomp, s);
-      ctx->launches += 2;
+      ctx->launches += 3;
     }
     if (e != cudaSuccess) {
       rc = cuda_fail(ctx, e, "node embedding epoch");

@@ -174,3 +174,42 @@ def test_errors_are_reported_not_faulted(blob_graph):
         evoc.label_prop_loop((g.indptr, bad, g.data, g.shape[0]), np.random.RandomState(1), 3, 100)
     with pytest.raises(evoc.EmptyData):
         evoc.node_embedding((np.zeros(1, np.int64), np.zeros(0, np.int32), np.zeros(0, np.float32), 0), 4, 5)
+
+
+def _hub_graph(n=6000, hubs=5, hub_deg=2500, seed=3):
+    """Symmetric random graph with a few rows of thousands of edges (above the one-CTA-per-row
+    threshold of the embedding kernel), weights in (0, 1]."""
+    rng = np.random.default_rng(seed)
+    r = rng.integers(0, n, 8 * n)
+    c = rng.integers(0, n, 8 * n)
+    for h in range(hubs):
+        t = rng.choice(n, hub_deg, replace=False)
+        r = np.concatenate([r, np.full(hub_deg, h)])
+        c = np.concatenate([c, t])
+    keep = r != c
+    r, c = r[keep], c[keep]
+    key = np.unique(np.minimum(r, c).astype(np.int64) * n + np.maximum(r, c))
+    a, b = key // n, key % n
+    w = rng.uniform(0.05, 1.0, len(key)).astype(np.float32)
+    rr = np.concatenate([a, b])
+    cc = np.concatenate([b, a])
+    ww = np.concatenate([w, w])
+    o = np.lexsort((cc, rr))
+    indptr = np.zeros(n + 1, np.int64)
+    np.cumsum(np.bincount(rr, minlength=n), out=indptr[1:])
+    return L.Csr.make(indptr, cc[o].astype(np.int32), ww[o], (n, n))
+
+
+@pytest.mark.parametrize("nsr,ncomp", [(1.0, 4), (5.0, 7), (5.0, 20)])
+def test_node_embedding_hub_rows_and_many_negative_samples(nsr, ncomp):
+    """Rows of ~2500 edges take the one-CTA-per-row path; a negative-sample rate of 5 gives edges
+    more negative samples than either kernel stages at once (their samples are then computed in
+    order by the accumulating warp)."""
+    g = _hub_graph()
+    assert np.diff(g.indptr).max() > 2000
+    rs = np.random.RandomState(11)
+    orng = _oracle_rng(rs)
+    emb = evoc.node_embedding(_tuple(g), ncomp, 6, None, 0.1, nsr, 0.5, rs)
+    want = L.node_embedding(g, ncomp, 6, None, 0.1, nsr, 0.5, orng)
+    assert np.array_equal(emb.view(np.uint32), want.view(np.uint32))
+    assert _same_state(rs, orng)
