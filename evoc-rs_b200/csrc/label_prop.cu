@@ -1,7 +1,7 @@
 // Label-propagation initialisation and reproducible node-embedding kernels.
 //
 //   label_prop_iteration ........ src/label_prop.rs:39-91     lp_iteration_kernel
-//   label_outliers .............. src/label_prop.rs:94-132    lp_outliers_kernel
+//   label_outliers .............. src/label_prop.rs:94-132    outlier_walk_kernel + pointer jumping
 //   remap_labels ................ src/label_prop.rs:135-157   remap_* kernels
 //   partition reduction maps .... src/label_prop.rs:188-230   part_* kernels
 //   csr_matmul_dense ............ src/label_prop.rs:233-250   reduce_data_kernel, expand_kernel
@@ -42,6 +42,7 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int32_t kNoKey = INT32_MIN;
+constexpr int64_t kOutlierStack = 4096;  // per-warp stack entries of the parallel outlier walks
 
 // tau RNG step, src/rng.rs:5-35 (int64 state words, 32-bit result).
 __device__ int32_t tau_rand_int(int64_t st[3]) {
@@ -60,19 +61,28 @@ __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, 
 // built by adding its values in entry order, the first value stored as is.
 // Returns false, with the table as before the chunk, when the chunk's new
 // keys do not fit in `cap` slots.
+// With `dix` (overflow rows), the slot of key k is dix[k + dix_off] (-1 when
+// absent) instead of a search of the table; the caller clears the entries it
+// set once the row is done.
 template <class Acc>
-__device__ bool table_chunk(int32_t key, Acc val, bool valid, int32_t* tkey, Acc* tsum, int cap, int& cnt) {
+__device__ bool table_chunk(int32_t key, Acc val, bool valid, int32_t* tkey, Acc* tsum, int cap, int& cnt,
+                            int32_t* dix = nullptr, int32_t dix_off = 0) {
   const int lane = threadIdx.x & 31;
   const int32_t k = valid ? key : kNoKey;
   const unsigned peers = __match_any_sync(kFull, k);
   const bool leader = valid && (__ffs(peers) - 1 == lane);
   int slot = -1;
-  if (leader)
-    for (int t = 0; t < cnt; t++)
-      if (tkey[t] == k) {
-        slot = t;
-        break;
-      }
+  if (leader) {
+    if (dix) {
+      slot = dix[k + dix_off];
+    } else {
+      for (int t = 0; t < cnt; t++)
+        if (tkey[t] == k) {
+          slot = t;
+          break;
+        }
+    }
+  }
   const unsigned newm = __ballot_sync(kFull, leader && slot < 0);
   if (cnt + __popc(newm) > cap) return false;
   const bool fresh = leader && slot < 0;
@@ -89,12 +99,20 @@ __device__ bool table_chunk(int32_t key, Acc val, bool valid, int32_t* tkey, Acc
     }
   }
   if (leader) {
-    if (fresh) tkey[slot] = k;
+    if (fresh) {
+      tkey[slot] = k;
+      if (dix) dix[k + dix_off] = slot;
+    }
     tsum[slot] = acc;
   }
   cnt += __popc(newm);
   __syncwarp();
   return true;
+}
+
+__device__ __forceinline__ void table_clear(const int32_t* tkey, int cnt, int32_t* dix, int32_t dix_off) {
+  for (int t = threadIdx.x & 31; t < cnt; t += 32) dix[tkey[t] + dix_off] = -1;
+  __syncwarp();
 }
 
 // ------------------------------------------------------------------ label propagation
@@ -104,7 +122,7 @@ __device__ bool table_chunk(int32_t key, Acc val, bool valid, int32_t* tkey, Acc
 // (the reference's loop, src/label_prop.rs:71-88, with cur == -1 for every
 // row that reaches it).
 __device__ bool vote_row(const Csr& g, int64_t r, const int32_t* lab, int32_t* tkey, double* tsum, int cap,
-                         int32_t cur, int32_t* res) {
+                         int32_t cur, int32_t* res, int32_t* dix = nullptr) {
   const int lane = threadIdx.x & 31;
   const int64_t s = g.indptr[r], e = g.indptr[r + 1];
   int cnt = 0;
@@ -117,7 +135,7 @@ __device__ bool vote_row(const Csr& g, int64_t r, const int32_t* lab, int32_t* t
       l = lab[g.indices[k]];
       w = (double)g.data[k];
     }
-    if (!table_chunk<double>(l, w, valid, tkey, tsum, cap, cnt)) return false;
+    if (!table_chunk<double>(l, w, valid, tkey, tsum, cap, cnt, dix, 1)) return false;
   }
   double m = 1.0;
   for (int t = lane; t < cnt; t += 32)
@@ -128,6 +146,7 @@ __device__ bool vote_row(const Csr& g, int64_t r, const int32_t* lab, int32_t* t
     if (tkey[t] != -1 && tsum[t] == m) last = t;
   last = __reduce_max_sync(kFull, last);
   *res = last >= 0 ? tkey[last] : cur;
+  if (dix) table_clear(tkey, cnt, dix, 1);
   return true;
 }
 
@@ -150,14 +169,16 @@ __global__ void __launch_bounds__(kRowWarps * 32)
 
 __global__ void __launch_bounds__(kRowWarps * 32)
     lp_overflow_kernel(Csr g, const int32_t* lab_in, int32_t* lab_out, const int32_t* overflow,
-                       const int32_t* n_overflow, int32_t* skey, double* ssum, int64_t cap) {
+                       const int32_t* n_overflow, int32_t* skey, double* ssum, int64_t cap, int32_t* dix,
+                       int64_t key_bound) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t gw = (int64_t)blockIdx.x * kRowWarps + warp, nw = (int64_t)gridDim.x * kRowWarps;
   const int32_t cnt = *n_overflow;
   for (int64_t i = gw; i < cnt; i += nw) {
     const int64_t r = overflow[i];
     int32_t res = lab_in[r];
-    vote_row(g, r, lab_in, skey + gw * cap, ssum + gw * cap, (int)cap, res, &res);
+    vote_row(g, r, lab_in, skey + gw * cap, ssum + gw * cap, (int)cap, res, &res,
+             dix ? dix + gw * key_bound : nullptr);
     if (lane == 0) lab_out[r] = res;
   }
 }
@@ -196,60 +217,139 @@ __global__ void outlier_flags_kernel(const int32_t* labels, int64_t n, int32_t* 
   if ((threadIdx.x & 31) == 0) atomicMax(max_label, m);
 }
 
-// label_outliers: one warp walks the unlabelled rows (rows[0 .. *count), in
-// row order).  The stack holds at most 1 + 64 * max_deg entries (64 pops,
-// each pushing at most one row's columns); a walk that would pass `cap` sets
-// status and stops.
-__global__ void lp_outliers_kernel(Csr g, int32_t* labels, const int64_t* rs_p, const int32_t* rows,
-                                   const int32_t* count, const int32_t* max_label, int32_t* stack, int64_t cap,
-                                   int32_t* status) {
+// label_outliers, all unlabelled rows at once.  In the reference's row-order
+// pass, row j reads as labelled at row i's turn exactly when it was labelled
+// before the pass or is an unlabelled row before i (those are all assigned by
+// then), so every walk's path is fixed in advance: each row's walk runs on
+// its own warp against the labels from before the pass.  A walk that stops at
+// an earlier unlabelled row records that row (its label is copied once
+// known); one that runs 64 pops or empties its stack takes the random label
+// from its own tau stream.
+struct WalkOut {
+  int32_t fin;  // label, or -1 when copied from `ptr`
+  int32_t ptr;  // earlier unlabelled row whose label is copied, or -1
+};
+
+// Returns false (nothing written) when the walk outgrows `cap` stack entries.
+__device__ bool outlier_walk(const Csr& g, const int32_t* labels, int64_t i, int32_t ml, int64_t rs0, int64_t rs1,
+                             int64_t rs2, int32_t* stack, int64_t cap, WalkOut* out) {
   const int lane = threadIdx.x & 31;
-  const int32_t ml = *max_label, n_rows = *count;
-  const int64_t rs0 = rs_p[0], rs1 = rs_p[1], rs2 = rs_p[2];
-  for (int32_t oi = 0; oi < n_rows; oi++) {
-    const int64_t row = rows[oi];
-    if (lane == 0) stack[0] = (int32_t)row;
-    __syncwarp();
-    int64_t top = 1;
-    bool unl = true;
-    int it = 0;
-    while (unl && it < 64 && top > 0) {
-      it++;
-      top--;
-      const int64_t node = stack[top];
-      const int64_t s = g.indptr[node], e = g.indptr[node + 1];
-      for (int64_t b = s; b < e; b += 32) {
-        const int64_t k = b + lane;
-        const bool valid = k < e;
-        const int32_t j = valid ? g.indices[k] : 0;
-        const int32_t lj = valid ? labels[j] : -1;
-        const unsigned hit = __ballot_sync(kFull, valid && lj >= 0);
-        const int npush = hit ? __ffs(hit) - 1 : __popc(__ballot_sync(kFull, valid));
-        if (top + npush > cap) {
-          if (lane == 0) atomicExch(status, 1);
-          return;
-        }
-        if (lane < npush) stack[top + lane] = j;
-        top += npush;
-        if (hit) {
-          const int32_t lab = __shfl_sync(kFull, lj, __ffs(hit) - 1);
-          if (lane == 0) labels[row] = lab;
-          unl = false;
-          break;
-        }
+  if (lane == 0) stack[0] = (int32_t)i;
+  __syncwarp();
+  int64_t top = 1;
+  bool unl = true;
+  int it = 0;
+  int32_t fin = -1, ptr = -1;
+  while (unl && it < 64 && top > 0) {
+    it++;
+    top--;
+    const int64_t node = stack[top];
+    const int64_t s = g.indptr[node], e = g.indptr[node + 1];
+    for (int64_t b = s; b < e; b += 32) {
+      const int64_t k = b + lane;
+      const bool valid = k < e;
+      const int32_t j = valid ? g.indices[k] : 0;
+      const int32_t lj = valid ? labels[j] : -1;
+      const unsigned hit = __ballot_sync(kFull, valid && (lj >= 0 || (int64_t)j < i));
+      const int npush = hit ? __ffs(hit) - 1 : __popc(__ballot_sync(kFull, valid));
+      if (top + npush > cap) return false;
+      if (lane < npush) stack[top + lane] = j;
+      top += npush;
+      if (hit) {
+        const int f = __ffs(hit) - 1;
+        const int32_t jj = __shfl_sync(kFull, j, f), ll = __shfl_sync(kFull, lj, f);
+        if (ll >= 0) fin = ll;
+        else ptr = jj;
+        unl = false;
+        break;
       }
-      __syncwarp();
-    }
-    if (lane == 0 && (it >= 64 || unl)) {
-      int64_t st[3] = {(int64_t)((uint64_t)rs0 + (uint64_t)row), (int64_t)((uint64_t)rs1 + (uint64_t)row),
-                       (int64_t)((uint64_t)rs2 + (uint64_t)row)};
-      const int64_t draw = tau_rand_int(st);
-      const int64_t mod = (int64_t)ml + 1;
-      const int64_t v = draw % mod;
-      labels[row] = (int32_t)(v < 0 ? v + mod : v);
     }
     __syncwarp();
   }
+  if (it >= 64 || unl) {
+    int64_t st[3] = {(int64_t)((uint64_t)rs0 + (uint64_t)i), (int64_t)((uint64_t)rs1 + (uint64_t)i),
+                     (int64_t)((uint64_t)rs2 + (uint64_t)i)};
+    const int64_t draw = tau_rand_int(st);
+    const int64_t mod = (int64_t)ml + 1;
+    const int64_t v = draw % mod;
+    fin = (int32_t)(v < 0 ? v + mod : v);
+    ptr = -1;
+  }
+  if (lane == 0) *out = WalkOut{fin, ptr};
+  __syncwarp();
+  return true;
+}
+
+__global__ void __launch_bounds__(kRowWarps * 32)
+    outlier_walk_kernel(Csr g, const int32_t* labels, const int64_t* rs, const int32_t* rows, const int32_t* count,
+                        const int32_t* max_label, int32_t* stacks, int64_t scap, WalkOut* out, int32_t* big,
+                        int32_t* n_big) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t gw = (int64_t)blockIdx.x * kRowWarps + warp, nw = (int64_t)gridDim.x * kRowWarps;
+  const int32_t cnt = *count, ml = *max_label;
+  for (int64_t oi = gw; oi < cnt; oi += nw)
+    if (!outlier_walk(g, labels, rows[oi], ml, rs[0], rs[1], rs[2], stacks + gw * scap, scap, out + oi) && lane == 0)
+      big[atomicAdd(n_big, 1)] = (int32_t)oi;
+}
+
+// The walks that outgrew the per-warp stacks, one warp with the full stack.
+__global__ void outlier_walk_big_kernel(Csr g, const int32_t* labels, const int64_t* rs, const int32_t* rows,
+                                        const int32_t* max_label, const int32_t* big, const int32_t* n_big,
+                                        int32_t* stack, int64_t cap, WalkOut* out, int32_t* status) {
+  const int32_t nb = *n_big, ml = *max_label;
+  for (int32_t b = 0; b < nb; b++) {
+    const int32_t oi = big[b];
+    if (!outlier_walk(g, labels, rows[oi], ml, rs[0], rs[1], rs[2], stack, cap, out + oi)) {
+      if ((threadIdx.x & 31) == 0) atomicExch(status, 1);
+      return;
+    }
+  }
+}
+
+// Copied labels by pointer jumping over the unlabelled rows (pointers go to
+// earlier rows, so the chains end): nxt = -1 marks a row whose label is known.
+__global__ void outlier_resolve_init_kernel(const WalkOut* out, const int32_t* count, const int32_t* rows,
+                                            int32_t* oidx, int32_t* lab, int32_t* nxt) {
+  const int32_t cnt = *count;
+  for (int64_t oi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; oi < cnt; oi += (int64_t)gridDim.x * blockDim.x)
+    oidx[rows[oi]] = (int32_t)oi;
+}
+
+__global__ void outlier_resolve_start_kernel(const WalkOut* out, const int32_t* count, const int32_t* oidx,
+                                             int32_t* lab, int32_t* nxt) {
+  const int32_t cnt = *count;
+  for (int64_t oi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; oi < cnt;
+       oi += (int64_t)gridDim.x * blockDim.x) {
+    const WalkOut w = out[oi];
+    lab[oi] = w.fin;
+    nxt[oi] = w.ptr < 0 ? -1 : oidx[w.ptr];
+  }
+}
+
+__global__ void outlier_resolve_round_kernel(const int32_t* count, const int32_t* lab_a, const int32_t* nxt_a,
+                                             int32_t* lab_b, int32_t* nxt_b, int32_t* pending) {
+  const int32_t cnt = *count;
+  for (int64_t oi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; oi < cnt;
+       oi += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t t = nxt_a[oi];
+    if (t < 0) {
+      lab_b[oi] = lab_a[oi];
+      nxt_b[oi] = -1;
+    } else if (nxt_a[t] < 0) {
+      lab_b[oi] = lab_a[t];
+      nxt_b[oi] = -1;
+    } else {
+      lab_b[oi] = -1;
+      nxt_b[oi] = nxt_a[t];
+      *pending = 1;
+    }
+  }
+}
+
+__global__ void outlier_scatter_kernel(const int32_t* count, const int32_t* rows, const int32_t* lab, int32_t* labels) {
+  const int32_t cnt = *count;
+  for (int64_t oi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; oi < cnt; oi += (int64_t)gridDim.x * blockDim.x)
+    labels[rows[oi]] = lab[oi];
 }
 
 __global__ void remap_flags_kernel(const int32_t* labels, int64_t n, int32_t bound, int32_t* flags,
@@ -303,7 +403,7 @@ __global__ void part_norm_kernel(const int32_t* count, int32_t n_parts, float* x
 }
 
 // One warp per (part, 32 columns): each lane sums its column over the part's
-// members in order; the member rows are loaded 8 ahead of the adds.
+// members in order; the members' rows are loaded 32 at a time ahead of the adds.
 __global__ void __launch_bounds__(256)
     reduce_data_kernel(const float* x, int64_t d, const int32_t* members, const int64_t* start, const int32_t* count,
                        const float* wred, int32_t n_parts, float* out) {
@@ -314,21 +414,25 @@ __global__ void __launch_bounds__(256)
   const int64_t tasks = (int64_t)n_parts * chunks;
   for (int64_t task = gw; task < tasks; task += nw) {
     const int64_t p = task / chunks, col = (task % chunks) * 32 + lane;
-    if (col >= d) continue;
+    const bool in = col < d;
     const double w = (double)wred[p];
     const int32_t* mem = members + start[p];
     const int32_t c = count[p];
     float acc = 0.0f;
-    int32_t t = 0;
-    for (; t + 8 <= c; t += 8) {
-      float v[8];
+    for (int32_t t0 = 0; t0 < c; t0 += 32) {
+      const int nb = min(32, c - t0);
+      const int32_t mine = lane < nb ? mem[t0 + lane] : 0;
+      float v[32];
 #pragma unroll
-      for (int u = 0; u < 8; u++) v[u] = x[(int64_t)mem[t + u] * d + col];
+      for (int u = 0; u < 32; u++) {
+        const int32_t m = __shfl_sync(kFull, mine, u);
+        v[u] = (in && u < nb) ? x[(int64_t)m * d + col] : 0.0f;
+      }
 #pragma unroll
-      for (int u = 0; u < 8; u++) acc = __fadd_rn(acc, __double2float_rn(__dmul_rn(w, (double)v[u])));
+      for (int u = 0; u < 32; u++)
+        if (u < nb) acc = __fadd_rn(acc, __double2float_rn(__dmul_rn(w, (double)v[u])));
     }
-    for (; t < c; t++) acc = __fadd_rn(acc, __double2float_rn(__dmul_rn(w, (double)x[(int64_t)mem[t] * d + col])));
-    out[p * d + col] = acc;
+    if (in) out[p * d + col] = acc;
   }
 }
 
@@ -500,7 +604,7 @@ __global__ void sym_write_kernel(const uint64_t* key, const uint32_t* prod, cons
 // stored (and summed for the L1 norm, and multiplied into the layout) in
 // reverse order; then the average with the row's own part layout.
 __device__ bool expand_row(const Csr& sym, int64_t r, const int32_t* part, const float* xnorm, const float* layout,
-                           int ncomp, int32_t* tkey, float* tsum, int cap, float* result) {
+                           int ncomp, int32_t* tkey, float* tsum, int cap, float* result, int32_t* dix = nullptr) {
   const int lane = threadIdx.x & 31;
   const int64_t s = sym.indptr[r], e = sym.indptr[r + 1];
   int cnt = 0;
@@ -513,7 +617,7 @@ __device__ bool expand_row(const Csr& sym, int64_t r, const int32_t* part, const
       q = part[sym.indices[k]];
       v = __fmul_rn(sym.data[k], xnorm[q]);
     }
-    if (!table_chunk<float>(q, v, valid, tkey, tsum, cap, cnt)) return false;
+    if (!table_chunk<float>(q, v, valid, tkey, tsum, cap, cnt, dix, 0)) return false;
   }
   float rs = 0.0f;
   for (int t = cnt - 1; t >= 0; t--) {
@@ -533,6 +637,7 @@ __device__ bool expand_row(const Csr& sym, int64_t r, const int32_t* part, const
     result[r * ncomp + lane] = __double2float_rn(__dmul_rn(__dadd_rn((double)a, (double)bb), 0.5));
   }
   __syncwarp();
+  if (dix) table_clear(tkey, cnt, dix, 0);
   return true;
 }
 
@@ -551,27 +656,53 @@ __global__ void __launch_bounds__(kRowWarps * 32)
 __global__ void __launch_bounds__(kRowWarps * 32)
     expand_overflow_kernel(Csr sym, const int32_t* part, const float* xnorm, const float* layout, int ncomp,
                            float* result, const int32_t* overflow, const int32_t* n_overflow, int32_t* skey,
-                           float* ssum, int64_t cap) {
+                           float* ssum, int64_t cap, int32_t* dix, int64_t key_bound) {
   const int warp = threadIdx.x >> 5;
   const int64_t gw = (int64_t)blockIdx.x * kRowWarps + warp, nw = (int64_t)gridDim.x * kRowWarps;
   const int32_t cnt = *n_overflow;
   for (int64_t i = gw; i < cnt; i += nw)
-    expand_row(sym, overflow[i], part, xnorm, layout, ncomp, skey + gw * cap, ssum + gw * cap, (int)cap, result);
+    expand_row(sym, overflow[i], part, xnorm, layout, ncomp, skey + gw * cap, ssum + gw * cap, (int)cap, result,
+               dix ? dix + gw * key_bound : nullptr);
 }
 
-// Column means summed in row order (f64), one thread per column, rows staged
-// through shared memory.
+// Column means summed in row order (f64).  The block streams tiles of rows
+// into shared memory (double-buffered) while lane c of warp 0 adds column c
+// of the previous tile in row order.
+constexpr int kCenterTile = 6144;  // floats per tile buffer
+
 __global__ void __launch_bounds__(1024) center_mean_kernel(const float* result, int64_t n, int ncomp, double* mean) {
-  __shared__ float tile[8192];
-  const int rows_per = 8192 / ncomp;
+  __shared__ float tile[2][kCenterTile];
+  const int rows_per = kCenterTile / ncomp;
+  const int64_t tiles = (n + rows_per - 1) / rows_per;
+  auto load = [&](int64_t t) {
+    const int64_t r0 = t * rows_per;
+    const int64_t cnt = min((int64_t)rows_per, n - r0) * ncomp;
+    for (int64_t i = threadIdx.x; i < cnt; i += blockDim.x) tile[t & 1][i] = result[r0 * ncomp + i];
+  };
   double acc = 0.0;
-  for (int64_t r0 = 0; r0 < n; r0 += rows_per) {
-    const int64_t rows = min((int64_t)rows_per, n - r0);
+  if (tiles > 0) load(0);
+  __syncthreads();
+  for (int64_t t = 0; t < tiles; t++) {
+    if (threadIdx.x < 32) {
+      if (threadIdx.x < ncomp) {
+        const int rows = (int)min((int64_t)rows_per, n - t * rows_per);
+        const float* src = tile[t & 1] + threadIdx.x;
+        int r = 0;
+        for (; r + 8 <= rows; r += 8) {
+          float v[8];
+#pragma unroll
+          for (int u = 0; u < 8; u++) v[u] = src[(r + u) * ncomp];
+#pragma unroll
+          for (int u = 0; u < 8; u++) acc = __dadd_rn(acc, (double)v[u]);
+        }
+        for (; r < rows; r++) acc = __dadd_rn(acc, (double)src[r * ncomp]);
+      }
+    } else if (t + 1 < tiles) {
+      const int64_t r0 = (t + 1) * rows_per;
+      const int64_t cnt = min((int64_t)rows_per, n - r0) * ncomp;
+      for (int64_t i = threadIdx.x - 32; i < cnt; i += blockDim.x - 32) tile[(t + 1) & 1][i] = result[r0 * ncomp + i];
+    }
     __syncthreads();
-    for (int64_t i = threadIdx.x; i < rows * ncomp; i += blockDim.x) tile[i] = result[r0 * ncomp + i];
-    __syncthreads();
-    if (threadIdx.x < ncomp)
-      for (int64_t r = 0; r < rows; r++) acc = __dadd_rn(acc, (double)tile[r * ncomp + threadIdx.x]);
   }
   if (threadIdx.x < ncomp) mean[threadIdx.x] = __ddiv_rn(acc, (double)n);
 }
@@ -837,8 +968,8 @@ __host__ __device__ inline size_t heavy_smem_bytes(int ncomp) {
 // reference's order of f32 additions for that component).  An edge wanting
 // more negative samples than the staging holds is flagged and its samples
 // are computed by warp 0 in order.
-template <int MAXD>
-__global__ void __launch_bounds__(kHeavyWarps * 32)
+template <int MAXD, int MINB>
+__global__ void __launch_bounds__(kHeavyWarps * 32, MINB)
     ne_heavy_kernel(Csr g, float* emb, float* upd, const uint32_t* order, const float* eps, const float* epns,
                     float* eonn, float* eons, uint32_t rng_state, int ncomp, float alpha, uint32_t epoch,
                     float noise, float gamma, float decay, int apply_decay, HeavyRows heavy) {
@@ -974,8 +1105,8 @@ __host__ __device__ inline int ne_stage_floats(int ncomp) { return 32 * (1 + kNe
 // the node's update row -- the reference's serial order of f32 additions.
 // Edges wanting more than kNegSlots negative samples in a chunk are handed
 // through the staging one contribution at a time instead.
-template <int MAXD>
-__global__ void __launch_bounds__(kNeWarps * 32)
+template <int MAXD, int MINB>
+__global__ void __launch_bounds__(kNeWarps * 32, MINB)
     ne_block_kernel(Csr g, float* emb, float* upd, const uint32_t* order, int64_t bs, int64_t be, const float* eps,
                     const float* epns, float* eonn, float* eons, uint32_t rng_state, int ncomp, float alpha,
                     uint32_t epoch, float noise, float gamma, float decay, int apply_decay, HeavyRows heavy) {
@@ -1145,7 +1276,7 @@ cudaError_t launch_seed_labels(int32_t* labels, const int64_t* idx, int64_t coun
 
 cudaError_t launch_lp_iteration(const Csr& g, const int32_t* lab_in, int32_t* lab_out, int32_t* overflow,
                                 int32_t* n_overflow, int32_t* scratch_key, double* scratch_sum, int64_t max_deg,
-                                int sms, cudaStream_t s) {
+                                int32_t* dix, int64_t key_bound, int sms, cudaStream_t s) {
   cudaError_t e = cudaMemsetAsync(n_overflow, 0, 4, s);
   if (e != cudaSuccess) return e;
   const int grid = grid_for(g.n, kRowWarps, sms * 8);
@@ -1153,7 +1284,7 @@ cudaError_t launch_lp_iteration(const Csr& g, const int32_t* lab_in, int32_t* la
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (max_deg > kVoteSlots) {
     lp_overflow_kernel<<<sms, kRowWarps * 32, 0, s>>>(g, lab_in, lab_out, overflow, n_overflow, scratch_key,
-                                                      scratch_sum, max_deg);
+                                                      scratch_sum, max_deg, dix, key_bound);
     e = cudaGetLastError();
   }
   return e;
@@ -1166,17 +1297,48 @@ size_t lp_outliers_tmp_bytes(int64_t n) {
   return b;
 }
 
-cudaError_t launch_lp_outliers(const Csr& g, int32_t* labels, const int64_t* rs, int32_t* stack, int64_t stack_cap,
-                               int32_t* flag, int32_t* rows, int32_t* count, int32_t* max_label, void* tmp,
-                               size_t tmp_bytes, int32_t* status, cudaStream_t s) {
-  cudaError_t e = cudaMemsetAsync(max_label, 0, 4, s);
+size_t outlier_stack_entries(int sms) { return size_t(sms) * 4 * kRowWarps * kOutlierStack; }
+
+cudaError_t run_lp_outliers(const Csr& g, int32_t* labels, const int64_t* rs, const OutlierScratch& w, int64_t max_deg,
+                            int sms, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(w.max_label, 0, 4, s);
   if (e != cudaSuccess) return e;
-  outlier_flags_kernel<<<grid_for(g.n, 256, 2048), 256, 0, s>>>(labels, g.n, flag, max_label);
+  if ((e = cudaMemsetAsync(w.n_big, 0, 4, s)) != cudaSuccess) return e;
+  outlier_flags_kernel<<<grid_for(g.n, 256, 2048), 256, 0, s>>>(labels, g.n, w.flag, w.max_label);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  e = cub::DeviceSelect::Flagged(tmp, tmp_bytes, thrust::counting_iterator<int32_t>(0), flag, rows, count, (int)g.n,
+  size_t tb = w.tmp_bytes;
+  e = cub::DeviceSelect::Flagged(w.tmp, tb, thrust::counting_iterator<int32_t>(0), w.flag, w.rows, w.count, (int)g.n,
                                  s);
   if (e != cudaSuccess) return e;
-  lp_outliers_kernel<<<1, 32, 0, s>>>(g, labels, rs, rows, count, max_label, stack, stack_cap, status);
+  int32_t cnt = 0;
+  if ((e = cudaMemcpyAsync(&cnt, w.count, 4, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+  if (cnt == 0) return cudaSuccess;
+  WalkOut* out = reinterpret_cast<WalkOut*>(w.walk);
+  outlier_walk_kernel<<<sms * 4, kRowWarps * 32, 0, s>>>(g, labels, rs, w.rows, w.count, w.max_label, w.stacks,
+                                                         kOutlierStack, out, w.big, w.n_big);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  outlier_walk_big_kernel<<<1, 32, 0, s>>>(g, labels, rs, w.rows, w.max_label, w.big, w.n_big, w.big_stack,
+                                           64 * max_deg + 1, out, w.status);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  const int grid = grid_for(cnt, 256, 4096);
+  outlier_resolve_init_kernel<<<grid, 256, 0, s>>>(out, w.count, w.rows, w.oidx, w.lab[0], w.nxt[0]);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  outlier_resolve_start_kernel<<<grid, 256, 0, s>>>(out, w.count, w.oidx, w.lab[0], w.nxt[0]);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  int cur = 0;
+  for (int round = 0; round < 64; round++) {  // chains halve each round: 2^64 > any row count
+    if ((e = cudaMemsetAsync(w.pending, 0, 4, s)) != cudaSuccess) return e;
+    outlier_resolve_round_kernel<<<grid, 256, 0, s>>>(w.count, w.lab[cur], w.nxt[cur], w.lab[cur ^ 1],
+                                                      w.nxt[cur ^ 1], w.pending);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    cur ^= 1;
+    int32_t pend = 0;
+    if ((e = cudaMemcpyAsync(&pend, w.pending, 4, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+    if (!pend) break;
+  }
+  outlier_scatter_kernel<<<grid, 256, 0, s>>>(w.count, w.rows, w.lab[cur], labels);
   return cudaGetLastError();
 }
 
@@ -1344,7 +1506,8 @@ cudaError_t launch_hadamard_sym(const Csr& g, const ReduceScratch& w, int64_t* s
 
 cudaError_t launch_expand(const Csr& sym, const int32_t* part, const float* xnorm, const float* layout, int ncomp,
                           float* result, int32_t* overflow, int32_t* n_overflow, int32_t* scratch_key,
-                          float* scratch_sum, int64_t max_deg, int sms, cudaStream_t s) {
+                          float* scratch_sum, int64_t max_deg, int32_t* dix, int64_t key_bound, int sms,
+                          cudaStream_t s) {
   cudaError_t e = cudaMemsetAsync(n_overflow, 0, 4, s);
   if (e != cudaSuccess) return e;
   expand_kernel<<<grid_for(sym.n, kRowWarps, sms * 8), kRowWarps * 32, 0, s>>>(sym, part, xnorm, layout, ncomp,
@@ -1352,7 +1515,8 @@ cudaError_t launch_expand(const Csr& sym, const int32_t* part, const float* xnor
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (max_deg > kVoteSlots) {
     expand_overflow_kernel<<<sms, kRowWarps * 32, 0, s>>>(sym, part, xnorm, layout, ncomp, result, overflow,
-                                                          n_overflow, scratch_key, scratch_sum, max_deg);
+                                                          n_overflow, scratch_key, scratch_sum, max_deg, dix,
+                                                          key_bound);
     e = cudaGetLastError();
   }
   return e;
@@ -1401,32 +1565,22 @@ cudaError_t launch_ne_block(const Csr& g, float* emb, float* upd, const uint32_t
   const int grid = (int)std::min<int64_t>((warps + kNeWarps - 1) / kNeWarps, 1 << 20);
   const size_t smem = size_t(kNeWarps) * ne_stage_floats(ncomp) * sizeof(float);
   const size_t hsmem = heavy_smem_bytes(ncomp);
-  if (ncomp <= 16) {
-    if ((e = cudaFuncSetAttribute(ne_block_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
-      return e;
-    ne_block_kernel<16><<<grid, kNeWarps * 32, smem, s>>>(g, emb, upd, order, bs, be, eps, epns, eonn, eons,
-                                                         rng_state, ncomp, alpha, epoch, noise, gamma, decay,
-                                                         apply_decay, heavy);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(ne_heavy_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem)))
-      return e;
-    ne_heavy_kernel<16><<<sms * 2, kHeavyWarps * 32, hsmem, s>>>(g, emb, upd, order, eps, epns, eonn, eons,
-                                                                 rng_state, ncomp, alpha, epoch, noise, gamma,
-                                                                 decay, apply_decay, heavy);
-  } else {
-    if ((e = cudaFuncSetAttribute(ne_block_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
-      return e;
-    ne_block_kernel<32><<<grid, kNeWarps * 32, smem, s>>>(g, emb, upd, order, bs, be, eps, epns, eonn, eons,
-                                                         rng_state, ncomp, alpha, epoch, noise, gamma, decay,
-                                                         apply_decay, heavy);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(ne_heavy_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem)))
-      return e;
-    ne_heavy_kernel<32><<<sms * 2, kHeavyWarps * 32, hsmem, s>>>(g, emb, upd, order, eps, epns, eonn, eons,
-                                                                 rng_state, ncomp, alpha, epoch, noise, gamma,
-                                                                 decay, apply_decay, heavy);
-  }
-  return cudaGetLastError();
+  auto run = [&](auto block_kernel, auto heavy_kernel) -> cudaError_t {
+    cudaError_t err = cudaFuncSetAttribute(block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return err;
+    block_kernel<<<grid, kNeWarps * 32, smem, s>>>(g, emb, upd, order, bs, be, eps, epns, eonn, eons, rng_state, ncomp,
+                                                   alpha, epoch, noise, gamma, decay, apply_decay, heavy);
+    if ((err = cudaGetLastError()) != cudaSuccess) return err;
+    if ((err = cudaFuncSetAttribute(heavy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem)))
+      return err;
+    heavy_kernel<<<sms * 2, kHeavyWarps * 32, hsmem, s>>>(g, emb, upd, order, eps, epns, eonn, eons, rng_state, ncomp,
+                                                          alpha, epoch, noise, gamma, decay, apply_decay, heavy);
+    return cudaGetLastError();
+  };
+  // narrow rows: more warps per SM (64 registers); wider rows keep their values in registers
+  if (ncomp <= 8) return run(ne_block_kernel<8, 8>, ne_heavy_kernel<8, 2>);
+  if (ncomp <= 16) return run(ne_block_kernel<16, 1>, ne_heavy_kernel<16, 1>);
+  return run(ne_block_kernel<32, 1>, ne_heavy_kernel<32, 1>);
 }
 
 cudaError_t launch_ne_apply(float* emb, const float* upd, const uint32_t* order, int64_t bs, int64_t be, int64_t nv,

@@ -33,17 +33,26 @@ cudaError_t launch_seed_labels(int32_t* labels, const int64_t* idx, int64_t coun
 // One label_prop_iteration sweep.  Rows whose table outgrows shared memory go
 // to overflow[] (count in *n_overflow) and are finished by the second launch
 // with tables in `scratch` (warps x max_deg slots).
+// dix: key_bound ints per overflow warp (labels -1 .. key_bound - 2), all -1, or null.
 cudaError_t launch_lp_iteration(const Csr& g, const int32_t* lab_in, int32_t* lab_out, int32_t* overflow,
                                 int32_t* n_overflow, int32_t* scratch_key, double* scratch_sum, int64_t max_deg,
-                                int sms, cudaStream_t s);
+                                int32_t* dix, int64_t key_bound, int sms, cudaStream_t s);
 
-// label_outliers in row order (one warp over the compacted unlabelled rows);
-// labels are int32; rs = tau seed (3 x int64); flag/rows hold n ints, count
-// and max_label one each, tmp lp_outliers_tmp_bytes(n).
-cudaError_t launch_lp_outliers(const Csr& g, int32_t* labels, const int64_t* rs, int32_t* stack, int64_t stack_cap,
-                               int32_t* flag, int32_t* rows, int32_t* count, int32_t* max_label, void* tmp,
-                               size_t tmp_bytes, int32_t* status, cudaStream_t s);
+// label_outliers (see label_prop.cu): all unlabelled rows walked at once,
+// copied labels resolved by pointer jumping.  Buffers: flag, rows, oidx,
+// lab[2], nxt[2], big: n ints each; walk: 2 n ints; stacks:
+// outlier_stack_entries(sms) ints; big_stack: 64 * max_deg + 1 ints; count,
+// max_label, n_big, pending, status: one int each; tmp: lp_outliers_tmp_bytes(n).
+struct OutlierScratch {
+  int32_t *flag, *rows, *oidx, *lab[2], *nxt[2], *big, *walk, *stacks, *big_stack;
+  int32_t *count, *max_label, *n_big, *pending, *status;
+  void* tmp;
+  size_t tmp_bytes;
+};
+cudaError_t run_lp_outliers(const Csr& g, int32_t* labels, const int64_t* rs, const OutlierScratch& w, int64_t max_deg,
+                            int sms, cudaStream_t s);
 size_t lp_outliers_tmp_bytes(int64_t n);
+size_t outlier_stack_entries(int sms);
 
 // remap_labels: dense ranks of the labels present (all labels are >= 0 here).
 // flags/map hold `bound` ints; *n_parts receives the number of labels.
@@ -97,9 +106,11 @@ cudaError_t launch_hadamard_sym(const Csr& g, const ReduceScratch& w, int64_t* s
 // result[r, :] = ((expander row r . layout) + layout[part[r], :]) / 2 in the
 // reference's rounding; rows whose part table overflows shared memory are
 // finished with `scratch` tables.
+// dix: key_bound (= number of parts) ints per overflow warp, all -1, or null.
 cudaError_t launch_expand(const Csr& sym, const int32_t* part, const float* xnorm, const float* layout, int ncomp,
                           float* result, int32_t* overflow, int32_t* n_overflow, int32_t* scratch_key,
-                          float* scratch_sum, int64_t max_deg, int sms, cudaStream_t s);
+                          float* scratch_sum, int64_t max_deg, int32_t* dix, int64_t key_bound, int sms,
+                          cudaStream_t s);
 
 // out[r, c] = f32(f64(scaling) * (f64(result[r, c]) - mean_c)), mean_c the f64
 // mean of column c summed in row order.

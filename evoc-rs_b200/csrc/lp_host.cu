@@ -143,15 +143,22 @@ int64_t read_i64(evoc_gpu_ctx* ctx, const int64_t* d, cudaError_t* err) {
 }
 
 // Row-overflow tables for the warp-per-row kernels: one table of max_deg
-// slots per resident warp, only when some row can outgrow shared memory.
+// slots per resident warp, only when some row can outgrow shared memory, and
+// (keys below key_bound <= 65537) a direct key -> slot index per warp.
 template <class Acc>
-int overflow_tables(evoc_gpu_ctx* ctx, Arena& A, int64_t max_deg, int32_t** key, Acc** sum) {
+int overflow_tables(evoc_gpu_ctx* ctx, Arena& A, int64_t max_deg, int64_t key_bound, int32_t** key, Acc** sum,
+                    int32_t** dix) {
   *key = nullptr;
   *sum = nullptr;
+  *dix = nullptr;
   if (max_deg <= lp::kVoteSlots) return EVOC_OK;
-  const size_t slots = size_t(ctx->sms) * lp::kRowWarps * size_t(max_deg);
-  EVOC_TRY(A.get(key, slots), "alloc overflow tables");
-  EVOC_TRY(A.get(sum, slots), "alloc overflow tables");
+  const size_t warps = size_t(ctx->sms) * lp::kRowWarps;
+  EVOC_TRY(A.get(key, warps * size_t(max_deg)), "alloc overflow tables");
+  EVOC_TRY(A.get(sum, warps * size_t(max_deg)), "alloc overflow tables");
+  if (key_bound <= 65537) {
+    EVOC_TRY(A.get(dix, warps * size_t(key_bound)), "alloc overflow index");
+    EVOC_TRY(cudaMemsetAsync(*dix, 0xff, warps * size_t(key_bound) * 4, ctx->stream), "clear overflow index");
+  }
   return EVOC_OK;
 }
 
@@ -164,7 +171,7 @@ int lp_loop_dev(evoc_gpu_ctx* ctx, Arena& A, const lp::Csr& g, Mt& rng, int32_t 
   std::vector<int64_t> seeds(size_t(std::max<int64_t>(approx, 0)));
   for (auto& v : seeds) v = rng.randint(0, g.n);
   int64_t *d_rs, *d_seeds, *d_maxdeg;
-  int32_t *tmp_lab, *overflow, *n_over, *stack, *status, *flags, *map, *d_nparts;
+  int32_t *tmp_lab, *overflow, *n_over, *status, *flags, *map, *d_nparts;
   EVOC_TRY(A.get(&d_rs, 3), "alloc");
   EVOC_TRY(A.get(&d_seeds, seeds.size()), "alloc");
   EVOC_TRY(A.get(&d_maxdeg, 1), "alloc");
@@ -181,9 +188,10 @@ int lp_loop_dev(evoc_gpu_ctx* ctx, Arena& A, const lp::Csr& g, Mt& rng, int32_t 
   cudaError_t e;
   const int64_t max_deg = read_i64(ctx, d_maxdeg, &e);
   EVOC_TRY(e, "max degree");
-  int32_t* okey;
+  int32_t *okey, *odix;
   double* osum;
-  if (int rc = overflow_tables(ctx, A, max_deg, &okey, &osum)) return rc;
+  const int64_t key_bound = std::max<int64_t>(approx, 1) + 1;  // labels -1 .. approx - 1
+  if (int rc = overflow_tables(ctx, A, max_deg, key_bound, &okey, &osum, &odix)) return rc;
   {
     Stage st(ctx, "label_prop_iterations");
     EVOC_TRY(cudaMemsetAsync(labels, 0xff, size_t(g.n) * 4, s), "labels");
@@ -192,7 +200,8 @@ int lp_loop_dev(evoc_gpu_ctx* ctx, Arena& A, const lp::Csr& g, Mt& rng, int32_t 
     int32_t* cur = labels;
     int32_t* nxt = tmp_lab;
     for (int32_t it = 0; it < n_iter; it++) {
-      EVOC_TRY(lp::launch_lp_iteration(g, cur, nxt, overflow, n_over, okey, osum, max_deg, ctx->sms, s),
+      EVOC_TRY(lp::launch_lp_iteration(g, cur, nxt, overflow, n_over, okey, osum, max_deg, odix, key_bound, ctx->sms,
+                                       s),
                "label_prop_iteration");
       ctx->launches += max_deg > lp::kVoteSlots ? 2 : 1;
       std::swap(cur, nxt);
@@ -201,19 +210,30 @@ int lp_loop_dev(evoc_gpu_ctx* ctx, Arena& A, const lp::Csr& g, Mt& rng, int32_t 
   }
   {
     Stage st(ctx, "label_outliers");
-    const int64_t cap = 64 * max_deg + 1;
-    int32_t *oflag, *orows, *ocount, *omax;
-    EVOC_TRY(A.get(&stack, size_t(cap)), "alloc outlier stack");
-    EVOC_TRY(A.get(&oflag, size_t(g.n)), "alloc");
-    EVOC_TRY(A.get(&orows, size_t(g.n)), "alloc");
-    EVOC_TRY(A.get(&ocount, 1), "alloc");
-    EVOC_TRY(A.get(&omax, 1), "alloc");
-    const size_t otb = lp::lp_outliers_tmp_bytes(g.n);
+    lp::OutlierScratch ow{};
+    const size_t nn = size_t(g.n);
+    EVOC_TRY(A.get(&ow.flag, nn), "alloc outliers");
+    EVOC_TRY(A.get(&ow.rows, nn), "alloc outliers");
+    EVOC_TRY(A.get(&ow.oidx, nn), "alloc outliers");
+    EVOC_TRY(A.get(&ow.lab[0], nn), "alloc outliers");
+    EVOC_TRY(A.get(&ow.lab[1], nn), "alloc outliers");
+    EVOC_TRY(A.get(&ow.nxt[0], nn), "alloc outliers");
+    EVOC_TRY(A.get(&ow.nxt[1], nn), "alloc outliers");
+    EVOC_TRY(A.get(&ow.big, nn), "alloc outliers");
+    EVOC_TRY(A.get(&ow.walk, 2 * nn), "alloc outliers");
+    EVOC_TRY(A.get(&ow.stacks, lp::outlier_stack_entries(ctx->sms)), "alloc outlier stacks");
+    EVOC_TRY(A.get(&ow.big_stack, size_t(64 * max_deg + 1)), "alloc outlier stack");
+    EVOC_TRY(A.get(&ow.count, 1), "alloc");
+    EVOC_TRY(A.get(&ow.max_label, 1), "alloc");
+    EVOC_TRY(A.get(&ow.n_big, 1), "alloc");
+    EVOC_TRY(A.get(&ow.pending, 1), "alloc");
+    ow.status = status;
+    ow.tmp_bytes = lp::lp_outliers_tmp_bytes(g.n);
     uint8_t* otmp;
-    EVOC_TRY(A.get(&otmp, otb), "alloc");
-    EVOC_TRY(lp::launch_lp_outliers(g, labels, d_rs, stack, cap, oflag, orows, ocount, omax, otmp, otb, status, s),
-             "label_outliers");
-    ctx->launches += 3;
+    EVOC_TRY(A.get(&otmp, ow.tmp_bytes), "alloc");
+    ow.tmp = otmp;
+    EVOC_TRY(lp::run_lp_outliers(g, labels, d_rs, ow, max_deg, ctx->sms, s), "label_outliers");
+    ctx->launches += 8;
   }
   const int32_t bound = int32_t(std::max<int64_t>(approx, 1));
   EVOC_TRY(A.get(&flags, size_t(bound)), "alloc");
@@ -425,13 +445,13 @@ int lp_init_level(evoc_gpu_ctx* ctx, const lp::ReduceScratch& W, const lp::Csr& 
   EVOC_TRY(lp::launch_max_degree(s_indptr, g.n, d_maxdeg, s), "max degree");
   const int64_t max_deg = read_i64(ctx, d_maxdeg, &e);
   EVOC_TRY(e, "max degree");
-  int32_t* okey;
+  int32_t *okey, *odix;
   float* osum;
-  if (int rc = overflow_tables(ctx, A, max_deg, &okey, &osum)) return rc;
+  if (int rc = overflow_tables(ctx, A, max_deg, n_parts, &okey, &osum, &odix)) return rc;
   {
     Stage st(ctx, "expand_and_scale");
-    EVOC_TRY(lp::launch_expand(sym, part, xnorm, rinit, L.ncomp, result, overflow, n_over, okey, osum, max_deg,
-                               ctx->sms, s),
+    EVOC_TRY(lp::launch_expand(sym, part, xnorm, rinit, L.ncomp, result, overflow, n_over, okey, osum, max_deg, odix,
+                               n_parts, ctx->sms, s),
              "partition expander");
     EVOC_TRY(lp::launch_center_scale(result, g.n, L.ncomp, L.scaling, out, mean, s), "centre and scale");
     ctx->launches += max_deg > lp::kVoteSlots ? 4 : 3;

@@ -213,3 +213,23 @@ def test_node_embedding_hub_rows_and_many_negative_samples(nsr, ncomp):
     want = L.node_embedding(g, ncomp, 6, None, 0.1, nsr, 0.5, orng)
     assert np.array_equal(emb.view(np.uint32), want.view(np.uint32))
     assert _same_state(rs, orng)
+
+
+def test_label_prop_and_init_on_hub_rows():
+    """Hub rows see more distinct labels / parts than a warp's shared-memory table holds: the
+    overflow passes (direct key index in global memory) must give the same votes and expander
+    rows as the oracle."""
+    g = _hub_graph(n=6000, hubs=6, hub_deg=3000, seed=5)
+    for seed, approx in ((2, 1500), (3, 400)):
+        rs = np.random.RandomState(seed)
+        orng = _oracle_rng(rs)
+        part = evoc.label_prop_loop(_tuple(g), rs, 20, approx)
+        want = L.label_prop_loop(g, orng, 20, approx)
+        assert np.array_equal(part, want), (seed, approx)
+    x = np.random.default_rng(4).normal(size=(g.shape[0], 24)).astype(np.float32)
+    rs = np.random.RandomState(8)
+    orng = _oracle_rng(rs)
+    init = evoc.label_propagation_init(_tuple(g), 20, 20, 1500, 5, 0.5, 0.1, 0.5, rs, x)
+    want = L.label_propagation_init(g, 20, 20, 1500, 5, 0.5, 0.1, 0.5, orng, x)
+    assert np.abs(init - want).max() <= 1e-4
+    assert _same_state(rs, orng)
