@@ -10,7 +10,8 @@
 //   pca_init + small-graph norm . src/label_prop.rs:251-309   pca_kernel
 //   final centring / scaling .... src/label_prop.rs:660-672   center_* kernels
 //   make_epochs_per_sample ...... src/embed.rs:10-23          ne_schedule_kernel
-//   node_embedding_epoch_repr ... src/embed.rs:138-248        ne_block_kernel, ne_apply_kernel
+//   node_embedding_epoch_repr ... src/embed.rs:138-248        ne_block_kernel, ne_heavy_kernel, ne_apply_kernel
+//   node_embedding_epoch ........ src/embed.rs:57-135         ne_hogwild_kernel (lock-free, not bit-exact)
 //
 // Every result matches the reference's rounding: f32 expressions are written
 // with __fmul_rn / __fadd_rn / __fsub_rn / __fdiv_rn / __fsqrt_rn so nvcc
@@ -866,8 +867,8 @@ __global__ void ne_maxw_kernel(const float* w, int64_t m, float* max_w) {
   if ((threadIdx.x & 31) == 0 && best > 0) atomicMax((int*)max_w, best);
 }
 
-__global__ void ne_schedule_kernel(const float* w, int64_t m, float nf, float nsr, const float* max_w, float* eps,
-                                   float* epns, float* eonn, float* eons) {
+__global__ void ne_schedule_kernel(const float* w, int64_t m, float nf, float nsr, float neg_scale,
+                                   const float* max_w, float* eps, float* epns, float* eonn, float* eons) {
   const float mx = *max_w;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
     float e;
@@ -879,7 +880,7 @@ __global__ void ne_schedule_kernel(const float* w, int64_t m, float nf, float ns
       e = __fdiv_rn(nf, ns);
     }
     float en = __fdiv_rn(e, nsr);
-    en = __fmul_rn(en, 1.5f);
+    en = __fmul_rn(en, neg_scale);
     eps[i] = e;
     eons[i] = e;
     epns[i] = en;
@@ -1228,6 +1229,83 @@ __global__ void __launch_bounds__(kNeWarps * 32, MINB)
   }
 }
 
+// node_embedding_epoch (the non-reproducible epoch, src/embed.rs:57-135): the
+// reference walks the edges in order and updates both ends in place; here
+// every edge of the epoch runs at once (lock-free, as Python's parallel
+// version does), the updates landing with atomic adds.  The per-edge sample
+// schedules advance exactly as in the serial loop; the embedding agrees with
+// it in distribution, not bit for bit.
+__global__ void edge_head_kernel(const int64_t* indptr, int64_t n, uint32_t* head) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
+    for (int64_t e = indptr[r]; e < indptr[r + 1]; e++) head[e] = (uint32_t)r;
+}
+
+template <int MAXD>
+__global__ void __launch_bounds__(256)
+    ne_hogwild_kernel(Csr g, const uint32_t* head, float* emb, const float* eps, const float* epns, float* eonn,
+                      float* eons, uint32_t rng_state, int ncomp, float alpha, uint32_t epoch, float noise) {
+  const uint64_t nv = (uint64_t)g.n;
+  const float nf = (float)epoch;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < g.nnz; i += (int64_t)gridDim.x * blockDim.x) {
+    if (eons[i] > nf) continue;
+    const uint64_t j = head[i], k = (uint64_t)(uint32_t)g.indices[i];
+    if (j >= nv || k >= nv) continue;
+    float ej[MAXD], ek[MAXD];
+#pragma unroll
+    for (int d = 0; d < MAXD; d++)
+      if (d < ncomp) {
+        ej[d] = emb[j * ncomp + d];
+        ek[d] = emb[k * ncomp + d];
+      }
+    float ds = 0.0f;
+#pragma unroll
+    for (int d = 0; d < MAXD; d++)
+      if (d < ncomp) {
+        const float df = __fsub_rn(ej[d], ek[d]);
+        ds = __fadd_rn(ds, __fmul_rn(df, df));
+      }
+    if (ds > 0.0f) {
+      const float dist = __fsqrt_rn(ds);
+      const float num = __fsub_rn(__fmul_rn(__fmul_rn(-2.0f, noise), dist), 2.0f);
+      const float den = __fadd_rn(__fsub_rn(__fmul_rn(2.0f, ds), __fmul_rn(0.5f, dist)), 1.0f);
+      const float gc = __fdiv_rn(num, den);
+#pragma unroll
+      for (int d = 0; d < MAXD; d++)
+        if (d < ncomp) {
+          const float step = __fmul_rn(__fmul_rn(gc, __fsub_rn(ej[d], ek[d])), alpha);
+          atomicAdd(&emb[j * ncomp + d], step);
+          atomicAdd(&emb[k * ncomp + d], -step);
+          ej[d] = __fadd_rn(ej[d], step);
+        }
+    }
+    eons[i] = __fadd_rn(eons[i], eps[i]);
+    const float rate = epns[i];
+    const uint64_t nneg = neg_count(nf, eonn[i], rate);
+    for (uint64_t p = 0; p < nneg; p++) {
+      const uint64_t nk = (((uint64_t)epoch + p) * (uint64_t)i * (uint64_t)rng_state) % nv;
+      const float* en = emb + nk * ncomp;
+      float dn = 0.0f;
+#pragma unroll
+      for (int d = 0; d < MAXD; d++)
+        if (d < ncomp) {
+          const float df = __fsub_rn(ej[d], en[d]);
+          dn = __fadd_rn(dn, __fmul_rn(df, df));
+        }
+      if (dn > 1e-2f) {
+        const float gc = __fdiv_rn(4.0f, __fmul_rn(__fadd_rn(1.0f, __fmul_rn(0.25f, dn)), dn));
+#pragma unroll
+        for (int d = 0; d < MAXD; d++)
+          if (d < ncomp) {
+            const float step = __fmul_rn(clip4(__fmul_rn(gc, __fsub_rn(ej[d], en[d]))), alpha);
+            atomicAdd(&emb[j * ncomp + d], step);
+            ej[d] = __fadd_rn(ej[d], step);
+          }
+      }
+    }
+    eonn[i] = __fadd_rn(eonn[i], __fmul_rn(__ull2float_rn(nneg), rate));
+  }
+}
+
 __global__ void ne_apply_kernel(float* emb, const float* upd, const uint32_t* order, int64_t bs, int64_t be,
                                 uint64_t nv, int ncomp) {
   const int64_t total = (be - bs) * ncomp;
@@ -1541,14 +1619,15 @@ cudaError_t launch_pca_init(const float* x, int64_t n, int64_t d, int ncomp, flo
   return cudaGetLastError();
 }
 
-cudaError_t launch_ne_schedule(const float* w, int64_t m, int32_t n_epochs, float negative_sample_rate, float* eps,
-                               float* epns, float* eonn, float* eons, float* max_w, cudaStream_t s) {
+cudaError_t launch_ne_schedule(const float* w, int64_t m, int32_t n_epochs, float negative_sample_rate,
+                               float neg_scale, float* eps, float* epns, float* eonn, float* eons, float* max_w,
+                               cudaStream_t s) {
   cudaError_t e = cudaMemsetAsync(max_w, 0, 4, s);
   if (e != cudaSuccess || m == 0) return e;
   ne_maxw_kernel<<<grid_for(m, 256, 4096), 256, 0, s>>>(w, m, max_w);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  ne_schedule_kernel<<<grid_for(m, 256, 4096), 256, 0, s>>>(w, m, (float)n_epochs, negative_sample_rate, max_w, eps,
-                                                           epns, eonn, eons);
+  ne_schedule_kernel<<<grid_for(m, 256, 4096), 256, 0, s>>>(w, m, (float)n_epochs, negative_sample_rate, neg_scale,
+                                                           max_w, eps, epns, eonn, eons);
   return cudaGetLastError();
 }
 
@@ -1581,6 +1660,27 @@ cudaError_t launch_ne_block(const Csr& g, float* emb, float* upd, const uint32_t
   if (ncomp <= 8) return run(ne_block_kernel<8, 8>, ne_heavy_kernel<8, 2>);
   if (ncomp <= 16) return run(ne_block_kernel<16, 1>, ne_heavy_kernel<16, 1>);
   return run(ne_block_kernel<32, 1>, ne_heavy_kernel<32, 1>);
+}
+
+cudaError_t launch_edge_head(const int64_t* indptr, int64_t n, uint32_t* head, cudaStream_t s) {
+  edge_head_kernel<<<grid_for(n, 256, 4096), 256, 0, s>>>(indptr, n, head);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ne_hogwild(const Csr& g, const uint32_t* head, float* emb, const float* eps, const float* epns,
+                              float* eonn, float* eons, uint32_t rng_state, int ncomp, float alpha, uint8_t epoch,
+                              float noise, int sms, cudaStream_t s) {
+  const int grid = grid_for(g.nnz, 256, sms * 32);
+  if (ncomp <= 8)
+    ne_hogwild_kernel<8><<<grid, 256, 0, s>>>(g, head, emb, eps, epns, eonn, eons, rng_state, ncomp, alpha, epoch,
+                                              noise);
+  else if (ncomp <= 16)
+    ne_hogwild_kernel<16><<<grid, 256, 0, s>>>(g, head, emb, eps, epns, eonn, eons, rng_state, ncomp, alpha, epoch,
+                                               noise);
+  else
+    ne_hogwild_kernel<32><<<grid, 256, 0, s>>>(g, head, emb, eps, epns, eonn, eons, rng_state, ncomp, alpha, epoch,
+                                               noise);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_ne_apply(float* emb, const float* upd, const uint32_t* order, int64_t bs, int64_t be, int64_t nv,

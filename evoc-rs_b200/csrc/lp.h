@@ -123,9 +123,16 @@ cudaError_t launch_center_scale(const float* result, int64_t n, int ncomp, float
 cudaError_t launch_pca_init(const float* x, int64_t n, int64_t d, int ncomp, float* out, float* mean_ws,
                             double* vws, int32_t* status, cudaStream_t s);
 
-// node_embedding (reproducible): per-edge schedules.
-cudaError_t launch_ne_schedule(const float* w, int64_t m, int32_t n_epochs, float negative_sample_rate, float* eps,
-                               float* epns, float* eonn, float* eons, float* max_w, cudaStream_t s);
+// node_embedding: per-edge schedules (neg_scale 1.5 for the reproducible epochs, else 1).
+cudaError_t launch_ne_schedule(const float* w, int64_t m, int32_t n_epochs, float negative_sample_rate,
+                               float neg_scale, float* eps, float* epns, float* eonn, float* eons, float* max_w,
+                               cudaStream_t s);
+// Row of every edge (head[e], nnz entries).
+cudaError_t launch_edge_head(const int64_t* indptr, int64_t n, uint32_t* head, cudaStream_t s);
+// One non-reproducible epoch: every edge at once, updates by atomic adds.
+cudaError_t launch_ne_hogwild(const Csr& g, const uint32_t* head, float* emb, const float* eps, const float* epns,
+                              float* eonn, float* eons, uint32_t rng_state, int ncomp, float alpha, uint8_t epoch,
+                              float noise, int sms, cudaStream_t s);
 // One block of one epoch: nodes order[bs, be), rows of more than heavy_deg
 // edges by one CTA each (heavy_rows holds be - bs ids); then the apply launch.
 cudaError_t launch_ne_block(const Csr& g, float* emb, float* upd, const uint32_t* order, int64_t bs, int64_t be,

@@ -279,7 +279,7 @@ int node_embedding_dev(evoc_gpu_ctx* ctx, Arena& A, const lp::Csr& g, const floa
   EVOC_TRY(cudaMemsetAsync(upd, 0, size_t(n * ncomp) * 4, s), "memset updates");
   {
     Stage st(ctx, "epochs_per_sample");
-    EVOC_TRY(lp::launch_ne_schedule(weights, m, n_epochs, nsr, eps, epns, eonn, eons, maxw, s), "schedule");
+    EVOC_TRY(lp::launch_ne_schedule(weights, m, n_epochs, nsr, 1.5f, eps, epns, eonn, eons, maxw, s), "schedule");
     ctx->launches += 2;
   }
   std::vector<uint32_t> seeds(size_t(std::max(n_epochs, 0)));
@@ -337,6 +337,49 @@ int node_embedding_dev(evoc_gpu_ctx* ctx, Arena& A, const lp::Csr& g, const floa
   cleanup();
   if (rc) return rc;
   if (e != cudaSuccess) return cuda_fail(ctx, e, "node embedding");
+  return EVOC_OK;
+}
+
+// node_embedding(reproducible_flag = false) on a device graph: the epochs of
+// node_embedding_epoch (src/embed.rs:57-135) run lock-free on the device;
+// same RNG draws as the reference (epoch seeds; no shuffles).
+int node_embedding_hogwild_dev(evoc_gpu_ctx* ctx, Arena& A, const lp::Csr& g, int32_t ncomp, int32_t n_epochs,
+                               float* emb, bool have_init, float alpha0, float nsr, float noise, Mt& rng) {
+  cudaStream_t s = ctx->stream;
+  const int64_t n = g.n, m = g.nnz;
+  if (!have_init) {
+    std::vector<float> init(static_cast<size_t>(n * ncomp));
+    for (auto& v : init) v = float(0.25 * rng.normal());
+    EVOC_TRY(cudaMemcpyAsync(emb, init.data(), init.size() * 4, cudaMemcpyHostToDevice, s), "upload init");
+    EVOC_TRY(cudaStreamSynchronize(s), "upload init");
+  }
+  float *eps, *epns, *eonn, *eons, *maxw;
+  uint32_t* head;
+  EVOC_TRY(A.get(&eps, size_t(m)), "alloc schedule");
+  EVOC_TRY(A.get(&epns, size_t(m)), "alloc schedule");
+  EVOC_TRY(A.get(&eonn, size_t(m)), "alloc schedule");
+  EVOC_TRY(A.get(&eons, size_t(m)), "alloc schedule");
+  EVOC_TRY(A.get(&maxw, 1), "alloc");
+  EVOC_TRY(A.get(&head, size_t(m)), "alloc edge rows");
+  {
+    Stage st(ctx, "epochs_per_sample");
+    EVOC_TRY(lp::launch_ne_schedule(g.data, m, n_epochs, nsr, 1.0f, eps, epns, eonn, eons, maxw, s), "schedule");
+    EVOC_TRY(lp::launch_edge_head(g.indptr, n, head, s), "edge rows");
+    ctx->launches += 3;
+  }
+  std::vector<uint32_t> seeds(size_t(std::max(n_epochs, 0)));
+  for (auto& v : seeds) v = uint32_t(rng.randint(0, 2147483646LL));
+  float alpha = alpha0;
+  Stage st(ctx, "node_embedding_epochs");
+  for (int32_t ep = 0; ep < n_epochs; ep++) {
+    EVOC_TRY(lp::launch_ne_hogwild(g, head, emb, eps, epns, eonn, eons, seeds[size_t(ep)], ncomp, alpha, uint8_t(ep),
+                                   noise, ctx->sms, s),
+             "node embedding epoch");
+    ctx->launches += 1;
+    alpha = alpha0 * (1.0f - (float(ep) / float(n_epochs)));
+  }
+  st.end();
+  EVOC_TRY(cudaStreamSynchronize(s), "node embedding");
   return EVOC_OK;
 }
 
@@ -569,9 +612,6 @@ int node_embedding_impl(evoc_gpu_ctx* ctx, const int64_t* indptr, const int32_t*
   if (int rc = begin_call(ctx)) return rc;
   if (n <= 0) return fail(ctx, EVOC_ERR_EMPTY, "empty graph");
   if (!indptr || !rs || !out) return fail(ctx, EVOC_ERR_ARG, "null argument");
-  if (!reproducible)
-    return fail(ctx, EVOC_ERR_UNSUPPORTED,
-                "only the reproducible (block-synchronous) epoch is available; the other one is serial in-place SGD");
   if (ncomp < 1 || ncomp > lp::kMaxComponents) return fail(ctx, EVOC_ERR_UNSUPPORTED, "n_components must be 1..32");
   if (n_epochs < 0) return fail(ctx, EVOC_ERR_ARG, "negative n_epochs");
   if (n > (int64_t(1) << 31) - 1) return fail(ctx, EVOC_ERR_UNSUPPORTED, "2^31 or more vertices");
@@ -589,9 +629,11 @@ int node_embedding_impl(evoc_gpu_ctx* ctx, const int64_t* indptr, const int32_t*
       EVOC_TRY(cudaMemcpyAsync(d_out, initial, size_t(n) * size_t(ncomp) * 4,
                                on_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s),
                "initial embedding");
-    if (int rc = node_embedding_dev(ctx, A, g, g.data, ncomp, n_epochs, d_out, initial != nullptr, alpha0, nsr, noise,
-                                    rng))
-      return rc;
+    const int rc = reproducible ? node_embedding_dev(ctx, A, g, g.data, ncomp, n_epochs, d_out, initial != nullptr,
+                                                     alpha0, nsr, noise, rng)
+                                : node_embedding_hogwild_dev(ctx, A, g, ncomp, n_epochs, d_out, initial != nullptr,
+                                                             alpha0, nsr, noise, rng);
+    if (rc) return rc;
     if (!on_dev)
       EVOC_TRY(cudaMemcpyAsync(out, d_out, size_t(n) * size_t(ncomp) * 4, cudaMemcpyDeviceToHost, s), "download");
   }

@@ -138,14 +138,15 @@ def label_propagation_init_device(indptr_ptr: int, indices_ptr: int, data_ptr: i
 
 def node_embedding_device(indptr_ptr: int, indices_ptr: int, data_ptr: int, n: int, n_components: int,
                           n_epochs: int, init_ptr: int, out_ptr: int, random_state, initial_alpha: float = 0.1,
-                          negative_sample_rate: float = 1.0, noise_level: float = 0.5, device: int = 0):
-    """node_embedding (reproducible) on device buffers; init_ptr 0 draws the initial embedding."""
+                          negative_sample_rate: float = 1.0, noise_level: float = 0.5, device: int = 0,
+                          reproducible: bool = True):
+    """node_embedding on device buffers; init_ptr 0 draws the initial embedding."""
     rs = _state(random_state)
     r = _rng_in(rs)
     ctx = _lib.context(device)
     st = _lib.lib().evoc_gpu_node_embedding(
         ctx.h, P(indptr_ptr), P(indices_ptr), P(data_ptr), int(n), int(n_components), int(n_epochs),
         P(init_ptr) if init_ptr else None, float(initial_alpha), float(negative_sample_rate), float(noise_level),
-        C.byref(r), 1, 1, P(out_ptr))
+        C.byref(r), 1 if reproducible else 0, 1, P(out_ptr))
     _check(st, ctx)
     _rng_out(rs, r)

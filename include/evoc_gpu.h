@@ -232,12 +232,15 @@ int evoc_gpu_label_propagation_init(evoc_gpu_ctx* ctx, const int64_t* indptr, co
 
 /*
  * UMAP-like node embedding.  Replaces node_embedding (src/embed.rs:251-369)
- * and RlxBackend::node_embedding (src/rlx_backend/mod.rs:161-173) with
- * reproducible_flag = true: block-synchronous epochs
- * (node_embedding_epoch_repr, 138-248), bit-identical to the reference.
+ * and RlxBackend::node_embedding (src/rlx_backend/mod.rs:161-173).
+ *   reproducible = 1: block-synchronous epochs (node_embedding_epoch_repr,
+ *                  138-248), bit-identical to the reference
+ *   reproducible = 0: the non-reproducible epoch (node_embedding_epoch,
+ *                  57-135) with every edge of an epoch updating the rows at
+ *                  once (lock-free atomic adds, as Python's parallel version);
+ *                  same schedules and RNG draws as the reference, embedding
+ *                  equal in distribution, not bit for bit
  *   initial_embedding  n x n_components, or NULL for normal(0.25) draws
- *   reproducible       must be 1 (the other epoch is serial in-place SGD);
- *                      0 returns EVOC_ERR_UNSUPPORTED
  */
 int evoc_gpu_node_embedding(evoc_gpu_ctx* ctx, const int64_t* indptr, const int32_t* indices, const float* data,
                             int64_t n, int32_t n_components, int32_t n_epochs, const float* initial_embedding,

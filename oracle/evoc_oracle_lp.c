@@ -16,6 +16,7 @@
  *   make_epochs_per_sample .......... src/embed.rs:10-23
  *   node_embedding_epoch_repr ....... src/embed.rs:138-248
  *   node_embedding (reproducible) ... src/embed.rs:251-369
+ *   node_embedding_epoch ............ src/embed.rs:57-135 (non-reproducible: serial, in place)
  *   NumPy shuffle ................... src/numpy_rng.rs:136-141
  *
  * Compiled with -ffp-contract=off so every f32 expression rounds the way the
@@ -426,4 +427,85 @@ void orc_node_embedding_repr(int64_t nv, const int64_t *indptr64, const int32_t 
     free(order);
     free(seeds);
     free(updates);
+}
+
+/* node_embedding(reproducible_flag = false): epochs of in-place SGD over the
+ * edges in CSR order (src/embed.rs:57-135), no momentum, no shuffles.
+ * Optional outputs: the per-edge next-negative / next-sample epochs. */
+void orc_node_embedding_serial(int64_t nv, const int64_t *indptr64, const int32_t *indices, const float *w,
+                               int32_t ncomp, int32_t n_epochs, float *emb, int32_t have_init, float initial_alpha,
+                               float negative_sample_rate, float noise, orc_mt *rng, float *eonn_out,
+                               float *eons_out) {
+    if (!have_init)
+        for (int64_t i = 0; i < nv * ncomp; i++) emb[i] = (float)(0.25 * orc_mt_normal(rng));
+    int64_t m = indptr64[nv];
+    float *eps = (float *)malloc(sizeof(float) * (size_t)(m + 1));
+    float *epns = (float *)malloc(sizeof(float) * (size_t)(m + 1));
+    float *eonn = (float *)malloc(sizeof(float) * (size_t)(m + 1));
+    float *eons = (float *)malloc(sizeof(float) * (size_t)(m + 1));
+    uint32_t *head = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)(m + 1));
+    uint32_t *seeds = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)(n_epochs + 1));
+    orc_make_epochs_per_sample(w, m, n_epochs, eps);
+    for (int64_t r = 0; r < nv; r++)
+        for (int64_t e = indptr64[r]; e < indptr64[r + 1]; e++) head[e] = (uint32_t)r;
+    for (int64_t e = 0; e < m; e++) {
+        epns[e] = eps[e] / negative_sample_rate;
+        eonn[e] = epns[e];
+        eons[e] = eps[e];
+    }
+    int32_t dim = ncomp < 255 ? ncomp : 255;
+    float alpha = initial_alpha;
+    for (int32_t e = 0; e < n_epochs; e++) seeds[e] = (uint32_t)orc_mt_randint(rng, 0, 2147483646);
+    for (int32_t ep = 0; ep < n_epochs; ep++) {
+        float nf = (float)(uint8_t)ep;
+        uint64_t n8 = (uint8_t)ep;
+        for (int64_t i = 0; i < m; i++) {
+            if (eons[i] > nf) continue;
+            uint64_t j = head[i], k = (uint32_t)indices[i];
+            if (j >= (uint64_t)nv || k >= (uint64_t)nv) continue;
+            float *ej = emb + j * ncomp, *ek = emb + k * ncomp;
+            float ds = 0.0f;
+            for (int d = 0; d < dim; d++) {
+                float df = ej[d] - ek[d];
+                ds += df * df;
+            }
+            if (ds > 0.0f) {
+                float dist = sqrtf(ds);
+                float gc = (-2.0f * noise * dist - 2.0f) / (2.0f * ds - 0.5f * dist + 1.0f);
+                for (int d = 0; d < dim; d++) {
+                    float g = gc * (ej[d] - ek[d]);
+                    ej[d] += g * alpha;
+                    ek[d] -= g * alpha;
+                }
+            }
+            eons[i] += eps[i];
+            uint64_t nneg = neg_count(nf, eonn[i], epns[i]);
+            for (uint64_t p = 0; p < nneg; p++) {
+                uint64_t nk = ((n8 + p) * (uint64_t)i * (uint64_t)seeds[ep]) % (uint64_t)nv;
+                float *en = emb + nk * ncomp;
+                float dn = 0.0f;
+                for (int d = 0; d < dim; d++) {
+                    float df = ej[d] - en[d];
+                    dn += df * df;
+                }
+                if (dn > 1e-2f) {
+                    float gc = 4.0f / ((1.0f + 0.25f * dn) * dn);
+                    for (int d = 0; d < dim; d++) {
+                        float g = clip4(gc * (ej[d] - en[d]));
+                        ej[d] += g * alpha;
+                    }
+                }
+            }
+            eonn[i] += (float)nneg * epns[i];
+        }
+        alpha = initial_alpha * (1.0f - ((float)ep / (float)n_epochs));
+    }
+    if (eonn_out) memcpy(eonn_out, eonn, sizeof(float) * (size_t)m);
+    if (eons_out) memcpy(eons_out, eons, sizeof(float) * (size_t)m);
+    free(eps);
+    free(epns);
+    free(eonn);
+    free(eons);
+    free(head);
+    free(seeds);
 }

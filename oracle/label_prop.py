@@ -35,6 +35,7 @@ def _lib():
         L.orc_csr_dense.argtypes = [i64, P, P, P, P, i64, P]
         L.orc_make_epochs_per_sample.argtypes = [P, i64, i32, P]
         L.orc_seg_sum_f32.argtypes = [P, P, i64, i64, P]
+        L.orc_node_embedding_serial.argtypes = [i64, P, P, P, i32, i32, P, i32, f32, f32, f32, C.POINTER(O.MT), P, P]
         L.orc_node_embedding_repr.argtypes = [i64, P, P, P, i32, i32, P, i32, f32, f32, f32, C.POINTER(O.MT), i32, P,
                                               P, P]
         _ready = True
@@ -222,6 +223,22 @@ def node_embedding(g: Csr, n_components: int, n_epochs: int, init, initial_alpha
                                    1 if have else 0, initial_alpha, negative_sample_rate, noise_level,
                                    C.byref(rng.s), n_run, _p(upd), _p(eonn), _p(eons))
     return (emb, upd, eonn, eons) if state else emb
+
+
+def node_embedding_serial(g: Csr, n_components: int, n_epochs: int, init, initial_alpha: float,
+                          negative_sample_rate: float, noise_level: float, rng: O.RandomState, *,
+                          state: bool = False):
+    """node_embedding(reproducible_flag=false): in-place SGD in edge order, src/embed.rs:57-135,251-369.
+    state=True also returns (epoch_of_next_negative_sample, epoch_of_next_sample)."""
+    n = g.shape[0]
+    have = init is not None
+    emb = np.array(init, np.float32, copy=True, order="C") if have else np.empty((n, n_components), np.float32)
+    eonn = np.empty(g.nnz, np.float32)
+    eons = np.empty(g.nnz, np.float32)
+    _lib().orc_node_embedding_serial(n, _p(g.indptr), _p(g.indices), _p(g.data), n_components, n_epochs, _p(emb),
+                                     1 if have else 0, initial_alpha, negative_sample_rate, noise_level,
+                                     C.byref(rng.s), _p(eonn), _p(eons))
+    return (emb, eonn, eons) if state else emb
 
 
 def _normalize_small_init(r: np.ndarray) -> np.ndarray:
