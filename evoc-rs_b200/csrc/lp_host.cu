@@ -33,13 +33,20 @@ namespace lp = evoc::lp;
 struct Mt {
   evoc_numpy_rng* s;
 
+  // The 624-word state update, in place: words 0..226 mix with the old words
+  // 397 ahead, words 227..622 with the new words 227 behind, word 623 with
+  // the new word 396 (split so no index needs a modulo).
   void regen() {
     constexpr uint32_t kUp = 0x80000000u, kLo = 0x7fffffffu, kA = 0x9908b0dfu;
     uint32_t* k = s->key;
-    for (int i = 0; i < 624; i++) {
-      const uint32_t y = (k[i] & kUp) | (k[(i + 1) % 624] & kLo);
-      k[i] = k[(i + 397) % 624] ^ (y >> 1) ^ ((y & 1u) ? kA : 0u);
-    }
+    auto mix = [&](int i, uint32_t next, uint32_t far) {
+      const uint32_t y = (k[i] & kUp) | (next & kLo);
+      k[i] = far ^ (y >> 1) ^ ((0u - (y & 1u)) & kA);
+    };
+    int i = 0;
+    for (; i < 227; i++) mix(i, k[i + 1], k[i + 397]);
+    for (; i < 623; i++) mix(i, k[i + 1], k[i - 227]);
+    mix(623, k[0], k[396]);
     s->pos = 0;
   }
   uint32_t next() {

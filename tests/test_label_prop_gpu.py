@@ -265,3 +265,35 @@ def test_node_embedding_non_reproducible(blob_graph):
     assert np.isfinite(emb).all()
     got_rate, want_rate = _knn_label_rate(emb, labels), _knn_label_rate(want, labels)
     assert got_rate >= want_rate - 0.03 and got_rate > 0.8, (got_rate, want_rate)
+
+
+def test_label_propagation_init_small_graph_and_wide_components():
+    """Fewer than 64 vertices: the PCA base init directly; 20 components takes the 32-wide kernels."""
+    rng = np.random.default_rng(6)
+    x = rng.normal(size=(50, 12)).astype(np.float32)
+    g = _hub_graph(n=50, hubs=1, hub_deg=30, seed=6)
+    rs = np.random.RandomState(4)
+    orng = _oracle_rng(rs)
+    init = evoc.label_propagation_init(_tuple(g), 20, 10, 256, 5, 0.5, 0.1, 0.5, rs, x)
+    want = L.label_propagation_init(g, 20, 10, 256, 5, 0.5, 0.1, 0.5, orng, x)
+    assert np.abs(init - want).max() <= 1e-4
+    assert _same_state(rs, orng)  # no draws below the threshold
+    g2 = _hub_graph(n=3000, hubs=2, hub_deg=800, seed=9)
+    x2 = rng.normal(size=(3000, 16)).astype(np.float32)
+    rs = np.random.RandomState(5)
+    orng = _oracle_rng(rs)
+    init = evoc.label_propagation_init(_tuple(g2), 20, 10, 400, 20, 0.5, 0.1, 0.5, rs, x2)
+    want = L.label_propagation_init(g2, 20, 10, 400, 20, 0.5, 0.1, 0.5, orng, x2)
+    assert init.shape == (3000, 20) and np.abs(init - want).max() <= 1e-4
+    assert _same_state(rs, orng)
+
+
+def test_label_propagation_limits_are_errors():
+    # 100,000 seeds on 300,000 vertices leave ~85,000 distinct parts: above the 65,536 the
+    # reduction's sort keys hold (the reference's own call clamps approx_n_parts to 16,384)
+    g = _hub_graph(n=300000, hubs=1, hub_deg=100, seed=2)
+    x = np.zeros((300000, 4), np.float32)
+    with pytest.raises(evoc.BackendError):
+        evoc.label_propagation_init(_tuple(g), 20, 5, 100000, 4, 0.5, 0.1, 0.5, np.random.RandomState(1), x)
+    with pytest.raises(evoc.BackendError):  # components above 32
+        evoc.label_propagation_init(_tuple(g), 20, 5, 300, 40, 0.5, 0.1, 0.5, np.random.RandomState(1), x)
