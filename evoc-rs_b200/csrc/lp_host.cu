@@ -126,7 +126,12 @@ struct Arena {
 
 constexpr int64_t kBaseInitThreshold = 64;  // src/label_prop.rs:507 default
 constexpr int32_t kMaxParts = 65536;        // parts fit the 16-bit fields of the sort keys
-constexpr int64_t kHeavyDegree = 512;       // embedding rows above this many edges get a CTA each
+// Embedding rows above this many edges get a CTA each.  A block of few nodes
+// (every node on its own warp) lasts as long as its longest row, so there the
+// threshold is lower; a block of many nodes is bound by throughput instead.
+constexpr int64_t kHeavyDegree = 512;
+constexpr int64_t kHeavyDegreeSmallBlock = 128;
+constexpr int64_t kSmallBlock = 32768;
 
 struct Level {
   int32_t n_iter, n_epochs, ncomp;
@@ -326,7 +331,8 @@ int node_embedding_dev(evoc_gpu_ctx* ctx, Arena& A, const lp::Csr& g, const floa
       const int64_t be = std::min(n, bs + block);
       e = lp::launch_ne_block(g, emb, upd, d_order + size_t(slot) * n, bs, be, eps, epns, eonn, eons,
                               seeds[size_t(ep)], ncomp, alpha, uint8_t(ep), noise, gamma, decay, ep > 0 ? 1 : 0,
-                              kHeavyDegree, heavy_rows, heavy_count, ctx->sms, s);
+                              be - bs < kSmallBlock ? kHeavyDegreeSmallBlock : kHeavyDegree, heavy_rows,
+                              heavy_count, ctx->sms, s);
       if (e == cudaSuccess) e = lp::launch_ne_apply(emb, upd, d_order + size_t(slot) * n, bs, be, n, ncomp, s);
       ctx->launches += 3;
     }
