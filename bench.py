@@ -42,6 +42,8 @@ import sys
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
+# where the raw clock samples go (the JSON line carries their summary)
+OUT_DIR = os.environ.get("EVOC_BENCH_OUT", os.path.join(ROOT, "bench_out"))
 sys.path.insert(0, os.path.join(ROOT, "evoc-rs_b200"))
 sys.path.insert(0, ROOT)
 
@@ -530,8 +532,8 @@ def run_exact_int(args, world, rank, local):
     for _ in range(args.warmup):
         step()
     gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
-    os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
-    clocks = ClockSampler(gpu_id, os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv"))
+    os.makedirs(OUT_DIR, exist_ok=True)
+    clocks = ClockSampler(gpu_id, os.path.join(OUT_DIR, f"clocks_rank{rank}.csv"))
     if pg:
         pg.barrier()
     torch.cuda.synchronize()
@@ -770,8 +772,8 @@ def run_ours(args, world, rank, local):
     for _ in range(args.warmup):
         step()
     gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
-    os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
-    clocks = ClockSampler(gpu_id, os.path.join(ROOT, "gpurun_out", f"clocks_rank{rank}.csv"))
+    os.makedirs(OUT_DIR, exist_ok=True)
+    clocks = ClockSampler(gpu_id, os.path.join(OUT_DIR, f"clocks_rank{rank}.csv"))
     if pg:
         pg.barrier()
     torch.cuda.synchronize()

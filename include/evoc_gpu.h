@@ -34,8 +34,8 @@ typedef enum {
   EVOC_ERR_PENDING = 9      /* serving: job has not finished            */
 } evoc_status;
 
-/* EmbeddingData variants (src/knn.rs:16-20).  BINARY is the name README and
- * the north star use for the UInt8 (packed bits, Jaccard) variant. */
+/* EmbeddingData variants (src/knn.rs:16-20).  BINARY is the name the
+ * reference's README uses for the UInt8 (packed bits, Jaccard) variant. */
 typedef enum {
   EVOC_DTYPE_F32 = 0,
   EVOC_DTYPE_I8 = 1,

@@ -1,4 +1,4 @@
-"""GPU NN-descent form (EVOC_FORM_NNDESCENT), judged by recall.
+"""GPU NN-descent form (EVOC_FORM_NNDESCENT), checked by recall.
 
 The reference's kNN is NN-descent (src/nndescent/*.rs); the GPU form is an
 NN-descent too, so it is held to recall@k against exact neighbours (FP64 for
