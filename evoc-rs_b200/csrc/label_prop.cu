@@ -309,8 +309,8 @@ __global__ void outlier_walk_big_kernel(Csr g, const int32_t* labels, const int6
 
 // Copied labels by pointer jumping over the unlabelled rows (pointers go to
 // earlier rows, so the chains end): nxt = -1 marks a row whose label is known.
-__global__ void outlier_resolve_init_kernel(const WalkOut* out, const int32_t* count, const int32_t* rows,
-                                            int32_t* oidx, int32_t* lab, int32_t* nxt) {
+// First, each unlabelled row's position in the list.
+__global__ void outlier_index_kernel(const int32_t* count, const int32_t* rows, int32_t* oidx) {
   const int32_t cnt = *count;
   for (int64_t oi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; oi < cnt; oi += (int64_t)gridDim.x * blockDim.x)
     oidx[rows[oi]] = (int32_t)oi;
@@ -1400,7 +1400,7 @@ cudaError_t run_lp_outliers(const Csr& g, int32_t* labels, const int64_t* rs, co
                                            64 * max_deg + 1, out, w.status);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   const int grid = grid_for(cnt, 256, 4096);
-  outlier_resolve_init_kernel<<<grid, 256, 0, s>>>(out, w.count, w.rows, w.oidx, w.lab[0], w.nxt[0]);
+  outlier_index_kernel<<<grid, 256, 0, s>>>(w.count, w.rows, w.oidx);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   outlier_resolve_start_kernel<<<grid, 256, 0, s>>>(out, w.count, w.oidx, w.lab[0], w.nxt[0]);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;

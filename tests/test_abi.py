@@ -58,6 +58,7 @@ def test_struct_layouts_match_the_header(tmp_path):
         "evoc_gpu_server_opts": _lib.ServerOpts,
         "evoc_gpu_server_counters": _lib.ServerCounters,
         "evoc_gpu_job_info": _lib.JobInfo,
+        "evoc_numpy_rng": _lib.NumpyRng,
     }
     src = ["#include <stdio.h>", "#include <stddef.h>", f'#include "{_lib.HEADER_PATH}"', "int main(void) {"]
     for name, cls in fields.items():
