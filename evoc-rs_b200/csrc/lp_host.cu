@@ -32,6 +32,8 @@ namespace lp = evoc::lp;
 
 struct Mt {
   evoc_numpy_rng* s;
+  uint32_t tempered[624];  // outputs of the current key block, tempered once per block
+  bool ready;
 
   // The 624-word state update, in place: words 0..226 mix with the old words
   // 397 ahead, words 227..622 with the new words 227 behind, word 623 with
@@ -49,14 +51,25 @@ struct Mt {
     mix(623, k[0], k[396]);
     s->pos = 0;
   }
+  void temper_block() {
+    for (int i = 0; i < 624; i++) {
+      uint32_t y = s->key[i];
+      y ^= y >> 11;
+      y ^= (y << 7) & 0x9d2c5680u;
+      y ^= (y << 15) & 0xefc60000u;
+      y ^= y >> 18;
+      tempered[i] = y;
+    }
+    ready = true;
+  }
   uint32_t next() {
-    if (s->pos >= 624) regen();
-    uint32_t y = s->key[s->pos++];
-    y ^= y >> 11;
-    y ^= (y << 7) & 0x9d2c5680u;
-    y ^= (y << 15) & 0xefc60000u;
-    y ^= y >> 18;
-    return y;
+    if (s->pos >= 624) {
+      regen();
+      temper_block();
+    } else if (!ready) {
+      temper_block();
+    }
+    return tempered[s->pos++];
   }
   // Masked rejection on 32-bit draws (ranges here stay below 2^32).
   uint64_t interval(uint64_t max) {
@@ -98,8 +111,31 @@ struct Mt {
   void tau_seed(int64_t out[3]) {
     for (int j = 0; j < 3; j++) out[j] = randint(-2147483647LL, 2147483646LL);
   }
+  // shuffle: for i = n-1 .. 1 swap a[i] with a[randint(0, i + 1)] -- the
+  // draws of interval() inlined (n < 2^32 here, so 32-bit masks).
   void shuffle(uint32_t* a, int64_t n) {
-    for (int64_t i = n - 1; i >= 1; i--) std::swap(a[i], a[randint(0, i + 1)]);
+    if (!ready && s->pos < 624) temper_block();
+    int pos = s->pos;
+    for (int64_t i = n - 1; i >= 1; i--) {
+      const uint32_t mx = uint32_t(i);
+      uint32_t m = mx;
+      m |= m >> 1;
+      m |= m >> 2;
+      m |= m >> 4;
+      m |= m >> 8;
+      m |= m >> 16;
+      uint32_t v;
+      do {
+        if (pos >= 624) {
+          regen();
+          temper_block();
+          pos = 0;
+        }
+        v = tempered[pos++] & m;
+      } while (v > mx);
+      std::swap(a[i], a[v]);
+    }
+    s->pos = pos;
   }
 };
 
@@ -578,7 +614,7 @@ int label_propagation_init_impl(evoc_gpu_ctx* ctx, const int64_t* indptr, const 
   if (x && dim <= 0) return fail(ctx, EVOC_ERR_ARG, "data dimension must be positive");
   if (n_iter < 0 || n_epochs < 0 || approx < 0) return fail(ctx, EVOC_ERR_ARG, "negative count");
   cudaStream_t s = ctx->stream;
-  Mt rng{rs};
+  Mt rng{rs, {}, false};
   Stage total(ctx, "total");
   int rc;
   {
@@ -629,7 +665,7 @@ int node_embedding_impl(evoc_gpu_ctx* ctx, const int64_t* indptr, const int32_t*
   if (n_epochs < 0) return fail(ctx, EVOC_ERR_ARG, "negative n_epochs");
   if (n > (int64_t(1) << 31) - 1) return fail(ctx, EVOC_ERR_UNSUPPORTED, "2^31 or more vertices");
   cudaStream_t s = ctx->stream;
-  Mt rng{rs};
+  Mt rng{rs, {}, false};
   Stage total(ctx, "total");
   {
     Arena A(ctx);
@@ -663,7 +699,7 @@ int label_prop_loop_impl(evoc_gpu_ctx* ctx, const int64_t* indptr, const int32_t
   if (n_iter < 0 || approx < 0) return fail(ctx, EVOC_ERR_ARG, "negative count");
   if (approx > (int64_t(1) << 31) - 1) return fail(ctx, EVOC_ERR_UNSUPPORTED, "approx_n_parts above 2^31 - 1");
   cudaStream_t s = ctx->stream;
-  Mt rng{rs};
+  Mt rng{rs, {}, false};
   Stage total(ctx, "total");
   {
     Arena A(ctx);
