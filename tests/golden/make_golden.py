@@ -18,7 +18,9 @@ lp_<fixture>.npz carries the label-propagation and node-embedding goldens
 intermediates): per-iteration labels, the partition, the reduced data/graph,
 init and layout, the final init_embedding and embedding, NumPy RNG states
 between the stages, and (large_2000) the reference's own Rust node orders and
-embedding state after 20 reproducible epochs (rust_*_after19.npy).
+embedding state after 20 reproducible epochs (rust_*_after19.npy); and
+(medium_800) the KD-tree index order, core distances and Borůvka MST edges
+Python computed on its final embedding.
 """
 import json
 import os
@@ -69,7 +71,7 @@ LP_ARRAYS = ["labels_seeded", "labels_iter0", "labels_iter1", "labels_iter2", "l
              "labels_iter19", "labels_after_outliers", "partition", "reduced_data", "reduced_init", "reduced_layout",
              "pre_scale_result", "init_embedding", "embedding", "rust_emb_after19", "rust_updates_after19",
              "rust_eon_after19", "rust_eos_after19", "rust_node_order_000", "rust_node_order_012",
-             "rust_node_order_024"]
+             "rust_node_order_024", "py_kdtree_idx_array", "py_core_distances", "py_boruvka_edges"]
 LP_CSR = ["graph_csr", "reduced_graph_csr", "temp_norm_t_graph"]
 LP_RNG = ["after_knn", "after_partition", "after_reduced_init", "after_init", "after_emb"]
 
