@@ -108,6 +108,12 @@ def _bind_optional(L) -> None:
                                                       C.POINTER(NumpyRng), P, i64, i32, P]
         L.evoc_gpu_node_embedding.argtypes = [P, P, P, P, i64, i32, i32, P, f32, f32, f32, C.POINTER(NumpyRng),
                                               i32, i32, P]
+    if hasattr(L, "evoc_npy_open"):
+        L.evoc_npy_open.argtypes = [C.c_char_p, C.POINTER(NpyArray)]
+        L.evoc_npz_open.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(NpyArray)]
+        L.evoc_npy_close.argtypes = [C.POINTER(NpyArray)]
+        L.evoc_npy_close.restype = None
+        L.evoc_graph_npz_read.argtypes = [C.c_char_p, C.POINTER(i64), C.POINTER(i64), P, P, P, i64]
     if hasattr(L, "evoc_gpu_server_create"):
         L.evoc_gpu_server_default_opts.argtypes = [C.POINTER(ServerOpts)]
         L.evoc_gpu_server_create.argtypes = [C.POINTER(ServerOpts), C.POINTER(P)]
@@ -135,6 +141,13 @@ class NumpyRng(C.Structure):
     """evoc_numpy_rng: the fields of numpy.random.RandomState.get_state()."""
 
     _fields_ = [("key", C.c_uint32 * 624), ("pos", C.c_int32), ("has_gauss", C.c_int32), ("gauss", C.c_double)]
+
+
+class NpyArray(C.Structure):
+    """evoc_npy_array."""
+
+    _fields_ = [("data", C.c_void_p), ("nbytes", C.c_int64), ("shape", C.c_int64 * 8), ("ndim", C.c_int32),
+                ("dtype", C.c_int32), ("fortran_order", C.c_int32), ("reserved", C.c_int32), ("handle", C.c_void_p)]
 
 
 class ServerOpts(C.Structure):

@@ -247,6 +247,57 @@ int evoc_gpu_node_embedding(evoc_gpu_ctx* ctx, const int64_t* indptr, const int3
                             float initial_alpha, float negative_sample_rate, float noise_level, evoc_numpy_rng* rng,
                             int32_t reproducible, int32_t buffers_on_device, float* out);
 
+/*
+ * .npy / .npz ingestion.  The reference reads its data sets, graphs and RNG
+ * states with ndarray_npy (src/graph_construction.rs:117-154,
+ * src/clustering.rs:350-356, src/numpy_rng.rs:170-193).  Here an array is
+ * read in place from a read-only mapping of the file: `data` points into the
+ * mapping (stored .npz members too), so rows can go straight to
+ * evoc_gpu_knn_graph or a server submit (EVOC_SUBMIT_BORROW) without a
+ * host-side copy; a deflated .npz member is inflated into a buffer the handle
+ * owns.  Little-endian f4/f8/i1/u1/i4/i8/u4/b1 arrays, .npy versions 1-3, ZIP
+ * and ZIP64 archives.  Release with evoc_npy_close.
+ */
+typedef enum {
+  EVOC_NPY_F32 = 0,
+  EVOC_NPY_F64 = 1,
+  EVOC_NPY_I8 = 2,
+  EVOC_NPY_U8 = 3,
+  EVOC_NPY_I32 = 4,
+  EVOC_NPY_I64 = 5,
+  EVOC_NPY_U32 = 6,
+  EVOC_NPY_BOOL = 7
+} evoc_npy_dtype;
+
+typedef struct {
+  const void* data;      /* first element                                  */
+  int64_t nbytes;        /* bytes of array data                            */
+  int64_t shape[8];
+  int32_t ndim;
+  int32_t dtype;         /* evoc_npy_dtype                                 */
+  int32_t fortran_order; /* 1: column-major                                */
+  int32_t reserved;
+  void* handle;          /* the mapping / buffer; owned by the library     */
+} evoc_npy_array;
+
+/* EVOC_ERR_ARG: unreadable file, bad header, missing member;
+ * EVOC_ERR_UNSUPPORTED: dtype or format version not listed above. */
+int evoc_npy_open(const char* path, evoc_npy_array* out);
+int evoc_npz_open(const char* path, const char* name, evoc_npy_array* out); /* name with or without ".npy" */
+void evoc_npy_close(evoc_npy_array* a);
+
+/*
+ * A graph .npz in the reference's layouts: CSR (indptr, indices, data, shape;
+ * load_graph_csr_npz, src/graph_construction.rs:133-154) or COO (rows, cols,
+ * data, shape; load_graph_coo_npz, 117-131), returned as CSR.  COO entries
+ * are sorted by (row, column) and entries with the same position summed in
+ * file order (TriMat::to_csr); CSR is copied as stored.  With indptr == NULL
+ * only *n and *nnz are set (a size query); otherwise indptr holds n + 1,
+ * indices / data `cap` entries (EVOC_ERR_ARG when cap < *nnz).
+ */
+int evoc_graph_npz_read(const char* path, int64_t* n, int64_t* nnz, int64_t* indptr, int32_t* indices, float* data,
+                        int64_t cap);
+
 /* The context's CUDA stream (a cudaStream_t), for callers that record their
  * own CUDA events around calls.  No counterpart in evoc-rs. */
 void* evoc_gpu_ctx_stream(const evoc_gpu_ctx* ctx);

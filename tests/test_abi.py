@@ -59,6 +59,7 @@ def test_struct_layouts_match_the_header(tmp_path):
         "evoc_gpu_server_counters": _lib.ServerCounters,
         "evoc_gpu_job_info": _lib.JobInfo,
         "evoc_numpy_rng": _lib.NumpyRng,
+        "evoc_npy_array": _lib.NpyArray,
     }
     src = ["#include <stdio.h>", "#include <stddef.h>", f'#include "{_lib.HEADER_PATH}"', "int main(void) {"]
     for name, cls in fields.items():
