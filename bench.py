@@ -659,7 +659,7 @@ def run_label_prop(args, dev, ctx, stream, x, f_indptr, f_ind, f_dat, nnz, opts)
         return st, ctx.launches()
 
     lp_once()
-    runs = [lp_once() for _ in range(3)]
+    runs = [lp_once() for _ in range(max(1, args.lp_reps))]
     lp_ms = statistics.median(r[0]["total"] for r in runs)
     stages = {nm: statistics.median(r[0][nm] for r in runs) for nm in runs[0][0] if nm != "total"}
 
@@ -668,16 +668,19 @@ def run_label_prop(args, dev, ctx, stream, x, f_indptr, f_ind, f_dat, nnz, opts)
                                  out.data_ptr(), emb.data_ptr(), np.random.RandomState(43))
         return dict(ctx.stages())
 
-    ne_once()
-    ne_ms = statistics.median(ne_once()["total"] for _ in range(2))
+    ne_ms = ne_free_ms = float("nan")
+    if args.ne_reps > 0:
+        ne_once()
+        ne_ms = statistics.median(ne_once()["total"] for _ in range(args.ne_reps))
 
     def ne_free_once():
         LP.node_embedding_device(f_indptr.data_ptr(), f_ind.data_ptr(), f_dat.data_ptr(), n, ncomp, 50,
                                  out.data_ptr(), emb.data_ptr(), np.random.RandomState(43), reproducible=False)
         return dict(ctx.stages())
 
-    ne_free_once()
-    ne_free_ms = statistics.median(ne_free_once()["total"] for _ in range(2))
+    if args.ne_reps > 0:
+        ne_free_once()
+        ne_free_ms = statistics.median(ne_free_once()["total"] for _ in range(args.ne_reps))
     # effective bandwidth of the full-graph epochs: per edge the five f32 schedule words (three read,
     # two written) and the column index, plus one embedding row gathered
     ne_bytes = 50 * nnz * (6 * 4 + ncomp * 4)
@@ -976,6 +979,8 @@ def main():
     ap.add_argument("--fuzzy", type=int, default=1, help="time the fuzzy graph of the built graph")
     ap.add_argument("--label-prop", type=int, default=1,
                     help="time label_propagation_init and the node embedding on the fuzzy graph")
+    ap.add_argument("--lp-reps", type=int, default=3, help="timed label_propagation_init calls")
+    ap.add_argument("--ne-reps", type=int, default=2, help="timed node_embedding calls of each kind (0: none)")
     ap.add_argument("--cpu-lp-rows", type=int, default=100000,
                     help="rows of the graph the oracle's label_propagation_init is timed on")
     ap.add_argument("--e2e-steps", type=int, default=3)
