@@ -63,8 +63,7 @@ WORKLOADS = {
 # DRAM bytes (read + write) of one launch of the BF16 scan: 5.826e9 B captured
 # with ncu (dram__bytes_read.sum + dram__bytes_write.sum) at n = 262,144, scaled
 # by the number of (query, key) pairs to n = 1,000,000 (the key rows are
-# re-streamed once per wave of query blocks, so traffic grows with n^2); see
-# profiles/tc_scan_bf16_zipf_1m_768.md.
+# re-streamed once per wave of query blocks, so traffic grows with n^2).
 SCAN_TRAFFIC_BYTES_262K = 5_825_927_424
 
 

@@ -15,6 +15,7 @@
 // between them) corrupt each other's results; calls on one stream are
 // ordered and safe.  No part of the array needs to start at zero: each
 // launch writes every candidate slot before it reads it.
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -65,6 +66,11 @@ extern "C" int evoc_gpu_knn_f32_noalloc(const float* rows, int64_t n, int64_t ld
   }
   if (n >= (int64_t(1) << 31) - 1) {
     set_err(errbuf, errlen, "n exceeds the int32 index range");
+    return EVOC_ERR_ARG;
+  }
+  // The kernel takes the stride as an int and indexes rows as int64 row * ld.
+  if (ld > INT32_MAX || n > INT64_MAX / ld) {
+    set_err(errbuf, errlen, "row stride (ld) exceeds the int32 range, or n * ld exceeds the int64 range");
     return EVOC_ERR_ARG;
   }
   int64_t kk = k < n - 1 ? k : n - 1;

@@ -137,11 +137,17 @@ int parse_npy(const uint8_t* p, size_t len, evoc_npy_array* out) {
     const long long v = std::strtoll(inner.c_str() + i, &end, 10);
     if (end == inner.c_str() + i || v < 0 || ndim >= 8) return EVOC_ERR_ARG;
     out->shape[ndim++] = v;
-    count *= v;
+    // A shape whose element count or byte size overflows 64 bits cannot
+    // describe the file: reject it before the size check below can wrap.
+    int64_t next = 0;
+    if (__builtin_mul_overflow(count, int64_t(v), &next)) return EVOC_ERR_ARG;
+    count = next;
     i = size_t(end - inner.c_str());
   }
-  const size_t bytes = size_t(count) * size_t(itemsize);
-  if (off + hlen + bytes > len) return EVOC_ERR_ARG;
+  int64_t nbytes = 0;
+  if (__builtin_mul_overflow(count, itemsize, &nbytes)) return EVOC_ERR_ARG;
+  const size_t bytes = size_t(nbytes);
+  if (off + hlen > len || bytes > len - (off + hlen)) return EVOC_ERR_ARG;
   out->ndim = ndim;
   out->dtype = code;
   out->fortran_order = fortran.find("True") != std::string::npos ? 1 : 0;
@@ -167,22 +173,24 @@ int zip_member(const Mapping& m, const char* name, const uint8_t** data, size_t*
   uint64_t entries = rd16(p + eocd + 10), cd_off = rd32(p + eocd + 16);
   if (eocd >= 20 && rd32(p + eocd - 20) == 0x07064b50u) {  // ZIP64 end-of-directory locator
     const uint64_t z = rd64(p + eocd - 20 + 8);
-    if (z + 56 > n || rd32(p + z) != 0x06064b50u) return EVOC_ERR_ARG;
+    if (z > n || n - z < 56 || rd32(p + z) != 0x06064b50u) return EVOC_ERR_ARG;
     entries = rd64(p + z + 32);
     cd_off = rd64(p + z + 48);
   }
   const std::string want(name), want_npy = want + ".npy";
   uint64_t at = cd_off;
   for (uint64_t e = 0; e < entries; e++) {
-    if (at + 46 > n || rd32(p + at) != 0x02014b50u) return EVOC_ERR_ARG;
+    if (at > n || n - at < 46 || rd32(p + at) != 0x02014b50u) return EVOC_ERR_ARG;
     const uint16_t method = rd16(p + at + 10), nlen = rd16(p + at + 28), xlen = rd16(p + at + 30),
                    clen = rd16(p + at + 32);
     uint64_t csize = rd32(p + at + 20), usize = rd32(p + at + 24), loff = rd32(p + at + 42);
     if (at + 46 + nlen + xlen > n) return EVOC_ERR_ARG;
     const std::string nm(reinterpret_cast<const char*>(p + at + 46), nlen);
     // ZIP64 extra field: the 64-bit values of the fields stored as 0xFFFFFFFF, in this order
-    for (uint64_t x = at + 46 + nlen; x + 4 <= at + 46 + nlen + xlen;) {
+    const uint64_t x_end = at + 46 + nlen + xlen;  // within the file (checked above)
+    for (uint64_t x = at + 46 + nlen; x + 4 <= x_end;) {
       const uint16_t id = rd16(p + x), sz = rd16(p + x + 2);
+      if (sz > x_end - (x + 4)) return EVOC_ERR_ARG;  // a field running past the extra region
       if (id == 0x0001) {
         uint64_t y = x + 4;
         if (usize == 0xFFFFFFFFu && y + 8 <= x + 4 + sz) usize = rd64(p + y), y += 8;
@@ -192,15 +200,18 @@ int zip_member(const Mapping& m, const char* name, const uint8_t** data, size_t*
       x += 4 + sz;
     }
     if (nm == want || nm == want_npy) {
-      if (loff + 30 > n || rd32(p + loff) != 0x04034b50u) return EVOC_ERR_ARG;
+      // Subtraction-form bounds: loff and csize may be 64-bit ZIP64 values.
+      if (loff > n || n - loff < 30 || rd32(p + loff) != 0x04034b50u) return EVOC_ERR_ARG;
       const uint64_t start = loff + 30 + rd16(p + loff + 26) + rd16(p + loff + 28);
-      if (start + csize > n) return EVOC_ERR_ARG;
+      if (start > n || csize > n - start) return EVOC_ERR_ARG;
       if (method == 0) {
         *data = p + start;
         *len = size_t(csize);
         return EVOC_OK;
       }
       if (method != 8) return EVOC_ERR_UNSUPPORTED;
+      // zlib counts in 32 bits: deflated members of 4 GiB or more are not read.
+      if (csize > 0xFFFFFFFFull || usize > 0xFFFFFFFFull) return EVOC_ERR_UNSUPPORTED;
       void* buf = std::malloc(usize ? size_t(usize) : 1);
       if (!buf) return EVOC_ERR_OOM;
       z_stream zs = {};
@@ -209,7 +220,7 @@ int zip_member(const Mapping& m, const char* name, const uint8_t** data, size_t*
         return EVOC_ERR_ARG;
       }
       zs.next_in = const_cast<Bytef*>(p + start);
-      zs.avail_in = uInt(csize);  // members here stay below 4 GiB compressed
+      zs.avail_in = uInt(csize);
       zs.next_out = static_cast<Bytef*>(buf);
       zs.avail_out = uInt(usize);
       const int rc = inflate(&zs, Z_FINISH);

@@ -321,9 +321,11 @@ int evoc_gpu_last_launch_count(const evoc_gpu_ctx* ctx);
  * synchronisation.  All pointers are device pointers; the work is enqueued on
  * `stream` (a cudaStream_t, 0 for the default stream) and the call returns
  * without waiting for it.
- *   rows       n rows of `ld` floats, 16-byte aligned, ld a multiple of 16,
- *              columns past the data zero, each row already L2-normalised
- *              (this entry point has no working copy to renormalise into)
+ *   rows       n rows of `ld` floats, 16-byte aligned, ld a multiple of 16
+ *              (at most INT32_MAX), columns past the data zero, each row
+ *              already L2-normalised (this entry point has no working copy
+ *              to renormalise into); rows holding NaN or infinities give
+ *              undefined neighbours (the call does not scan for them)
  *   k          clamped to max(1, min(k, n-1)); at most 64 after the clamp,
  *              larger values return EVOC_ERR_UNSUPPORTED
  *   out_idx / out_dist   n x k_eff, as evoc_gpu_knn_graph with EVOC_FORM_FP32

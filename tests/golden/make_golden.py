@@ -28,7 +28,8 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+# The evoc-rs checkout: the first argument, else $EVOC_REFERENCE_TREE, else /root/reference.
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("EVOC_REFERENCE_TREE", "/root/reference")
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 

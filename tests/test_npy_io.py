@@ -114,6 +114,48 @@ def test_errors(tmp_path):
     assert st == _lib.EVOC_ERR_ARG and nnz.value == 2  # cap below nnz
 
 
+def _npy_with_header(path, header: str, payload: bytes):
+    h = header.encode("latin1")
+    pad = 64 - (10 + len(h) + 1) % 64
+    h = h + b" " * pad + b"\n"
+    with open(path, "wb") as fh:
+        fh.write(b"\x93NUMPY\x01\x00" + len(h).to_bytes(2, "little") + h + payload)
+
+
+@pytest.mark.parametrize("shape", ["(4611686018427387904, 4)", "(9223372036854775807, 2)",
+                                   "(4294967296, 4294967296, 2)", "(2305843009213693952,)"])
+def test_overflowing_shape_is_rejected(tmp_path, shape):
+    """A shape whose element count or byte size wraps 64 bits must not pass the size check."""
+    p = str(tmp_path / "wrap.npy")
+    _npy_with_header(p, "{'descr': '<f4', 'fortran_order': False, 'shape': %s, }" % shape, b"\0" * 64)
+    with pytest.raises(evoc.BackendError):
+        npy.load(p)
+
+
+def test_zip_extra_field_past_its_region_is_rejected(tmp_path):
+    """A ZIP64 extra field whose size runs past the central-directory entry is refused."""
+    import io
+    import struct
+    import zipfile
+
+    p = tmp_path / "x.npz"
+    body = io.BytesIO()
+    np.save(body, np.arange(6, dtype=np.float32))
+    zi = zipfile.ZipInfo("a.npy")
+    zi.extra = struct.pack("<HH", 0xCAFE, 4) + b"abcd"  # one private extra field of 4 bytes
+    with zipfile.ZipFile(p, "w") as zf:
+        zf.writestr(zi, body.getvalue())
+    assert np.array_equal(npy.load(str(p), "a"), np.arange(6, dtype=np.float32))  # well-formed: readable
+    raw = bytearray(p.read_bytes())
+    at = raw.rfind(b"PK\x01\x02")
+    nlen, xlen = struct.unpack_from("<HH", raw, at + 28)
+    assert xlen >= 4
+    struct.pack_into("<H", raw, at + 46 + nlen + 2, 0xFFF0)  # first extra field claims 65,520 bytes
+    p.write_bytes(bytes(raw))
+    with pytest.raises(evoc.BackendError):
+        npy.load(str(p), "a")
+
+
 @pytest.mark.gpu
 def test_mapped_rows_feed_knn_graph(tmp_path):
     """Rows read in place from an .npy file go to the kNN entry point as they are."""

@@ -86,3 +86,37 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
     assert b"at most 64" in err.value
     rc = f(xt.data_ptr(), 200, 20, 10, oi.data_ptr(), od.data_ptr(), None, None, err, 256)
     assert rc == _lib.EVOC_ERR_ARG
+    rc = f(xt.data_ptr(), 200, (1 << 31) + 16, 10, oi.data_ptr(), od.data_ptr(), None, None, err, 256)
+    assert rc == _lib.EVOC_ERR_ARG and b"int32" in err.value  # stride beyond the kernel's int range
+
+
+def test_noalloc_k64_grid_capped_by_the_fixed_scratch():
+    """k = 64 with more than 128 * 128 rows: the persistent grid is capped by what fits in the fixed
+    array (128 CTAs), so every CTA reuses its candidate buffers over several query blocks.  Checked
+    against an FP64 brute force on a sample of rows (sets equal up to ties within 1e-6)."""
+    import torch
+
+    f = _noalloc()
+    n, d, k = 20_000, 64, 64
+    x = _rows(n, d, 5)
+    xt = torch.from_numpy(x).cuda()
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    oi, od = _run(f, xt, n, d, k, stream)
+    torch.cuda.synchronize()
+    gi, gd = oi.cpu().numpy(), od.cpu().numpy()
+    x64 = x.astype(np.float64)
+    rows = np.arange(0, n, 97)
+    for r in rows:
+        dots = x64 @ x64[r]
+        raw = np.where(dots > 0, -dots, 1.17549435e-38)
+        raw[r] = -1.0
+        order = np.lexsort((np.arange(n), raw))
+        want = order[:k]
+        kth = raw[want[-1]]
+        got = gi[r]
+        assert got[0] == r
+        assert len(set(got)) == k
+        # every returned key is within 1e-6 of the k-th, or among the exact k
+        extra = set(got) - set(want)
+        assert all(raw[j] <= kth + 1e-6 for j in extra), (r, extra)
+        assert np.all(np.diff(gd[r]) >= -1e-6)
