@@ -58,12 +58,18 @@ struct evoc_gpu_ctx {
   evoc::DevBuf xb, cand, labels, order, hist, cursor, pivots, popc;
   evoc::DevBuf g_idx, g_dist, g_sigma, g_rho, g_indptr, g_indices, g_data, g_work;
   evoc::DevBuf nnd_work;
+  // 16-bit form certificate: per-row residual / operand norms, their maxima,
+  // the scan's C-th kept value per query row, the lists of rows that failed;
+  // and the rescan arena for those rows (bounded chunks).
+  evoc::DevBuf cert, repair;
+  int64_t cert_checked = 0, cert_second = 0, cert_exact = 0;  // last call's counts
   evoc::DevBuf batch_ws, batch_tab;  // batches: per-request work arena, device tables
   void* batch_host = nullptr;  // pinned staging of the tables
   size_t batch_host_bytes = 0;
   struct BatchGraph {
     bool f32;
     int keep_odd;
+    int key;  // certificate on/off and the 16-bit operand type
     void* tab;
     int grids[4];  // rows, norms, scan, rerank
     cudaGraphExec_t exec;

@@ -25,6 +25,8 @@ enum CtxBuf {
   kBufNnd,
   kBufBatchWs,   // batches: per-request work arena
   kBufBatchTab,  // batches: device tables
+  kBufCert,      // 16-bit form: certificate norms, bounds, failed-row lists
+  kBufRepair,    // 16-bit form: rescan arena for rows that failed the certificate
   kBufCount
 };
 

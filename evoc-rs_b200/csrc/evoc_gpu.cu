@@ -117,7 +117,7 @@ int64_t pivot_count(int64_t n) {
 }
 
 int locality_order(evoc_gpu_ctx* ctx, const Job& j, const void* rows, int64_t row_bytes, bool int8,
-                   bool sorted_cells) {
+                   bool sorted_cells, int half_type = evoc::kHalfF16) {
   Stage st(ctx, "pivot_order");
   const int64_t n_piv = pivot_count(j.n);
   const int64_t piv_rows = evoc::padded_rows(n_piv);
@@ -127,10 +127,10 @@ int locality_order(evoc_gpu_ctx* ctx, const Job& j, const void* rows, int64_t ro
            "gather pivots");
   const int grid = scan_grid(ctx, j.nq);
   EVOC_TRY(ctx->labels.ensure(size_t(j.nq) * 4), "alloc labels");
-  EVOC_TRY(evoc::launch_tc_scan(int8 ? evoc::kScanInt8 : evoc::kScanBf16, rows, evoc::padded_rows(j.n), j.r0, j.nq,
+  EVOC_TRY(evoc::launch_tc_scan(int8 ? evoc::kScanInt8 : evoc::kScanHalf, rows, evoc::padded_rows(j.n), j.r0, j.nq,
                                 ctx->pivots.p, piv_rows, n_piv,
                                 row_bytes, 1, nullptr, grid, 0, 0, 0, ctx->labels.as<int32_t>(), nullptr, nullptr,
-                                j.status, ctx->timeout_ns, nullptr, ctx->stream),
+                                j.status, ctx->timeout_ns, nullptr, ctx->stream, -1, half_type),
            "pivot scan");
   EVOC_TRY(ctx->order.ensure(size_t(j.nq) * 4), "alloc order");
   EVOC_TRY(ctx->hist.ensure(size_t(n_piv) * 4), "alloc hist");
@@ -143,7 +143,11 @@ int locality_order(evoc_gpu_ctx* ctx, const Job& j, const void* rows, int64_t ro
   return EVOC_OK;
 }
 
-// Candidates kept per row by the BF16 scan: oversample * k, within [k, n].
+// Rows the certificate's rescans take per pass (bounds their arena; 128
+// query blocks, one wave of the scan).
+constexpr int64_t kRepairChunk = 16384;
+
+// Candidates kept per row by the 16-bit scan: oversample * k, within [k, n].
 int64_t bf16_candidates(const evoc_gpu_opts& opts, int64_t n, int keff) {
   const int over = opts.oversample > 0 ? opts.oversample : 2;
   int64_t C = int64_t(over) * keff;
@@ -152,42 +156,243 @@ int64_t bf16_candidates(const evoc_gpu_opts& opts, int64_t n, int keff) {
   return C;
 }
 
+// Certificate buffer of the 16-bit form (one allocation, parts 256-byte
+// aligned): residual and operand norms of the n rows, their two maxima, the
+// scan's C-th kept value per query row (first and second pass), the failed-row
+// counters and lists.  The second pass's lists are indexed by chunk item.
+struct CertLayout {
+  size_t rnorm, hnorm, maxes, bound, bound2, counts, fail1, fail2, total;
+};
+
+CertLayout cert_layout(int64_t n, int64_t nq) {
+  CertLayout L{};
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t at = off;
+    off += (bytes + 255) / 256 * 256;
+    return at;
+  };
+  L.rnorm = take(size_t(n) * 4);
+  L.hnorm = take(size_t(n) * 4);
+  L.maxes = take(8);
+  L.bound = take(size_t(nq) * 4);
+  L.bound2 = take(size_t(kRepairChunk) * 4);
+  L.counts = take(8);
+  L.fail1 = take(size_t(nq) * 4);
+  L.fail2 = take(size_t(nq) * 4);
+  L.total = off;
+  return L;
+}
+
+// Rescan arena for at most kRepairChunk rows: gathered 16-bit query rows,
+// their candidates, and gathered f32 query rows for the exact pass.
+struct RepairLayout {
+  size_t qh, cand2, qf, total;
+};
+
+RepairLayout repair_layout(int64_t nq, int64_t ld, int64_t ldb, int64_t C2) {
+  const int64_t R = std::min<int64_t>(nq, kRepairChunk);
+  RepairLayout L{};
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t at = off;
+    off += (bytes + 255) / 256 * 256;
+    return at;
+  };
+  L.qh = take(size_t(evoc::padded_rows(R) * ldb * 2));
+  L.cand2 = take(size_t(R * C2) * 4);
+  L.qf = take(size_t(R * ld) * 4);
+  L.total = off;
+  return L;
+}
+
+// Candidates of the second certificate pass: 256 (the rerank's limit), at most n.
+int64_t second_pass_candidates(int64_t n) { return std::min<int64_t>(256, n); }
+
+// Scratch of the scan for `rows` query rows keeping C candidates.
+size_t scan_scratch_bytes(const evoc_gpu_ctx* ctx, int64_t rows, int64_t C) {
+  return size_t(scan_grid(ctx, rows)) * 256 * size_t(C) * 8;
+}
+
+// One request's data as the certificate's rescans see it: its f32 rows and
+// 16-bit rows (n keys, `rows` padded), query rows r0 .. r0+nq-1 written to
+// output rows 0 .. nq-1, the first pass's candidate count, and the
+// certificate's norms.
+struct RescanJob {
+  const float* x;
+  int ld, d;
+  const void* xh;
+  int64_t ldb, rows, n, r0, nq;
+  int keff, half;
+  int64_t C;
+  int32_t* idx;
+  float* raw;
+  float* dist;
+  int* status;
+  evoc::CertArgs cert;  // rnorm, hnorm, maxes, half_len of the request
+};
+
+// The exact FP32 pass over rows listed on the device (output rows of j).
+int exact_rows(evoc_gpu_ctx* ctx, const RescanJob& j, const int32_t* list, int64_t count, float* qf) {
+  const int cap = evoc::topk_capacity(j.keff);
+  const int64_t qblocks = (count + 127) / 128;
+  const int grid = int(std::min<int64_t>(qblocks, int64_t(ctx->sms) * 2));
+  EVOC_TRY(evoc::launch_gather_rows_list(j.x, int64_t(j.ld) * 4, j.r0, list, count, count, qf, ctx->sms,
+                                         ctx->stream),
+           "gather rows");
+  EVOC_TRY(ctx->scratch.ensure(size_t(grid) * 128 * size_t(cap) * 8), "alloc scratch");
+  EVOC_TRY(evoc::launch_knn_f32_simt(j.x, j.n, j.ld, j.keff, cap, ctx->scratch.as<uint64_t>(), grid, j.idx, j.raw,
+                                     j.dist, 0, count, ctx->stream, qf, list, j.r0),
+           "exact rescan");
+  ctx->launches += 2;
+  return EVOC_OK;
+}
+
+int32_t read_count(evoc_gpu_ctx* ctx, const int32_t* d_count, int* rc) {
+  int32_t v = 0;
+  cudaError_t e = cudaMemcpyAsync(&v, d_count, 4, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) *rc = cuda_fail(ctx, e, "read certificate count");
+  return v;
+}
+
+// Rows of j (output rows listed in fail1, `failed1` of them) that failed the
+// first certificate: the 16-bit scan again over those rows, gathered, keeping
+// 256 candidates, the rerank with the certificate; rows failing again (listed
+// in fail2 through count2, whose C-th bounds go to bound2) get the exact FP32
+// scan.  *second / *exact: rows of each rescan.
+int certify_rescan(evoc_gpu_ctx* ctx, const RescanJob& j, int32_t* fail1, int64_t failed1, int32_t* fail2,
+                   float* bound2, int32_t* count2, int64_t* second, int64_t* exact) {
+  Stage st(ctx, "certify_rescan");
+  const int64_t C2 = second_pass_candidates(j.n);
+  const RepairLayout RL = repair_layout(std::min<int64_t>(failed1, kRepairChunk), j.ld, j.ldb, C2);
+  EVOC_TRY(ctx->repair.ensure(RL.total), "alloc rescan arena");
+  uint8_t* rb = ctx->repair.as<uint8_t>();
+  float* qf = reinterpret_cast<float*>(rb + RL.qf);
+  int64_t failed2 = 0;
+  int rc = EVOC_OK;
+  *second = failed1;
+  if (C2 > j.C) {
+    void* qh = rb + RL.qh;
+    int32_t* cand2 = reinterpret_cast<int32_t*>(rb + RL.cand2);
+    EVOC_TRY(ctx->scratch.ensure(scan_scratch_bytes(ctx, std::min<int64_t>(failed1, kRepairChunk), C2)),
+             "alloc scratch");
+    EVOC_TRY(cudaMemsetAsync(count2, 0, 4, ctx->stream), "clear certificate count");
+    evoc::CertArgs c2 = j.cert;
+    c2.bound = bound2;
+    c2.fail_list = fail2;
+    c2.fail_count = count2;
+    c2.fail_cap = failed1;
+    for (int64_t c0 = 0; c0 < failed1; c0 += kRepairChunk) {
+      const int64_t cnt = std::min<int64_t>(kRepairChunk, failed1 - c0);
+      const int64_t qrows = evoc::padded_rows(cnt);
+      // the list holds output rows; the scan's self rule takes r0 + list[i]
+      EVOC_TRY(evoc::launch_gather_rows_list(j.xh, j.ldb * 2, j.r0, fail1 + c0, cnt, qrows, qh, ctx->sms,
+                                             ctx->stream),
+               "gather 16-bit rows");
+      EVOC_TRY(evoc::launch_tc_scan(evoc::kScanHalf, qh, qrows, 0, cnt, j.xh, j.rows, j.n, j.ldb * 2, int(C2),
+                                    ctx->scratch.as<uint64_t>(), scan_grid(ctx, cnt), 1, 0, 0, cand2, nullptr, nullptr,
+                                    j.status, ctx->timeout_ns, nullptr, ctx->stream, -1, j.half, fail1 + c0, bound2,
+                                    j.r0),
+               "16-bit rescan");
+      EVOC_TRY(evoc::launch_rerank_f32(j.x, j.ld, j.d, cnt, j.n, j.r0, cand2, int(C2), j.keff, fail1 + c0, j.idx,
+                                       j.raw, j.dist, j.status, ctx->sms, ctx->stream, &c2, true, j.nq),
+               "rescan rerank");
+      ctx->launches += 3;
+    }
+    failed2 = read_count(ctx, count2, &rc);
+    if (rc) return rc;
+  } else {
+    fail2 = fail1;  // no larger candidate set exists: every failed row goes to the exact pass
+    failed2 = failed1;
+  }
+  *exact = failed2;
+  for (int64_t c0 = 0; c0 < failed2; c0 += kRepairChunk) {
+    const int64_t cnt = std::min<int64_t>(kRepairChunk, failed2 - c0);
+    rc = exact_rows(ctx, j, fail2 + c0, cnt, qf);
+    if (rc) return rc;
+  }
+  return EVOC_OK;
+}
+
+// The 16-bit form: FP16 (or BF16) tensor-core scan keeping C candidates per
+// row, FP32 rerank with the per-row certificate (rerank.cu), then for rows
+// that fail it a second scan keeping 256 candidates, and for rows that fail
+// again an exact FP32 scan.  Every returned row is either certified or exact.
 int run_bf16_rerank(evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, const Job& j, int ld, int d) {
   const int64_t C = bf16_candidates(opts, j.n, j.keff);
   if (C > 256) return fail(ctx, EVOC_ERR_UNSUPPORTED, "oversample * k must be <= 256");
+  if (opts.scan_type != evoc::kHalfF16 && opts.scan_type != evoc::kHalfBf16)
+    return fail(ctx, EVOC_ERR_ARG, "scan_type must be 0 (FP16) or 1 (BF16)");
+  const int half = opts.scan_type;
+  const bool certify = opts.certify != 0;
   const int64_t ldb = round_up(d, 64);
   const int64_t rows = evoc::padded_rows(j.n);
+  const CertLayout CL = cert_layout(j.n, j.nq);
+  uint8_t* cb = nullptr;
+  if (certify) {
+    EVOC_TRY(ctx->cert.ensure(CL.total), "alloc certificate");
+    cb = ctx->cert.as<uint8_t>();
+  }
+  auto cf = [&](size_t off) { return reinterpret_cast<float*>(cb + off); };
+  auto ci = [&](size_t off) { return reinterpret_cast<int32_t*>(cb + off); };
+  unsigned int* maxes = certify ? reinterpret_cast<unsigned int*>(cb + CL.maxes) : nullptr;
   {
-    Stage st(ctx, "to_bf16");
-    EVOC_TRY(ctx->xb.ensure(size_t(rows * ldb * 2)), "alloc bf16 rows");
-    EVOC_TRY(evoc::launch_to_bf16(ctx->x.as<float>(), rows, ld, d, ctx->xb.p, int(ldb), ctx->sms, ctx->stream),
-             "to bf16");
+    Stage st(ctx, "to_half");
+    EVOC_TRY(ctx->xb.ensure(size_t(rows * ldb * 2)), "alloc 16-bit rows");
+    EVOC_TRY(evoc::launch_to_half(ctx->x.as<float>(), rows, j.n, ld, d, ctx->xb.p, int(ldb), half,
+                                  certify ? cf(CL.rnorm) : nullptr, certify ? cf(CL.hnorm) : nullptr, maxes, ctx->sms,
+                                  ctx->stream),
+             "to 16-bit");
     ctx->launches += 1;
   }
   const int grid = scan_grid(ctx, j.nq);
   EVOC_TRY(ctx->cand.ensure(size_t(j.nq * C) * 4), "alloc candidates");
   {
     Stage st(ctx, "bf16_scan");
-    EVOC_TRY(ctx->scratch.ensure(size_t(grid) * 256 * size_t(C) * 8), "alloc scratch");
-    EVOC_TRY(evoc::launch_tc_scan(evoc::kScanBf16, ctx->xb.p, rows, j.r0, j.nq, ctx->xb.p, rows, j.n, ldb * 2, int(C),
+    EVOC_TRY(ctx->scratch.ensure(scan_scratch_bytes(ctx, j.nq, C)), "alloc scratch");
+    EVOC_TRY(evoc::launch_tc_scan(evoc::kScanHalf, ctx->xb.p, rows, j.r0, j.nq, ctx->xb.p, rows, j.n, ldb * 2, int(C),
                                   ctx->scratch.as<uint64_t>(), grid, 1, 0, 0, ctx->cand.as<int32_t>(), nullptr,
                                   nullptr, j.status, ctx->timeout_ns, nullptr, ctx->stream,
-                                  tuned_variant(ctx, evoc::kScanBf16, int(C), ldb * 2, j.n)),
-             "bf16 scan");
+                                  tuned_variant(ctx, evoc::kScanHalf, int(C), ldb * 2, j.n), half, nullptr,
+                                  certify ? cf(CL.bound) : nullptr),
+             "16-bit scan");
     ctx->launches += 1;
   }
   const int32_t* order = nullptr;
   if (j.nq >= 65536) {
-    int rc = locality_order(ctx, j, ctx->xb.p, ldb * 2, false, false);  // the order only schedules the rerank
+    // the order only schedules the rerank
+    int rc = locality_order(ctx, j, ctx->xb.p, ldb * 2, false, false, half);
     if (rc) return rc;
     order = ctx->order.as<int32_t>();
   }
-  Stage st(ctx, "rerank");
-  EVOC_TRY(evoc::launch_rerank_f32(ctx->x.as<float>(), ld, d, j.nq, j.n, j.r0, ctx->cand.as<int32_t>(), int(C),
-                                   j.keff, order, j.idx, j.raw, j.dist, j.status, ctx->sms, ctx->stream),
-           "rerank");
-  ctx->launches += 1;
-  return EVOC_OK;
+  int32_t* counts = certify ? ci(CL.counts) : nullptr;
+  evoc::CertArgs ca{};
+  if (certify) {
+    EVOC_TRY(cudaMemsetAsync(counts, 0, 8, ctx->stream), "clear certificate counts");
+    ca = evoc::CertArgs{cf(CL.bound), cf(CL.rnorm), cf(CL.hnorm), maxes, int(ldb), ci(CL.fail1), counts, j.nq};
+  }
+  {
+    Stage st(ctx, "rerank");
+    EVOC_TRY(evoc::launch_rerank_f32(ctx->x.as<float>(), ld, d, j.nq, j.n, j.r0, ctx->cand.as<int32_t>(), int(C),
+                                     j.keff, order, j.idx, j.raw, j.dist, j.status, ctx->sms, ctx->stream,
+                                     certify ? &ca : nullptr),
+             "rerank");
+    ctx->launches += 1;
+  }
+  ctx->cert_checked = certify ? j.nq : 0;
+  if (!certify) return EVOC_OK;
+  int rc = EVOC_OK;
+  const int64_t failed1 = read_count(ctx, counts, &rc);
+  if (rc) return rc;
+  if (failed1 == 0) return EVOC_OK;
+  RescanJob rj{ctx->x.as<float>(), ld, d, ctx->xb.p, ldb, rows, j.n, j.r0, j.nq, j.keff, half, C, j.idx, j.raw,
+               j.dist, j.status, ca};
+  int64_t second = 0, exact = 0;
+  rc = certify_rescan(ctx, rj, ci(CL.fail1), failed1, ci(CL.fail2), cf(CL.bound2), counts + 1, &second, &exact);
+  ctx->cert_second = second;
+  ctx->cert_exact = exact;
+  return rc;
 }
 
 int run_int8(evoc_gpu_ctx* ctx, const Job& j, int64_t ldb) {
@@ -504,6 +709,7 @@ int knn_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtype, con
   ctx->err.clear();
   ctx->n_stages = 0;
   ctx->launches = 0;
+  ctx->cert_checked = ctx->cert_second = ctx->cert_exact = 0;
   evoc_gpu_opts opts;
   evoc_gpu_default_opts(&opts);
   if (opts_in) {
@@ -552,7 +758,27 @@ int knn_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtype, con
   EVOC_TRY(cudaMemsetAsync(d_flags, 0, 64, ctx->stream), "clear flags");
   job.status = d_flags + 1;
   int rc = EVOC_OK;
-  if (dtype == EVOC_DTYPE_F32) {
+  // The reference's integer brute-force branch (src/knn.rs:418-421) takes
+  // precedence over the form, as it does over NN-descent there.
+  const bool brute = dtype != EVOC_DTYPE_F32 && n <= opts.brute_force_max_n;
+  if (opts.strict_precision && !brute)
+    return fail(ctx, EVOC_ERR_UNSUPPORTED,
+                "strict_precision: the Strict backend's results come from its RP-forest NN-descent "
+                "(src/knn.rs:423-445), which no GPU form reproduces bit for bit; only i8/u8 data with "
+                "n <= brute_force_max_n (the reference's brute-force branch) is bit-identical here. "
+                "Set strict_precision = false to take the exact GPU search");
+  if (brute) {
+    const int64_t ldb = dtype == EVOC_DTYPE_I8 ? round_up(dim, 128) : round_up(dim, 64);
+    if (evoc::brute_force_smem_per_warp(ldb, keff) > 200 * 1024)
+      return fail(ctx, EVOC_ERR_UNSUPPORTED, "k and row length too large for the brute-force branch");
+    rc = stage_rows(ctx, data, n, dim, ldb, on_dev);
+    if (rc) return rc;
+    Stage st(ctx, "brute_force");
+    EVOC_TRY(evoc::launch_brute_force_heap(dtype, ctx->x.p, n, ldb, keff, r0, r1, job.idx, job.raw, job.dist, ctx->sms,
+                                           ctx->stream),
+             "brute force");
+    ctx->launches += 1;
+  } else if (dtype == EVOC_DTYPE_F32) {
     if (form != EVOC_FORM_FP32 && form != EVOC_FORM_BF16_RERANK && form != EVOC_FORM_NNDESCENT)
       return fail(ctx, EVOC_ERR_UNSUPPORTED, "form not built for f32 in this library");
     const int ld = int(round_up(dim, 16));
@@ -569,15 +795,15 @@ int knn_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtype, con
     if (form == EVOC_FORM_FP32) rc = run_fp32(ctx, job, ld);
     else if (form == EVOC_FORM_BF16_RERANK) rc = run_bf16_rerank(ctx, opts, job, ld, int(dim));
     else {
-      // The pivot cells come from the BF16 tensor-core scan; the join reads the f32 rows.
+      // The pivot cells come from the FP16 tensor-core scan; the join reads the f32 rows.
       const int64_t ldb = round_up(dim, 64);
       const int64_t rows = evoc::padded_rows(n);
       {
-        Stage st(ctx, "to_bf16");
-        EVOC_TRY(ctx->xb.ensure(size_t(rows * ldb * 2)), "alloc bf16 rows");
-        EVOC_TRY(evoc::launch_to_bf16(ctx->x.as<float>(), rows, ld, int(dim), ctx->xb.p, int(ldb), ctx->sms,
-                                      ctx->stream),
-                 "to bf16");
+        Stage st(ctx, "to_half");
+        EVOC_TRY(ctx->xb.ensure(size_t(rows * ldb * 2)), "alloc 16-bit rows");
+        EVOC_TRY(evoc::launch_to_half(ctx->x.as<float>(), rows, n, ld, int(dim), ctx->xb.p, int(ldb), evoc::kHalfF16,
+                                      nullptr, nullptr, nullptr, ctx->sms, ctx->stream),
+                 "to 16-bit");
         ctx->launches += 1;
       }
       rc = run_nndescent(ctx, opts, job, EVOC_DTYPE_F32, int64_t(ld) * 4, ctx->x.p, ld, int(dim), rng_state,
@@ -631,10 +857,13 @@ struct BatchJobPlan {
   int64_t n, dim, rows, ld, ldb;
   int keff, C, keep;
   size_t off_x, off_xb, off_norms, off_cand, off_flag;
+  size_t off_rnorm, off_hnorm, off_maxes, off_bound;  // f32 with the certificate
 };
 
 struct BatchLayout {
   std::vector<BatchJobPlan> jobs;
+  size_t off_fail = 0;  // (request, row) pairs of rows that failed the certificate
+  int64_t max_n = 0;
   size_t ws_bytes = 0;
   size_t off_sj = 0, off_rj = 0, off_it = 0, tab_bytes = 0;
   int max_keep = 1;
@@ -674,6 +903,18 @@ int batch_layout(bool f32, const evoc_gpu_opts& opts, int32_t n_jobs, const int6
       ws += align_up(size_t(J.n) * size_t(J.C) * 4, 256);
       J.off_flag = ws;
       ws += 256;
+      if (opts.certify) {
+        J.off_rnorm = ws;
+        ws += align_up(size_t(J.n) * 4, 256);
+        J.off_hnorm = ws;
+        ws += align_up(size_t(J.n) * 4, 256);
+        J.off_maxes = ws;
+        ws += 256;
+        J.off_bound = ws;
+        ws += align_up(size_t(J.n) * 4, 256);
+      } else {
+        J.off_rnorm = J.off_hnorm = J.off_maxes = J.off_bound = 0;
+      }
     } else {
       J.ld = 0;
       J.ldb = round_up(J.dim, 128);
@@ -682,11 +923,17 @@ int batch_layout(bool f32, const evoc_gpu_opts& opts, int32_t n_jobs, const int6
       J.off_xb = ws;
       ws += align_up(size_t(J.rows * J.ldb), 256);
       J.off_x = J.off_norms = J.off_cand = J.off_flag = 0;
+      J.off_rnorm = J.off_hnorm = J.off_maxes = J.off_bound = 0;
     }
+    L->max_n = std::max(L->max_n, J.n);
     L->max_keep = std::max(L->max_keep, J.keep);
     L->n_items += (J.n + 127) / 128;
     L->total_rows += J.n;
     L->total_blocks += (J.n + 127) / 128;
+  }
+  if (f32 && opts.certify) {
+    L->off_fail = ws;
+    ws += align_up(size_t(L->total_rows) * 8, 256);
   }
   L->ws_bytes = std::max<size_t>(ws, 256);
   // Fixed offsets (room for the largest batch), so the tables' addresses --
@@ -707,6 +954,7 @@ int knn_batch_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtyp
   ctx->err.clear();
   ctx->n_stages = 0;
   ctx->launches = 0;
+  ctx->cert_checked = ctx->cert_second = ctx->cert_exact = 0;
   evoc_gpu_opts opts;
   evoc_gpu_default_opts(&opts);
   if (opts_in) {
@@ -752,8 +1000,14 @@ int knn_batch_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtyp
   hdr->n_jobs = n_jobs;
   hdr->n_items = int32_t(L.n_items);
   hdr->status = 0;
+  hdr->fail_count = 0;
   hdr->total_rows = L.total_rows;
   hdr->total_blocks = L.total_blocks;
+  const bool certify = f32 && opts.certify != 0;
+  hdr->fail_list = certify ? reinterpret_cast<int32_t*>(W + L.off_fail) : nullptr;
+  hdr->fail_cap = certify ? L.total_rows : 0;
+  if (f32 && opts.scan_type != evoc::kHalfF16 && opts.scan_type != evoc::kHalfBf16)
+    return fail(ctx, EVOC_ERR_ARG, "scan_type must be 0 (FP16) or 1 (BF16)");
   auto* sj = reinterpret_cast<evoc::ScanJob*>(H + L.off_sj);
   auto* rj = reinterpret_cast<evoc::BatchRowJob*>(H + L.off_rj);
   auto* it = reinterpret_cast<evoc::ScanItem*>(H + L.off_it);
@@ -782,11 +1036,17 @@ int knn_batch_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtyp
     R.out_idx = out_idx[i];
     R.out_dist = out_dist ? out_dist[i] : nullptr;
     R.out_raw = out_raw ? out_raw[i] : nullptr;
+    R.half_type = f32 ? opts.scan_type : 0;
+    R.certify = certify ? 1 : 0;
+    R.rnorm = certify ? reinterpret_cast<float*>(W + J.off_rnorm) : nullptr;
+    R.hnorm = certify ? reinterpret_cast<float*>(W + J.off_hnorm) : nullptr;
+    R.maxes = certify ? reinterpret_cast<unsigned int*>(W + J.off_maxes) : nullptr;
+    R.bound = certify ? reinterpret_cast<float*>(W + J.off_bound) : nullptr;
     const bool ok =
-        f32 ? evoc::encode_scan_job(&sj[i], evoc::kScanBf16, R.xb, J.rows, J.n, J.ldb, J.C, 0, 0, R.cand, nullptr,
-                                    nullptr)
+        f32 ? evoc::encode_scan_job(&sj[i], evoc::kScanHalf, R.xb, J.rows, J.n, J.ldb, J.C, 0, 0, R.cand, nullptr,
+                                    nullptr, R.bound, R.half_type)
             : evoc::encode_scan_job(&sj[i], evoc::kScanInt8, R.xb, J.rows, J.n, J.ldb, J.keff, 1, EVOC_DTYPE_I8,
-                                    R.out_idx, R.out_raw, R.out_dist);
+                                    R.out_idx, R.out_raw, R.out_dist, nullptr, 0);
     if (!ok) return fail(ctx, EVOC_ERR_CUDA, "tensor map encoding failed for a batch request");
     if (out_k) out_k[i] = J.keff;
   }
@@ -812,7 +1072,7 @@ int knn_batch_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtyp
   auto* d_sj = reinterpret_cast<const evoc::ScanJob*>(T + L.off_sj);
   auto* d_rj = reinterpret_cast<const evoc::BatchRowJob*>(T + L.off_rj);
   auto* d_it = reinterpret_cast<const evoc::ScanItem*>(T + L.off_it);
-  const int mode = f32 ? evoc::kScanBf16 : evoc::kScanInt8;
+  const int mode = f32 ? evoc::kScanHalf : evoc::kScanInt8;
   EVOC_TRY(evoc::prepare_tc_scan_batch(mode, L.max_keep), "batch scan attributes");
   // Grids sized for this batch (rounded up to a power of two, so few distinct
   // launch configurations occur): a small batch takes a few SMs and runs
@@ -830,10 +1090,12 @@ int knn_batch_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtyp
   // The table offsets are fixed; the graph is keyed on everything else its
   // launch parameters hold.
   const int keep_odd = L.max_keep | 1;
+  const int gkey = (certify ? 1 : 0) | (f32 ? opts.scan_type : 0) << 1;  // kernels' per-batch constants
   auto launch_all = [&](cudaStream_t st) -> cudaError_t {
     cudaError_t e = evoc::launch_batch_rows(f32, d_hdr, d_rj, grids[0], grids[1], st);
     if (e == cudaSuccess)
-      e = evoc::launch_tc_scan_batch(mode, d_hdr, d_sj, d_it, L.max_keep, grids[2], ctx->timeout_ns, st);
+      e = evoc::launch_tc_scan_batch(mode, d_hdr, d_sj, d_it, L.max_keep, grids[2], ctx->timeout_ns, st,
+                                     f32 ? opts.scan_type : 0);
     if (e == cudaSuccess && f32) e = evoc::launch_batch_rerank(d_hdr, d_rj, grids[3], st);
     return e;
   };
@@ -850,7 +1112,7 @@ int knn_batch_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtyp
     }
     cudaGraphExec_t exec = nullptr;
     for (const auto& g : ctx->batch_graphs)
-      if (g.f32 == f32 && g.keep_odd == keep_odd && g.tab == ctx->batch_tab.p &&
+      if (g.f32 == f32 && g.keep_odd == keep_odd && g.tab == ctx->batch_tab.p && g.key == gkey &&
           std::equal(grids, grids + 4, g.grids))
         exec = g.exec;
     if (!exec) {
@@ -866,17 +1128,57 @@ int knn_batch_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtyp
       const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
       cudaGraphDestroy(graph);
       EVOC_TRY(ie, "instantiate batch graph");
-      ctx->batch_graphs.push_back({f32, keep_odd, ctx->batch_tab.p, {grids[0], grids[1], grids[2], grids[3]}, exec});
+      ctx->batch_graphs.push_back(
+          {f32, keep_odd, gkey, ctx->batch_tab.p, {grids[0], grids[1], grids[2], grids[3]}, exec});
     }
     EVOC_TRY(cudaGraphLaunch(exec, ctx->stream), "launch batch graph");
   } else {
     EVOC_TRY(launch_all(ctx->stream), "batch launches");
   }
-  int status = 0;
-  EVOC_TRY(cudaMemcpyAsync(&status, &d_hdr->status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream),
+  int32_t st2[2] = {0, 0};  // status, fail_count
+  EVOC_TRY(cudaMemcpyAsync(st2, &d_hdr->status, sizeof(st2), cudaMemcpyDeviceToHost, ctx->stream),
            "read batch status");
-  total.end();
   EVOC_TRY(cudaStreamSynchronize(ctx->stream), "batch");
+  int status = st2[0];
+  ctx->cert_checked = certify ? L.total_rows : 0;
+  if (status == 0 && certify && st2[1] > 0) {
+    // Rows that failed the certificate: each request's rescans, as a single call makes them.
+    const int64_t nf = std::min<int64_t>(st2[1], L.total_rows);
+    std::vector<int32_t> pairs(size_t(nf) * 2);
+    EVOC_TRY(cudaMemcpy(pairs.data(), W + L.off_fail, pairs.size() * 4, cudaMemcpyDeviceToHost), "read failed rows");
+    std::vector<std::vector<int32_t>> by_job(static_cast<size_t>(n_jobs));
+    for (int64_t f = 0; f < nf; f++) by_job[size_t(pairs[size_t(2 * f)])].push_back(pairs[size_t(2 * f + 1)]);
+    const CertLayout CL = cert_layout(L.max_n, L.max_n);
+    EVOC_TRY(ctx->cert.ensure(CL.total), "alloc certificate");
+    uint8_t* cb = ctx->cert.as<uint8_t>();
+    int64_t second = 0, exact = 0;
+    for (int i = 0; i < n_jobs; i++) {
+      std::vector<int32_t>& rows_i = by_job[size_t(i)];
+      if (rows_i.empty()) continue;
+      std::sort(rows_i.begin(), rows_i.end());
+      const BatchJobPlan& J = L.jobs[size_t(i)];
+      const evoc::BatchRowJob& R = rj[i];
+      int32_t* fail1 = reinterpret_cast<int32_t*>(cb + CL.fail1);
+      EVOC_TRY(cudaMemcpyAsync(fail1, rows_i.data(), rows_i.size() * 4, cudaMemcpyHostToDevice, ctx->stream),
+               "upload failed rows");
+      evoc::CertArgs ca{R.bound, R.rnorm, R.hnorm, R.maxes, int(J.ldb / 2), nullptr, nullptr, 0};
+      RescanJob rsj{R.x, int(J.ld), int(J.dim), R.xb, J.ldb / 2, J.rows, J.n, 0, J.n, J.keff, R.half_type, J.C,
+                    R.out_idx, R.out_raw, R.out_dist, &d_hdr->status, ca};
+      int64_t s2 = 0, ex = 0;
+      const int rc = certify_rescan(ctx, rsj, fail1, int64_t(rows_i.size()), reinterpret_cast<int32_t*>(cb + CL.fail2),
+                                    reinterpret_cast<float*>(cb + CL.bound2),
+                                    reinterpret_cast<int32_t*>(cb + CL.counts), &s2, &ex);
+      if (rc) return rc;
+      second += s2;
+      exact += ex;
+    }
+    ctx->cert_second = second;
+    ctx->cert_exact = exact;
+    EVOC_TRY(cudaMemcpyAsync(&status, &d_hdr->status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream),
+             "read batch status");
+    EVOC_TRY(cudaStreamSynchronize(ctx->stream), "batch rescans");
+  }
+  total.end();
   if (status == evoc::kStatusBadOrder || status == evoc::kStatusBadCandidate)
     return fail(ctx, EVOC_ERR_CUDA, "device self-check failed in a batch (code " + std::to_string(status) + ")");
   if (status != 0)
@@ -923,7 +1225,7 @@ int autotune_impl(evoc_gpu_ctx* ctx, int32_t dtype, int32_t form_in, int64_t n, 
   int mode, keep, final_mode, out_dtype;
   int64_t row_bytes;
   if (dtype == EVOC_DTYPE_F32 && form == EVOC_FORM_BF16_RERANK) {
-    mode = evoc::kScanBf16;
+    mode = evoc::kScanHalf;
     keep = int(bf16_candidates(opts, n, keff));
     row_bytes = round_up(dim, 64) * 2;
     final_mode = 0;
@@ -961,8 +1263,8 @@ int autotune_impl(evoc_gpu_ctx* ctx, int32_t dtype, int32_t form_in, int64_t n, 
              "expand bits");
     pc = ctx->popc.as<int32_t>();
   } else {
-    const int64_t bytes = mode == evoc::kScanBf16 ? dim * 2 : dim;
-    EVOC_TRY(evoc::launch_fill_random(mode == evoc::kScanBf16 ? 0 : 1, ctx->xb.p, rows, row_bytes, nt, bytes, 0x7157u,
+    const int64_t bytes = mode == evoc::kScanHalf ? dim * 2 : dim;
+    EVOC_TRY(evoc::launch_fill_random(mode == evoc::kScanHalf ? 0 : 1, ctx->xb.p, rows, row_bytes, nt, bytes, 0x7157u,
                                       ctx->sms, ctx->stream),
              "fill");
   }
@@ -1043,7 +1345,7 @@ int autotune_impl(evoc_gpu_ctx* ctx, int32_t dtype, int32_t form_in, int64_t n, 
 
 extern "C" {
 
-int evoc_gpu_version(void) { return 100; }
+int evoc_gpu_version(void) { return 200; }
 
 void evoc_gpu_default_opts(evoc_gpu_opts* o) {
   if (!o) return;
@@ -1053,6 +1355,8 @@ void evoc_gpu_default_opts(evoc_gpu_opts* o) {
   o->oversample = 2;
   o->delta = 0.001f;
   o->delta_improv = 0.001f;
+  o->scan_type = 0;  // FP16 operands
+  o->certify = 1;
 }
 
 int evoc_gpu_ctx_create(int device, evoc_gpu_ctx** out) {
@@ -1088,7 +1392,7 @@ void evoc_gpu_ctx_destroy(evoc_gpu_ctx* ctx) {
                     &ctx->out_raw,  &ctx->out_dist, &ctx->xb,   &ctx->cand,   &ctx->labels,
                     &ctx->order,    &ctx->hist,    &ctx->cursor, &ctx->pivots, &ctx->popc,
                     &ctx->g_idx,    &ctx->g_dist,  &ctx->g_sigma, &ctx->g_rho, &ctx->g_indptr,
-                    &ctx->g_indices, &ctx->g_data, &ctx->g_work, &ctx->nnd_work};
+                    &ctx->g_indices, &ctx->g_data, &ctx->g_work, &ctx->nnd_work, &ctx->cert, &ctx->repair};
   for (DevBuf* b : bufs) b->release();
   for (auto& g : ctx->batch_graphs) cudaGraphExecDestroy(g.exec);
   ctx->batch_ws.release();
@@ -1131,6 +1435,14 @@ int evoc_gpu_profile_stage(const evoc_gpu_ctx* ctx, int i, char* name, int name_
 }
 
 int evoc_gpu_last_launch_count(const evoc_gpu_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int evoc_gpu_last_certify(const evoc_gpu_ctx* ctx, int64_t* checked, int64_t* second_pass, int64_t* exact_rescan) {
+  if (!ctx) return EVOC_ERR_ARG;
+  if (checked) *checked = ctx->cert_checked;
+  if (second_pass) *second_pass = ctx->cert_second;
+  if (exact_rescan) *exact_rescan = ctx->cert_exact;
+  return EVOC_OK;
+}
 
 int evoc_gpu_smooth_knn_dist(evoc_gpu_ctx* ctx, const float* dist, int64_t n, int32_t k, float n_neighbors,
                              int32_t buffers_on_device, float* sigma, float* rho) {
@@ -1216,6 +1528,16 @@ void knn_buffer_needs(const evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, int32_
       b[kBufCand] = size_t(n * C) * 4;
       b[kBufScratch] = size_t(grid) * 256 * size_t(C) * 8;
       if (n >= 65536) locality(ldb * 2);
+      if (opts.certify) {
+        // the certificate and, should rows fail it, their rescans (bounded chunks)
+        const int64_t C2 = second_pass_candidates(n);
+        const int64_t R = std::min<int64_t>(n, kRepairChunk);
+        b[kBufCert] = cert_layout(n, n).total;
+        b[kBufRepair] = repair_layout(R, round_up(dim, 16), ldb, C2).total;
+        const int64_t g3 = std::min<int64_t>((R + 127) / 128, int64_t(ctx->sms) * 2);
+        b[kBufScratch] = std::max({b[kBufScratch], scan_scratch_bytes(ctx, R, C2),
+                                   size_t(g3) * 128 * size_t(topk_capacity(int(keff))) * 8});
+      }
     } else if (form == EVOC_FORM_NNDESCENT) {
       b[kBufXb] = size_t(rows * ldb * 2);
       locality(ldb * 2);
@@ -1258,13 +1580,32 @@ bool batch_buffer_needs(const evoc_gpu_opts& opts, int32_t dtype, int32_t n_jobs
   if (batch_layout(f32, opts, n_jobs, n, dim, k, &L) != EVOC_OK || L.max_keep > kBatchMaxKeep) return false;
   need->b[kBufBatchWs] = L.ws_bytes;
   need->b[kBufBatchTab] = L.tab_bytes;
+  if (f32 && opts.certify) {
+    // rescans of rows that fail the certificate, request by request
+    int64_t max_dim = 1, max_keff = 1;
+    for (int i = 0; i < n_jobs; i++) {
+      max_dim = std::max(max_dim, dim[i]);
+      max_keff = std::max<int64_t>(max_keff, std::min<int64_t>(k, n[i] - 1));
+    }
+    const int64_t R = std::min<int64_t>(L.max_n, kRepairChunk);
+    const int64_t C2 = second_pass_candidates(L.max_n);
+    need->b[kBufCert] = cert_layout(L.max_n, L.max_n).total;
+    need->b[kBufRepair] = repair_layout(R, round_up(max_dim, 16), round_up(max_dim, 64), C2).total;
+    // the batch's plan holds no context scratch: the rescans' scan and exact pass size it
+    const int sms = 148;  // upper bound of the grids on B200 (scan_grid caps at the SM count)
+    const int64_t g2 = std::min<int64_t>((R + 127) / 128, sms);
+    const int64_t g3 = std::min<int64_t>((R + 127) / 128, int64_t(sms) * 2);
+    need->b[kBufScratch] = std::max(size_t(g2) * 256 * size_t(C2) * 8,
+                                    size_t(g3) * 128 * size_t(topk_capacity(int(max_keff))) * 8);
+  }
   return true;
 }
 
 void ctx_buffer_sizes(const evoc_gpu_ctx* ctx, CtxSizes* cur) {
-  const DevBuf* bufs[kBufCount] = {&ctx->x,      &ctx->scratch, &ctx->norms,    &ctx->flag,     &ctx->xb,
-                                   &ctx->cand,   &ctx->labels,  &ctx->order,    &ctx->hist,     &ctx->cursor,
-                                   &ctx->pivots, &ctx->popc,    &ctx->nnd_work, &ctx->batch_ws, &ctx->batch_tab};
+  const DevBuf* bufs[kBufCount] = {&ctx->x,      &ctx->scratch, &ctx->norms,    &ctx->flag,      &ctx->xb,
+                                   &ctx->cand,   &ctx->labels,  &ctx->order,    &ctx->hist,      &ctx->cursor,
+                                   &ctx->pivots, &ctx->popc,    &ctx->nnd_work, &ctx->batch_ws,  &ctx->batch_tab,
+                                   &ctx->cert,   &ctx->repair};
   for (int i = 0; i < kBufCount; i++) cur->b[i] = bufs[i]->bytes;
 }
 
@@ -1279,9 +1620,10 @@ void ctx_release_buffers(evoc_gpu_ctx* ctx) {
   std::lock_guard<std::mutex> lock(ctx->mu);
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
-  DevBuf* bufs[kBufCount] = {&ctx->x,      &ctx->scratch, &ctx->norms,    &ctx->flag,     &ctx->xb,
-                             &ctx->cand,   &ctx->labels,  &ctx->order,    &ctx->hist,     &ctx->cursor,
-                             &ctx->pivots, &ctx->popc,    &ctx->nnd_work, &ctx->batch_ws, &ctx->batch_tab};
+  DevBuf* bufs[kBufCount] = {&ctx->x,      &ctx->scratch, &ctx->norms,    &ctx->flag,      &ctx->xb,
+                             &ctx->cand,   &ctx->labels,  &ctx->order,    &ctx->hist,      &ctx->cursor,
+                             &ctx->pivots, &ctx->popc,    &ctx->nnd_work, &ctx->batch_ws,  &ctx->batch_tab,
+                             &ctx->cert,   &ctx->repair};
   for (DevBuf* b : bufs) b->release();
   for (auto& g : ctx->batch_graphs) cudaGraphExecDestroy(g.exec);  // they name the freed tables
   ctx->batch_graphs.clear();

@@ -53,7 +53,8 @@ __device__ __forceinline__ void store_tile(float (*dst)[APAD], int tid, const fl
 __global__ void __launch_bounds__(NT, 2)
 knn_f32_simt_kernel(const float* __restrict__ X, int64_t n, int ld, int k, int cap,
                     uint64_t* __restrict__ scratch, int32_t* __restrict__ out_idx, float* __restrict__ out_raw,
-                    float* __restrict__ out_dist, int64_t q_begin, int64_t q_end) {
+                    float* __restrict__ out_dist, int64_t q_begin, int64_t q_end, const float* __restrict__ Q,
+                    const int32_t* __restrict__ q_list, int64_t q_row0) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   F32Smem& sm = *reinterpret_cast<F32Smem*>(smem_raw);
   const int tid = threadIdx.x;
@@ -67,6 +68,8 @@ knn_f32_simt_kernel(const float* __restrict__ X, int64_t n, int ld, int k, int c
     RowTopK top;
     top.init(my_buf, k, cap);
     const int64_t my_q = q0 + tid;
+    // this query's row of X (the self rule) and its output row
+    const int64_t my_self = (q_list && tid < BM && my_q < q_end) ? q_row0 + q_list[my_q] : my_q;
 
     for (int64_t kt = 0; kt < n_ktiles; kt++) {
       const int64_t c0 = kt * BN;
@@ -77,7 +80,7 @@ knn_f32_simt_kernel(const float* __restrict__ X, int64_t n, int ld, int k, int c
         for (int j = 0; j < 8; j++) acc[i][j] = 0.f;
 
       float4 ra[2], rb[2];
-      load_tile(X, q_end, ld, q0, 0, tid, ra);
+      load_tile(Q, q_end, ld, q0, 0, tid, ra);
       load_tile(X, n, ld, c0, 0, tid, rb);
       store_tile(sm.a[0], tid, ra);
       store_tile(sm.b[0], tid, rb);
@@ -86,7 +89,7 @@ knn_f32_simt_kernel(const float* __restrict__ X, int64_t n, int ld, int k, int c
       for (int k0 = 0; k0 < ld; k0 += BK) {
         const bool more = k0 + BK < ld;
         if (more) {
-          load_tile(X, q_end, ld, q0, k0 + BK, tid, ra);
+          load_tile(Q, q_end, ld, q0, k0 + BK, tid, ra);
           load_tile(X, n, ld, c0, k0 + BK, tid, rb);
         }
 #pragma unroll
@@ -127,7 +130,7 @@ knn_f32_simt_kernel(const float* __restrict__ X, int64_t n, int ld, int k, int c
         const int lim = (n - c0 < BN) ? int(n - c0) : BN;
         for (int c = 0; c < lim; c++) {
           const int64_t key = c0 + c;
-          const float raw = (key == my_q) ? -1.0f : raw_cosine(sm.s[tid][c]);
+          const float raw = (key == my_self) ? -1.0f : raw_cosine(sm.s[tid][c]);
           top.offer(raw, int32_t(key));
         }
       }
@@ -135,7 +138,7 @@ knn_f32_simt_kernel(const float* __restrict__ X, int64_t n, int ld, int k, int c
     }
     if (tid < BM && my_q < q_end) {
       const int got = top.finish();
-      const int64_t orow = (my_q - q_begin) * k;
+      const int64_t orow = (q_list ? int64_t(q_list[my_q]) : my_q - q_begin) * k;
       for (int j = 0; j < k; j++) {
         float raw = kHeapInf;
         int32_t idx = -1;
@@ -155,12 +158,14 @@ size_t knn_f32_simt_smem() { return sizeof(F32Smem); }
 
 cudaError_t launch_knn_f32_simt(const float* X, int64_t n, int ld, int k, int cap, uint64_t* scratch,
                                 int grid, int32_t* out_idx, float* out_raw, float* out_dist, int64_t q_begin,
-                                int64_t q_end, cudaStream_t stream) {
+                                int64_t q_end, cudaStream_t stream, const float* Q, const int32_t* q_list,
+                                int64_t q_row0) {
+  if ((Q == nullptr) != (q_list == nullptr)) return cudaErrorInvalidValue;
   const size_t smem = sizeof(F32Smem);
   cudaError_t e = cudaFuncSetAttribute(knn_f32_simt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   knn_f32_simt_kernel<<<grid, NT, smem, stream>>>(X, n, ld, k, cap, scratch, out_idx, out_raw, out_dist, q_begin,
-                                                   q_end);
+                                                   q_end, Q ? Q : X, q_list, q_row0);
   return cudaGetLastError();
 }
 

@@ -11,10 +11,14 @@ cudaError_t launch_prepare_float(float* X, int64_t n, int ld, int d, float* norm
                                  cudaStream_t stream);
 
 // exact_f32.cu: plain FP32 exact search with fused top-k.
+//   Queries q_begin .. q_end-1 of X against the n rows of X, query q written to output row
+//   q - q_begin.  With Q and q_list (query rows gathered from X): query i is row i of Q, row
+//   q_row0 + q_list[i] of X for the self rule, and is written to output row q_list[i].
 size_t knn_f32_simt_smem();
 cudaError_t launch_knn_f32_simt(const float* X, int64_t n, int ld, int k, int cap, uint64_t* scratch, int grid,
                                 int32_t* out_idx, float* out_raw, float* out_dist, int64_t q_begin, int64_t q_end,
-                                cudaStream_t stream);
+                                cudaStream_t stream, const float* Q = nullptr, const int32_t* q_list = nullptr,
+                                int64_t q_row0 = 0);
 
 // Candidate-buffer capacity used by every fused top-k epilogue for k kept keys.
 // Rows allocated for an n-row device matrix: the tensor-core scan's TMA boxes
@@ -31,38 +35,70 @@ inline int topk_capacity(int k) {
 
 namespace evoc {
 
-// prep.cu: f32 rows (ld) -> zero-padded bf16 rows (ldb elements).
-cudaError_t launch_to_bf16(const float* X, int64_t n, int ld, int d, void* Y, int ldb, int sms, cudaStream_t stream);
+// 16-bit operand type of the f32 tensor-core scan (evoc_gpu_opts.scan_type).
+enum HalfType { kHalfF16 = 0, kHalfBf16 = 1 };
 
-// tc_scan.cu: tcgen05 exact scan (BF16 -> F32, or S8 -> S32) with fused top-k.
+// prep.cu: f32 rows (ld) -> zero-padded 16-bit rows (ldb elements) for rows
+// 0 .. n_rows-1 (rows n .. n_rows-1 zero).  FP16 flushes values below 2^-14
+// to zero.  With rnorm/hnorm (n each) and maxes (2 words): each row's
+// |x - half(x)| and |half(x)| rounded up, and their maxima as f32 bit patterns.
+cudaError_t launch_to_half(const float* X, int64_t n_rows, int64_t n, int ld, int d, void* Y, int ldb, int half_type,
+                           float* rnorm, float* hnorm, unsigned int* maxes, int sms, cudaStream_t stream);
+// prep.cu: dst row i = src row row0 + list[i] (i < count), zero rows up to rows_out.
+cudaError_t launch_gather_rows_list(const void* src, int64_t row_bytes, int64_t row0, const int32_t* list,
+                                    int64_t count, int64_t rows_out, void* dst, int sms, cudaStream_t stream);
+
+// tc_scan.cu: tcgen05 exact scan (FP16 or BF16 -> F32, or S8 -> S32) with fused top-k.
 //   Q: query rows q_row0 .. q_row0+n_q-1 of a q_rows-row matrix; K: the first n_k of k_rows rows;
 //   `row_bytes` per row (multiple of 128, 16-byte aligned bases); q_rows and k_rows are multiples
 //   of 256 and rows past the data are zero.  Query i is written to output row i.
 //   final_mode 1: out rows of `keep` sorted (idx, raw, transformed dist); 0: candidates (idx, raw).
-//   mode 0: BF16 rows, cosine; 1: int8 rows, -(dot); 2: 0/1 int8 rows (expanded bits), Jaccard from
-//   the intersection counts and the row popcounts `pc` (self_mode, Q == K).
+//   mode 0: 16-bit float rows (half_type), cosine; 1: int8 rows, -(dot); 2: 0/1 int8 rows (expanded
+//   bits), Jaccard from the intersection counts and the row popcounts `pc` (self_mode, Q == K).
+//   q_self (optional): key index of query i for the self rule is q_self_base + q_self[i] (default
+//   q_row0 + i), for query rows gathered from elsewhere.  out_bound (optional): per query, the raw
+//   value of the keep-th kept key.
 size_t tc_scan_smem_bytes();
-enum ScanMode { kScanBf16 = 0, kScanInt8 = 1, kScanJaccard = 2 };
+enum ScanMode { kScanHalf = 0, kScanInt8 = 1, kScanJaccard = 2 };
 cudaError_t launch_tc_scan(int mode, const void* Q, int64_t q_rows, int64_t q_row0, int64_t n_q, const void* K,
                            int64_t k_rows, int64_t n_k, int64_t row_bytes, int keep, uint64_t* scratch, int grid,
                            int self_mode, int final_mode, int dtype, int32_t* out_idx, float* out_raw, float* out_dist,
                            int* status, uint64_t timeout_ns, const int32_t* pc, cudaStream_t stream,
-                           int variant = -1);
+                           int variant = -1, int half_type = kHalfF16, const int32_t* q_self = nullptr,
+                           float* out_bound = nullptr, int64_t q_self_base = 0);
 // Kernel variants of the scan (0..5; -1 = automatic: the first that fits
 // shared memory in the order 0..3, else 4 with global heaps; 5 -- 2 stages,
 // 2 groups -- is chosen only by the autotuner).
 constexpr int kScanVariants = 6;
 bool tc_scan_variant_feasible(int variant, int keep, bool has_scratch);
 const char* tc_scan_variant_name(int variant);
-// prep.cu: synthetic rows for the autotuner (mode 0: BF16 values in [-1, 1];
+// prep.cu: synthetic rows for the autotuner (mode 0: FP16 values in [-1, 1];
 // 1: int8; 2: packed bits, about 1 in 8 set), zero past n rows / `bytes` bytes.
 cudaError_t launch_fill_random(int mode, void* rows, int64_t n_rows_mem, int64_t row_bytes, int64_t n,
                                int64_t bytes, uint64_t seed, int sms, cudaStream_t stream);
 
 // rerank.cu
+// Certificate of the 16-bit scan's candidate sets (see rerank.cu): per query row the scan's
+// keep-th kept raw value (`bound`, indexed like the candidates), the rows' residual and operand
+// norms with their maxima, the operand row length; rows whose k nearest cannot be proven to lie
+// among the candidates are appended (output row index) to fail_list.
+struct CertArgs {
+  const float* bound;
+  const float* rnorm;
+  const float* hnorm;
+  const unsigned int* maxes;
+  int half_len;      // elements per 16-bit operand row (the contraction length)
+  int32_t* fail_list;
+  int32_t* fail_count;
+  int64_t fail_cap;
+};
+// rerank.cu.  n_q work items; order (optional): item w reranks output row order[w] (of n_out
+// output rows; default n_q); with by_item the candidates (and the certificate's bound) of item w
+// are row w of `cand`, else row order[w].
 cudaError_t launch_rerank_f32(const float* X, int ld, int d, int64_t n_q, int64_t n_keys, int64_t q_row0,
                               const int32_t* cand, int C, int k, const int32_t* order, int32_t* out_idx, float* out_raw,
-                              float* out_dist, int* status, int sms, cudaStream_t stream);
+                              float* out_dist, int* status, int sms, cudaStream_t stream,
+                              const CertArgs* cert = nullptr, bool by_item = false, int64_t n_out = -1);
 cudaError_t launch_gather_pivots(const void* src, int64_t row_bytes, int64_t n, int64_t n_piv, void* dst, int sms,
                                  cudaStream_t stream);
 // Counting sort of rows by label.  sorted_cells: rows inside each cell ordered
@@ -78,6 +114,16 @@ cudaError_t launch_order_by_label(const int32_t* label, int64_t n, int nb, int32
 cudaError_t launch_copy_rows(const void* src, int64_t n, int64_t row_bytes, void* dst, int64_t rows, int64_t ld_bytes,
                              int sms, cudaStream_t stream);
 
+}  // namespace evoc
+
+namespace evoc {
+// brute.cu: the reference's brute_force_knn for i8 (dtype 1) / u8 (dtype 2) rows of row_bytes
+// (multiple of 16, zero padded), rows q_begin .. q_end-1, each output row in the reference's heap
+// order.  The k-slot heap and the query row sit in shared memory (at most 200 KB per row).
+size_t brute_force_smem_per_warp(int64_t row_bytes, int k);
+cudaError_t launch_brute_force_heap(int dtype, const void* X, int64_t n, int64_t row_bytes, int k, int64_t q_begin,
+                                    int64_t q_end, int32_t* out_idx, float* out_raw, float* out_dist, int sms,
+                                    cudaStream_t stream);
 }  // namespace evoc
 
 namespace evoc {

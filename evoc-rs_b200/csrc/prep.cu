@@ -8,6 +8,7 @@
 // row; rows are staged through shared memory in 32-column slabs so the
 // global reads stay coalesced.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include "batch.h"
 #include "common.cuh"
@@ -84,19 +85,92 @@ cudaError_t launch_prepare_float(float* X, int64_t n, int ld, int d, float* norm
 
 namespace evoc {
 
-// f32 rows (ld floats) -> bf16 rows (ldb elements, zero padded), round to nearest even.
-__global__ void to_bf16_kernel(const float* __restrict__ X, int64_t n, int ld, int d, __nv_bfloat16* __restrict__ Y,
-                               int ldb) {
-  const int64_t total = n * int64_t(ldb);
-  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x) {
-    const int64_t r = e / ldb;
-    const int c = int(e % ldb);
-    Y[e] = __float2bfloat16_rn(c < d ? X[r * ld + c] : 0.0f);
+// One f32 value as the 16-bit operand of the tensor-core scan.  FP16: round
+// to nearest even, with values below the smallest normal (2^-14) flushed to
+// zero, so no subnormal ever reaches the tensor cores and the residual
+// x - half(x) below accounts for the whole difference whatever the hardware
+// does with subnormal inputs.  BF16: round to nearest even.
+__device__ __forceinline__ uint16_t half_bits(float v, int half_type) {
+  if (half_type == kHalfBf16) return __bfloat16_as_ushort(__float2bfloat16_rn(v));
+  if (fabsf(v) < 6.103515625e-05f) return 0;
+  return __half_as_ushort(__float2half_rn(v));
+}
+
+__device__ __forceinline__ float half_value(uint16_t b, int half_type) {
+  return half_type == kHalfBf16 ? __bfloat162float(__ushort_as_bfloat16(b)) : __half2float(__ushort_as_half(b));
+}
+
+// f32 rows (ld floats) -> 16-bit rows (ldb elements, zero padded).  Warp per
+// row.  With `cert`, also the two norms the BF16/FP16 form certifies its rows
+// with: |x - half(x)| (the residual, exact in f32) and |half(x)|, summed in
+// f64 and rounded up to f32, and their maxima over all rows (non-negative
+// floats compare as their bit patterns).
+__global__ void to_half_kernel(const float* __restrict__ X, int64_t n_rows, int64_t n, int ld, int d,
+                               uint16_t* __restrict__ Y, int ldb, int half_type, float* __restrict__ rnorm,
+                               float* __restrict__ hnorm, unsigned int* __restrict__ maxes) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = int64_t(gridDim.x) * (blockDim.x >> 5);
+  for (int64_t r = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); r < n_rows; r += warps) {
+    double rr = 0.0, hh = 0.0;
+    for (int c = lane; c < ldb; c += 32) {
+      const float v = (c < d && r < n) ? X[r * ld + c] : 0.0f;
+      const uint16_t b = half_bits(v, half_type);
+      Y[r * ldb + c] = b;
+      const float h = half_value(b, half_type);
+      const double res = double(v) - double(h);
+      rr += res * res;
+      hh += double(h) * double(h);
+    }
+    if (rnorm && r < n) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        rr += __shfl_xor_sync(0xffffffffu, rr, o);
+        hh += __shfl_xor_sync(0xffffffffu, hh, o);
+      }
+      if (lane == 0) {
+        // f64 sums of at most 2^16 squares are within a relative 2^-36 of
+        // exact: one part in 2^-30 more before rounding up covers them.
+        const float a = __double2float_ru(__dsqrt_ru(rr * (1.0 + 0x1p-30)));
+        const float b = __double2float_ru(__dsqrt_ru(hh * (1.0 + 0x1p-30)));
+        rnorm[r] = a;
+        hnorm[r] = b;
+        atomicMax(&maxes[0], __float_as_uint(a));
+        atomicMax(&maxes[1], __float_as_uint(b));
+      }
+    }
   }
 }
 
-cudaError_t launch_to_bf16(const float* X, int64_t n, int ld, int d, void* Y, int ldb, int sms, cudaStream_t stream) {
-  to_bf16_kernel<<<sms * 8, 256, 0, stream>>>(X, n, ld, d, static_cast<__nv_bfloat16*>(Y), ldb);
+cudaError_t launch_to_half(const float* X, int64_t n_rows, int64_t n, int ld, int d, void* Y, int ldb, int half_type,
+                           float* rnorm, float* hnorm, unsigned int* maxes, int sms, cudaStream_t stream) {
+  if (rnorm) {
+    cudaError_t e = cudaMemsetAsync(maxes, 0, 2 * sizeof(unsigned int), stream);
+    if (e != cudaSuccess) return e;
+  }
+  to_half_kernel<<<sms * 8, 256, 0, stream>>>(X, n_rows, n, ld, d, static_cast<uint16_t*>(Y), ldb, half_type, rnorm,
+                                               hnorm, maxes);
+  return cudaGetLastError();
+}
+
+// Rows list[i] (+ row0) of src -> row i of dst (row_bytes each, 16-byte
+// multiples); dst rows count .. rows_out-1 are zeroed.
+__global__ void gather_rows_list_kernel(const uint8_t* __restrict__ src, int64_t row_bytes, int64_t row0,
+                                        const int32_t* __restrict__ list, int64_t count, int64_t rows_out,
+                                        uint8_t* __restrict__ dst) {
+  const int64_t wpr = row_bytes / 16, total = rows_out * wpr;
+  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t i = e / wpr, w = e % wpr;
+    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+    if (i < count) v = reinterpret_cast<const uint4*>(src + (row0 + list[i]) * row_bytes)[w];
+    reinterpret_cast<uint4*>(dst + i * row_bytes)[w] = v;
+  }
+}
+
+cudaError_t launch_gather_rows_list(const void* src, int64_t row_bytes, int64_t row0, const int32_t* list,
+                                    int64_t count, int64_t rows_out, void* dst, int sms, cudaStream_t stream) {
+  if (row_bytes % 16 != 0 || rows_out < count) return cudaErrorInvalidValue;
+  gather_rows_list_kernel<<<sms * 4, 256, 0, stream>>>(static_cast<const uint8_t*>(src), row_bytes, row0, list, count,
+                                                       rows_out, static_cast<uint8_t*>(dst));
   return cudaGetLastError();
 }
 
@@ -163,6 +237,7 @@ __global__ void batch_copy_kernel(const BatchHeader* __restrict__ hdr, const Bat
   for (int j = 0; j < nj; j++) {
     const BatchRowJob& J = jobs[j];
     if (blockIdx.x == 0 && threadIdx.x == 0 && J.flag) *J.flag = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && J.maxes) J.maxes[0] = J.maxes[1] = 0u;
     uint8_t* dst = f32 ? reinterpret_cast<uint8_t*>(J.x) : J.xb;
     const int64_t ld_bytes = f32 ? J.ld * 4 : J.ldb;
     if (J.row_bytes % 4 == 0) {
@@ -211,15 +286,56 @@ __global__ void batch_normalize_kernel(const BatchHeader* __restrict__ hdr, cons
   }
 }
 
-__global__ void batch_to_bf16_kernel(const BatchHeader* __restrict__ hdr, const BatchRowJob* __restrict__ jobs) {
+__global__ void batch_to_half_kernel(const BatchHeader* __restrict__ hdr, const BatchRowJob* __restrict__ jobs) {
   const int nj = hdr->n_jobs;
   for (int j = 0; j < nj; j++) {
     const BatchRowJob& J = jobs[j];
     const int64_t lde = J.ldb / 2, total = J.rows * lde;
-    __nv_bfloat16* Y = reinterpret_cast<__nv_bfloat16*>(J.xb);
+    uint16_t* Y = reinterpret_cast<uint16_t*>(J.xb);
     for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total; e += int64_t(gridDim.x) * blockDim.x) {
       const int64_t r = e / lde, c = e % lde;
-      Y[e] = __float2bfloat16_rn(c < J.dim ? J.x[r * J.ld + c] : 0.0f);
+      Y[e] = half_bits((c < J.dim && r < J.n) ? J.x[r * J.ld + c] : 0.0f, J.half_type);
+    }
+  }
+}
+
+// The certificate's row norms of every f32 request (warp per row, as
+// to_half_kernel computes them).
+__global__ void batch_half_norms_kernel(const BatchHeader* __restrict__ hdr, const BatchRowJob* __restrict__ jobs) {
+  const int nj = hdr->n_jobs;
+  const int64_t total = hdr->total_rows;
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = int64_t(gridDim.x) * (blockDim.x >> 5);
+  for (int64_t w = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); w < total; w += warps) {
+    int lo = 0, hi = nj - 1;
+    while (lo < hi) {  // last request with row_base <= w
+      const int mid = (lo + hi + 1) >> 1;
+      if (jobs[mid].row_base <= w) lo = mid;
+      else hi = mid - 1;
+    }
+    const BatchRowJob& J = jobs[lo];
+    if (!J.rnorm) continue;
+    const int64_t r = w - J.row_base;
+    double rr = 0.0, hh = 0.0;
+    for (int c = lane; c < J.dim; c += 32) {
+      const float v = J.x[r * J.ld + c];
+      const float h = half_value(half_bits(v, J.half_type), J.half_type);
+      const double res = double(v) - double(h);
+      rr += res * res;
+      hh += double(h) * double(h);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      rr += __shfl_xor_sync(0xffffffffu, rr, o);
+      hh += __shfl_xor_sync(0xffffffffu, hh, o);
+    }
+    if (lane == 0) {
+      const float a = __double2float_ru(__dsqrt_ru(rr * (1.0 + 0x1p-30)));
+      const float b = __double2float_ru(__dsqrt_ru(hh * (1.0 + 0x1p-30)));
+      J.rnorm[r] = a;
+      J.hnorm[r] = b;
+      atomicMax(&J.maxes[0], __float_as_uint(a));
+      atomicMax(&J.maxes[1], __float_as_uint(b));
     }
   }
 }
@@ -230,7 +346,8 @@ cudaError_t launch_batch_rows(bool f32, const BatchHeader* hdr, const BatchRowJo
   if (!f32) return cudaGetLastError();
   batch_row_norms_kernel<<<grid_norms, kRows, 0, stream>>>(hdr, jobs);
   batch_normalize_kernel<<<grid_rows, 256, 0, stream>>>(hdr, jobs);
-  batch_to_bf16_kernel<<<grid_rows, 256, 0, stream>>>(hdr, jobs);
+  batch_to_half_kernel<<<grid_rows, 256, 0, stream>>>(hdr, jobs);
+  batch_half_norms_kernel<<<grid_norms, kRows, 0, stream>>>(hdr, jobs);
   return cudaGetLastError();
 }
 
@@ -258,7 +375,7 @@ __global__ void fill_random_kernel(int mode, uint8_t* __restrict__ rows, int64_t
     const uint64_t h = fill_hash(seed ^ uint64_t(e));
     if (mode == 0) {
       const float v = live ? float(int32_t(h & 0xffff) - 32768) / 32768.0f : 0.0f;
-      *reinterpret_cast<__nv_bfloat16*>(rows + e) = __float2bfloat16_rn(v);
+      *reinterpret_cast<__half*>(rows + e) = __float2half_rn(v);
     } else if (mode == 1) {
       rows[e] = live ? uint8_t(int8_t(int32_t(h % 255) - 127)) : uint8_t(0);
     } else {

@@ -1,13 +1,35 @@
-// Second stage of the BF16 form: FP32 rerank of the oversampled candidates.
+// Second stage of the 16-bit form: FP32 rerank of the oversampled candidates,
+// and the certificate that the candidates hold the row's true k nearest.
 //
-// The BF16 tensor-core scan (tc_scan.cu) keeps C = oversample*k candidates
-// per row.  Here each warp takes one query row, recomputes the C dot products
-// in FP32 from the original (renormalised) f32 rows, ranks them by the
-// reference's dissimilarity (src/fast_cosine.rs:33-45; self = -1.0) with ties
-// by index, and only for candidates whose FP32 value lies within 1e-6 of the
-// k-th value recomputes the dot product in FP64 to settle the order at the
-// boundary.  Output is the final sorted row with transformed distances
-// (src/knn.rs:156-171).
+// The FP16 (or BF16) tensor-core scan (tc_scan.cu) keeps C = oversample*k
+// candidates per row.  Here each warp takes one query row, recomputes the C
+// dot products in FP32 from the original (renormalised) f32 rows, ranks them
+// by the reference's dissimilarity (src/fast_cosine.rs:33-45; self = -1.0)
+// with ties by index, and only for candidates whose FP32 value lies within
+// 1e-6 of the k-th value recomputes the dot product in FP64 to settle the
+// order at the boundary.  Output is the final sorted row with transformed
+// distances (src/knn.rs:156-171).
+//
+// Certificate.  Every key the scan did not keep scored no better than its
+// C-th kept key (raw value b_C).  With x~, y~ the 16-bit operands and
+// r = x - x~ their residuals (exact in f32), the scan's score of (x, y)
+// differs from the exact dot x.y by at most
+//   E = |r_x| |y~| + |x~| |r_y| + |r_x| |r_y|          (Cauchy-Schwarz on
+//       x.y - x~.y~ = x~.r_y + r_x.y~ + r_x.r_y)
+//     + (L/4 + 2) 2^-21 |x~| |y~|                      (tensor-core f32
+//       accumulation of L products, exact products, at most two units of
+//       2^-22 of the running magnitude lost per four-term step),
+// taking the maxima of |r_y| and |y~| over all keys.  So every key not kept
+// has an exact dissimilarity of at least min(b_C, 0) - E.  The k-th value
+// found here is within e32 = (ceil(d/32) + 8) 2^-24 of exact (this kernel's
+// FP32 summation: ceil(d/32) FMAs per lane and five shuffle additions, on
+// rows of norm at most 1 + 1e-5).  A row is certified when
+//   min(b_C, 0) - E >= min(r_k + e32, 0) - 1e-6,
+// i.e. a key the scan dropped can at most tie the k-th within the 1e-6 the
+// exact FP32 form also allows.  Rows that fail are listed for a second scan
+// with a larger candidate set and, failing that, an exact FP32 scan
+// (evoc_gpu.cu).  FP16 operands (11-bit significands) make E about 8x smaller
+// than BF16 (8-bit) on unit rows, which is what lets nearly every row pass.
 //
 // The candidate rows are gathered from HBM, so the order in which query rows
 // are reranked decides how often those rows are found in L2.  Rows are
@@ -58,16 +80,48 @@ __device__ __forceinline__ void warp_bitonic(uint64_t* keys, int P, int lane) {
 }
 
 __device__ __forceinline__ float key_raw(uint64_t key) { return from_orderable(uint32_t(key >> 32)); }
+
+// The certificate above for one reranked row (kw holds its C sorted keys).
+// Warp-uniform result.
+__device__ __forceinline__ bool certify_row(const CertArgs& ct, const uint64_t* kw, int C, int k, int d,
+                                            int64_t n_keys, int64_t qg, float b_c, int lane) {
+  if (C >= n_keys) return true;  // every key was a candidate
+  bool self_in = false;
+  float worst = -3.0e38f;  // largest FP32 raw value among the k reported
+  bool full = true;
+  for (int j = lane; j < C; j += 32) {
+    const uint64_t key = kw[j];
+    if (key != kKeyInf && key_index(key) == qg) self_in = true;
+    if (j < k) {
+      if (key == kKeyInf) full = false;
+      else worst = fmaxf(worst, key_raw(key));
+    }
+  }
+  self_in = __any_sync(0xffffffffu, self_in);
+  full = __all_sync(0xffffffffu, full);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) worst = fmaxf(worst, __shfl_xor_sync(0xffffffffu, worst, o));
+  if (!self_in || !full || k > C) return false;
+  const double e32 = (double((d + 31) / 32) + 8.0) * 0x1p-24 * 1.0001;
+  const double U = fmin(double(worst) + e32, 0.0);
+  const double rq = ct.rnorm[qg], hq = ct.hnorm[qg];
+  const double rm = double(__uint_as_float(ct.maxes[0])), hm = double(__uint_as_float(ct.maxes[1]));
+  const double E = rq * hm + hq * rm + rq * rm + (double(ct.half_len) / 4.0 + 2.0) * 0x1p-21 * hq * hm;
+  const double LB = fmin(double(b_c), 0.0) - E;
+  return LB >= U - 1e-6 + 1e-12;
+}
 }  // namespace
 
 // One query row: FP32 dot products with its C candidates, a warp bitonic
 // sort of (raw, index) keys, FP64 at the k-th boundary, the sorted row
 // written to output row q.  kw: this warp's P key slots; dw: its 32 doubles.
-__device__ __forceinline__ void rerank_row(const float* __restrict__ X, int ld, int d, int64_t n_keys, int64_t q,
+// With ct (and b_c, the scan's C-th kept raw value), returns whether the row
+// is certified (always true without).
+__device__ __forceinline__ bool rerank_row(const float* __restrict__ X, int ld, int d, int64_t n_keys, int64_t q,
                                            int64_t qg, const int32_t* __restrict__ cq, int C, int P, int k,
                                            int32_t* __restrict__ out_idx, float* __restrict__ out_raw,
                                            float* __restrict__ out_dist, int* status, uint64_t* kw, double* dw,
-                                           int lane) {
+                                           int lane, const CertArgs* ct = nullptr, float b_c = 0.0f) {
   const float* xq = X + qg * ld;
   for (int j0 = 0; j0 < C; j0 += GROUP) {
     int32_t id[GROUP];
@@ -138,6 +192,7 @@ __device__ __forceinline__ void rerank_row(const float* __restrict__ X, int ld, 
       __syncwarp();
     }
   }
+  const bool certified = ct ? certify_row(*ct, kw, C, k, d, n_keys, qg, b_c, lane) : true;
   // Write the row (lane j writes entries j, j+32, ...).
   for (int j = lane; j < k; j += 32) {
     const uint64_t key = j < C ? kw[j] : kKeyInf;
@@ -148,13 +203,14 @@ __device__ __forceinline__ void rerank_row(const float* __restrict__ X, int ld, 
     if (out_dist) out_dist[q * k + j] = transform_raw(0, raw);
   }
   __syncwarp();
+  return certified;
 }
 
 __global__ void __launch_bounds__(RW * 32)
 rerank_f32_kernel(const float* __restrict__ X, int ld, int d, int64_t n, int64_t n_keys, int64_t q_row0,
                   const int32_t* __restrict__ cand, int C, int k, const int32_t* __restrict__ order,
                   int32_t* __restrict__ out_idx, float* __restrict__ out_raw, float* __restrict__ out_dist,
-                  int* status) {
+                  int* status, const CertArgs cert, bool use_cert, bool by_item, int64_t n_out) {
   __shared__ uint64_t keys[RW][MAXC];
   __shared__ double d64[RW][32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -164,12 +220,18 @@ rerank_f32_kernel(const float* __restrict__ X, int ld, int d, int64_t n, int64_t
   while (P < C) P <<= 1;
   for (int64_t w = int64_t(blockIdx.x) * RW + warp; w < n; w += int64_t(gridDim.x) * RW) {
     int64_t q = order ? order[w] : w;  // output row
-    if (q < 0 || q >= n) {               // a malformed order: record it, skip the row
+    if (q < 0 || q >= n_out) {           // a malformed order: record it, skip the row
       if (lane == 0 && status) atomicCAS(status, 0, kStatusBadOrder);
       continue;
     }
-    rerank_row(X, ld, d, n_keys, q, q_row0 + q, cand + q * C, C, P, k, out_idx, out_raw, out_dist, status, keys[warp],
-               d64[warp], lane);
+    const int64_t ci = by_item ? w : q;  // candidate row
+    const bool ok = rerank_row(X, ld, d, n_keys, q, q_row0 + q, cand + ci * C, C, P, k, out_idx, out_raw, out_dist,
+                               status, keys[warp], d64[warp], lane, use_cert ? &cert : nullptr,
+                               use_cert ? cert.bound[ci] : 0.0f);
+    if (!ok && lane == 0) {
+      const int slot = atomicAdd(cert.fail_count, 1);
+      if (slot < cert.fail_cap) cert.fail_list[slot] = int32_t(q);
+    }
   }
 }
 
@@ -199,19 +261,35 @@ batch_rerank_kernel(BatchHeader* hdr, const BatchRowJob* __restrict__ jobs) {
     }
     int P = 1;
     while (P < J.C) P <<= 1;
-    rerank_row(J.x, int(J.ld), int(J.dim), J.n, q, q, J.cand + q * J.C, J.C, P, J.keff, J.out_idx, J.out_raw,
-               J.out_dist, status, keys[warp], d64[warp], lane);
+    CertArgs ct{J.bound, J.rnorm, J.hnorm, J.maxes, int(J.ldb / 2), nullptr, nullptr, 0};
+    const bool ok = rerank_row(J.x, int(J.ld), int(J.dim), J.n, q, q, J.cand + q * J.C, J.C, P, J.keff, J.out_idx,
+                               J.out_raw, J.out_dist, status, keys[warp], d64[warp], lane,
+                               J.certify ? &ct : nullptr, J.certify ? J.bound[q] : 0.0f);
+    if (!ok && lane == 0) {
+      const int slot = atomicAdd(&hdr->fail_count, 1);
+      if (slot < hdr->fail_cap) {
+        hdr->fail_list[2 * slot] = lo;
+        hdr->fail_list[2 * slot + 1] = int32_t(q);
+      }
+    }
   }
 }
 
 cudaError_t launch_rerank_f32(const float* X, int ld, int d, int64_t n, int64_t n_keys, int64_t q_row0,
                               const int32_t* cand, int C, int k, const int32_t* order, int32_t* out_idx, float* out_raw,
-                              float* out_dist, int* status, int sms, cudaStream_t stream) {
+                              float* out_dist, int* status, int sms, cudaStream_t stream, const CertArgs* cert,
+                              bool by_item, int64_t n_out) {
   if (C > MAXC || C < 1) return cudaErrorInvalidValue;
+  if (by_item && !order) return cudaErrorInvalidValue;
+  if (cert && (!cert->bound || !cert->rnorm || !cert->hnorm || !cert->maxes || !cert->fail_list || !cert->fail_count))
+    return cudaErrorInvalidValue;
   int64_t blocks = (n + RW - 1) / RW;
   if (blocks > int64_t(sms) * 16) blocks = int64_t(sms) * 16;
+  CertArgs ct{};
+  if (cert) ct = *cert;
   rerank_f32_kernel<<<unsigned(blocks), RW * 32, 0, stream>>>(X, ld, d, n, n_keys, q_row0, cand, C, k, order,
-                                                               out_idx, out_raw, out_dist, status);
+                                                               out_idx, out_raw, out_dist, status, ct, cert != nullptr,
+                                                               by_item, n_out < 0 ? n : n_out);
   return cudaGetLastError();
 }
 

@@ -1,6 +1,7 @@
 // Blackwell (sm_100a) primitives written as inline PTX: mbarriers with
 // bounded waits, TMA tile loads (no multicast), TMEM allocation and loads,
-// tcgen05.mma (kind::f16 / kind::i8, cta_group::1) and its commit.
+// tcgen05.mma (kind::f16 with FP16 or BF16 operands / kind::i8, cta_group::1) and
+// its commit.
 //
 // Descriptor layouts follow the PTX ISA (tcgen05 "shared memory descriptor"
 // and "instruction descriptor" tables); field positions were checked against
@@ -133,10 +134,13 @@ __device__ __forceinline__ uint64_t sw128_kmajor_desc(uint32_t saddr) {
 }
 
 // Instruction descriptor: dense, A/B K-major, no negation.
-//   c_format [4,6): 1 = F32, 2 = S32;  a/b format [7,10)/[10,13): BF16 = 1 (kind::f16), S8 = 1 (kind::i8)
-//   N >> 3 at [17,23), M >> 4 at [24,29)
+//   c_format [4,6): 1 = F32, 2 = S32;  a/b format [7,10)/[10,13): kind::f16 F16 = 0, BF16 = 1;
+//   kind::i8 S8 = 1.  A and B always carry the same format.  N >> 3 at [17,23), M >> 4 at [24,29)
 __host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N) {
   return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);
+}
+__host__ __device__ constexpr uint32_t idesc_f16_f32(int M, int N) {
+  return (1u << 4) | (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);
 }
 __host__ __device__ constexpr uint32_t idesc_s8_s32(int M, int N) {
   return (2u << 4) | (1u << 7) | (1u << 10) | (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);

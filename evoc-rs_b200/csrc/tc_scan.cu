@@ -3,7 +3,7 @@
 // One persistent CTA per SM walks 128-row query blocks; for each it streams
 // every 256-row key tile through a 4-stage shared-memory pipeline and
 // multiplies on the 5th-generation tensor cores (tcgen05.mma, M=128, N=256,
-// BF16 -> F32 or S8 -> S32), accumulating in TMEM.  Two accumulators let the
+// FP16 or BF16 -> F32, or S8 -> S32), accumulating in TMEM.  Two accumulators let the
 // epilogue read tile t while the MMAs of tile t+1 run.  Nothing of the n x n
 // score matrix is written to HBM: each epilogue thread owns one query row,
 // reads its 256 scores straight from TMEM and offers the few that beat its
@@ -14,8 +14,9 @@
 //   warp 1      TMEM allocator + MMA issuer (one elected lane)
 //   warps 2..5  epilogue; warp w reads TMEM lanes 32*(w%4) .. +31
 //
-// Three score modes share the kernel: BF16 dot products (cosine), int8 dot
-// products, and binary Jaccard, where the packed bits are expanded to 0/1
+// Three score modes share the kernel: 16-bit float dot products (cosine; FP16
+// or BF16 operands, the same instruction and rate), int8 dot products, and
+// binary Jaccard, where the packed bits are expanded to 0/1
 // int8 rows so that the intersection popcount is an exact s8 x s8 -> s32
 // contraction; the epilogue then forms -(inter / union) with union =
 // |a| + |b| - inter from per-row popcounts, as the reference does
@@ -69,6 +70,10 @@ struct ScanParams {
   int* status;       // 0 ok; set non-zero by the first role that gives up
   uint64_t timeout_ns;
   const int32_t* pc; // Jaccard mode: popcount of every row (queries and keys)
+  int half_type;     // 16-bit mode: kHalfF16 or kHalfBf16 operands
+  const int32_t* q_self;  // optional: key index of query i is q_self_base + q_self[i] (gathered query rows)
+  int64_t q_self_base;
+  float* out_bound;  // optional: raw value of the keep-th kept key of each query
   // Batch mode: the work-list of (request, query block) items and the
   // requests' tensor maps and parameters, all in device memory.
   const ScanJob* jobs;
@@ -80,14 +85,14 @@ namespace {
 
 __device__ __forceinline__ void set_status(int* status, int code) { atomicCAS(status, 0, code); }
 
-constexpr int kModeBf16 = 0;     // BF16 dot products, cosine dissimilarity
+constexpr int kModeHalf = 0;     // FP16 / BF16 dot products, cosine dissimilarity
 constexpr int kModeInt8 = 1;     // int8 dot products, -(dot as f32)
 constexpr int kModeJaccard = 2;  // 0/1 int8 rows: intersection counts, -(inter / union)
 
 // Quick-reject threshold as the raw 32-bit score pattern the accumulator holds:
 // a score below it cannot enter the heap.  For int8 it is an s32 lower bound
 // (exact while |dot| < 2^24, loosened by 256 beyond, where f32 rounds); for
-// BF16 it is an f32.  For Jaccard it is a lower bound on the intersection:
+// 16-bit float operands it is an f32.  For Jaccard it is a lower bound on the intersection:
 // J = inter / (pa + pb - inter) <= inter / pa, so a key reaching the heap's
 // similarity t needs inter >= t * pa (taken 1e-6 looser so f32 rounding of J
 // never rejects a key the exact compare would admit).  Passing scores are
@@ -121,7 +126,7 @@ __device__ __forceinline__ uint32_t pass_threshold(const KeyHeap& heap, int32_t 
 
 template <int MODE>
 __device__ __forceinline__ bool passes(uint32_t v, uint32_t thr) {
-  return MODE != kModeBf16 ? (int32_t(v) >= int32_t(thr)) : (__uint_as_float(v) >= __uint_as_float(thr));
+  return MODE != kModeHalf ? (int32_t(v) >= int32_t(thr)) : (__uint_as_float(v) >= __uint_as_float(thr));
 }
 
 // Jaccard dissimilarity from exact counts, as the reference computes it.
@@ -171,7 +176,7 @@ __device__ __forceinline__ void offer_chunk(const uint32_t (&v)[32], uint32_t ma
 template <int MODE>
 __device__ __forceinline__ bool chunk_any(const uint32_t (&v)[32], uint32_t thr) {
   if (MODE == kModeJaccard) return true;
-  if (MODE != kModeBf16) {
+  if (MODE != kModeHalf) {
     int32_t m[16];
 #pragma unroll
     for (int j = 0; j < 16; j++) m[j] = max(int32_t(v[j]), int32_t(v[j + 16]));
@@ -196,7 +201,7 @@ __device__ __forceinline__ uint32_t chunk_mask(const uint32_t (&v)[32], uint32_t
   uint32_t f[4] = {0u, 0u, 0u, 0u};  // fail bits
 #pragma unroll
   for (int j = 0; j < 32; j++) {
-    const uint32_t d = MODE != kModeBf16 ? uint32_t(int32_t(v[j]) - int32_t(thr))
+    const uint32_t d = MODE != kModeHalf ? uint32_t(int32_t(v[j]) - int32_t(thr))
                                          : __float_as_uint(__uint_as_float(v[j]) - __uint_as_float(thr));
     f[j >> 3] = __funnelshift_l(d, f[j >> 3], 1);  // (f << 1) | sign(d)
   }
@@ -213,6 +218,9 @@ struct ItemView {
   float* out_raw;
   float* out_dist;
   const int32_t* pc;
+  const int32_t* q_self;
+  int64_t q_self_base;
+  float* out_bound;
 };
 
 template <bool kBatch>
@@ -237,6 +245,9 @@ __device__ __forceinline__ ItemView item_view(const ScanParams& p, const CUtenso
     v.out_raw = J->out_raw;
     v.out_dist = J->out_dist;
     v.pc = J->pc;
+    v.q_self = nullptr;
+    v.q_self_base = 0;
+    v.out_bound = J->out_bound;
   } else {
     v.ma = tmA;
     v.mb = tmB;
@@ -253,6 +264,9 @@ __device__ __forceinline__ ItemView item_view(const ScanParams& p, const CUtenso
     v.out_raw = p.out_raw;
     v.out_dist = p.out_dist;
     v.pc = p.pc;
+    v.q_self = p.q_self;
+    v.q_self_base = p.q_self_base;
+    v.out_bound = p.out_bound;
   }
   v.n_ktiles = (v.n_k + BN - 1) / BN;
   return v;
@@ -314,11 +328,12 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
 
-  constexpr bool kInt8 = MODE != kModeBf16;
+  constexpr bool kInt8 = MODE != kModeHalf;
   const int64_t n_items = kBatch ? int64_t(*p.n_items) : (p.n_q + BM - 1) / BM;
   const volatile int* abort = p.status;
   constexpr int KC_ELEMS = kInt8 ? KCB : KCB / 2;
-  constexpr uint32_t IDESC = kInt8 ? idesc_s8_s32(BM, BN) : idesc_bf16_f32(BM, BN);
+  const uint32_t IDESC = kInt8 ? idesc_s8_s32(BM, BN)
+                               : (p.half_type == kHalfBf16 ? idesc_bf16_f32(BM, BN) : idesc_f16_f32(BM, BN));
 
   if (warp == 0) {
     // ------------------------------------------------------------ producer
@@ -411,8 +426,9 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     for (int64_t itm = blockIdx.x; ok && itm < n_items; itm += gridDim.x) {
       const ItemView v = item_view<kBatch>(p, &tmA, &tmB, itm);
       const int64_t q = v.qb * BM + row_local;  // output row
-      const int64_t qg = v.q_row0 + q;          // row of the data set
       const bool valid = q < v.n_q;
+      // row of the data set (its key index for the self rule)
+      const int64_t qg = v.q_self ? (valid ? v.q_self_base + v.q_self[q] : -1) : v.q_row0 + q;
       KeyHeap heap;
       heap.init(hstore, v.keep);
       if (valid && v.self_mode && group == 0) heap.offer(make_key(-1.0f, int32_t(qg)));
@@ -487,6 +503,7 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
           v.out_idx[orow + j] = idx;
           if (v.out_raw) v.out_raw[orow + j] = raw;
           if (v.final_mode && v.out_dist) v.out_dist[orow + j] = transform_raw(v.dtype, raw);
+          if (v.out_bound && j == v.keep - 1) v.out_bound[q] = raw;
         }
       }
       if (GROUPS > 1) epilogue_sync(GROUPS * 128);  // heaps are reused by the next block
@@ -522,14 +539,18 @@ PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
 }
 
 // 2-D map over `rows` rows of `row_bytes` (a multiple of 128); box = 128 bytes x box_rows.
-bool make_map(CUtensorMap* m, const void* base, int64_t rows, int64_t row_bytes, int elem_bytes, int box_rows) {
+bool make_map(CUtensorMap* m, const void* base, int64_t rows, int64_t row_bytes, int elem_bytes, int box_rows,
+              int half_type = kHalfF16) {
   auto enc = get_encode();
   if (!enc) return false;
   const cuuint64_t dims[2] = {cuuint64_t(row_bytes / elem_bytes), cuuint64_t(rows)};
   const cuuint64_t strides[1] = {cuuint64_t(row_bytes)};
   const cuuint32_t box[2] = {cuuint32_t(KCB / elem_bytes), cuuint32_t(box_rows)};
   const cuuint32_t estr[2] = {1, 1};
-  CUresult r = enc(m, elem_bytes == 2 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_UINT8, 2,
+  const CUtensorMapDataType dt = elem_bytes == 1          ? CU_TENSOR_MAP_DATA_TYPE_UINT8
+                                 : half_type == kHalfBf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                                          : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+  CUresult r = enc(m, dt, 2,
                    const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                    CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
@@ -607,19 +628,23 @@ cudaError_t launch_tc_scan(int mode, const void* Q, int64_t q_rows, int64_t q_ro
                            int64_t k_rows, int64_t n_k, int64_t row_bytes, int keep, uint64_t* scratch, int grid,
                            int self_mode, int final_mode, int dtype, int32_t* out_idx, float* out_raw, float* out_dist,
                            int* status, uint64_t timeout_ns, const int32_t* pc, cudaStream_t stream,
-                           int variant) {
+                           int variant, int half_type, const int32_t* q_self, float* out_bound,
+                           int64_t q_self_base) {
   // q_rows / k_rows: rows present in memory (multiples of the box heights);
   // n_q / n_k: rows that take part.  Rows past n are zero and never offered.
   if (row_bytes % KCB != 0 || n_q <= 0 || n_k <= 0 || keep < 1) return cudaErrorInvalidValue;
   if (q_row0 < 0 || q_rows < q_row0 + n_q || k_rows < n_k || q_rows % BN != 0 || k_rows % BN != 0)
     return cudaErrorInvalidValue;
   if ((reinterpret_cast<uintptr_t>(Q) & 15) || (reinterpret_cast<uintptr_t>(K) & 15)) return cudaErrorInvalidValue;
-  if (mode < kModeBf16 || mode > kModeJaccard) return cudaErrorInvalidValue;
+  if (mode < kModeHalf || mode > kModeJaccard) return cudaErrorInvalidValue;
   // Jaccard reads one popcount per query row and key row: queries are keys.
   if (mode == kModeJaccard && (!pc || !self_mode || Q != K)) return cudaErrorInvalidValue;
-  const int eb = mode == kModeBf16 ? 2 : 1;
+  if (half_type != kHalfF16 && half_type != kHalfBf16) return cudaErrorInvalidValue;
+  if (q_self && q_row0 != 0) return cudaErrorInvalidValue;
+  const int eb = mode == kModeHalf ? 2 : 1;
   alignas(64) CUtensorMap ma, mb;
-  if (!make_map(&ma, Q, q_rows, row_bytes, eb, BM) || !make_map(&mb, K, k_rows, row_bytes, eb, BN))
+  if (!make_map(&ma, Q, q_rows, row_bytes, eb, BM, half_type) ||
+      !make_map(&mb, K, k_rows, row_bytes, eb, BN, half_type))
     return cudaErrorInvalidValue;
   ScanParams p{};
   p.n_q = n_q;
@@ -637,9 +662,13 @@ cudaError_t launch_tc_scan(int mode, const void* Q, int64_t q_rows, int64_t q_ro
   p.status = status;
   p.timeout_ns = timeout_ns;
   p.pc = pc;
+  p.half_type = half_type;
+  p.q_self = q_self;
+  p.q_self_base = q_self_base;
+  p.out_bound = out_bound;
   if (mode == kModeInt8) return launch_mode<kModeInt8>(ma, mb, p, grid, variant, stream);
   if (mode == kModeJaccard) return launch_mode<kModeJaccard>(ma, mb, p, grid, variant, stream);
-  return launch_mode<kModeBf16>(ma, mb, p, grid, variant, stream);
+  return launch_mode<kModeHalf>(ma, mb, p, grid, variant, stream);
 }
 
 bool tc_scan_variant_feasible(int variant, int keep, bool has_scratch) {
@@ -660,12 +689,14 @@ const char* tc_scan_variant_name(int variant) {
 // Batches: one persistent launch over the work-list of many requests.
 // ---------------------------------------------------------------------------
 bool encode_scan_job(ScanJob* sj, int mode, const void* rows, int64_t rows_mem, int64_t n, int64_t row_bytes,
-                     int keep, int final_mode, int dtype, int32_t* out_idx, float* out_raw, float* out_dist) {
-  if (mode != kModeBf16 && mode != kModeInt8) return false;
+                     int keep, int final_mode, int dtype, int32_t* out_idx, float* out_raw, float* out_dist,
+                     float* out_bound, int half_type) {
+  if (mode != kModeHalf && mode != kModeInt8) return false;
   if (row_bytes % KCB != 0 || n <= 0 || keep < 1 || rows_mem < n || rows_mem % BN != 0) return false;
   if (reinterpret_cast<uintptr_t>(rows) & 15) return false;
-  const int eb = mode == kModeBf16 ? 2 : 1;
-  if (!make_map(&sj->ma, rows, rows_mem, row_bytes, eb, BM) || !make_map(&sj->mb, rows, rows_mem, row_bytes, eb, BN))
+  const int eb = mode == kModeHalf ? 2 : 1;
+  if (!make_map(&sj->ma, rows, rows_mem, row_bytes, eb, BM, half_type) ||
+      !make_map(&sj->mb, rows, rows_mem, row_bytes, eb, BN, half_type))
     return false;
   sj->n_q = n;
   sj->n_k = n;
@@ -680,6 +711,7 @@ bool encode_scan_job(ScanJob* sj, int mode, const void* rows, int64_t rows_mem, 
   sj->out_raw = out_raw;
   sj->out_dist = out_dist;
   sj->pc = nullptr;
+  sj->out_bound = out_bound;
   return true;
 }
 
@@ -733,9 +765,9 @@ cudaError_t launch_batch_mode(const ScanParams& p, int max_keep, int grid, cudaS
 
 cudaError_t prepare_tc_scan_batch(int mode, int max_keep) {
   size_t smem = 0;
-  if (mode == kModeBf16) {
-    const int v = batch_variant<kModeBf16>(max_keep, &smem);
-    return v < 0 ? cudaErrorInvalidValue : set_batch_attr<kModeBf16>(v);
+  if (mode == kModeHalf) {
+    const int v = batch_variant<kModeHalf>(max_keep, &smem);
+    return v < 0 ? cudaErrorInvalidValue : set_batch_attr<kModeHalf>(v);
   }
   if (mode == kModeInt8) {
     const int v = batch_variant<kModeInt8>(max_keep, &smem);
@@ -745,15 +777,16 @@ cudaError_t prepare_tc_scan_batch(int mode, int max_keep) {
 }
 
 cudaError_t launch_tc_scan_batch(int mode, BatchHeader* hdr, const ScanJob* jobs, const ScanItem* items,
-                                 int max_keep, int grid, uint64_t timeout_ns, cudaStream_t stream) {
+                                 int max_keep, int grid, uint64_t timeout_ns, cudaStream_t stream, int half_type) {
   ScanParams p{};
+  p.half_type = half_type;
   p.heap_stride = max_keep | 1;
   p.status = &hdr->status;
   p.timeout_ns = timeout_ns;
   p.jobs = jobs;
   p.items = items;
   p.n_items = &hdr->n_items;
-  if (mode == kModeBf16) return launch_batch_mode<kModeBf16>(p, max_keep, grid, stream);
+  if (mode == kModeHalf) return launch_batch_mode<kModeHalf>(p, max_keep, grid, stream);
   if (mode == kModeInt8) return launch_batch_mode<kModeInt8>(p, max_keep, grid, stream);
   return cudaErrorInvalidValue;
 }

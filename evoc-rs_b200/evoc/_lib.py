@@ -28,7 +28,9 @@ EVOC_ERR_PENDING = 9
 DTYPE_F32, DTYPE_I8, DTYPE_U8 = 0, 1, 2
 FORM_AUTO, FORM_FP32, FORM_BF16_RERANK, FORM_EXACT_INT, FORM_NNDESCENT, FORM_POPCOUNT = 0, 1, 2, 3, 4, 5
 FORM_NAMES = {"auto": FORM_AUTO, "fp32": FORM_FP32, "bf16_rerank": FORM_BF16_RERANK,
-              "exact_int": FORM_EXACT_INT, "nndescent": FORM_NNDESCENT, "popcount": FORM_POPCOUNT}
+              "half_rerank": FORM_BF16_RERANK, "exact_int": FORM_EXACT_INT, "nndescent": FORM_NNDESCENT,
+              "popcount": FORM_POPCOUNT}
+SCAN_TYPES = {"fp16": 0, "bf16": 1}
 
 
 class Opts(C.Structure):
@@ -44,7 +46,11 @@ class Opts(C.Structure):
         ("delta_improv", C.c_float),
         ("row_begin", C.c_int64),
         ("row_end", C.c_int64),
-        ("reserved", C.c_int32 * 4),
+        ("strict_precision", C.c_int32),
+        ("scan_type", C.c_int32),
+        ("brute_force_max_n", C.c_int64),
+        ("certify", C.c_int32),
+        ("reserved", C.c_int32 * 3),
     ]
 
 
@@ -81,6 +87,7 @@ def lib():
             L.evoc_gpu_profile_count.argtypes = [P]
             L.evoc_gpu_profile_stage.argtypes = [P, C.c_int, C.c_char_p, C.c_int, C.POINTER(C.c_float)]
             L.evoc_gpu_last_launch_count.argtypes = [P]
+            L.evoc_gpu_last_certify.argtypes = [P, C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)]
             _bind_optional(L)
             _lib = L
     return _lib
@@ -108,6 +115,8 @@ def _bind_optional(L) -> None:
                                                       C.POINTER(NumpyRng), P, i64, i32, P]
         L.evoc_gpu_node_embedding.argtypes = [P, P, P, P, i64, i32, i32, P, f32, f32, f32, C.POINTER(NumpyRng),
                                               i32, i32, P]
+    if hasattr(L, "evoc_gpu_boruvka_mst"):
+        L.evoc_gpu_boruvka_mst.argtypes = [P, P, i64, i32, i32, i32, P, P, C.POINTER(i64)]
     if hasattr(L, "evoc_npy_open"):
         L.evoc_npy_open.argtypes = [C.c_char_p, C.POINTER(NpyArray)]
         L.evoc_npz_open.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(NpyArray)]
@@ -234,6 +243,13 @@ class Context:
 
     def launches(self) -> int:
         return int(lib().evoc_gpu_last_launch_count(self.h))
+
+    def certify_counts(self) -> dict:
+        """Rows the last 16-bit-form call certified (checked), rescanned with 256 candidates
+        (second_pass), and rescanned exactly in FP32 (exact_rescan)."""
+        a, b, c = C.c_int64(0), C.c_int64(0), C.c_int64(0)
+        lib().evoc_gpu_last_certify(self.h, C.byref(a), C.byref(b), C.byref(c))
+        return {"checked": a.value, "second_pass": b.value, "exact_rescan": c.value}
 
     def close(self) -> None:
         if self.h:

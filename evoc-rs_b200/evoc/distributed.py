@@ -13,6 +13,7 @@ runs the same code on CPU, which the tests use).
 """
 from __future__ import annotations
 
+import os
 from dataclasses import replace
 from typing import Callable, Optional
 
@@ -32,6 +33,18 @@ def shard_rows(n: int, world: int, rank: int) -> tuple[int, int]:
     return min(n, lo * BLOCK), min(n, hi * BLOCK)
 
 
+def rank_device(options: KnnGraphOptions) -> int:
+    """The GPU a rank computes on: options.device when set, else the device torch made current
+    (torchrun ranks call torch.cuda.set_device(LOCAL_RANK)), else LOCAL_RANK."""
+    if options.device is not None:
+        return int(options.device)
+    import torch
+
+    if torch.cuda.is_available() and torch.cuda.is_initialized():
+        return int(torch.cuda.current_device())
+    return int(os.environ.get("LOCAL_RANK", "0"))
+
+
 def _local_gpu(data: EmbeddingData, options: KnnGraphOptions, begin: int, end: int):
     from .knn import knn_graph
 
@@ -41,9 +54,9 @@ def _local_gpu(data: EmbeddingData, options: KnnGraphOptions, begin: int, end: i
 def knn_graph_sharded(data, options: KnnGraphOptions, rng=None, *, group=None,
                       compute: Optional[Callable] = None):
     """The whole (indices, distances) graph on every rank, each rank computing its query-row shard.
-    `compute(data, options, begin, end)` builds one shard (default: the GPU library); it must
-    return int32 (end-begin, k) indices and f32 distances.  The caller's RandomState is advanced by
-    knn_graph's draws, as on one GPU."""
+    `compute(data, options, begin, end)` builds one shard (default: the GPU library) on the rank's
+    device (options.device, resolved by rank_device); it must return int32 (end-begin, k) indices
+    and f32 distances.  The caller's RandomState is advanced by knn_graph's draws, as on one GPU."""
     import torch
     import torch.distributed as dist
 
@@ -59,6 +72,7 @@ def knn_graph_sharded(data, options: KnnGraphOptions, rng=None, *, group=None,
     rank = dist.get_rank(group)
     k = max(1, min(options.n_neighbors, n - 1))
     begin, end = shard_rows(n, world, rank)
+    options = replace(options, device=rank_device(options))
     if end > begin:
         ind, dst = (compute or _local_gpu)(data, options, begin, end)
     else:
@@ -66,7 +80,7 @@ def knn_graph_sharded(data, options: KnnGraphOptions, rng=None, *, group=None,
     # Gather the slices: pad to the largest shard (shards differ by at most one block).
     largest = max(e - b for b, e in (shard_rows(n, world, r) for r in range(world)))
     backend = dist.get_backend(group)
-    dev = torch.device("cuda", torch.cuda.current_device()) if backend == "nccl" else torch.device("cpu")
+    dev = torch.device("cuda", options.device) if backend == "nccl" else torch.device("cpu")
     pi = torch.full((largest, k), -1, dtype=torch.int32, device=dev)
     pd = torch.zeros((largest, k), dtype=torch.float32, device=dev)
     pi[: end - begin] = torch.from_numpy(np.ascontiguousarray(ind))

@@ -113,11 +113,16 @@ class KnnGraphOptions:
     brute_force_max_n: int = 0
     deterministic: bool = False
     # GPU-only fields
-    form: str = "auto"          # auto | fp32 | bf16_rerank | exact_int | nndescent | popcount
+    form: str = "auto"          # auto | fp32 | bf16_rerank (= half_rerank) | exact_int | nndescent | popcount
     oversample: int = 2         # bf16_rerank: candidates per row = oversample * k
-    device: int = 0
+    scan_type: str = "fp16"     # bf16_rerank: 16-bit operands of the tensor-core scan, fp16 | bf16
+    certify: bool = True        # bf16_rerank: certify every row, rescan the rows that fail
+    device: Optional[int] = None  # CUDA device; None = torch's current device when torch is loaded, else 0
     row_begin: int = 0          # exact forms: query rows [row_begin, row_end) only; 0,0 = all
     row_end: int = 0
+    # RlxBackend::knn_graph's strict_precision (src/rlx_backend/mod.rs:133-144); knn_graph itself
+    # (the crate's free function) has no such argument, so False here
+    strict_precision: bool = False
 
 
 def _n_trees(options: KnnGraphOptions) -> int:
@@ -139,7 +144,24 @@ def _to_opts(options: KnnGraphOptions, on_device: bool = False) -> _lib.Opts:
     o.delta_improv = float(options.delta_improv)
     o.row_begin = int(options.row_begin)
     o.row_end = int(options.row_end)
+    o.strict_precision = 1 if options.strict_precision else 0
+    o.scan_type = _lib.SCAN_TYPES[options.scan_type]
+    o.brute_force_max_n = int(options.brute_force_max_n)
+    o.certify = 1 if options.certify else 0
     return o
+
+
+def device_of(options: KnnGraphOptions) -> int:
+    """The CUDA device a call runs on: options.device, else torch's current device (so a process
+    that pinned its GPU with torch.cuda.set_device -- one rank per GPU -- computes there), else 0."""
+    if options.device is not None:
+        return int(options.device)
+    import sys
+
+    torch = sys.modules.get("torch")
+    if torch is not None and torch.cuda.is_available() and torch.cuda.is_initialized():
+        return int(torch.cuda.current_device())
+    return 0
 
 
 def _advance_rng(rng, data: EmbeddingData, options: KnnGraphOptions) -> np.ndarray:
@@ -172,12 +194,16 @@ def knn_graph(data, options: KnnGraphOptions, rng=None, *, return_raw: bool = Fa
         raise InvalidNeighbors()
     if data.nrows() == 0:
         raise EmptyData()
+    if options.strict_precision and not (data.kind != "Float32" and data.nrows() <= options.brute_force_max_n):
+        # refused before any RNG draw (the library refuses the same call with EVOC_ERR_UNSUPPORTED)
+        raise BackendError(_lib.EVOC_ERR_UNSUPPORTED, "strict_precision: only i8/u8 data with n <= "
+                           "brute_force_max_n (the reference's brute-force branch) is bit-identical to Strict")
     tau = _advance_rng(rng, data, options) if rng is not None else np.zeros(3, np.int64)
     arr = np.ascontiguousarray(data.array)
     n, dim = arr.shape
     k = max(1, min(options.n_neighbors, n - 1))
     m = (options.row_end - options.row_begin) if (options.row_begin or options.row_end) else n
-    ctx = _lib.context(options.device)
+    ctx = _lib.context(device_of(options))
     o = _to_opts(options)
     if out is not None:
         ind, dst = out
@@ -213,7 +239,7 @@ def knn_graph_device(ptr: int, dtype_code: int, n: int, dim: int, k: int, out_id
                      out_raw_ptr: int = 0) -> int:
     """Device-pointer entry: all buffers live on the context's GPU (e.g. torch tensors)."""
     options = options or KnnGraphOptions(n_neighbors=k)
-    ctx = _lib.context(options.device)
+    ctx = _lib.context(device_of(options))
     o = _to_opts(options, on_device=True)
     tau = np.zeros(3, np.int64) if tau is None else np.ascontiguousarray(tau, np.int64)
     kout = C.c_int32(0)
@@ -230,7 +256,7 @@ def knn_graph_batch_device(ptrs, dtype_code: int, ns, dims, k: int, out_idx_ptrs
     """Many graphs in one pass (evoc_gpu_knn_graph_batch); every pointer is a device pointer.
     Returns k_eff of each request."""
     options = options or KnnGraphOptions(n_neighbors=k)
-    ctx = _lib.context(options.device)
+    ctx = _lib.context(device_of(options))
     o = _to_opts(options, on_device=True)
     m = len(ptrs)
     P = C.c_void_p
@@ -262,7 +288,7 @@ def knn_graph_batch(datas, options: KnnGraphOptions, rngs=None):
         for x, r in zip(datas, rngs):
             _advance_rng(r, x, options)
     code = datas[0].dtype_code
-    dev = torch.device("cuda", options.device)
+    dev = torch.device("cuda", device_of(options))
     xs = [torch.from_numpy(np.ascontiguousarray(x.array)).to(dev) for x in datas]
     ks = [max(1, min(options.n_neighbors, x.nrows() - 1)) for x in datas]
     oi = [torch.empty((x.nrows(), kk), dtype=torch.int32, device=dev) for x, kk in zip(datas, ks)]

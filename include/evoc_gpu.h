@@ -47,9 +47,12 @@ typedef enum {
 typedef enum {
   EVOC_FORM_AUTO = 0,        /* f32 -> BF16_RERANK; i8/u8 -> EXACT_INT            */
   EVOC_FORM_FP32 = 1,        /* f32 exact search, FP32 SIMT dot products          */
-  EVOC_FORM_BF16_RERANK = 2, /* f32: tcgen05 BF16 scan keeps oversample*k         */
+  EVOC_FORM_BF16_RERANK = 2, /* f32: tcgen05 16-bit scan (FP16 operands by        */
+                             /* default, BF16 with scan_type) keeps oversample*k  */
                              /* candidates per row, reranked in FP32 (FP64 at the */
-                             /* k-th boundary)                                    */
+                             /* k-th boundary); every row certified, rows that    */
+                             /* fail rescanned (see `certify`)                    */
+  EVOC_FORM_HALF_RERANK = 2, /* the same form under its operand-neutral name      */
   EVOC_FORM_EXACT_INT = 3,   /* i8: tcgen05 int8 dots; u8: tcgen05 int8 on bits  */
                              /* expanded to 0/1 bytes (exact intersection counts) */
   EVOC_FORM_NNDESCENT = 4,   /* GPU NN-descent (approximate, all dtypes)          */
@@ -73,7 +76,22 @@ typedef struct {
   int64_t row_begin;         /* exact forms: compute query rows [row_begin,     */
   int64_t row_end;           /* row_end) against all n rows; 0,0 = all rows.    */
                              /* Outputs then hold (row_end-row_begin) rows.     */
-  int32_t reserved[4];
+  int32_t strict_precision;  /* RlxBackend::knn_graph's strict_precision        */
+                             /* (src/rlx_backend/mod.rs:133-144): 1 = the call  */
+                             /* must give the Strict backend's bits or fail.    */
+                             /* Only the brute-force branch below can; every    */
+                             /* other request returns EVOC_ERR_UNSUPPORTED.     */
+  int32_t scan_type;         /* BF16_RERANK operands: 0 FP16 (default), 1 BF16  */
+  int64_t brute_force_max_n; /* KnnGraphOptions.brute_force_max_n: i8/u8 data  */
+                             /* with n <= it take the reference's brute_force_  */
+                             /* knn (src/knn.rs:189-281,418-421): self excluded, */
+                             /* each row in the reference's max-heap order      */
+  int32_t certify;           /* BF16_RERANK: 1 (default) prove for every row    */
+                             /* that the candidates hold its k nearest (within  */
+                             /* the 1e-6 tie tolerance) and rescan rows that    */
+                             /* cannot be proven -- with 256 candidates, then   */
+                             /* exactly in FP32; 0 = skip the certificate       */
+  int32_t reserved[3];
 } evoc_gpu_opts;
 
 typedef struct evoc_gpu_ctx evoc_gpu_ctx;
@@ -298,6 +316,26 @@ void evoc_npy_close(evoc_npy_array* a);
 int evoc_graph_npz_read(const char* path, int64_t* n, int64_t* nnz, int64_t* indptr, int32_t* indices, float* data,
                         int64_t cap);
 
+/*
+ * Minimum spanning tree under mutual-reachability distance, with the core
+ * distances.  Replaces build_kdtree (src/kdtree.rs:367-413) and
+ * parallel_boruvka with reproducible = false (src/boruvka.rs:437-593), which
+ * build_cluster_layers runs on the node embedding (src/clustering.rs:50-80).
+ *   data         n x dim f32 points, row-major (dim 1..32)
+ *   min_samples  core distance = squared distance to the (min_samples + 1)-th
+ *                nearest point, the point itself included; <= 1: zero core
+ *                distances (as the reference); at most 31; n must exceed it
+ *   out_edges    (n - 1) x 3 f32 rows (from, to, distance), distance the
+ *                square root of max(squared distance, core[from], core[to])
+ *   out_core     n f32 squared core distances (may be NULL)
+ *   n_edges      receives n - 1
+ * The total weight and the sorted edge weights equal the reference's; edges
+ * (and their order) can differ where several have equal weight, as they do
+ * between the reference's non-reproducible runs.
+ */
+int evoc_gpu_boruvka_mst(evoc_gpu_ctx* ctx, const float* data, int64_t n, int32_t dim, int32_t min_samples,
+                         int32_t buffers_on_device, float* out_edges, float* out_core, int64_t* n_edges);
+
 /* The context's CUDA stream (a cudaStream_t), for callers that record their
  * own CUDA events around calls.  No counterpart in evoc-rs. */
 void* evoc_gpu_ctx_stream(const evoc_gpu_ctx* ctx);
@@ -312,6 +350,12 @@ int evoc_gpu_profile_stage(const evoc_gpu_ctx* ctx, int i, char* name, int name_
 
 /* Number of kernels the last call launched. */
 int evoc_gpu_last_launch_count(const evoc_gpu_ctx* ctx);
+
+/* Certificate counts of the last BF16_RERANK call on this context: query
+ * rows checked, rows that failed the first certificate (rescanned with 256
+ * candidates), and rows rescanned exactly in FP32 after failing the second.
+ * No counterpart in evoc-rs. */
+int evoc_gpu_last_certify(const evoc_gpu_ctx* ctx, int64_t* checked, int64_t* second_pass, int64_t* exact_rescan);
 
 /*
  * Exact FP32 kNN that allocates no device memory.  It has no counterpart in

@@ -38,6 +38,8 @@ def test_version_and_default_opts(libpath):
     assert o.struct_size == C.sizeof(_lib.Opts)
     assert o.form == _lib.FORM_AUTO and o.oversample == 2
     assert abs(o.delta - 0.001) < 1e-9 and abs(o.delta_improv - 0.001) < 1e-9
+    assert o.scan_type == 0 and o.certify == 1  # FP16 operands, every row certified
+    assert o.strict_precision == 0 and o.brute_force_max_n == 0  # KnnGraphOptions' default (src/knn.rs:72)
 
 
 def test_null_context_is_rejected(libpath):

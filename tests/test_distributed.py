@@ -44,6 +44,8 @@ def _data(n, d, seed):
 def _oracle_shard(data, options, begin, end):
     from oracle import oracle as O
 
+    # the shard is built on the rank's own GPU: LOCAL_RANK here (no CUDA in these processes)
+    assert options.device == int(os.environ["LOCAL_RANK"]), (options.device, os.environ["LOCAL_RANK"])
     x = data.array
     k = max(1, min(options.n_neighbors, len(x) - 1))
     ind, raw = O.exact_knn(x, k, begin, end)
@@ -58,6 +60,7 @@ def _rank_main(rank, world, port, n, d, k, out_dir, fail_rank):
 
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
+    os.environ["LOCAL_RANK"] = str(rank)
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=6))
     try:
         if rank == fail_rank:
@@ -140,7 +143,8 @@ def _gpu_rank_main(rank, world, port, out_dir):
     try:
         x = _data(3000, 96, 8)
         for form in ("bf16_rerank", "fp32"):
-            ind, dst = knn_graph_sharded(x, evoc.KnnGraphOptions(n_neighbors=15, form=form))
+            # one GPU here, so both ranks name device 0 explicitly
+            ind, dst = knn_graph_sharded(x, evoc.KnnGraphOptions(n_neighbors=15, form=form, device=0))
             np.savez(os.path.join(out_dir, f"gpu_{form}_rank{rank}.npz"), ind=ind, dst=dst)
     finally:
         dist.destroy_process_group()
