@@ -486,26 +486,17 @@ def sampled_exact_check(x, oi, oraw, k, kind, rows=128):
     return {"rows": int(len(q)), "indices_exact": ok_i, "raw_exact": ok_r}
 
 
-def run_exact_int(args, world, rank, local):
-    """C3 / C4: the exact integer forms (int8 dots; binary Jaccard on 0/1-expanded int8 rows)."""
+def exact_int_leg(workload, n, d, k, dev, local, rank, world, pg, steps, warmup, e2e_steps, check_rows, cpu_rows,
+                  autotune=True):
+    """C3 / C4: the exact integer forms (int8 dots; binary Jaccard on 0/1-expanded int8 rows) on one
+    workload; returns its JSON object (value, e2e, roofline, sampled exactness, CPU baseline)."""
     import numpy as np
     import torch
 
     import evoc
     from evoc import _lib, synthetic
 
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    pg = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
-        pg = dist
-    n, d, k = args.n, args.dim, args.k
-    i8 = args.workload == "gmm_i8"
+    i8 = workload == "gmm_i8"
     if i8:
         x = synthetic.gmm_i8(n=n, dim=d, seed=11 + rank, device=dev)
         code, stage, kind = _lib.DTYPE_I8, "int8_scan", "i8"
@@ -522,24 +513,24 @@ def run_exact_int(args, world, rank, local):
     ctx.profile(True)
     stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=dev)
     opts = evoc.KnnGraphOptions(n_neighbors=k, form="exact_int", device=local)
-    tuned = evoc.autotune("Int8" if i8 else "UInt8", n, d, k, "exact_int", device=local) if args.autotune else None
+    tuned = evoc.autotune("Int8" if i8 else "UInt8", n, d, k, "exact_int", device=local) if autotune else None
 
     def step():
         evoc.knn_graph_device(x.data_ptr(), code, n, d, k, oi.data_ptr(), od.data_ptr(), opts,
                               out_raw_ptr=oraw.data_ptr())
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         step()
     gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
     os.makedirs(OUT_DIR, exist_ok=True)
-    clocks = ClockSampler(gpu_id, os.path.join(OUT_DIR, f"clocks_rank{rank}.csv"))
+    clocks = ClockSampler(gpu_id, os.path.join(OUT_DIR, f"clocks_{workload}_rank{rank}.csv"))
     if pg:
         pg.barrier()
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     stage_ms, launches = {}, 0
     ev0.record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         step()
         for name, ms in ctx.stages():
             stage_ms.setdefault(name, []).append(ms)
@@ -549,13 +540,13 @@ def run_exact_int(args, world, rank, local):
     if pg:
         pg.barrier()
     clk = clocks.stop()
-    ms_step = ev0.elapsed_time(ev1) / args.steps
+    ms_step = ev0.elapsed_time(ev1) / steps
     if pg:
         t = torch.tensor([ms_step], device=dev)
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         ms_step = float(t.item())
     value = world * n * k / (ms_step / 1000.0)
-    check = sampled_exact_check(x, oi, oraw, k, kind, rows=args.check_rows)
+    check = sampled_exact_check(x, oi, oraw, k, kind, rows=check_rows)
 
     # End to end through the public API with pinned host buffers.
     xh = torch.empty(x.shape, dtype=x.dtype, pin_memory=True)
@@ -567,11 +558,11 @@ def run_exact_int(args, world, rank, local):
         pg.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(args.e2e_steps):
+    for _ in range(e2e_steps):
         evoc.knn_graph(xh_np, opts, None, out=(ih_np, dh_np))
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1) / args.e2e_steps
+    e2e_ms = e0.elapsed_time(e1) / e2e_steps
     if pg:
         t = torch.tensor([e2e_ms], device=dev)
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
@@ -587,11 +578,11 @@ def run_exact_int(args, world, rank, local):
                 "launch_ms": scan_ms, "ops_per_launch": ops_per_pair * n * n}
 
     cpu = None
-    if rank == 0 and world == 1 and args.cpu_rows > 0:
+    if rank == 0 and world == 1 and cpu_rows > 0:
         from oracle import oracle as O
 
         threads = os.cpu_count() or 1
-        rows = min(args.cpu_rows, n)
+        rows = min(cpu_rows, n)
         xs = x[:rows].cpu().numpy()
         O.build()
         O.set_num_threads(threads)
@@ -608,10 +599,10 @@ def run_exact_int(args, world, rank, local):
 
     metric = METRIC_INT.format(kind="Int8" if i8 else "Binary (UInt8)")
     line = {
-        "metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": warmup,
         "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "int8" if i8 else "u8 (expanded to 0/1 int8)", "data": "synthetic (generated on device, seeded)",
-        "config": {"workload": WORKLOADS[args.workload][3], "n": n, "d": d, "k": k, "form": "exact_int",
+        "config": {"workload": WORKLOADS[workload][3], "n": n, "d": d, "k": k, "form": "exact_int",
                    "l2": f"inputs larger than L2 ({x.numel() / 1e9:.2f} GB vs 126 MB)",
                    "per_rank": "independent graph per rank"},
         "sampled_exact_check": check,
@@ -624,12 +615,199 @@ def run_exact_int(args, world, rank, local):
         "clocks": clk,
         "gpu_launches": launches,
     }
+    del x, oi, od, oraw, xh, ih, dh
+    torch.cuda.empty_cache()
+    return line
+
+
+def run_exact_int(args, world, rank, local):
+    """--workload gmm_i8 / bits: the exact integer forms as the headline line."""
+    import torch
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+        pg = dist
+    line = exact_int_leg(args.workload, args.n, args.dim, args.k, dev, local, rank, world, pg, args.steps,
+                         args.warmup, args.e2e_steps, args.check_rows, args.cpu_rows, bool(args.autotune))
     if rank == 0:
         print(json.dumps(line), flush=True)
     if pg:
         pg.barrier()
         pg.destroy_process_group()
     return 0
+
+
+def deterministic_cpu_baseline(x_host, k, rows):
+    """The reference's deterministic path on one thread (knn_graph with deterministic = true: RP forest
+    and sorted NN-descent on a 1-thread pool, src/knn.rs:345-359) with the reference's own compiled
+    native/fast_cosine.c as the distance when oracle/_ref holds it; on the first `rows` rows."""
+    from oracle import oracle as O
+
+    O.build()
+    ref = O.use_reference_cosine(True)
+    O.set_num_threads(1)
+    sub = x_host[:rows].copy()
+    t0 = time.perf_counter()
+    ind, _ = O.knn_graph(sub, k, O.RandomState(7), deterministic=True, n_threads=1)
+    t = time.perf_counter() - t0
+    O.use_reference_cosine(False)
+    return t, ind, ref
+
+
+def recall_on_host(x, ind, k, rows):
+    """recall@k of `ind` (rows 0..rows-1 of x, self first) against FP64 brute force, on the host."""
+    import numpy as np
+
+    x64 = x.astype(np.float64)
+    hits = 0
+    for r0 in range(0, rows, 512):
+        r1 = min(rows, r0 + 512)
+        s = x64[r0:r1] @ x64.T
+        s[np.arange(r1 - r0), np.arange(r0, r1)] = 2.0
+        top = np.argpartition(-s, k - 1, axis=1)[:, :k]
+        hits += sum(len(set(top[i]) & set(ind[r0 + i][:k])) for i in range(r1 - r0))
+    return hits / (rows * k)
+
+
+def blobs_leg(dev, local, steps=20, warmup=5):
+    """C1: 2,000 x 128 f32, 10 Gaussian blobs (sigma 0.3), k=15, seed 42 -- the reference's own
+    CPU-runnable case: edges/s of the default (FP16 scan + FP32 rerank) form with the rows resident,
+    end to end with host buffers, parity against the oracle's exact selection, and the reference's
+    deterministic path (single thread) on the same rows."""
+    import numpy as np
+    import torch
+
+    import evoc
+    from evoc import _lib, synthetic
+    from oracle import oracle as O
+
+    x = synthetic.blobs_2k_128()
+    n, d, k = x.shape[0], x.shape[1], 15
+    xd = torch.from_numpy(x).to(dev)
+    oi = torch.empty((n, k), dtype=torch.int32, device=dev)
+    od = torch.empty((n, k), dtype=torch.float32, device=dev)
+    oraw = torch.empty((n, k), dtype=torch.float32, device=dev)
+    ctx = _lib.context(local)
+    ctx.profile(True)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=dev)
+    opts = evoc.KnnGraphOptions(n_neighbors=k, form="bf16_rerank", device=local)
+
+    def step():
+        evoc.knn_graph_device(xd.data_ptr(), 0, n, d, k, oi.data_ptr(), od.data_ptr(), opts,
+                              out_raw_ptr=oraw.data_ptr())
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches, scan = 0, []
+    ev0.record(stream)
+    for _ in range(steps):
+        step()
+        launches += ctx.launches()
+        scan.append(dict(ctx.stages()).get("bf16_scan", float("nan")))
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / steps
+    cert = ctx.certify_counts()
+    ind, raw = oi.cpu().numpy(), oraw.cpu().numpy()
+    ei, er = O.exact_knn(x, k)
+    same = ind == ei
+    x64 = x.astype(np.float64)
+    dots = np.einsum("rkd,rd->rk", x64[ind], x64)
+    want = np.where(dots > 0, -dots, 1.17549435e-38)
+    want[ind == np.arange(n)[:, None]] = -1.0
+    xh = torch.empty((n, d), dtype=torch.float32, pin_memory=True)
+    xh.copy_(xd)
+    ih = torch.empty((n, k), dtype=torch.int32, pin_memory=True)
+    dh = torch.empty((n, k), dtype=torch.float32, pin_memory=True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    evoc.knn_graph(xh.numpy(), opts, None, out=(ih.numpy(), dh.numpy()))
+    e0.record(stream)
+    for _ in range(steps):
+        evoc.knn_graph(xh.numpy(), opts, None, out=(ih.numpy(), dh.numpy()))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / steps
+    t, cind, ref = deterministic_cpu_baseline(x, k, n)
+    crec = float(np.mean([len(set(cind[r]) & set(ei[r])) / k for r in range(n)]))
+    scan_ms = statistics.median(scan)
+    peaks, peak_kind = measured_peaks()
+    flops = 2.0 * n * n * d
+    return {
+        "workload": "blobs_2k_128: 2,000 x 128 f32, 10 N(0,1) centres, sigma 0.3, L2-normalised, k=15, seed 42",
+        "value": n * k / (ms / 1000.0), "unit": UNIT, "ms_per_step": ms, "steps": steps, "warmup": warmup,
+        "form": "fp16 tensor-core scan + fp32 rerank (certified)", "certificate": cert,
+        "parity": {"recall_at_k_vs_oracle_exact": float(np.mean([len(set(ind[r]) & set(ei[r])) / k for r in range(n)])),
+                   "indices_equal_to_oracle": int(same.sum()), "entries": int(same.size),
+                   "max_abs_raw_err_vs_fp64": float(np.abs(raw.astype(np.float64) - want).max()),
+                   "max_abs_raw_diff_vs_oracle": float(np.abs(raw.astype(np.float64) - er).max())},
+        "roofline": {"bound": "latency", "achieved": flops / (scan_ms / 1e3) / 1e12, "unit": "TFLOP/s",
+                     "peak": float(peaks.get("bf16_tflops")), "peak_kind": f"{peak_kind} bf16 burst",
+                     "frac": flops / (scan_ms / 1e3) / 1e12 / float(peaks.get("bf16_tflops")),
+                     "launch_ms": scan_ms, "traffic": None,
+                     "note": "16 query blocks of 128 rows: 16 of 148 SMs busy, launch/latency-bound by size"},
+        "e2e": {"value": n * k / (e2e_ms / 1000.0), "unit": UNIT, "h2d_bytes_per_step": n * d * 4,
+                "d2h_bytes_per_step": n * k * 8, "ms_per_step": e2e_ms},
+        "cpu_baseline": {"value": n * k / t, "unit": UNIT, "cores": 1, "kind": "reference" if ref else "port",
+                         "sample": (f"the reference's deterministic path (RP forest + sorted NN-descent, one "
+                                    f"thread) restated in oracle/, distance = "
+                                    f"{'the reference native/fast_cosine.c compiled unchanged' if ref else 'its restatement'}"
+                                    f", all {n} rows: {t:.2f} s; recall@{k} vs exact {crec:.4f}")},
+        "gpu_launches": launches,
+    }
+
+
+def mst_leg(emb, n, ncomp, dev, ctx, cpu_rows, min_samples=5):
+    """Borůvka MST of the node embedding under mutual reachability (build_cluster_layers' input,
+    src/clustering.rs:50-80) on the device, with the oracle's (the reference's reproducible Borůvka,
+    restated) timed on a prefix of the same points and both MSTs' weights compared there."""
+    import numpy as np
+    import torch
+
+    from evoc import boruvka as BV
+
+    edges = torch.empty((n - 1, 3), dtype=torch.float32, device=dev)
+    core = torch.empty(n, dtype=torch.float32, device=dev)
+    emb = emb.contiguous()
+    BV.parallel_boruvka_device(emb.data_ptr(), n, ncomp, min_samples, edges.data_ptr(), core.data_ptr(),
+                               device=ctx.device)
+    runs = []
+    for _ in range(2):
+        BV.parallel_boruvka_device(emb.data_ptr(), n, ncomp, min_samples, edges.data_ptr(), core.data_ptr(),
+                                   device=ctx.device)
+        runs.append((dict(ctx.stages()), ctx.launches()))
+    ms = statistics.median(r[0]["total"] for r in runs)
+    out = {"metric": "points/s through the MST (KD-tree, core distances, Boruvka rounds)",
+           "value": n / (ms / 1000.0), "unit": "points/s", "ms": ms, "points": n, "dim": ncomp,
+           "min_samples": min_samples, "mode": "non-reproducible (atomic component bounds)",
+           "stages_ms": {nm: statistics.median(r[0][nm] for r in runs) for nm in runs[0][0] if nm != "total"},
+           "gpu_launches": runs[-1][1]}
+    m = min(cpu_rows, n)
+    if m > 1:
+        from oracle import mst as OM
+
+        sub = emb[:m].cpu().numpy()
+        t0 = time.perf_counter()
+        oe, oc, _ = OM.boruvka_mst(sub, min_samples=min_samples)
+        to = time.perf_counter() - t0
+        ge, gc = BV.parallel_boruvka(sub, min_samples, device=ctx.device, return_core=True)
+        gw, ow = np.sort(ge[:, 2].astype(np.float64)), np.sort(oe[:, 2].astype(np.float64))
+        out["cpu_baseline"] = {
+            "value": m / to, "unit": "points/s", "cores": 1, "kind": "port",
+            "sample": (f"oracle restatement of build_kdtree + parallel_boruvka (reproducible, one thread, as "
+                       f"build_cluster_layers runs it for reproducible fits) on the first {m} points: {to:.2f} s")}
+        out["parity_on_cpu_sample"] = {"points": m, "max_abs_sorted_weight_diff": float(np.abs(gw - ow).max()),
+                                       "total_weight_rel_diff": float(abs(gw.sum() - ow.sum()) / ow.sum()),
+                                       "max_abs_core_diff": float(np.abs(gc - oc).max())}
+    return out
 
 
 def run_label_prop(args, dev, ctx, stream, x, f_indptr, f_ind, f_dat, nnz, opts):
@@ -705,6 +883,11 @@ def run_label_prop(args, dev, ctx, stream, x, f_indptr, f_ind, f_dat, nnz, opts)
         "parity": "bit-identical to the oracle (tests/test_label_prop_gpu.py); oracle pinned to the "
                   "reference's golden intermediates",
     }
+    if args.mst:
+        try:
+            res["boruvka_mst"] = mst_leg(emb if args.ne_reps > 0 else out, n, ncomp, dev, ctx, args.cpu_mst_rows)
+        except Exception as e:  # noqa: BLE001 -- reported in the line, the other measurements stand
+            res["boruvka_mst"] = {"error": repr(e)}
     m = min(args.cpu_lp_rows, n)
     if m > 0:
         from oracle import label_prop as OL
@@ -794,6 +977,7 @@ def run_ours(args, world, rank, local):
     if pg:
         pg.barrier()
     clk = clocks.stop()
+    cert = ctx.certify_counts() if form == "bf16_rerank" else None
     total_ms = ev0.elapsed_time(ev1)
     ms_step = total_ms / args.steps
     if pg:
@@ -885,9 +1069,16 @@ def run_ours(args, world, rank, local):
         fms = f0.elapsed_time(f1)
         frec, _ = recall_vs_fp64(x, fi, min(sample, rows), k)
         same = (fi[:sample] == oi[:sample]).float().mean().item()
+        ffma = ctx.peak_ffma()
+        tfl = 2.0 * rows * n * d / (fms / 1000.0) / 1e12
         fp32 = {"value": rows * k / (fms / 1000.0), "unit": UNIT, "query_rows": rows, "key_rows": n,
-                "ms": fms, "recall_at_k_vs_fp64": frec, "index_agreement_with_bf16_form": same,
-                "tflops_fp32": 2.0 * rows * n * d / (fms / 1000.0) / 1e12}
+                "ms": fms, "recall_at_k_vs_fp64": frec, "index_agreement_with_fp16_form": same,
+                "tflops_fp32": tfl,
+                "roofline": {"bound": "fp32 ffma", "achieved": tfl, "peak": ffma, "unit": "TFLOP/s",
+                             "frac": tfl / ffma,
+                             "peak_kind": "measured in this run: hand-written FFMA loop over every SM "
+                                          "(evoc_gpu_peak_ffma)"},
+                "fp16_form_speedup": value / (rows * k / (fms / 1000.0))}
 
     peaks, peak_kind = measured_peaks()
     if form == "bf16_rerank":
@@ -927,6 +1118,18 @@ def run_ours(args, world, rank, local):
                "sample": (f"reference NN-descent restated in oracle/ (rlx-cpu path: serial-order f32 dot, "
                           f"{threads} threads) on the first {args.cpu_rows} rows of the workload; "
                           f"{t:.1f} s; its recall@{k} vs FP64 on {qrows} of those rows {crec:.4f}")}
+    cpu_det = None
+    if rank == 0 and world == 1 and args.cpu_det_rows > 0:
+        rows = min(args.cpu_det_rows, n)
+        xs = x[:rows].cpu().numpy()
+        t, cind, ref = deterministic_cpu_baseline(xs, k, rows)
+        crec = recall_on_host(xs, cind, k, min(2000, rows))
+        cpu_det = {"value": rows * k / t, "unit": UNIT, "cores": 1, "kind": "reference" if ref else "port",
+                   "sample": (f"the reference's deterministic C path: RP forest + sorted NN-descent on one "
+                              f"thread (src/knn.rs deterministic = true) restated in oracle/, distance = "
+                              f"{'native/fast_cosine.c compiled unchanged from the reference' if ref else 'its restatement'}"
+                              f", on the first {rows} rows: {t:.1f} s; recall@{k} vs FP64 on {min(2000, rows)} "
+                              f"of those rows {crec:.4f}")}
 
     metric = METRIC if form == "bf16_rerank" else "kNN edges/s, GPU NN-descent form (recall vs FP64 reported)"
     line = {
@@ -946,13 +1149,148 @@ def run_ours(args, world, rank, local):
         "fuzzy_graph": fuzzy,
         "autotune": tuned and {"variants_ms_65536_rows": tuned["variants_ms"], "chosen": tuned["chosen"]},
         "cpu_baseline": cpu,
+        "cpu_baseline_deterministic": cpu_det,
+        "certificate": cert and dict(cert, note=(
+            "rows whose k nearest the 16-bit scan's candidates provably hold (rigorous FP16 error bound); "
+            "second_pass rows were rescanned with 256 candidates, exact_rescan rows in FP32")),
         "clocks": clk,
         "gpu_launches": launches,
     }
+    del xh, ih, dh, xh_np, ih_np, dh_np
+    if world == 1 and args.configs:
+        torch.cuda.empty_cache()
+        cfg = {}
+        cfg["C1 blobs_2k_128"] = blobs_leg(dev, local)
+        for wl, steps in (("gmm_i8", args.int_steps), ("bits", args.int_steps)):
+            wn, wd, wk, _ = WORKLOADS[wl]
+            cfg[{"gmm_i8": "C3 gmm_i8_2m_384", "bits": "C4 bits_4m_1024"}[wl]] = exact_int_leg(
+                wl, wn, wd, wk, dev, local, rank, world, None, steps, 1, 1, args.int_check_rows,
+                {"gmm_i8": 150_000, "bits": 50_000}[wl], bool(args.autotune))
+        line["configs"] = cfg
     if world == 1 and args.serve_requests > 0:
-        del xh, ih, dh, xh_np, ih_np, dh_np, x, oi, od
+        del x, oi, od
         torch.cuda.empty_cache()
         line["serving"] = run_serving(args, dev)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+def run_shard(args, world, rank, local):
+    """--shard: ONE graph of the workload on N GPUs.  Every rank holds all rows, builds the complete
+    neighbour lists of its query-row shard (evoc_gpu_opts.row_begin/row_end, 128-row blocks,
+    evoc.distributed.shard_rows) and the shards are all-gathered over NCCL so every rank ends with
+    the whole (n, k) graph.  value = n * k / (slowest rank's shard build + gather): strong scaling."""
+    import datetime
+
+    import numpy as np
+    import torch
+
+    import evoc
+    from evoc import _lib, synthetic
+    from evoc.distributed import knn_graph_sharded, shard_rows
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+        pg = dist
+    n, d, k = args.n, args.dim, args.k
+    x = synthetic.zipf_f32(n=n, dim=d, seed=7, device=dev)  # the same rows on every rank
+    b, e = shard_rows(n, world, rank)
+    largest = max(hi - lo for lo, hi in (shard_rows(n, world, r) for r in range(world)))
+    si = torch.full((largest, k), -1, dtype=torch.int32, device=dev)
+    sd = torch.zeros((largest, k), dtype=torch.float32, device=dev)
+    gi = [torch.empty_like(si) for _ in range(world)]
+    gd = [torch.empty_like(sd) for _ in range(world)]
+    ctx = _lib.context(local)
+    ctx.profile(True)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=dev)
+    opts = evoc.KnnGraphOptions(n_neighbors=k, form="bf16_rerank", device=local, row_begin=b, row_end=e)
+
+    def step():
+        if e > b:
+            evoc.knn_graph_device(x.data_ptr(), 0, n, d, k, si.data_ptr(), sd.data_ptr(), opts)
+        if pg:
+            with torch.cuda.stream(stream):
+                pg.all_gather(gi, si)
+                pg.all_gather(gd, sd)
+
+    for _ in range(args.warmup):
+        step()
+    gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    os.makedirs(OUT_DIR, exist_ok=True)
+    clocks = ClockSampler(gpu_id, os.path.join(OUT_DIR, f"clocks_shard_rank{rank}.csv"))
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches = 0
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+        launches += ctx.launches()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    if pg:
+        t = torch.tensor([ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    value = n * k / (ms / 1000.0)
+    # the gathered graph equals a whole-graph call on every rank (checked on its first rows)
+    if pg:
+        spans = [shard_rows(n, world, r) for r in range(world)]
+        full_i = torch.cat([gi[r][: hi - lo] for r, (lo, hi) in enumerate(spans)])
+    else:
+        full_i = si
+    rows = min(2048, n)
+    ri = torch.empty((rows, k), dtype=torch.int32, device=dev)
+    rd = torch.empty((rows, k), dtype=torch.float32, device=dev)
+    evoc.knn_graph_device(x.data_ptr(), 0, n, d, k, ri.data_ptr(), rd.data_ptr(),
+                          evoc.KnnGraphOptions(n_neighbors=k, form="bf16_rerank", device=local, row_begin=0,
+                                               row_end=rows))
+    torch.cuda.synchronize()
+    consistent = bool(torch.equal(full_i[:rows], ri))
+    # End to end through the public API (knn_graph_sharded with host arrays).
+    xh = x.cpu().numpy()
+    so = evoc.KnnGraphOptions(n_neighbors=k, form="bf16_rerank", device=local)
+    if pg:
+        pg.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        if pg:
+            knn_graph_sharded(xh, so)
+        else:
+            evoc.knn_graph(xh, so)
+    e2e_s = (time.perf_counter() - t0) / args.e2e_steps
+    if pg:
+        t = torch.tensor([e2e_s], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "fp16 tensor-core scan + f32 rerank", "data": "synthetic (generated on device)",
+        "config": {"workload": WORKLOAD, "n": n, "d": d, "k": k, "form": "bf16_rerank",
+                   "parallelism": f"query-row shards of one graph over {world} GPUs + NCCL all-gather",
+                   "shard_rows": [list(shard_rows(n, world, r)) for r in range(world)],
+                   "l2": "inputs larger than L2"},
+        "gathered_graph_matches_single_call": consistent,
+        "e2e": {"value": n * k / e2e_s, "unit": UNIT, "h2d_bytes_per_step": n * d * 4,
+                "d2h_bytes_per_step": n * k * 8, "ms_per_step": e2e_s * 1e3,
+                "timing": "host clock around evoc.distributed.knn_graph_sharded (max over ranks)"},
+        "clocks": clk, "gpu_launches": launches,
+    }
     if rank == 0:
         print(json.dumps(line), flush=True)
     if pg:
@@ -982,10 +1320,20 @@ def main():
     ap.add_argument("--ne-reps", type=int, default=2, help="timed node_embedding calls of each kind (0: none)")
     ap.add_argument("--cpu-lp-rows", type=int, default=100000,
                     help="rows of the graph the oracle's label_propagation_init is timed on")
+    ap.add_argument("--mst", type=int, default=1, help="time the Boruvka MST of the node embedding")
+    ap.add_argument("--cpu-mst-rows", type=int, default=100_000, help="points of the oracle's MST baseline")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--fp32-rows", type=int, default=75_776)  # 2 full waves of 296 CTAs x 128 rows
     ap.add_argument("--recall-rows", type=int, default=10_000)
     ap.add_argument("--cpu-rows", type=int, default=None, help="CPU baseline sample rows (default per workload)")
+    ap.add_argument("--cpu-det-rows", type=int, default=20_000,
+                    help="rows of the single-thread deterministic CPU baseline (0: none)")
+    ap.add_argument("--configs", type=int, default=1,
+                    help="also measure C1 (2k x 128 f32), C3 (2M x 384 i8) and C4 (4M x 1024 bits) at N=1")
+    ap.add_argument("--int-steps", type=int, default=3, help="timed steps of the C3 / C4 objects")
+    ap.add_argument("--int-check-rows", type=int, default=256, help="sampled exactness rows of C3 / C4")
+    ap.add_argument("--shard", action="store_true",
+                    help="one graph over all ranks: query-row shards + NCCL all-gather (strong scaling)")
     ap.add_argument("--serve-requests", type=int, default=10_000)
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-lanes", type=int, default=8)
@@ -1005,6 +1353,8 @@ def main():
         return run_reference(args, world, rank)
     if args.workload != "zipf_f32":
         return run_exact_int(args, world, rank, local)
+    if args.shard:
+        return run_shard(args, world, rank, local)
     return run_ours(args, world, rank, local)
 
 

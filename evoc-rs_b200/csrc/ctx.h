@@ -79,6 +79,7 @@ struct evoc_gpu_ctx {
   // Autotuned scan variants: (scan mode, keep, row bytes, floor(log2 n)) -> variant.
   std::map<std::tuple<int, int, int64_t, int>, int> tune;
   uint64_t timeout_ns = 4000000000ull;  // longest a pipeline wait inside a kernel may take
+  uint64_t delay_ns = 0;  // tests of the timeout path: the scan's producer starts this late
   bool sync_check = false;  // EVOC_SYNC_CHECK=1: wait for and check every kernel stage (fault diagnosis)
   bool profiling = false;
   std::vector<evoc::StageRec> stages;  // event pool; the first n_stages belong to the last call

@@ -355,7 +355,7 @@ int run_bf16_rerank(evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, const Job& j, 
                                   ctx->scratch.as<uint64_t>(), grid, 1, 0, 0, ctx->cand.as<int32_t>(), nullptr,
                                   nullptr, j.status, ctx->timeout_ns, nullptr, ctx->stream,
                                   tuned_variant(ctx, evoc::kScanHalf, int(C), ldb * 2, j.n), half, nullptr,
-                                  certify ? cf(CL.bound) : nullptr),
+                                  certify ? cf(CL.bound) : nullptr, 0, ctx->delay_ns),
              "16-bit scan");
     ctx->launches += 1;
   }
@@ -403,7 +403,8 @@ int run_int8(evoc_gpu_ctx* ctx, const Job& j, int64_t ldb) {
   EVOC_TRY(evoc::launch_tc_scan(evoc::kScanInt8, ctx->x.p, rows, j.r0, j.nq, ctx->x.p, rows, j.n, ldb, j.keff,
                                 ctx->scratch.as<uint64_t>(), grid, 1, 1, EVOC_DTYPE_I8, j.idx, j.raw, j.dist, j.status,
                                 ctx->timeout_ns, nullptr, ctx->stream,
-                                tuned_variant(ctx, evoc::kScanInt8, j.keff, ldb, j.n)),
+                                tuned_variant(ctx, evoc::kScanInt8, j.keff, ldb, j.n), evoc::kHalfF16, nullptr,
+                                nullptr, 0, ctx->delay_ns),
            "int8 scan");
   ctx->launches += 1;
   return EVOC_OK;
@@ -588,19 +589,25 @@ int fuzzy_impl(evoc_gpu_ctx* ctx, const int32_t* idx, const float* dist, int64_t
 
 // GPU NN-descent over the staged rows (see nndescent.cu).  Row slices are not
 // supported: the graph is built for every row.
-// `piv_rows` / `piv_row_bytes`: the rows the pivot scan runs on (BF16 for f32
-// data, the int8 rows themselves for i8); unused for binary rows.
+// `rows` / `row_bytes`: the rows the join reads (FP16 rows for f32 data,
+// which the pivot scan also runs on; the int8 rows; the packed bits).
 constexpr int kNndParts = 11;
 
+// max_candidates: the option, else min(60, floor(1.5 k)) as the reference
+// defaults it (src/knn.rs:410-412), capped at 64.
+int nnd_max_candidates(const evoc_gpu_opts& opts, int k) {
+  int mc = opts.max_candidates > 0 ? opts.max_candidates : std::min(60, int(float(k) * 1.5f));
+  return std::max(1, std::min(mc, 64));
+}
+
 // Parts of the NN-descent work buffer (graph keys and newness flags, double
-// buffered; reverse-edge counts, offsets, fill cursors, rows; the sampled
-// reverse lists and their lengths; the change counter), each 256-byte aligned.
+// buffered; reverse-edge counts, offsets, fill cursors, rows; the candidate
+// lists; the change counter and the distance sum), each 256-byte aligned.
 // Returns the total.
-size_t nnd_work_sizes(int64_t n, int k, size_t* sizes) {
+size_t nnd_work_sizes(int64_t n, int k, int mc, size_t* sizes) {
   const size_t nk = size_t(n) * size_t(k);
-  const size_t rcap = size_t(k);
   const size_t v[kNndParts] = {nk * 8, nk * 8, nk, nk, size_t(n) * 4, size_t(n + 1) * 8, size_t(n) * 4, nk * 4,
-                               size_t(n) * rcap * 4, size_t(n) * 4, 64};
+                               size_t(n) * size_t(2 * mc) * 4, 64, 64};
   size_t total = 0;
   for (int i = 0; i < kNndParts; i++) {
     sizes[i] = v[i];
@@ -610,21 +617,20 @@ size_t nnd_work_sizes(int64_t n, int k, size_t* sizes) {
 }
 
 int run_nndescent(evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, const Job& j, int32_t dtype, int64_t row_bytes,
-                  const void* rows, int ld_f32, int d, const int64_t* rng_state, const void* piv_rows,
-                  int64_t piv_row_bytes) {
+                  const void* rows, int ld_f32, int d, const int64_t* rng_state) {
   if (j.r0 != 0 || j.nq != j.n) return fail(ctx, EVOC_ERR_UNSUPPORTED, "the NN-descent form builds whole graphs only");
-  if (j.keff > 32) return fail(ctx, EVOC_ERR_UNSUPPORTED, "the NN-descent form supports k <= 32");
+  if (j.keff > 64) return fail(ctx, EVOC_ERR_UNSUPPORTED, "the NN-descent form supports k <= 64");
   const int64_t n = j.n;
   const int k = j.keff;
-  const int rcap = k;
+  const int mc = nnd_max_candidates(opts, k);
   evoc::NndArgs a{};
   a.X = static_cast<const uint8_t*>(rows);
   a.row_bytes = row_bytes;
   a.n = n;
   a.k = k;
+  a.mc = mc;
   a.dtype = dtype;
   a.sms = ctx->sms;
-  a.rcap = rcap;
   uint64_t seed = 0x5eed5eedull;
   if (rng_state)
     seed = (uint64_t(rng_state[0]) * 0x9e3779b97f4a7c15ull) ^ (uint64_t(rng_state[1]) << 21) ^ uint64_t(rng_state[2]);
@@ -637,7 +643,7 @@ int run_nndescent(evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, const Job& j, in
     ctx->launches += 1;
   } else {
     // Pivot cells seed the graph and fix the visiting order.
-    int rc = locality_order(ctx, j, piv_rows, piv_row_bytes, dtype == EVOC_DTYPE_I8, true);
+    int rc = locality_order(ctx, j, rows, row_bytes, dtype == EVOC_DTYPE_I8, true);
     if (rc) return rc;
     a.order = ctx->order.as<int32_t>();
     a.label = ctx->labels.as<int32_t>();
@@ -646,7 +652,7 @@ int run_nndescent(evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, const Job& j, in
   }
   const size_t nk = size_t(n) * size_t(k);
   size_t sizes[kNndParts];
-  const size_t total = nnd_work_sizes(n, k, sizes);
+  const size_t total = nnd_work_sizes(n, k, mc, sizes);
   EVOC_TRY(ctx->nnd_work.ensure(total), "alloc NN-descent work");
   uint8_t* p = ctx->nnd_work.as<uint8_t>();
   void* ptrs[kNndParts];
@@ -662,9 +668,9 @@ int run_nndescent(evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, const Job& j, in
   a.rptr = static_cast<int64_t*>(ptrs[5]);
   a.rfill = static_cast<int32_t*>(ptrs[6]);
   a.rrows = static_cast<int32_t*>(ptrs[7]);
-  a.rsel = static_cast<int32_t*>(ptrs[8]);
-  a.rn = static_cast<int32_t*>(ptrs[9]);
-  a.changes = static_cast<unsigned long long*>(ptrs[10]);
+  a.cand = static_cast<int32_t*>(ptrs[8]);
+  a.changes = static_cast<unsigned long long*>(ptrs[9]);
+  a.sum = static_cast<double*>(ptrs[10]);
   {
     Stage st(ctx, "nnd_init");
     EVOC_TRY(evoc::launch_nnd_init(a, ctx->stream), "NN-descent init");
@@ -672,19 +678,31 @@ int run_nndescent(evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, const Job& j, in
   }
   int n_iters = opts.n_iters > 0 ? opts.n_iters : int(std::max(5.0, std::round(std::log2(double(n)))));
   const float delta = opts.delta;
-  const double limit = double(float(delta * float(k)) * float(n));
+  // c <= (delta * n_neighbors as f32 * n as f32) as u32 (src/nndescent/float.rs:849)
+  const double limit = double(uint32_t(delta * float(k) * float(n)));
+  double prev_sum = 0.0;
+  bool has_prev = false;
   int cur = 0;
   for (int it = 0; it < n_iters; it++) {
     Stage st(ctx, "nnd_iteration");
     EVOC_TRY(cudaMemsetAsync(a.changes, 0, 8, ctx->stream), "clear changes");
     EVOC_TRY(evoc::launch_nnd_iteration(a, cur, it, ctx->stream), "NN-descent iteration");
-    ctx->launches += 5;
+    ctx->launches += 6;
     cur ^= 1;
     unsigned long long ch = 0;
+    double sum = 0.0;
     EVOC_TRY(cudaMemcpyAsync(&ch, a.changes, 8, cudaMemcpyDeviceToHost, ctx->stream), "read changes");
+    EVOC_TRY(cudaMemcpyAsync(&sum, a.sum, 8, cudaMemcpyDeviceToHost, ctx->stream), "read distance sum");
     EVOC_TRY(cudaStreamSynchronize(ctx->stream), "NN-descent iteration");
     ctx->nnd_iterations = it + 1;
     if (double(ch) <= limit) break;
+    // delta_improv (src/nndescent/float.rs:857-870): relative change of the
+    // sum of distances from the previous iteration; <= 0 switches it off
+    if (opts.delta_improv > 0.0f) {
+      if (has_prev && std::fabs(sum - prev_sum) / std::fabs(prev_sum) < double(opts.delta_improv)) break;
+      prev_sum = sum;
+      has_prev = true;
+    }
   }
   Stage st(ctx, "nnd_finish");
   if (dtype == EVOC_DTYPE_F32) {
@@ -806,8 +824,7 @@ int knn_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtype, con
                  "to 16-bit");
         ctx->launches += 1;
       }
-      rc = run_nndescent(ctx, opts, job, EVOC_DTYPE_F32, int64_t(ld) * 4, ctx->x.p, ld, int(dim), rng_state,
-                         ctx->xb.p, ldb * 2);
+      rc = run_nndescent(ctx, opts, job, EVOC_DTYPE_F32, ldb * 2, ctx->xb.p, ld, int(dim), rng_state);
     }
   } else if (dtype == EVOC_DTYPE_I8) {
     if (form != EVOC_FORM_EXACT_INT && form != EVOC_FORM_NNDESCENT)
@@ -816,7 +833,7 @@ int knn_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtype, con
     rc = stage_rows(ctx, data, n, dim, ldb, on_dev);
     if (rc) return rc;
     if (form == EVOC_FORM_EXACT_INT) rc = run_int8(ctx, job, ldb);
-    else rc = run_nndescent(ctx, opts, job, EVOC_DTYPE_I8, ldb, ctx->x.p, 0, int(dim), rng_state, ctx->x.p, ldb);
+    else rc = run_nndescent(ctx, opts, job, EVOC_DTYPE_I8, ldb, ctx->x.p, 0, int(dim), rng_state);
   } else {
     if (form != EVOC_FORM_EXACT_INT && form != EVOC_FORM_POPCOUNT && form != EVOC_FORM_NNDESCENT)
       return fail(ctx, EVOC_ERR_UNSUPPORTED, "form not built for u8 in this library");
@@ -825,7 +842,7 @@ int knn_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtype, con
     if (rc) return rc;
     if (form == EVOC_FORM_EXACT_INT) rc = run_jaccard_tc(ctx, job, ldb, dim);
     else if (form == EVOC_FORM_POPCOUNT) rc = run_jaccard(ctx, job, ldb);
-    else rc = run_nndescent(ctx, opts, job, EVOC_DTYPE_U8, ldb, ctx->x.p, 0, int(dim), rng_state, nullptr, 0);
+    else rc = run_nndescent(ctx, opts, job, EVOC_DTYPE_U8, ldb, ctx->x.p, 0, int(dim), rng_state);
   }
   if (rc) return rc;
   int flags[2] = {0, 0};
@@ -1436,6 +1453,15 @@ int evoc_gpu_profile_stage(const evoc_gpu_ctx* ctx, int i, char* name, int name_
 
 int evoc_gpu_last_launch_count(const evoc_gpu_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
+int evoc_gpu_set_wait_limit(evoc_gpu_ctx* ctx, uint64_t ns, uint64_t producer_delay_ns) {
+  if (!ctx) return EVOC_ERR_ARG;
+  if (producer_delay_ns > 100000000ull) return fail(ctx, EVOC_ERR_ARG, "producer delay above 100 ms");
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  ctx->timeout_ns = ns ? ns : 4000000000ull;
+  ctx->delay_ns = producer_delay_ns;
+  return EVOC_OK;
+}
+
 int evoc_gpu_last_certify(const evoc_gpu_ctx* ctx, int64_t* checked, int64_t* second_pass, int64_t* exact_rescan) {
   if (!ctx) return EVOC_ERR_ARG;
   if (checked) *checked = ctx->cert_checked;
@@ -1512,7 +1538,7 @@ void knn_buffer_needs(const evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, int32_
   };
   auto nnd = [&]() {
     size_t sizes[kNndParts];
-    b[kBufNnd] = nnd_work_sizes(n, int(keff), sizes);
+    b[kBufNnd] = nnd_work_sizes(n, int(keff), nnd_max_candidates(opts, int(keff)), sizes);
   };
   b[kBufFlag] = 64;
   if (dtype == EVOC_DTYPE_F32) {

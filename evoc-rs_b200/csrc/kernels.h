@@ -65,7 +65,7 @@ cudaError_t launch_tc_scan(int mode, const void* Q, int64_t q_rows, int64_t q_ro
                            int self_mode, int final_mode, int dtype, int32_t* out_idx, float* out_raw, float* out_dist,
                            int* status, uint64_t timeout_ns, const int32_t* pc, cudaStream_t stream,
                            int variant = -1, int half_type = kHalfF16, const int32_t* q_self = nullptr,
-                           float* out_bound = nullptr, int64_t q_self_base = 0);
+                           float* out_bound = nullptr, int64_t q_self_base = 0, uint64_t delay_ns = 0);
 // Kernel variants of the scan (0..5; -1 = automatic: the first that fits
 // shared memory in the order 0..3, else 4 with global heaps; 5 -- 2 stages,
 // 2 groups -- is chosen only by the autotuner).
@@ -172,12 +172,13 @@ cudaError_t launch_expand_bits(const void* X, int64_t n, int64_t ld_in, int64_t 
 
 // nndescent.cu: GPU NN-descent.
 struct NndArgs {
-  const uint8_t* X;       // rows of row_bytes (f32, int8, or packed bits)
+  const uint8_t* X;       // rows of row_bytes (FP16 rows of f32 data, int8, or packed bits)
   int64_t row_bytes;      // multiple of 16
   const int32_t* pc;      // row popcounts (binary rows), else null
   int64_t n;
-  int k;                  // <= 32
-  int dtype;              // 0 f32, 1 i8, 2 u8
+  int k;                  // <= 64
+  int mc;                 // max_candidates, <= 64
+  int dtype;              // 0 f32 (joined on FP16 rows), 1 i8, 2 u8
   int sms;
   const int32_t* order;   // visit order (rows grouped by pivot cell) or null
   const int32_t* label;   // pivot cell of each row or null
@@ -190,10 +191,9 @@ struct NndArgs {
   int64_t* rptr;          // n + 1
   int32_t* rfill;         // n
   int32_t* rrows;         // n x k
-  int32_t* rsel;          // n x rcap
-  int32_t* rn;            // n
-  int rcap;
+  int32_t* cand;          // n x 2 mc: tagged candidate ids (bit 31 = new), -1 past the end
   unsigned long long* changes;
+  double* sum;            // the new graph's sum of finite raw dissimilarities
 };
 cudaError_t launch_nnd_init(const NndArgs& a, cudaStream_t stream);
 cudaError_t launch_nnd_iteration(const NndArgs& a, int cur, int iter, cudaStream_t stream);

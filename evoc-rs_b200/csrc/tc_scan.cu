@@ -46,6 +46,7 @@ constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
 constexpr int TMEM_COLS = 2 * BN;    // two f32/s32 accumulators
 constexpr size_t SMEM_LIMIT = 232448;      // 227 KB opt-in maximum per block
 constexpr size_t SMEM_FIXED = 1024 /*align*/ + 256 /*barriers*/;
+constexpr uint64_t kDrainNs = 4000000000ull;  // limit of the drain waits whatever the pipeline limit
 
 // Shared memory for a pipeline depth, a number of epilogue warp groups (each
 // with one heap per row) and a heap stride (0: heaps in global memory).
@@ -68,7 +69,9 @@ struct ScanParams {
   float* out_raw;
   float* out_dist;
   int* status;       // 0 ok; set non-zero by the first role that gives up
-  uint64_t timeout_ns;
+  uint64_t timeout_ns;  // limit of each pipeline wait (settable per context)
+  uint64_t drain_ns;    // limit of the waits for loads and MMAs already issued (never shorter than 4 s)
+  uint64_t delay_ns;    // tests of the timeout path: the producer starts this late (0 in normal use)
   const int32_t* pc; // Jaccard mode: popcount of every row (queries and keys)
   int half_type;     // 16-bit mode: kHalfF16 or kHalfBf16 operands
   const int32_t* q_self;  // optional: key index of query i is q_self_base + q_self[i] (gathered query rows)
@@ -283,6 +286,23 @@ __device__ __forceinline__ void epilogue_sync(int nthreads) {
   asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
 }
 
+// Whether every epilogue thread finished the block (a barrier with an AND
+// reduction over the same named barrier): the groups then stop, or fold their
+// heaps, together.  Without it a warp that gave up on a wait could skip the
+// fold barrier another group's warps wait at, and those would never return.
+__device__ __forceinline__ bool epilogue_vote(int nthreads, bool ok) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 q, %1, 0;\n\t"
+      "bar.red.and.pred p, 1, %2, q;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(r)
+      : "r"(uint32_t(ok ? 1 : 0)), "r"(nthreads)
+      : "memory");
+  return r != 0;
+}
+
 }  // namespace
 
 template <int MODE, int STAGES, int GROUPS, bool kSmemHeap, bool kBatch>
@@ -338,6 +358,10 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
   if (warp == 0) {
     // ------------------------------------------------------------ producer
     if (lane == 0) {
+      if (p.delay_ns) {  // bounded: the host caps it
+        const uint64_t t0 = globaltimer_ns();
+        while (globaltimer_ns() - t0 < p.delay_ns) __nanosleep(1000);
+      }
       uint32_t it = 0;
       bool ok = true;
       for (int64_t itm = blockIdx.x; ok && itm < n_items; itm += gridDim.x) {
@@ -362,9 +386,10 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
           }
         }
       }
-      // Let the last loads land before the CTA can exit.
+      // Let the last loads land before the CTA can exit (full-length limit:
+      // these loads were issued and complete on their own).
       for (uint32_t j = (it > STAGES ? it - STAGES : 0); j < it; j++)
-        mbar_wait(&full[j % STAGES], (j / STAGES) & 1u, nullptr, p.timeout_ns);
+        mbar_wait(&full[j % STAGES], (j / STAGES) & 1u, nullptr, p.drain_ns);
     }
   } else if (warp == 1) {
     // ----------------------------------------------------------- MMA issuer
@@ -406,8 +431,8 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
           mma_commit(&tfull[a]);  // accumulator ready for the epilogue
         }
       }
-      mma_commit(mma_done);
-      mbar_wait(mma_done, 0, nullptr, p.timeout_ns);
+      mma_commit(mma_done);  // every MMA issued completes before TMEM is freed
+      mbar_wait(mma_done, 0, nullptr, p.drain_ns);
     }
   } else {
     // -------------------------------------------------------------- epilogue
@@ -467,6 +492,7 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         tc_fence_before();
         mbar_arrive(&tempty[a]);
       }
+      if (GROUPS > 1) ok = epilogue_vote(GROUPS * 128, ok);
       if (!ok) break;
       if (GROUPS > 1) {
         // Fold the other groups' heaps for this row into group 0's.  Unused
@@ -629,7 +655,7 @@ cudaError_t launch_tc_scan(int mode, const void* Q, int64_t q_rows, int64_t q_ro
                            int self_mode, int final_mode, int dtype, int32_t* out_idx, float* out_raw, float* out_dist,
                            int* status, uint64_t timeout_ns, const int32_t* pc, cudaStream_t stream,
                            int variant, int half_type, const int32_t* q_self, float* out_bound,
-                           int64_t q_self_base) {
+                           int64_t q_self_base, uint64_t delay_ns) {
   // q_rows / k_rows: rows present in memory (multiples of the box heights);
   // n_q / n_k: rows that take part.  Rows past n are zero and never offered.
   if (row_bytes % KCB != 0 || n_q <= 0 || n_k <= 0 || keep < 1) return cudaErrorInvalidValue;
@@ -661,6 +687,8 @@ cudaError_t launch_tc_scan(int mode, const void* Q, int64_t q_rows, int64_t q_ro
   p.out_dist = out_dist;
   p.status = status;
   p.timeout_ns = timeout_ns;
+  p.drain_ns = timeout_ns > kDrainNs ? timeout_ns : kDrainNs;
+  p.delay_ns = delay_ns;
   p.pc = pc;
   p.half_type = half_type;
   p.q_self = q_self;
@@ -783,6 +811,7 @@ cudaError_t launch_tc_scan_batch(int mode, BatchHeader* hdr, const ScanJob* jobs
   p.heap_stride = max_keep | 1;
   p.status = &hdr->status;
   p.timeout_ns = timeout_ns;
+  p.drain_ns = timeout_ns > kDrainNs ? timeout_ns : kDrainNs;
   p.jobs = jobs;
   p.items = items;
   p.n_items = &hdr->n_items;

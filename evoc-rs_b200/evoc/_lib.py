@@ -88,6 +88,7 @@ def lib():
             L.evoc_gpu_profile_stage.argtypes = [P, C.c_int, C.c_char_p, C.c_int, C.POINTER(C.c_float)]
             L.evoc_gpu_last_launch_count.argtypes = [P]
             L.evoc_gpu_last_certify.argtypes = [P, C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)]
+            L.evoc_gpu_set_wait_limit.argtypes = [P, C.c_uint64, C.c_uint64]
             _bind_optional(L)
             _lib = L
     return _lib
@@ -115,6 +116,8 @@ def _bind_optional(L) -> None:
                                                       C.POINTER(NumpyRng), P, i64, i32, P]
         L.evoc_gpu_node_embedding.argtypes = [P, P, P, P, i64, i32, i32, P, f32, f32, f32, C.POINTER(NumpyRng),
                                               i32, i32, P]
+    if hasattr(L, "evoc_gpu_peak_ffma"):
+        L.evoc_gpu_peak_ffma.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     if hasattr(L, "evoc_gpu_boruvka_mst"):
         L.evoc_gpu_boruvka_mst.argtypes = [P, P, i64, i32, i32, i32, P, P, C.POINTER(i64)]
     if hasattr(L, "evoc_npy_open"):
@@ -243,6 +246,19 @@ class Context:
 
     def launches(self) -> int:
         return int(lib().evoc_gpu_last_launch_count(self.h))
+
+    def peak_ffma(self) -> float:
+        """FP32 FMA TFLOP/s of this device, measured by a hand-written kernel."""
+        t, ms = C.c_double(0.0), C.c_double(0.0)
+        if lib().evoc_gpu_peak_ffma(self.h, C.byref(t), C.byref(ms)) != EVOC_OK:
+            raise RuntimeError(self.last_error())
+        return t.value
+
+    def set_wait_limit(self, ns: int, producer_delay_ns: int = 0) -> None:
+        """Limit of each pipeline wait in the tensor-core scan (0: the 4 s default); producer_delay_ns
+        delays the scan's producer (tests of the timeout path)."""
+        if lib().evoc_gpu_set_wait_limit(self.h, int(ns), int(producer_delay_ns)) != EVOC_OK:
+            raise ValueError(self.last_error())
 
     def certify_counts(self) -> dict:
         """Rows the last 16-bit-form call certified (checked), rescanned with 256 candidates

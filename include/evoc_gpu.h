@@ -336,6 +336,11 @@ int evoc_graph_npz_read(const char* path, int64_t* n, int64_t* nnz, int64_t* ind
 int evoc_gpu_boruvka_mst(evoc_gpu_ctx* ctx, const float* data, int64_t n, int32_t dim, int32_t min_samples,
                          int32_t buffers_on_device, float* out_edges, float* out_core, int64_t* n_edges);
 
+/* FP32 FMA throughput of the context's device (TFLOP/s, 2 FLOPs per FMA),
+ * measured with a hand-written kernel over every SM; *ms its duration.  The
+ * plain FP32 form's roofline denominator.  No counterpart in evoc-rs. */
+int evoc_gpu_peak_ffma(evoc_gpu_ctx* ctx, double* tflops, double* ms);
+
 /* The context's CUDA stream (a cudaStream_t), for callers that record their
  * own CUDA events around calls.  No counterpart in evoc-rs. */
 void* evoc_gpu_ctx_stream(const evoc_gpu_ctx* ctx);
@@ -350,6 +355,17 @@ int evoc_gpu_profile_stage(const evoc_gpu_ctx* ctx, int i, char* name, int name_
 
 /* Number of kernels the last call launched. */
 int evoc_gpu_last_launch_count(const evoc_gpu_ctx* ctx);
+
+/* Limit, in ns, of each wait inside the tensor-core scan's pipeline on this
+ * context (its producer, MMA and epilogue roles wait on one another); 0
+ * restores the default of 4 s.  A wait that runs out ends the call with
+ * EVOC_ERR_TIMEOUT and leaves the context usable: the roles stop together,
+ * loads and MMAs already issued are waited for (always with the full 4 s
+ * limit) and the tensor memory is freed.  producer_delay_ns (at most 100 ms,
+ * normally 0) makes the main scan's producer start that late, so a limit
+ * below it is sure to run out: the timeout path's test.  No counterpart in
+ * evoc-rs. */
+int evoc_gpu_set_wait_limit(evoc_gpu_ctx* ctx, uint64_t ns, uint64_t producer_delay_ns);
 
 /* Certificate counts of the last BF16_RERANK call on this context: query
  * rows checked, rows that failed the first certificate (rescanned with 256

@@ -92,9 +92,44 @@ def test_nndescent_binary_recall_exact_values():
             assert raw[r, j] == np.float32(want)
 
 
+@pytest.mark.parametrize("k", [40, 64])
+def test_nndescent_k_above_32(k):
+    """Lists of up to 64 neighbours (two keys per lane)."""
+    from evoc import synthetic
+
+    x = synthetic.blobs(n_per=500, centres=8, dim=48, noise=0.3, seed=4)
+    ind, dst, raw = evoc.knn_graph(x, nnd(k), np.random.RandomState(3), return_raw=True)
+    ei, er = O.exact_knn(x, k)
+    rec = _recall(ind, ei)
+    assert rec >= 0.95, rec
+    assert np.all(ind[:, 0] == np.arange(len(x)))
+    assert np.all(np.diff(raw, axis=1) >= -1e-6)
+    assert all(len(set(r)) == k for r in ind)  # no index twice in a row
+
+
+def test_nndescent_options_max_candidates_and_delta_improv():
+    """max_candidates bounds the sampled candidates (fewer candidates: recall can only drop a little,
+    never the exactness of reported pairs); a large delta_improv stops after fewer iterations."""
+    from evoc import _lib, synthetic
+
+    x = synthetic.blobs(n_per=400, centres=10, dim=32, noise=0.3, seed=6)
+    ei, _ = O.exact_knn(x, 15)
+    ctx = _lib.context(0)
+    a, _ = evoc.knn_graph(x, nnd(15, max_candidates=4), np.random.RandomState(1))
+    b, _ = evoc.knn_graph(x, nnd(15), np.random.RandomState(1))
+    assert _recall(b, ei) >= 0.95 and _recall(a, ei) >= 0.5
+    ctx.profile(True)  # stage records count the iterations
+    evoc.knn_graph(x, nnd(15, delta=0.0, delta_improv=0.0, n_iters=8), np.random.RandomState(1))
+    full = [nm for nm, _ in ctx.stages()].count("nnd_iteration")
+    evoc.knn_graph(x, nnd(15, delta=0.0, delta_improv=0.5, n_iters=8), np.random.RandomState(1))
+    early = [nm for nm, _ in ctx.stages()].count("nnd_iteration")
+    # delta_improv = 0.5: the second iteration's sum moves by far less than half, so it stops there
+    assert early == 2 and full > early, (full, early)
+
+
 def test_nndescent_rejects_unsupported():
     x = np.random.default_rng(0).standard_normal((100, 16)).astype(np.float32)
     with pytest.raises(evoc.BackendError):
-        evoc.knn_graph(x, nnd(40))
+        evoc.knn_graph(x, nnd(65))
     with pytest.raises(evoc.BackendError):
         evoc.knn_graph(x, nnd(5, row_begin=0, row_end=50))
