@@ -1093,10 +1093,18 @@ def run_ours(args, world, rank, local):
                     "launch_ms": scan_ms}
     else:
         it_ms = stage_ms.get("nnd_iteration", [float("nan")])
-        roofline = {"bound": "hbm", "achieved": None, "peak": float(peaks.get("hbm_gbs")), "unit": "GB/s",
-                    "frac": None, "traffic": None, "kernel": "nnd_join_kernel (candidate row gathers)",
-                    "launch_ms": statistics.mean(it_ms),
-                    "note": "the join's gathered bytes depend on the candidate sets; DRAM counters in profiles/"}
+        nst = ctx.nndescent_stats()  # of the last timed step
+        step_iter_ms = sum(it_ms) / args.steps
+        gathered = nst["distance_evals"] * nst["row_bytes"]
+        achieved = gathered / (step_iter_ms / 1e3) / 1e9
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": float(peaks.get("hbm_gbs")), "unit": "GB/s",
+                    "frac": achieved / float(peaks.get("hbm_gbs")), "traffic": None,
+                    "kernel": "nnd_join_kernel (candidate row gathers)", "launch_ms": statistics.mean(it_ms),
+                    "iterations": nst["iterations"], "distance_evals": nst["distance_evals"],
+                    "row_bytes": nst["row_bytes"],
+                    "note": ("achieved = candidate-row bytes the joins gathered (distance evaluations x FP16 row "
+                             "bytes) over the iterations' device time; rows found in L2 count too, so the "
+                             "fraction can pass 1")}
 
     cpu = None
     if rank == 0 and world == 1 and args.cpu_rows > 0:

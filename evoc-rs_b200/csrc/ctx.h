@@ -51,7 +51,9 @@ struct StageRec {
 struct evoc_gpu_ctx {
   int device = 0;
   int sms = 148;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;       // the stream calls run on (a serving lane may swap in another)
+  cudaStream_t base_stream = nullptr;  // the context's own stream (destroyed with it)
+  bool scan_per_block = false;         // main scans launch one CTA per query block (serving, big requests)
   std::mutex mu;
   std::string err;
   evoc::DevBuf x, scratch, norms, flag, out_idx, out_raw, out_dist;
@@ -86,6 +88,8 @@ struct evoc_gpu_ctx {
   int n_stages = 0;
   int launches = 0;
   int nnd_iterations = 0;
+  unsigned long long nnd_evals = 0;  // distances the last NN-descent call's joins computed
+  int64_t nnd_row_bytes = 0;         // bytes of each row those distances gathered
   // Stream-ordered pool of the label-propagation / embedding calls; it keeps
   // freed blocks (release threshold = max) so repeated calls do not remap.
   cudaMemPool_t lp_pool = nullptr;

@@ -84,6 +84,18 @@ int scan_grid(const evoc_gpu_ctx* ctx, int64_t n_q) {
   return int(qblocks < ctx->sms ? qblocks : ctx->sms);
 }
 
+// Grid of a request's main scan.  Persistent by default (a CTA per SM walking
+// many query blocks); a context with scan_per_block (a serving lane running a
+// big request) launches a CTA per query block instead, so SMs come free block
+// by block -- every few ms -- for other streams' kernels, high-priority ones
+// first.  Global-memory heaps are sized for the persistent grid, so a launch
+// that uses them stays persistent.
+int main_scan_grid(const evoc_gpu_ctx* ctx, int64_t n_q, int keep, int variant) {
+  const int persistent = scan_grid(ctx, n_q);
+  if (!ctx->scan_per_block || evoc::tc_scan_uses_global_heaps(variant, keep)) return persistent;
+  return int(std::min<int64_t>((n_q + 127) / 128, int64_t(1) << 30));
+}
+
 // One kNN request: all n rows are keys; query rows r0 .. r0+nq-1 are output rows 0 .. nq-1.
 struct Job {
   int64_t n, r0, nq;
@@ -100,6 +112,16 @@ int run_fp32(evoc_gpu_ctx* ctx, const Job& j, int ld) {
   const int64_t qblocks = (j.nq + 127) / 128;
   const int grid = int(qblocks < int64_t(ctx->sms) * 2 ? qblocks : int64_t(ctx->sms) * 2);
   EVOC_TRY(ctx->scratch.ensure(size_t(grid) * 128 * size_t(cap) * 8), "alloc scratch");
+  if (j.r0 % 4 == 0) {
+    // k-major copy of the rows in the (otherwise unused) 16-bit row buffer
+    EVOC_TRY(ctx->xb.ensure(size_t(evoc::knn_f32_kt_cols(j.n)) * size_t(ld) * 4), "alloc k-major rows");
+    EVOC_TRY(evoc::launch_knn_f32_kt(ctx->x.as<float>(), j.n, ld, ctx->xb.as<float>(), j.keff, cap,
+                                     ctx->scratch.as<uint64_t>(), grid, j.idx, j.raw, j.dist, j.r0, j.r0 + j.nq,
+                                     ctx->sms, ctx->stream),
+             "knn_f32_kt");
+    ctx->launches += 2;
+    return EVOC_OK;
+  }
   EVOC_TRY(evoc::launch_knn_f32_simt(ctx->x.as<float>(), j.n, ld, j.keff, cap, ctx->scratch.as<uint64_t>(), grid,
                                      j.idx, j.raw, j.dist, j.r0, j.r0 + j.nq, ctx->stream),
            "knn_f32_simt");
@@ -346,15 +368,15 @@ int run_bf16_rerank(evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, const Job& j, 
              "to 16-bit");
     ctx->launches += 1;
   }
-  const int grid = scan_grid(ctx, j.nq);
+  const int variant = tuned_variant(ctx, evoc::kScanHalf, int(C), ldb * 2, j.n);
+  const int grid = main_scan_grid(ctx, j.nq, int(C), variant);
   EVOC_TRY(ctx->cand.ensure(size_t(j.nq * C) * 4), "alloc candidates");
   {
     Stage st(ctx, "bf16_scan");
     EVOC_TRY(ctx->scratch.ensure(scan_scratch_bytes(ctx, j.nq, C)), "alloc scratch");
     EVOC_TRY(evoc::launch_tc_scan(evoc::kScanHalf, ctx->xb.p, rows, j.r0, j.nq, ctx->xb.p, rows, j.n, ldb * 2, int(C),
                                   ctx->scratch.as<uint64_t>(), grid, 1, 0, 0, ctx->cand.as<int32_t>(), nullptr,
-                                  nullptr, j.status, ctx->timeout_ns, nullptr, ctx->stream,
-                                  tuned_variant(ctx, evoc::kScanHalf, int(C), ldb * 2, j.n), half, nullptr,
+                                  nullptr, j.status, ctx->timeout_ns, nullptr, ctx->stream, variant, half, nullptr,
                                   certify ? cf(CL.bound) : nullptr, 0, ctx->delay_ns),
              "16-bit scan");
     ctx->launches += 1;
@@ -397,14 +419,14 @@ int run_bf16_rerank(evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, const Job& j, 
 
 int run_int8(evoc_gpu_ctx* ctx, const Job& j, int64_t ldb) {
   Stage st(ctx, "int8_scan");
-  const int grid = scan_grid(ctx, j.nq);
+  const int variant = tuned_variant(ctx, evoc::kScanInt8, j.keff, ldb, j.n);
+  const int grid = main_scan_grid(ctx, j.nq, j.keff, variant);
   const int64_t rows = evoc::padded_rows(j.n);
-  EVOC_TRY(ctx->scratch.ensure(size_t(grid) * 256 * size_t(j.keff) * 8), "alloc scratch");
+  EVOC_TRY(ctx->scratch.ensure(size_t(scan_grid(ctx, j.nq)) * 256 * size_t(j.keff) * 8), "alloc scratch");
   EVOC_TRY(evoc::launch_tc_scan(evoc::kScanInt8, ctx->x.p, rows, j.r0, j.nq, ctx->x.p, rows, j.n, ldb, j.keff,
                                 ctx->scratch.as<uint64_t>(), grid, 1, 1, EVOC_DTYPE_I8, j.idx, j.raw, j.dist, j.status,
-                                ctx->timeout_ns, nullptr, ctx->stream,
-                                tuned_variant(ctx, evoc::kScanInt8, j.keff, ldb, j.n), evoc::kHalfF16, nullptr,
-                                nullptr, 0, ctx->delay_ns),
+                                ctx->timeout_ns, nullptr, ctx->stream, variant, evoc::kHalfF16, nullptr, nullptr, 0,
+                                ctx->delay_ns),
            "int8 scan");
   ctx->launches += 1;
   return EVOC_OK;
@@ -591,7 +613,7 @@ int fuzzy_impl(evoc_gpu_ctx* ctx, const int32_t* idx, const float* dist, int64_t
 // supported: the graph is built for every row.
 // `rows` / `row_bytes`: the rows the join reads (FP16 rows for f32 data,
 // which the pivot scan also runs on; the int8 rows; the packed bits).
-constexpr int kNndParts = 11;
+constexpr int kNndParts = 12;
 
 // max_candidates: the option, else min(60, floor(1.5 k)) as the reference
 // defaults it (src/knn.rs:410-412), capped at 64.
@@ -607,7 +629,7 @@ int nnd_max_candidates(const evoc_gpu_opts& opts, int k) {
 size_t nnd_work_sizes(int64_t n, int k, int mc, size_t* sizes) {
   const size_t nk = size_t(n) * size_t(k);
   const size_t v[kNndParts] = {nk * 8, nk * 8, nk, nk, size_t(n) * 4, size_t(n + 1) * 8, size_t(n) * 4, nk * 4,
-                               size_t(n) * size_t(2 * mc) * 4, 64, 64};
+                               size_t(n) * size_t(2 * mc) * 4, 64, 64, 64};
   size_t total = 0;
   for (int i = 0; i < kNndParts; i++) {
     sizes[i] = v[i];
@@ -671,6 +693,8 @@ int run_nndescent(evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, const Job& j, in
   a.cand = static_cast<int32_t*>(ptrs[8]);
   a.changes = static_cast<unsigned long long*>(ptrs[9]);
   a.sum = static_cast<double*>(ptrs[10]);
+  a.evals = static_cast<unsigned long long*>(ptrs[11]);
+  EVOC_TRY(cudaMemsetAsync(a.evals, 0, 8, ctx->stream), "clear evaluation count");
   {
     Stage st(ctx, "nnd_init");
     EVOC_TRY(evoc::launch_nnd_init(a, ctx->stream), "NN-descent init");
@@ -704,6 +728,8 @@ int run_nndescent(evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, const Job& j, in
       has_prev = true;
     }
   }
+  EVOC_TRY(cudaMemcpyAsync(&ctx->nnd_evals, a.evals, 8, cudaMemcpyDeviceToHost, ctx->stream), "read evaluations");
+  ctx->nnd_row_bytes = row_bytes;
   Stage st(ctx, "nnd_finish");
   if (dtype == EVOC_DTYPE_F32) {
     EVOC_TRY(ctx->cand.ensure(nk * 4), "alloc candidates");
@@ -1397,6 +1423,7 @@ int evoc_gpu_ctx_create(int device, evoc_gpu_ctx** out) {
     delete ctx;
     return EVOC_ERR_CUDA;
   }
+  ctx->base_stream = ctx->stream;
   *out = ctx;
   return EVOC_OK;
 }
@@ -1404,6 +1431,8 @@ int evoc_gpu_ctx_create(int device, evoc_gpu_ctx** out) {
 void evoc_gpu_ctx_destroy(evoc_gpu_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  ctx->stream = ctx->base_stream;
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   DevBuf* bufs[] = {&ctx->x,        &ctx->scratch, &ctx->norms, &ctx->flag,   &ctx->out_idx,
                     &ctx->out_raw,  &ctx->out_dist, &ctx->xb,   &ctx->cand,   &ctx->labels,
@@ -1452,6 +1481,15 @@ int evoc_gpu_profile_stage(const evoc_gpu_ctx* ctx, int i, char* name, int name_
 }
 
 int evoc_gpu_last_launch_count(const evoc_gpu_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int evoc_gpu_last_nndescent(const evoc_gpu_ctx* ctx, int32_t* iterations, int64_t* distance_evals,
+                            int64_t* row_bytes) {
+  if (!ctx) return EVOC_ERR_ARG;
+  if (iterations) *iterations = ctx->nnd_iterations;
+  if (distance_evals) *distance_evals = int64_t(ctx->nnd_evals);
+  if (row_bytes) *row_bytes = ctx->nnd_row_bytes;
+  return EVOC_OK;
+}
 
 int evoc_gpu_set_wait_limit(evoc_gpu_ctx* ctx, uint64_t ns, uint64_t producer_delay_ns) {
   if (!ctx) return EVOC_ERR_ARG;
@@ -1548,6 +1586,7 @@ void knn_buffer_needs(const evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, int32_
     if (form == EVOC_FORM_FP32) {
       const int64_t g = std::min<int64_t>(qblocks, int64_t(ctx->sms) * 2);
       b[kBufScratch] = size_t(g) * 128 * size_t(topk_capacity(int(keff))) * 8;
+      b[kBufXb] = size_t(knn_f32_kt_cols(n)) * size_t(round_up(dim, 16)) * 4;  // the k-major copy
     } else if (form == EVOC_FORM_BF16_RERANK) {
       const int64_t C = bf16_candidates(opts, n, int(keff));
       b[kBufXb] = size_t(rows * ldb * 2);

@@ -11,6 +11,8 @@
 // (register-prefetched double buffer), the 128x128 score tile is staged in
 // shared memory, and 128 owner threads (one per query row) feed their row's
 // scores to a thread-private candidate buffer in global scratch.
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -166,6 +168,206 @@ cudaError_t launch_knn_f32_simt(const float* X, int64_t n, int ld, int k, int ca
   if (e != cudaSuccess) return e;
   knn_f32_simt_kernel<<<grid, NT, smem, stream>>>(X, n, ld, k, cap, scratch, out_idx, out_raw, out_dist, q_begin,
                                                    q_end, Q ? Q : X, q_list, q_row0);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// The k-major form of the same search.  XT holds the rows transposed: ld rows
+// (one per coordinate) of `cols` floats, cols = round_up(n, 128) + 128, with
+// zeros past row n-1.  An operand tile (16 coordinates x 128 rows) is then 16
+// contiguous 512-byte runs, copied to shared memory by cp.async with no
+// register staging or transposition; a two-stage pipeline keeps one k-step in
+// flight and takes one barrier per k-step.  The score tile has its own shared
+// memory, so the next tile's first copy overlaps the top-k epilogue.
+//
+// Alignment: query block starts q_begin + 128 i must be multiples of 4 floats
+// (the host takes this form only when q_begin % 4 == 0); key tiles start at
+// multiples of 128.  Bounds: a query tile reads columns q0 .. q0+127 with
+// q0 < n, so below round_up(n, 128) + 128 = cols.
+
+namespace {
+struct F32KtSmem {
+  float a[2][BK][APAD];
+  float b[2][BK][APAD];
+  float s[BM][SPAD];
+};
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Queues the copies of k-step `ks` of the (q0, c0) tile pair into stage `st`:
+// 2 x 16 runs of 128 floats, 512 16-byte chunks each, two per thread.
+__device__ __forceinline__ void kt_issue(F32KtSmem& sm, int st, const float* __restrict__ XT, int64_t cols,
+                                         int64_t q0, int64_t c0, int ks, int tid) {
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    const int id = tid + h * NT;
+    const int r = id >> 5, c = (id & 31) * 4;
+    const float* src = XT + int64_t(ks * BK + r) * cols;
+    cp_async16(&sm.a[st][r][c], src + q0 + c);
+    cp_async16(&sm.b[st][r][c], src + c0 + c);
+  }
+  cp_async_commit();
+}
+}  // namespace
+
+__global__ void __launch_bounds__(NT, 2)
+knn_f32_kt_kernel(const float* __restrict__ XT, int64_t cols, int64_t n, int ld, int k, int cap,
+                  uint64_t* __restrict__ scratch, int32_t* __restrict__ out_idx, float* __restrict__ out_raw,
+                  float* __restrict__ out_dist, int64_t q_begin, int64_t q_end) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  F32KtSmem& sm = *reinterpret_cast<F32KtSmem*>(smem_raw);
+  const int tid = threadIdx.x;
+  const int ty = tid >> 4, tx = tid & 15;
+  const int nk = ld / BK;
+  const int64_t n_qblocks = (q_end - q_begin + BM - 1) / BM;
+  const int64_t n_ktiles = (n + BN - 1) / BN;
+  uint64_t* my_buf = scratch + (int64_t(blockIdx.x) * BM + (tid & (BM - 1))) * cap;
+
+  for (int64_t qb = blockIdx.x; qb < n_qblocks; qb += gridDim.x) {
+    const int64_t q0 = q_begin + qb * BM;
+    const int64_t my_q = q0 + tid;
+    RowTopK top;
+    top.init(my_buf, k, cap);
+    float acc[8][8];
+    int stage = 0;
+    kt_issue(sm, 0, XT, cols, q0, 0, 0, tid);
+    int64_t kt = 0;
+    int ks = 0;
+    while (kt < n_ktiles) {
+      cp_async_wait_all();
+      __syncthreads();  // stage `stage` landed for all threads; stage^1 is free (its k-step is done)
+      {
+        int64_t nkt = kt;
+        int nks = ks + 1;
+        if (nks == nk) {
+          nks = 0;
+          nkt++;
+        }
+        if (nkt < n_ktiles) kt_issue(sm, stage ^ 1, XT, cols, q0, nkt * BN, nks, tid);
+      }
+      if (ks == 0) {
+#pragma unroll
+        for (int i = 0; i < 8; i++)
+#pragma unroll
+          for (int j = 0; j < 8; j++) acc[i][j] = 0.f;
+      }
+#pragma unroll
+      for (int kk = 0; kk < BK; kk++) {
+        float av[8], bv[8];
+        const float4 t0 = *reinterpret_cast<const float4*>(&sm.a[stage][kk][ty * 4]);
+        const float4 t1 = *reinterpret_cast<const float4*>(&sm.a[stage][kk][64 + ty * 4]);
+        const float4 u0 = *reinterpret_cast<const float4*>(&sm.b[stage][kk][tx * 4]);
+        const float4 u1 = *reinterpret_cast<const float4*>(&sm.b[stage][kk][64 + tx * 4]);
+        av[0] = t0.x; av[1] = t0.y; av[2] = t0.z; av[3] = t0.w;
+        av[4] = t1.x; av[5] = t1.y; av[6] = t1.z; av[7] = t1.w;
+        bv[0] = u0.x; bv[1] = u0.y; bv[2] = u0.z; bv[3] = u0.w;
+        bv[4] = u1.x; bv[5] = u1.y; bv[6] = u1.z; bv[7] = u1.w;
+#pragma unroll
+        for (int i = 0; i < 8; i++)
+#pragma unroll
+          for (int j = 0; j < 8; j++) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+      }
+      stage ^= 1;
+      if (++ks == nk) {
+        // The tile is complete: stage it and let the 128 row owners take it.
+        // The score tile is next written a full tile later, after at least one
+        // more top-of-step barrier, so the owners' reads below are done by then.
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+          const int r = (i < 4) ? ty * 4 + i : 64 + ty * 4 + (i - 4);
+#pragma unroll
+          for (int j = 0; j < 8; j++) {
+            const int c = (j < 4) ? tx * 4 + j : 64 + tx * 4 + (j - 4);
+            sm.s[r][c] = acc[i][j];
+          }
+        }
+        __syncthreads();
+        if (tid < BM && my_q < q_end) {
+          const int64_t c0 = kt * BN;
+          const int lim = (n - c0 < BN) ? int(n - c0) : BN;
+          for (int c = 0; c < lim; c++) {
+            const int64_t key = c0 + c;
+            const float raw = (key == my_q) ? -1.0f : raw_cosine(sm.s[tid][c]);
+            top.offer(raw, int32_t(key));
+          }
+        }
+        ks = 0;
+        kt++;
+      }
+    }
+    if (tid < BM && my_q < q_end) {
+      const int got = top.finish();
+      const int64_t orow = (my_q - q_begin) * k;
+      for (int j = 0; j < k; j++) {
+        float raw = kHeapInf;
+        int32_t idx = -1;
+        if (j < got) {
+          raw = from_orderable(uint32_t(top.buf[j] >> 32));
+          idx = key_index(top.buf[j]);
+        }
+        out_idx[orow + j] = idx;
+        if (out_raw) out_raw[orow + j] = raw;
+        if (out_dist) out_dist[orow + j] = transform_raw(0, raw);
+      }
+    }
+    __syncthreads();  // the score tile and both stages are free before the next query block
+  }
+}
+
+// XT[c][j] = X[j][c] for rows j < n, zero for n <= j < cols.  One 64-row x
+// 16-coordinate tile per step: reads of 64-byte row pieces, writes of
+// 256-byte runs of XT.
+__global__ void __launch_bounds__(256) transpose_rows_kernel(const float* __restrict__ X, int64_t n, int ld,
+                                                             float* __restrict__ XT, int64_t cols) {
+  __shared__ float t[16][65];
+  const int tid = threadIdx.x;
+  const int64_t ctiles = cols / 64;
+  const int64_t tiles = ctiles * (ld / 16);
+  for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const int64_t j0 = (tile % ctiles) * 64;
+    const int k0 = int(tile / ctiles) * 16;
+    {
+      const int r = tid >> 2, c4 = (tid & 3) * 4;
+      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (j0 + r < n) v = *reinterpret_cast<const float4*>(X + (j0 + r) * ld + k0 + c4);
+      t[c4 + 0][r] = v.x;
+      t[c4 + 1][r] = v.y;
+      t[c4 + 2][r] = v.z;
+      t[c4 + 3][r] = v.w;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const int id = tid + i * 256;
+      const int kk = id >> 6, jj = id & 63;
+      XT[int64_t(k0 + kk) * cols + j0 + jj] = t[kk][jj];
+    }
+    __syncthreads();
+  }
+}
+
+int64_t knn_f32_kt_cols(int64_t n) { return (n + 127) / 128 * 128 + 128; }
+
+cudaError_t launch_knn_f32_kt(const float* X, int64_t n, int ld, float* XT, int k, int cap, uint64_t* scratch,
+                              int grid, int32_t* out_idx, float* out_raw, float* out_dist, int64_t q_begin,
+                              int64_t q_end, int sms, cudaStream_t stream) {
+  if (ld % BK != 0 || q_begin % 4 != 0 || q_begin < 0 || q_end > n || q_begin > q_end) return cudaErrorInvalidValue;
+  const int64_t cols = knn_f32_kt_cols(n);
+  const int64_t tiles = cols / 64 * (ld / 16);
+  const int tgrid = int(std::min<int64_t>(tiles, int64_t(sms) * 8));
+  transpose_rows_kernel<<<tgrid, 256, 0, stream>>>(X, n, ld, XT, cols);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || q_begin == q_end) return e;
+  const size_t smem = sizeof(F32KtSmem);
+  e = cudaFuncSetAttribute(knn_f32_kt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return e;
+  knn_f32_kt_kernel<<<grid, NT, smem, stream>>>(XT, cols, n, ld, k, cap, scratch, out_idx, out_raw, out_dist,
+                                                q_begin, q_end);
   return cudaGetLastError();
 }
 

@@ -15,6 +15,14 @@ cudaError_t launch_prepare_float(float* X, int64_t n, int ld, int d, float* norm
 //   q - q_begin.  With Q and q_list (query rows gathered from X): query i is row i of Q, row
 //   q_row0 + q_list[i] of X for the self rule, and is written to output row q_list[i].
 size_t knn_f32_simt_smem();
+// Columns of the k-major copy launch_knn_f32_kt writes for n rows.
+int64_t knn_f32_kt_cols(int64_t n);
+// Exact FP32 kNN from a k-major copy: writes XT (ld x knn_f32_kt_cols(n)
+// floats) from the n x ld rows X, then searches queries q_begin .. q_end-1
+// (q_begin % 4 == 0) against all n rows.
+cudaError_t launch_knn_f32_kt(const float* X, int64_t n, int ld, float* XT, int k, int cap, uint64_t* scratch,
+                              int grid, int32_t* out_idx, float* out_raw, float* out_dist, int64_t q_begin,
+                              int64_t q_end, int sms, cudaStream_t stream);
 cudaError_t launch_knn_f32_simt(const float* X, int64_t n, int ld, int k, int cap, uint64_t* scratch, int grid,
                                 int32_t* out_idx, float* out_raw, float* out_dist, int64_t q_begin, int64_t q_end,
                                 cudaStream_t stream, const float* Q = nullptr, const int32_t* q_list = nullptr,
@@ -71,6 +79,8 @@ cudaError_t launch_tc_scan(int mode, const void* Q, int64_t q_rows, int64_t q_ro
 // 2 groups -- is chosen only by the autotuner).
 constexpr int kScanVariants = 6;
 bool tc_scan_variant_feasible(int variant, int keep, bool has_scratch);
+// Whether a launch with this variant (-1: automatic) and keep keeps its heaps in global scratch.
+bool tc_scan_uses_global_heaps(int variant, int keep);
 const char* tc_scan_variant_name(int variant);
 // prep.cu: synthetic rows for the autotuner (mode 0: FP16 values in [-1, 1];
 // 1: int8; 2: packed bits, about 1 in 8 set), zero past n rows / `bytes` bytes.
@@ -194,6 +204,7 @@ struct NndArgs {
   int32_t* cand;          // n x 2 mc: tagged candidate ids (bit 31 = new), -1 past the end
   unsigned long long* changes;
   double* sum;            // the new graph's sum of finite raw dissimilarities
+  unsigned long long* evals;  // distances the joins computed (accumulates over iterations)
 };
 cudaError_t launch_nnd_init(const NndArgs& a, cudaStream_t stream);
 cudaError_t launch_nnd_iteration(const NndArgs& a, int cur, int iter, cudaStream_t stream);

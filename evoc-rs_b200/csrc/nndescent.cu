@@ -178,8 +178,9 @@ __device__ __forceinline__ bool hash_claim(uint32_t* hs, uint32_t id) {
 template <int DT>
 __device__ __forceinline__ void eval_taken(const uint8_t* __restrict__ X, int64_t row_bytes,
                                            const int32_t* __restrict__ pc, int64_t u, int32_t w, bool take,
-                                           WarpList& L, int k, int lane) {
+                                           WarpList& L, int k, int lane, uint32_t& evals) {
   uint32_t m = __ballot_sync(0xffffffffu, take);
+  evals += __popc(m);
   while (m) {
     int32_t b[4];
 #pragma unroll
@@ -346,10 +347,11 @@ __global__ void __launch_bounds__(NW * 32)
 nnd_join_kernel(const uint8_t* __restrict__ X, int64_t row_bytes, const int32_t* __restrict__ pc, int64_t n, int k,
                 const int32_t* __restrict__ order, const uint64_t* __restrict__ keys, const int32_t* __restrict__ cand,
                 int mc2, uint64_t* __restrict__ keys_out, uint8_t* __restrict__ new_out,
-                unsigned long long* __restrict__ changes) {
+                unsigned long long* __restrict__ changes, unsigned long long* __restrict__ n_evals) {
   extern __shared__ uint32_t nnd_hash[];  // NW x HSLOTS
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint32_t* hs = nnd_hash + warp * HSLOTS;
+  uint32_t evals = 0;  // distances this warp computed (uniform across the warp)
   for (int64_t w = int64_t(blockIdx.x) * NW + warp; w < n; w += int64_t(gridDim.x) * NW) {
     const int64_t u = order ? order[w] : w;
     WarpList L{lane < k ? keys[u * k + lane] : kKeyInf, lane + 32 < k ? keys[u * k + 32 + lane] : kKeyInf};
@@ -370,7 +372,7 @@ nnd_join_kernel(const uint8_t* __restrict__ X, int64_t row_bytes, const int32_t*
       // the source itself
       bool take = false;
       if (lane == 0) take = hash_claim(hs, uint32_t(src));
-      eval_taken<DT>(X, row_bytes, pc, u, src, take, L, k, lane);
+      eval_taken<DT>(X, row_bytes, pc, u, src, take, L, k, lane, evals);
       // its candidates
       const int32_t* cs = cand + int64_t(src) * mc2;
       for (int c0 = 0; c0 < mc2; c0 += 32) {
@@ -385,7 +387,7 @@ nnd_join_kernel(const uint8_t* __restrict__ X, int64_t row_bytes, const int32_t*
         }
         bool tk = wv >= 0 && wv != int32_t(u) && (src_new || wn);
         if (tk) tk = hash_claim(hs, uint32_t(wv));
-        eval_taken<DT>(X, row_bytes, pc, u, wv, tk, L, k, lane);
+        eval_taken<DT>(X, row_bytes, pc, u, wv, tk, L, k, lane, evals);
       }
     }
     // New flag: the entry was not in the list at the start of the iteration.
@@ -408,6 +410,7 @@ nnd_join_kernel(const uint8_t* __restrict__ X, int64_t row_bytes, const int32_t*
     if (lane == 0 && (ch | ch2)) atomicAdd(changes, (unsigned long long)(__popc(ch) + __popc(ch2)));
     __syncwarp();
   }
+  if (lane == 0 && evals) atomicAdd(n_evals, (unsigned long long)evals);
 }
 
 // Sum over the graph of the finite raw dissimilarities, in f64 (the
@@ -468,7 +471,8 @@ cudaError_t join(const NndArgs& a, int cur, int blocks, size_t smem, cudaStream_
   if (e != cudaSuccess) return e;
   const int nxt = cur ^ 1;
   nnd_join_kernel<DT><<<blocks, NW * 32, smem, stream>>>(a.X, a.row_bytes, a.pc, a.n, a.k, a.order, a.keys[cur],
-                                                         a.cand, 2 * a.mc, a.keys[nxt], a.isnew[nxt], a.changes);
+                                                         a.cand, 2 * a.mc, a.keys[nxt], a.isnew[nxt], a.changes,
+                                                         a.evals);
   return cudaGetLastError();
 }
 }  // namespace

@@ -37,6 +37,7 @@
 #include <nvtx3/nvToolsExt.h>
 
 #include "../../include/evoc_gpu.h"
+#include "ctx.h"
 #include "ctx_plan.h"
 #include "kernels.h"
 
@@ -96,6 +97,9 @@ constexpr double kBatchWork = 4e12;
 // A batch forms only under backlog: at least this many compatible small
 // requests pending.  With fewer, each runs alone at its lowest latency.
 constexpr int kBatchMin = 4;
+// Requests below this many rows are latency-sensitive: they run on a lane's
+// high-priority stream.
+constexpr int64_t kUrgentRows = 65536;
 
 }  // namespace
 
@@ -114,7 +118,8 @@ struct evoc_gpu_server {
   std::vector<evoc::CtxSizes> lane_sizes;  // each lane context's buffers (counted in in_use)
   int64_t ws_misses = 0;
   std::vector<evoc_gpu_ctx*> ctxs;
-  std::vector<cudaStream_t> streams;
+  std::vector<cudaStream_t> streams;  // each lane context's own stream (normal priority)
+  std::vector<cudaStream_t> urgent;   // each lane's high-priority stream, for small requests
   cudaStream_t free_stream = nullptr;
   std::mutex copy_mu;
   cudaStream_t copy_stream = nullptr;
@@ -184,7 +189,14 @@ std::string tag(const Job* j, int lane, size_t batch) {
 // evoc_gpu_knn_graph, or a batch of small ones through evoc_gpu_knn_graph_batch.
 void run_work(evoc_gpu_server* s, int lane, const std::vector<Job*>& group, bool batch) {
   evoc_gpu_ctx* ctx = s->ctxs[size_t(lane)];
-  cudaStream_t st = s->streams[size_t(lane)];
+  // Small requests (and batches of them) run on the lane's high-priority
+  // stream; a big request runs at normal priority with a CTA per query block,
+  // so the SMs it holds come free block by block and the small requests'
+  // kernels, queued at higher priority, take them first.
+  const bool small = batch || group.front()->n < kUrgentRows;
+  cudaStream_t st = small ? s->urgent[size_t(lane)] : s->streams[size_t(lane)];
+  ctx->stream = st;  // the lane's previous call left its streams idle
+  ctx->scan_per_block = !small;
   nvtxRangePushA(batch ? "evoc_batch" : "evoc_job");
   const size_t m = group.size();
   int rc = EVOC_OK;
@@ -478,6 +490,7 @@ int evoc_gpu_server_create(const evoc_gpu_server_opts* opts, evoc_gpu_server** o
   s->lane_sizes.assign(size_t(s->lanes), evoc::CtxSizes{});
   auto bail = [&](int rc) {
     for (evoc_gpu_ctx* p : s->ctxs) evoc_gpu_ctx_destroy(p);
+    for (cudaStream_t u : s->urgent) cudaStreamDestroy(u);
     if (s->free_stream) cudaStreamDestroy(s->free_stream);
     if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
     if (s->pool) cudaMemPoolDestroy(s->pool);
@@ -486,6 +499,8 @@ int evoc_gpu_server_create(const evoc_gpu_server_opts* opts, evoc_gpu_server** o
   };
   s->profile = o.profile != 0;
   s->batch_max = std::min(std::max(o.batch_max, 0), kBatchJobs);
+  int least = 0, greatest = 0;
+  cudaDeviceGetStreamPriorityRange(&least, &greatest);
   for (int i = 0; i < s->lanes; i++) {
     evoc_gpu_ctx* c = nullptr;
     const int rc = evoc_gpu_ctx_create(o.device, &c);
@@ -493,6 +508,9 @@ int evoc_gpu_server_create(const evoc_gpu_server_opts* opts, evoc_gpu_server** o
     if (s->profile) evoc_gpu_profile_enable(c, 1);
     s->ctxs.push_back(c);
     s->streams.push_back(static_cast<cudaStream_t>(evoc_gpu_ctx_stream(c)));
+    cudaStream_t u = nullptr;
+    if (cudaStreamCreateWithPriority(&u, cudaStreamNonBlocking, greatest) != cudaSuccess) return bail(EVOC_ERR_CUDA);
+    s->urgent.push_back(u);
   }
   if (cudaStreamCreateWithFlags(&s->free_stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking) != cudaSuccess)
@@ -533,6 +551,7 @@ void evoc_gpu_server_destroy(evoc_gpu_server* s) {
   }
   cudaStreamSynchronize(s->free_stream);
   for (evoc_gpu_ctx* c : s->ctxs) evoc_gpu_ctx_destroy(c);
+  for (cudaStream_t u : s->urgent) cudaStreamDestroy(u);
   cudaStreamDestroy(s->free_stream);
   cudaStreamDestroy(s->copy_stream);
   cudaMemPoolDestroy(s->pool);

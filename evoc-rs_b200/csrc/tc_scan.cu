@@ -703,6 +703,11 @@ bool tc_scan_variant_feasible(int variant, int keep, bool has_scratch) {
   return variant_feasible(variant, keep, has_scratch);
 }
 
+bool tc_scan_uses_global_heaps(int variant, int keep) {
+  if (variant >= 0 && variant_feasible(variant, keep, true)) return kVariantCfg[variant][2] == 0;
+  return smem_bytes(3, 1, keep | 1) > SMEM_LIMIT;  // the automatic choice: no shared-memory variant fits
+}
+
 const char* tc_scan_variant_name(int variant) {
   static const char* names[6] = {"4 stages, 2 epilogue groups, shared-memory heaps",
                                  "3 stages, 2 epilogue groups, shared-memory heaps",

@@ -89,6 +89,7 @@ def lib():
             L.evoc_gpu_last_launch_count.argtypes = [P]
             L.evoc_gpu_last_certify.argtypes = [P, C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)]
             L.evoc_gpu_set_wait_limit.argtypes = [P, C.c_uint64, C.c_uint64]
+            L.evoc_gpu_last_nndescent.argtypes = [P, C.POINTER(i32), C.POINTER(i64), C.POINTER(i64)]
             _bind_optional(L)
             _lib = L
     return _lib
@@ -259,6 +260,12 @@ class Context:
         delays the scan's producer (tests of the timeout path)."""
         if lib().evoc_gpu_set_wait_limit(self.h, int(ns), int(producer_delay_ns)) != EVOC_OK:
             raise ValueError(self.last_error())
+
+    def nndescent_stats(self) -> dict:
+        """Iterations, distance evaluations and gathered row bytes of the last NN-descent call."""
+        it, ev, rb = C.c_int32(0), C.c_int64(0), C.c_int64(0)
+        lib().evoc_gpu_last_nndescent(self.h, C.byref(it), C.byref(ev), C.byref(rb))
+        return {"iterations": it.value, "distance_evals": ev.value, "row_bytes": rb.value}
 
     def certify_counts(self) -> dict:
         """Rows the last 16-bit-form call certified (checked), rescanned with 256 candidates

@@ -367,6 +367,13 @@ int evoc_gpu_last_launch_count(const evoc_gpu_ctx* ctx);
  * evoc-rs. */
 int evoc_gpu_set_wait_limit(evoc_gpu_ctx* ctx, uint64_t ns, uint64_t producer_delay_ns);
 
+/* The last NN-descent call on this context: iterations run, distances its
+ * joins computed, and the bytes of each row those distances gathered (the
+ * join's algorithmic traffic is distance_evals x row_bytes).  No counterpart
+ * in evoc-rs. */
+int evoc_gpu_last_nndescent(const evoc_gpu_ctx* ctx, int32_t* iterations, int64_t* distance_evals,
+                            int64_t* row_bytes);
+
 /* Certificate counts of the last BF16_RERANK call on this context: query
  * rows checked, rows that failed the first certificate (rescanned with 256
  * candidates), and rows rescanned exactly in FP32 after failing the second.

@@ -125,3 +125,15 @@ def test_device_pointer_entry():
     assert k == 10
     hi, hd = evoc.knn_graph(x, opts(10))
     assert np.array_equal(oi.cpu().numpy(), hi) and np.array_equal(od.cpu().numpy(), hd)
+
+
+@pytest.mark.parametrize("r0,r1", [(100, 612), (301, 777), (0, 1000), (996, 1000), (3, 4)])
+def test_fp32_row_slices_match_full_graph(r0, r1):
+    """Row slices give the full graph's rows bit for bit.  Slices starting at a
+    multiple of 4 take the k-major kernel, the others the row-major one; both
+    sum each dot in coordinate order, so their FP32 results agree exactly."""
+    rng = np.random.default_rng(11)
+    x = rng.standard_normal((1000, 100)).astype(np.float32)
+    fi, fd = evoc.knn_graph(x, opts(15))
+    si, sd = evoc.knn_graph(x, opts(15, row_begin=r0, row_end=r1))
+    assert np.array_equal(si, fi[r0:r1]) and np.array_equal(sd, fd[r0:r1])
