@@ -34,8 +34,13 @@ namespace {
 
 inline int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 
-int resolve_form(int32_t dtype, int32_t form) {
-  if (form == EVOC_FORM_AUTO) return dtype == EVOC_DTYPE_F32 ? EVOC_FORM_BF16_RERANK : EVOC_FORM_EXACT_INT;
+// The form a request runs.  NN-descent keeps a row's list in a warp's
+// registers, two keys per lane, so above k = 64 the request takes the dtype's
+// exact form instead (exact neighbour sets, at least the NN-descent recall).
+int resolve_form(int32_t dtype, int32_t form, int64_t keff = 0) {
+  const int exact = dtype == EVOC_DTYPE_F32 ? EVOC_FORM_BF16_RERANK : EVOC_FORM_EXACT_INT;
+  if (form == EVOC_FORM_AUTO) return exact;
+  if (form == EVOC_FORM_NNDESCENT && keff > 64) return exact;
   return form;
 }
 
@@ -209,10 +214,10 @@ CertLayout cert_layout(int64_t n, int64_t nq) {
 // Rescan arena for at most kRepairChunk rows: gathered 16-bit query rows,
 // their candidates, and gathered f32 query rows for the exact pass.
 struct RepairLayout {
-  size_t qh, cand2, qf, total;
+  size_t qh, cand2, qf, part, total;
 };
 
-RepairLayout repair_layout(int64_t nq, int64_t ld, int64_t ldb, int64_t C2) {
+RepairLayout repair_layout(int64_t nq, int64_t ld, int64_t ldb, int64_t C2, int64_t keff) {
   const int64_t R = std::min<int64_t>(nq, kRepairChunk);
   RepairLayout L{};
   size_t off = 0;
@@ -224,6 +229,7 @@ RepairLayout repair_layout(int64_t nq, int64_t ld, int64_t ldb, int64_t C2) {
   L.qh = take(size_t(evoc::padded_rows(R) * ldb * 2));
   L.cand2 = take(size_t(R * C2) * 4);
   L.qf = take(size_t(R * ld) * 4);
+  L.part = take(size_t(evoc::kSplitRowsMax) * size_t(keff) * 8);  // key-split partial lists of the exact pass
   L.total = off;
   return L;
 }
@@ -254,19 +260,39 @@ struct RescanJob {
   evoc::CertArgs cert;  // rnorm, hnorm, maxes, half_len of the request
 };
 
+// Key splits of the exact pass over `count` rows: enough work items for two
+// CTAs per SM, at least four 128-row key tiles per split, and the partial
+// lists within the arena (n_splits * count <= kSplitRowsMax).
+int exact_splits(const evoc_gpu_ctx* ctx, int64_t count, int64_t n) {
+  const int64_t qblocks = (count + 127) / 128;
+  int64_t s = int64_t(ctx->sms) * 2 / std::max<int64_t>(qblocks, 1);
+  s = std::min(s, ((n + 127) / 128) / 4);
+  s = std::min(s, evoc::kSplitRowsMax / std::max<int64_t>(count, 1));
+  return int(std::max<int64_t>(s, 1));
+}
+
 // The exact FP32 pass over rows listed on the device (output rows of j).
-int exact_rows(evoc_gpu_ctx* ctx, const RescanJob& j, const int32_t* list, int64_t count, float* qf) {
+// part: the arena's split lists (kSplitRowsMax x keff keys).
+int exact_rows(evoc_gpu_ctx* ctx, const RescanJob& j, const int32_t* list, int64_t count, float* qf,
+               uint64_t* part) {
   const int cap = evoc::topk_capacity(j.keff);
   const int64_t qblocks = (count + 127) / 128;
-  const int grid = int(std::min<int64_t>(qblocks, int64_t(ctx->sms) * 2));
+  const int splits = exact_splits(ctx, count, j.n);
+  const int grid = int(std::min<int64_t>(qblocks * splits, int64_t(ctx->sms) * 2));
   EVOC_TRY(evoc::launch_gather_rows_list(j.x, int64_t(j.ld) * 4, j.r0, list, count, count, qf, ctx->sms,
                                          ctx->stream),
            "gather rows");
   EVOC_TRY(ctx->scratch.ensure(size_t(grid) * 128 * size_t(cap) * 8), "alloc scratch");
   EVOC_TRY(evoc::launch_knn_f32_simt(j.x, j.n, j.ld, j.keff, cap, ctx->scratch.as<uint64_t>(), grid, j.idx, j.raw,
-                                     j.dist, 0, count, ctx->stream, qf, list, j.r0),
+                                     j.dist, 0, count, ctx->stream, qf, list, j.r0, splits, part),
            "exact rescan");
   ctx->launches += 2;
+  if (splits > 1) {
+    EVOC_TRY(evoc::launch_merge_key_splits(part, count, j.keff, splits, list, j.idx, j.raw, j.dist, ctx->sms,
+                                           ctx->stream),
+             "merge key splits");
+    ctx->launches += 1;
+  }
   return EVOC_OK;
 }
 
@@ -278,6 +304,20 @@ int32_t read_count(evoc_gpu_ctx* ctx, const int32_t* d_count, int* rc) {
   return v;
 }
 
+// Whether `rows` failed rows take the exact FP32 pass directly.  The 16-bit
+// rescan runs a CTA per 128 query rows over every key (a handful of rows
+// leave most SMs idle and pay the 256-candidate epilogue), while the exact
+// pass splits the keys over all SMs at the FP32 rate.  Estimated costs:
+// 16-bit waves x (128 n d 2 FLOP at ~6 TFLOP/s per SM) against
+// rows n d 2 FLOP at ~45 TFLOP/s.
+bool exact_first(const evoc_gpu_ctx* ctx, int64_t rows, int64_t n, int d) {
+  const double work = double(n) * double(d) * 2.0;
+  const double waves = std::ceil(double((rows + 127) / 128) / double(ctx->sms));
+  const double half_ms = waves * 128.0 * work / 6e12 * 1e3;
+  const double exact_ms = double(rows) * work / 45e12 * 1e3;
+  return exact_ms <= half_ms;
+}
+
 // Rows of j (output rows listed in fail1, `failed1` of them) that failed the
 // first certificate: the 16-bit scan again over those rows, gathered, keeping
 // 256 candidates, the rerank with the certificate; rows failing again (listed
@@ -287,14 +327,15 @@ int certify_rescan(evoc_gpu_ctx* ctx, const RescanJob& j, int32_t* fail1, int64_
                    float* bound2, int32_t* count2, int64_t* second, int64_t* exact) {
   Stage st(ctx, "certify_rescan");
   const int64_t C2 = second_pass_candidates(j.n);
-  const RepairLayout RL = repair_layout(std::min<int64_t>(failed1, kRepairChunk), j.ld, j.ldb, C2);
+  const RepairLayout RL = repair_layout(std::min<int64_t>(failed1, kRepairChunk), j.ld, j.ldb, C2, j.keff);
   EVOC_TRY(ctx->repair.ensure(RL.total), "alloc rescan arena");
   uint8_t* rb = ctx->repair.as<uint8_t>();
   float* qf = reinterpret_cast<float*>(rb + RL.qf);
+  uint64_t* part = reinterpret_cast<uint64_t*>(rb + RL.part);
   int64_t failed2 = 0;
   int rc = EVOC_OK;
   *second = failed1;
-  if (C2 > j.C) {
+  if (C2 > j.C && !exact_first(ctx, failed1, j.n, j.d)) {
     void* qh = rb + RL.qh;
     int32_t* cand2 = reinterpret_cast<int32_t*>(rb + RL.cand2);
     EVOC_TRY(ctx->scratch.ensure(scan_scratch_bytes(ctx, std::min<int64_t>(failed1, kRepairChunk), C2)),
@@ -325,13 +366,15 @@ int certify_rescan(evoc_gpu_ctx* ctx, const RescanJob& j, int32_t* fail1, int64_
     failed2 = read_count(ctx, count2, &rc);
     if (rc) return rc;
   } else {
-    fail2 = fail1;  // no larger candidate set exists: every failed row goes to the exact pass
+    // no larger candidate set exists, or the rows are few enough that the
+    // exact pass over key splits is the cheaper: every failed row goes there
+    fail2 = fail1;
     failed2 = failed1;
   }
   *exact = failed2;
   for (int64_t c0 = 0; c0 < failed2; c0 += kRepairChunk) {
     const int64_t cnt = std::min<int64_t>(kRepairChunk, failed2 - c0);
-    rc = exact_rows(ctx, j, fail2 + c0, cnt, qf);
+    rc = exact_rows(ctx, j, fail2 + c0, cnt, qf, part);
     if (rc) return rc;
   }
   return EVOC_OK;
@@ -341,9 +384,11 @@ int certify_rescan(evoc_gpu_ctx* ctx, const RescanJob& j, int32_t* fail1, int64_
 // row, FP32 rerank with the per-row certificate (rerank.cu), then for rows
 // that fail it a second scan keeping 256 candidates, and for rows that fail
 // again an exact FP32 scan.  Every returned row is either certified or exact.
+// Beyond 256 candidates per row (the rerank's shared-memory limit) every row
+// takes the exact FP32 scan directly.
 int run_bf16_rerank(evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, const Job& j, int ld, int d) {
   const int64_t C = bf16_candidates(opts, j.n, j.keff);
-  if (C > 256) return fail(ctx, EVOC_ERR_UNSUPPORTED, "oversample * k must be <= 256");
+  if (C > 256) return run_fp32(ctx, j, ld);
   if (opts.scan_type != evoc::kHalfF16 && opts.scan_type != evoc::kHalfBf16)
     return fail(ctx, EVOC_ERR_ARG, "scan_type must be 0 (FP16) or 1 (BF16)");
   const int half = opts.scan_type;
@@ -515,7 +560,7 @@ int fuzzy_impl(evoc_gpu_ctx* ctx, const int32_t* idx, const float* dist, int64_t
   ctx->n_stages = 0;
   ctx->launches = 0;
   if (n <= 0) return fail(ctx, EVOC_ERR_EMPTY, "empty kNN graph");
-  if (k <= 0 || k > 64) return fail(ctx, EVOC_ERR_ARG, "k must be in 1..64");
+  if (k <= 0) return fail(ctx, EVOC_ERR_ARG, "k must be positive");
   if (!dist || (graph && (!idx || !indptr))) return fail(ctx, EVOC_ERR_ARG, "null input or output");
   EVOC_TRY(cudaSetDevice(ctx->device), "cudaSetDevice");
   Stage total(ctx, "total");
@@ -629,7 +674,7 @@ int nnd_max_candidates(const evoc_gpu_opts& opts, int k) {
 size_t nnd_work_sizes(int64_t n, int k, int mc, size_t* sizes) {
   const size_t nk = size_t(n) * size_t(k);
   const size_t v[kNndParts] = {nk * 8, nk * 8, nk, nk, size_t(n) * 4, size_t(n + 1) * 8, size_t(n) * 4, nk * 4,
-                               size_t(n) * size_t(2 * mc) * 4, 64, 64, 64};
+                               size_t(n) * size_t(2 * mc) * 4, 64, size_t(1 + evoc::kNndSumParts) * 8, 64};
   size_t total = 0;
   for (int i = 0; i < kNndParts; i++) {
     sizes[i] = v[i];
@@ -641,7 +686,6 @@ size_t nnd_work_sizes(int64_t n, int k, int mc, size_t* sizes) {
 int run_nndescent(evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, const Job& j, int32_t dtype, int64_t row_bytes,
                   const void* rows, int ld_f32, int d, const int64_t* rng_state) {
   if (j.r0 != 0 || j.nq != j.n) return fail(ctx, EVOC_ERR_UNSUPPORTED, "the NN-descent form builds whole graphs only");
-  if (j.keff > 64) return fail(ctx, EVOC_ERR_UNSUPPORTED, "the NN-descent form supports k <= 64");
   const int64_t n = j.n;
   const int k = j.keff;
   const int mc = nnd_max_candidates(opts, k);
@@ -711,7 +755,7 @@ int run_nndescent(evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, const Job& j, in
     Stage st(ctx, "nnd_iteration");
     EVOC_TRY(cudaMemsetAsync(a.changes, 0, 8, ctx->stream), "clear changes");
     EVOC_TRY(evoc::launch_nnd_iteration(a, cur, it, ctx->stream), "NN-descent iteration");
-    ctx->launches += 6;
+    ctx->launches += 7;
     cur ^= 1;
     unsigned long long ch = 0;
     double sum = 0.0;
@@ -776,7 +820,7 @@ int knn_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtype, con
   if (kk < 1) kk = 1;
   const int keff = int(kk);
   if (out_k) *out_k = keff;
-  const int form = resolve_form(dtype, opts.form);
+  const int form = resolve_form(dtype, opts.form, keff);
   const bool on_dev = opts.buffers_on_device != 0;
   EVOC_TRY(cudaSetDevice(ctx->device), "cudaSetDevice");
   Stage total(ctx, "total");
@@ -1562,7 +1606,7 @@ void knn_buffer_needs(const evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, int32_
   *need = CtxSizes{};
   size_t* b = need->b;
   const int64_t keff = std::max<int64_t>(1, std::min<int64_t>(k, n - 1));
-  const int form = resolve_form(dtype, opts.form);
+  const int form = resolve_form(dtype, opts.form, keff);
   const int64_t rows = padded_rows(n);
   const int64_t qblocks = (n + 127) / 128;
   const int64_t grid = std::min<int64_t>(qblocks, ctx->sms);
@@ -1583,7 +1627,8 @@ void knn_buffer_needs(const evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, int32_
     b[kBufX] = size_t(rows * round_up(dim, 16) * 4);
     b[kBufNorms] = size_t(n) * 4;
     const int64_t ldb = round_up(dim, 64);
-    if (form == EVOC_FORM_FP32) {
+    if (form == EVOC_FORM_FP32 ||
+        (form == EVOC_FORM_BF16_RERANK && bf16_candidates(opts, n, int(keff)) > 256)) {
       const int64_t g = std::min<int64_t>(qblocks, int64_t(ctx->sms) * 2);
       b[kBufScratch] = size_t(g) * 128 * size_t(topk_capacity(int(keff))) * 8;
       b[kBufXb] = size_t(knn_f32_kt_cols(n)) * size_t(round_up(dim, 16)) * 4;  // the k-major copy
@@ -1598,7 +1643,7 @@ void knn_buffer_needs(const evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, int32_
         const int64_t C2 = second_pass_candidates(n);
         const int64_t R = std::min<int64_t>(n, kRepairChunk);
         b[kBufCert] = cert_layout(n, n).total;
-        b[kBufRepair] = repair_layout(R, round_up(dim, 16), ldb, C2).total;
+        b[kBufRepair] = repair_layout(R, round_up(dim, 16), ldb, C2, keff).total;
         const int64_t g3 = std::min<int64_t>((R + 127) / 128, int64_t(ctx->sms) * 2);
         b[kBufScratch] = std::max({b[kBufScratch], scan_scratch_bytes(ctx, R, C2),
                                    size_t(g3) * 128 * size_t(topk_capacity(int(keff))) * 8});
@@ -1655,7 +1700,7 @@ bool batch_buffer_needs(const evoc_gpu_opts& opts, int32_t dtype, int32_t n_jobs
     const int64_t R = std::min<int64_t>(L.max_n, kRepairChunk);
     const int64_t C2 = second_pass_candidates(L.max_n);
     need->b[kBufCert] = cert_layout(L.max_n, L.max_n).total;
-    need->b[kBufRepair] = repair_layout(R, round_up(max_dim, 16), round_up(max_dim, 64), C2).total;
+    need->b[kBufRepair] = repair_layout(R, round_up(max_dim, 16), round_up(max_dim, 64), C2, max_keff).total;
     // the batch's plan holds no context scratch: the rescans' scan and exact pass size it
     const int sms = 148;  // upper bound of the grids on B200 (scan_grid caps at the SM count)
     const int64_t g2 = std::min<int64_t>((R + 127) / 128, sms);

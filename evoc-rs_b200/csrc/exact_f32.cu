@@ -11,6 +11,12 @@
 // (register-prefetched double buffer), the 128x128 score tile is staged in
 // shared memory, and 128 owner threads (one per query row) feed their row's
 // scores to a thread-private candidate buffer in global scratch.
+//
+// Key splits: with n_splits > 1 a query block is n_splits work items, each
+// over a contiguous range of key tiles, writing its rows' sorted top-k keys
+// to `partial` (split-major); merge_key_splits_kernel then takes each row's k
+// smallest keys of all splits.  A few query rows (the certificate's failed
+// rows) then still spread over every SM.
 #include <algorithm>
 
 #include "common.cuh"
@@ -56,16 +62,22 @@ __global__ void __launch_bounds__(NT, 2)
 knn_f32_simt_kernel(const float* __restrict__ X, int64_t n, int ld, int k, int cap,
                     uint64_t* __restrict__ scratch, int32_t* __restrict__ out_idx, float* __restrict__ out_raw,
                     float* __restrict__ out_dist, int64_t q_begin, int64_t q_end, const float* __restrict__ Q,
-                    const int32_t* __restrict__ q_list, int64_t q_row0) {
+                    const int32_t* __restrict__ q_list, int64_t q_row0, int n_splits, uint64_t* __restrict__ partial) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   F32Smem& sm = *reinterpret_cast<F32Smem*>(smem_raw);
   const int tid = threadIdx.x;
   const int ty = tid >> 4, tx = tid & 15;
   const int64_t n_qblocks = (q_end - q_begin + BM - 1) / BM;
-  const int64_t n_ktiles = (n + BN - 1) / BN;
+  const int64_t n_tiles_all = (n + BN - 1) / BN;
+  const int64_t tiles_per = (n_tiles_all + n_splits - 1) / n_splits;
+  const int64_t n_items = n_qblocks * n_splits;
   uint64_t* my_buf = scratch + (int64_t(blockIdx.x) * BM + (tid & (BM - 1))) * cap;
 
-  for (int64_t qb = blockIdx.x; qb < n_qblocks; qb += gridDim.x) {
+  for (int64_t item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int64_t qb = item / n_splits;
+    const int sp = int(item % n_splits);
+    const int64_t kt_begin = sp * tiles_per;
+    const int64_t n_ktiles = kt_begin + tiles_per < n_tiles_all ? kt_begin + tiles_per : n_tiles_all;
     const int64_t q0 = q_begin + qb * BM;
     RowTopK top;
     top.init(my_buf, k, cap);
@@ -73,7 +85,7 @@ knn_f32_simt_kernel(const float* __restrict__ X, int64_t n, int ld, int k, int c
     // this query's row of X (the self rule) and its output row
     const int64_t my_self = (q_list && tid < BM && my_q < q_end) ? q_row0 + q_list[my_q] : my_q;
 
-    for (int64_t kt = 0; kt < n_ktiles; kt++) {
+    for (int64_t kt = kt_begin; kt < n_ktiles; kt++) {
       const int64_t c0 = kt * BN;
       float acc[8][8];
 #pragma unroll
@@ -138,7 +150,12 @@ knn_f32_simt_kernel(const float* __restrict__ X, int64_t n, int ld, int k, int c
       }
       __syncthreads();
     }
-    if (tid < BM && my_q < q_end) {
+    if (tid < BM && my_q < q_end && partial) {
+      // this split's sorted top-k keys of the row (kKeyInf past the end)
+      const int got = top.finish();
+      uint64_t* dst = partial + (int64_t(sp) * (q_end - q_begin) + (my_q - q_begin)) * k;
+      for (int j = 0; j < k; j++) dst[j] = j < got ? top.buf[j] : kKeyInf;
+    } else if (tid < BM && my_q < q_end) {
       const int got = top.finish();
       const int64_t orow = (q_list ? int64_t(q_list[my_q]) : my_q - q_begin) * k;
       for (int j = 0; j < k; j++) {
@@ -156,18 +173,69 @@ knn_f32_simt_kernel(const float* __restrict__ X, int64_t n, int ld, int k, int c
   }
 }
 
+// Warp per row r of `rows`: the k smallest of the row's n_splits sorted
+// partial lists (keys are unique but for kKeyInf), taken one at a time as the
+// smallest key above the last one taken; written to output row q_list[r] (or
+// r) as (index, raw, transformed distance).
+__global__ void merge_key_splits_kernel(const uint64_t* __restrict__ partial, int64_t rows, int k, int n_splits,
+                                        const int32_t* __restrict__ q_list, int32_t* __restrict__ out_idx,
+                                        float* __restrict__ out_raw, float* __restrict__ out_dist) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = int64_t(gridDim.x) * (blockDim.x >> 5);
+  for (int64_t r = int64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); r < rows; r += warps) {
+    const int64_t orow = (q_list ? int64_t(q_list[r]) : r) * k;
+    const int total = n_splits * k;
+    uint64_t last = 0;
+    bool first = true;
+    for (int j = 0; j < k; j++) {
+      uint64_t best = kKeyInf;
+      for (int e = lane; e < total; e += 32) {
+        const int s = e / k, t = e - s * k;
+        const uint64_t key = partial[(int64_t(s) * rows + r) * k + t];
+        if ((first || key > last) && key < best) best = key;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const uint64_t other = __shfl_xor_sync(0xffffffffu, best, o);
+        best = other < best ? other : best;
+      }
+      first = false;
+      last = best;
+      if (lane == 0) {
+        const bool ok = best != kKeyInf;
+        const float raw = ok ? from_orderable(uint32_t(best >> 32)) : kHeapInf;
+        out_idx[orow + j] = ok ? key_index(best) : -1;
+        if (out_raw) out_raw[orow + j] = raw;
+        if (out_dist) out_dist[orow + j] = transform_raw(0, raw);
+      }
+    }
+  }
+}
+
 size_t knn_f32_simt_smem() { return sizeof(F32Smem); }
 
 cudaError_t launch_knn_f32_simt(const float* X, int64_t n, int ld, int k, int cap, uint64_t* scratch,
                                 int grid, int32_t* out_idx, float* out_raw, float* out_dist, int64_t q_begin,
                                 int64_t q_end, cudaStream_t stream, const float* Q, const int32_t* q_list,
-                                int64_t q_row0) {
+                                int64_t q_row0, int n_splits, uint64_t* partial) {
   if ((Q == nullptr) != (q_list == nullptr)) return cudaErrorInvalidValue;
+  if (n_splits < 1 || (n_splits > 1 && partial == nullptr)) return cudaErrorInvalidValue;
   const size_t smem = sizeof(F32Smem);
   cudaError_t e = cudaFuncSetAttribute(knn_f32_simt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   knn_f32_simt_kernel<<<grid, NT, smem, stream>>>(X, n, ld, k, cap, scratch, out_idx, out_raw, out_dist, q_begin,
-                                                   q_end, Q ? Q : X, q_list, q_row0);
+                                                   q_end, Q ? Q : X, q_list, q_row0, n_splits,
+                                                   n_splits > 1 ? partial : nullptr);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_merge_key_splits(const uint64_t* partial, int64_t rows, int k, int n_splits,
+                                    const int32_t* q_list, int32_t* out_idx, float* out_raw, float* out_dist,
+                                    int sms, cudaStream_t stream) {
+  if (rows <= 0) return cudaSuccess;
+  const int64_t blocks = std::min<int64_t>((rows + 7) / 8, int64_t(sms) * 8);
+  merge_key_splits_kernel<<<int(blocks), 256, 0, stream>>>(partial, rows, k, n_splits, q_list, out_idx, out_raw,
+                                                          out_dist);
   return cudaGetLastError();
 }
 
@@ -180,6 +248,13 @@ cudaError_t launch_knn_f32_simt(const float* X, int64_t n, int ld, int k, int ca
 // flight and takes one barrier per k-step.  The score tile has its own shared
 // memory, so the next tile's first copy overlaps the top-k epilogue.
 //
+// Epilogue: every thread filters its 8 x 8 scores against their rows'
+// current admission thresholds (published in shared memory by the row
+// owners) and marks the survivors in a per-row 128-bit mask; a row owner
+// then offers only the marked columns, in column order.  The filter drops
+// exactly the scores the owner's offer would reject on the raw value, so the
+// kept sets are those of a full scan.
+//
 // Alignment: query block starts q_begin + 128 i must be multiples of 4 floats
 // (the host takes this form only when q_begin % 4 == 0); key tiles start at
 // multiples of 128.  Bounds: a query tile reads columns q0 .. q0+127 with
@@ -189,7 +264,9 @@ namespace {
 struct F32KtSmem {
   float a[2][BK][APAD];
   float b[2][BK][APAD];
-  float s[BM][SPAD];
+  float s[BM][SPAD];      // surviving scores (raw), at their columns
+  uint32_t mask[BM][4];   // survivor columns of each row
+  float thr[BM];          // each row's admission threshold (raw); -inf: no row
 };
 
 __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
@@ -233,6 +310,11 @@ knn_f32_kt_kernel(const float* __restrict__ XT, int64_t cols, int64_t n, int ld,
     const int64_t my_q = q0 + tid;
     RowTopK top;
     top.init(my_buf, k, cap);
+    if (tid < BM) {
+      sm.thr[tid] = (my_q < q_end) ? top.thr_raw : __int_as_float(0xff800000);
+#pragma unroll
+      for (int w = 0; w < 4; w++) sm.mask[tid][w] = 0u;
+    }
     float acc[8][8];
     int stage = 0;
     kt_issue(sm, 0, XT, cols, q0, 0, 0, tid);
@@ -274,27 +356,47 @@ knn_f32_kt_kernel(const float* __restrict__ XT, int64_t cols, int64_t n, int ld,
       }
       stage ^= 1;
       if (++ks == nk) {
-        // The tile is complete: stage it and let the 128 row owners take it.
-        // The score tile is next written a full tile later, after at least one
-        // more top-of-step barrier, so the owners' reads below are done by then.
+        // The tile is complete: filter it, then let the 128 row owners take
+        // the survivors.  Scores, masks and thresholds are next written a full
+        // tile later, after at least one more top-of-step barrier, so the
+        // owners' reads and updates below are done by then.
+        const int64_t c0 = kt * BN;
 #pragma unroll
         for (int i = 0; i < 8; i++) {
           const int r = (i < 4) ? ty * 4 + i : 64 + ty * 4 + (i - 4);
+          const float t = sm.thr[r];
+          const int64_t qrow = q0 + r;
+          uint32_t lo = 0u, hi = 0u;
 #pragma unroll
           for (int j = 0; j < 8; j++) {
             const int c = (j < 4) ? tx * 4 + j : 64 + tx * 4 + (j - 4);
-            sm.s[r][c] = acc[i][j];
+            const int64_t key = c0 + c;
+            const float raw = (key == qrow) ? -1.0f : raw_cosine(acc[i][j]);
+            if (key < n && raw <= t) {
+              sm.s[r][c] = raw;
+              if (j < 4) lo |= 1u << ((tx & 7) * 4 + j);
+              else hi |= 1u << ((tx & 7) * 4 + (j - 4));
+            }
           }
+          if (lo) atomicOr(&sm.mask[r][tx >> 3], lo);
+          if (hi) atomicOr(&sm.mask[r][2 + (tx >> 3)], hi);
         }
         __syncthreads();
-        if (tid < BM && my_q < q_end) {
-          const int64_t c0 = kt * BN;
-          const int lim = (n - c0 < BN) ? int(n - c0) : BN;
-          for (int c = 0; c < lim; c++) {
-            const int64_t key = c0 + c;
-            const float raw = (key == my_q) ? -1.0f : raw_cosine(sm.s[tid][c]);
-            top.offer(raw, int32_t(key));
+        if (tid < BM) {
+          if (my_q < q_end) {
+#pragma unroll
+            for (int w = 0; w < 4; w++) {
+              uint32_t m = sm.mask[tid][w];
+              while (m) {
+                const int c = w * 32 + __ffs(m) - 1;
+                m &= m - 1u;
+                top.offer(sm.s[tid][c], int32_t(c0 + c));
+              }
+            }
+            sm.thr[tid] = top.thr_raw;
           }
+#pragma unroll
+          for (int w = 0; w < 4; w++) sm.mask[tid][w] = 0u;
         }
         ks = 0;
         kt++;

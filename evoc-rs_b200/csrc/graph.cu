@@ -12,17 +12,14 @@
 //                         order SciPy's row-wise merge rounds it, zeros dropped,
 //                         rows sorted by column (canonical CSR)
 //
-// One thread owns one row for sigma/rho/membership (k <= 64 distances); the
+// One thread owns one row for sigma/rho/membership (any k: the row's
+// membership entries are insertion-sorted in place in its output slots); the
 // transpose is a column-count / scan / scatter / per-bucket sort; the union
 // is a per-row two-pointer merge done twice (count, then write).
 #include "common.cuh"
 #include "kernels.h"
 
 namespace evoc {
-
-namespace {
-constexpr int kMaxK = 64;
-}
 
 // Sets *need_mean when some row has no positive distance (its sigma floor uses
 // the mean of all distances).
@@ -107,8 +104,8 @@ __global__ void fuzzy_rows_kernel(const int32_t* __restrict__ idx, const float* 
     sigma_out[i] = sig;
     rho_out[i] = rh;
 
-    int32_t cols[kMaxK];
-    float vals[kMaxK];
+    int32_t* cols = a_cols + i * k;  // the row's k output slots, filled in column order
+    float* vals = a_vals + i * k;
     int cnt = 0;
     for (int j = 0; j < k; j++) {
       const int32_t c = idx[i * k + j];
@@ -129,11 +126,7 @@ __global__ void fuzzy_rows_kernel(const int32_t* __restrict__ idx, const float* 
       cols[p] = c;
       vals[p] = w;
     }
-    for (int t = 0; t < cnt; t++) {
-      a_cols[i * k + t] = cols[t];
-      a_vals[i * k + t] = vals[t];
-      atomicAdd(&indeg[cols[t]], 1);
-    }
+    for (int t = 0; t < cnt; t++) atomicAdd(&indeg[cols[t]], 1);
     a_cnt[i] = cnt;
   }
 }
@@ -357,7 +350,7 @@ cudaError_t launch_scan_counts(const int32_t* cnt, int64_t n, int64_t* out, cuda
 
 cudaError_t launch_smooth_and_membership(const int32_t* idx, const float* dist, int64_t n, int k, float n_neighbors,
                                          const FuzzyWork& w, float* sigma, float* rho, int sms, cudaStream_t stream) {
-  if (k < 1 || k > kMaxK) return cudaErrorInvalidValue;
+  if (k < 1) return cudaErrorInvalidValue;
   cudaError_t e = cudaMemsetAsync(w.flags, 0, 2 * sizeof(int), stream);
   if (e != cudaSuccess) return e;
   e = cudaMemsetAsync(w.indeg, 0, size_t(n) * sizeof(int32_t), stream);

@@ -26,7 +26,15 @@ cudaError_t launch_knn_f32_kt(const float* X, int64_t n, int ld, float* XT, int 
 cudaError_t launch_knn_f32_simt(const float* X, int64_t n, int ld, int k, int cap, uint64_t* scratch, int grid,
                                 int32_t* out_idx, float* out_raw, float* out_dist, int64_t q_begin, int64_t q_end,
                                 cudaStream_t stream, const float* Q = nullptr, const int32_t* q_list = nullptr,
-                                int64_t q_row0 = 0);
+                                int64_t q_row0 = 0, int n_splits = 1, uint64_t* partial = nullptr);
+// With n_splits > 1, launch_knn_f32_simt writes each split's sorted top-k keys
+// of the (q_end - q_begin) rows to `partial` (n_splits x rows x k); this
+// takes each row's k best of them into the outputs (row q_list[r], or r).
+cudaError_t launch_merge_key_splits(const uint64_t* partial, int64_t rows, int k, int n_splits,
+                                    const int32_t* q_list, int32_t* out_idx, float* out_raw, float* out_dist,
+                                    int sms, cudaStream_t stream);
+// Bound on n_splits x rows x ... : the host keeps n_splits * rows <= this.
+constexpr int64_t kSplitRowsMax = 2 * 148 * 128;
 
 // Candidate-buffer capacity used by every fused top-k epilogue for k kept keys.
 // Rows allocated for an n-row device matrix: the tensor-core scan's TMA boxes
@@ -203,9 +211,10 @@ struct NndArgs {
   int32_t* rrows;         // n x k
   int32_t* cand;          // n x 2 mc: tagged candidate ids (bit 31 = new), -1 past the end
   unsigned long long* changes;
-  double* sum;            // the new graph's sum of finite raw dissimilarities
+  double* sum;            // [0]: the new graph's sum of finite raw dissimilarities; [1 ..]: kNndSumParts partials
   unsigned long long* evals;  // distances the joins computed (accumulates over iterations)
 };
+constexpr int kNndSumParts = 1024;
 cudaError_t launch_nnd_init(const NndArgs& a, cudaStream_t stream);
 cudaError_t launch_nnd_iteration(const NndArgs& a, int cur, int iter, cudaStream_t stream);
 cudaError_t launch_nnd_emit(const NndArgs& a, int cur, int32_t* out_idx, float* out_raw, float* out_dist,

@@ -719,6 +719,69 @@ __global__ void center_apply_kernel(const float* result, int64_t n, int ncomp, f
 
 constexpr int kPcaMax = 64;
 
+// Cyclic Jacobi rotations by one warp on the symmetric nn x nn matrix A (row
+// stride kPcaMax, f64, in shared memory), accumulating the eigenvectors into
+// V (columns; V starts as the identity).  Stops when the off-diagonal mass is
+// below 1e-30 of the total, or after 60 sweeps.
+__device__ void jacobi_warp(double* A, double* V, int nn, int lane) {
+  for (int sweep = 0; sweep < 60; sweep++) {
+    double off = 0.0, tot = 0.0;
+    for (int i = lane; i < nn * nn; i += 32) {
+      const int a = i / nn, b = i % nn;
+      const double v = A[a * kPcaMax + b] * A[a * kPcaMax + b];
+      tot += v;
+      if (a != b) off += v;
+    }
+    for (int o = 16; o; o >>= 1) {
+      off += __shfl_xor_sync(kFull, off, o);
+      tot += __shfl_xor_sync(kFull, tot, o);
+    }
+    if (off <= 1e-30 * tot || off == 0.0) break;
+    for (int p = 0; p < nn - 1; p++)
+      for (int q = p + 1; q < nn; q++) {
+        const double apq = A[p * kPcaMax + q];
+        if (apq == 0.0) continue;
+        const double tau = (A[q * kPcaMax + q] - A[p * kPcaMax + p]) / (2.0 * apq);
+        const double tt = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+        const double c = 1.0 / sqrt(1.0 + tt * tt), s = tt * c;
+        for (int k = lane; k < nn; k += 32) {
+          const double akp = A[k * kPcaMax + p], akq = A[k * kPcaMax + q];
+          A[k * kPcaMax + p] = c * akp - s * akq;
+          A[k * kPcaMax + q] = s * akp + c * akq;
+          const double vkp = V[k * kPcaMax + p], vkq = V[k * kPcaMax + q];
+          V[k * kPcaMax + p] = c * vkp - s * vkq;
+          V[k * kPcaMax + q] = s * vkp + c * vkq;
+        }
+        __syncwarp();
+        for (int k = lane; k < nn; k += 32) {
+          const double apk = A[p * kPcaMax + k], aqk = A[q * kPcaMax + k];
+          A[p * kPcaMax + k] = c * apk - s * aqk;
+          A[q * kPcaMax + k] = s * apk + c * aqk;
+        }
+        __syncwarp();
+      }
+  }
+}
+
+// normalize_small_graph_init_like_python (src/label_prop.rs:251-262), by one
+// thread: subtract the f64 mean of all entries (element order), then divide
+// by (max - min) / 2 in f32 when positive.
+__device__ void small_init_normalise(float* out, int count) {
+  double m = 0.0;
+  for (int i = 0; i < count; i++) m = __dadd_rn(m, (double)out[i]);
+  m = __ddiv_rn(m, (double)count);
+  float lo = INFINITY, hi = -INFINITY;
+  for (int i = 0; i < count; i++) {
+    const float v = __double2float_rn(__dsub_rn((double)out[i], m));
+    out[i] = v;
+    lo = fminf(lo, v);
+    hi = fmaxf(hi, v);
+  }
+  const float scale = __fdiv_rn(__fsub_rn(hi, lo), 2.0f);
+  if (scale > 0.0f)
+    for (int i = 0; i < count; i++) out[i] = __fdiv_rn(out[i], scale);
+}
+
 // One block.  Centred rows X (f64, f32 column means), Gram G = X X^T, cyclic
 // Jacobi (one warp) for G's eigenpairs; component j = sign_j * sqrt(l_j) *
 // u_j with the sign that makes the largest-|.| entry of X^T u_j (the last on
@@ -754,43 +817,7 @@ __global__ void __launch_bounds__(256) pca_kernel(const float* x, int64_t n, int
   __syncthreads();
   if (t < 32) {
     const int lane = t;
-    for (int sweep = 0; sweep < 60; sweep++) {
-      double off = 0.0, tot = 0.0;
-      for (int i = lane; i < nn * nn; i += 32) {
-        const int a = i / nn, b = i % nn;
-        const double v = A[a * kPcaMax + b] * A[a * kPcaMax + b];
-        tot += v;
-        if (a != b) off += v;
-      }
-      for (int o = 16; o; o >>= 1) {
-        off += __shfl_xor_sync(kFull, off, o);
-        tot += __shfl_xor_sync(kFull, tot, o);
-      }
-      if (off <= 1e-30 * tot || off == 0.0) break;
-      for (int p = 0; p < nn - 1; p++)
-        for (int q = p + 1; q < nn; q++) {
-          const double apq = A[p * kPcaMax + q];
-          if (apq == 0.0) continue;
-          const double tau = (A[q * kPcaMax + q] - A[p * kPcaMax + p]) / (2.0 * apq);
-          const double tt = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-          const double c = 1.0 / sqrt(1.0 + tt * tt), s = tt * c;
-          for (int k = lane; k < nn; k += 32) {
-            const double akp = A[k * kPcaMax + p], akq = A[k * kPcaMax + q];
-            A[k * kPcaMax + p] = c * akp - s * akq;
-            A[k * kPcaMax + q] = s * akp + c * akq;
-            const double vkp = V[k * kPcaMax + p], vkq = V[k * kPcaMax + q];
-            V[k * kPcaMax + p] = c * vkp - s * vkq;
-            V[k * kPcaMax + q] = s * vkp + c * vkq;
-          }
-          __syncwarp();
-          for (int k = lane; k < nn; k += 32) {
-            const double apk = A[p * kPcaMax + k], aqk = A[q * kPcaMax + k];
-            A[p * kPcaMax + k] = c * apk - s * aqk;
-            A[q * kPcaMax + k] = s * apk + c * aqk;
-          }
-          __syncwarp();
-        }
-    }
+    jacobi_warp(A, V, nn, lane);
     if (lane == 0) {
       for (int i = 0; i < nn; i++) {
         s_eval[i] = A[i * kPcaMax + i];
@@ -839,20 +866,192 @@ __global__ void __launch_bounds__(256) pca_kernel(const float* x, int64_t n, int
     out[i] = v;
   }
   __syncthreads();
-  if (t == 0) {
-    double m = 0.0;
-    for (int i = 0; i < nn * ncomp; i++) m = __dadd_rn(m, (double)out[i]);
-    m = __ddiv_rn(m, (double)(nn * ncomp));
-    float lo = INFINITY, hi = -INFINITY;
-    for (int i = 0; i < nn * ncomp; i++) {
-      const float v = __double2float_rn(__dsub_rn((double)out[i], m));
-      out[i] = v;
-      lo = fminf(lo, v);
-      hi = fmaxf(hi, v);
+  if (t == 0) small_init_normalise(out, nn * ncomp);
+}
+
+// ------------------------------------------------------------------ spectral / MDS / random base inits
+
+// pairwise_sq_distances (src/label_prop.rs:322-337): f32, coordinates summed
+// in order with separate multiply and add; D is nn x nn (row stride kPcaMax).
+__device__ void pairwise_sq(const float* x, int nn, int64_t d, float* D) {
+  for (int pq = threadIdx.x; pq < nn * nn; pq += blockDim.x) {
+    const int a = pq / nn, b = pq % nn;
+    if (b < a) continue;
+    float sq = 0.0f;
+    for (int64_t c = 0; c < d; c++) {
+      const float diff = __fsub_rn(x[(int64_t)a * d + c], x[(int64_t)b * d + c]);
+      sq = __fadd_rn(sq, __fmul_rn(diff, diff));
     }
-    const float scale = __fdiv_rn(__fsub_rn(hi, lo), 2.0f);
-    if (scale > 0.0f)
-      for (int i = 0; i < nn * ncomp; i++) out[i] = __fdiv_rn(out[i], scale);
+    D[a * kPcaMax + b] = sq;
+    D[b * kPcaMax + a] = sq;
+  }
+}
+
+// One block: spectral_init (mode 0, src/label_prop.rs:364-423) or mds_init
+// (mode 1, 339-362) of nn <= 64 rows, then the small-graph normalisation.
+// The symmetric eigen-decomposition is cyclic Jacobi in f64 on the f32
+// matrix (the reference: faer's f32 solver), eigenvalues ascending (stable
+// in index order), each eigenvector's largest-|.| entry (the first on ties)
+// made non-negative.
+__global__ void __launch_bounds__(256) spectral_mds_kernel(const float* x, int64_t n, int64_t d, int ncomp, int mode,
+                                                           float* out) {
+  extern __shared__ double sh[];
+  double* A = sh;                         // nn x nn
+  double* V = sh + kPcaMax * kPcaMax;     // nn x nn
+  double* T = sh + 2 * kPcaMax * kPcaMax; // nn x nn (MDS: H D)
+  float* D = reinterpret_cast<float*>(sh + 3 * kPcaMax * kPcaMax);  // nn x nn
+  __shared__ float s_deg[kPcaMax];
+  __shared__ double s_eval[kPcaMax];
+  __shared__ int s_order[kPcaMax];
+  __shared__ float s_sigma;
+  const int t = threadIdx.x;
+  const int nn = (int)n;
+  pairwise_sq(x, nn, d, D);
+  for (int i = t; i < kPcaMax * kPcaMax; i += blockDim.x) V[i] = (i / kPcaMax == i % kPcaMax) ? 1.0 : 0.0;
+  __syncthreads();
+  if (mode == 0) {
+    // sigma: sqrt of the element at index len/2 of the sorted positive
+    // distances (both triangles), floored at 1e-8; 1 when none is positive.
+    int npos = 0;
+    for (int i = 0; i < nn * nn; i++) npos += D[(i / nn) * kPcaMax + i % nn] > 0.0f;
+    if (t == 0) s_sigma = 1.0f;
+    __syncthreads();
+    const int r = npos / 2;
+    for (int i = t; i < nn * nn; i += blockDim.x) {
+      const float v = D[(i / nn) * kPcaMax + i % nn];
+      if (!(v > 0.0f)) continue;
+      int less = 0, le = 0;
+      for (int j = 0; j < nn * nn; j++) {
+        const float w = D[(j / nn) * kPcaMax + j % nn];
+        if (w > 0.0f) {
+          less += w < v;
+          le += w <= v;
+        }
+      }
+      if (less <= r && r < le) s_sigma = fmaxf(sqrtf(v), 1e-8f);  // every writer writes the same value
+    }
+    __syncthreads();
+    const float sg = s_sigma;
+    const float den = __fmul_rn(__fmul_rn(2.0f, sg), sg);
+    // affinities W (i != j, kept above 1e-12) into T as f32 values, degrees by rows in column order
+    for (int i = t; i < nn * nn; i += blockDim.x) {
+      const int a = i / nn, b = i % nn;
+      float w = 0.0f;
+      if (a != b) {
+        w = expf(__fdiv_rn(-D[a * kPcaMax + b], den));
+        if (!(w > 1e-12f)) w = 0.0f;
+      }
+      T[a * kPcaMax + b] = (double)w;
+    }
+    __syncthreads();
+    for (int a = t; a < nn; a += blockDim.x) {
+      float s = 0.0f;
+      for (int b = 0; b < nn; b++)
+        if (T[a * kPcaMax + b] != 0.0) s = __fadd_rn(s, (float)T[a * kPcaMax + b]);
+      s_deg[a] = s;
+    }
+    __syncthreads();
+    for (int i = t; i < nn * nn; i += blockDim.x) {
+      const int a = i / nn, b = i % nn;
+      float l = (a == b) ? 1.0f : 0.0f;
+      const float w = (float)T[a * kPcaMax + b];
+      if (w != 0.0f) {
+        const float dn = fmaxf(sqrtf(__fmul_rn(s_deg[a], s_deg[b])), 1e-12f);
+        l = __fsub_rn(l, __fdiv_rn(w, dn));
+      }
+      A[a * kPcaMax + b] = (double)l;
+    }
+  } else {
+    // B = -0.5 * (H D) H with H = I - 1/n, in f64, then rounded to f32
+    const double inv = 1.0 / (double)nn;
+    for (int i = t; i < nn * nn; i += blockDim.x) {
+      const int a = i / nn, b = i % nn;
+      double s = 0.0;
+      for (int c = 0; c < nn; c++) s += ((a == c ? 1.0 : 0.0) - inv) * (double)D[c * kPcaMax + b];
+      T[a * kPcaMax + b] = s;
+    }
+    __syncthreads();
+    for (int i = t; i < nn * nn; i += blockDim.x) {
+      const int a = i / nn, b = i % nn;
+      double s = 0.0;
+      for (int c = 0; c < nn; c++) s += T[a * kPcaMax + c] * ((c == b ? 1.0 : 0.0) - inv);
+      A[a * kPcaMax + b] = (double)(float)(-0.5 * s);
+    }
+  }
+  __syncthreads();
+  if (t < 32) {
+    jacobi_warp(A, V, nn, t);
+    if (t == 0) {
+      for (int i = 0; i < nn; i++) {  // ascending eigenvalues, equal ones in index order (insertion sort)
+        s_eval[i] = A[i * kPcaMax + i];
+        int p = i;
+        while (p > 0 && s_eval[s_order[p - 1]] > s_eval[i]) {
+          s_order[p] = s_order[p - 1];
+          p--;
+        }
+        s_order[p] = i;
+      }
+    }
+  }
+  __syncthreads();
+  // spectral: eigenvectors 1 .. ncomp of the ascending order; MDS: 0 .. ncomp-1 scaled by sqrt(max(l, 0))
+  const int first = mode == 0 ? 1 : 0;
+  const int kc = max(0, min(ncomp, nn - first));
+  for (int i = t; i < nn * ncomp; i += blockDim.x) {
+    const int r = i / ncomp, j = i % ncomp;
+    float v = 0.0f;
+    if (j < kc) {
+      const int col = s_order[j + first];
+      int best = 0;
+      for (int q = 1; q < nn; q++)
+        if (fabs(V[q * kPcaMax + col]) > fabs(V[best * kPcaMax + col])) best = q;
+      const float sign = V[best * kPcaMax + col] < 0.0 ? -1.0f : 1.0f;
+      const float u = __fmul_rn(sign, (float)V[r * kPcaMax + col]);
+      v = mode == 0 ? u : __fmul_rn(u, sqrtf(fmaxf((float)s_eval[col], 0.0f)));
+    }
+    out[i] = v;
+  }
+  __syncthreads();
+  if (t == 0) small_init_normalise(out, nn * ncomp);
+}
+
+// random_unit_init's rows (src/label_prop.rs:311-320): each row of the drawn
+// normals divided by sqrt of its f32 dot with itself (ndarray's unrolled dot:
+// eight partial sums over whole blocks of eight, paired 0+4, 1+5, 2+6, 3+7,
+// then the tail in order), when positive.
+__global__ void unit_rows_kernel(float* r, int64_t n, int ncomp) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    float* row = r + i * ncomp;
+    float p[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    int c = 0;
+    for (; c + 8 <= ncomp; c += 8)
+      for (int j = 0; j < 8; j++) p[j] = __fadd_rn(p[j], __fmul_rn(row[c + j], row[c + j]));
+    float s = 0.0f;
+    s = __fadd_rn(s, __fadd_rn(p[0], p[4]));
+    s = __fadd_rn(s, __fadd_rn(p[1], p[5]));
+    s = __fadd_rn(s, __fadd_rn(p[2], p[6]));
+    s = __fadd_rn(s, __fadd_rn(p[3], p[7]));
+    for (; c < ncomp; c++) s = __fadd_rn(s, __fmul_rn(row[c], row[c]));
+    const float norm = sqrtf(s);
+    if (norm > 0.0f)
+      for (int j = 0; j < ncomp; j++) row[j] = __fdiv_rn(row[j], norm);
+  }
+}
+
+// The jitter and node-embedding upscalers (src/label_prop.rs:606-656):
+// j = f32(layout[part[r], c] (0 for part < 0) + noise[r, c]); the jitter
+// expander writes f32((f64(result) + f64(j)) * 0.5), the node-embedding
+// upscaler writes j.
+__global__ void upscale_kernel(float* result, const int32_t* part, const float* layout, const float* noise,
+                               int64_t n, int ncomp, int jitter) {
+  const int64_t total = n * ncomp;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = i / ncomp;
+    const int c = (int)(i % ncomp);
+    const int32_t p = part[r];
+    const float base = p >= 0 ? layout[(int64_t)p * ncomp + c] : 0.0f;
+    const float j = __fadd_rn(base, noise[i]);
+    result[i] = jitter ? __double2float_rn(__dmul_rn(__dadd_rn((double)result[i], (double)j), 0.5)) : j;
   }
 }
 
@@ -1616,6 +1815,27 @@ cudaError_t launch_pca_init(const float* x, int64_t n, int64_t d, int ncomp, flo
   cudaError_t e = cudaFuncSetAttribute(pca_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   pca_kernel<<<1, 256, smem, s>>>(x, n, d, ncomp, out, mean_ws, vws, status);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_spectral_mds_init(const float* x, int64_t n, int64_t d, int ncomp, int mode, float* out,
+                                    cudaStream_t s) {
+  if (n <= 0 || n > kPcaMax || (mode != 0 && mode != 1)) return cudaErrorInvalidValue;
+  const size_t smem = size_t(3) * kPcaMax * kPcaMax * sizeof(double) + size_t(kPcaMax) * kPcaMax * sizeof(float);
+  cudaError_t e = cudaFuncSetAttribute(spectral_mds_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  spectral_mds_kernel<<<1, 256, smem, s>>>(x, n, d, ncomp, mode, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_unit_rows(float* r, int64_t n, int ncomp, cudaStream_t s) {
+  unit_rows_kernel<<<grid_for(n, 256, 4096), 256, 0, s>>>(r, n, ncomp);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_upscale(float* result, const int32_t* part, const float* layout, const float* noise, int64_t n,
+                           int ncomp, int jitter, cudaStream_t s) {
+  upscale_kernel<<<grid_for(n * ncomp, 256, 4096), 256, 0, s>>>(result, part, layout, noise, n, ncomp, jitter);
   return cudaGetLastError();
 }
 

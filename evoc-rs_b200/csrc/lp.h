@@ -123,6 +123,19 @@ cudaError_t launch_center_scale(const float* result, int64_t n, int ncomp, float
 cudaError_t launch_pca_init(const float* x, int64_t n, int64_t d, int ncomp, float* out, float* mean_ws,
                             double* vws, int32_t* status, cudaStream_t s);
 
+// Spectral (mode 0) or MDS (mode 1) base init of n <= 64 rows, then the
+// small-graph normalisation; out is n x ncomp.
+cudaError_t launch_spectral_mds_init(const float* x, int64_t n, int64_t d, int ncomp, int mode, float* out,
+                                     cudaStream_t s);
+
+// Rows of r (n x ncomp) divided by their f32 L2 norm (random_unit_init).
+cudaError_t launch_unit_rows(float* r, int64_t n, int ncomp, cudaStream_t s);
+
+// The jitter (jitter = 1) or node-embedding (0) upscaler on result (n x ncomp):
+// noise holds the f32 draws, part the row's part, layout the reduced layout.
+cudaError_t launch_upscale(float* result, const int32_t* part, const float* layout, const float* noise, int64_t n,
+                           int ncomp, int jitter, cudaStream_t s);
+
 // node_embedding: per-edge schedules (neg_scale 1.5 for the reproducible epochs, else 1).
 cudaError_t launch_ne_schedule(const float* w, int64_t m, int32_t n_epochs, float negative_sample_rate,
                                float neg_scale, float* eps, float* epns, float* eonn, float* eons, float* max_w,

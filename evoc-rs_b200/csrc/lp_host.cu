@@ -4,9 +4,10 @@
 // and dispatch to the kernels in label_prop.cu.
 //
 // Host logic restated from:
-//   label_propagation_init_with_options  src/label_prop.rs:497-674 (PCA base
-//       init, recursive init, partition expander: the defaults of
-//       label_propagation_init, src/label_prop.rs:464-494)
+//   label_propagation_init_with_options  src/label_prop.rs:497-674 (recursive
+//       or not; PCA, random, spectral or MDS base init below the threshold;
+//       partition, jitter or node-embedding upscaling; the defaults are those
+//       of label_propagation_init, src/label_prop.rs:464-494)
 //   label_prop_loop                      src/label_prop.rs:160-185
 //   node_embedding (reproducible)        src/embed.rs:251-369
 //   NumpyRandomState randint / normal / shuffle
@@ -160,7 +161,8 @@ struct Arena {
   }
 };
 
-constexpr int64_t kBaseInitThreshold = 64;  // src/label_prop.rs:507 default
+constexpr int64_t kBaseInitThreshold = 64;  // src/label_prop.rs:489 default
+constexpr int64_t kEigenMaxRows = 64;       // the one-block eigen-decompositions (PCA, spectral, MDS)
 constexpr int32_t kMaxParts = 65536;        // parts fit the 16-bit fields of the sort keys
 // Embedding rows above this many edges get a CTA each.  A block of few nodes
 // (every node on its own warp) lasts as long as its longest row, so there the
@@ -173,7 +175,50 @@ struct Level {
   int32_t n_iter, n_epochs, ncomp;
   int64_t approx;
   float scaling, noise;
+  float random_scale;
+  evoc_lp_options opt;
 };
+
+int check_status(evoc_gpu_ctx* ctx, int32_t* d_status, const char* what);
+
+// small_graph_init (src/label_prop.rs:425-447) on the level's rows.
+int small_graph_init(evoc_gpu_ctx* ctx, Arena& A, int64_t n, const float* x, int64_t d, const Level& L, Mt& rng,
+                     float* out) {
+  cudaStream_t s = ctx->stream;
+  if (L.opt.base_init == EVOC_BASE_INIT_RANDOM) {
+    // n x n_components normal(1.0) draws in row order, rows L2-normalised
+    std::vector<float> h(static_cast<size_t>(n) * size_t(L.ncomp));
+    for (float& v : h) v = float(1.0 * rng.normal());
+    Stage st(ctx, "random_init");
+    EVOC_TRY(cudaMemcpyAsync(out, h.data(), h.size() * 4, cudaMemcpyHostToDevice, s), "upload draws");
+    EVOC_TRY(lp::launch_unit_rows(out, n, L.ncomp, s), "random_init");
+    ctx->launches += 1;
+    EVOC_TRY(cudaStreamSynchronize(s), "random_init");
+    return EVOC_OK;
+  }
+  if (!x) return fail(ctx, EVOC_ERR_ARG, "base_init 'pca' requires data");
+  if (L.opt.base_init != EVOC_BASE_INIT_PCA) {
+    Stage st(ctx, L.opt.base_init == EVOC_BASE_INIT_SPECTRAL ? "spectral_init" : "mds_init");
+    EVOC_TRY(lp::launch_spectral_mds_init(x, n, d, L.ncomp, L.opt.base_init == EVOC_BASE_INIT_SPECTRAL ? 0 : 1, out,
+                                          s),
+             "spectral / mds init");
+    ctx->launches += 1;
+    EVOC_TRY(cudaStreamSynchronize(s), "spectral / mds init");
+    return EVOC_OK;
+  }
+  float* mean_ws;
+  double* vws;
+  int32_t* status;
+  EVOC_TRY(A.get(&mean_ws, size_t(d)), "alloc");
+  EVOC_TRY(A.get(&vws, size_t(d)), "alloc");
+  EVOC_TRY(A.get(&status, 1), "alloc");
+  EVOC_TRY(cudaMemsetAsync(status, 0, 4, s), "memset");
+  Stage st(ctx, "pca_init");
+  EVOC_TRY(lp::launch_pca_init(x, n, d, L.ncomp, out, mean_ws, vws, status, s), "pca_init");
+  ctx->launches += 1;
+  st.end();
+  return check_status(ctx, status, "pca_init");
+}
 
 int check_status(evoc_gpu_ctx* ctx, int32_t* d_status, const char* what) {
   int32_t st = 0;
@@ -432,26 +477,20 @@ int node_embedding_hogwild_dev(evoc_gpu_ctx* ctx, Arena& A, const lp::Csr& g, in
   return EVOC_OK;
 }
 
+// count normal(scale) draws in order, rounded to f32 (normal_scaled(..) as f32), into dev.
+int upload_normals(evoc_gpu_ctx* ctx, int64_t count, double scale, Mt& rng, float* dev) {
+  std::vector<float> h(static_cast<size_t>(count));
+  for (float& v : h) v = float(scale * rng.normal());
+  EVOC_TRY(cudaMemcpyAsync(dev, h.data(), h.size() * 4, cudaMemcpyHostToDevice, ctx->stream), "upload draws");
+  return EVOC_OK;
+}
+
 // One level of label_propagation_init_with_options (recursive on the reduced graph).
 int lp_init_level(evoc_gpu_ctx* ctx, const lp::ReduceScratch& W, const lp::Csr& g, const float* x, int64_t d,
                   const Level& L, Mt& rng, float* out) {
   cudaStream_t s = ctx->stream;
   Arena A(ctx);
-  if (g.n < kBaseInitThreshold) {
-    if (!x) return fail(ctx, EVOC_ERR_ARG, "base_init 'pca' requires data");
-    float* mean_ws;
-    double* vws;
-    int32_t* status;
-    EVOC_TRY(A.get(&mean_ws, size_t(d)), "alloc");
-    EVOC_TRY(A.get(&vws, size_t(d)), "alloc");
-    EVOC_TRY(A.get(&status, 1), "alloc");
-    EVOC_TRY(cudaMemsetAsync(status, 0, 4, s), "memset");
-    Stage st(ctx, "pca_init");
-    EVOC_TRY(lp::launch_pca_init(x, g.n, d, L.ncomp, out, mean_ws, vws, status, s), "pca_init");
-    ctx->launches += 1;
-    st.end();
-    return check_status(ctx, status, "pca_init");
-  }
+  if (g.n < L.opt.base_init_threshold) return small_graph_init(ctx, A, g.n, x, d, L, rng, out);
   int32_t* part;
   EVOC_TRY(A.get(&part, size_t(g.n)), "alloc partition");
   int32_t n_parts = 0;
@@ -507,12 +546,30 @@ int lp_init_level(evoc_gpu_ctx* ctx, const lp::ReduceScratch& W, const lp::Csr& 
   Level sub = L;
   sub.n_epochs = std::min(L.n_epochs, 255);
   sub.approx = L.approx / 4;
-  if (int rc = lp_init_level(ctx, W, red, rdata, d, sub, rng, rinit)) return rc;
-  // reduced layout: node_embedding of the reduced graph from the recursive init
-  if (int rc = node_embedding_dev(ctx, A, red, r_data, L.ncomp, L.n_epochs, rinit, true,
+  if (L.opt.recursive_init)
+    if (int rc = lp_init_level(ctx, W, red, rdata, d, sub, rng, rinit)) return rc;
+  // reduced layout: node_embedding of the reduced graph from the recursive
+  // init, or from normal(0.25) draws without one
+  if (int rc = node_embedding_dev(ctx, A, red, r_data, L.ncomp, L.n_epochs, rinit, L.opt.recursive_init != 0,
                                   0.001f * float(L.n_epochs), 1.0f, L.noise, rng))
     return rc;
-  // partition expander
+  if (L.opt.upscaling == EVOC_UPSCALE_NODE_EMBEDDING) {
+    // the part layout plus normal(random_scale) draws, row order
+    float *result, *noise;
+    double* mean;
+    EVOC_TRY(A.get(&result, size_t(g.n) * L.ncomp), "alloc");
+    EVOC_TRY(A.get(&noise, size_t(g.n) * L.ncomp), "alloc");
+    EVOC_TRY(A.get(&mean, size_t(L.ncomp)), "alloc");
+    if (int rc = upload_normals(ctx, g.n * L.ncomp, double(L.random_scale), rng, noise)) return rc;
+    Stage st(ctx, "upscale_and_scale");
+    EVOC_TRY(lp::launch_upscale(result, part, rinit, noise, g.n, L.ncomp, 0, s), "node-embedding upscaler");
+    EVOC_TRY(lp::launch_center_scale(result, g.n, L.ncomp, L.scaling, out, mean, s), "centre and scale");
+    ctx->launches += 3;
+    st.end();
+    EVOC_TRY(cudaStreamSynchronize(s), "label propagation level");
+    return EVOC_OK;
+  }
+  // partition expander (the jitter expander starts from it)
   int64_t *s_indptr, *s_nnz, *d_maxdeg;
   int32_t *s_indices, *overflow, *n_over;
   float *s_data, *result;
@@ -545,8 +602,20 @@ int lp_init_level(evoc_gpu_ctx* ctx, const lp::ReduceScratch& W, const lp::Csr& 
     EVOC_TRY(lp::launch_expand(sym, part, xnorm, rinit, L.ncomp, result, overflow, n_over, okey, osum, max_deg, odix,
                                n_parts, ctx->sms, s),
              "partition expander");
+    ctx->launches += max_deg > lp::kVoteSlots ? 2 : 1;
+  }
+  if (L.opt.upscaling == EVOC_UPSCALE_JITTER_EXPANDER) {
+    // averaged with the part layout plus normal(random_scale / 4) draws
+    float* noise;
+    EVOC_TRY(A.get(&noise, size_t(g.n) * L.ncomp), "alloc");
+    if (int rc = upload_normals(ctx, g.n * L.ncomp, double(L.random_scale / 4.0f), rng, noise)) return rc;
+    EVOC_TRY(lp::launch_upscale(result, part, rinit, noise, g.n, L.ncomp, 1, s), "jitter expander");
+    ctx->launches += 1;
+  }
+  {
+    Stage st(ctx, "centre_and_scale");
     EVOC_TRY(lp::launch_center_scale(result, g.n, L.ncomp, L.scaling, out, mean, s), "centre and scale");
-    ctx->launches += max_deg > lp::kVoteSlots ? 4 : 3;
+    ctx->launches += 2;
   }
   EVOC_TRY(cudaStreamSynchronize(s), "label propagation level");
   return EVOC_OK;
@@ -605,9 +674,18 @@ int begin_call(evoc_gpu_ctx* ctx) {
 
 int label_propagation_init_impl(evoc_gpu_ctx* ctx, const int64_t* indptr, const int32_t* indices, const float* data,
                                 int64_t n, int32_t n_iter, int32_t n_epochs, int64_t approx, int32_t ncomp,
-                                float scaling, float noise, evoc_numpy_rng* rs, const float* x, int64_t dim,
-                                int32_t on_dev, float* out) {
+                                float scaling, float random_scale, float noise, evoc_numpy_rng* rs, const float* x,
+                                int64_t dim, int32_t on_dev, const evoc_lp_options& opt, float* out) {
   if (int rc = begin_call(ctx)) return rc;
+  if (opt.base_init < EVOC_BASE_INIT_PCA || opt.base_init > EVOC_BASE_INIT_MDS)
+    return fail(ctx, EVOC_ERR_ARG, "unknown base_init");
+  if (opt.upscaling < EVOC_UPSCALE_PARTITION_EXPANDER || opt.upscaling > EVOC_UPSCALE_NODE_EMBEDDING)
+    return fail(ctx, EVOC_ERR_ARG, "unknown upscaling");
+  if (opt.base_init_threshold < 0) return fail(ctx, EVOC_ERR_ARG, "negative base_init_threshold");
+  if (opt.base_init != EVOC_BASE_INIT_RANDOM && opt.base_init_threshold > kEigenMaxRows + 1)
+    return fail(ctx, EVOC_ERR_UNSUPPORTED,
+                "base_init_threshold above 65 with the pca, spectral or mds base init (one-block "
+                "eigen-decompositions of at most 64 rows)");
   if (n <= 0) return fail(ctx, EVOC_ERR_EMPTY, "empty graph");
   if (!indptr || !rs || !out) return fail(ctx, EVOC_ERR_ARG, "null argument");
   if (ncomp < 1 || ncomp > lp::kMaxComponents) return fail(ctx, EVOC_ERR_UNSUPPORTED, "n_components must be 1..32");
@@ -646,7 +724,7 @@ int label_propagation_init_impl(evoc_gpu_ctx* ctx, const int64_t* indptr, const 
     EVOC_TRY(A.get(&W.rcount, size_t(n) + 2), "alloc sort scratch");
     EVOC_TRY(A.get(&W.counter, 4), "alloc sort scratch");
     EVOC_TRY(A.get(reinterpret_cast<uint8_t**>(&W.tmp), W.tmp_bytes), "alloc sort scratch");
-    Level L{n_iter, n_epochs, ncomp, approx, scaling, noise};
+    Level L{n_iter, n_epochs, ncomp, approx, scaling, noise, random_scale, opt};
     if ((rc = lp_init_level(ctx, W, g, d_x, dim, L, rng, d_out))) return rc;
     if (!on_dev)
       EVOC_TRY(cudaMemcpyAsync(out, d_out, size_t(n) * size_t(ncomp) * 4, cudaMemcpyDeviceToHost, s), "download");
@@ -742,12 +820,36 @@ int evoc_gpu_label_propagation_init(evoc_gpu_ctx* ctx, const int64_t* indptr, co
                                     int32_t n_embedding_epochs, int64_t approx_n_parts, int32_t n_components,
                                     float scaling, float random_scale, float noise_level, evoc_numpy_rng* rng,
                                     const float* x, int64_t dim, int32_t buffers_on_device, float* out) {
+  return evoc_gpu_label_propagation_init_with_options(ctx, indptr, indices, data, n, n_label_prop_iter,
+                                                      n_embedding_epochs, approx_n_parts, n_components, scaling,
+                                                      random_scale, noise_level, rng, x, dim, buffers_on_device,
+                                                      nullptr, out);
+}
+
+void evoc_lp_options_default(evoc_lp_options* o) {
+  if (!o) return;
+  *o = evoc_lp_options{};
+  o->recursive_init = 1;
+  o->base_init = EVOC_BASE_INIT_PCA;
+  o->base_init_threshold = kBaseInitThreshold;
+  o->upscaling = EVOC_UPSCALE_PARTITION_EXPANDER;
+}
+
+int evoc_gpu_label_propagation_init_with_options(evoc_gpu_ctx* ctx, const int64_t* indptr, const int32_t* indices,
+                                                 const float* data, int64_t n, int32_t n_label_prop_iter,
+                                                 int32_t n_embedding_epochs, int64_t approx_n_parts,
+                                                 int32_t n_components, float scaling, float random_scale,
+                                                 float noise_level, evoc_numpy_rng* rng, const float* x, int64_t dim,
+                                                 int32_t buffers_on_device, const evoc_lp_options* options,
+                                                 float* out) {
   if (!ctx) return EVOC_ERR_ARG;
-  (void)random_scale;  // used only by the jitter / node-embedding upscalers, not the partition expander
+  evoc_lp_options opt;
+  evoc_lp_options_default(&opt);
+  if (options) opt = *options;
   std::lock_guard<std::mutex> lock(ctx->mu);
   return label_propagation_init_impl(ctx, indptr, indices, data, n, n_label_prop_iter, n_embedding_epochs,
-                                     approx_n_parts, n_components, scaling, noise_level, rng, x, dim,
-                                     buffers_on_device, out);
+                                     approx_n_parts, n_components, scaling, random_scale, noise_level, rng, x, dim,
+                                     buffers_on_device, opt, out);
 }
 
 int evoc_gpu_node_embedding(evoc_gpu_ctx* ctx, const int64_t* indptr, const int32_t* indices, const float* data,

@@ -33,6 +33,8 @@
 // rerank.cu, from the f32 rows).
 #include <cuda_fp16.h>
 
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -40,7 +42,8 @@ namespace evoc {
 
 namespace {
 constexpr int NW = 4;           // warps per block
-constexpr int HSLOTS = 4096;    // hash-set slots per warp (ids evaluated for the current row)
+constexpr int HSLOTS = 2048;    // hash-set slots per warp (ids evaluated for the current row): 8 KB,
+                                // so seven 4-warp blocks fit an SM's shared memory
 constexpr int KMAX = 64;
 constexpr int MCMAX = 64;       // max_candidates
 constexpr uint32_t kEmpty = 0xffffffffu;
@@ -164,7 +167,7 @@ struct WarpList {
 // the list itself rejects a repeated index).
 __device__ __forceinline__ bool hash_claim(uint32_t* hs, uint32_t id) {
   uint32_t h = uint32_t(mix64(id)) & (HSLOTS - 1);
-  for (int t = 0; t < 8; t++) {
+  for (int t = 0; t < 16; t++) {
     const uint32_t prev = atomicCAS(&hs[h], kEmpty, id);
     if (prev == kEmpty) return true;
     if (prev == id) return false;
@@ -289,10 +292,25 @@ __global__ void nnd_reverse_kernel(const uint64_t* __restrict__ keys, const uint
 }
 
 namespace {
-// Keeps the mc smallest (priority, id) of a row's new or old candidates.
+// Keeps, of a row's new or old candidates, the mc ids of smallest priority,
+// an id offered more than once (u -> v and v -> u both listed) counting at
+// its smallest priority.  The kept set is then independent of the order the
+// reverse edges were filled in (atomics): it always equals the mc smallest
+// of {id -> min priority} over the pushes so far.
 __device__ __forceinline__ void cand_push(uint64_t* best, int32_t* bid, int& got, int mc, uint64_t pr, int32_t id) {
   for (int j = 0; j < got; j++)
-    if ((bid[j] & 0x7fffffff) == (id & 0x7fffffff)) return;  // already a candidate
+    if ((bid[j] & 0x7fffffff) == (id & 0x7fffffff)) {
+      if (pr >= best[j]) return;
+      int p = j;  // smaller priority: move the entry up
+      while (p > 0 && best[p - 1] > pr) {
+        best[p] = best[p - 1];
+        bid[p] = bid[p - 1];
+        p--;
+      }
+      best[p] = pr;
+      bid[p] = id;
+      return;
+    }
   if (got == mc && pr >= best[mc - 1]) return;
   int p = got < mc ? got++ : mc - 1;
   while (p > 0 && best[p - 1] > pr) {
@@ -415,6 +433,8 @@ nnd_join_kernel(const uint8_t* __restrict__ X, int64_t row_bytes, const int32_t*
 
 // Sum over the graph of the finite raw dissimilarities, in f64 (the
 // delta_improv test, src/nndescent/float.rs:857-870).
+// Per-block partial sums into sum[1 + block]; nnd_sum_final_kernel adds them
+// in block order into sum[0], so the total does not depend on scheduling.
 __global__ void nnd_sum_kernel(const uint64_t* __restrict__ keys, int64_t total, double* __restrict__ sum) {
   __shared__ double part[8];
   double s = 0.0;
@@ -432,8 +452,15 @@ __global__ void nnd_sum_kernel(const uint64_t* __restrict__ keys, int64_t total,
   if (threadIdx.x == 0) {
     double t = 0.0;
     for (int i = 0; i < int(blockDim.x >> 5); i++) t += part[i];
-    atomicAdd(sum, t);
+    sum[1 + blockIdx.x] = t;
   }
+}
+
+__global__ void nnd_sum_final_kernel(double* __restrict__ sum, int parts) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double t = 0.0;
+  for (int i = 0; i < parts; i++) t += sum[1 + i];
+  sum[0] = t;
 }
 
 // Final rows: sorted keys -> (index, raw, transformed distance); optionally the
@@ -503,9 +530,9 @@ cudaError_t launch_nnd_iteration(const NndArgs& a, int cur, int iter, cudaStream
   else if (a.dtype == 1) e = join<1>(a, cur, blocks, smem, stream);
   else e = join<2>(a, cur, blocks, smem, stream);
   if (e != cudaSuccess) return e;
-  e = cudaMemsetAsync(a.sum, 0, sizeof(double), stream);
-  if (e != cudaSuccess) return e;
-  nnd_sum_kernel<<<a.sms * 4, 256, 0, stream>>>(a.keys[cur ^ 1], a.n * a.k, a.sum);
+  const int parts = std::min(a.sms * 4, kNndSumParts);
+  nnd_sum_kernel<<<parts, 256, 0, stream>>>(a.keys[cur ^ 1], a.n * a.k, a.sum);
+  nnd_sum_final_kernel<<<1, 32, 0, stream>>>(a.sum, parts);
   return cudaGetLastError();
 }
 

@@ -98,8 +98,11 @@ constexpr double kBatchWork = 4e12;
 // requests pending.  With fewer, each runs alone at its lowest latency.
 constexpr int kBatchMin = 4;
 // Requests below this many rows are latency-sensitive: they run on a lane's
-// high-priority stream.
+// high-priority stream, and the last lanes (a quarter of them, with four or
+// more lanes) admit only these, so a burst of big requests never leaves the
+// small ones queueing for a lane.
 constexpr int64_t kUrgentRows = 65536;
+int small_only_lanes(int lanes) { return lanes >= 4 ? lanes / 4 : 0; }
 
 }  // namespace
 
@@ -314,7 +317,7 @@ evoc::CtxSizes batch_need(evoc_gpu_server* s, const std::vector<Job*>& group) {
 // ones after it as one batch (first fit for each addition).  Returns false,
 // admitting nothing, when fewer than kBatchMin would go together.
 bool try_admit_batch(evoc_gpu_server* s, std::deque<std::shared_ptr<Job>>::iterator it, evoc::CtxSizes& mine,
-                     std::vector<std::shared_ptr<Job>>* group) {
+                     std::vector<std::shared_ptr<Job>>* group, bool small_only) {
   Job* j = it->get();
   std::vector<Job*> cand{j};
   evoc::CtxSizes grown = evoc::grown_sizes(mine, batch_need(s, cand));
@@ -336,7 +339,8 @@ bool try_admit_batch(evoc_gpu_server* s, std::deque<std::shared_ptr<Job>>::itera
     work += o->work;
   }
   if (int(cand.size()) < kBatchMin) return false;
-  if (it != s->pending.begin()) s->pending.front()->skipped++;
+  if (it != s->pending.begin() && !(small_only && s->pending.front()->n >= kUrgentRows))
+    s->pending.front()->skipped++;
   s->in_use += held + int64_t(grown.total()) - int64_t(mine.total());
   for (Job* c : cand) {
     for (auto kt = s->pending.begin(); kt != s->pending.end(); ++kt)
@@ -355,6 +359,7 @@ bool try_admit_batch(evoc_gpu_server* s, std::deque<std::shared_ptr<Job>>::itera
 void worker(evoc_gpu_server* s, int lane) {
   cudaSetDevice(s->device);
   evoc::CtxSizes& mine = s->lane_sizes[size_t(lane)];
+  const bool small_only = lane >= s->lanes - small_only_lanes(s->lanes);
   std::unique_lock<std::mutex> lock(s->mu);
   for (;;) {
     std::vector<std::shared_ptr<Job>> group;
@@ -364,9 +369,11 @@ void worker(evoc_gpu_server* s, int lane) {
       // First fit over the pending requests, oldest first; a request skipped
       // kMaxSkips times holds the next admission for itself.  A small request
       // takes compatible small ones after it into the same batch.
+      // A small-only lane passes over big requests without counting a skip.
       for (auto it = s->pending.begin(); it != s->pending.end(); ++it) {
         Job* j = it->get();
-        if (j->batch_ok && s->batch_max > 1 && try_admit_batch(s, it, mine, &group)) {
+        if (small_only && j->n >= kUrgentRows) continue;
+        if (j->batch_ok && s->batch_max > 1 && try_admit_batch(s, it, mine, &group, small_only)) {
           batch = true;
           break;
         }
@@ -374,7 +381,8 @@ void worker(evoc_gpu_server* s, int lane) {
         const int64_t grow = int64_t(grown.total()) - int64_t(mine.total());
         const int64_t need = j->row_bytes_total + j->out_bytes + grow;
         if (s->in_use + need <= s->budget) {
-          if (it != s->pending.begin()) s->pending.front()->skipped++;
+          if (it != s->pending.begin() && !(small_only && s->pending.front()->n >= kUrgentRows))
+            s->pending.front()->skipped++;
           group.push_back(*it);
           s->pending.erase(it);
           s->in_use += need;

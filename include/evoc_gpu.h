@@ -182,7 +182,7 @@ int evoc_gpu_knn_graph_raw(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts, int32_t
  * (src/graph_construction.rs:16-80): rho = first positive distance; sigma by
  * f64 bisection (64 steps, tolerance 1e-5) on log2(n_neighbors), floored at
  * 1e-3 x the row mean (rho > 0) or 1e-3 x the mean of all distances.
- *   dist   n x k transformed distances, rows sorted ascending (k <= 64)
+ *   dist   n x k transformed distances, rows sorted ascending (any k >= 1)
  */
 int evoc_gpu_smooth_knn_dist(evoc_gpu_ctx* ctx, const float* dist, int64_t n, int32_t k, float n_neighbors,
                              int32_t buffers_on_device, float* sigma, float* rho);
@@ -237,7 +237,8 @@ int evoc_gpu_label_prop_loop(evoc_gpu_ctx* ctx, const int64_t* indptr, const int
  *            when the recursion reaches a graph of fewer than 64 vertices,
  *            else EVOC_ERR_ARG as LabelPropError::PcaRequiresData)
  *   out      n x n_components f32 (n_components 1..32)
- *   random_scale  unused by the partition expander (kept for the signature)
+ *   random_scale  unused by the partition expander (used by the other
+ *            upscalers of evoc_gpu_label_propagation_init_with_options)
  * Partitions, reduced graphs, node orders and the embedding epochs match the
  * reference bit for bit; the PCA base init is f64 eigen-decomposition (the
  * reference uses an f64 thin SVD), equal within its rounding.
@@ -247,6 +248,58 @@ int evoc_gpu_label_propagation_init(evoc_gpu_ctx* ctx, const int64_t* indptr, co
                                     int32_t n_embedding_epochs, int64_t approx_n_parts, int32_t n_components,
                                     float scaling, float random_scale, float noise_level, evoc_numpy_rng* rng,
                                     const float* x, int64_t dim, int32_t buffers_on_device, float* out);
+
+/* Base initialisation of graphs below base_init_threshold vertices (BaseInit,
+ * src/label_prop.rs:20-27) and the upscaling of a partition layout (Upscaling,
+ * 29-36). */
+typedef enum {
+  EVOC_BASE_INIT_PCA = 0,       /* pca_init (265-309): needs x */
+  EVOC_BASE_INIT_RANDOM = 1,    /* random_unit_init (311-320): normal draws, rows L2-normalised */
+  EVOC_BASE_INIT_SPECTRAL = 2,  /* spectral_init (364-423): needs x */
+  EVOC_BASE_INIT_MDS = 3        /* mds_init (339-362): needs x */
+} evoc_base_init;
+
+typedef enum {
+  EVOC_UPSCALE_PARTITION_EXPANDER = 0,  /* src/label_prop.rs:590-605 */
+  EVOC_UPSCALE_JITTER_EXPANDER = 1,     /* 606-642: expander averaged with the jittered part layout */
+  EVOC_UPSCALE_NODE_EMBEDDING = 2       /* 643-656: part layout plus normal(random_scale) draws */
+} evoc_upscaling;
+
+/* The keyword arguments of label_propagation_init_with_options
+ * (src/label_prop.rs:497-512).  evoc_lp_options_default gives the values of
+ * label_propagation_init: recursive, PCA, 64, partition expander. */
+typedef struct {
+  int32_t recursive_init;       /* nonzero: the reduced layout starts from the recursive init */
+  int32_t base_init;            /* evoc_base_init */
+  int64_t base_init_threshold;  /* graphs of fewer vertices take the base init */
+  int32_t upscaling;            /* evoc_upscaling */
+  int32_t reserved[3];
+} evoc_lp_options;
+
+void evoc_lp_options_default(evoc_lp_options* o);
+
+/*
+ * label_propagation_init_with_options (src/label_prop.rs:497-674): as
+ * evoc_gpu_label_propagation_init, with the options above (NULL: defaults).
+ * The options pass down the recursion as in the reference.  RNG draws, in
+ * the reference's order per level: label_prop_loop, the recursion, the
+ * reduced layout's node_embedding (normal(0.25) initial draws when
+ * recursive_init is 0), then the upscaler's n x n_components normals
+ * (jitter: normal(random_scale / 4), node embedding: normal(random_scale)).
+ * The random base init draws n x n_components normals.  Spectral and MDS
+ * eigen-decompose in f64 on the host (the reference: faer's f32 solver), with
+ * eigenvalues ascending and each eigenvector's largest-magnitude entry (the
+ * first on ties) made positive -- the reference's signs are faer's.
+ * Errors: EVOC_ERR_ARG for an unknown base_init / upscaling, a threshold
+ * below 0, or a base init that needs x without it.
+ */
+int evoc_gpu_label_propagation_init_with_options(evoc_gpu_ctx* ctx, const int64_t* indptr, const int32_t* indices,
+                                                 const float* data, int64_t n, int32_t n_label_prop_iter,
+                                                 int32_t n_embedding_epochs, int64_t approx_n_parts,
+                                                 int32_t n_components, float scaling, float random_scale,
+                                                 float noise_level, evoc_numpy_rng* rng, const float* x, int64_t dim,
+                                                 int32_t buffers_on_device, const evoc_lp_options* options,
+                                                 float* out);
 
 /*
  * UMAP-like node embedding.  Replaces node_embedding (src/embed.rs:251-369)

@@ -122,3 +122,32 @@ def test_batch_rescans_match_single_calls():
         si, sd = evoc.knn_graph(x, opts)
         assert np.array_equal(bi, si)
         assert np.array_equal(bd.view(np.uint32), sd.view(np.uint32))
+
+
+def test_half_form_beyond_256_candidates_is_exact():
+    # oversample * k > 256 (k = 150): every row takes the exact FP32 scan
+    rng = np.random.default_rng(21)
+    x = rng.standard_normal((700, 40)).astype(np.float32)
+    a = evoc.knn_graph(x, evoc.KnnGraphOptions(n_neighbors=150, form="half_rerank"))
+    b = evoc.knn_graph(x, evoc.KnnGraphOptions(n_neighbors=150, form="fp32"))
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+def test_few_failed_rows_take_the_split_exact_pass():
+    """A few rows fail (planted near-duplicate groups in benign data): they go straight to the exact
+    FP32 pass with the keys split over the SMs, and match the oracle's exact selection."""
+    rng = np.random.default_rng(9)
+    n, d, k = 12000, 64, 15
+    c = rng.standard_normal((6, d))
+    x = (c[rng.integers(0, 6, n)] + 0.25 * rng.standard_normal((n, d))).astype(np.float32)
+    for t in range(6):
+        base = x[t * 1000]
+        x[t * 1000 + 1:t * 1000 + 25] = base + 1e-4 * rng.standard_normal((24, d)).astype(np.float32)
+    x /= np.linalg.norm(x, axis=1, keepdims=True)
+    ind, dst, raw = evoc.knn_graph(x, half(k), return_raw=True)
+    counts = _lib.context(0).certify_counts()
+    assert 0 < counts["second_pass"] <= 1000 and counts["exact_rescan"] == counts["second_pass"], counts
+    ei, er = O.exact_knn(O.prepare_float(x), k)
+    same = ind == ei
+    assert np.all(np.abs(raw[~same].astype(np.float64) - er[~same].astype(np.float64)) <= 1e-6)
+    assert np.all(np.abs(raw.astype(np.float64) - er.astype(np.float64)) <= 1e-6)

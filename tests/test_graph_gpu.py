@@ -90,3 +90,15 @@ def test_fuzzy_graph_hub_columns():
     dst = np.sort(rng.random((n, k)).astype(np.float32) * 2.0, axis=1)
     dst[:, 0] = 0.0
     _compare_with_oracle(ind, dst, 10.0)
+
+
+def test_fuzzy_graph_large_k():
+    # k = 150 (no k limit, as smooth_knn_dist has none): rows keep their
+    # membership entries in column order in place
+    from evoc import synthetic
+
+    x = synthetic.blobs(n_per=100, centres=8, dim=32, seed=9)
+    ind, dst = evoc.knn_graph(x, evoc.KnnGraphOptions(n_neighbors=150, form="fp32"))
+    assert ind.shape == (800, 150)
+    _compare_with_oracle(ind, dst, 150.0)
+    _compare_with_oracle(ind, dst, 150.0, symmetrize=False)

@@ -130,6 +130,17 @@ def test_nndescent_options_max_candidates_and_delta_improv():
 def test_nndescent_rejects_unsupported():
     x = np.random.default_rng(0).standard_normal((100, 16)).astype(np.float32)
     with pytest.raises(evoc.BackendError):
-        evoc.knn_graph(x, nnd(65))
-    with pytest.raises(evoc.BackendError):
         evoc.knn_graph(x, nnd(5, row_begin=0, row_end=50))
+
+
+def test_nndescent_large_k_takes_the_exact_form():
+    # above k = 64 the NN-descent request is built by the dtype's exact form
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal((400, 24)).astype(np.float32)
+    a = evoc.knn_graph(x, nnd(80), np.random.RandomState(0))
+    b = evoc.knn_graph(x, evoc.KnnGraphOptions(n_neighbors=80, form="half_rerank"))
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    xi = np.clip(np.round(40 * rng.standard_normal((300, 32))), -127, 127).astype(np.int8)
+    a = evoc.knn_graph(xi, nnd(70), np.random.RandomState(0))
+    b = evoc.knn_graph(xi, evoc.KnnGraphOptions(n_neighbors=70, form="exact_int"))
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
