@@ -117,6 +117,13 @@ def _bind_optional(L) -> None:
                                                       C.POINTER(NumpyRng), P, i64, i32, P]
         L.evoc_gpu_node_embedding.argtypes = [P, P, P, P, i64, i32, i32, P, f32, f32, f32, C.POINTER(NumpyRng),
                                               i32, i32, P]
+    if hasattr(L, "evoc_gpu_label_propagation_init_with_options"):
+        f32 = C.c_float
+        L.evoc_gpu_label_propagation_init_with_options.argtypes = [
+            P, P, P, P, i64, i32, i32, i64, i32, f32, f32, f32, C.POINTER(NumpyRng), P, i64, i32,
+            C.POINTER(LpOptions), P]
+        L.evoc_lp_options_default.argtypes = [C.POINTER(LpOptions)]
+        L.evoc_lp_options_default.restype = None
     if hasattr(L, "evoc_gpu_peak_ffma"):
         L.evoc_gpu_peak_ffma.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     if hasattr(L, "evoc_gpu_boruvka_mst"):
@@ -154,6 +161,17 @@ class NumpyRng(C.Structure):
     """evoc_numpy_rng: the fields of numpy.random.RandomState.get_state()."""
 
     _fields_ = [("key", C.c_uint32 * 624), ("pos", C.c_int32), ("has_gauss", C.c_int32), ("gauss", C.c_double)]
+
+
+class LpOptions(C.Structure):
+    """evoc_lp_options: label_propagation_init_with_options's keyword arguments."""
+
+    _fields_ = [("recursive_init", C.c_int32), ("base_init", C.c_int32), ("base_init_threshold", C.c_int64),
+                ("upscaling", C.c_int32), ("reserved", C.c_int32 * 3)]
+
+
+BASE_INITS = {"pca": 0, "random": 1, "spectral": 2, "mds": 3}
+UPSCALINGS = {"partition_expander": 0, "jitter_expander": 1, "node_embedding": 2}
 
 
 class NpyArray(C.Structure):

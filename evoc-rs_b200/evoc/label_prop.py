@@ -2,7 +2,7 @@
 mirror of evoc-rs src/label_prop.rs and src/embed.rs over the C ABI.
 
   label_prop_loop          src/label_prop.rs:160-185   (-> evoc_gpu_label_prop_loop)
-  label_propagation_init   src/label_prop.rs:464-494   (-> evoc_gpu_label_propagation_init)
+  label_propagation_init   src/label_prop.rs:464-674   (-> evoc_gpu_label_propagation_init_with_options)
   node_embedding           src/embed.rs:251-369        (-> evoc_gpu_node_embedding)
 
 The graph is a scipy.sparse.csr_matrix (or an (indptr, indices, data, n)
@@ -75,11 +75,29 @@ def label_prop_loop(graph, random_state, n_iter: int = 20, approx_n_parts: int =
     return out
 
 
+def _lp_options(recursive_init: bool, base_init: str, base_init_threshold: int, upscaling: str) -> _lib.LpOptions:
+    if base_init not in _lib.BASE_INITS:
+        raise ValueError(f"base_init must be one of {sorted(_lib.BASE_INITS)}")
+    if upscaling not in _lib.UPSCALINGS:
+        raise ValueError(f"upscaling must be one of {sorted(_lib.UPSCALINGS)}")
+    o = _lib.LpOptions()
+    o.recursive_init = 1 if recursive_init else 0
+    o.base_init = _lib.BASE_INITS[base_init]
+    o.base_init_threshold = int(base_init_threshold)
+    o.upscaling = _lib.UPSCALINGS[upscaling]
+    return o
+
+
 def label_propagation_init(graph, n_label_prop_iter: int = 20, n_embedding_epochs: int = 50,
                            approx_n_parts: int = 512, n_components: int = 4, scaling: float = 0.5,
                            random_scale: float = 0.1, noise_level: float = 0.5, random_state=None, data=None,
-                           device: int = 0) -> np.ndarray:
-    """Initial (n, n_components) f32 embedding; src/label_prop.rs:464-494."""
+                           device: int = 0, recursive_init: bool = True, base_init: str = "pca",
+                           base_init_threshold: int = 64, upscaling: str = "partition_expander") -> np.ndarray:
+    """Initial (n, n_components) f32 embedding; src/label_prop.rs:464-494, and with the keyword
+    arguments of label_propagation_init_with_options (src/label_prop.rs:497-674): base_init one of
+    pca / random / spectral / mds, upscaling one of partition_expander / jitter_expander /
+    node_embedding."""
+    opt = _lp_options(recursive_init, base_init, base_init_threshold, upscaling)
     indptr, indices, gdata, n = _csr(graph)
     rs = _state(random_state)
     r = _rng_in(rs)
@@ -87,11 +105,11 @@ def label_propagation_init(graph, n_label_prop_iter: int = 20, n_embedding_epoch
     dim = 0 if x is None else x.shape[1]
     out = np.empty((n, int(n_components)), np.float32)
     ctx = _lib.context(device)
-    st = _lib.lib().evoc_gpu_label_propagation_init(
+    st = _lib.lib().evoc_gpu_label_propagation_init_with_options(
         ctx.h, indptr.ctypes.data_as(P), indices.ctypes.data_as(P), gdata.ctypes.data_as(P), n,
         int(n_label_prop_iter), int(n_embedding_epochs), int(approx_n_parts), int(n_components), float(scaling),
         float(random_scale), float(noise_level), C.byref(r), None if x is None else x.ctypes.data_as(P), dim, 0,
-        out.ctypes.data_as(P))
+        C.byref(opt), out.ctypes.data_as(P))
     _check(st, ctx)
     _rng_out(rs, r)
     return out

@@ -274,16 +274,154 @@ def pca_init(data: np.ndarray, n_components: int) -> np.ndarray:
     return _normalize_small_init(out)
 
 
+def _ndarray_dot_f32(v: np.ndarray) -> np.float32:
+    """ndarray's unrolled f32 dot of a contiguous row with itself (no BLAS feature in the
+    reference's build, Cargo.toml:29): eight partial sums over whole blocks of eight, added
+    as (0+4), (1+5), (2+6), (3+7) to a zero sum, then the tail in order; separate multiply and add."""
+    f = np.float32
+    p = [f(0.0)] * 8
+    c = 0
+    while c + 8 <= len(v):
+        for j in range(8):
+            p[j] = f(p[j] + f(v[c + j] * v[c + j]))
+        c += 8
+    s = f(0.0)
+    for a, b in ((0, 4), (1, 5), (2, 6), (3, 7)):
+        s = f(s + f(p[a] + p[b]))
+    for j in range(c, len(v)):
+        s = f(s + f(v[j] * v[j]))
+    return s
+
+
+def random_unit_init(n: int, n_components: int, rng: O.RandomState) -> np.ndarray:
+    """src/label_prop.rs:311-320: n x c normal(1.0) draws in row order (f32), each row divided by
+    the f32 sqrt of its dot with itself when positive."""
+    r = np.empty((n, n_components), np.float32)
+    for i in range(n):
+        for c in range(n_components):
+            r[i, c] = np.float32(1.0 * rng.normal())
+    for i in range(n):
+        norm = np.float32(np.sqrt(_ndarray_dot_f32(r[i])))
+        if norm > 0:
+            r[i] = (r[i] / norm).astype(np.float32)
+    return r
+
+
+def _pairwise_sq(data: np.ndarray) -> np.ndarray:
+    """src/label_prop.rs:322-337: f32, coordinates summed in order, separate multiply and add."""
+    x = np.asarray(data, np.float32)
+    n, d = x.shape
+    sq = np.zeros((n, n), np.float32)
+    for c in range(d):
+        diff = (x[:, None, c] - x[None, :, c]).astype(np.float32)
+        sq = (sq + (diff * diff).astype(np.float32)).astype(np.float32)
+    return sq
+
+
+def _eigh_signed(a: np.ndarray):
+    """Symmetric eigen-decomposition in f64 (the CUDA path's; the reference uses faer 0.20.2's f32
+    solver, whose eigenvector signs are its own): eigenvalues ascending, each eigenvector's
+    largest-|.| entry (the first on ties) made non-negative."""
+    w, v = np.linalg.eigh(np.asarray(a, np.float64))
+    order = np.argsort(w, kind="stable")
+    w, v = w[order], v[:, order]
+    for j in range(v.shape[1]):
+        i = int(np.argmax(np.abs(v[:, j])))
+        if v[i, j] < 0:
+            v[:, j] = -v[:, j]
+    return w, v
+
+
+def spectral_init(data: np.ndarray, n_components: int) -> np.ndarray:
+    """src/label_prop.rs:364-423: Gaussian affinities with sigma = sqrt of the median positive squared
+    distance (floored at 1e-8), the symmetric normalised Laplacian I - D^-1/2 W D^-1/2 in f32,
+    eigenvectors 1 .. n_components of the ascending order, then the small-graph normalisation."""
+    f = np.float32
+    dsq = _pairwise_sq(data)
+    n = dsq.shape[0]
+    flat = np.sort(dsq[dsq > 0].ravel(), kind="stable")
+    sigma = f(max(np.sqrt(f(flat[len(flat) // 2])) if len(flat) else f(1.0), f(1e-8)))
+    den = f(f(f(2.0) * sigma) * sigma)
+    w = np.zeros((n, n), np.float32)
+    for i in range(n):
+        for j in range(n):
+            if i != j:
+                v = f(np.exp(f(-dsq[i, j] / den)))
+                if v > f(1e-12):
+                    w[i, j] = v
+    deg = np.zeros(n, np.float32)
+    for i in range(n):
+        for j in range(n):
+            if w[i, j] != 0:
+                deg[i] = f(deg[i] + w[i, j])
+    lap = np.eye(n, dtype=np.float32)
+    for i in range(n):
+        for j in range(n):
+            if w[i, j] != 0:
+                dn = max(f(np.sqrt(f(deg[i] * deg[j]))), f(1e-12))
+                lap[i, j] = f(lap[i, j] - f(w[i, j] / dn))
+    _, v = _eigh_signed(lap)
+    out = np.zeros((n, n_components), np.float32)
+    kc = max(0, min(n_components, n - 1))
+    out[:, :kc] = v[:, 1:1 + kc].astype(np.float32)
+    return _normalize_small_init(out)
+
+
+def mds_init(data: np.ndarray, n_components: int) -> np.ndarray:
+    """src/label_prop.rs:339-362: B = -0.5 (H D) H in f64 (H = I - 1/n) rounded to f32, the
+    eigenvectors of the n_components smallest eigenvalues (ascending order) scaled by
+    sqrt(max(lambda, 0)) in f32, then the small-graph normalisation."""
+    dsq = _pairwise_sq(data).astype(np.float64)
+    n = dsq.shape[0]
+    h = np.eye(n) - 1.0 / n
+    b = (-0.5 * ((h @ dsq) @ h)).astype(np.float32)
+    w, v = _eigh_signed(b)
+    out = np.zeros((n, n_components), np.float32)
+    kc = min(n_components, n)
+    eig = np.sqrt(np.maximum(w[:kc].astype(np.float32), np.float32(0.0))).astype(np.float32)
+    out[:, :kc] = (v[:, :kc].astype(np.float32) * eig[None, :]).astype(np.float32)
+    return _normalize_small_init(out)
+
+
+def small_graph_init(data, n: int, n_components: int, base_init: str, rng: O.RandomState) -> np.ndarray:
+    """src/label_prop.rs:425-447."""
+    if base_init == "random":
+        return random_unit_init(n, n_components, rng)
+    if data is None:
+        raise ValueError("base_init 'pca' requires data")
+    if base_init == "pca":
+        return pca_init(data, n_components)
+    if base_init == "spectral":
+        return spectral_init(data, n_components)
+    if base_init == "mds":
+        return mds_init(data, n_components)
+    raise ValueError(base_init)
+
+
+def _part_layout_plus_noise(part: np.ndarray, layout: np.ndarray, n_components: int, scale: float,
+                            rng: O.RandomState) -> np.ndarray:
+    """layout[part] (zeros where part < 0) plus normal_scaled(scale) as f32, drawn in row order and
+    added in f32 (src/label_prop.rs:628-640, 643-656)."""
+    n = len(part)
+    out = np.zeros((n, n_components), np.float32)
+    ok = part >= 0
+    out[ok] = layout[part[ok]]
+    for i in range(n):
+        for c in range(n_components):
+            out[i, c] = np.float32(out[i, c] + np.float32(scale * rng.normal()))
+    return out
+
+
 def label_propagation_init(g: Csr, n_label_prop_iter: int, n_embedding_epochs: int, approx_n_parts: int,
                            n_components: int, scaling: float, random_scale: float, noise_level: float,
-                           rng: O.RandomState, data=None, base_init_threshold: int = 64, trace=None) -> np.ndarray:
-    """label_propagation_init_with_options with recursive_init, PCA base init and the partition
-    expander (the defaults of label_propagation_init), src/label_prop.rs:464-674."""
+                           rng: O.RandomState, data=None, base_init_threshold: int = 64, trace=None,
+                           recursive_init: bool = True, base_init: str = "pca",
+                           upscaling: str = "partition_expander") -> np.ndarray:
+    """label_propagation_init_with_options (src/label_prop.rs:497-674); the defaults are those of
+    label_propagation_init (464-494): recursive init, PCA base init, the partition expander."""
     n = g.shape[0]
     if n < base_init_threshold:
-        if data is None:
-            raise ValueError("base_init 'pca' requires data")
-        return pca_init(data, n_components)
+        return small_graph_init(data, n, n_components, base_init, rng)
     part = label_prop_loop(g, rng, n_label_prop_iter, approx_n_parts)
     base = partition_reduction_map(part)
     norm = normalize_cols_l2(base)
@@ -292,17 +430,29 @@ def label_propagation_init(g: Csr, n_label_prop_iter: int, n_embedding_epochs: i
     reduced_data = csr_matmul_dense(reducer, data) if data is not None else None
     reduced = smmp(smmp(norm_t, g), base)
     reduced = Csr.make(reduced.indptr, reduced.indices, np.clip(reduced.data, 0.0, 1.0), reduced.shape)
-    reduced_init = label_propagation_init(reduced, n_label_prop_iter, min(n_embedding_epochs, 255),
-                                          approx_n_parts // 4, n_components, scaling, random_scale, noise_level,
-                                          rng, reduced_data, base_init_threshold, trace)
+    reduced_init = None
+    if recursive_init:
+        reduced_init = label_propagation_init(reduced, n_label_prop_iter, min(n_embedding_epochs, 255),
+                                              approx_n_parts // 4, n_components, scaling, random_scale,
+                                              noise_level, rng, reduced_data, base_init_threshold, trace,
+                                              recursive_init, base_init, upscaling)
     layout = node_embedding(reduced, n_components, n_embedding_epochs, reduced_init,
                             np.float32(0.001) * np.float32(n_embedding_epochs), 1.0, noise_level, rng)
-    sym = hadamard_symmetric(g)
-    expander = normalize_rows_l1(smmp(sym, norm))
-    part_norm = normalize_rows_l1(norm)
-    a = csr_matmul_dense(expander, layout)
-    b = csr_matmul_dense(part_norm, layout)
-    result = ((a.astype(np.float64) + b.astype(np.float64)) * 0.5).astype(np.float32)
+    if upscaling == "node_embedding":
+        result = _part_layout_plus_noise(part, layout, n_components, float(np.float32(random_scale)), rng)
+    else:
+        sym = hadamard_symmetric(g)
+        expander = normalize_rows_l1(smmp(sym, norm))
+        part_norm = normalize_rows_l1(norm)
+        a = csr_matmul_dense(expander, layout)
+        b = csr_matmul_dense(part_norm, layout)
+        result = ((a.astype(np.float64) + b.astype(np.float64)) * 0.5).astype(np.float32)
+        if upscaling == "jitter_expander":
+            quarter = float(np.float32(np.float32(random_scale) / np.float32(4.0)))
+            jit = _part_layout_plus_noise(part, layout, n_components, quarter, rng)
+            result = ((result.astype(np.float64) + jit.astype(np.float64)) * 0.5).astype(np.float32)
+        elif upscaling != "partition_expander":
+            raise ValueError(upscaling)
     mean = np.add.accumulate(result.astype(np.float64), axis=0)[-1] / n  # f64, row order
     if trace is not None:
         trace.append(dict(n=n, partition=part, reduced=reduced, reduced_data=reduced_data,

@@ -297,3 +297,64 @@ def test_label_propagation_limits_are_errors():
         evoc.label_propagation_init(_tuple(g), 20, 5, 100000, 4, 0.5, 0.1, 0.5, np.random.RandomState(1), x)
     with pytest.raises(evoc.BackendError):  # components above 32
         evoc.label_propagation_init(_tuple(g), 20, 5, 300, 40, 0.5, 0.1, 0.5, np.random.RandomState(1), x)
+
+
+@pytest.mark.parametrize("base_init,upscaling,recursive", [
+    ("pca", "jitter_expander", True),
+    ("pca", "node_embedding", True),
+    ("pca", "partition_expander", False),
+    ("random", "partition_expander", True),
+    ("spectral", "partition_expander", True),
+    ("spectral", "jitter_expander", False),
+])
+def test_label_propagation_init_with_options_matches_oracle(blob_graph, base_init, upscaling, recursive):
+    """label_propagation_init_with_options (src/label_prop.rs:497-674) against the oracle: the
+    recursion, the base init of the < 64-vertex level, the upscaler's normal draws in the
+    reference's order (the caller's RNG ends in the same state)."""
+    g, x = blob_graph
+    rs = np.random.RandomState(13)
+    orng = _oracle_rng(rs)
+    kw = dict(recursive_init=recursive, base_init=base_init, upscaling=upscaling)
+    init = evoc.label_propagation_init(_tuple(g), 20, 20, _approx(g.shape[0]), 5, 0.5, 0.1, 0.5, rs, x, **kw)
+    want = L.label_propagation_init(g, 20, 20, _approx(g.shape[0]), 5, 0.5, 0.1, 0.5, orng, x, **kw)
+    assert init.shape == (len(x), 5)
+    assert np.abs(init - want).max() <= 1e-4
+    assert _same_state(rs, orng)
+
+
+def test_small_graph_base_inits_match_oracle():
+    """Below the threshold the base init is the result (src/label_prop.rs:513-515): random draws
+    bit for bit; spectral within 1e-4; MDS within 5e-3 -- its first column belongs to the zero
+    eigenvalue of the doubly centred matrix, f32 rounding noise in every implementation."""
+    rng = np.random.default_rng(31)
+    x = rng.normal(size=(40, 48)).astype(np.float32)
+    g = _hub_graph(n=40, hubs=1, hub_deg=20, seed=8)
+    for base, tol in (("random", 0.0), ("spectral", 1e-4), ("mds", 5e-3), ("pca", 1e-4)):
+        rs = np.random.RandomState(3)
+        orng = _oracle_rng(rs)
+        got = evoc.label_propagation_init(_tuple(g), 20, 10, 256, 6, 0.5, 0.1, 0.5, rs, x, base_init=base)
+        want = L.small_graph_init(x, 40, 6, base, orng)
+        assert got.shape == (40, 6)
+        assert np.abs(got - want).max() <= tol, (base, np.abs(got - want).max())
+        assert _same_state(rs, orng)
+    # the random init needs no data
+    rs = np.random.RandomState(3)
+    got = evoc.label_propagation_init(_tuple(g), 20, 10, 256, 6, 0.5, 0.1, 0.5, rs, None, base_init="random")
+    assert np.allclose(np.linalg.norm(got, axis=1), 1.0, atol=1e-6)
+
+
+def test_label_propagation_option_errors(blob_graph):
+    g, x = blob_graph
+    with pytest.raises(ValueError):
+        evoc.label_propagation_init(_tuple(g), 20, 5, 300, 4, 0.5, 0.1, 0.5, np.random.RandomState(1), x,
+                                    base_init="tsne")
+    with pytest.raises(evoc.BackendError):  # eigen-decompositions are one block of at most 64 rows
+        evoc.label_propagation_init(_tuple(g), 20, 5, 300, 4, 0.5, 0.1, 0.5, np.random.RandomState(1), x,
+                                    base_init_threshold=200)
+    with pytest.raises(evoc.BackendError):  # spectral needs the data (LabelPropError::PcaRequiresData)
+        evoc.label_propagation_init(_tuple(g), 20, 5, 300, 4, 0.5, 0.1, 0.5, np.random.RandomState(1), None,
+                                    base_init="spectral")
+    # the random base init takes any threshold
+    out = evoc.label_propagation_init(_tuple(g), 20, 5, 300, 4, 0.5, 0.1, 0.5, np.random.RandomState(1), None,
+                                      base_init="random", base_init_threshold=500)
+    assert out.shape == (len(x), 4) and np.all(np.isfinite(out))

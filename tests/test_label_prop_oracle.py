@@ -164,3 +164,31 @@ def test_node_embedding_state_equals_reference_rust_after_20_epochs():
             order[i], order[j] = order[j], order[i]
         if f"rust_node_order_{e:03d}" in z.files:
             assert np.array_equal(order, z[f"rust_node_order_{e:03d}"]), e
+
+
+def test_random_unit_init_draws_numpy_normals_in_row_order():
+    """random_unit_init (src/label_prop.rs:311-320) takes NumPy's standard normals row by row."""
+    from oracle import oracle as O
+
+    got = L.random_unit_init(7, 3, O.RandomState(11))
+    x = np.random.RandomState(11).standard_normal((7, 3)).astype(np.float32)
+    want = x / np.sqrt((x * x).sum(axis=1, keepdims=True, dtype=np.float32))
+    assert np.allclose(got, want, rtol=0, atol=1e-7)
+    # eight or more components take ndarray's eight partial sums
+    wide = L.random_unit_init(4, 10, O.RandomState(2))
+    assert np.allclose(np.linalg.norm(wide.astype(np.float64), axis=1), 1.0, atol=1e-6)
+
+
+def test_spectral_and_mds_inits_are_normalised_embeddings():
+    rng = np.random.default_rng(4)
+    x = rng.normal(size=(30, 40)).astype(np.float32)
+    for f in (L.spectral_init, L.mds_init):
+        r = f(x, 3)
+        assert r.shape == (30, 3) and r.dtype == np.float32
+        # the small-graph normalisation: global mean ~0, (max - min) / 2 == 1
+        assert abs(float(r.astype(np.float64).mean())) < 1e-6
+        assert abs(float(r.max()) - float(r.min()) - 2.0) < 1e-5
+    # spectral columns are eigenvectors of the normalised Laplacian, orthonormal before scaling
+    s = L.spectral_init(x, 3).astype(np.float64)
+    s -= s.mean(axis=0)
+    assert np.linalg.matrix_rank(s) == 3
