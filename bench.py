@@ -7,8 +7,10 @@ seed 7 (+ rank), k = 30; generated on the device (synthetic stand-in for the
 reference's own make_blobs workloads; no dataset is downloaded).
 
 One step = one kNN-graph build of the whole workload (every row's 30
-neighbours) in the headline form: tcgen05 BF16 exact scan keeping 2k
-candidates per row, FP32 rerank (FP64 at the k-th boundary).
+neighbours) in the headline form (the metric's "BF16+rerank" form): tcgen05
+16-bit exact scan with FP16 operands keeping ceil(2.5k) candidates per row,
+FP32 rerank (FP64 at the k-th boundary) with a per-row certificate, rescans of
+the rows that fail it.
 
   value    edges/s (rows x k / step time) with the rows already in HBM,
            step timed with CUDA events on the library's own stream, max over
@@ -16,8 +18,9 @@ candidates per row, FP32 rerank (FP64 at the k-th boundary).
   e2e      the same through the public API with pinned HOST buffers: the
            host->device copy of the rows and the device->host copy of the
            indices and distances are inside every timed step.
-  roofline the dominant kernel (the BF16 scan): 2 n^2 d algorithmic FLOPs per
-           launch over its CUDA-event duration, against the measured BF16 peak.
+  roofline the dominant kernel (the 16-bit scan): 2 n^2 d algorithmic FLOPs per
+           launch over its CUDA-event duration, against the measured dense
+           BF16 peak (FP16 and BF16 MMAs run at the same rate).
   fp32_form the plain FP32 SIMT form on a slice of query rows against all rows.
   cpu_baseline  the reference's NN-descent (restated in oracle/, all host
            threads) on a bounded prefix of the same workload.
@@ -947,7 +950,7 @@ def run_ours(args, world, rank, local):
     ctx.profile(True)
     stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=dev)
     form = args.form
-    opts = evoc.KnnGraphOptions(n_neighbors=k, form=form, oversample=2, device=local)
+    opts = evoc.KnnGraphOptions(n_neighbors=k, form=form, oversample=0, device=local)
     tuned = (evoc.autotune("Float32", n, d, k, "bf16_rerank", device=local)
              if args.autotune and form == "bf16_rerank" else None)
 
@@ -1088,7 +1091,7 @@ def run_ours(args, world, rank, local):
         peak = float(peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops")))
         roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                     "traffic": scan_traffic(n), "traffic_unit": "bytes per launch (ncu, scaled)",
-                    "kernel": "tc_scan_kernel (BF16, fused top-2k)",
+                    "kernel": "tc_scan_kernel (FP16 operands, fused top-C, C = ceil(2.5k))",
                     "peak_kind": f"{peak_kind} bf16 sustained (burst {peaks.get('bf16_tflops')})",
                     "launch_ms": scan_ms}
     else:
@@ -1143,10 +1146,10 @@ def run_ours(args, world, rank, local):
     line = {
         "metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "bf16 tensor-core scan + f32 rerank" if form == "bf16_rerank" else "f32 (NN-descent joins, f32 rerank)",
+        "dtype": "fp16 tensor-core scan + f32 rerank" if form == "bf16_rerank" else "f32 (NN-descent joins, f32 rerank)",
         "data": "synthetic (generated on device, seeded)",
-        "config": {"workload": WORKLOAD, "n": n, "d": d, "k": k, "form": form, "oversample": 2,
-                   "l2": "inputs larger than L2 (3.1 GB f32 + 1.5 GB bf16 vs 126 MB)",
+        "config": {"workload": WORKLOAD, "n": n, "d": d, "k": k, "form": form, "oversample": "ceil(2.5 k)",
+                   "l2": "inputs larger than L2 (3.1 GB f32 + 1.5 GB fp16 vs 126 MB)",
                    "per_rank": "independent graph per rank"},
         "recall_at_k_vs_fp64": rec, "max_abs_dist_err_vs_fp64": max_err, "recall_sample_rows": sample,
         "stages_ms": {kname: statistics.mean(v) for kname, v in stage_ms.items()},
@@ -1307,6 +1310,62 @@ def run_shard(args, world, rank, local):
     return 0
 
 
+
+def run_case(args):
+    """One small case of a kernel, for timings and ncu captures (`--case NAME [--n N]`): prints
+    one JSON line with the stage times (CUDA events on the library stream) of the last of two
+    identical calls.  Cases: scan (the 16-bit form of zipf rows with the certificate counts), fp32
+    (the plain FP32 form on the first 37,888 query rows), nnd (the NN-descent form), mst (the
+    Boruvka MST of a 7-d blob set)."""
+    import numpy as np
+    import torch
+
+    import evoc
+    from evoc import _lib, synthetic
+
+    dev = torch.device("cuda", 0)
+    ctx = _lib.context(0)
+    ctx.profile(True)
+    out = {"case": args.case}
+    if args.case == "mst":
+        n = args.n or 300_000
+        rng = np.random.default_rng(11)
+        c = rng.normal(size=(200, 7)) * 3
+        x = (c[rng.integers(0, 200, n)] + 0.5 * rng.normal(size=(n, 7))).astype(np.float32)
+        for _ in range(2):
+            e = evoc.parallel_boruvka(x, 5)
+        out.update(n=n, dim=7, stages_ms=dict(ctx.stages()), total_weight=float(e[:, 2].sum()))
+    else:
+        n = args.n or 262_144
+        k = args.k or 30
+        dim = args.dim or 768
+        x = synthetic.zipf_f32(n=n, dim=dim, seed=7, device=dev)
+        rows = n if args.case != "fp32" else min(n, 37_888)
+        oi = torch.empty((rows, k), dtype=torch.int32, device=dev)
+        od = torch.empty((rows, k), dtype=torch.float32, device=dev)
+        form = {"scan": "bf16_rerank", "fp32": "fp32", "nnd": "nndescent"}[args.case]
+        kw = {"row_begin": 0, "row_end": rows} if args.case == "fp32" else {}
+        o = evoc.KnnGraphOptions(n_neighbors=k, form=form, device=0, scan_type=args.scan_type, **kw)
+        for _ in range(2):
+            evoc.knn_graph_device(x.data_ptr(), 0, n, dim, k, oi.data_ptr(), od.data_ptr(), o)
+        st = ctx.stages()
+        out.update(n=n, dim=dim, k=k, form=form, query_rows=rows)
+        if args.case == "nnd":
+            out["stages_ms"] = {nm: ms for nm, ms in st if nm != "nnd_iteration"}
+            out["iteration_ms"] = [ms for nm, ms in st if nm == "nnd_iteration"]
+            out["nndescent"] = ctx.nndescent_stats()
+        else:
+            out["stages_ms"] = dict(st)
+        if args.case == "scan":
+            out["certificate"] = ctx.certify_counts()
+            out["scan_type"] = args.scan_type
+        if args.case == "fp32":
+            out["tflops_fp32"] = 2.0 * rows * n * dim / (out["stages_ms"]["fp32_scan"] / 1e3) / 1e12
+    torch.cuda.synchronize()
+    print(json.dumps(out))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1348,7 +1407,12 @@ def main():
     ap.add_argument("--serve-capacity", type=int, default=2000)
     ap.add_argument("--serve-baseline", type=int, default=250)
     ap.add_argument("--serve-batch", type=int, default=64, help="most small requests per batch (0: none)")
+    ap.add_argument("--case", default=None, choices=["scan", "fp32", "nnd", "mst"],
+                    help="run one small case of a kernel (timings, ncu captures) instead of the bench")
+    ap.add_argument("--scan-type", default="fp16", choices=["fp16", "bf16"], help="operands of --case scan")
     args = ap.parse_args()
+    if args.case:
+        return run_case(args)  # --n / --dim / --k: the case's own defaults when not given
     wn, wd, wk, _ = WORKLOADS[args.workload]
     args.n = wn if args.n is None else args.n
     args.dim = wd if args.dim is None else args.dim

@@ -174,10 +174,10 @@ int locality_order(evoc_gpu_ctx* ctx, const Job& j, const void* rows, int64_t ro
 // query blocks, one wave of the scan).
 constexpr int64_t kRepairChunk = 16384;
 
-// Candidates kept per row by the 16-bit scan: oversample * k, within [k, n].
+// Candidates kept per row by the 16-bit scan: oversample * k (automatic:
+// ceil(2.5 k)), within [k, n].
 int64_t bf16_candidates(const evoc_gpu_opts& opts, int64_t n, int keff) {
-  const int over = opts.oversample > 0 ? opts.oversample : 2;
-  int64_t C = int64_t(over) * keff;
+  int64_t C = opts.oversample > 0 ? int64_t(opts.oversample) * keff : (int64_t(5) * keff + 1) / 2;
   if (C > n) C = n;
   if (C < keff) C = keff;
   return C;
@@ -306,14 +306,14 @@ int32_t read_count(evoc_gpu_ctx* ctx, const int32_t* d_count, int* rc) {
 
 // Whether `rows` failed rows take the exact FP32 pass directly.  The 16-bit
 // rescan runs a CTA per 128 query rows over every key (a handful of rows
-// leave most SMs idle and pay the 256-candidate epilogue), while the exact
-// pass splits the keys over all SMs at the FP32 rate.  Estimated costs:
-// 16-bit waves x (128 n d 2 FLOP at ~6 TFLOP/s per SM) against
-// rows n d 2 FLOP at ~45 TFLOP/s.
+// leave most SMs idle) and is paced by its 256-candidate epilogue with heaps
+// in global memory, ~2 TFLOP/s per CTA measured; the exact pass splits the
+// keys over all SMs at the FP32 rate (~48 TFLOP/s measured).  Estimated
+// costs: 16-bit waves x 128 n d 2 FLOP / 2e12 against rows n d 2 FLOP / 45e12.
 bool exact_first(const evoc_gpu_ctx* ctx, int64_t rows, int64_t n, int d) {
   const double work = double(n) * double(d) * 2.0;
   const double waves = std::ceil(double((rows + 127) / 128) / double(ctx->sms));
-  const double half_ms = waves * 128.0 * work / 6e12 * 1e3;
+  const double half_ms = waves * 128.0 * work / 2e12 * 1e3;
   const double exact_ms = double(rows) * work / 45e12 * 1e3;
   return exact_ms <= half_ms;
 }
@@ -1439,7 +1439,7 @@ void evoc_gpu_default_opts(evoc_gpu_opts* o) {
   std::memset(o, 0, sizeof(*o));
   o->struct_size = sizeof(evoc_gpu_opts);
   o->form = EVOC_FORM_AUTO;
-  o->oversample = 2;
+  o->oversample = 0;
   o->delta = 0.001f;
   o->delta_improv = 0.001f;
   o->scan_type = 0;  // FP16 operands

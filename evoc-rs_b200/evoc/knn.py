@@ -114,7 +114,7 @@ class KnnGraphOptions:
     deterministic: bool = False
     # GPU-only fields
     form: str = "auto"          # auto | fp32 | bf16_rerank (= half_rerank) | exact_int | nndescent | popcount
-    oversample: int = 2         # bf16_rerank: candidates per row = oversample * k
+    oversample: int = 0         # bf16_rerank: candidates per row = oversample * k (0: ceil(2.5 k))
     scan_type: str = "fp16"     # bf16_rerank: 16-bit operands of the tensor-core scan, fp16 | bf16
     certify: bool = True        # bf16_rerank: certify every row, rescan the rows that fail
     device: Optional[int] = None  # CUDA device; None = torch's current device when torch is loaded, else 0

@@ -64,8 +64,11 @@ typedef enum {
 typedef struct {
   uint32_t struct_size;      /* sizeof(evoc_gpu_opts)                          */
   int32_t form;              /* evoc_form                                      */
-  int32_t oversample;        /* BF16 form: candidates per row = oversample*k;  */
-                             /* <= 0 -> 2                                      */
+  int32_t oversample;        /* 16-bit form: candidates per row =             */
+                             /* oversample*k; <= 0 (the default) -> ceil(2.5k) */
+                             /* (a wider margin between the k-th and the last  */
+                             /* kept candidate: fewer rows fail the           */
+                             /* certificate)                                   */
   int32_t buffers_on_device; /* 1: data and outputs are device pointers on the */
                              /* context's device; 0: host pointers             */
   int32_t deterministic;     /* KnnGraphOptions.deterministic                  */

@@ -36,7 +36,7 @@ def test_version_and_default_opts(libpath):
     assert L.evoc_gpu_version() >= 100
     o = _lib.default_opts()
     assert o.struct_size == C.sizeof(_lib.Opts)
-    assert o.form == _lib.FORM_AUTO and o.oversample == 2
+    assert o.form == _lib.FORM_AUTO and o.oversample == 0  # automatic: ceil(2.5 k) candidates
     assert abs(o.delta - 0.001) < 1e-9 and abs(o.delta_improv - 0.001) < 1e-9
     assert o.scan_type == 0 and o.certify == 1  # FP16 operands, every row certified
     assert o.strict_precision == 0 and o.brute_force_max_n == 0  # KnnGraphOptions' default (src/knn.rs:72)
