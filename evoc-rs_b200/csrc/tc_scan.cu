@@ -14,6 +14,16 @@
 //   warp 1      TMEM allocator + MMA issuer (one elected lane)
 //   warps 2..5  epilogue; warp w reads TMEM lanes 32*(w%4) .. +31
 //
+// CTA-pair variants (cluster of 2, tcgen05 cta_group::2): the two CTAs take
+// two neighbouring query blocks (256 rows) through one M = 256 MMA per key
+// tile.  Each CTA loads its own 128 query rows and half of the 256-row key
+// tile (128 rows) -- 32 KB per pipeline stage instead of 48 KB, a third less
+// L2-to-SM traffic per product -- and the leader CTA issues the MMAs, whose
+// 256 x 256 product lands as 128 x 256 in each CTA's TMEM.  Both CTAs'
+// loads complete on the leader's stage barrier; the leader's commits arrive
+// on both CTAs' stage-free and accumulator-ready barriers; both CTAs'
+// epilogues arrive on the leader's accumulator-free barrier.
+//
 // Three score modes share the kernel: 16-bit float dot products (cosine; FP16
 // or BF16 operands, the same instruction and rate), int8 dot products, and
 // binary Jaccard, where the packed bits are expanded to 0/1
@@ -25,6 +35,7 @@
 // Replaces the distance evaluations of the reference's NN-descent local join
 // (src/nndescent/float.rs:552-660 with fast_cosine, src/fast_cosine.rs:33-45;
 // src/nndescent/int8.rs:15-21 for the int8 dissimilarity).
+#include <algorithm>
 #include <cstring>
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -43,6 +54,7 @@ constexpr int KCB = 128;             // bytes of K per pipeline stage (one 128B 
 constexpr int A_BYTES = BM * KCB;    // 16 KB
 constexpr int B_BYTES = BN * KCB;    // 32 KB
 constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+constexpr int PAIR_STAGE_BYTES = A_BYTES + B_BYTES / 2;  // a CTA of a pair: its query rows and half the key tile
 constexpr int TMEM_COLS = 2 * BN;    // two f32/s32 accumulators
 constexpr size_t SMEM_LIMIT = 232448;      // 227 KB opt-in maximum per block
 constexpr size_t SMEM_FIXED = 1024 /*align*/ + 256 /*barriers*/;
@@ -50,8 +62,9 @@ constexpr uint64_t kDrainNs = 4000000000ull;  // limit of the drain waits whatev
 
 // Shared memory for a pipeline depth, a number of epilogue warp groups (each
 // with one heap per row) and a heap stride (0: heaps in global memory).
-constexpr size_t smem_bytes(int stages, int groups, int heap_stride) {
-  return size_t(stages) * STAGE_BYTES + size_t(groups) * BM * size_t(heap_stride) * 8 + SMEM_FIXED;
+constexpr size_t smem_bytes(int stages, int groups, int heap_stride, bool pair = false) {
+  return size_t(stages) * (pair ? PAIR_STAGE_BYTES : STAGE_BYTES) + size_t(groups) * BM * size_t(heap_stride) * 8 +
+         SMEM_FIXED;
 }
 }  // namespace
 
@@ -305,14 +318,16 @@ __device__ __forceinline__ bool epilogue_vote(int nthreads, bool ok) {
 
 }  // namespace
 
-template <int MODE, int STAGES, int GROUPS, bool kSmemHeap, bool kBatch>
+template <int MODE, int STAGES, int GROUPS, bool kSmemHeap, bool kBatch, bool kPair = false>
 __global__ void __launch_bounds__(64 + GROUPS * 128, 1)
 tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const ScanParams p) {
   using namespace sm100;
+  static_assert(!(kPair && kBatch), "CTA pairs run single requests");
+  constexpr int SB = kPair ? PAIR_STAGE_BYTES : STAGE_BYTES;  // bytes of one stage in this CTA
   extern __shared__ uint8_t smem_dyn[];
   const uint32_t pad = (1024u - (smem_addr(smem_dyn) & 1023u)) & 1023u;
   uint8_t* smem = smem_dyn + pad;
-  uint64_t* heaps = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
+  uint64_t* heaps = reinterpret_cast<uint64_t*>(smem + STAGES * SB);
   // Barriers follow every group's heaps (GROUPS x BM rows of heap_stride words).
   uint64_t* bars = kSmemHeap ? heaps + GROUPS * BM * p.heap_stride : heaps;
   uint64_t* full = bars;
@@ -323,6 +338,8 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 5);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = kPair ? cluster_rank() : 0u;  // 0: the leader (it issues the pair's MMAs)
+  const bool leader = rank == 0;
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; s++) {
       mbar_init(&full[s], 1);
@@ -330,7 +347,7 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     }
     for (int a = 0; a < 2; a++) {
       mbar_init(&tfull[a], 1);
-      mbar_init(&tempty[a], GROUPS * 128);
+      mbar_init(&tempty[a], (kPair ? 2 : 1) * GROUPS * 128);  // a pair: both CTAs' epilogue threads
     }
     mbar_init(mma_done, 1);
     fence_barrier_init();
@@ -340,20 +357,32 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     prefetch_tmap(&tmB);
   }
   if (warp == 1) {
-    tmem_alloc(tmem_slot, TMEM_COLS);
-    tmem_relinquish();
+    if (kPair) {
+      tmem_alloc_pair(tmem_slot, TMEM_COLS);
+      tmem_relinquish_pair();
+    } else {
+      tmem_alloc(tmem_slot, TMEM_COLS);
+      tmem_relinquish();
+    }
   }
   tc_fence_before();
   __syncthreads();
+  if (kPair) cluster_sync();  // both CTAs' barriers are initialised before either signals the other's
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
 
   constexpr bool kInt8 = MODE != kModeHalf;
-  const int64_t n_items = kBatch ? int64_t(*p.n_items) : (p.n_q + BM - 1) / BM;
+  // Work items: query blocks (a pair: pairs of neighbouring blocks), strided
+  // over the CTAs (the clusters).
+  const int64_t n_blocks = kBatch ? int64_t(*p.n_items) : (p.n_q + BM - 1) / BM;
+  const int64_t n_items = kPair ? (n_blocks + 1) / 2 : n_blocks;
+  const int64_t item0 = kPair ? int64_t(blockIdx.x >> 1) : int64_t(blockIdx.x);
+  const int64_t item_step = kPair ? int64_t(gridDim.x >> 1) : int64_t(gridDim.x);
   const volatile int* abort = p.status;
   constexpr int KC_ELEMS = kInt8 ? KCB : KCB / 2;
-  const uint32_t IDESC = kInt8 ? idesc_s8_s32(BM, BN)
-                               : (p.half_type == kHalfBf16 ? idesc_bf16_f32(BM, BN) : idesc_f16_f32(BM, BN));
+  constexpr int MM = kPair ? 2 * BM : BM;  // rows of one MMA
+  const uint32_t IDESC = kInt8 ? idesc_s8_s32(MM, BN)
+                               : (p.half_type == kHalfBf16 ? idesc_bf16_f32(MM, BN) : idesc_f16_f32(MM, BN));
 
   if (warp == 0) {
     // ------------------------------------------------------------ producer
@@ -364,8 +393,8 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
       }
       uint32_t it = 0;
       bool ok = true;
-      for (int64_t itm = blockIdx.x; ok && itm < n_items; itm += gridDim.x) {
-        const ItemView v = item_view<kBatch>(p, &tmA, &tmB, itm);
+      for (int64_t itm = item0; ok && itm < n_items; itm += item_step) {
+        const ItemView v = item_view<kBatch>(p, &tmA, &tmB, kPair ? 2 * itm + rank : itm);
         if (kBatch) {
           tensormap_acquire(v.ma);
           tensormap_acquire(v.mb);
@@ -378,26 +407,38 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
               ok = false;
               break;
             }
-            uint8_t* a_dst = smem + s * STAGE_BYTES;
-            mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
-            tma_load_2d(a_dst, v.ma, &full[s], kc * KC_ELEMS, int32_t(v.q_row0 + v.qb * BM));
-            tma_load_2d(a_dst + A_BYTES, v.mb, &full[s], kc * KC_ELEMS, int32_t(kt * BN));
+            uint8_t* a_dst = smem + s * SB;
+            if (kPair) {
+              // both CTAs' bytes complete on the leader's barrier, armed by the leader for the two
+              const uint32_t bar = mapa_shared(smem_addr(&full[s]), 0);
+              if (leader) mbar_arrive_expect_tx(&full[s], 2 * SB);
+              tma_load_2d_pair(a_dst, v.ma, bar, kc * KC_ELEMS, int32_t(v.q_row0 + v.qb * BM));
+              tma_load_2d_pair(a_dst + A_BYTES, v.mb, bar, kc * KC_ELEMS, int32_t(kt * BN + rank * BM));
+            } else {
+              mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
+              tma_load_2d(a_dst, v.ma, &full[s], kc * KC_ELEMS, int32_t(v.q_row0 + v.qb * BM));
+              tma_load_2d(a_dst + A_BYTES, v.mb, &full[s], kc * KC_ELEMS, int32_t(kt * BN));
+            }
             it++;
           }
         }
       }
       // Let the last loads land before the CTA can exit (full-length limit:
-      // these loads were issued and complete on their own).
-      for (uint32_t j = (it > STAGES ? it - STAGES : 0); j < it; j++)
-        mbar_wait(&full[j % STAGES], (j / STAGES) & 1u, nullptr, p.drain_ns);
+      // these loads were issued and complete on their own).  A pair's second
+      // CTA cannot see the leader's barrier: it waits for the MMAs to release
+      // its last stages instead, which they do only after reading them.
+      for (uint32_t j = (it > STAGES ? it - STAGES : 0); j < it; j++) {
+        if (!kPair || leader) mbar_wait(&full[j % STAGES], (j / STAGES) & 1u, nullptr, p.drain_ns);
+        else mbar_wait(&empty[j % STAGES], (j / STAGES) & 1u, nullptr, p.drain_ns);
+      }
     }
   } else if (warp == 1) {
     // ----------------------------------------------------------- MMA issuer
-    if (lane == 0) {
+    if (lane == 0 && leader) {
       uint32_t it = 0, tile = 0;
       bool ok = true;
-      for (int64_t itm = blockIdx.x; ok && itm < n_items; itm += gridDim.x) {
-        const ItemView v = item_view<kBatch>(p, &tmA, &tmB, itm);
+      for (int64_t itm = item0; ok && itm < n_items; itm += item_step) {
+        const ItemView v = item_view<kBatch>(p, &tmA, &tmB, kPair ? 2 * itm : itm);
         for (int64_t kt = 0; ok && kt < v.n_ktiles; kt++, tile++) {
           const uint32_t a = tile & 1u, tph = (tile >> 1) & 1u;
           if (!mbar_wait(&tempty[a], tph ^ 1u, abort, p.timeout_ns)) {
@@ -415,23 +456,34 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
               break;
             }
             tc_fence_after();
-            const uint32_t a_addr = smem_addr(smem + s * STAGE_BYTES);
+            const uint32_t a_addr = smem_addr(smem + s * SB);
             const uint64_t adesc = sw128_kmajor_desc(a_addr);
             const uint64_t bdesc = sw128_kmajor_desc(a_addr + A_BYTES);
 #pragma unroll
             for (int j = 0; j < KCB / 32; j++) {  // 32 bytes of K per instruction
               const uint32_t acc = (kc > 0 || j > 0) ? 1u : 0u;
-              if (kInt8) mma_i8(d_tmem, adesc + 2 * j, bdesc + 2 * j, IDESC, acc);
-              else mma_f16(d_tmem, adesc + 2 * j, bdesc + 2 * j, IDESC, acc);
+              if (kPair) {
+                if (kInt8) mma_i8_pair(d_tmem, adesc + 2 * j, bdesc + 2 * j, IDESC, acc);
+                else mma_f16_pair(d_tmem, adesc + 2 * j, bdesc + 2 * j, IDESC, acc);
+              } else {
+                if (kInt8) mma_i8(d_tmem, adesc + 2 * j, bdesc + 2 * j, IDESC, acc);
+                else mma_f16(d_tmem, adesc + 2 * j, bdesc + 2 * j, IDESC, acc);
+              }
             }
-            mma_commit(&empty[s]);  // stage is free once these MMAs have read it
+            // stage is free (in both CTAs of a pair) once these MMAs have read it
+            if (kPair) mma_commit_pair_mc(&empty[s], 3);
+            else mma_commit(&empty[s]);
             it++;
           }
           if (!ok) break;
-          mma_commit(&tfull[a]);  // accumulator ready for the epilogue
+          // accumulator ready for the epilogue (both CTAs' TMEM)
+          if (kPair) mma_commit_pair_mc(&tfull[a], 3);
+          else mma_commit(&tfull[a]);
         }
       }
-      mma_commit(mma_done);  // every MMA issued completes before TMEM is freed
+      // every MMA issued completes before TMEM is freed
+      if (kPair) mma_commit_pair_mc(mma_done, 1);
+      else mma_commit(mma_done);
       mbar_wait(mma_done, 0, nullptr, p.drain_ns);
     }
   } else {
@@ -446,10 +498,13 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     const int heap_slot = group * BM + row_local;
     uint64_t* hstore = kSmemHeap ? heaps + int64_t(heap_slot) * p.heap_stride
                                  : p.scratch + (int64_t(blockIdx.x) * GROUPS * BM + heap_slot) * p.heap_stride;
+    // a pair's second CTA frees the accumulator on the leader's barrier
+    const uint32_t tempty_c0 = kPair ? mapa_shared(smem_addr(&tempty[0]), 0) : 0u;
+    const uint32_t tempty_c1 = kPair ? mapa_shared(smem_addr(&tempty[1]), 0) : 0u;
     uint32_t tile = 0;
     bool ok = true;
-    for (int64_t itm = blockIdx.x; ok && itm < n_items; itm += gridDim.x) {
-      const ItemView v = item_view<kBatch>(p, &tmA, &tmB, itm);
+    for (int64_t itm = item0; ok && itm < n_items; itm += item_step) {
+      const ItemView v = item_view<kBatch>(p, &tmA, &tmB, kPair ? 2 * itm + rank : itm);
       const int64_t q = v.qb * BM + row_local;  // output row
       const bool valid = q < v.n_q;
       // row of the data set (its key index for the self rule)
@@ -490,7 +545,8 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
           }
         }
         tc_fence_before();
-        mbar_arrive(&tempty[a]);
+        if (kPair && !leader) mbar_arrive_cluster(a ? tempty_c1 : tempty_c0);
+        else mbar_arrive(&tempty[a]);
       }
       if (GROUPS > 1) ok = epilogue_vote(GROUPS * 128, ok);
       if (!ok) break;
@@ -538,9 +594,13 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
 
   tc_fence_before();
   __syncthreads();
+  // A pair's CTAs leave together: the leader's MMAs have read the peer's
+  // stages, the peer's arrivals and loads have reached the leader's barriers.
+  if (kPair) cluster_sync();
   if (warp == 1) {
     tc_fence_after();
-    tmem_dealloc(tmem_base, TMEM_COLS);
+    if (kPair) tmem_dealloc_pair(tmem_base, TMEM_COLS);
+    else tmem_dealloc(tmem_base, TMEM_COLS);
   }
 }
 
@@ -600,14 +660,58 @@ cudaError_t launch_variant(const CUtensorMap& ma, const CUtensorMap& mb, const S
   return cudaGetLastError();
 }
 
+// CTA-pair variants: clusters of two, at most as many as the GPU holds at
+// once (neighbouring SMs of a GPC pair up; one CTA per SM), a pair of query
+// blocks per cluster and item.  `grid` is the caller's CTA budget.
+template <int MODE, int STAGES, int GROUPS>
+cudaError_t launch_pair(const CUtensorMap& ma, const CUtensorMap& mb, const ScanParams& p, int grid, size_t smem,
+                        cudaStream_t stream) {
+  auto kern = tc_scan_kernel<MODE, STAGES, GROUPS, true, false, true>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_LIMIT));
+  if (e != cudaSuccess) return e;
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.blockDim = dim3(64 + GROUPS * 128);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  // Clusters resident at once, for this instantiation at the largest shared
+  // memory any launch of it asks for (one CTA per SM); looked up once, the
+  // initialisation of a local static being thread-safe for serving lanes.
+  static const int max_clusters = [&]() {
+    cudaLaunchConfig_t c = cfg;
+    c.gridDim = dim3(2);
+    c.dynamicSmemBytes = SMEM_LIMIT;
+    int m = 0;
+    if (cudaOccupancyMaxActiveClusters(&m, kern, &c) != cudaSuccess) {
+      cudaGetLastError();
+      m = 0;
+    }
+    return m > 0 ? m : 1;
+  }();
+  const int64_t items = (p.n_q + 2 * BM - 1) / (2 * BM);
+  int64_t clusters = std::min<int64_t>({items, int64_t(grid + 1) / 2, int64_t(max_clusters)});
+  if (clusters < 1) clusters = 1;
+  cfg.gridDim = dim3(unsigned(2 * clusters));
+  e = cudaLaunchKernelEx(&cfg, kern, ma, mb, p);
+  if (e != cudaSuccess) return e;
+  return cudaGetLastError();
+}
+
 // The kernel variants an autotuner may choose between: pipeline stages,
-// epilogue warp groups, heaps in shared (s) or global (g) memory.
-constexpr int kVariantCfg[6][3] = {{4, 2, 1}, {3, 2, 1}, {4, 1, 1}, {3, 1, 1}, {4, 1, 0}, {2, 2, 1}};
+// epilogue warp groups, heaps in shared (1) or global (0) memory, CTA pair (1).
+constexpr int kVariantCfg[kScanVariants][4] = {{4, 2, 1, 0}, {3, 2, 1, 0}, {4, 1, 1, 0}, {3, 1, 1, 0}, {4, 1, 0, 0},
+                                               {2, 2, 1, 0}, {4, 2, 1, 1}, {4, 1, 1, 1}, {6, 1, 1, 1}, {3, 2, 1, 1}};
 
 bool variant_feasible(int v, int keep, bool has_scratch) {
-  if (v < 0 || v > 5) return false;
+  if (v < 0 || v >= kScanVariants) return false;
   if (kVariantCfg[v][2] == 0) return has_scratch;
-  return smem_bytes(kVariantCfg[v][0], kVariantCfg[v][1], keep | 1) <= SMEM_LIMIT;
+  return smem_bytes(kVariantCfg[v][0], kVariantCfg[v][1], keep | 1, kVariantCfg[v][3] != 0) <= SMEM_LIMIT;
 }
 
 template <int MODE>
@@ -621,6 +725,10 @@ cudaError_t launch_forced(const CUtensorMap& ma, const CUtensorMap& mb, ScanPara
     case 2: return launch_variant<MODE, 4, 1, true>(ma, mb, p, grid, smem_bytes(4, 1, odd), stream);
     case 3: return launch_variant<MODE, 3, 1, true>(ma, mb, p, grid, smem_bytes(3, 1, odd), stream);
     case 5: return launch_variant<MODE, 2, 2, true>(ma, mb, p, grid, smem_bytes(2, 2, odd), stream);
+    case 6: return launch_pair<MODE, 4, 2>(ma, mb, p, grid, smem_bytes(4, 2, odd, true), stream);
+    case 7: return launch_pair<MODE, 4, 1>(ma, mb, p, grid, smem_bytes(4, 1, odd, true), stream);
+    case 8: return launch_pair<MODE, 6, 1>(ma, mb, p, grid, smem_bytes(6, 1, odd, true), stream);
+    case 9: return launch_pair<MODE, 3, 2>(ma, mb, p, grid, smem_bytes(3, 2, odd, true), stream);
     default:
       p.heap_stride = p.keep;
       return launch_variant<MODE, 4, 1, false>(ma, mb, p, grid, smem_bytes(4, 1, 0), stream);
@@ -668,9 +776,12 @@ cudaError_t launch_tc_scan(int mode, const void* Q, int64_t q_rows, int64_t q_ro
   if (half_type != kHalfF16 && half_type != kHalfBf16) return cudaErrorInvalidValue;
   if (q_self && q_row0 != 0) return cudaErrorInvalidValue;
   const int eb = mode == kModeHalf ? 2 : 1;
+  // A CTA pair loads half of each key tile per CTA: 128-row boxes (the
+  // variant launch_mode takes, a forced one when it is feasible).
+  const bool pair = variant >= 0 && variant_feasible(variant, keep, scratch != nullptr) && kVariantCfg[variant][3];
   alignas(64) CUtensorMap ma, mb;
   if (!make_map(&ma, Q, q_rows, row_bytes, eb, BM, half_type) ||
-      !make_map(&mb, K, k_rows, row_bytes, eb, BN, half_type))
+      !make_map(&mb, K, k_rows, row_bytes, eb, pair ? BM : BN, half_type))
     return cudaErrorInvalidValue;
   ScanParams p{};
   p.n_q = n_q;
@@ -709,13 +820,17 @@ bool tc_scan_uses_global_heaps(int variant, int keep) {
 }
 
 const char* tc_scan_variant_name(int variant) {
-  static const char* names[6] = {"4 stages, 2 epilogue groups, shared-memory heaps",
-                                 "3 stages, 2 epilogue groups, shared-memory heaps",
-                                 "4 stages, 1 epilogue group, shared-memory heaps",
-                                 "3 stages, 1 epilogue group, shared-memory heaps",
-                                 "4 stages, 1 epilogue group, global-memory heaps",
-                                 "2 stages, 2 epilogue groups, shared-memory heaps"};
-  return variant >= 0 && variant < 6 ? names[variant] : "automatic";
+  static const char* names[kScanVariants] = {"4 stages, 2 epilogue groups, shared-memory heaps",
+                                             "3 stages, 2 epilogue groups, shared-memory heaps",
+                                             "4 stages, 1 epilogue group, shared-memory heaps",
+                                             "3 stages, 1 epilogue group, shared-memory heaps",
+                                             "4 stages, 1 epilogue group, global-memory heaps",
+                                             "2 stages, 2 epilogue groups, shared-memory heaps",
+                                             "CTA pair, 4 stages, 2 epilogue groups, shared-memory heaps",
+                                             "CTA pair, 4 stages, 1 epilogue group, shared-memory heaps",
+                                             "CTA pair, 6 stages, 1 epilogue group, shared-memory heaps",
+                                             "CTA pair, 3 stages, 2 epilogue groups, shared-memory heaps"};
+  return variant >= 0 && variant < kScanVariants ? names[variant] : "automatic";
 }
 
 // ---------------------------------------------------------------------------

@@ -71,3 +71,60 @@ def test_tune_load_and_errors(tmp_path):
         ctx.close()
     with pytest.raises(evoc.BackendError):
         evoc.autotune("Float32", 1000, 64, 15, "fp32")
+
+
+def _forced_graph(tmp_path, monkeypatch, x, kind, form, k, variant, **opt):
+    """The graph with the scan's kernel variant forced through a fresh context's tune cache."""
+    import ctypes as C
+
+    n, dim = x.shape
+    mode = {"Float32": 0, "Int8": 1, "UInt8": 2}[kind]
+    keep = k if form == "exact_int" else (5 * k + 1) // 2
+    log2n = int(np.floor(np.log2(n)))
+    forced = tmp_path / f"forced{variant}.txt"
+    forced.write_text(f"evoc-tune 1 mode={mode} keep={keep} row_bytes={{rb}} log2n={log2n} variant={variant} ms=0\n")
+    row_bytes = {"Float32": ((dim + 63) // 64) * 64 * 2, "Int8": ((dim + 127) // 128) * 128,
+                 "UInt8": ((dim * 8 + 127) // 128) * 128}[kind]
+    forced.write_text(forced.read_text().replace("{rb}", str(row_bytes)))
+    monkeypatch.setenv("EVOC_TUNE_CACHE", str(forced))
+    ctx = _lib.Context(0)
+    try:
+        arr = np.ascontiguousarray(x)
+        r0, r1 = opt.get("row_begin", 0), opt.get("row_end", 0)
+        m = (r1 - r0) if (r0 or r1) else n
+        ind = np.empty((m, k), np.int32)
+        dst = np.empty((m, k), np.float32)
+        o = _lib.default_opts()
+        o.form = _lib.FORM_NAMES[form]
+        o.row_begin, o.row_end = r0, r1
+        P = C.c_void_p
+        st = _lib.lib().evoc_gpu_knn_graph(ctx.h, C.byref(o), {"Float32": 0, "Int8": 1, "UInt8": 2}[kind],
+                                          arr.ctypes.data_as(P), n, dim, k, None, ind.ctypes.data_as(P),
+                                          dst.ctypes.data_as(P), None)
+        assert st == 0, ctx.last_error()
+        return ind, dst
+    finally:
+        ctx.close()
+        monkeypatch.delenv("EVOC_TUNE_CACHE")
+
+
+@pytest.mark.parametrize("variant", [6, 7, 8, 9])
+@pytest.mark.parametrize("n", [2900, 300, 129])
+def test_cta_pair_variants_match_single_cta(tmp_path, monkeypatch, variant, n):
+    """The CTA-pair scans (cluster of two, M = 256 MMAs) give the single-CTA graph bit for bit, with an
+    odd number of query blocks (the last pair half empty), a single block, and a row slice starting
+    mid-block."""
+    x = _f32(n, 96, 7)
+    base = evoc.knn_graph(x, evoc.KnnGraphOptions(n_neighbors=15, form="bf16_rerank"))
+    ind, dst = _forced_graph(tmp_path, monkeypatch, x, "Float32", "bf16_rerank", 15, variant)
+    assert np.array_equal(ind, base[0]) and np.array_equal(dst.view(np.uint32), base[1].view(np.uint32))
+    if n > 200:
+        r0, r1 = 37, n - 11
+        ind, dst = _forced_graph(tmp_path, monkeypatch, x, "Float32", "bf16_rerank", 15, variant, row_begin=r0,
+                                 row_end=r1)
+        assert np.array_equal(ind, base[0][r0:r1]) and np.array_equal(dst.view(np.uint32),
+                                                                      base[1][r0:r1].view(np.uint32))
+    xi = np.clip(np.round(127 * x), -127, 127).astype(np.int8)
+    bi = evoc.knn_graph(xi, evoc.KnnGraphOptions(n_neighbors=15, form="exact_int"))
+    ind, dst = _forced_graph(tmp_path, monkeypatch, xi, "Int8", "exact_int", 15, variant)
+    assert np.array_equal(ind, bi[0]) and np.array_equal(dst.view(np.uint32), bi[1].view(np.uint32))
