@@ -377,7 +377,7 @@ def run_serving(args, dev):
            "data": "rows cut from 4 pinned-host mixtures per (d, dtype), window chosen by request id",
            "timing": "host monotonic clock: scheduled arrival -> graph copied back to host memory"}
     with Server(budget_bytes=150 * 10**9, max_inflight=args.serve_lanes, profile=True,
-                batch_max=args.serve_batch) as srv:
+                batch_max=args.serve_batch, small_lanes=args.serve_small_lanes) as srv:
         serve_stream(srv, pools, warm_sched, list(range(len(warm_sched["n"]))), k, paced=False)
         t0, rec = serve_stream(srv, pools, sched, list(range(len(sched["n"]))), k, paced=True)
         out.update(serving_summary(t0, rec, sched))
@@ -1324,6 +1324,10 @@ def run_case(args):
     from evoc import _lib, synthetic
 
     dev = torch.device("cuda", 0)
+    if args.case == "serve":  # the serving leg alone (its own JSON object)
+        print(json.dumps({"case": "serve", "lanes": args.serve_lanes, "small_lanes": args.serve_small_lanes,
+                          "serving": run_serving(args, dev)}))
+        return 0
     ctx = _lib.context(0)
     ctx.profile(True)
     out = {"case": args.case}
@@ -1407,7 +1411,9 @@ def main():
     ap.add_argument("--serve-capacity", type=int, default=2000)
     ap.add_argument("--serve-baseline", type=int, default=250)
     ap.add_argument("--serve-batch", type=int, default=64, help="most small requests per batch (0: none)")
-    ap.add_argument("--case", default=None, choices=["scan", "fp32", "nnd", "mst"],
+    ap.add_argument("--serve-small-lanes", type=int, default=-1,
+                    help="serving lanes for requests under 65,536 rows only (-1: a quarter of the lanes)")
+    ap.add_argument("--case", default=None, choices=["scan", "fp32", "nnd", "mst", "serve"],
                     help="run one small case of a kernel (timings, ncu captures) instead of the bench")
     ap.add_argument("--scan-type", default="fp16", choices=["fp16", "bf16"], help="operands of --case scan")
     args = ap.parse_args()

@@ -98,11 +98,14 @@ constexpr double kBatchWork = 4e12;
 // requests pending.  With fewer, each runs alone at its lowest latency.
 constexpr int kBatchMin = 4;
 // Requests below this many rows are latency-sensitive: they run on a lane's
-// high-priority stream, and the last lanes (a quarter of them, with four or
-// more lanes) admit only these, so a burst of big requests never leaves the
-// small ones queueing for a lane.
+// high-priority stream, and the last lanes (small_lanes of the options; by
+// default a quarter of them, with four or more lanes) admit only these, so a
+// burst of big requests never leaves the small ones queueing for a lane.
 constexpr int64_t kUrgentRows = 65536;
-int small_only_lanes(int lanes) { return lanes >= 4 ? lanes / 4 : 0; }
+int small_only_lanes(int lanes, int asked) {
+  if (asked >= 0) return asked < lanes ? asked : lanes - 1;  // at least one lane takes big requests
+  return lanes >= 4 ? lanes / 4 : 0;
+}
 
 }  // namespace
 
@@ -110,6 +113,7 @@ struct evoc_gpu_server {
   int device = 0;
   int64_t budget = 0;
   int lanes = 0;
+  int small_lanes = 0;  // the last lanes admit only requests under kUrgentRows rows
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   std::deque<std::shared_ptr<Job>> pending;
@@ -359,7 +363,7 @@ bool try_admit_batch(evoc_gpu_server* s, std::deque<std::shared_ptr<Job>>::itera
 void worker(evoc_gpu_server* s, int lane) {
   cudaSetDevice(s->device);
   evoc::CtxSizes& mine = s->lane_sizes[size_t(lane)];
-  const bool small_only = lane >= s->lanes - small_only_lanes(s->lanes);
+  const bool small_only = lane >= s->lanes - s->small_lanes;
   std::unique_lock<std::mutex> lock(s->mu);
   for (;;) {
     std::vector<std::shared_ptr<Job>> group;
@@ -475,6 +479,7 @@ void evoc_gpu_server_default_opts(evoc_gpu_server_opts* o) {
   o->budget_bytes = int64_t(150) * 1000 * 1000 * 1000;
   o->max_inflight = 4;
   o->batch_max = kBatchJobs;
+  o->small_lanes = -1;
 }
 
 int evoc_gpu_server_create(const evoc_gpu_server_opts* opts, evoc_gpu_server** out) {
@@ -495,6 +500,7 @@ int evoc_gpu_server_create(const evoc_gpu_server_opts* opts, evoc_gpu_server** o
   s->device = o.device;
   s->budget = o.budget_bytes;
   s->lanes = o.max_inflight;
+  s->small_lanes = small_only_lanes(s->lanes, o.small_lanes);
   s->lane_sizes.assign(size_t(s->lanes), evoc::CtxSizes{});
   auto bail = [&](int rc) {
     for (evoc_gpu_ctx* p : s->ctxs) evoc_gpu_ctx_destroy(p);

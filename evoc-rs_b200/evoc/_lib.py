@@ -189,7 +189,8 @@ class ServerOpts(C.Structure):
         ("max_inflight", C.c_int32),
         ("profile", C.c_int32),
         ("batch_max", C.c_int32),
-        ("reserved", C.c_int32 * 3),
+        ("small_lanes", C.c_int32),
+        ("reserved", C.c_int32 * 2),
     ]
 
 

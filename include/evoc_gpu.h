@@ -496,7 +496,10 @@ typedef struct {
                          /* and keep per-stage totals (server_stage)        */
   int32_t batch_max;     /* most small requests in one batch; 0 or 1: no    */
                          /* batching; default 64                            */
-  int32_t reserved[3];
+  int32_t small_lanes;   /* lanes that admit only requests under 65,536     */
+                         /* rows (of max_inflight); < 0 (default): a       */
+                         /* quarter of the lanes when there are 4 or more  */
+  int32_t reserved[2];
 } evoc_gpu_server_opts;
 
 typedef struct {
