@@ -63,11 +63,13 @@ WORKLOADS = {
                                  "128 B/row, Jaccard k=15, seed 13"),
 }
 
-# DRAM bytes (read + write) of one launch of the BF16 scan: 5.826e9 B captured
-# with ncu (dram__bytes_read.sum + dram__bytes_write.sum) at n = 262,144, scaled
-# by the number of (query, key) pairs to n = 1,000,000 (the key rows are
-# re-streamed once per wave of query blocks, so traffic grows with n^2).
-SCAN_TRAFFIC_BYTES_262K = 5_825_927_424
+# DRAM bytes (read + write) of one launch of the 16-bit scan (FP16 operands,
+# keep 75, 3 stages, 1 epilogue group -- the variant the tuner picks): 6.393e9 B
+# captured with ncu (dram__bytes_read.sum + dram__bytes_write.sum) at
+# n = 262,144, scaled by the number of (query, key) pairs to n = 1,000,000 (the
+# key rows are re-streamed once per wave of query blocks, so traffic grows
+# with n^2).
+SCAN_TRAFFIC_BYTES_262K = 6_392_895_864
 
 
 def scan_traffic(n):
@@ -377,7 +379,8 @@ def run_serving(args, dev):
            "data": "rows cut from 4 pinned-host mixtures per (d, dtype), window chosen by request id",
            "timing": "host monotonic clock: scheduled arrival -> graph copied back to host memory"}
     with Server(budget_bytes=150 * 10**9, max_inflight=args.serve_lanes, profile=True,
-                batch_max=args.serve_batch, small_lanes=args.serve_small_lanes) as srv:
+                batch_max=args.serve_batch, small_lanes=args.serve_small_lanes,
+                admission=args.serve_admission) as srv:
         serve_stream(srv, pools, warm_sched, list(range(len(warm_sched["n"]))), k, paced=False)
         t0, rec = serve_stream(srv, pools, sched, list(range(len(sched["n"]))), k, paced=True)
         out.update(serving_summary(t0, rec, sched))
@@ -1326,6 +1329,7 @@ def run_case(args):
     dev = torch.device("cuda", 0)
     if args.case == "serve":  # the serving leg alone (its own JSON object)
         print(json.dumps({"case": "serve", "lanes": args.serve_lanes, "small_lanes": args.serve_small_lanes,
+                          "admission": args.serve_admission,
                           "serving": run_serving(args, dev)}))
         return 0
     ctx = _lib.context(0)
@@ -1411,8 +1415,10 @@ def main():
     ap.add_argument("--serve-capacity", type=int, default=2000)
     ap.add_argument("--serve-baseline", type=int, default=250)
     ap.add_argument("--serve-batch", type=int, default=64, help="most small requests per batch (0: none)")
-    ap.add_argument("--serve-small-lanes", type=int, default=-1,
-                    help="serving lanes for requests under 65,536 rows only (-1: a quarter of the lanes)")
+    ap.add_argument("--serve-small-lanes", type=int, default=0,
+                    help="serving lanes for requests under 65,536 rows only")
+    ap.add_argument("--serve-admission", default="oldest", choices=["oldest", "smallest"],
+                    help="serving admission order: oldest request first, or smallest scan first")
     ap.add_argument("--case", default=None, choices=["scan", "fp32", "nnd", "mst", "serve"],
                     help="run one small case of a kernel (timings, ncu captures) instead of the bench")
     ap.add_argument("--scan-type", default="fp16", choices=["fp16", "bf16"], help="operands of --case scan")

@@ -103,8 +103,8 @@ constexpr int kBatchMin = 4;
 // burst of big requests never leaves the small ones queueing for a lane.
 constexpr int64_t kUrgentRows = 65536;
 int small_only_lanes(int lanes, int asked) {
-  if (asked >= 0) return asked < lanes ? asked : lanes - 1;  // at least one lane takes big requests
-  return lanes >= 4 ? lanes / 4 : 0;
+  if (asked <= 0) return 0;
+  return asked < lanes ? asked : lanes - 1;  // at least one lane takes big requests
 }
 
 }  // namespace
@@ -114,6 +114,7 @@ struct evoc_gpu_server {
   int64_t budget = 0;
   int lanes = 0;
   int small_lanes = 0;  // the last lanes admit only requests under kUrgentRows rows
+  bool smallest_first = false;  // admission order: smallest scan first (else oldest first)
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   std::deque<std::shared_ptr<Job>> pending;
@@ -370,11 +371,18 @@ void worker(evoc_gpu_server* s, int lane) {
     bool batch = false;
     bool trim = false;
     while (!s->stopping) {
-      // First fit over the pending requests, oldest first; a request skipped
-      // kMaxSkips times holds the next admission for itself.  A small request
-      // takes compatible small ones after it into the same batch.
-      // A small-only lane passes over big requests without counting a skip.
-      for (auto it = s->pending.begin(); it != s->pending.end(); ++it) {
+      // First fit over the pending requests, oldest first (or smallest scan
+      // first); a request skipped kMaxSkips times holds the next admission
+      // for itself.  A small request takes compatible small ones after it
+      // into the same batch.  A small-only lane passes over big requests
+      // without counting a skip.
+      std::vector<std::deque<std::shared_ptr<Job>>::iterator> order;
+      order.reserve(s->pending.size());
+      for (auto it = s->pending.begin(); it != s->pending.end(); ++it) order.push_back(it);
+      if (s->smallest_first && !s->pending.empty() && s->pending.front()->skipped < kMaxSkips)
+        std::stable_sort(order.begin(), order.end(),
+                         [](const auto& a, const auto& b) { return (*a)->work < (*b)->work; });
+      for (auto it : order) {  // every branch that erases from pending leaves the loop
         Job* j = it->get();
         if (small_only && j->n >= kUrgentRows) continue;
         if (j->batch_ok && s->batch_max > 1 && try_admit_batch(s, it, mine, &group, small_only)) {
@@ -479,7 +487,8 @@ void evoc_gpu_server_default_opts(evoc_gpu_server_opts* o) {
   o->budget_bytes = int64_t(150) * 1000 * 1000 * 1000;
   o->max_inflight = 4;
   o->batch_max = kBatchJobs;
-  o->small_lanes = -1;
+  o->small_lanes = 0;
+  o->admission = 0;
 }
 
 int evoc_gpu_server_create(const evoc_gpu_server_opts* opts, evoc_gpu_server** out) {
@@ -492,6 +501,7 @@ int evoc_gpu_server_create(const evoc_gpu_server_opts* opts, evoc_gpu_server** o
     o = *opts;
   }
   if (o.max_inflight < 1 || o.max_inflight > 64 || o.budget_bytes <= 0) return EVOC_ERR_ARG;
+  if (o.admission < 0 || o.admission > 1) return EVOC_ERR_ARG;
   if (cudaSetDevice(o.device) != cudaSuccess) {
     cudaGetLastError();
     return EVOC_ERR_CUDA;
@@ -501,6 +511,7 @@ int evoc_gpu_server_create(const evoc_gpu_server_opts* opts, evoc_gpu_server** o
   s->budget = o.budget_bytes;
   s->lanes = o.max_inflight;
   s->small_lanes = small_only_lanes(s->lanes, o.small_lanes);
+  s->smallest_first = o.admission == 1;
   s->lane_sizes.assign(size_t(s->lanes), evoc::CtxSizes{});
   auto bail = [&](int rc) {
     for (evoc_gpu_ctx* p : s->ctxs) evoc_gpu_ctx_destroy(p);

@@ -190,7 +190,8 @@ class ServerOpts(C.Structure):
         ("profile", C.c_int32),
         ("batch_max", C.c_int32),
         ("small_lanes", C.c_int32),
-        ("reserved", C.c_int32 * 2),
+        ("admission", C.c_int32),
+        ("reserved", C.c_int32 * 1),
     ]
 
 

@@ -33,7 +33,7 @@ class Server:
     """One evoc_gpu_server on one device."""
 
     def __init__(self, budget_bytes: int = 150 * 10**9, max_inflight: int = 4, device: int = 0,
-                 profile: bool = False, batch_max: int = 64, small_lanes: int = -1):
+                 profile: bool = False, batch_max: int = 64, small_lanes: int = 0, admission: str = "oldest"):
         L = _lib.lib()
         o = _lib.ServerOpts()
         L.evoc_gpu_server_default_opts(C.byref(o))
@@ -42,7 +42,10 @@ class Server:
         o.max_inflight = int(max_inflight)
         o.profile = 1 if profile else 0
         o.batch_max = int(batch_max)
-        o.small_lanes = int(small_lanes)  # lanes for requests under 65,536 rows only (-1: a quarter)
+        o.small_lanes = int(small_lanes)  # lanes for requests under 65,536 rows only
+        if admission not in ("oldest", "smallest"):
+            raise ValueError("admission must be 'oldest' or 'smallest'")
+        o.admission = 0 if admission == "oldest" else 1  # oldest request first, or smallest scan first
         self.h = C.c_void_p()
         rc = L.evoc_gpu_server_create(C.byref(o), C.byref(self.h))
         if rc != _lib.EVOC_OK:

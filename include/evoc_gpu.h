@@ -497,9 +497,11 @@ typedef struct {
   int32_t batch_max;     /* most small requests in one batch; 0 or 1: no    */
                          /* batching; default 64                            */
   int32_t small_lanes;   /* lanes that admit only requests under 65,536     */
-                         /* rows (of max_inflight); < 0 (default): a       */
-                         /* quarter of the lanes when there are 4 or more  */
-  int32_t reserved[2];
+                         /* rows (of max_inflight); default 0              */
+  int32_t admission;     /* 0: oldest request first (first fit);           */
+                         /* 1: smallest scan (n^2 d) first; both let a     */
+                         /* request passed over 16 times go next           */
+  int32_t reserved[1];
 } evoc_gpu_server_opts;
 
 typedef struct {

@@ -65,9 +65,10 @@ def alone():
     return out
 
 
-@pytest.mark.parametrize("lanes", [1, 4])
-def test_same_result_alone_and_in_the_mix(alone, lanes):
-    with Server(max_inflight=lanes) as srv:
+@pytest.mark.parametrize("lanes,admission,small_lanes", [(1, "oldest", 0), (4, "oldest", 0), (4, "smallest", 0),
+                                                         (4, "smallest", 2)])
+def test_same_result_alone_and_in_the_mix(alone, lanes, admission, small_lanes):
+    with Server(max_inflight=lanes, admission=admission, small_lanes=small_lanes) as srv:
         jobs = []
         for rep in range(2):  # every request twice, interleaved
             for (form, _, k), (x, _, _) in zip(MIX, alone):
