@@ -108,12 +108,12 @@ def _forced_graph(tmp_path, monkeypatch, x, kind, form, k, variant, **opt):
         monkeypatch.delenv("EVOC_TUNE_CACHE")
 
 
-@pytest.mark.parametrize("variant", [6, 7, 8, 9])
+@pytest.mark.parametrize("variant", [6, 7, 8, 9, 10, 11])
 @pytest.mark.parametrize("n", [2900, 300, 129])
 def test_cta_pair_variants_match_single_cta(tmp_path, monkeypatch, variant, n):
-    """The CTA-pair scans (cluster of two, M = 256 MMAs) give the single-CTA graph bit for bit, with an
-    odd number of query blocks (the last pair half empty), a single block, and a row slice starting
-    mid-block."""
+    """The CTA-pair scans (cluster of two, M = 256 MMAs; variants 6-9) and the four-epilogue-group
+    scans (10, 11) give the default graph bit for bit, with an odd number of query blocks (the last
+    pair half empty), a single block, and a row slice starting mid-block."""
     x = _f32(n, 96, 7)
     base = evoc.knn_graph(x, evoc.KnnGraphOptions(n_neighbors=15, form="bf16_rerank"))
     ind, dst = _forced_graph(tmp_path, monkeypatch, x, "Float32", "bf16_rerank", 15, variant)
