@@ -612,7 +612,8 @@ def exact_int_leg(workload, n, d, k, dev, local, rank, world, pg, steps, warmup,
                    "l2": f"inputs larger than L2 ({x.numel() / 1e9:.2f} GB vs 126 MB)",
                    "per_rank": "independent graph per rank"},
         "sampled_exact_check": check,
-        "autotune": tuned and {"variants_ms_65536_rows": tuned["variants_ms"], "chosen": tuned["chosen"]},
+        "autotune": tuned and {"sample_rows": min(n, 262144 if n >= 1_000_000 else 65536),
+                               "variants_ms": tuned["variants_ms"], "chosen": tuned["chosen"]},
         "stages_ms": {kname: statistics.mean(v) for kname, v in stage_ms.items()},
         "roofline": roofline,
         "e2e": {"value": world * n * k / (e2e_ms / 1000.0), "unit": UNIT, "h2d_bytes_per_step": int(x.numel()),
@@ -1161,7 +1162,8 @@ def run_ours(args, world, rank, local):
                 "ms_per_step": e2e_ms, "matches_device_path": e2e_consistent},
         "fp32_form": fp32,
         "fuzzy_graph": fuzzy,
-        "autotune": tuned and {"variants_ms_65536_rows": tuned["variants_ms"], "chosen": tuned["chosen"]},
+        "autotune": tuned and {"sample_rows": min(n, 262144 if n >= 1_000_000 else 65536),
+                               "variants_ms": tuned["variants_ms"], "chosen": tuned["chosen"]},
         "cpu_baseline": cpu,
         "cpu_baseline_deterministic": cpu_det,
         "certificate": cert and dict(cert, note=(
@@ -1353,7 +1355,8 @@ def run_case(args):
         od = torch.empty((rows, k), dtype=torch.float32, device=dev)
         form = {"scan": "bf16_rerank", "fp32": "fp32", "nnd": "nndescent"}[args.case]
         kw = {"row_begin": 0, "row_end": rows} if args.case == "fp32" else {}
-        o = evoc.KnnGraphOptions(n_neighbors=k, form=form, device=0, scan_type=args.scan_type, **kw)
+        o = evoc.KnnGraphOptions(n_neighbors=k, form=form, device=0, scan_type=args.scan_type,
+                                 oversample=args.oversample, **kw)
         for _ in range(2):
             evoc.knn_graph_device(x.data_ptr(), 0, n, dim, k, oi.data_ptr(), od.data_ptr(), o)
         st = ctx.stages()
@@ -1367,6 +1370,7 @@ def run_case(args):
         if args.case == "scan":
             out["certificate"] = ctx.certify_counts()
             out["scan_type"] = args.scan_type
+            out["oversample"] = args.oversample
         if args.case == "fp32":
             out["tflops_fp32"] = 2.0 * rows * n * dim / (out["stages_ms"]["fp32_scan"] / 1e3) / 1e12
     torch.cuda.synchronize()
@@ -1422,6 +1426,8 @@ def main():
     ap.add_argument("--case", default=None, choices=["scan", "fp32", "nnd", "mst", "serve"],
                     help="run one small case of a kernel (timings, ncu captures) instead of the bench")
     ap.add_argument("--scan-type", default="fp16", choices=["fp16", "bf16"], help="operands of --case scan")
+    ap.add_argument("--oversample", type=int, default=0,
+                    help="--case scan: candidates per row = oversample * k (0: ceil(2.5 k))")
     args = ap.parse_args()
     if args.case:
         return run_case(args)  # --n / --dim / --k: the case's own defaults when not given

@@ -1333,9 +1333,12 @@ int autotune_impl(evoc_gpu_ctx* ctx, int32_t dtype, int32_t form_in, int64_t n, 
     return fail(ctx, EVOC_ERR_UNSUPPORTED, "only the tensor-core forms (BF16+rerank, exact int8 / binary) are tuned");
   }
   EVOC_TRY(cudaSetDevice(ctx->device), "cudaSetDevice");
-  // Synthetic rows of the request's shape; a sample of up to 65,536 rows is
-  // enough to rank the variants (their cost per (query, key) pair).
-  const int64_t nt = std::min<int64_t>(n, 65536);
+  // Synthetic rows of the request's shape: a sample that ranks the variants
+  // by their cost per (query, key) pair.  65,536 rows, or 262,144 for
+  // requests of a million rows and more: the share of the epilogue's heap
+  // inserts falls as n grows, so a small sample over-rewards epilogue warps
+  // at the expense of pipeline stages.
+  const int64_t nt = std::min<int64_t>(n, n >= 1000000 ? 262144 : 65536);
   const int64_t rows = evoc::padded_rows(nt);
   EVOC_TRY(ctx->xb.ensure(size_t(rows * row_bytes)), "alloc tuning rows");
   const int32_t* pc = nullptr;

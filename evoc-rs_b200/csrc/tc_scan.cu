@@ -707,7 +707,8 @@ cudaError_t launch_pair(const CUtensorMap& ma, const CUtensorMap& mb, const Scan
 // epilogue warp groups, heaps in shared (1) or global (0) memory, CTA pair (1).
 constexpr int kVariantCfg[kScanVariants][4] = {{4, 2, 1, 0}, {3, 2, 1, 0}, {4, 1, 1, 0}, {3, 1, 1, 0},
                                                {4, 1, 0, 0}, {2, 2, 1, 0}, {4, 2, 1, 1}, {4, 1, 1, 1},
-                                               {6, 1, 1, 1}, {3, 2, 1, 1}, {3, 4, 1, 0}, {2, 4, 1, 0}};
+                                               {6, 1, 1, 1}, {3, 2, 1, 1}, {3, 4, 1, 0}, {2, 4, 1, 0},
+                                               {5, 1, 1, 1}};
 
 bool variant_feasible(int v, int keep, bool has_scratch) {
   if (v < 0 || v >= kScanVariants) return false;
@@ -732,6 +733,7 @@ cudaError_t launch_forced(const CUtensorMap& ma, const CUtensorMap& mb, ScanPara
     case 9: return launch_pair<MODE, 3, 2>(ma, mb, p, grid, smem_bytes(3, 2, odd, true), stream);
     case 10: return launch_variant<MODE, 3, 4, true>(ma, mb, p, grid, smem_bytes(3, 4, odd), stream);
     case 11: return launch_variant<MODE, 2, 4, true>(ma, mb, p, grid, smem_bytes(2, 4, odd), stream);
+    case 12: return launch_pair<MODE, 5, 1>(ma, mb, p, grid, smem_bytes(5, 1, odd, true), stream);
     default:
       p.heap_stride = p.keep;
       return launch_variant<MODE, 4, 1, false>(ma, mb, p, grid, smem_bytes(4, 1, 0), stream);
@@ -834,7 +836,8 @@ const char* tc_scan_variant_name(int variant) {
                                              "CTA pair, 6 stages, 1 epilogue group, shared-memory heaps",
                                              "CTA pair, 3 stages, 2 epilogue groups, shared-memory heaps",
                                              "3 stages, 4 epilogue groups, shared-memory heaps",
-                                             "2 stages, 4 epilogue groups, shared-memory heaps"};
+                                             "2 stages, 4 epilogue groups, shared-memory heaps",
+                                             "CTA pair, 5 stages, 1 epilogue group, shared-memory heaps"};
   return variant >= 0 && variant < kScanVariants ? names[variant] : "automatic";
 }
 
