@@ -708,7 +708,7 @@ cudaError_t launch_pair(const CUtensorMap& ma, const CUtensorMap& mb, const Scan
 constexpr int kVariantCfg[kScanVariants][4] = {{4, 2, 1, 0}, {3, 2, 1, 0}, {4, 1, 1, 0}, {3, 1, 1, 0},
                                                {4, 1, 0, 0}, {2, 2, 1, 0}, {4, 2, 1, 1}, {4, 1, 1, 1},
                                                {6, 1, 1, 1}, {3, 2, 1, 1}, {3, 4, 1, 0}, {2, 4, 1, 0},
-                                               {5, 1, 1, 1}};
+                                               {5, 1, 1, 1}, {2, 2, 1, 1}};
 
 bool variant_feasible(int v, int keep, bool has_scratch) {
   if (v < 0 || v >= kScanVariants) return false;
@@ -734,6 +734,7 @@ cudaError_t launch_forced(const CUtensorMap& ma, const CUtensorMap& mb, ScanPara
     case 10: return launch_variant<MODE, 3, 4, true>(ma, mb, p, grid, smem_bytes(3, 4, odd), stream);
     case 11: return launch_variant<MODE, 2, 4, true>(ma, mb, p, grid, smem_bytes(2, 4, odd), stream);
     case 12: return launch_pair<MODE, 5, 1>(ma, mb, p, grid, smem_bytes(5, 1, odd, true), stream);
+    case 13: return launch_pair<MODE, 2, 2>(ma, mb, p, grid, smem_bytes(2, 2, odd, true), stream);
     default:
       p.heap_stride = p.keep;
       return launch_variant<MODE, 4, 1, false>(ma, mb, p, grid, smem_bytes(4, 1, 0), stream);
@@ -837,7 +838,8 @@ const char* tc_scan_variant_name(int variant) {
                                              "CTA pair, 3 stages, 2 epilogue groups, shared-memory heaps",
                                              "3 stages, 4 epilogue groups, shared-memory heaps",
                                              "2 stages, 4 epilogue groups, shared-memory heaps",
-                                             "CTA pair, 5 stages, 1 epilogue group, shared-memory heaps"};
+                                             "CTA pair, 5 stages, 1 epilogue group, shared-memory heaps",
+                                             "CTA pair, 2 stages, 2 epilogue groups, shared-memory heaps"};
   return variant >= 0 && variant < kScanVariants ? names[variant] : "automatic";
 }
 

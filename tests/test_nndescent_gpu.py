@@ -144,3 +144,25 @@ def test_nndescent_large_k_takes_the_exact_form():
     a = evoc.knn_graph(xi, nnd(70), np.random.RandomState(0))
     b = evoc.knn_graph(xi, evoc.KnnGraphOptions(n_neighbors=70, form="exact_int"))
     assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+def test_nndescent_f32_recall_at_60k_rows():
+    """A larger graph (60,000 rows of 40 overlapping clusters, k = 20): recall against the exact
+    graph (the FP32 form, itself held to the oracle) above a floor, and on the first 10,000 rows at
+    least the reference NN-descent's there (the oracle's restatement), less 0.02."""
+    rng = np.random.default_rng(17)
+    d, k = 48, 20
+    c = rng.standard_normal((40, d))
+    x = (c[rng.integers(0, 40, 60000)] + 0.6 * rng.standard_normal((60000, d))).astype(np.float32)
+    x /= np.linalg.norm(x, axis=1, keepdims=True)
+    ind, _ = evoc.knn_graph(x, nnd(k), np.random.RandomState(4))
+    ei, _ = evoc.knn_graph(x, evoc.KnnGraphOptions(n_neighbors=k, form="fp32"))
+    rec = _recall(ind, ei)
+    xs = x[:10000]
+    ref_ind, _ = O.knn_graph(xs, k, O.RandomState(4), deterministic=False, n_threads=8)
+    es, _ = O.exact_knn(xs, k)
+    ref_rec = _recall(ref_ind, es)
+    sub, _ = evoc.knn_graph(xs, nnd(k), np.random.RandomState(4))
+    print(f"GPU NN-descent recall {rec:.4f} (60,000 rows), {_recall(sub, es):.4f} (10,000); "
+          f"reference {ref_rec:.4f} (10,000)")
+    assert rec >= 0.8 and _recall(sub, es) >= ref_rec - 0.02

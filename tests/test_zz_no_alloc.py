@@ -73,6 +73,31 @@ def test_noalloc_matches_regular_entry_point_on_two_calls():
         assert np.all(gi[:, 0] == np.arange(n))
 
 
+def test_noalloc_matches_the_oracle():
+    """Directly against the oracle's exact FP32 selection (not only through the regular entry point):
+    indices equal except ties within 1e-6, raw values held to FP64 truth within 1e-6."""
+    import torch
+
+    from oracle import oracle as O
+
+    f = _noalloc()
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    n, d, k = 1200, 48, 12
+    x = _rows(n, d, 9)
+    oi, od = _run(f, torch.from_numpy(x).cuda(), n, d, k, stream)
+    torch.cuda.synchronize()
+    gi, gd = oi.cpu().numpy(), od.cpu().numpy()
+    ei, er = O.exact_knn(x, k)
+    x64 = x.astype(np.float64)
+    dots = np.einsum("rkd,rd->rk", x64[gi], x64)
+    want = np.where(dots > 0, -dots, 1.17549435e-38)  # FP64 raw of the pairs the GPU returned
+    want[gi == np.arange(n)[:, None]] = -1.0
+    diff = gi != ei
+    assert np.all(np.abs(want[diff] - er[diff]) <= 1e-6)  # a differing entry ties the oracle's
+    assert diff.sum() <= max(8, 0.01 * gi.size)
+    assert np.allclose(gd, O.transform(O.DT_F32, want.astype(np.float32)), atol=1e-5)
+
+
 def test_noalloc_rejects_sizes_beyond_its_scratch():
     import torch
 
