@@ -1389,7 +1389,9 @@ def main():
     ap.add_argument("--dim", type=int, default=None, help="features (f32, i8) or bytes per row (bits)")
     ap.add_argument("--k", type=int, default=None)
     ap.add_argument("--check-rows", type=int, default=128)
-    ap.add_argument("--autotune", type=int, default=1, help="tune the scan's kernel variant before timing")
+    ap.add_argument("--autotune", type=int, default=0,
+                    help="tune the scan's kernel variant before timing (default: the library's automatic "
+                         "choice, which encodes full-size measurements the short tuning runs do not reproduce)")
     ap.add_argument("--form", default="bf16_rerank", choices=["bf16_rerank", "nndescent"],
                     help="zipf_f32 workload: the exact BF16+rerank form (headline) or GPU NN-descent")
     ap.add_argument("--fuzzy", type=int, default=1, help="time the fuzzy graph of the built graph")

@@ -1368,11 +1368,9 @@ int autotune_impl(evoc_gpu_ctx* ctx, int32_t dtype, int32_t form_in, int64_t n, 
   EVOC_TRY(cudaEventCreate(&e0), "event");
   EVOC_TRY(cudaEventCreate(&e1), "event");
   std::string rep;
-  // The automatic choice (first that fits) stays unless another variant is
-  // clearly faster: timings within a few percent are noise at this sample size.
-  int automatic = -1;
-  for (int v = 0; v <= 4 && automatic < 0; v++)
-    if (evoc::tc_scan_variant_feasible(v, keep, v == 4)) automatic = v;
+  // The automatic choice stays unless another variant is clearly faster:
+  // timings within a few percent are noise at this sample size.
+  const int automatic = evoc::tc_scan_automatic_variant(mode, keep);
   std::vector<float> times(evoc::kScanVariants, -1.0f);
   for (int v = 0; v < evoc::kScanVariants; v++) {
     if (!evoc::tc_scan_variant_feasible(v, keep, true)) continue;

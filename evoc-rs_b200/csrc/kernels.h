@@ -90,6 +90,8 @@ constexpr int kScanVariants = 14;
 bool tc_scan_variant_feasible(int variant, int keep, bool has_scratch);
 // Whether a launch with this variant (-1: automatic) and keep keeps its heaps in global scratch.
 bool tc_scan_uses_global_heaps(int variant, int keep);
+// The variant an automatic (-1) launch of this mode and keep takes.
+int tc_scan_automatic_variant(int mode, int keep);
 const char* tc_scan_variant_name(int variant);
 // prep.cu: synthetic rows for the autotuner (mode 0: FP16 values in [-1, 1];
 // 1: int8; 2: packed bits, about 1 in 8 set), zero past n rows / `bytes` bytes.

@@ -748,8 +748,17 @@ cudaError_t launch_mode(const CUtensorMap& ma, const CUtensorMap& mb, ScanParams
     return launch_forced<MODE>(ma, mb, p, grid, variant, stream);
   const int odd = p.keep | 1;
   p.heap_stride = odd;
-  // Prefer two epilogue groups (more warps to hide TMEM/issue latency), then
-  // the deeper pipeline; heaps fall back to global memory for very large keep.
+  // int8 dot products with small keep: four epilogue groups.  Measured at
+  // full size (2M x 384, k = 15), they beat two groups by 18 %: the scan is
+  // epilogue-paced and the wider epilogue also draws less power, so the
+  // clocks under the power cap rise (1,642 vs 1,125 MHz).  Short tuning runs
+  // do not see that, so it is the automatic choice rather than the tuner's.
+  if (MODE == kModeInt8 && smem_bytes(3, 4, odd) <= SMEM_LIMIT)
+    return launch_variant<MODE, 3, 4, true>(ma, mb, p, grid, smem_bytes(3, 4, odd), stream);
+  // Otherwise prefer two epilogue groups (more warps to hide TMEM/issue
+  // latency), then the deeper pipeline; heaps fall back to global memory for
+  // very large keep.  (Jaccard at 4M x 1,024 bits: two groups with four
+  // stages beat four groups with three by 8 % at full size.)
   if (smem_bytes(4, 2, odd) <= SMEM_LIMIT)
     return launch_variant<MODE, 4, 2, true>(ma, mb, p, grid, smem_bytes(4, 2, odd), stream);
   if (smem_bytes(3, 2, odd) <= SMEM_LIMIT)
@@ -823,6 +832,16 @@ bool tc_scan_variant_feasible(int variant, int keep, bool has_scratch) {
 bool tc_scan_uses_global_heaps(int variant, int keep) {
   if (variant >= 0 && variant_feasible(variant, keep, true)) return kVariantCfg[variant][2] == 0;
   return smem_bytes(3, 1, keep | 1) > SMEM_LIMIT;  // the automatic choice: no shared-memory variant fits
+}
+
+int tc_scan_automatic_variant(int mode, int keep) {
+  const int odd = keep | 1;
+  if (mode == kModeInt8 && smem_bytes(3, 4, odd) <= SMEM_LIMIT) return 10;
+  if (smem_bytes(4, 2, odd) <= SMEM_LIMIT) return 0;
+  if (smem_bytes(3, 2, odd) <= SMEM_LIMIT) return 1;
+  if (smem_bytes(4, 1, odd) <= SMEM_LIMIT) return 2;
+  if (smem_bytes(3, 1, odd) <= SMEM_LIMIT) return 3;
+  return 4;
 }
 
 const char* tc_scan_variant_name(int variant) {
