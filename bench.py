@@ -70,6 +70,11 @@ WORKLOADS = {
 # key rows are re-streamed once per wave of query blocks, so traffic grows
 # with n^2).
 SCAN_TRAFFIC_BYTES_262K = 6_392_895_864
+# The same for the int8 scan (gmm_i8 rows, d = 384, keep 15, 3 stages, 4
+# epilogue groups): 1.380e9 B at n = 262,144, scaled by n^2.  The Jaccard scan
+# has no such figure: its 262,144-row capture (130 GB, twice L2 in keys) is
+# not a proxy for 4M rows, and a full-size capture is beyond ncu's limits here.
+I8_TRAFFIC_BYTES_262K = 1_379_694_592
 
 
 def scan_traffic(n):
@@ -579,7 +584,9 @@ def exact_int_leg(workload, n, d, k, dev, local, rank, world, pg, steps, warmup,
     scan_ms = statistics.mean(stage_ms[stage])
     achieved = ops_per_pair * n * n / (scan_ms / 1000.0) / 1e12
     roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TOPS (int8)", "frac": achieved / peak,
-                "traffic": None, "kernel": f"tc_scan_kernel ({'int8' if i8 else 'Jaccard on 0/1 int8'}, fused top-k)",
+                "traffic": I8_TRAFFIC_BYTES_262K * (n / 262144.0) ** 2 if i8 else None,
+                "traffic_unit": "bytes per launch (ncu at 262,144 rows, scaled by n^2)" if i8 else None,
+                "kernel": f"tc_scan_kernel ({'int8' if i8 else 'Jaccard on 0/1 int8'}, fused top-k)",
                 "peak_kind": peak_kind, "peak_burst": peak_burst, "frac_of_burst": achieved / peak_burst,
                 "launch_ms": scan_ms, "ops_per_launch": ops_per_pair * n * n}
 
