@@ -150,20 +150,58 @@ __device__ __forceinline__ float jaccard_raw_counts(int32_t inter, int32_t uni) 
   return uni > 0 ? -__fdiv_rn(__int2float_rn(inter), __int2float_rn(uni)) : 0.0f;
 }
 
+// Survivors waiting for the heap: a thread's pass check stays against its
+// heap root while up to kPend survivor keys wait in registers; they go into
+// the heap when the buffer fills, and otherwise after the tile's accumulator
+// has been released to the MMA.  A warp's rows then mostly insert together
+// (lanes in step) instead of one lane at a time inside the chunk loop, where
+// a survivor in any of the 32 rows held the whole warp and with it the
+// accumulator the next tile needs.  Keys are unique, so the heap ends with
+// the same top-C whatever the order of the inserts.
+// Eight keys, or four in the 576-thread four-group variants (their register
+// budget is 112 per thread).
+template <int P>
+struct Pending {
+  uint64_t k[P];
+  int n;
+};
+
+template <int MODE, int P>
+__device__ __forceinline__ void flush_pending(Pending<P>& pend, KeyHeap& heap, uint32_t& thr, int32_t pa) {
+#pragma unroll
+  for (int i = 0; i < P; i++)
+    if (i < pend.n) heap.offer(pend.k[i]);
+  if (pend.n) thr = pass_threshold<MODE>(heap, pa);
+  pend.n = 0;
+}
+
+// Column j of a chunk's 32 values: a five-level select tree (31 selects,
+// dependency depth 5) instead of a 32-deep chain.
+__device__ __forceinline__ uint32_t pick(const uint32_t (&v)[32], int j) {
+  uint32_t s[16];
+#pragma unroll
+  for (int i = 0; i < 16; i++) s[i] = (j & 16) ? v[i + 16] : v[i];
+#pragma unroll
+  for (int i = 0; i < 8; i++) s[i] = (j & 8) ? s[i + 8] : s[i];
+#pragma unroll
+  for (int i = 0; i < 4; i++) s[i] = (j & 4) ? s[i + 4] : s[i];
+#pragma unroll
+  for (int i = 0; i < 2; i++) s[i] = (j & 2) ? s[i + 2] : s[i];
+  return (j & 1) ? s[1] : s[0];
+}
+
 // Offers the scores of one 32-column chunk that beat the threshold.  The
-// chunk's values stay in registers; a survivor's value is picked by an
-// unrolled select (survivors are rare once the heap is full).  Bit 31 - j of
-// `mask` stands for column j (the order chunk_mask builds).
-template <int MODE>
+// chunk's values stay in registers; a survivor's value is picked by a select
+// tree (survivors are rare once the heap is full).  Bit 31 - j of `mask`
+// stands for column j (the order chunk_mask builds).
+template <int MODE, int P>
 __device__ __forceinline__ void offer_chunk(const uint32_t (&v)[32], uint32_t mask, int64_t col0, int64_t n_k,
                                             bool self_mode, int64_t q, KeyHeap& heap, uint32_t& thr, int32_t pa,
-                                            const int32_t* __restrict__ pc) {
+                                            const int32_t* __restrict__ pc, Pending<P>& pend) {
   while (mask) {
     const int j = __clz(mask);
     mask &= ~(0x80000000u >> j);
-    uint32_t bits = 0;
-#pragma unroll
-    for (int jj = 0; jj < 32; jj++) bits = (jj == j) ? v[jj] : bits;
+    const uint32_t bits = pick(v, j);
     if (!passes<MODE>(bits, thr)) continue;  // threshold may have moved
     const int64_t key = col0 + j;
     if (key >= n_k || (self_mode && key == q)) continue;
@@ -174,8 +212,11 @@ __device__ __forceinline__ void offer_chunk(const uint32_t (&v)[32], uint32_t ma
     } else {
       raw = MODE == kModeInt8 ? -__int2float_rn(int32_t(bits)) : raw_cosine(__uint_as_float(bits));
     }
-    heap.offer(make_key(raw, int32_t(key)));
-    thr = pass_threshold<MODE>(heap, pa);
+    const uint64_t kk = make_key(raw, int32_t(key));
+#pragma unroll
+    for (int i = 0; i < P; i++)
+      if (i == pend.n) pend.k[i] = kk;
+    if (++pend.n == P) flush_pending<MODE>(pend, heap, thr, pa);
   }
 }
 
@@ -514,6 +555,8 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
       if (valid && v.self_mode && group == 0) heap.offer(make_key(-1.0f, int32_t(qg)));
       const int32_t pa = (MODE == kModeJaccard && valid) ? v.pc[qg] : 0;
       uint32_t thr = pass_threshold<MODE>(heap, pa);
+      Pending<(GROUPS >= 4 ? 4 : 8)> pend;
+      pend.n = 0;
       for (int64_t kt = 0; kt < v.n_ktiles; kt++, tile++) {
         const uint32_t a = tile & 1u, tph = (tile >> 1) & 1u;
         int got = 1;
@@ -535,19 +578,21 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
           tmem_ld_32x32b_x32(tbase + (c + 1) * 32, vb);
           if (valid && chunk_any<MODE>(va, thr)) {
             const uint32_t m = chunk_mask<MODE>(va, thr);
-            offer_chunk<MODE>(va, m, k0 + c * 32, v.n_k, v.self_mode, qg, heap, thr, pa, v.pc);
+            offer_chunk<MODE>(va, m, k0 + c * 32, v.n_k, v.self_mode, qg, heap, thr, pa, v.pc, pend);
           }
           tmem_ld_wait();
           if (c + 2 < NCH) tmem_ld_32x32b_x32(tbase + (c + 2) * 32, va);
           if (valid && chunk_any<MODE>(vb, thr)) {
             const uint32_t m = chunk_mask<MODE>(vb, thr);
-            offer_chunk<MODE>(vb, m, k0 + (c + 1) * 32, v.n_k, v.self_mode, qg, heap, thr, pa, v.pc);
+            offer_chunk<MODE>(vb, m, k0 + (c + 1) * 32, v.n_k, v.self_mode, qg, heap, thr, pa, v.pc, pend);
           }
         }
         tc_fence_before();
         if (kPair && !leader) mbar_arrive_cluster(a ? tempty_c1 : tempty_c0);
         else mbar_arrive(&tempty[a]);
+        flush_pending<MODE>(pend, heap, thr, pa);  // the accumulator is already the MMA's again
       }
+      flush_pending<MODE>(pend, heap, thr, pa);
       if (GROUPS > 1) ok = epilogue_vote(GROUPS * 128, ok);
       if (!ok) break;
       if (GROUPS > 1) {
