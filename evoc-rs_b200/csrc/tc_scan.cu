@@ -150,31 +150,6 @@ __device__ __forceinline__ float jaccard_raw_counts(int32_t inter, int32_t uni) 
   return uni > 0 ? -__fdiv_rn(__int2float_rn(inter), __int2float_rn(uni)) : 0.0f;
 }
 
-// Survivors waiting for the heap: a thread's pass check stays against its
-// heap root while up to kPend survivor keys wait in registers; they go into
-// the heap when the buffer fills, and otherwise after the tile's accumulator
-// has been released to the MMA.  A warp's rows then mostly insert together
-// (lanes in step) instead of one lane at a time inside the chunk loop, where
-// a survivor in any of the 32 rows held the whole warp and with it the
-// accumulator the next tile needs.  Keys are unique, so the heap ends with
-// the same top-C whatever the order of the inserts.
-// Eight keys, or four in the 576-thread four-group variants (their register
-// budget is 112 per thread).
-template <int P>
-struct Pending {
-  uint64_t k[P];
-  int n;
-};
-
-template <int MODE, int P>
-__device__ __forceinline__ void flush_pending(Pending<P>& pend, KeyHeap& heap, uint32_t& thr, int32_t pa) {
-#pragma unroll
-  for (int i = 0; i < P; i++)
-    if (i < pend.n) heap.offer(pend.k[i]);
-  if (pend.n) thr = pass_threshold<MODE>(heap, pa);
-  pend.n = 0;
-}
-
 // Column j of a chunk's 32 values: a five-level select tree (31 selects,
 // dependency depth 5) instead of a 32-deep chain.
 __device__ __forceinline__ uint32_t pick(const uint32_t (&v)[32], int j) {
@@ -194,10 +169,10 @@ __device__ __forceinline__ uint32_t pick(const uint32_t (&v)[32], int j) {
 // chunk's values stay in registers; a survivor's value is picked by a select
 // tree (survivors are rare once the heap is full).  Bit 31 - j of `mask`
 // stands for column j (the order chunk_mask builds).
-template <int MODE, int P>
+template <int MODE>
 __device__ __forceinline__ void offer_chunk(const uint32_t (&v)[32], uint32_t mask, int64_t col0, int64_t n_k,
                                             bool self_mode, int64_t q, KeyHeap& heap, uint32_t& thr, int32_t pa,
-                                            const int32_t* __restrict__ pc, Pending<P>& pend) {
+                                            const int32_t* __restrict__ pc) {
   while (mask) {
     const int j = __clz(mask);
     mask &= ~(0x80000000u >> j);
@@ -212,11 +187,8 @@ __device__ __forceinline__ void offer_chunk(const uint32_t (&v)[32], uint32_t ma
     } else {
       raw = MODE == kModeInt8 ? -__int2float_rn(int32_t(bits)) : raw_cosine(__uint_as_float(bits));
     }
-    const uint64_t kk = make_key(raw, int32_t(key));
-#pragma unroll
-    for (int i = 0; i < P; i++)
-      if (i == pend.n) pend.k[i] = kk;
-    if (++pend.n == P) flush_pending<MODE>(pend, heap, thr, pa);
+    heap.offer(make_key(raw, int32_t(key)));
+    thr = pass_threshold<MODE>(heap, pa);
   }
 }
 
@@ -225,24 +197,29 @@ __device__ __forceinline__ void offer_chunk(const uint32_t (&v)[32], uint32_t ma
 // f32 subtraction on the FMA pipe for BF16 -- is funnel-shifted into one of
 // four independent accumulators (short dependency chains), then inverted.
 // Equal scores pass (their difference is +0), as `passes` admits them.
-// Whether any score of the chunk passes: a max tree (one min/max instruction
-// per score, independent at each level) and one compare.  Once a row's heap
-// is full most chunks fail here and skip the per-column mask.  Not for
-// Jaccard: its intersection bound is loose enough that the pre-check passes
-// too often to pay for itself.
+// Largest of 32 signed integers by three-input max (16 instructions).
+__device__ __forceinline__ int32_t max32_s32(const uint32_t (&v)[32]) {
+  int32_t m[11];
+#pragma unroll
+  for (int i = 0; i < 10; i++) m[i] = __vimax3_s32(int32_t(v[3 * i]), int32_t(v[3 * i + 1]), int32_t(v[3 * i + 2]));
+  m[10] = max(int32_t(v[30]), int32_t(v[31]));
+  const int32_t a = __vimax3_s32(m[0], m[1], m[2]), b = __vimax3_s32(m[3], m[4], m[5]),
+                c = __vimax3_s32(m[6], m[7], m[8]), d = max(m[9], m[10]);
+  return max(__vimax3_s32(a, b, c), d);
+}
+
+// Whether any score of the chunk passes: a max tree (independent at each
+// level) and one compare.  Once a row's heap is full most chunks fail here
+// and skip the per-column mask.  Not for Jaccard: its intersection bound is
+// loose enough that the pre-check passes too often to pay for itself.
 template <int MODE>
 __device__ __forceinline__ bool chunk_any(const uint32_t (&v)[32], uint32_t thr) {
   if (MODE == kModeJaccard) return true;
-  if (MODE != kModeHalf) {
-    int32_t m[16];
-#pragma unroll
-    for (int j = 0; j < 16; j++) m[j] = max(int32_t(v[j]), int32_t(v[j + 16]));
-#pragma unroll
-    for (int w = 8; w > 0; w >>= 1)
-#pragma unroll
-      for (int j = 0; j < w; j++) m[j] = max(m[j], m[j + w]);
-    return m[0] >= int32_t(thr);
-  }
+  if (MODE != kModeHalf) return max32_s32(v) >= int32_t(thr);
+  // 16-bit float scores: against a positive threshold the bit patterns as
+  // signed integers order as the floats do (a negative score is a negative
+  // integer, below any positive threshold), so the integer max tree serves.
+  if (int32_t(thr) > 0) return max32_s32(v) >= int32_t(thr);
   float m[16];
 #pragma unroll
   for (int j = 0; j < 16; j++) m[j] = fmaxf(__uint_as_float(v[j]), __uint_as_float(v[j + 16]));
@@ -555,8 +532,6 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
       if (valid && v.self_mode && group == 0) heap.offer(make_key(-1.0f, int32_t(qg)));
       const int32_t pa = (MODE == kModeJaccard && valid) ? v.pc[qg] : 0;
       uint32_t thr = pass_threshold<MODE>(heap, pa);
-      Pending<(GROUPS >= 4 ? 4 : 8)> pend;
-      pend.n = 0;
       for (int64_t kt = 0; kt < v.n_ktiles; kt++, tile++) {
         const uint32_t a = tile & 1u, tph = (tile >> 1) & 1u;
         int got = 1;
@@ -578,21 +553,19 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
           tmem_ld_32x32b_x32(tbase + (c + 1) * 32, vb);
           if (valid && chunk_any<MODE>(va, thr)) {
             const uint32_t m = chunk_mask<MODE>(va, thr);
-            offer_chunk<MODE>(va, m, k0 + c * 32, v.n_k, v.self_mode, qg, heap, thr, pa, v.pc, pend);
+            offer_chunk<MODE>(va, m, k0 + c * 32, v.n_k, v.self_mode, qg, heap, thr, pa, v.pc);
           }
           tmem_ld_wait();
           if (c + 2 < NCH) tmem_ld_32x32b_x32(tbase + (c + 2) * 32, va);
           if (valid && chunk_any<MODE>(vb, thr)) {
             const uint32_t m = chunk_mask<MODE>(vb, thr);
-            offer_chunk<MODE>(vb, m, k0 + (c + 1) * 32, v.n_k, v.self_mode, qg, heap, thr, pa, v.pc, pend);
+            offer_chunk<MODE>(vb, m, k0 + (c + 1) * 32, v.n_k, v.self_mode, qg, heap, thr, pa, v.pc);
           }
         }
         tc_fence_before();
         if (kPair && !leader) mbar_arrive_cluster(a ? tempty_c1 : tempty_c0);
         else mbar_arrive(&tempty[a]);
-        flush_pending<MODE>(pend, heap, thr, pa);  // the accumulator is already the MMA's again
       }
-      flush_pending<MODE>(pend, heap, thr, pa);
       if (GROUPS > 1) ok = epilogue_vote(GROUPS * 128, ok);
       if (!ok) break;
       if (GROUPS > 1) {
