@@ -646,7 +646,7 @@ def run_exact_int(args, world, rank, local):
 
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
         pg = dist
     line = exact_int_leg(args.workload, args.n, args.dim, args.k, dev, local, rank, world, pg, args.steps,
                          args.warmup, args.e2e_steps, args.check_rows, args.cpu_rows, bool(args.autotune))
@@ -950,7 +950,7 @@ def run_ours(args, world, rank, local):
 
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
         pg = dist
     n, d, k = args.n, args.dim, args.k
     x = synthetic.zipf_f32(n=n, dim=d, seed=7 + rank, device=dev)
@@ -1222,7 +1222,7 @@ def run_shard(args, world, rank, local):
     if world > 1:
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
         pg = dist
     n, d, k = args.n, args.dim, args.k
     x = synthetic.zipf_f32(n=n, dim=d, seed=7, device=dev)  # the same rows on every rank
