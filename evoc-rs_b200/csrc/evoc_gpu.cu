@@ -174,10 +174,14 @@ int locality_order(evoc_gpu_ctx* ctx, const Job& j, const void* rows, int64_t ro
 // query blocks, one wave of the scan).
 constexpr int64_t kRepairChunk = 16384;
 
-// Candidates kept per row by the 16-bit scan: oversample * k (automatic:
-// ceil(2.5 k)), within [k, n].
+// Candidates kept per row by the 16-bit scan: oversample * k; automatic:
+// 2k from 500,000 rows (the scan's epilogue costs grow with the kept count,
+// and the few rows that then fail the certificate are rescanned cheaply),
+// ceil(2.5 k) below (fewer rescans, which small requests cannot amortise);
+// within [k, n].
 int64_t bf16_candidates(const evoc_gpu_opts& opts, int64_t n, int keff) {
-  int64_t C = opts.oversample > 0 ? int64_t(opts.oversample) * keff : (int64_t(5) * keff + 1) / 2;
+  int64_t C = opts.oversample > 0 ? int64_t(opts.oversample) * keff
+              : (n >= 500000 ? int64_t(2) * keff : (int64_t(5) * keff + 1) / 2);
   if (C > n) C = n;
   if (C < keff) C = keff;
   return C;
@@ -234,8 +238,10 @@ RepairLayout repair_layout(int64_t nq, int64_t ld, int64_t ldb, int64_t C2, int6
   return L;
 }
 
-// Candidates of the second certificate pass: 256 (the rerank's limit), at most n.
-int64_t second_pass_candidates(int64_t n) { return std::min<int64_t>(256, n); }
+// Candidates of the second certificate pass: 120 when the first pass kept
+// fewer (heaps of 120 fit shared memory beside two pipeline stages), else 256
+// (the rerank's limit); at most n.
+int64_t second_pass_candidates(int64_t n, int64_t C) { return std::min<int64_t>(C < 120 ? 120 : 256, n); }
 
 // Scratch of the scan for `rows` query rows keeping C candidates.
 size_t scan_scratch_bytes(const evoc_gpu_ctx* ctx, int64_t rows, int64_t C) {
@@ -306,14 +312,15 @@ int32_t read_count(evoc_gpu_ctx* ctx, const int32_t* d_count, int* rc) {
 
 // Whether `rows` failed rows take the exact FP32 pass directly.  The 16-bit
 // rescan runs a CTA per 128 query rows over every key (a handful of rows
-// leave most SMs idle) and is paced by its 256-candidate epilogue with heaps
-// in global memory, ~2 TFLOP/s per CTA measured; the exact pass splits the
-// keys over all SMs at the FP32 rate (~48 TFLOP/s measured).  Estimated
-// costs: 16-bit waves x 128 n d 2 FLOP / 2e12 against rows n d 2 FLOP / 45e12.
-bool exact_first(const evoc_gpu_ctx* ctx, int64_t rows, int64_t n, int d) {
+// leave most SMs idle) and is paced by its epilogue: ~2 TFLOP/s per CTA
+// measured with 256-entry heaps in global memory, taken as ~5 with 120-entry
+// heaps in shared memory; the exact pass splits the keys over all SMs at the
+// FP32 rate (~48 TFLOP/s measured).  Estimated costs: 16-bit waves x
+// 128 n d 2 FLOP / per-CTA rate against rows n d 2 FLOP / 45e12.
+bool exact_first(const evoc_gpu_ctx* ctx, int64_t rows, int64_t n, int d, int64_t C2) {
   const double work = double(n) * double(d) * 2.0;
   const double waves = std::ceil(double((rows + 127) / 128) / double(ctx->sms));
-  const double half_ms = waves * 128.0 * work / 2e12 * 1e3;
+  const double half_ms = waves * 128.0 * work / (C2 <= 120 ? 5e12 : 2e12) * 1e3;
   const double exact_ms = double(rows) * work / 45e12 * 1e3;
   return exact_ms <= half_ms;
 }
@@ -326,7 +333,7 @@ bool exact_first(const evoc_gpu_ctx* ctx, int64_t rows, int64_t n, int d) {
 int certify_rescan(evoc_gpu_ctx* ctx, const RescanJob& j, int32_t* fail1, int64_t failed1, int32_t* fail2,
                    float* bound2, int32_t* count2, int64_t* second, int64_t* exact) {
   Stage st(ctx, "certify_rescan");
-  const int64_t C2 = second_pass_candidates(j.n);
+  const int64_t C2 = second_pass_candidates(j.n, j.C);
   const RepairLayout RL = repair_layout(std::min<int64_t>(failed1, kRepairChunk), j.ld, j.ldb, C2, j.keff);
   EVOC_TRY(ctx->repair.ensure(RL.total), "alloc rescan arena");
   uint8_t* rb = ctx->repair.as<uint8_t>();
@@ -335,7 +342,7 @@ int certify_rescan(evoc_gpu_ctx* ctx, const RescanJob& j, int32_t* fail1, int64_
   int64_t failed2 = 0;
   int rc = EVOC_OK;
   *second = failed1;
-  if (C2 > j.C && !exact_first(ctx, failed1, j.n, j.d)) {
+  if (C2 > j.C && !exact_first(ctx, failed1, j.n, j.d, C2)) {
     void* qh = rb + RL.qh;
     int32_t* cand2 = reinterpret_cast<int32_t*>(rb + RL.cand2);
     EVOC_TRY(ctx->scratch.ensure(scan_scratch_bytes(ctx, std::min<int64_t>(failed1, kRepairChunk), C2)),
@@ -1641,7 +1648,7 @@ void knn_buffer_needs(const evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, int32_
       if (n >= 65536) locality(ldb * 2);
       if (opts.certify) {
         // the certificate and, should rows fail it, their rescans (bounded chunks)
-        const int64_t C2 = second_pass_candidates(n);
+        const int64_t C2 = second_pass_candidates(n, 256);  // the largest second pass
         const int64_t R = std::min<int64_t>(n, kRepairChunk);
         b[kBufCert] = cert_layout(n, n).total;
         b[kBufRepair] = repair_layout(R, round_up(dim, 16), ldb, C2, keff).total;
@@ -1699,7 +1706,7 @@ bool batch_buffer_needs(const evoc_gpu_opts& opts, int32_t dtype, int32_t n_jobs
       max_keff = std::max<int64_t>(max_keff, std::min<int64_t>(k, n[i] - 1));
     }
     const int64_t R = std::min<int64_t>(L.max_n, kRepairChunk);
-    const int64_t C2 = second_pass_candidates(L.max_n);
+    const int64_t C2 = second_pass_candidates(L.max_n, 256);  // the largest second pass
     need->b[kBufCert] = cert_layout(L.max_n, L.max_n).total;
     need->b[kBufRepair] = repair_layout(R, round_up(max_dim, 16), round_up(max_dim, 64), C2, max_keff).total;
     // the batch's plan holds no context scratch: the rescans' scan and exact pass size it

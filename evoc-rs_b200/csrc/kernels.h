@@ -82,11 +82,11 @@ cudaError_t launch_tc_scan(int mode, const void* Q, int64_t q_rows, int64_t q_ro
                            int* status, uint64_t timeout_ns, const int32_t* pc, cudaStream_t stream,
                            int variant = -1, int half_type = kHalfF16, const int32_t* q_self = nullptr,
                            float* out_bound = nullptr, int64_t q_self_base = 0, uint64_t delay_ns = 0);
-// Kernel variants of the scan (0..13; -1 = automatic: the first that fits
-// shared memory in the order 0..3, else 4 with global heaps; 5 -- 2 stages,
-// 2 groups --, the CTA-pair variants 6..9, 12, 13 and the four-group
-// variants 10, 11 are chosen only by the autotuner).
-constexpr int kScanVariants = 14;
+// Kernel variants of the scan (0..14; -1 = automatic, tc_scan_automatic_variant:
+// int8 with small keep 10, else the first that fits shared memory in the order
+// 0..3, 14, else 4 with global heaps; 5, the CTA-pair variants 6..9, 12, 13
+// and the four-group variant 11 are chosen only by the autotuner).
+constexpr int kScanVariants = 15;
 bool tc_scan_variant_feasible(int variant, int keep, bool has_scratch);
 // Whether a launch with this variant (-1: automatic) and keep keeps its heaps in global scratch.
 bool tc_scan_uses_global_heaps(int variant, int keep);

@@ -726,7 +726,7 @@ cudaError_t launch_pair(const CUtensorMap& ma, const CUtensorMap& mb, const Scan
 constexpr int kVariantCfg[kScanVariants][4] = {{4, 2, 1, 0}, {3, 2, 1, 0}, {4, 1, 1, 0}, {3, 1, 1, 0},
                                                {4, 1, 0, 0}, {2, 2, 1, 0}, {4, 2, 1, 1}, {4, 1, 1, 1},
                                                {6, 1, 1, 1}, {3, 2, 1, 1}, {3, 4, 1, 0}, {2, 4, 1, 0},
-                                               {5, 1, 1, 1}, {2, 2, 1, 1}};
+                                               {5, 1, 1, 1}, {2, 2, 1, 1}, {2, 1, 1, 0}};
 
 bool variant_feasible(int v, int keep, bool has_scratch) {
   if (v < 0 || v >= kScanVariants) return false;
@@ -753,6 +753,7 @@ cudaError_t launch_forced(const CUtensorMap& ma, const CUtensorMap& mb, ScanPara
     case 11: return launch_variant<MODE, 2, 4, true>(ma, mb, p, grid, smem_bytes(2, 4, odd), stream);
     case 12: return launch_pair<MODE, 5, 1>(ma, mb, p, grid, smem_bytes(5, 1, odd, true), stream);
     case 13: return launch_pair<MODE, 2, 2>(ma, mb, p, grid, smem_bytes(2, 2, odd, true), stream);
+    case 14: return launch_variant<MODE, 2, 1, true>(ma, mb, p, grid, smem_bytes(2, 1, odd), stream);
     default:
       p.heap_stride = p.keep;
       return launch_variant<MODE, 4, 1, false>(ma, mb, p, grid, smem_bytes(4, 1, 0), stream);
@@ -785,6 +786,10 @@ cudaError_t launch_mode(const CUtensorMap& ma, const CUtensorMap& mb, ScanParams
     return launch_variant<MODE, 4, 1, true>(ma, mb, p, grid, smem_bytes(4, 1, odd), stream);
   if (smem_bytes(3, 1, odd) <= SMEM_LIMIT)
     return launch_variant<MODE, 3, 1, true>(ma, mb, p, grid, smem_bytes(3, 1, odd), stream);
+  // heaps in shared memory beside two stages beat heaps in global memory by
+  // far (each heap insert is a chain of dependent loads)
+  if (smem_bytes(2, 1, odd) <= SMEM_LIMIT)
+    return launch_variant<MODE, 2, 1, true>(ma, mb, p, grid, smem_bytes(2, 1, odd), stream);
   if (!p.scratch) return cudaErrorInvalidValue;
   p.heap_stride = p.keep;
   return launch_variant<MODE, 4, 1, false>(ma, mb, p, grid, smem_bytes(4, 1, 0), stream);
@@ -849,7 +854,7 @@ bool tc_scan_variant_feasible(int variant, int keep, bool has_scratch) {
 
 bool tc_scan_uses_global_heaps(int variant, int keep) {
   if (variant >= 0 && variant_feasible(variant, keep, true)) return kVariantCfg[variant][2] == 0;
-  return smem_bytes(3, 1, keep | 1) > SMEM_LIMIT;  // the automatic choice: no shared-memory variant fits
+  return smem_bytes(2, 1, keep | 1) > SMEM_LIMIT;  // the automatic choice: no shared-memory variant fits
 }
 
 int tc_scan_automatic_variant(int mode, int keep) {
@@ -859,6 +864,7 @@ int tc_scan_automatic_variant(int mode, int keep) {
   if (smem_bytes(3, 2, odd) <= SMEM_LIMIT) return 1;
   if (smem_bytes(4, 1, odd) <= SMEM_LIMIT) return 2;
   if (smem_bytes(3, 1, odd) <= SMEM_LIMIT) return 3;
+  if (smem_bytes(2, 1, odd) <= SMEM_LIMIT) return 14;
   return 4;
 }
 
@@ -876,7 +882,8 @@ const char* tc_scan_variant_name(int variant) {
                                              "3 stages, 4 epilogue groups, shared-memory heaps",
                                              "2 stages, 4 epilogue groups, shared-memory heaps",
                                              "CTA pair, 5 stages, 1 epilogue group, shared-memory heaps",
-                                             "CTA pair, 2 stages, 2 epilogue groups, shared-memory heaps"};
+                                             "CTA pair, 2 stages, 2 epilogue groups, shared-memory heaps",
+                                             "2 stages, 1 epilogue group, shared-memory heaps"};
   return variant >= 0 && variant < kScanVariants ? names[variant] : "automatic";
 }
 

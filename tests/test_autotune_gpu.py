@@ -108,7 +108,7 @@ def _forced_graph(tmp_path, monkeypatch, x, kind, form, k, variant, **opt):
         monkeypatch.delenv("EVOC_TUNE_CACHE")
 
 
-@pytest.mark.parametrize("variant", [6, 7, 8, 9, 10, 11, 12, 13])
+@pytest.mark.parametrize("variant", [6, 7, 8, 9, 10, 11, 12, 13, 14])
 @pytest.mark.parametrize("n", [2900, 300, 129])
 def test_cta_pair_variants_match_single_cta(tmp_path, monkeypatch, variant, n):
     """The CTA-pair scans (cluster of two, M = 256 MMAs; variants 6-9) and the four-epilogue-group
