@@ -992,6 +992,7 @@ def run_ours(args, world, rank, local):
         pg.barrier()
     clk = clocks.stop()
     cert = ctx.certify_counts() if form == "bf16_rerank" else None
+    sym = ctx.symmetric_stats() if form == "bf16_rerank" else None
     total_ms = ev0.elapsed_time(ev1)
     ms_step = total_ms / args.steps
     if pg:
@@ -1097,12 +1098,21 @@ def run_ours(args, world, rank, local):
     peaks, peak_kind = measured_peaks()
     if form == "bf16_rerank":
         scan_ms = statistics.mean(stage_ms.get("bf16_scan", [float("nan")]))
-        flops = 2.0 * n * n * d
-        achieved = flops / (scan_ms / 1000.0) / 1e12
         peak = float(peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops")))
+        if sym and sym["sample_rows"]:
+            # one score per unordered pair of rows (self pairs included): n (n + 1) / 2 dot products
+            flops = 1.0 * n * (n + 1) * d
+            kernel = ("tc_scan_kernel, symmetric mode (FP16 operands, each pair of rows once, fused top-C "
+                      "with per-row mailboxes, C = 2k)")
+            traffic = None
+        else:
+            flops = 2.0 * n * n * d
+            kernel = "tc_scan_kernel (FP16 operands, fused top-C, C = ceil(2.5k))"
+            traffic = scan_traffic(n)
+        achieved = flops / (scan_ms / 1000.0) / 1e12
         roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                    "traffic": scan_traffic(n), "traffic_unit": "bytes per launch (ncu, scaled)",
-                    "kernel": "tc_scan_kernel (FP16 operands, fused top-C, C = ceil(2.5k))",
+                    "traffic": traffic, "traffic_unit": "bytes per launch (ncu, scaled)",
+                    "kernel": kernel, "algorithmic_flops": flops,
                     "peak_kind": f"{peak_kind} bf16 sustained (burst {peaks.get('bf16_tflops')})",
                     "launch_ms": scan_ms}
     else:
@@ -1176,6 +1186,10 @@ def run_ours(args, world, rank, local):
         "certificate": cert and dict(cert, note=(
             "rows whose k nearest the 16-bit scan's candidates provably hold (rigorous FP16 error bound); "
             "second_pass rows were rescanned with 256 candidates, exact_rescan rows in FP32")),
+        "symmetric_scan": sym and sym["sample_rows"] and dict(sym, note=(
+            "each pair of rows multiplied once; scores for the later row reach it through a per-row mailbox "
+            "filtered by thresholds from a pre-scan against sample_rows strided rows; overflowed rows are "
+            "rescanned by the certificate")),
         "clocks": clk,
         "gpu_launches": launches,
     }
@@ -1376,6 +1390,7 @@ def run_case(args):
             out["stages_ms"] = dict(st)
         if args.case == "scan":
             out["certificate"] = ctx.certify_counts()
+            out["symmetric_scan"] = ctx.symmetric_stats()
             out["scan_type"] = args.scan_type
             out["oversample"] = args.oversample
         if args.case == "fp32":

@@ -65,6 +65,13 @@ struct evoc_gpu_ctx {
   // and the rescan arena for those rows (bounded chunks).
   evoc::DevBuf cert, repair;
   int64_t cert_checked = 0, cert_second = 0, cert_exact = 0;  // last call's counts
+  // Symmetric 16-bit scan (sym.cu, opt-in): self-joins of at least
+  // sym_min_rows rows (0: never, the default); the arena; the last call's
+  // sample rows (0: not taken), mailbox capacity, most mirror keys a row was
+  // offered, overflowed rows.
+  evoc::DevBuf sym;
+  int64_t sym_min_rows = 0;
+  int64_t sym_sample = 0, sym_cap = 0, sym_max_offers = 0, sym_overflow = 0;
   evoc::DevBuf batch_ws, batch_tab;  // batches: per-request work arena, device tables
   void* batch_host = nullptr;  // pinned staging of the tables
   size_t batch_host_bytes = 0;

@@ -27,6 +27,7 @@ enum CtxBuf {
   kBufBatchTab,  // batches: device tables
   kBufCert,      // 16-bit form: certificate norms, bounds, failed-row lists
   kBufRepair,    // 16-bit form: rescan arena for rows that failed the certificate
+  kBufSym,       // 16-bit form: symmetric scan arena (mailboxes, thresholds, sample rows)
   kBufCount
 };
 

@@ -387,6 +387,124 @@ int certify_rescan(evoc_gpu_ctx* ctx, const RescanJob& j, int32_t* fail1, int64_
   return EVOC_OK;
 }
 
+// Symmetric scan (sym.cu): a self-join computes only the key tiles from each
+// query block on, and scores for later rows reach them through mailboxes
+// filtered by thresholds from a pre-scan of every row against a strided
+// sample of n / kSymSampleStride rows.  The sample's (C+1)-th best is at
+// about rank (C+1) * stride among all keys (for any data), so a row collects
+// about that many mailbox keys plus the few within the threshold's rounding
+// slack: kSymCap gives it twice that and 256 more (a row that overflows is
+// rescanned, so the capacity only matters for speed).
+constexpr int64_t kSymSampleStride = 16;
+
+int64_t sym_cap(int64_t C) { return round_up(2 * (C + 1) * kSymSampleStride + 256, 256); }
+
+struct SymLayout {
+  size_t thr, umin, perm, count, bound, own_raw, stats, rows, sample, mail, total;
+  int64_t m, m_pad, n_pad, cap;
+};
+
+SymLayout sym_layout(int64_t n, int64_t C, int64_t ldb) {
+  SymLayout L{};
+  L.m = n / kSymSampleStride;
+  L.m_pad = round_up(L.m, 256);
+  L.n_pad = round_up(n, 256);
+  L.cap = sym_cap(C);
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t at = off;
+    off += (bytes + 255) / 256 * 256;
+    return at;
+  };
+  L.thr = take(size_t(L.n_pad) * 4);
+  L.umin = take(size_t(L.n_pad / 32) * 4);
+  L.perm = take(size_t(L.n_pad) * 4);  // scanned row -> data-set row
+  L.count = take(size_t(n) * 4);
+  L.bound = take(size_t(n) * 4);  // the pre-scan's (C+1)-th raw values
+  L.own_raw = take(size_t(n * C) * 4);
+  L.stats = take(8);
+  L.rows = take(size_t(evoc::padded_rows(n) * ldb) * 2);  // the 16-bit rows in scanned order
+  L.sample = take(size_t(L.m_pad * ldb) * 2);
+  // the pre-scan's candidate output is written there too, before the mailboxes
+  L.mail = take(std::max(size_t(n) * size_t(L.cap) * 8, size_t(n * (C + 1)) * 4));
+  L.total = off;
+  return L;
+}
+
+// Whether a 16-bit form request takes the symmetric scan: certified (an
+// overflowed row is repaired by the certificate's rescan), all rows as
+// queries, a persistent grid (not a serving lane's per-block launch), and a
+// sample large enough for its (C+1)-th best to mean something.
+bool use_symmetric(const evoc_gpu_ctx* ctx, bool certify, int64_t n, int64_t r0, int64_t nq, int64_t C) {
+  return certify && !ctx->scan_per_block && ctx->sym_min_rows > 0 && n >= ctx->sym_min_rows && r0 == 0 &&
+         nq == n && n / kSymSampleStride >= 4 * (C + 1) && evoc::tc_scan_sym_feasible(int(C));
+}
+
+// The symmetric scan of all rows: candidates into ctx->cand, the certificate's
+// bound (C-th kept raw value) into `bound`.  The rows are scanned grouped by
+// nearest pivot (ctx->order, which the rerank then reuses): the 32 key rows
+// of a chunk mostly share a cluster, so their mailbox thresholds are alike
+// and a query row of another cluster falls below all of them, which one
+// compare with their minimum shows.
+int symmetric_scan(evoc_gpu_ctx* ctx, const Job& j, int half, int64_t ldb, int64_t rows, int64_t C, float* bound,
+                   const float* hnorm, const unsigned int* maxes) {
+  const SymLayout S = sym_layout(j.n, C, ldb);
+  EVOC_TRY(ctx->sym.ensure(S.total), "alloc symmetric scan");
+  uint8_t* b = ctx->sym.as<uint8_t>();
+  float* thr = reinterpret_cast<float*>(b + S.thr);
+  float* umin = reinterpret_cast<float*>(b + S.umin);
+  int32_t* count = reinterpret_cast<int32_t*>(b + S.count);
+  float* T = reinterpret_cast<float*>(b + S.bound);
+  float* own_raw = reinterpret_cast<float*>(b + S.own_raw);
+  int32_t* stats = reinterpret_cast<int32_t*>(b + S.stats);
+  int32_t* perm = reinterpret_cast<int32_t*>(b + S.perm);
+  void* xs = b + S.rows;
+  void* sample = b + S.sample;
+  uint64_t* mail = reinterpret_cast<uint64_t*>(b + S.mail);
+  int rc = locality_order(ctx, j, ctx->xb.p, ldb * 2, false, false, half);
+  if (rc) return rc;
+  {
+    Stage st(ctx, "sym_sample");
+    const int32_t* order = ctx->order.as<int32_t>();
+    EVOC_TRY(cudaMemcpyAsync(perm, order, size_t(j.n) * 4, cudaMemcpyDeviceToDevice, ctx->stream), "copy order");
+    EVOC_TRY(cudaMemsetAsync(perm + j.n, 0, size_t(S.n_pad - j.n) * 4, ctx->stream), "pad order");
+    EVOC_TRY(evoc::launch_gather_rows_list(ctx->xb.p, ldb * 2, 0, order, j.n, rows, xs, ctx->sms, ctx->stream),
+             "rows in scanned order");
+    EVOC_TRY(evoc::launch_gather_strided_rows(xs, ldb * 2, kSymSampleStride, S.m, S.m_pad, sample, ctx->sms,
+                                              ctx->stream),
+             "gather sample rows");
+    EVOC_TRY(ctx->scratch.ensure(scan_scratch_bytes(ctx, j.n, C + 1)), "alloc scratch");
+    EVOC_TRY(evoc::launch_tc_scan(evoc::kScanHalf, xs, rows, 0, j.n, sample, S.m_pad, S.m, ldb * 2,
+                                  int(C + 1), ctx->scratch.as<uint64_t>(), scan_grid(ctx, j.n), 0, 0, 0,
+                                  reinterpret_cast<int32_t*>(mail), nullptr, nullptr, j.status, ctx->timeout_ns,
+                                  nullptr, ctx->stream, -1, half, nullptr, T),
+             "sample pre-scan");
+    EVOC_TRY(evoc::launch_sym_thresholds(j.n, S.n_pad, T, hnorm, perm, maxes, int(ldb), thr, umin, count, ctx->sms,
+                                         ctx->stream),
+             "mailbox thresholds");
+    EVOC_TRY(cudaMemsetAsync(stats, 0, 8, ctx->stream), "clear merge statistics");
+    ctx->launches += 4;
+  }
+  {
+    Stage st(ctx, "bf16_scan");
+    EVOC_TRY(evoc::launch_tc_scan_sym(xs, rows, j.n, ldb * 2, int(C), scan_grid(ctx, j.n), ctx->cand.as<int32_t>(),
+                                      own_raw, j.status, ctx->timeout_ns, ctx->stream, half, thr, umin, perm, count,
+                                      mail, int(S.cap), ctx->delay_ns),
+             "symmetric 16-bit scan");
+    ctx->launches += 1;
+  }
+  {
+    Stage st(ctx, "sym_merge");
+    EVOC_TRY(evoc::launch_sym_merge(j.n, int(C), ctx->cand.as<int32_t>(), own_raw, count, mail, int(S.cap), bound,
+                                    stats, ctx->sms, ctx->stream),
+             "merge mailboxes");
+    ctx->launches += 1;
+  }
+  ctx->sym_sample = S.m;
+  ctx->sym_cap = S.cap;
+  return EVOC_OK;
+}
+
 // The 16-bit form: FP16 (or BF16) tensor-core scan keeping C candidates per
 // row, FP32 rerank with the per-row certificate (rerank.cu), then for rows
 // that fail it a second scan keeping 256 candidates, and for rows that fail
@@ -423,7 +541,11 @@ int run_bf16_rerank(evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, const Job& j, 
   const int variant = tuned_variant(ctx, evoc::kScanHalf, int(C), ldb * 2, j.n);
   const int grid = main_scan_grid(ctx, j.nq, int(C), variant);
   EVOC_TRY(ctx->cand.ensure(size_t(j.nq * C) * 4), "alloc candidates");
-  {
+  const bool sym = use_symmetric(ctx, certify, j.n, j.r0, j.nq, C);
+  if (sym) {
+    int rc = symmetric_scan(ctx, j, half, ldb, rows, C, cf(CL.bound), cf(CL.hnorm), maxes);
+    if (rc) return rc;
+  } else {
     Stage st(ctx, "bf16_scan");
     EVOC_TRY(ctx->scratch.ensure(scan_scratch_bytes(ctx, j.nq, C)), "alloc scratch");
     EVOC_TRY(evoc::launch_tc_scan(evoc::kScanHalf, ctx->xb.p, rows, j.r0, j.nq, ctx->xb.p, rows, j.n, ldb * 2, int(C),
@@ -435,9 +557,11 @@ int run_bf16_rerank(evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, const Job& j, 
   }
   const int32_t* order = nullptr;
   if (j.nq >= 65536) {
-    // the order only schedules the rerank
-    int rc = locality_order(ctx, j, ctx->xb.p, ldb * 2, false, false, half);
-    if (rc) return rc;
+    // the order only schedules the rerank (the symmetric scan computed it already)
+    if (!sym) {
+      int rc = locality_order(ctx, j, ctx->xb.p, ldb * 2, false, false, half);
+      if (rc) return rc;
+    }
     order = ctx->order.as<int32_t>();
   }
   int32_t* counts = certify ? ci(CL.counts) : nullptr;
@@ -459,6 +583,12 @@ int run_bf16_rerank(evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, const Job& j, 
   int rc = EVOC_OK;
   const int64_t failed1 = read_count(ctx, counts, &rc);
   if (rc) return rc;
+  if (sym) {
+    const int32_t* stats = reinterpret_cast<const int32_t*>(ctx->sym.as<uint8_t>() + sym_layout(j.n, C, ldb).stats);
+    ctx->sym_overflow = read_count(ctx, stats, &rc);
+    if (rc == EVOC_OK) ctx->sym_max_offers = read_count(ctx, stats + 1, &rc);
+    if (rc) return rc;
+  }
   if (failed1 == 0) return EVOC_OK;
   RescanJob rj{ctx->x.as<float>(), ld, d, ctx->xb.p, ldb, rows, j.n, j.r0, j.nq, j.keff, half, C, j.idx, j.raw,
                j.dist, j.status, ca};
@@ -805,6 +935,7 @@ int knn_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtype, con
   ctx->n_stages = 0;
   ctx->launches = 0;
   ctx->cert_checked = ctx->cert_second = ctx->cert_exact = 0;
+  ctx->sym_sample = ctx->sym_cap = ctx->sym_max_offers = ctx->sym_overflow = 0;
   evoc_gpu_opts opts;
   evoc_gpu_default_opts(&opts);
   if (opts_in) {
@@ -1049,6 +1180,7 @@ int knn_batch_impl(evoc_gpu_ctx* ctx, const evoc_gpu_opts* opts_in, int32_t dtyp
   ctx->n_stages = 0;
   ctx->launches = 0;
   ctx->cert_checked = ctx->cert_second = ctx->cert_exact = 0;
+  ctx->sym_sample = ctx->sym_cap = ctx->sym_max_offers = ctx->sym_overflow = 0;
   evoc_gpu_opts opts;
   evoc_gpu_default_opts(&opts);
   if (opts_in) {
@@ -1468,6 +1600,10 @@ int evoc_gpu_ctx_create(int device, evoc_gpu_ctx** out) {
   cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device);
   if (const char* v = std::getenv("EVOC_SYNC_CHECK")) ctx->sync_check = v[0] == '1';
   if (const char* v = std::getenv("EVOC_NO_GRAPHS")) ctx->use_graphs = v[0] != '1';
+  if (const char* v = std::getenv("EVOC_SYM_MIN_ROWS")) {
+    const long long r = std::atoll(v);
+    ctx->sym_min_rows = r < 0 ? 0 : r;
+  }
   if (const char* v = std::getenv("EVOC_TUNE_CACHE"))
     if (v[0]) tune_load_impl(ctx, v);
   e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
@@ -1549,6 +1685,23 @@ int evoc_gpu_set_wait_limit(evoc_gpu_ctx* ctx, uint64_t ns, uint64_t producer_de
   std::lock_guard<std::mutex> lock(ctx->mu);
   ctx->timeout_ns = ns ? ns : 4000000000ull;
   ctx->delay_ns = producer_delay_ns;
+  return EVOC_OK;
+}
+
+int evoc_gpu_set_symmetric_scan(evoc_gpu_ctx* ctx, int64_t min_rows) {
+  if (!ctx) return EVOC_ERR_ARG;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  ctx->sym_min_rows = min_rows < 0 ? 0 : min_rows;
+  return EVOC_OK;
+}
+
+int evoc_gpu_last_symmetric(const evoc_gpu_ctx* ctx, int64_t* sample_rows, int64_t* mailbox_cap,
+                            int64_t* max_offers, int64_t* overflowed) {
+  if (!ctx) return EVOC_ERR_ARG;
+  if (sample_rows) *sample_rows = ctx->sym_sample;
+  if (mailbox_cap) *mailbox_cap = ctx->sym_cap;
+  if (max_offers) *max_offers = ctx->sym_max_offers;
+  if (overflowed) *overflowed = ctx->sym_overflow;
   return EVOC_OK;
 }
 
@@ -1646,6 +1799,7 @@ void knn_buffer_needs(const evoc_gpu_ctx* ctx, const evoc_gpu_opts& opts, int32_
       b[kBufCand] = size_t(n * C) * 4;
       b[kBufScratch] = size_t(grid) * 256 * size_t(C) * 8;
       if (n >= 65536) locality(ldb * 2);
+      if (use_symmetric(ctx, opts.certify != 0, n, 0, n, C)) b[kBufSym] = sym_layout(n, C, ldb).total;
       if (opts.certify) {
         // the certificate and, should rows fail it, their rescans (bounded chunks)
         const int64_t C2 = second_pass_candidates(n, 256);  // the largest second pass
@@ -1723,7 +1877,7 @@ void ctx_buffer_sizes(const evoc_gpu_ctx* ctx, CtxSizes* cur) {
   const DevBuf* bufs[kBufCount] = {&ctx->x,      &ctx->scratch, &ctx->norms,    &ctx->flag,      &ctx->xb,
                                    &ctx->cand,   &ctx->labels,  &ctx->order,    &ctx->hist,      &ctx->cursor,
                                    &ctx->pivots, &ctx->popc,    &ctx->nnd_work, &ctx->batch_ws,  &ctx->batch_tab,
-                                   &ctx->cert,   &ctx->repair};
+                                   &ctx->cert,   &ctx->repair,  &ctx->sym};
   for (int i = 0; i < kBufCount; i++) cur->b[i] = bufs[i]->bytes;
 }
 
@@ -1741,7 +1895,7 @@ void ctx_release_buffers(evoc_gpu_ctx* ctx) {
   DevBuf* bufs[kBufCount] = {&ctx->x,      &ctx->scratch, &ctx->norms,    &ctx->flag,      &ctx->xb,
                              &ctx->cand,   &ctx->labels,  &ctx->order,    &ctx->hist,      &ctx->cursor,
                              &ctx->pivots, &ctx->popc,    &ctx->nnd_work, &ctx->batch_ws,  &ctx->batch_tab,
-                             &ctx->cert,   &ctx->repair};
+                             &ctx->cert,   &ctx->repair,  &ctx->sym};
   for (DevBuf* b : bufs) b->release();
   for (auto& g : ctx->batch_graphs) cudaGraphExecDestroy(g.exec);  // they name the freed tables
   ctx->batch_graphs.clear();

@@ -82,6 +82,35 @@ cudaError_t launch_tc_scan(int mode, const void* Q, int64_t q_rows, int64_t q_ro
                            int* status, uint64_t timeout_ns, const int32_t* pc, cudaStream_t stream,
                            int variant = -1, int half_type = kHalfF16, const int32_t* q_self = nullptr,
                            float* out_bound = nullptr, int64_t q_self_base = 0, uint64_t delay_ns = 0);
+// Symmetric scan of all n rows against themselves (16-bit operands, self
+// rule, candidates out).  X holds the rows in a permuted order: scanned row i
+// is data-set row perm[i].  Query block b multiplies only the key tiles from
+// its own rows on, and scores of key rows past the block that reach thr[key]
+// go to that row's mailbox (count[row] offers, the first cap kept in
+// mail[row * cap ..], rows of the data set).  thr and perm hold n_ktiles *
+// 256 entries (thr +inf past n), umin the smallest threshold of each 32, all
+// in scanned order; out_idx / out_raw rows are data-set rows.  sym.cu
+// computes the thresholds and merges the mailboxes.
+bool tc_scan_sym_feasible(int keep);
+cudaError_t launch_tc_scan_sym(const void* X, int64_t rows, int64_t n, int64_t row_bytes, int keep, int grid,
+                               int32_t* out_idx, float* out_raw, int* status, uint64_t timeout_ns,
+                               cudaStream_t stream, int half_type, const float* thr, const float* umin,
+                               const int32_t* perm, int32_t* count, uint64_t* mail, int cap,
+                               uint64_t delay_ns = 0);
+// sym.cu.  Row j of dst = row j * stride of src for j < m, zero rows up to m_pad.
+cudaError_t launch_gather_strided_rows(const void* src, int64_t row_bytes, int64_t stride, int64_t m, int64_t m_pad,
+                                       void* dst, int sms, cudaStream_t stream);
+// Mailbox thresholds of the scanned rows from the sample pre-scan's (C+1)-th
+// raw values T (scanned order; hnorm of data-set row perm[i]); clears count.
+cudaError_t launch_sym_thresholds(int64_t n, int64_t n_pad, const float* T, const float* hnorm,
+                                  const int32_t* perm, const unsigned int* maxes, int half_len, float* thr,
+                                  float* umin, int32_t* count, int sms, cudaStream_t stream);
+// Folds each row's mailbox into its C own-side candidates (cand, own_raw), in
+// place; bound[r] = C-th kept raw value (-f32::MAX after an overflow).
+// stats[0] += overflowed rows, stats[1] = max(stats[1], most offers to a row).
+cudaError_t launch_sym_merge(int64_t n, int C, int32_t* cand, const float* own_raw, const int32_t* count,
+                             const uint64_t* mail, int cap, float* bound, int32_t* stats, int sms,
+                             cudaStream_t stream);
 // Kernel variants of the scan (0..14; -1 = automatic, tc_scan_automatic_variant:
 // int8 with small keep 10, else the first that fits shared memory in the order
 // 0..3, 14, else 4 with global heaps; 5, the CTA-pair variants 6..9, 12, 13

@@ -257,5 +257,16 @@ __device__ __forceinline__ void mma_commit_pair_mc(uint64_t* bar, uint16_t cta_m
       : "memory");
 }
 
+// Asynchronous 16-byte global -> shared copies (L2 only), in commit groups.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// Waits until at most N of this thread's commit groups are still in flight.
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 }  // namespace sm100
 }  // namespace evoc

@@ -90,6 +90,22 @@ struct ScanParams {
   const int32_t* q_self;  // optional: key index of query i is q_self_base + q_self[i] (gathered query rows)
   int64_t q_self_base;
   float* out_bound;  // optional: raw value of the keep-th kept key of each query
+  // Symmetric mode (queries = keys = all rows, self rule): query block b
+  // multiplies only key tiles from its own rows on; a score counts for its
+  // query row (own side) and, for key rows past the block, for the key row
+  // too (mirror side): a score reaching sym_thr[key] is appended to the key
+  // row's mailbox, which a merge folds into the row's kept keys afterwards.
+  const float* sym_thr;   // per key row, padded to whole tiles with +inf: the mirror side's score threshold
+  const float* sym_umin;  // per 32 key rows: the smallest of their thresholds (quick reject)
+  int32_t* sym_count;     // per row: mirror keys offered (beyond sym_cap the row's mailbox overflowed)
+  uint64_t* sym_mail;     // per row: sym_cap keys
+  int sym_cap;
+  // The rows are scanned in a permuted order (rows of one pivot group side by
+  // side, so that a chunk's key rows have similar thresholds and the quick
+  // reject works): scanned row i is row sym_perm[i] of the data set (padded
+  // to whole tiles).  Keys, outputs and mailboxes use data-set rows;
+  // sym_thr / sym_umin follow the scanned order.
+  const int32_t* sym_perm;
   // Batch mode: the work-list of (request, query block) items and the
   // requests' tensor maps and parameters, all in device memory.
   const ScanJob* jobs;
@@ -172,7 +188,7 @@ __device__ __forceinline__ uint32_t pick(const uint32_t (&v)[32], int j) {
 template <int MODE>
 __device__ __forceinline__ void offer_chunk(const uint32_t (&v)[32], uint32_t mask, int64_t col0, int64_t n_k,
                                             bool self_mode, int64_t q, KeyHeap& heap, uint32_t& thr, int32_t pa,
-                                            const int32_t* __restrict__ pc) {
+                                            const int32_t* __restrict__ pc, const int32_t* ids = nullptr) {
   while (mask) {
     const int j = __clz(mask);
     mask &= ~(0x80000000u >> j);
@@ -187,7 +203,7 @@ __device__ __forceinline__ void offer_chunk(const uint32_t (&v)[32], uint32_t ma
     } else {
       raw = MODE == kModeInt8 ? -__int2float_rn(int32_t(bits)) : raw_cosine(__uint_as_float(bits));
     }
-    heap.offer(make_key(raw, int32_t(key)));
+    heap.offer(make_key(raw, ids ? ids[j] : int32_t(key)));  // ids: the chunk's row indices of the data set
     thr = pass_threshold<MODE>(heap, pa);
   }
 }
@@ -242,11 +258,107 @@ __device__ __forceinline__ uint32_t chunk_mask(const uint32_t (&v)[32], uint32_t
   return ~((f[0] << 24) | (f[1] << 16) | (f[2] << 8) | f[3]);
 }
 
+// Symmetric mode, mirror side.  The keys for later rows wait in a per-warp
+// shared-memory stage and go to the mailboxes kMirrorStage at a time: one
+// round trip of the global atomics per flush, both halves' atomics issued
+// before either store, instead of one per chunk.
+constexpr int kMirrorStage = 64;
+constexpr size_t kMirrorStageBytes = size_t(kMirrorStage) * 12;  // keys, then rows
+// Each epilogue warp also holds two tiles' mailbox thresholds (256), their
+// per-32 minima (8) and the data-set rows of the tile's keys (256), copied
+// one tile ahead by cp.async: a global load inside the chunk loop would stall
+// the warp for an L2 round trip.
+constexpr int kTileThr = BN + BN / 32 + BN;
+constexpr int kTileIds = BN + BN / 32;  // offset of the row ids in a tile buffer (words)
+constexpr size_t kMirrorWarpBytes = kMirrorStageBytes + 2 * kTileThr * 4;
+
+struct MirrorStage {
+  uint64_t* key;
+  int32_t* row;
+  int n;
+};
+
+__device__ __forceinline__ void mirror_flush(MirrorStage& st, int lane, const ScanParams& p) {
+  int s0 = -1, s1 = -1;
+  int32_t c0 = 0, c1 = 0;
+  if (lane < st.n) {
+    c0 = st.row[lane];
+    s0 = atomicAdd(p.sym_count + c0, 1);
+  }
+  if (lane + 32 < st.n) {
+    c1 = st.row[lane + 32];
+    s1 = atomicAdd(p.sym_count + c1, 1);
+  }
+  if (s0 >= 0 && s0 < p.sym_cap) p.sym_mail[int64_t(c0) * p.sym_cap + s0] = st.key[lane];
+  if (s1 >= 0 && s1 < p.sym_cap) p.sym_mail[int64_t(c1) * p.sym_cap + s1] = st.key[lane + 32];
+  __syncwarp();
+  st.n = 0;
+}
+
+// One 32-column chunk of query row r (warp-collective: every lane of the warp
+// calls it, rows past n_q with valid = false).  Scores reaching their key
+// rows' thresholds (th) are staged for those rows (ids: data-set rows; r is
+// one too).  mx is the chunk's largest score as a
+// signed integer (against a positive threshold the float bit patterns order
+// as integers); umin the loosest threshold of the chunk's key rows.
+__device__ __forceinline__ void mirror_chunk(const uint32_t (&v)[32], int32_t mx, float umin, const float* th,
+                                             const int32_t* ids, int64_t col, int64_t n_k, int32_t r, bool valid,
+                                             MirrorStage& st, int lane, const ScanParams& p) {
+  const bool maybe = valid && !(umin > 0.0f && mx < __float_as_int(umin));
+  if (!__any_sync(0xffffffffu, maybe)) return;
+  uint32_t mask = 0;
+  if (maybe) {
+    const float4* t4 = reinterpret_cast<const float4*>(th);  // the chunk's 32 thresholds (shared memory)
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const float4 t = t4[i];
+      mask |= (__uint_as_float(v[4 * i]) >= t.x ? 1u : 0u) << (4 * i);
+      mask |= (__uint_as_float(v[4 * i + 1]) >= t.y ? 1u : 0u) << (4 * i + 1);
+      mask |= (__uint_as_float(v[4 * i + 2]) >= t.z ? 1u : 0u) << (4 * i + 2);
+      mask |= (__uint_as_float(v[4 * i + 3]) >= t.w ? 1u : 0u) << (4 * i + 3);
+    }
+    if (col + 32 > n_k) mask &= col >= n_k ? 0u : (1u << (n_k - col)) - 1u;  // padding thresholds are +inf anyway
+  }
+  const int cnt = __popc(mask);
+  int incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  const int total = __shfl_sync(0xffffffffu, incl, 31);
+  if (total == 0) return;
+  if (total > kMirrorStage) {  // more than a stage at once (many near-duplicate rows): straight to the mailboxes
+    while (mask) {
+      const int j = __ffs(mask) - 1;
+      mask &= mask - 1;
+      const int64_t c = ids[j];
+      const uint64_t key = make_key(raw_cosine(__uint_as_float(pick(v, j))), r);
+      const int slot = atomicAdd(p.sym_count + c, 1);
+      if (slot < p.sym_cap) p.sym_mail[c * p.sym_cap + slot] = key;
+    }
+    __syncwarp();
+    return;
+  }
+  if (st.n + total > kMirrorStage) mirror_flush(st, lane, p);
+  int at = st.n + incl - cnt;
+  while (mask) {
+    const int j = __ffs(mask) - 1;
+    mask &= mask - 1;
+    st.key[at] = make_key(raw_cosine(__uint_as_float(pick(v, j))), r);
+    st.row[at] = ids[j];
+    at++;
+  }
+  __syncwarp();
+  st.n += total;
+}
+
 // One work item as every role sees it: a 128-row query block of one request.
 struct ItemView {
   const CUtensorMap* ma;
   const CUtensorMap* mb;
   int64_t qb, n_q, n_k, q_row0, n_ktiles;
+  int64_t kt0;  // first key tile (symmetric mode: the tile holding the block's own rows)
   int n_kchunks, keep, self_mode, final_mode, dtype;
   int32_t* out_idx;
   float* out_raw;
@@ -257,7 +369,17 @@ struct ItemView {
   float* out_bound;
 };
 
-template <bool kBatch>
+// Symmetric mode: block b multiplies n_ktiles - b/2 key tiles, so the work
+// shrinks with b.  Items are dealt to the CTAs in rounds of gridDim.x, every
+// other full round in reverse, so that each CTA's pair of rounds sums to the
+// same work.
+__device__ __forceinline__ int64_t sym_block(int64_t it, int64_t n_blocks) {
+  const int64_t g = gridDim.x, round = it / g, pos = it % g;
+  if ((round & 1) && (round + 1) * g <= n_blocks) return round * g + (g - 1 - pos);
+  return it;
+}
+
+template <bool kBatch, bool kSym = false>
 __device__ __forceinline__ ItemView item_view(const ScanParams& p, const CUtensorMap* tmA, const CUtensorMap* tmB,
                                               int64_t it) {
   ItemView v;
@@ -285,7 +407,7 @@ __device__ __forceinline__ ItemView item_view(const ScanParams& p, const CUtenso
   } else {
     v.ma = tmA;
     v.mb = tmB;
-    v.qb = it;
+    v.qb = kSym ? sym_block(it, (p.n_q + BM - 1) / BM) : it;
     v.n_q = p.n_q;
     v.n_k = p.n_k;
     v.q_row0 = p.q_row0;
@@ -303,7 +425,18 @@ __device__ __forceinline__ ItemView item_view(const ScanParams& p, const CUtenso
     v.out_bound = p.out_bound;
   }
   v.n_ktiles = (v.n_k + BN - 1) / BN;
+  v.kt0 = kSym ? v.qb * BM / BN : 0;
   return v;
+}
+
+// Tile ti of an item's sequence.  Symmetric mode: the tile of the block's
+// own rows first (its nearest keys, so the heap's threshold tightens at
+// once), then the rest from the last tile down: the CTAs of a round of items
+// all start at the top and stream the same key tiles nearly in step, as in
+// the plain scan, so each tile is read from HBM once and then from L2.
+template <bool kSym>
+__device__ __forceinline__ int64_t tile_at(const ItemView& v, int64_t ti) {
+  return (kSym && ti > 0) ? v.n_ktiles - ti : v.kt0 + ti;
 }
 
 // A tensor map in global memory written before the launch: order the
@@ -336,11 +469,12 @@ __device__ __forceinline__ bool epilogue_vote(int nthreads, bool ok) {
 
 }  // namespace
 
-template <int MODE, int STAGES, int GROUPS, bool kSmemHeap, bool kBatch, bool kPair = false>
+template <int MODE, int STAGES, int GROUPS, bool kSmemHeap, bool kBatch, bool kPair = false, bool kSym = false>
 __global__ void __launch_bounds__(64 + GROUPS * 128, 1)
 tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const ScanParams p) {
   using namespace sm100;
   static_assert(!(kPair && kBatch), "CTA pairs run single requests");
+  static_assert(!kSym || (MODE == kModeHalf && !kBatch && !kPair), "symmetric mode: 16-bit single requests");
   constexpr int SB = kPair ? PAIR_STAGE_BYTES : STAGE_BYTES;  // bytes of one stage in this CTA
   extern __shared__ uint8_t smem_dyn[];
   const uint32_t pad = (1024u - (smem_addr(smem_dyn) & 1023u)) & 1023u;
@@ -412,12 +546,13 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
       uint32_t it = 0;
       bool ok = true;
       for (int64_t itm = item0; ok && itm < n_items; itm += item_step) {
-        const ItemView v = item_view<kBatch>(p, &tmA, &tmB, kPair ? 2 * itm + rank : itm);
+        const ItemView v = item_view<kBatch, kSym>(p, &tmA, &tmB, kPair ? 2 * itm + rank : itm);
         if (kBatch) {
           tensormap_acquire(v.ma);
           tensormap_acquire(v.mb);
         }
-        for (int64_t kt = 0; ok && kt < v.n_ktiles; kt++) {
+        for (int64_t ti = 0; ok && ti < v.n_ktiles - v.kt0; ti++) {
+          const int64_t kt = tile_at<kSym>(v, ti);
           for (int kc = 0; kc < v.n_kchunks; kc++) {
             const uint32_t s = it % STAGES, ph = (it / STAGES) & 1u;
             if (!mbar_wait(&empty[s], ph ^ 1u, abort, p.timeout_ns)) {
@@ -456,8 +591,8 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
       uint32_t it = 0, tile = 0;
       bool ok = true;
       for (int64_t itm = item0; ok && itm < n_items; itm += item_step) {
-        const ItemView v = item_view<kBatch>(p, &tmA, &tmB, kPair ? 2 * itm : itm);
-        for (int64_t kt = 0; ok && kt < v.n_ktiles; kt++, tile++) {
+        const ItemView v = item_view<kBatch, kSym>(p, &tmA, &tmB, kPair ? 2 * itm : itm);
+        for (int64_t ti = 0; ok && ti < v.n_ktiles - v.kt0; ti++, tile++) {
           const uint32_t a = tile & 1u, tph = (tile >> 1) & 1u;
           if (!mbar_wait(&tempty[a], tph ^ 1u, abort, p.timeout_ns)) {
             set_status(p.status, 2);
@@ -519,20 +654,42 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     // a pair's second CTA frees the accumulator on the leader's barrier
     const uint32_t tempty_c0 = kPair ? mapa_shared(smem_addr(&tempty[0]), 0) : 0u;
     const uint32_t tempty_c1 = kPair ? mapa_shared(smem_addr(&tempty[1]), 0) : 0u;
+    // symmetric mode: this warp's stage of mirror keys, after the barriers
+    MirrorStage mst{nullptr, nullptr, 0};
+    float* sthr = nullptr;  // two tiles' thresholds, minima and row ids (tile ti of an item in buffer ti & 1)
+    if (kSym) {
+      uint8_t* sb = reinterpret_cast<uint8_t*>(bars) + 256 + size_t(warp - 2) * kMirrorWarpBytes;
+      mst.key = reinterpret_cast<uint64_t*>(sb);
+      mst.row = reinterpret_cast<int32_t*>(sb + kMirrorStage * 8);
+      sthr = reinterpret_cast<float*>(sb + kMirrorStageBytes);
+    }
+    // copy tile t's thresholds (64 x 16 bytes), minima (2 x 16 bytes) and row ids (64 x 16 bytes) to buffer b
+    auto fetch_thr = [&](int64_t t, int64_t b) {
+      float* dst = sthr + b * kTileThr;
+      cp_async16(dst + lane * 4, p.sym_thr + t * BN + lane * 4);
+      cp_async16(dst + 128 + lane * 4, p.sym_thr + t * BN + 128 + lane * 4);
+      if (lane < 2) cp_async16(dst + BN + lane * 4, p.sym_umin + t * (BN / 32) + lane * 4);
+      int32_t* ids = reinterpret_cast<int32_t*>(dst + kTileIds);
+      cp_async16(ids + lane * 4, p.sym_perm + t * BN + lane * 4);
+      cp_async16(ids + 128 + lane * 4, p.sym_perm + t * BN + 128 + lane * 4);
+    };
     uint32_t tile = 0;
     bool ok = true;
     for (int64_t itm = item0; ok && itm < n_items; itm += item_step) {
-      const ItemView v = item_view<kBatch>(p, &tmA, &tmB, kPair ? 2 * itm + rank : itm);
+      const ItemView v = item_view<kBatch, kSym>(p, &tmA, &tmB, kPair ? 2 * itm + rank : itm);
       const int64_t q = v.qb * BM + row_local;  // output row
       const bool valid = q < v.n_q;
       // row of the data set (its key index for the self rule)
       const int64_t qg = v.q_self ? (valid ? v.q_self_base + v.q_self[q] : -1) : v.q_row0 + q;
+      // symmetric mode: qg is the scanned row, qd its row of the data set (keys and outputs)
+      const int32_t qd = kSym ? (valid ? p.sym_perm[q] : -1) : int32_t(qg);
       KeyHeap heap;
       heap.init(hstore, v.keep);
-      if (valid && v.self_mode && group == 0) heap.offer(make_key(-1.0f, int32_t(qg)));
+      if (valid && v.self_mode && group == 0) heap.offer(make_key(-1.0f, qd));
       const int32_t pa = (MODE == kModeJaccard && valid) ? v.pc[qg] : 0;
       uint32_t thr = pass_threshold<MODE>(heap, pa);
-      for (int64_t kt = 0; kt < v.n_ktiles; kt++, tile++) {
+      for (int64_t ti = 0; ti < v.n_ktiles - v.kt0; ti++, tile++) {
+        const int64_t kt = tile_at<kSym>(v, ti);
         const uint32_t a = tile & 1u, tph = (tile >> 1) & 1u;
         int got = 1;
         if (lane == 0) got = mbar_wait(&tfull[a], tph, abort, p.timeout_ns) ? 1 : 0;
@@ -545,22 +702,50 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         tc_fence_after();
         const uint32_t tbase = tmem_base + (uint32_t(quad * 32) << 16) + a * BN + col_base;
         const int64_t k0 = kt * BN + col_base;
+        const float* tth = nullptr;  // this tile's thresholds, then minima, for this group's columns
+        if (kSym) {
+          // this tile's copy was issued with the tile before (the first of an item: now); the next tile's goes now
+          if (ti == 0) fetch_thr(kt, 0);
+          cp_async_commit();
+          if (ti + 1 < v.n_ktiles - v.kt0) fetch_thr(tile_at<kSym>(v, ti + 1), (ti + 1) & 1);
+          cp_async_commit();
+          cp_async_wait<1>();
+          __syncwarp();
+          tth = sthr + (ti & 1) * kTileThr;
+        }
         uint32_t va[32], vb[32];
         tmem_ld_32x32b_x32(tbase, va);
+        // One chunk of 32 columns.  Symmetric mode: key rows before the
+        // block's own (the first tile of an odd block) belong to the block
+        // before; those past the block also feed their own rows' mailboxes.
+        auto chunk = [&](const uint32_t(&vv)[32], int c, float um) {
+          const int64_t col = k0 + c * 32;
+          if (kSym) {
+            if (col < v.qb * BM) return;  // warp-uniform
+            const int32_t mx = max32_s32(vv);
+            const int32_t* ids = reinterpret_cast<const int32_t*>(tth + kTileIds) + col_base + c * 32;
+            if (valid && (int32_t(thr) > 0 ? mx >= int32_t(thr) : chunk_any<MODE>(vv, thr)))
+              offer_chunk<MODE>(vv, chunk_mask<MODE>(vv, thr), col, v.n_k, v.self_mode, qg, heap, thr, pa, v.pc,
+                                ids);
+            if (col >= (v.qb + 1) * BM)
+              mirror_chunk(vv, mx, um, tth + (col_base + c * 32), ids, col, v.n_k, qd, valid, mst, lane, p);
+          } else if (valid && chunk_any<MODE>(vv, thr)) {
+            offer_chunk<MODE>(vv, chunk_mask<MODE>(vv, thr), col, v.n_k, v.self_mode, qg, heap, thr, pa, v.pc);
+          }
+        };
 #pragma unroll 1
         for (int c = 0; c < NCH; c += 2) {
+          float um0 = 0.0f, um1 = 0.0f;
+          if (kSym) {
+            um0 = tth[BN + col_base / 32 + c];
+            um1 = tth[BN + col_base / 32 + c + 1];
+          }
           tmem_ld_wait();
           tmem_ld_32x32b_x32(tbase + (c + 1) * 32, vb);
-          if (valid && chunk_any<MODE>(va, thr)) {
-            const uint32_t m = chunk_mask<MODE>(va, thr);
-            offer_chunk<MODE>(va, m, k0 + c * 32, v.n_k, v.self_mode, qg, heap, thr, pa, v.pc);
-          }
+          chunk(va, c, um0);
           tmem_ld_wait();
           if (c + 2 < NCH) tmem_ld_32x32b_x32(tbase + (c + 2) * 32, va);
-          if (valid && chunk_any<MODE>(vb, thr)) {
-            const uint32_t m = chunk_mask<MODE>(vb, thr);
-            offer_chunk<MODE>(vb, m, k0 + (c + 1) * 32, v.n_k, v.self_mode, qg, heap, thr, pa, v.pc);
-          }
+          chunk(vb, c + 1, um1);
         }
         tc_fence_before();
         if (kPair && !leader) mbar_arrive_cluster(a ? tempty_c1 : tempty_c0);
@@ -588,7 +773,7 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
       }
       if (group == 0 && valid) {
         const int got = heap.finish();
-        const int64_t orow = q * v.keep;
+        const int64_t orow = (kSym ? int64_t(qd) : q) * v.keep;  // symmetric mode: rows of the data set
         for (int j = 0; j < v.keep; j++) {
           float raw = kHeapInf;
           int32_t idx = -1;
@@ -608,6 +793,7 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
       }
       if (GROUPS > 1) epilogue_sync(GROUPS * 128);  // heaps are reused by the next block
     }
+    if (kSym) mirror_flush(mst, lane, p);  // the keys still staged
   }
 
   tc_fence_before();
@@ -846,6 +1032,68 @@ cudaError_t launch_tc_scan(int mode, const void* Q, int64_t q_rows, int64_t q_ro
   if (mode == kModeInt8) return launch_mode<kModeInt8>(ma, mb, p, grid, variant, stream);
   if (mode == kModeJaccard) return launch_mode<kModeJaccard>(ma, mb, p, grid, variant, stream);
   return launch_mode<kModeHalf>(ma, mb, p, grid, variant, stream);
+}
+
+namespace {
+// A symmetric variant also holds each epilogue warp's stage of mirror keys.
+constexpr size_t sym_smem_bytes(int stages, int groups, int heap_stride) {
+  return smem_bytes(stages, groups, heap_stride) + size_t(groups) * 4 * kMirrorWarpBytes;
+}
+
+template <int STAGES, int GROUPS>
+cudaError_t launch_sym_variant(const CUtensorMap& ma, const CUtensorMap& mb, const ScanParams& p, int grid,
+                               cudaStream_t stream) {
+  auto kern = tc_scan_kernel<kModeHalf, STAGES, GROUPS, true, false, false, true>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_LIMIT));
+  if (e != cudaSuccess) return e;
+  kern<<<grid, 64 + GROUPS * 128, sym_smem_bytes(STAGES, GROUPS, p.heap_stride), stream>>>(ma, mb, p);
+  return cudaGetLastError();
+}
+}  // namespace
+
+bool tc_scan_sym_feasible(int keep) { return sym_smem_bytes(2, 1, keep | 1) <= SMEM_LIMIT; }
+
+cudaError_t launch_tc_scan_sym(const void* X, int64_t rows, int64_t n, int64_t row_bytes, int keep, int grid,
+                               int32_t* out_idx, float* out_raw, int* status, uint64_t timeout_ns,
+                               cudaStream_t stream, int half_type, const float* thr, const float* umin,
+                               const int32_t* perm, int32_t* count, uint64_t* mail, int cap, uint64_t delay_ns) {
+  if (row_bytes % KCB != 0 || n <= 0 || keep < 1 || rows < n || rows % BN != 0 || cap < 1) return cudaErrorInvalidValue;
+  // the tile copies (cp.async, 16 bytes) read thr, umin and perm in whole tiles
+  if ((reinterpret_cast<uintptr_t>(X) & 15) || (reinterpret_cast<uintptr_t>(thr) & 15) ||
+      (reinterpret_cast<uintptr_t>(umin) & 15) || (reinterpret_cast<uintptr_t>(perm) & 15) || !count || !mail)
+    return cudaErrorInvalidValue;
+  if (half_type != kHalfF16 && half_type != kHalfBf16) return cudaErrorInvalidValue;
+  if (!tc_scan_sym_feasible(keep)) return cudaErrorInvalidValue;
+  // the same rows as queries (128-row boxes) and keys (256-row boxes)
+  alignas(64) CUtensorMap ma, mb;
+  if (!make_map(&ma, X, rows, row_bytes, 2, BM, half_type) || !make_map(&mb, X, rows, row_bytes, 2, BN, half_type))
+    return cudaErrorInvalidValue;
+  ScanParams p{};
+  p.n_q = n;
+  p.n_k = n;
+  p.n_kchunks = int(row_bytes / KCB);
+  p.keep = keep;
+  p.heap_stride = keep | 1;
+  p.self_mode = 1;
+  p.out_idx = out_idx;
+  p.out_raw = out_raw;
+  p.status = status;
+  p.timeout_ns = timeout_ns;
+  p.drain_ns = timeout_ns > kDrainNs ? timeout_ns : kDrainNs;
+  p.delay_ns = delay_ns;
+  p.half_type = half_type;
+  p.sym_thr = thr;
+  p.sym_umin = umin;
+  p.sym_count = count;
+  p.sym_mail = mail;
+  p.sym_cap = cap;
+  p.sym_perm = perm;
+  const int odd = keep | 1;
+  if (sym_smem_bytes(4, 2, odd) <= SMEM_LIMIT) return launch_sym_variant<4, 2>(ma, mb, p, grid, stream);
+  if (sym_smem_bytes(3, 2, odd) <= SMEM_LIMIT) return launch_sym_variant<3, 2>(ma, mb, p, grid, stream);
+  if (sym_smem_bytes(4, 1, odd) <= SMEM_LIMIT) return launch_sym_variant<4, 1>(ma, mb, p, grid, stream);
+  if (sym_smem_bytes(3, 1, odd) <= SMEM_LIMIT) return launch_sym_variant<3, 1>(ma, mb, p, grid, stream);
+  return launch_sym_variant<2, 1>(ma, mb, p, grid, stream);
 }
 
 bool tc_scan_variant_feasible(int variant, int keep, bool has_scratch) {

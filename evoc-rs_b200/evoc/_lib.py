@@ -90,6 +90,9 @@ def lib():
             L.evoc_gpu_last_certify.argtypes = [P, C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)]
             L.evoc_gpu_set_wait_limit.argtypes = [P, C.c_uint64, C.c_uint64]
             L.evoc_gpu_last_nndescent.argtypes = [P, C.POINTER(i32), C.POINTER(i64), C.POINTER(i64)]
+            L.evoc_gpu_set_symmetric_scan.argtypes = [P, C.c_int64]
+            L.evoc_gpu_last_symmetric.argtypes = [P, C.POINTER(i64), C.POINTER(i64), C.POINTER(i64),
+                                                  C.POINTER(i64)]
             _bind_optional(L)
             _lib = L
     return _lib
@@ -293,6 +296,19 @@ class Context:
         a, b, c = C.c_int64(0), C.c_int64(0), C.c_int64(0)
         lib().evoc_gpu_last_certify(self.h, C.byref(a), C.byref(b), C.byref(c))
         return {"checked": a.value, "second_pass": b.value, "exact_rescan": c.value}
+
+    def set_symmetric_scan(self, min_rows: int) -> None:
+        """16-bit-form self-joins of at least min_rows rows take the symmetric scan (0 or
+        negative: never, the default)."""
+        if lib().evoc_gpu_set_symmetric_scan(self.h, int(min_rows)) != EVOC_OK:
+            raise ValueError(self.last_error())
+
+    def symmetric_stats(self) -> dict:
+        """The last call's symmetric scan: sample rows of its pre-scan (0: not taken), mailbox
+        capacity per row, the most mailbox keys a row was offered, rows that overflowed."""
+        a, b, c, d = C.c_int64(0), C.c_int64(0), C.c_int64(0), C.c_int64(0)
+        lib().evoc_gpu_last_symmetric(self.h, C.byref(a), C.byref(b), C.byref(c), C.byref(d))
+        return {"sample_rows": a.value, "mailbox_cap": b.value, "max_offers": c.value, "overflowed": d.value}
 
     def close(self) -> None:
         if self.h:

@@ -423,6 +423,26 @@ int evoc_gpu_last_launch_count(const evoc_gpu_ctx* ctx);
  * evoc-rs. */
 int evoc_gpu_set_wait_limit(evoc_gpu_ctx* ctx, uint64_t ns, uint64_t producer_delay_ns);
 
+/* Symmetric scan of the 16-bit form (opt-in; off by default).  A self-join
+ * (all rows as queries, the certificate on) of at least min_rows rows
+ * multiplies each pair of rows once: a query block takes only the key tiles
+ * from its own rows on, and the scores for later rows reach them through
+ * per-row mailboxes, filtered by thresholds from a pre-scan against a strided
+ * 1/16 sample of the rows.  Half the tensor-core work of the plain scan and
+ * the same candidates, but on B200 at 1M x 768 it measured slower end to end
+ * than the plain scan, hence off.  0 or a negative value turns it off.  The
+ * environment variable EVOC_SYM_MIN_ROWS sets it when a context is created.
+ * No counterpart in evoc-rs (its NN-descent evaluates each pair once per join
+ * by its own bookkeeping, src/nndescent/float.rs:552-660). */
+int evoc_gpu_set_symmetric_scan(evoc_gpu_ctx* ctx, int64_t min_rows);
+
+/* The last call's symmetric scan: rows of its sample pre-scan (0 when the
+ * call did not take it), mailbox capacity per row, the most mailbox keys any
+ * row was offered, and rows whose mailbox overflowed (the certificate rescans
+ * those).  Any pointer may be NULL. */
+int evoc_gpu_last_symmetric(const evoc_gpu_ctx* ctx, int64_t* sample_rows, int64_t* mailbox_cap,
+                            int64_t* max_offers, int64_t* overflowed);
+
 /* The last NN-descent call on this context: iterations run, distances its
  * joins computed, and the bytes of each row those distances gathered (the
  * join's algorithmic traffic is distance_evals x row_bytes).  No counterpart
