@@ -156,6 +156,14 @@ __device__ __forceinline__ uint32_t pass_threshold(const KeyHeap& heap, int32_t 
   return raw < 0.0f ? __float_as_uint(-raw) : NEG_INF;  // raw = -score, or MIN_POSITIVE for scores <= 0
 }
 
+// The threshold with a row's seed (16-bit scores only; -inf: none): a score
+// below the seed provably cannot be among the row's kept keys, so the heap
+// admits only scores reaching both.
+template <int MODE>
+__device__ __forceinline__ uint32_t seeded(uint32_t thr, float seed) {
+  return MODE == kModeHalf ? __float_as_uint(fmaxf(__uint_as_float(thr), seed)) : thr;
+}
+
 template <int MODE>
 __device__ __forceinline__ bool passes(uint32_t v, uint32_t thr) {
   return MODE != kModeHalf ? (int32_t(v) >= int32_t(thr)) : (__uint_as_float(v) >= __uint_as_float(thr));
@@ -188,7 +196,8 @@ __device__ __forceinline__ uint32_t pick(const uint32_t (&v)[32], int j) {
 template <int MODE>
 __device__ __forceinline__ void offer_chunk(const uint32_t (&v)[32], uint32_t mask, int64_t col0, int64_t n_k,
                                             bool self_mode, int64_t q, KeyHeap& heap, uint32_t& thr, int32_t pa,
-                                            const int32_t* __restrict__ pc, const int32_t* ids = nullptr) {
+                                            const int32_t* __restrict__ pc, const int32_t* ids = nullptr,
+                                            float seed = -__builtin_huge_valf()) {
   while (mask) {
     const int j = __clz(mask);
     mask &= ~(0x80000000u >> j);
@@ -204,7 +213,7 @@ __device__ __forceinline__ void offer_chunk(const uint32_t (&v)[32], uint32_t ma
       raw = MODE == kModeInt8 ? -__int2float_rn(int32_t(bits)) : raw_cosine(__uint_as_float(bits));
     }
     heap.offer(make_key(raw, ids ? ids[j] : int32_t(key)));  // ids: the chunk's row indices of the data set
-    thr = pass_threshold<MODE>(heap, pa);
+    thr = seeded<MODE>(pass_threshold<MODE>(heap, pa), seed);
   }
 }
 
@@ -687,7 +696,10 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
       heap.init(hstore, v.keep);
       if (valid && v.self_mode && group == 0) heap.offer(make_key(-1.0f, qd));
       const int32_t pa = (MODE == kModeJaccard && valid) ? v.pc[qg] : 0;
-      uint32_t thr = pass_threshold<MODE>(heap, pa);
+      // symmetric mode: the row's mailbox threshold also bounds its own side (a score
+      // below it cannot be among the row's C best over all keys)
+      const float seed = kSym && valid ? p.sym_thr[q] : -__builtin_huge_valf();
+      uint32_t thr = seeded<MODE>(pass_threshold<MODE>(heap, pa), seed);
       for (int64_t ti = 0; ti < v.n_ktiles - v.kt0; ti++, tile++) {
         const int64_t kt = tile_at<kSym>(v, ti);
         const uint32_t a = tile & 1u, tph = (tile >> 1) & 1u;
@@ -726,7 +738,7 @@ tc_scan_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
             const int32_t* ids = reinterpret_cast<const int32_t*>(tth + kTileIds) + col_base + c * 32;
             if (valid && (int32_t(thr) > 0 ? mx >= int32_t(thr) : chunk_any<MODE>(vv, thr)))
               offer_chunk<MODE>(vv, chunk_mask<MODE>(vv, thr), col, v.n_k, v.self_mode, qg, heap, thr, pa, v.pc,
-                                ids);
+                                ids, seed);
             if (col >= (v.qb + 1) * BM)
               mirror_chunk(vv, mx, um, tth + (col_base + c * 32), ids, col, v.n_k, qd, valid, mst, lane, p);
           } else if (valid && chunk_any<MODE>(vv, thr)) {
