@@ -24,6 +24,14 @@
 // on both CTAs' stage-free and accumulator-ready barriers; both CTAs'
 // epilogues arrive on the leader's accumulator-free barrier.
 //
+// Symmetric mode (opt-in; sym.cu has the pre-scan, thresholds and merge):
+// all rows are queries and keys, in a permuted order (pivot groups side by
+// side); query block b multiplies only the key tiles from its own rows on,
+// its own tile first and then the rest from the last tile down.  A score for
+// a key row past the block also counts for that row: if it reaches the row's
+// mailbox threshold it is staged in shared memory and appended to the row's
+// mailbox in HBM, 64 keys per warp at a time.
+//
 // Three score modes share the kernel: 16-bit float dot products (cosine; FP16
 // or BF16 operands, the same instruction and rate), int8 dot products, and
 // binary Jaccard, where the packed bits are expanded to 0/1
